@@ -1,0 +1,157 @@
+// C entry points around the reference's own integral code, compiled in place
+// from the reference sources (see oracle/Makefile) into oracle/_ref/libhfref.so.
+//
+// TEST INFRASTRUCTURE ONLY.  Nothing in the product links or loads this
+// library; tests and the CPU-baseline leg of bench.py use it as the checker.
+//
+// The shell-quartet loops below restate the reference's drivers:
+//   - hfref_eri_packed: Mol::hf_solver::create_repulsion_matrix
+//       (src/scfsolver/hfscf_hf_hamiltonian.cpp:67-112)
+//   - hfref_deriv1: Mol::scf_gradient::calc_coulomb_exchange_integral_centers
+//       (src/gradient/hfscf_grad_ints.cpp:110-151)
+// Shell offsets follow BASIS::Basisset::get_shells (src/basis/hfscf_basis.cpp:244-274)
+// and shell pairs are built for all ordered pairs as in
+// MOLEC::Molecule::create_shell_pairs (src/molecule/hfscf_molecule.cpp:661-669).
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "integrals/hfscf_oseri.hpp"
+#include "math/gamma.hpp"
+#include "math/solid_harmonics.hpp"
+
+namespace {
+
+struct RefBasis {
+  std::vector<BASIS::Shell> shells;
+  std::vector<BASIS::ShellPair> pairs;
+  Eigen::Index ncart = 0, npure = 0;
+};
+
+std::unique_ptr<RefBasis> make_basis(int nshell, const int* L, const double* xyz, const int* nprim,
+                                     const double* alpha, const double* coef, int pure) {
+  auto b = std::make_unique<RefBasis>();
+  b->shells.reserve(static_cast<std::size_t>(nshell));
+  Eigen::Index idx = 0, ids = 0, off = 0;
+  for (int s = 0; s < nshell; ++s) {
+    EigenVector<double> c(nprim[s]), a(nprim[s]);
+    for (int k = 0; k < nprim[s]; ++k) {
+      c(k) = coef[off + k];
+      a(k) = alpha[off + k];
+    }
+    off += nprim[s];
+    Vec3D r(xyz[3 * s], xyz[3 * s + 1], xyz[3 * s + 2]);
+    b->shells.emplace_back(pure != 0, L[s], idx, ids, r, c, a);
+    idx += (L[s] + 1) * (L[s] + 2) / 2;
+    ids += 2 * L[s] + 1;
+  }
+  b->ncart = idx;
+  b->npure = ids;
+  b->pairs.reserve(static_cast<std::size_t>(nshell) * nshell);
+  for (int i = 0; i < nshell; ++i)
+    for (int j = 0; j < nshell; ++j) b->pairs.emplace_back(b->shells[i], b->shells[j]);
+  return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Normalised contraction coefficients, as BASIS::Shell's constructor makes them.
+int hfref_shell_coefs(int L, int nprim, const double* alpha, const double* coef, double* c_out) {
+  EigenVector<double> c(nprim), a(nprim);
+  for (int k = 0; k < nprim; ++k) {
+    c(k) = coef[k];
+    a(k) = alpha[k];
+  }
+  Vec3D r(0.0, 0.0, 0.0);
+  BASIS::Shell sh(false, L, 0, 0, r, c, a);
+  for (int k = 0; k < nprim; ++k) c_out[k] = sh.c()(k);
+  return 0;
+}
+
+// Cartesian -> pure matrix, (L+1)(L+2)/2 rows by 2L+1 columns, row-major.
+int hfref_ylm(int L, double* out) {
+  EigenMatrix<double> m = hfscfmath::Ylm_transmat(L);
+  for (Eigen::Index i = 0; i < m.rows(); ++i)
+    for (Eigen::Index j = 0; j < m.cols(); ++j) out[i * m.cols() + j] = m(i, j);
+  return 0;
+}
+
+double hfref_boys(double m, double T) { return extramath::F_nu(m, T); }
+
+// Number of basis functions for the given shells.
+long long hfref_nbf(int nshell, const int* L, int pure) {
+  long long n = 0;
+  for (int s = 0; s < nshell; ++s) n += pure ? 2 * L[s] + 1 : (L[s] + 1) * (L[s] + 2) / 2;
+  return n;
+}
+
+// Packed 8-fold ERI vector, length n(n+1)(n^2+n+2)/8, filled by the reference's
+// Erios::compute_contracted_shell_quartet over all unique shell quartets.
+int hfref_eri_packed(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
+                     const double* coef, int pure, double cutoff, int do_screen, double* eri_out) {
+  auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, pure);
+  const Eigen::Index n = pure ? b->npure : b->ncart;
+  const Eigen::Index len = n * (n + 1) * (n * n + n + 2) / 8;
+  EigenVector<double> eri(len);
+  eri.setZero();
+  ERIOS::Erios os(pure != 0, cutoff);
+  if (do_screen) {
+    os.init_screen(b->ncart);
+    for (int i = 0; i < nshell; ++i)
+      for (int j = i; j < nshell; ++j) os.compute_screen_matrix(b->pairs[i * nshell + j]);
+  }
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < nshell; ++i)
+    for (int j = i; j < nshell; ++j) {
+      const Eigen::Index ij = hfscfmath::index_ij(i, j);
+      for (int k = 0; k < nshell; ++k)
+        for (int l = k; l < nshell; ++l) {
+          const Eigen::Index kl = hfscfmath::index_ij(k, l);
+          if (ij > kl) continue;
+          os.compute_contracted_shell_quartet(eri, b->pairs[i * nshell + j], b->pairs[k * nshell + l],
+                                              do_screen != 0);
+        }
+    }
+  for (Eigen::Index p = 0; p < len; ++p) eri_out[p] = eri(p);
+  return 0;
+}
+
+// Nine packed derivative-ERI tensors (d/dXa, d/dXb, d/dXc, d/dYa, ..., d/dZc), each
+// of the packed 8-fold length, from Erios::compute_contracted_shell_quartet_deriv1.
+// coords[3] selects the Cartesian directions, as the reference's out_of_plane mask.
+int hfref_deriv1(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
+                 const double* coef, int pure, double cutoff, const int* coords, double* out9) {
+  auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, pure);
+  const Eigen::Index n = pure ? b->npure : b->ncart;
+  const Eigen::Index len = n * (n + 1) * (n * n + n + 2) / 8;
+  std::vector<bool> mask = {coords[0] != 0, coords[1] != 0, coords[2] != 0};
+  std::vector<tensor4dmath::symm4dTensor<double>> t(9);
+  for (int c = 0; c < 3; ++c)
+    if (mask[c])
+      for (int k = 0; k < 3; ++k) t[3 * c + k] = tensor4dmath::symm4dTensor<double>(n);
+  ERIOS::Erios os(pure != 0, cutoff);
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < nshell; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const Eigen::Index ij = hfscfmath::index_ij(i, j);
+      for (int k = 0; k < nshell; ++k)
+        for (int l = 0; l <= k; ++l) {
+          const Eigen::Index kl = hfscfmath::index_ij(k, l);
+          if (ij > kl) continue;
+          os.compute_contracted_shell_quartet_deriv1(t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8],
+                                                     b->pairs[i * nshell + j], b->pairs[k * nshell + l], mask);
+        }
+    }
+  for (int q = 0; q < 9; ++q) {
+    if (!mask[q / 3]) {
+      for (Eigen::Index p = 0; p < len; ++p) out9[q * len + p] = 0.0;
+      continue;
+    }
+    for (Eigen::Index p = 0; p < len; ++p) out9[q * len + p] = t[q][p];
+  }
+  return 0;
+}
+
+}  // extern "C"
