@@ -1,0 +1,942 @@
+"""Generator of the per-class ERI device code (straight-line CUDA).
+
+For every shell-quartet class (la lb|lc ld) with la >= lb, lc >= ld, L <= 2 it
+emits a device function that computes one contracted Cartesian block by the
+Head-Gordon-Pople scheme:
+
+  * Obara-Saika vertical recurrence (VRR) per primitive quartet, building
+    [e0|f0]^(0) for la <= |e| <= la+lb, lc <= |f| <= lc+ld from
+    [00|00]^(m) = K_ab K_cd 2 pi^2.5 / (p q sqrt(p+q)) F_m(T);
+  * contraction over primitive pairs into register accumulators;
+  * horizontal recurrence (HRR) on the contracted set,
+    (a b+1_i| = (a+1_i b| + AB_i (a b|, then the same on the ket;
+  * optionally the Cartesian -> pure transform with the solid-harmonic
+    coefficients of src/math/solid_harmonics.cpp:30-108.
+
+It also emits, per class, the adjoint gradient function: the same VRR run one
+order higher, accumulated four ways (unweighted and weighted by 2 alpha of
+centres A, B, C), HRR to the shifted classes, and contraction with a
+Cartesian weight block W, giving dE/dA, dE/dB, dE/dC (dE/dD by translational
+invariance).  The rule d/dA_i g_a = 2 alpha g_{a+1_i} - a_i g_{a-1_i} is the
+one the reference applies (src/integrals/hfscf_oserideriv1.cpp:227-231).
+
+Cartesian components are ordered as the reference orders them,
+l = L-i, m = i-j, n = j (src/integrals/hfscf_shell.cpp:27-40).
+
+Usage: python gen_eri.py OUT.cuh   (prints per-class operation counts)
+"""
+from __future__ import annotations
+
+import json
+import math
+import sys
+from fractions import Fraction
+
+LMAX = 2
+XYZ = "xyz"
+
+
+def cart(L):
+    return [(L - i, i - j, j) for i in range(L + 1) for j in range(i + 1)]
+
+
+def cidx(c):
+    L = sum(c)
+    return cart(L).index(tuple(c))
+
+
+def add(v, i, k=1):
+    w = list(v)
+    w[i] += k
+    return tuple(w)
+
+
+def tag(v):
+    return "".join(str(x) for x in v)
+
+
+# ---------------------------------------------------------------------------
+# Real solid harmonics in the reference's convention (Cartesian x^L normalised,
+# columns m = -L..L, prefactor 2^-L sqrt(2 (L-|m|)!/(L+|m|)!) for m != 0).
+# ---------------------------------------------------------------------------
+def ylm(L):
+    nc = (L + 1) * (L + 2) // 2
+    out = [[0.0] * (2 * L + 1) for _ in range(nc)]
+    for mval in range(-L, L + 1):
+        m = abs(mval)
+        prefac = 2.0 ** (-L)
+        if m:
+            prefac *= math.sqrt(math.factorial(L - m) * 2.0 / math.factorial(L + m))
+        for k in range((L - m) // 2 + 1):
+            ffac = (-1) ** k * math.comb(L, k) * math.comb(2 * (L - k), L)
+            if m:
+                ffac *= math.factorial(L - 2 * k) / math.factorial(L - 2 * k - m)
+            ffac *= prefac
+            for a in range(k + 1):
+                afac = math.comb(k, a) * ffac
+                for b in range(a + 1):
+                    fac = math.comb(a, b) * afac
+                    zexp = 2 * (b - k) + L - m
+                    yexp = 2 * (a - b)
+                    if m == 0:
+                        ii = yexp + zexp
+                        out[ii * (ii + 1) // 2 + zexp][L + mval] += fac
+                        continue
+                    for p in range(m + 1):
+                        r = (m - p) % 4
+                        f = ({0: 1, 2: -1}.get(r, 0)) if mval > 0 else ({1: 1, 3: -1}.get(r, 0))
+                        if f:
+                            ii = yexp + m - p + zexp
+                            out[ii * (ii + 1) // 2 + zexp][L + mval] += f * math.comb(m, p) * fac
+    return out
+
+
+class Emitter:
+    """Collects straight-line statements and counts floating-point operations."""
+
+    def __init__(self, indent="  "):
+        self.lines = []
+        self.indent = indent
+        self.flops = 0
+
+    def emit(self, s, flops=0):
+        self.lines.append(self.indent + s)
+        self.flops += flops
+
+
+def lit(x):
+    """A floating literal typed by the template parameter R."""
+    if float(x).is_integer():
+        return f"R({int(x)})"
+    return f"R({repr(float(x))})"
+
+
+# ---------------------------------------------------------------------------
+# VRR: [e0|f0]^(m)
+# ---------------------------------------------------------------------------
+class VRR:
+    def __init__(self, em: Emitter, prefix="v"):
+        self.em = em
+        self.memo = {}
+        self.prefix = prefix
+        self.consts = {}
+
+    def kconst(self, base, k):
+        """k * base as a named constant (base is inv2p, inv2q or inv2pq)."""
+        if k == 1:
+            return base
+        key = (base, k)
+        if key not in self.consts:
+            name = f"{base}_{k}"
+            self.em.emit(f"const R {name} = R({k}) * {base};", 1)
+            self.consts[key] = name
+        return self.consts[key]
+
+    def get(self, e, f, m):
+        key = (e, f, m)
+        if key in self.memo:
+            return self.memo[key]
+        name = f"{self.prefix}_{tag(e)}_{tag(f)}_{m}"
+        if sum(f) > 0:
+            # ket vertical step on the direction with the largest f_i
+            i = max(range(3), key=lambda d: (f[d], -d))
+            f1 = add(f, i, -1)
+            a = self.get(e, f1, m)
+            b = self.get(e, f1, m + 1)
+            expr = f"QC{XYZ[i]} * {a} + WQ{XYZ[i]} * {b}"
+            fl = 3
+            if f1[i] > 0:
+                f2 = add(f1, i, -1)
+                c = self.get(e, f2, m)
+                d = self.get(e, f2, m + 1)
+                expr += f" + {self.kconst('inv2q', f1[i])} * ({c} - rq * {d})"
+                fl += 3
+            if e[i] > 0:
+                e1 = add(e, i, -1)
+                g = self.get(e1, f1, m + 1)
+                expr += f" + {self.kconst('inv2pq', e[i])} * {g}"
+                fl += 2
+        elif sum(e) > 0:
+            i = max(range(3), key=lambda d: (e[d], -d))
+            e1 = add(e, i, -1)
+            a = self.get(e1, f, m)
+            b = self.get(e1, f, m + 1)
+            expr = f"PA{XYZ[i]} * {a} + WP{XYZ[i]} * {b}"
+            fl = 3
+            if e1[i] > 0:
+                e2 = add(e1, i, -1)
+                c = self.get(e2, f, m)
+                d = self.get(e2, f, m + 1)
+                expr += f" + {self.kconst('inv2p', e1[i])} * ({c} - rp * {d})"
+                fl += 3
+        else:
+            expr = f"F[{m}]"
+            fl = 0
+            name = f"F[{m}]"
+            self.memo[key] = name
+            return name
+        self.em.emit(f"const R {name} = {expr};", fl)
+        self.memo[key] = name
+        return name
+
+
+def vrr_targets(lo_e, hi_e, lo_f, hi_f):
+    out = []
+    for le in range(lo_e, hi_e + 1):
+        for e in cart(le):
+            for lf in range(lo_f, hi_f + 1):
+                for f in cart(lf):
+                    out.append((e, f))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# HRR on contracted [e0|f0] -> (a b|c d)
+# ---------------------------------------------------------------------------
+class HRR:
+    def __init__(self, em: Emitter, acc, prefix="h"):
+        self.em = em
+        self.acc = acc  # function (e, f) -> accumulator expression
+        self.kmemo = {}
+        self.bmemo = {}
+        self.prefix = prefix
+
+    def ket(self, e, c, d):
+        key = (e, c, d)
+        if key in self.kmemo:
+            return self.kmemo[key]
+        if sum(d) == 0:
+            name = self.acc(e, c)
+        else:
+            i = max(range(3), key=lambda k: (d[k], -k))
+            d1 = add(d, i, -1)
+            a = self.ket(e, add(c, i), d1)
+            b = self.ket(e, c, d1)
+            name = f"{self.prefix}k_{tag(e)}_{tag(c)}_{tag(d)}"
+            self.em.emit(f"const R {name} = {a} + CD{XYZ[i]} * {b};", 2)
+        self.kmemo[key] = name
+        return name
+
+    def bra(self, a, b, c, d):
+        key = (a, b, c, d)
+        if key in self.bmemo:
+            return self.bmemo[key]
+        if sum(b) == 0:
+            name = self.ket(a, c, d)
+        else:
+            i = max(range(3), key=lambda k: (b[k], -k))
+            b1 = add(b, i, -1)
+            x = self.bra(add(a, i), b1, c, d)
+            y = self.bra(a, b1, c, d)
+            name = f"{self.prefix}b_{tag(a)}_{tag(b)}_{tag(c)}_{tag(d)}"
+            self.em.emit(f"const R {name} = {x} + AB{XYZ[i]} * {y};", 2)
+        self.bmemo[key] = name
+        return name
+
+
+PRIM_HEADER = """\
+      // primitive-quartet scalars
+      const R pq = p + q;
+      const R ipq = R(1) / pq;
+      const R rho = p * q * ipq;
+      const R rp = q * ipq;          // rho / p
+      const R rq = p * ipq;          // rho / q
+      const R inv2p = R(0.5) / p;
+      const R inv2q = R(0.5) / q;
+      const R inv2pq = R(0.5) * ipq;
+      const R PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+      const R WPx = -rp * PQx, WPy = -rp * PQy, WPz = -rp * PQz;
+      const R WQx = rq * PQx, WQy = rq * PQy, WQz = rq * PQz;
+      const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+      const R pre = Kab * Kcd * R(PI_2_5) / (p * q * sqrt_t(pq));
+"""
+PRIM_HEADER_FLOPS = 1 + 1 + 2 + 1 + 1 + 1 + 1 + 1 + 3 + 3 + 3 + 6 + 5
+
+
+def ncart(L):
+    return (L + 1) * (L + 2) // 2
+
+
+def gen_eri_class(la, lb, lc, ld):
+    """Device function computing the contracted Cartesian block of class (la lb|lc ld)."""
+    L = la + lb + lc + ld
+    em = Emitter("      ")
+    vrr = VRR(em)
+    targets = vrr_targets(la, la + lb, lc, lc + ld)
+    names = [vrr.get(e, f, 0) for e, f in targets]
+    prim_body = list(em.lines)
+    prim_flops = em.flops + PRIM_HEADER_FLOPS + len(targets)  # + accumulation
+    acc_index = {t: n for n, t in enumerate(targets)}
+    em2 = Emitter("  ")
+    hrr = HRR(em2, lambda e, f: f"acc[{acc_index[(e, f)]}]")
+    outs = []
+    for a in cart(la):
+        for b in cart(lb):
+            for c in cart(lc):
+                for d in cart(ld):
+                    outs.append(hrr.bra(a, b, c, d))
+    nout = len(outs)
+    s = []
+    fn = f"eri_{la}{lb}{lc}{ld}"
+    s.append(f"// ({'spdf'[la]}{'spdf'[lb]}|{'spdf'[lc]}{'spdf'[ld]}): {len(targets)} contracted VRR targets, "
+             f"{len(vrr.memo)} VRR values, {nout} outputs")
+    s.append("template <typename R>")
+    s.append(f"__device__ __forceinline__ void {fn}(const PrimPair<R>* __restrict__ bp, int nbp, "
+             f"const PrimPair<R>* __restrict__ kp, int nkp, R ABx, R ABy, R ABz, R CDx, R CDy, R CDz, "
+             f"const BoysTable<R>& boys, R* __restrict__ out) {{")
+    s.append(f"  R acc[{len(targets)}];")
+    s.append(f"#pragma unroll")
+    s.append(f"  for (int t = 0; t < {len(targets)}; ++t) acc[t] = R(0);")
+    s.append("  for (int ib = 0; ib < nbp; ++ib) {")
+    s.append("    const R p = bp[ib].p, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
+    s.append("    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].K;")
+    s.append("    for (int ik = 0; ik < nkp; ++ik) {")
+    s.append("      const R q = kp[ik].p, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
+    s.append("      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].K;")
+    s.append(PRIM_HEADER.rstrip("\n"))
+    s.append(f"      R F[{L + 1}];")
+    s.append(f"      boys.template eval<{L}>(T, pre, F);")
+    s += prim_body
+    for t, n in enumerate(names):
+        s.append(f"      acc[{t}] += {n};")
+    s.append("    }")
+    s.append("  }")
+    s += em2.lines
+    for o, n in enumerate(outs):
+        s.append(f"  out[{o}] = {n};")
+    s.append("}")
+    meta = {"class": [la, lb, lc, ld], "vrr_targets": len(targets), "vrr_values": len(vrr.memo),
+            "prim_flops": prim_flops, "hrr_flops": em2.flops, "nout": nout, "boys_m": L}
+    return "\n".join(s), meta
+
+
+def gen_pure(la, lb, lc, ld):
+    """Cartesian -> pure transform of one block, index by index (as TRANSFORM::transform,
+    src/integrals/hfscf_transform.cpp:80-154), skipping zero coefficients."""
+    Ls = (la, lb, lc, ld)
+    ncs = [ncart(x) for x in Ls]
+    nps = [2 * x + 1 for x in Ls]
+    Y = [ylm(x) for x in Ls]
+    em = Emitter("  ")
+    cur = {}
+    dims = list(ncs)
+    # current[(i0,i1,i2,i3)] -> expression name
+    import itertools
+    for idx in itertools.product(*[range(n) for n in ncs]):
+        flat = ((idx[0] * ncs[1] + idx[1]) * ncs[2] + idx[2]) * ncs[3] + idx[3]
+        cur[idx] = f"in[{flat}]"
+    for stage in range(4):
+        if Ls[stage] < 2:
+            # L = 0: identity; L = 1: a permutation (pure p = y, z, x) -- no arithmetic
+            new = {}
+            newdims = list(dims)
+            newdims[stage] = nps[stage]
+            for idx in itertools.product(*[range(n) for n in newdims]):
+                col = idx[stage]
+                src = [r for r in range(ncs[stage]) if Y[stage][r][col] != 0.0]
+                assert len(src) == 1 and Y[stage][src[0]][col] == 1.0
+                j = list(idx)
+                j[stage] = src[0]
+                new[idx] = cur[tuple(j)]
+            cur, dims = new, newdims
+            continue
+        new = {}
+        newdims = list(dims)
+        newdims[stage] = nps[stage]
+        for idx in itertools.product(*[range(n) for n in newdims]):
+            col = idx[stage]
+            terms = []
+            for r in range(ncs[stage]):
+                c = Y[stage][r][col]
+                if c != 0.0:
+                    j = list(idx)
+                    j[stage] = r
+                    terms.append((c, cur[tuple(j)]))
+            name = f"t{stage}_{''.join(map(str, idx))}"
+            expr = " + ".join(f"{lit(c)} * {v}" if c != 1.0 else v for c, v in terms)
+            em.emit(f"const R {name} = {expr};", 2 * len(terms) - 1)
+            new[idx] = name
+        cur, dims = new, newdims
+    body = list(em.lines)
+    nout = nps[0] * nps[1] * nps[2] * nps[3]
+    for idx in itertools.product(*[range(n) for n in nps]):
+        flat = ((idx[0] * nps[1] + idx[1]) * nps[2] + idx[2]) * nps[3] + idx[3]
+        body.append(f"  out[{flat}] = {cur[idx]};")
+    fn = f"to_pure_{la}{lb}{lc}{ld}"
+    s = ["template <typename R>",
+         f"__device__ __forceinline__ void {fn}(const R* __restrict__ in, R* __restrict__ out) {{"]
+    s += body
+    s.append("}")
+    return "\n".join(s), em.flops
+
+
+def gen_pure_T(la, lb, lc, ld):
+    """Transpose transform: Cartesian weights from pure weights (for the gradient),
+    W_cart[abcd] = sum_ijkl Y[a][i] Y[b][j] Y[c][k] Y[d][l] W_pure[ijkl]."""
+    import itertools
+    Ls = (la, lb, lc, ld)
+    ncs = [ncart(x) for x in Ls]
+    nps = [2 * x + 1 for x in Ls]
+    Y = [ylm(x) for x in Ls]
+    em = Emitter("  ")
+    cur = {}
+    for idx in itertools.product(*[range(n) for n in nps]):
+        flat = ((idx[0] * nps[1] + idx[1]) * nps[2] + idx[2]) * nps[3] + idx[3]
+        cur[idx] = f"in[{flat}]"
+    dims = list(nps)
+    for stage in range(4):
+        new = {}
+        newdims = list(dims)
+        newdims[stage] = ncs[stage]
+        for idx in itertools.product(*[range(n) for n in newdims]):
+            row = idx[stage]
+            terms = []
+            for col in range(nps[stage]):
+                c = Y[stage][row][col]
+                if c != 0.0:
+                    j = list(idx)
+                    j[stage] = col
+                    terms.append((c, cur[tuple(j)]))
+            if not terms:
+                new[idx] = "R(0)"
+                continue
+            if len(terms) == 1 and terms[0][0] == 1.0:
+                new[idx] = terms[0][1]
+                continue
+            name = f"u{stage}_{''.join(map(str, idx))}"
+            expr = " + ".join(f"{lit(c)} * {v}" if c != 1.0 else v for c, v in terms)
+            em.emit(f"const R {name} = {expr};", 2 * len(terms) - 1)
+            new[idx] = name
+        cur, dims = new, newdims
+    body = list(em.lines)
+    for idx in itertools.product(*[range(n) for n in ncs]):
+        flat = ((idx[0] * ncs[1] + idx[1]) * ncs[2] + idx[2]) * ncs[3] + idx[3]
+        body.append(f"  out[{flat}] = {cur[idx]};")
+    fn = f"from_pure_{la}{lb}{lc}{ld}"
+    s = ["template <typename R>",
+         f"__device__ __forceinline__ void {fn}(const R* __restrict__ in, R* __restrict__ out) {{"]
+    s += body
+    s.append("}")
+    return "\n".join(s)
+
+
+# ---------------------------------------------------------------------------
+# Adjoint gradient: contraction of W with d(ab|cd)/dA, dB, dC.
+# ---------------------------------------------------------------------------
+def grad_sets(la, lb, lc, ld):
+    """Contracted [e0|f0] sets the adjoint gradient needs, by weight."""
+    em = Emitter("      ")
+    vrr = VRR(em)
+    # Which contracted [e0|f0] sets are needed, by weight.
+    need = {"U": set(), "A": set(), "B": set(), "C": set()}
+    for le in range(max(la - 1, 0), la + lb):          # (a-1 b|cd) and (a b-1|cd): |e| <= la+lb-1
+        for lf in range(lc, lc + ld + 1):
+            for e in cart(le):
+                for f in cart(lf):
+                    need["U"].add((e, f))
+    for le in range(la, la + lb + 1):                   # (ab|c-1 d), (ab|c d-1): |f| <= lc+ld-1
+        for lf in range(max(lc - 1, 0), lc + ld):
+            for e in cart(le):
+                for f in cart(lf):
+                    need["U"].add((e, f))
+    for le in range(la + 1, la + lb + 2):
+        for lf in range(lc, lc + ld + 1):
+            for e in cart(le):
+                for f in cart(lf):
+                    need["A"].add((e, f))
+    for le in range(la, la + lb + 2):
+        for lf in range(lc, lc + ld + 1):
+            for e in cart(le):
+                for f in cart(lf):
+                    need["B"].add((e, f))
+    for le in range(la, la + lb + 1):
+        for lf in range(lc + 1, lc + ld + 2):
+            for e in cart(le):
+                for f in cart(lf):
+                    need["C"].add((e, f))
+    order = {k: sorted(v, key=lambda t: (sum(t[0]), cidx(t[0]), sum(t[1]), cidx(t[1]))) for k, v in need.items()}
+    return order
+
+
+def grad_terms(la, lb, lc, ld):
+    """For every (centre, direction): list of (W index, [(coef, set, a, b, c, d), ...])."""
+    gsum = {(c, d): [] for c in "ABC" for d in range(3)}
+    w = 0
+    for a in cart(la):
+        for b in cart(lb):
+            for c in cart(lc):
+                for d in cart(ld):
+                    for dr in range(3):
+                        t = [(1, "A", add(a, dr), b, c, d)]
+                        if a[dr] > 0:
+                            t.append((-a[dr], "U", add(a, dr, -1), b, c, d))
+                        gsum[("A", dr)].append((w, t))
+                        t = [(1, "B", a, add(b, dr), c, d)]
+                        if b[dr] > 0:
+                            t.append((-b[dr], "U", a, add(b, dr, -1), c, d))
+                        gsum[("B", dr)].append((w, t))
+                        t = [(1, "C", a, b, add(c, dr), d)]
+                        if c[dr] > 0:
+                            t.append((-c[dr], "U", a, b, add(c, dr, -1), d))
+                        gsum[("C", dr)].append((w, t))
+                    w += 1
+    return gsum
+
+
+def gen_grad_class(la, lb, lc, ld):
+    L = la + lb + lc + ld + 1
+    em = Emitter("      ")
+    vrr = VRR(em)
+    order = grad_sets(la, lb, lc, ld)
+    allt = sorted(set().union(*[set(v) for v in order.values()]),
+                  key=lambda t: (sum(t[0]), cidx(t[0]), sum(t[1]), cidx(t[1])))
+    vals = {t: vrr.get(t[0], t[1], 0) for t in allt}
+    prim_body = list(em.lines)
+    idx = {}
+    n = 0
+    for k in ("U", "A", "B", "C"):
+        for t in order[k]:
+            idx[(k, t)] = n
+            n += 1
+    nacc = n
+    # HRR + contraction
+    em2 = Emitter("  ")
+    hr = {k: HRR(em2, (lambda kk: (lambda e, f: f"acc[{idx[(kk, (e, f))]}]"))(k), prefix=f"h{k}")
+          for k in ("U", "A", "B", "C")}
+    gt = grad_terms(la, lb, lc, ld)
+    gsum = {}
+    for key, items in gt.items():
+        gsum[key] = []
+        for wi, terms in items:
+            t = [hr[terms[0][1]].bra(*terms[0][2:])]
+            if len(terms) > 1:
+                t.append((-terms[1][0], hr["U"].bra(*terms[1][2:])))
+            gsum[key].append((wi, t))
+    for (cen, dr), items in gsum.items():
+        terms = []
+        for wi, t in items:
+            e = t[0]
+            if len(t) > 1:
+                k, u = t[1]
+                e = f"({e} - {lit(k)} * {u})"
+            terms.append(f"W[{wi}] * {e}")
+        em2.emit(f"g{cen}[{dr}] = " + " + ".join(terms) + ";", 2 * len(terms) + sum(2 for _, t in items if len(t) > 1))
+    fn = f"grad_{la}{lb}{lc}{ld}"
+    s = [f"// adjoint gradient of ({'spdf'[la]}{'spdf'[lb]}|{'spdf'[lc]}{'spdf'[ld]}): {nacc} accumulators, "
+         f"{len(vrr.memo)} VRR values"]
+    s.append("template <typename R>")
+    s.append(f"__device__ __forceinline__ void {fn}(const PrimPair<R>* __restrict__ bp, const R* __restrict__ ea, "
+             f"const R* __restrict__ eb, int nbp, const PrimPair<R>* __restrict__ kp, const R* __restrict__ ec, int nkp, "
+             f"R ABx, R ABy, R ABz, R CDx, R CDy, R CDz, const BoysTable<R>& boys, const R* __restrict__ W, "
+             f"R* __restrict__ gA, R* __restrict__ gB, R* __restrict__ gC) {{")
+    s.append(f"  R acc[{nacc}];")
+    s.append("#pragma unroll")
+    s.append(f"  for (int t = 0; t < {nacc}; ++t) acc[t] = R(0);")
+    s.append("  for (int ib = 0; ib < nbp; ++ib) {")
+    s.append("    const R p = bp[ib].p, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
+    s.append("    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].K;")
+    s.append("    const R wa = R(2) * ea[ib], wb = R(2) * eb[ib];")
+    s.append("    for (int ik = 0; ik < nkp; ++ik) {")
+    s.append("      const R q = kp[ik].p, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
+    s.append("      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].K;")
+    s.append("      const R wc = R(2) * ec[ik];")
+    s.append(PRIM_HEADER.rstrip("\n"))
+    s.append(f"      R F[{L + 1}];")
+    s.append(f"      boys.template eval<{L}>(T, pre, F);")
+    s += prim_body
+    for k, wname in (("U", None), ("A", "wa"), ("B", "wb"), ("C", "wc")):
+        for t in order[k]:
+            v = vals[t]
+            s.append(f"      acc[{idx[(k, t)]}] += {v};" if wname is None else
+                     f"      acc[{idx[(k, t)]}] += {wname} * {v};")
+    s.append("    }")
+    s.append("  }")
+    s += em2.lines
+    s.append("}")
+    meta = {"class": [la, lb, lc, ld], "accumulators": nacc, "vrr_values": len(vrr.memo),
+            "prim_flops": em.flops + PRIM_HEADER_FLOPS + 2 * nacc, "hrr_flops": em2.flops, "boys_m": L}
+    return "\n".join(s), meta
+
+
+def classes():
+    pairs = [(a, b) for a in range(LMAX + 1) for b in range(a + 1)]  # ss ps pp ds dp dd
+    out = []
+    for i, (la, lb) in enumerate(pairs):
+        for j, (lc, ld) in enumerate(pairs):
+            if j <= i:
+                out.append((la, lb, lc, ld))
+    return pairs, out
+
+
+GRAD_STRAIGHT_MAX_VRR = 250   # larger gradient classes run in table mode
+
+
+def class_args_sig():
+    return ("const PrimPair<R>* __restrict__ bp, int nbp, const PrimPair<R>* __restrict__ kp, int nkp, "
+            "R ABx, R ABy, R ABz, R CDx, R CDy, R CDz, const BoysTable<R>& boys, R* __restrict__ out")
+
+
+GRAD_SIG = ("const PrimPair<R>* __restrict__ bp, const R* __restrict__ ea, const R* __restrict__ eb, int nbp, "
+            "const PrimPair<R>* __restrict__ kp, const R* __restrict__ ec, int nkp, R ABx, R ABy, R ABz, "
+            "R CDx, R CDy, R CDz, const BoysTable<R>& boys, const R* __restrict__ W, R* __restrict__ gA, "
+            "R* __restrict__ gB, R* __restrict__ gC")
+GRAD_ARGS = "bp, ea, eb, nbp, kp, ec, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, W, gA, gB, gC"
+
+
+def common_header():
+    out = ["// GENERATED by gen_eri.py -- do not edit.", "#pragma once", '#include "../hfgpu_common.cuh"', "",
+           "// Cartesian -> pure coefficients for L = 0, 1, 2 (ncart x npure, row-major),",
+           "// hfscfmath::Ylm_transmat (src/math/solid_harmonics.cpp:16-27).",
+           "static __constant__ double c_ylm[3][30] = {"]
+    for L in range(3):
+        Y = ylm(L)
+        flat = [Y[r][c] for r in range(len(Y)) for c in range(2 * L + 1)]
+        flat += [0.0] * (30 - len(flat))
+        out.append("  {" + ", ".join(repr(float(x)) for x in flat) + "},")
+    out.append("};")
+    out.append("")
+    out.append("template <int LA, int LB, int LC, int LD>")
+    out.append("struct ClassCode;")
+    return "\n".join(out) + "\n"
+
+
+def class_header(c):
+    la, lb, lc, ld = c
+    t = f"{la}{lb}{lc}{ld}"
+    parts = ["// GENERATED by gen_eri.py -- do not edit.", "#pragma once", '#include "common.cuh"', ""]
+    code, m = gen_eri_class(*c)
+    parts += [code, ""]
+    pc, pf = gen_pure(*c)
+    parts += [pc, ""]
+    parts += [gen_pure_T(*c), ""]
+    m["pure_flops"] = pf
+    # the adjoint gradient: straight-line for small classes, op tables for large ones
+    code_g, mg = gen_grad_class(*c)
+    straight = mg["vrr_values"] <= GRAD_STRAIGHT_MAX_VRR
+    if not straight:
+        code_g, mg = gen_grad_table(*c)
+    parts += [code_g, ""]
+    mg["table"] = not straight
+    parts.append(f"template <>")
+    parts.append(f"struct ClassCode<{la}, {lb}, {lc}, {ld}> {{")
+    parts.append(f"  static constexpr bool kGradTable = {'false' if straight else 'true'};")
+    parts.append(f"  using GradTab = {'void' if straight else 'GradTable' + t};")
+    parts.append(f"  template <typename R>")
+    parts.append(f"  static __device__ __forceinline__ void eri({class_args_sig()}) {{")
+    parts.append(f"    eri_{t}<R>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out);")
+    parts.append("  }")
+    parts.append("  template <typename R>")
+    parts.append(f"  static __device__ __forceinline__ void to_pure(const R* __restrict__ in, R* __restrict__ out) {{ to_pure_{t}<R>(in, out); }}")
+    parts.append("  template <typename R>")
+    parts.append(f"  static __device__ __forceinline__ void from_pure(const R* __restrict__ in, R* __restrict__ out) {{ from_pure_{t}<R>(in, out); }}")
+    if straight:
+        parts.append("  template <typename R>")
+        parts.append(f"  static __device__ __forceinline__ void grad({GRAD_SIG}) {{ grad_{t}<R>({GRAD_ARGS}); }}")
+    parts.append("};")
+    return "\n".join(parts) + "\n", m, mg
+
+
+INST_TEMPLATE = """// GENERATED by gen_eri.py -- do not edit.
+#include "../hfgpu_kernels.cuh"
+#include "class_{t}.cuh"
+#include "../hfgpu_launch.h"
+
+namespace hfgpu {{
+template <typename R>
+static void launch_quartet(const QuartetArgs<R>& a, const int2* q, int nq, cudaStream_t s) {{
+  if (nq <= 0) return;
+  quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 127) / 128, 128, 0, s>>>(a, q, nq);
+}}
+template <typename R>
+static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, int grid, cudaStream_t s) {{
+  if (nq <= 0) return;
+  grad_kernel<{la}, {lb}, {lc}, {ld}, R><<<grid, 128, 0, s>>>(a, pure, q, nq);
+}}
+template <typename CC, int NCART>
+static int grad_scratch_slots_impl() {{
+  if constexpr (CC::kGradTable) {{
+    using Tab = typename CC::GradTab;
+    return Tab::NVSLOT + Tab::NHSLOT + 3 * NCART;
+  }} else {{
+    return 0;
+  }}
+}}
+static int grad_scratch_slots(int) {{
+  return grad_scratch_slots_impl<ClassCode<{la}, {lb}, {lc}, {ld}>, BlockDims<{la}, {lb}, {lc}, {ld}, false>::NCART>();
+}}
+extern const ClassLaunchers launchers_{t};
+const ClassLaunchers launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_quartet<double>, &launch_quartet<float>,
+                                      &launch_grad<double>, &launch_grad<float>, &grad_scratch_slots}};
+}}  // namespace hfgpu
+"""
+
+
+def main(outdir):
+    import os
+    os.makedirs(outdir, exist_ok=True)
+    pairs, cls = classes()
+    meta = {"pair_classes": pairs, "eri": [], "grad": []}
+
+    def write_if_changed(path, text):
+        if os.path.exists(path) and open(path).read() == text:
+            return
+        with open(path, "w") as f:
+            f.write(text)
+
+    write_if_changed(os.path.join(outdir, "common.cuh"), common_header())
+    names = []
+    for c in cls:
+        t = "".join(map(str, c))
+        text, m, mg = class_header(c)
+        meta["eri"].append(m)
+        meta["grad"].append(mg)
+        write_if_changed(os.path.join(outdir, f"class_{t}.cuh"), text)
+        la, lb, lc, ld = c
+        write_if_changed(os.path.join(outdir, f"inst_{t}.cu"), INST_TEMPLATE.format(t=t, la=la, lb=lb, lc=lc, ld=ld))
+        names.append(t)
+    disp = ["// GENERATED by gen_eri.py -- do not edit.", '#include "../hfgpu_launch.h"', "namespace hfgpu {"]
+    for t in names:
+        disp.append(f"extern const ClassLaunchers launchers_{t};")
+    disp.append(f"const ClassLaunchers* const kClassLaunchers[{len(names)}] = {{")
+    disp += [f"  &launchers_{t}," for t in names]
+    disp.append("};")
+    disp.append(f"const int kNumClasses = {len(names)};")
+    disp.append("}  // namespace hfgpu")
+    write_if_changed(os.path.join(outdir, "dispatch.cu"), "\n".join(disp) + "\n")
+    write_if_changed(os.path.join(outdir, "ops.json"), json.dumps(meta, indent=1))
+    for m in meta["eri"]:
+        print("eri ", m["class"], "vrr", m["vrr_values"], "acc", m["vrr_targets"], "prim_fl", m["prim_flops"],
+              "hrr_fl", m["hrr_flops"], "pure_fl", m["pure_flops"])
+    for m in meta["grad"]:
+        print("grad", m["class"], "table" if m.get("table") else "straight", "prim_fl", m["prim_flops"],
+              "hrr_fl", m["hrr_flops"])
+
+
+
+
+# ---------------------------------------------------------------------------
+# Table mode: the large gradient classes run as op lists through a generic
+# executor (hfgpu_table.cuh) on thread-interleaved scratch, because their
+# straight-line form does not fit the register file and takes ptxas far too long.
+# ---------------------------------------------------------------------------
+class Dag:
+    """VRR as a DAG of ops: node = (kind, dir, a, b, c, d, g, k1, k2)."""
+
+    def __init__(self, L):
+        self.nodes = []   # list of tuples
+        self.memo = {}
+        self.L = L
+        for m in range(L + 1):
+            self.memo[((0, 0, 0), (0, 0, 0), m)] = len(self.nodes)
+            self.nodes.append(("F", m))
+
+    def get(self, e, f, m):
+        key = (e, f, m)
+        if key in self.memo:
+            return self.memo[key]
+        Z = -1
+        if sum(f) > 0:
+            i = max(range(3), key=lambda d: (f[d], -d))
+            f1 = add(f, i, -1)
+            a = self.get(e, f1, m)
+            b = self.get(e, f1, m + 1)
+            c = d = Z
+            k1 = k2 = 0
+            g = Z
+            if f1[i] > 0:
+                f2 = add(f1, i, -1)
+                c = self.get(e, f2, m)
+                d = self.get(e, f2, m + 1)
+                k1 = f1[i]
+            if e[i] > 0:
+                g = self.get(add(e, i, -1), f1, m + 1)
+                k2 = e[i]
+            node = ("K", i, a, b, c, d, g, k1, k2)
+        else:
+            i = max(range(3), key=lambda d: (e[d], -d))
+            e1 = add(e, i, -1)
+            a = self.get(e1, f, m)
+            b = self.get(e1, f, m + 1)
+            c = d = Z
+            k1 = 0
+            if e1[i] > 0:
+                e2 = add(e1, i, -1)
+                c = self.get(e2, f, m)
+                d = self.get(e2, f, m + 1)
+                k1 = e1[i]
+            node = ("B", i, a, b, c, d, Z, k1, 0)
+        self.memo[key] = len(self.nodes)
+        self.nodes.append(node)
+        return self.memo[key]
+
+
+def linear_scan(n_values, uses_per_op, defs_per_op, preassigned):
+    """Slot allocation.  uses_per_op[i] / defs_per_op[i]: value ids used / defined by op i.
+    preassigned: value id -> slot for values that exist before op 0.  Slot 0 stays zero."""
+    last = {}
+    for i, us in enumerate(uses_per_op):
+        for u in us:
+            last[u] = i
+    slot = dict(preassigned)
+    free = []
+    top = max(list(preassigned.values()) + [0]) + 1
+    for v, s in preassigned.items():
+        if v not in last:
+            free.append(s)
+    for i in range(len(uses_per_op)):
+        for v in defs_per_op[i]:
+            if free:
+                slot[v] = free.pop()
+            else:
+                slot[v] = top
+                top += 1
+        for u in set(uses_per_op[i]):
+            if last.get(u) == i:
+                free.append(slot[u])
+        for v in defs_per_op[i]:
+            if v not in last:  # dead store (should not happen)
+                free.append(slot[v])
+    return slot, top
+
+
+def gen_grad_table(la, lb, lc, ld):
+    L = la + lb + lc + ld + 1
+    order = grad_sets(la, lb, lc, ld)
+    dag = Dag(L)
+    setoff = {}
+    nacc = 0
+    for k in ("U", "A", "B", "C"):
+        setoff[k] = nacc
+        nacc += len(order[k])
+    tgt_nodes = {}
+    for k in ("U", "A", "B", "C"):
+        for j, (e, f) in enumerate(order[k]):
+            n = dag.get(e, f, 0)
+            tgt_nodes.setdefault(n, []).append((k, setoff[k] + j))
+    # ---- VRR op list: (kind, dir, dst, a, b, c, d, g, k1, k2) in value ids; acc ops after targets
+    ops, uses, defs = [], [], []
+    for nid, node in enumerate(dag.nodes):
+        if node[0] == "F":
+            continue
+        kind, i, a, b, c, d, g, k1, k2 = node
+        ops.append(["K" if kind == "K" else "B", i, nid, a, b, c, d, g, k1, k2])
+        uses.append([x for x in (a, b, c, d, g) if x >= 0])
+        defs.append([nid])
+        for (k, ai) in tgt_nodes.get(nid, []):
+            ops.append(["A", "UABC".index(k), ai, nid, -1, -1, -1, -1, 0, 0])
+            uses.append([nid])
+            defs.append([])
+    # F[m] seeds that are targets themselves (only for the all-s class)
+    pre_ops = []
+    for nid, node in enumerate(dag.nodes):
+        if node[0] == "F" and nid in tgt_nodes:
+            for (k, ai) in tgt_nodes[nid]:
+                pre_ops.append(["A", "UABC".index(k), ai, nid, -1, -1, -1, -1, 0, 0])
+    ops = pre_ops + ops
+    uses = [[o[3]] for o in pre_ops] + uses
+    defs = [[] for _ in pre_ops] + defs
+    pre = {m: 1 + m for m in range(L + 1)}  # F[m] lives in slot 1+m
+    slot, nvslot = linear_scan(len(dag.nodes), uses, defs, pre)
+    kinds = {"B": 0, "K": 1, "A": 2}
+    vrr_rows = []
+    for o in ops:
+        k, i, dst, a, b, c, d, g, k1, k2 = o
+        if k == "A":
+            vrr_rows.append((2, i, dst, slot[a], 0, 0, 0, 0, 0, 0))
+        else:
+            sl = lambda x: slot[x] if x >= 0 else 0
+            vrr_rows.append((kinds[k], i, slot[dst], sl(a), sl(b), sl(c), sl(d), sl(g), k1, k2))
+    # ---- HRR + contraction list on the second region: slot 0 zero, acc j at slot 1+j
+    hnodes = {}
+    hops, huses, hdefs = [], [], []
+    counter = [nacc + 1]
+
+    def acc_id(k, e, f):
+        return 1 + setoff[k] + order[k].index((e, f))
+
+    def new_id():
+        counter[0] += 1
+        return counter[0] - 1
+
+    def ket(k, e, c, d):
+        key = ("k", k, e, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(d) == 0:
+            v = acc_id(k, e, c)
+        else:
+            i = max(range(3), key=lambda q: (d[q], -q))
+            d1 = add(d, i, -1)
+            x = ket(k, e, add(c, i), d1)
+            y = ket(k, e, c, d1)
+            v = new_id()
+            hops.append((1, i, v, x, y, 0, 0))
+            huses.append([x, y])
+            hdefs.append([v])
+        hnodes[key] = v
+        return v
+
+    def bra(k, a, b, c, d):
+        key = ("b", k, a, b, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(b) == 0:
+            v = ket(k, a, c, d)
+        else:
+            i = max(range(3), key=lambda q: (b[q], -q))
+            b1 = add(b, i, -1)
+            x = bra(k, add(a, i), b1, c, d)
+            y = bra(k, a, b1, c, d)
+            v = new_id()
+            hops.append((0, i, v, x, y, 0, 0))
+            huses.append([x, y])
+            hdefs.append([v])
+        hnodes[key] = v
+        return v
+
+    gt = grad_terms(la, lb, lc, ld)
+    for (cen, dr), items in gt.items():
+        gi = "ABC".index(cen) * 3 + dr
+        for wi, terms in items:
+            x = bra(terms[0][1], *terms[0][2:])
+            if len(terms) > 1:
+                y = bra("U", *terms[1][2:])
+                kk = -terms[1][0]
+            else:
+                y, kk = -1, 0
+            hops.append((2, gi, wi, x, y, kk, 0))
+            huses.append([x] + ([y] if y >= 0 else []))
+            hdefs.append([])
+    hpre = {1 + j: 1 + j for j in range(nacc)}
+    hslot, nhslot = linear_scan(counter[0], huses, hdefs, hpre)
+    hrows = []
+    for o in hops:
+        kind, i, dst, x, y, kk, _ = o
+        if kind == 2:
+            hrows.append((2, i, dst, hslot[x], hslot[y] if y >= 0 else 0, kk, 0, 0))
+        else:
+            hrows.append((kind, i, hslot[dst], hslot[x], hslot[y], 0, 0, 0))
+    tagc = f"{la}{lb}{lc}{ld}"
+    s = [f"// table-mode adjoint gradient of class {tagc}: {len(vrr_rows)} VRR ops over {nvslot} slots, "
+         f"{nacc} accumulators, {len(hrows)} HRR/contraction ops over {nhslot} slots"]
+    s.append(f"__device__ const int gvrr_{tagc}[{len(vrr_rows)}][10] = {{")
+    s += ["  {" + ",".join(map(str, r)) + "}," for r in vrr_rows]
+    s.append("};")
+    s.append(f"__device__ const int ghrr_{tagc}[{len(hrows)}][8] = {{")
+    s += ["  {" + ",".join(map(str, r)) + "}," for r in hrows]
+    s.append("};")
+    s.append(f"struct GradTable{tagc} {{ static constexpr int L = {L}, NVOPS = {len(vrr_rows)}, NVSLOT = {nvslot}, "
+             f"NACC = {nacc}, NHOPS = {len(hrows)}, NHSLOT = {nhslot}; "
+             f"static __device__ const int (*vrr())[10] {{ return gvrr_{tagc}; }} "
+             f"static __device__ const int (*hrr())[8] {{ return ghrr_{tagc}; }} }};")
+    flops = sum(3 + (3 if r[8] else 0) + (2 if r[9] else 0) for r in vrr_rows if r[0] < 2) + \
+        2 * sum(1 for r in vrr_rows if r[0] == 2)
+    hfl = sum(2 if r[0] < 2 else 4 for r in hrows)
+    meta = {"class": [la, lb, lc, ld], "table": True, "vrr_ops": len(vrr_rows), "vrr_slots": nvslot,
+            "accumulators": nacc, "hrr_ops": len(hrows), "hrr_slots": nhslot,
+            "prim_flops": flops + PRIM_HEADER_FLOPS, "hrr_flops": hfl, "boys_m": L}
+    return "\n".join(s), meta
+
+
+if __name__ == "__main__":
+    main(sys.argv[1])

@@ -1,0 +1,114 @@
+// Device-side data layout and helpers shared by the two-electron kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define PI_2_5 34.986836655249725  // 2 pi^(5/2), hfscfmath::PI_25 (src/math/hfscf_math.hpp:25)
+
+// ---------------------------------------------------------------------------
+// Primitive pair of a shell pair (a b): p = alpha_a + alpha_b, P, PA = P - A,
+// K = exp(-alpha_a alpha_b / p |AB|^2) c_a c_b -- BASIS::ShellPair::set_params
+// (src/integrals/hfscf_shellpair.cpp:33-61).  64 bytes in FP64, one cache-line half.
+// ---------------------------------------------------------------------------
+template <typename R>
+struct __align__(sizeof(R) * 8) PrimPair {
+  R p, Px, Py, Pz, PAx, PAy, PAz, K;
+};
+
+// One canonical shell pair (La >= Lb after an optional swap of the two shells).
+struct PairInfo {
+  int sa, sb;        // shell indices
+  int fa, fb;        // first function of each shell in the final (pure or Cartesian) basis
+  int prim_off;      // first primitive pair
+  int nprim;         // primitive pairs kept
+  int cls;           // pair class: 0 ss, 1 ps, 2 pp, 3 ds, 4 dp, 5 dd
+  int atom_a, atom_b;
+  int pad;
+  double ABx, ABy, ABz;  // A - B
+  double schwarz;        // sqrt(max |(ab|ab)|) over the pair's functions
+};
+
+// Status word written by kernels that detect a problem (bad input seen on device).
+enum : int { HFGPU_DEV_OK = 0, HFGPU_DEV_NONFINITE = 1 };
+
+template <typename R>
+__device__ __forceinline__ R sqrt_t(R x);
+template <>
+__device__ __forceinline__ double sqrt_t<double>(double x) { return sqrt(x); }
+template <>
+__device__ __forceinline__ float sqrt_t<float>(float x) { return sqrtf(x); }
+template <typename R>
+__device__ __forceinline__ R exp_t(R x);
+template <>
+__device__ __forceinline__ double exp_t<double>(double x) { return exp(x); }
+template <>
+__device__ __forceinline__ float exp_t<float>(float x) { return expf(x); }
+
+// ---------------------------------------------------------------------------
+// Boys function F_m(T), m = 0..M, scaled by `pre`.
+//
+// Method (Gill, Johnson & Pople, Int. J. Quantum Chem. 40, 745 (1991); Helgaker,
+// Jorgensen & Olsen, "Molecular Electronic-Structure Theory", sec. 9.8.2):
+//   T <  BOYS_TMAX: six-term Taylor expansion of F_M about the nearest grid point
+//                  T_k = k h (h = 0.1), F_M(T) = sum_j F_{M+j}(T_k) (-dT)^j / j!,
+//                  then the stable downward recursion
+//                  F_{m-1} = (2T F_m + e^-T) / (2m - 1);
+//   T >= BOYS_TMAX: F_0 = sqrt(pi/T)/2 (erf(sqrt T) = 1 to double precision there)
+//                  and the upward recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T).
+// The table F_m(T_k) is computed on the host from the convergent series
+// F_m(T) = e^-T sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)) in long double.
+// ---------------------------------------------------------------------------
+#define BOYS_H 0.1
+#define BOYS_NGRID 361           // T_k = 0 .. 36
+#define BOYS_TMAX 36.0
+#define BOYS_NM 18               // m = 0 .. 17 tabulated (m <= 10 used + 7 Taylor terms)
+
+template <typename R>
+struct BoysTable {
+  const R* __restrict__ tab;  // [BOYS_NGRID][BOYS_NM]
+
+  template <int M>
+  __device__ __forceinline__ void eval(R T, R pre, R* F) const {
+    if (T < R(BOYS_TMAX)) {
+      const int k = __float2int_rn(float(T * R(10)));
+      const R d = R(k) * R(BOYS_H) - T;  // -(T - T_k)
+      const R* row = tab + k * BOYS_NM + M;
+      R f;
+      if constexpr (sizeof(R) == 8) {
+        f = row[6];
+        f = row[5] + f * d * R(1.0 / 6.0);
+        f = row[4] + f * d * R(1.0 / 5.0);
+        f = row[3] + f * d * R(1.0 / 4.0);
+        f = row[2] + f * d * R(1.0 / 3.0);
+        f = row[1] + f * d * R(1.0 / 2.0);
+        f = row[0] + f * d;
+      } else {
+        f = row[3];
+        f = row[2] + f * d * R(1.0 / 3.0);
+        f = row[1] + f * d * R(1.0 / 2.0);
+        f = row[0] + f * d;
+      }
+      F[M] = f;
+      if constexpr (M > 0) {
+        const R e = exp_t<R>(-T);
+        const R t2 = T + T;
+#pragma unroll
+        for (int m = M; m > 0; --m) F[m - 1] = (t2 * F[m] + e) * R(1.0 / (2 * m - 1));
+      }
+    } else {
+      const R it = R(1) / T;
+      F[0] = R(0.88622692545275801365) * sqrt_t<R>(it);  // sqrt(pi)/2 / sqrt(T)
+      if constexpr (M > 0) {
+        const R e = exp_t<R>(-T);
+        const R h = R(0.5) * it;
+#pragma unroll
+        for (int m = 0; m < M; ++m) F[m + 1] = (R(2 * m + 1) * F[m] - e) * h;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] *= pre;
+  }
+};
+
+__host__ __device__ constexpr int ncart_of(int L) { return (L + 1) * (L + 2) / 2; }
+__host__ __device__ constexpr int npure_of(int L) { return 2 * L + 1; }

@@ -1,0 +1,823 @@
+// Host side of the hfgpu engine: basis set-up, primitive-pair data, Schwarz
+// factors, screened quartet lists, and the C ABI of include/hfgpu.h.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hfgpu.h"
+#include "hfgpu_kernels.cuh"
+#include "hfgpu_launch.h"
+#include "hfgpu_onee.h"
+
+namespace {
+
+constexpr int kPairClasses = 6;
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kPrimPairCut = 1e-24;  // |K_ab| below this cannot reach 1e-14 in any integral
+
+int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }  // la >= lb: ss ps pp ds dp dd
+int quartet_class(int cp, int cq) { return cp * (cp + 1) / 2 + cq; }  // cp >= cq
+
+// Boys table F_m(k h), m < BOYS_NM, from the series e^-T sum_i (2T)^i / (2m+1)(2m+3)...(2m+2i+1).
+std::vector<double> boys_table() {
+  std::vector<double> t((size_t)BOYS_NGRID * BOYS_NM);
+  for (int k = 0; k < BOYS_NGRID; ++k) {
+    const long double T = (long double)k * (long double)BOYS_H;
+    for (int m = 0; m < BOYS_NM; ++m) {
+      long double term = 1.0L / (2 * m + 1), sum = term;
+      for (int i = 0; i < 2000; ++i) {
+        term *= 2.0L * T / (long double)(2 * m + 2 * i + 3);
+        sum += term;
+        if (term < sum * 1e-21L) break;
+      }
+      t[(size_t)k * BOYS_NM + m] = (double)(expl(-T) * sum);
+    }
+  }
+  return t;
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+}  // namespace
+
+struct hfgpu_handle {
+  // basis
+  int nshell = 0, natoms = 0, pure = 0, n = 0;
+  std::vector<int> L, shell_atom, nprim, prim_off, first;
+  std::vector<double> exps, coefs;  // normalised coefficients
+  std::vector<double> xyz;
+  bool have_geometry = false;
+  hfgpu_opts opts{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+
+  // pair data (host mirror) and class ranges
+  std::vector<PairInfo> pairs;
+  int class_begin[kPairClasses + 1] = {0};
+  int nprimpairs = 0;
+
+  // quartet lists per class: [beg, mid) high bound (FP64 always), [mid, end) low bound
+  std::vector<long long> q_beg, q_mid, q_end;
+  long long nquartets = 0;
+
+  DevBuf d_pairs, d_prim_d, d_prim_f, d_alpha_d, d_alpha_f, d_boys_d, d_boys_f, d_quart;
+  DevBuf d_mats, d_half, d_dmax, d_counters, d_grad, d_scratch, d_eri, d_eriq;
+  long long last_launched = 0, last_skipped = 0;
+
+  hfgpu_handle() : q_beg(21), q_mid(21), q_end(21) {}
+};
+
+namespace {
+
+int fail(hfgpu_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+int cuda_fail(hfgpu_handle* h, cudaError_t e, const char* where) {
+  return fail(h, e == cudaErrorMemoryAllocation ? HFGPU_ERR_NOMEM : HFGPU_ERR_CUDA,
+              std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define HF_CUDA(h, call)                                    \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, #call);  \
+  } while (0)
+
+#define HF_CHECK_LAUNCH(h, what)                              \
+  do {                                                        \
+    cudaError_t e_ = cudaGetLastError();                      \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, what);     \
+  } while (0)
+
+// Normalisation of BASIS::Shell::Shell (src/integrals/hfscf_shell.cpp:44-54).
+void normalise(int L, int np, const double* a, const double* c, double* out) {
+  const double m = L + 1.5, m2 = 0.5 * m;
+  double sum = 0.0;
+  for (int j = 0; j < np; ++j)
+    for (int k = 0; k < np; ++k) sum += c[j] * c[k] * std::pow(a[j] * a[k], m2) / std::pow(a[j] + a[k], m);
+  double dfac = 1.0;
+  for (int x = 2 * L - 1; x > 1; x -= 2) dfac *= x;
+  const double norm = 1.0 / std::sqrt(sum * std::pow(kPi, 1.5) * dfac / std::pow(2.0, L));
+  for (int j = 0; j < np; ++j) out[j] = c[j] * norm * std::pow(a[j], m2);
+}
+
+int set_device(hfgpu_handle* h) {
+  HF_CUDA(h, cudaSetDevice(h->device));
+  return HFGPU_OK;
+}
+
+// Primitive pairs of every canonical shell pair; pairs sorted by class, then by
+// primitive count (descending) so that quartet lists group equal loop lengths.
+int build_pairs(hfgpu_handle* h) {
+  const int ns = h->nshell;
+  struct Tmp {
+    int sa, sb, cls, np;
+  };
+  std::vector<Tmp> tmp;
+  tmp.reserve((size_t)ns * (ns + 1) / 2);
+  for (int i = 0; i < ns; ++i)
+    for (int j = i; j < ns; ++j) {
+      int sa = i, sb = j;
+      if (h->L[sa] < h->L[sb]) std::swap(sa, sb);
+      tmp.push_back({sa, sb, pair_class(h->L[sa], h->L[sb]), h->nprim[sa] * h->nprim[sb]});
+    }
+  std::stable_sort(tmp.begin(), tmp.end(), [](const Tmp& x, const Tmp& y) {
+    if (x.cls != y.cls) return x.cls < y.cls;
+    return x.np > y.np;
+  });
+  h->pairs.assign(tmp.size(), PairInfo{});
+  std::vector<PrimPair<double>> pd;
+  std::vector<double> aa, ab;
+  pd.reserve(tmp.size() * 4);
+  for (int c = 0; c <= kPairClasses; ++c) h->class_begin[c] = (int)tmp.size();
+  for (size_t x = 0; x < tmp.size(); ++x) {
+    const Tmp& t = tmp[x];
+    h->class_begin[t.cls] = std::min(h->class_begin[t.cls], (int)x);
+    PairInfo& P = h->pairs[x];
+    P.sa = t.sa;
+    P.sb = t.sb;
+    P.fa = h->first[t.sa];
+    P.fb = h->first[t.sb];
+    P.cls = t.cls;
+    P.atom_a = h->shell_atom[t.sa];
+    P.atom_b = h->shell_atom[t.sb];
+    const double* A = &h->xyz[3 * P.atom_a];
+    const double* B = &h->xyz[3 * P.atom_b];
+    P.ABx = A[0] - B[0];
+    P.ABy = A[1] - B[1];
+    P.ABz = A[2] - B[2];
+    const double R2 = P.ABx * P.ABx + P.ABy * P.ABy + P.ABz * P.ABz;
+    P.prim_off = (int)pd.size();
+    for (int i = 0; i < h->nprim[t.sa]; ++i)
+      for (int j = 0; j < h->nprim[t.sb]; ++j) {
+        const double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
+        const double c1 = h->coefs[h->prim_off[t.sa] + i], c2 = h->coefs[h->prim_off[t.sb] + j];
+        const double p = a1 + a2;
+        const double K = std::exp(-a1 * a2 / p * R2) * c1 * c2;
+        if (std::fabs(K) < kPrimPairCut) continue;
+        PrimPair<double> q;
+        q.p = p;
+        q.Px = (a1 * A[0] + a2 * B[0]) / p;
+        q.Py = (a1 * A[1] + a2 * B[1]) / p;
+        q.Pz = (a1 * A[2] + a2 * B[2]) / p;
+        q.PAx = q.Px - A[0];
+        q.PAy = q.Py - A[1];
+        q.PAz = q.Pz - A[2];
+        q.K = K;
+        pd.push_back(q);
+        aa.push_back(a1);
+        ab.push_back(a2);
+      }
+    P.nprim = (int)pd.size() - P.prim_off;
+    P.schwarz = 0.0;
+  }
+  for (int c = kPairClasses - 1; c >= 0; --c)
+    if (h->class_begin[c] > h->class_begin[c + 1]) h->class_begin[c] = h->class_begin[c + 1];
+  h->nprimpairs = (int)pd.size();
+  const size_t np = std::max<size_t>(pd.size(), 1);
+  std::vector<PrimPair<float>> pf(np);
+  std::vector<float> aaf(np), abf(np);
+  for (size_t i = 0; i < pd.size(); ++i) {
+    pf[i] = {(float)pd[i].p, (float)pd[i].Px, (float)pd[i].Py, (float)pd[i].Pz,
+             (float)pd[i].PAx, (float)pd[i].PAy, (float)pd[i].PAz, (float)pd[i].K};
+    aaf[i] = (float)aa[i];
+    abf[i] = (float)ab[i];
+  }
+  HF_CUDA(h, h->d_pairs.ensure(sizeof(PairInfo) * std::max<size_t>(h->pairs.size(), 1)));
+  HF_CUDA(h, h->d_prim_d.ensure(sizeof(PrimPair<double>) * np));
+  HF_CUDA(h, h->d_prim_f.ensure(sizeof(PrimPair<float>) * np));
+  HF_CUDA(h, h->d_alpha_d.ensure(sizeof(double) * 2 * np));
+  HF_CUDA(h, h->d_alpha_f.ensure(sizeof(float) * 2 * np));
+  cudaStream_t s = h->stream;
+  HF_CUDA(h, cudaMemcpyAsync(h->d_pairs.p, h->pairs.data(), sizeof(PairInfo) * h->pairs.size(), cudaMemcpyHostToDevice, s));
+  if (!pd.empty()) {
+    HF_CUDA(h, cudaMemcpyAsync(h->d_prim_d.p, pd.data(), sizeof(PrimPair<double>) * pd.size(), cudaMemcpyHostToDevice, s));
+    HF_CUDA(h, cudaMemcpyAsync(h->d_prim_f.p, pf.data(), sizeof(PrimPair<float>) * pd.size(), cudaMemcpyHostToDevice, s));
+    HF_CUDA(h, cudaMemcpyAsync(h->d_alpha_d.p, aa.data(), sizeof(double) * pd.size(), cudaMemcpyHostToDevice, s));
+    HF_CUDA(h, cudaMemcpyAsync(h->d_alpha_d.as<double>() + np, ab.data(), sizeof(double) * pd.size(), cudaMemcpyHostToDevice, s));
+    HF_CUDA(h, cudaMemcpyAsync(h->d_alpha_f.p, aaf.data(), sizeof(float) * pd.size(), cudaMemcpyHostToDevice, s));
+    HF_CUDA(h, cudaMemcpyAsync(h->d_alpha_f.as<float>() + np, abf.data(), sizeof(float) * pd.size(), cudaMemcpyHostToDevice, s));
+  }
+  HF_CUDA(h, cudaStreamSynchronize(s));
+  return HFGPU_OK;
+}
+
+JKArgs<double> jk_args_d(hfgpu_handle* h) {
+  JKArgs<double> a{};
+  a.pairs = h->d_pairs.as<PairInfo>();
+  a.prims = h->d_prim_d.as<PrimPair<double>>();
+  a.boys.tab = h->d_boys_d.as<double>();
+  a.n = h->n;
+  a.nshell = h->nshell;
+  return a;
+}
+
+JKArgs<float> jk_args_f(hfgpu_handle* h) {
+  JKArgs<float> a{};
+  a.pairs = h->d_pairs.as<PairInfo>();
+  a.prims = h->d_prim_f.as<PrimPair<float>>();
+  a.boys.tab = h->d_boys_f.as<float>();
+  a.n = h->n;
+  a.nshell = h->nshell;
+  return a;
+}
+
+// Schwarz factors: (P|P) for every pair, class by class.
+int compute_schwarz(hfgpu_handle* h) {
+  const int npairs = (int)h->pairs.size();
+  std::vector<int2> diag(std::max(npairs, 1));
+  for (int x = 0; x < npairs; ++x) diag[x] = make_int2(x, x);
+  HF_CUDA(h, h->d_quart.ensure(sizeof(int2) * diag.size()));
+  HF_CUDA(h, cudaMemcpyAsync(h->d_quart.p, diag.data(), sizeof(int2) * npairs, cudaMemcpyHostToDevice, h->stream));
+  QuartetArgs<double> qa{};
+  qa.jk = jk_args_d(h);
+  qa.mode = QMODE_SCHWARZ;
+  qa.pure = h->pure;
+  qa.pairs_rw = h->d_pairs.as<PairInfo>();
+  for (int c = 0; c < kPairClasses; ++c) {
+    const int b = h->class_begin[c], e = h->class_begin[c + 1];
+    if (e <= b) continue;
+    const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[quartet_class(c, c)];
+    L->quartet_d(qa, h->d_quart.as<int2>() + b, e - b, h->stream);
+    HF_CHECK_LAUNCH(h, "schwarz kernel");
+  }
+  HF_CUDA(h, cudaMemcpyAsync(h->pairs.data(), h->d_pairs.p, sizeof(PairInfo) * npairs, cudaMemcpyDeviceToHost, h->stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (const PairInfo& P : h->pairs)
+    if (!std::isfinite(P.schwarz)) return fail(h, HFGPU_ERR_NONFINITE, "non-finite Schwarz factor");
+  return HFGPU_OK;
+}
+
+// Screened unique quartets (P <= Q within a class; bra class >= ket class), per class.
+int build_quartets(hfgpu_handle* h) {
+  const double tol = h->opts.schwarz_tol, mix = h->opts.mixed_fp32_bound;
+  std::vector<int2> all;
+  std::vector<int2> low;
+  h->nquartets = 0;
+  for (int cp = 0; cp < kPairClasses; ++cp)
+    for (int cq = 0; cq <= cp; ++cq) {
+      const int qc = quartet_class(cp, cq);
+      low.clear();
+      h->q_beg[qc] = (long long)all.size();
+      const int pb = h->class_begin[cp], pe = h->class_begin[cp + 1];
+      const int kb = h->class_begin[cq], ke = h->class_begin[cq + 1];
+      for (int P = pb; P < pe; ++P) {
+        const double qp = h->pairs[P].schwarz;
+        const int k0 = (cp == cq) ? P : kb;
+        for (int Q = k0; Q < ke; ++Q) {
+          const double b = qp * h->pairs[Q].schwarz;
+          if (b < tol) continue;
+          if (b >= mix)
+            all.push_back(make_int2(P, Q));
+          else
+            low.push_back(make_int2(P, Q));
+        }
+      }
+      h->q_mid[qc] = (long long)all.size();
+      all.insert(all.end(), low.begin(), low.end());
+      h->q_end[qc] = (long long)all.size();
+    }
+  h->nquartets = (long long)all.size();
+  HF_CUDA(h, h->d_quart.ensure(sizeof(int2) * std::max<size_t>(all.size(), 1)));
+  if (!all.empty())
+    HF_CUDA(h, cudaMemcpyAsync(h->d_quart.p, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, h->stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->stream));
+  return HFGPU_OK;
+}
+
+__global__ void dmax_kernel(const int* __restrict__ first, int nshell, int n, const double* __restrict__ DJ, int nK,
+                            const double* __restrict__ DK, float* __restrict__ out) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nshell * nshell) return;
+  const int s = idx / nshell, t = idx % nshell;
+  double m = 0.0;
+  for (int i = first[s]; i < first[s + 1]; ++i)
+    for (int j = first[t]; j < first[t + 1]; ++j) {
+      if (DJ) m = fmax(m, fabs(DJ[(size_t)i * n + j]));
+      for (int k = 0; k < nK; ++k) m = fmax(m, fabs(DK[(size_t)k * n * n + (size_t)i * n + j]));
+    }
+  out[idx] = (float)m;
+}
+
+// J = Jh + Jh^T, K = Kh + Kh^T (in place into J/K outputs).
+__global__ void symmetrise_kernel(const double* __restrict__ h, double* __restrict__ out, int n, int nmat) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int tot = n * n;
+  if (idx >= tot * nmat) return;
+  const int m = idx / tot, e = idx % tot;
+  const int i = e / n, j = e % n;
+  out[idx] = h[(size_t)m * tot + i * n + j] + h[(size_t)m * tot + j * n + i];
+}
+
+}  // namespace
+
+// Device J/K: all pointers on the device.  Jout/Kout may be null to skip.
+static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* Jout, double* Kout,
+                          int precision) {
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  if (nK < 0 || nK > 8) return fail(h, HFGPU_ERR_INVALID, "nK out of range");
+  const int n = h->n, ns = h->nshell;
+  const size_t nn = (size_t)n * n;
+  HF_CUDA(h, h->d_half.ensure(sizeof(double) * nn * (1 + std::max(nK, 1))));
+  HF_CUDA(h, h->d_counters.ensure(sizeof(unsigned long long) * 2));
+  double* Jh = h->d_half.as<double>();
+  double* Kh = Jh + nn;
+  HF_CUDA(h, cudaMemsetAsync(Jh, 0, sizeof(double) * nn * (1 + nK), h->stream));
+  HF_CUDA(h, cudaMemsetAsync(h->d_counters.p, 0, sizeof(unsigned long long) * 2, h->stream));
+  const float* dmax = nullptr;
+  if (h->opts.density_tol > 0.0) {
+    HF_CUDA(h, h->d_dmax.ensure(sizeof(float) * ns * ns + sizeof(int) * (ns + 1)));
+    int* dfirst = reinterpret_cast<int*>(h->d_dmax.as<float>() + (size_t)ns * ns);
+    HF_CUDA(h, cudaMemcpyAsync(dfirst, h->first.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, h->stream));
+    dmax_kernel<<<(ns * ns + 127) / 128, 128, 0, h->stream>>>(dfirst, ns, n, DJ, nK, DK, h->d_dmax.as<float>());
+    HF_CHECK_LAUNCH(h, "dmax kernel");
+    dmax = h->d_dmax.as<float>();
+  }
+  QuartetArgs<double> qd{};
+  qd.jk = jk_args_d(h);
+  QuartetArgs<float> qf{};
+  qf.jk = jk_args_f(h);
+  for (JKArgs<double>* a : {&qd.jk}) {
+    a->DJ = DJ; a->nK = nK; a->DK = DK; a->Jh = Jh; a->Kh = Kh; a->dmax = dmax; a->dtol = h->opts.density_tol;
+    a->counters = h->d_counters.as<unsigned long long>();
+  }
+  qf.jk.DJ = DJ; qf.jk.nK = nK; qf.jk.DK = DK; qf.jk.Jh = Jh; qf.jk.Kh = Kh; qf.jk.dmax = dmax;
+  qf.jk.dtol = h->opts.density_tol; qf.jk.counters = h->d_counters.as<unsigned long long>();
+  qd.mode = qf.mode = QMODE_JK;
+  qd.pure = qf.pure = h->pure;
+  const int2* q = h->d_quart.as<int2>();
+  long long launched = 0;
+  // largest classes first so that they overlap the tail of the smaller ones
+  for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
+    const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
+    const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
+    if (precision == HFGPU_MIXED) {
+      if (m > b) L->quartet_d(qd, q + b, (int)(m - b), h->stream);
+      if (e > m) L->quartet_f(qf, q + m, (int)(e - m), h->stream);
+    } else if (e > b) {
+      L->quartet_d(qd, q + b, (int)(e - b), h->stream);
+    }
+    HF_CHECK_LAUNCH(h, "quartet kernel");
+    launched += e - b;
+  }
+  h->last_launched = launched;
+  const int tot = (int)nn;
+  if (Jout && DJ) {
+    symmetrise_kernel<<<(tot + 255) / 256, 256, 0, h->stream>>>(Jh, Jout, n, 1);
+    HF_CHECK_LAUNCH(h, "symmetrise J");
+  }
+  if (Kout && nK > 0) {
+    symmetrise_kernel<<<(tot * nK + 255) / 256, 256, 0, h->stream>>>(Kh, Kout, n, nK);
+    HF_CHECK_LAUNCH(h, "symmetrise K");
+  }
+  return HFGPU_OK;
+}
+
+static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
+                            double* grad, int precision) {
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  GradArgs<double> gd{};
+  gd.pairs = h->d_pairs.as<PairInfo>();
+  gd.prims = h->d_prim_d.as<PrimPair<double>>();
+  const size_t np = std::max<size_t>(h->nprimpairs, 1);
+  gd.alpha_a = h->d_alpha_d.as<double>();
+  gd.alpha_b = h->d_alpha_d.as<double>() + np;
+  gd.boys.tab = h->d_boys_d.as<double>();
+  gd.n = h->n;
+  gd.DJ = DJ; gd.cJ = cJ; gd.nK = nK; gd.DK = DK; gd.cK = cK; gd.grad = grad;
+  GradArgs<float> gf{};
+  gf.pairs = gd.pairs;
+  gf.prims = h->d_prim_f.as<PrimPair<float>>();
+  gf.alpha_a = h->d_alpha_f.as<float>();
+  gf.alpha_b = h->d_alpha_f.as<float>() + np;
+  gf.boys.tab = h->d_boys_f.as<float>();
+  gf.n = h->n;
+  gf.DJ = DJ; gf.cJ = cJ; gf.nK = nK; gf.DK = DK; gf.cK = cK; gf.grad = grad;
+  const int2* q = h->d_quart.as<int2>();
+  const size_t budget = (size_t)1 << 30;  // scratch bytes for table-mode classes
+  for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
+    const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
+    const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
+    if (e <= b) continue;
+    const int slots = L->grad_scratch_slots(h->pure);
+    auto run = [&](bool fp32, long long lo, long long hi) -> int {
+      const int nq = (int)(hi - lo);
+      if (nq <= 0) return HFGPU_OK;
+      int grid = (nq + 127) / 128;
+      if (slots > 0) {
+        const size_t rb = fp32 ? sizeof(float) : sizeof(double);
+        long long thr = (long long)(budget / ((size_t)slots * rb));
+        thr = std::max<long long>(thr, 4736);
+        thr = std::min<long long>(thr, (long long)grid * 128);
+        grid = (int)((thr + 127) / 128);
+        const size_t need = (size_t)slots * rb * (size_t)grid * 128;
+        HF_CUDA(h, h->d_scratch.ensure(need));
+      }
+      if (fp32) {
+        gf.scratch = h->d_scratch.as<float>();
+        gf.scratch_threads = grid * 128;
+        L->grad_f(gf, h->pure, q + lo, nq, grid, h->stream);
+      } else {
+        gd.scratch = h->d_scratch.as<double>();
+        gd.scratch_threads = grid * 128;
+        L->grad_d(gd, h->pure, q + lo, nq, grid, h->stream);
+      }
+      HF_CHECK_LAUNCH(h, "grad kernel");
+      return HFGPU_OK;
+    };
+    int rc;
+    if (precision == HFGPU_MIXED) {
+      if ((rc = run(false, b, m))) return rc;
+      if ((rc = run(true, m, e))) return rc;
+    } else if ((rc = run(false, b, e))) {
+      return rc;
+    }
+  }
+  return HFGPU_OK;
+}
+
+extern "C" {
+
+int hfgpu_default_opts(hfgpu_opts* o) {
+  if (!o) return HFGPU_ERR_INVALID;
+  std::memset(o, 0, sizeof(*o));
+  o->schwarz_tol = 1e-12;
+  o->density_tol = 1e-12;
+  o->mixed_fp32_bound = 1e-4;
+  o->device = 0;
+  return HFGPU_OK;
+}
+
+const char* hfgpu_last_error(const hfgpu_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int hfgpu_nbf(const hfgpu_handle* h, int* nbf) {
+  if (!h || !nbf) return HFGPU_ERR_INVALID;
+  *nbf = h->n;
+  return HFGPU_OK;
+}
+
+int hfgpu_create(const hfgpu_basis* b, const hfgpu_opts* opts, hfgpu_handle** out) {
+  if (!b || !out || b->nshell <= 0 || b->natoms <= 0 || !b->L || !b->shell_atom || !b->nprim || !b->exps || !b->coefs)
+    return HFGPU_ERR_INVALID;
+  *out = nullptr;
+  hfgpu_handle* h = new (std::nothrow) hfgpu_handle();
+  if (!h) return HFGPU_ERR_NOMEM;
+  if (opts)
+    h->opts = *opts;
+  else
+    hfgpu_default_opts(&h->opts);
+  h->device = h->opts.device;
+  h->nshell = b->nshell;
+  h->natoms = b->natoms;
+  h->pure = b->pure ? 1 : 0;
+  h->L.assign(b->L, b->L + b->nshell);
+  h->shell_atom.assign(b->shell_atom, b->shell_atom + b->nshell);
+  h->nprim.assign(b->nprim, b->nprim + b->nshell);
+  h->prim_off.resize(b->nshell + 1);
+  h->first.resize(b->nshell + 1);
+  h->prim_off[0] = 0;
+  h->first[0] = 0;
+  for (int s = 0; s < b->nshell; ++s) {
+    if (h->L[s] < 0 || h->L[s] > 2 || h->nprim[s] < 1 || h->shell_atom[s] < 0 || h->shell_atom[s] >= b->natoms) {
+      delete h;
+      return HFGPU_ERR_INVALID;
+    }
+    h->prim_off[s + 1] = h->prim_off[s] + h->nprim[s];
+    h->first[s + 1] = h->first[s] + (h->pure ? 2 * h->L[s] + 1 : (h->L[s] + 1) * (h->L[s] + 2) / 2);
+  }
+  const int nprim_tot = h->prim_off[b->nshell];
+  h->exps.assign(b->exps, b->exps + nprim_tot);
+  h->coefs.resize(nprim_tot);
+  for (int p = 0; p < nprim_tot; ++p)
+    if (!std::isfinite(b->exps[p]) || !(b->exps[p] > 0.0) || !std::isfinite(b->coefs[p])) {
+      delete h;
+      return HFGPU_ERR_INVALID;
+    }
+  for (int s = 0; s < b->nshell; ++s)
+    normalise(h->L[s], h->nprim[s], &b->exps[h->prim_off[s]], &b->coefs[h->prim_off[s]], &h->coefs[h->prim_off[s]]);
+  h->n = h->first[b->nshell];
+  int rc = set_device(h);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return HFGPU_ERR_CUDA;
+  }
+  h->own_stream = true;
+  std::vector<double> bt = boys_table();
+  std::vector<float> btf(bt.size());
+  for (size_t i = 0; i < bt.size(); ++i) btf[i] = (float)bt[i];
+  if (h->d_boys_d.ensure(sizeof(double) * bt.size()) || h->d_boys_f.ensure(sizeof(float) * bt.size()) ||
+      cudaMemcpy(h->d_boys_d.p, bt.data(), sizeof(double) * bt.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(h->d_boys_f.p, btf.data(), sizeof(float) * bt.size(), cudaMemcpyHostToDevice)) {
+    hfgpu_destroy(h);
+    return HFGPU_ERR_CUDA;
+  }
+  *out = h;
+  return HFGPU_OK;
+}
+
+int hfgpu_destroy(hfgpu_handle* h) {
+  if (!h) return HFGPU_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (DevBuf* d : {&h->d_pairs, &h->d_prim_d, &h->d_prim_f, &h->d_alpha_d, &h->d_alpha_f, &h->d_boys_d, &h->d_boys_f,
+                    &h->d_quart, &h->d_mats, &h->d_half, &h->d_dmax, &h->d_counters, &h->d_grad, &h->d_scratch,
+                    &h->d_eri, &h->d_eriq})
+    d->release();
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return HFGPU_OK;
+}
+
+int hfgpu_set_stream(hfgpu_handle* h, void* stream) {
+  if (!h) return HFGPU_ERR_INVALID;
+  if (h->own_stream && h->stream) {
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+  }
+  h->own_stream = false;
+  h->stream = static_cast<cudaStream_t>(stream);
+  if (!stream) {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return HFGPU_ERR_CUDA;
+    h->own_stream = true;
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_set_geometry(hfgpu_handle* h, const double* xyz, int natoms) {
+  if (!h || !xyz || natoms != h->natoms) return fail(h, HFGPU_ERR_INVALID, "bad geometry arguments");
+  for (int i = 0; i < 3 * natoms; ++i)
+    if (!std::isfinite(xyz[i])) return fail(h, HFGPU_ERR_INVALID, "non-finite coordinate");
+  int rc = set_device(h);
+  if (rc) return rc;
+  h->xyz.assign(xyz, xyz + 3 * natoms);
+  h->have_geometry = false;
+  if ((rc = build_pairs(h))) return rc;
+  if ((rc = compute_schwarz(h))) return rc;
+  if ((rc = build_quartets(h))) return rc;
+  h->have_geometry = true;
+  return HFGPU_OK;
+}
+
+int hfgpu_schwarz(hfgpu_handle* h, double* Q) {
+  if (!h || !Q) return HFGPU_ERR_INVALID;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  const int ns = h->nshell;
+  for (const PairInfo& P : h->pairs) {
+    Q[P.sa * ns + P.sb] = P.schwarz;
+    Q[P.sb * ns + P.sa] = P.schwarz;
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_eri_packed(hfgpu_handle* h, double* eri_out, long long eri_len) {
+  if (!h || !eri_out) return HFGPU_ERR_INVALID;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  const long long n = h->n, len = n * (n + 1) * (n * n + n + 2) / 8;
+  if (eri_len != len) return fail(h, HFGPU_ERR_INVALID, "eri_len must be n(n+1)(n^2+n+2)/8");
+  int rc = set_device(h);
+  if (rc) return rc;
+  HF_CUDA(h, h->d_eri.ensure(sizeof(double) * len));
+  HF_CUDA(h, cudaMemsetAsync(h->d_eri.p, 0, sizeof(double) * len, h->stream));
+  QuartetArgs<double> qa{};
+  qa.jk = jk_args_d(h);
+  qa.mode = QMODE_PACKED;
+  qa.pure = h->pure;
+  qa.eri = h->d_eri.as<double>();
+  for (int cp = 0; cp < kPairClasses; ++cp)
+    for (int cq = 0; cq <= cp; ++cq) {
+      std::vector<int2> list;
+      for (int P = h->class_begin[cp]; P < h->class_begin[cp + 1]; ++P)
+        for (int Q = (cp == cq) ? P : h->class_begin[cq]; Q < h->class_begin[cq + 1]; ++Q)
+          list.push_back(make_int2(P, Q));
+      if (list.empty()) continue;
+      HF_CUDA(h, h->d_eriq.ensure(sizeof(int2) * list.size()));
+      HF_CUDA(h, cudaMemcpyAsync(h->d_eriq.p, list.data(), sizeof(int2) * list.size(), cudaMemcpyHostToDevice, h->stream));
+      hfgpu::kClassLaunchers[quartet_class(cp, cq)]->quartet_d(qa, h->d_eriq.as<int2>(), (int)list.size(), h->stream);
+      HF_CHECK_LAUNCH(h, "packed eri kernel");
+      HF_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+  HF_CUDA(h, cudaMemcpyAsync(eri_out, h->d_eri.p, sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->stream));
+  return HFGPU_OK;
+}
+
+int hfgpu_jk_device(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* J, double* K, int precision) {
+  if (!h) return HFGPU_ERR_INVALID;
+  int rc = set_device(h);
+  if (rc) return rc;
+  return jk_device_impl(h, DJ, nK, DK, J, K, precision);
+}
+
+int hfgpu_jk(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* J, double* K, int precision) {
+  if (!h || (nK > 0 && (!DK || !K)) || (DJ && !J)) return HFGPU_ERR_INVALID;
+  int rc = set_device(h);
+  if (rc) return rc;
+  const size_t nn = (size_t)h->n * h->n;
+  // device layout: [DJ | DK (nK) | J | K (nK)]
+  HF_CUDA(h, h->d_mats.ensure(sizeof(double) * nn * (2 + 2 * nK)));
+  double* dDJ = h->d_mats.as<double>();
+  double* dDK = dDJ + nn;
+  double* dJ = dDK + nn * nK;
+  double* dK = dJ + nn;
+  if (DJ) HF_CUDA(h, cudaMemcpyAsync(dDJ, DJ, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream));
+  if (nK) HF_CUDA(h, cudaMemcpyAsync(dDK, DK, sizeof(double) * nn * nK, cudaMemcpyHostToDevice, h->stream));
+  if ((rc = jk_device_impl(h, DJ ? dDJ : nullptr, nK, dDK, dJ, dK, precision))) return rc;
+  if (DJ) HF_CUDA(h, cudaMemcpyAsync(J, dJ, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->stream));
+  if (nK) HF_CUDA(h, cudaMemcpyAsync(K, dK, sizeof(double) * nn * nK, cudaMemcpyDeviceToHost, h->stream));
+  unsigned long long cnt[2] = {0, 0};
+  HF_CUDA(h, cudaMemcpyAsync(cnt, h->d_counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->last_skipped = (long long)cnt[1];
+  return HFGPU_OK;
+}
+
+int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* skipped) {
+  if (!h) return HFGPU_ERR_INVALID;
+  if (launched) *launched = h->last_launched;
+  if (skipped) *skipped = h->last_skipped;
+  return HFGPU_OK;
+}
+
+int hfgpu_fock_rhf(hfgpu_handle* h, const double* D, const double* H, double* F, int precision) {
+  if (!h || !D || !H || !F) return HFGPU_ERR_INVALID;
+  const size_t nn = (size_t)h->n * h->n;
+  std::vector<double> J(nn), K(nn);
+  int rc = hfgpu_jk(h, D, 1, D, J.data(), K.data(), precision);
+  if (rc) return rc;
+  for (size_t i = 0; i < nn; ++i) F[i] = H[i] + 2.0 * J[i] - K[i];
+  return HFGPU_OK;
+}
+
+int hfgpu_fock_uhf(hfgpu_handle* h, const double* Da, const double* Db, const double* H, double* Fa, double* Fb,
+                   int precision) {
+  if (!h || !Da || !Db || !H || !Fa || !Fb) return HFGPU_ERR_INVALID;
+  const size_t nn = (size_t)h->n * h->n;
+  std::vector<double> Dt(nn), DK(2 * nn), J(nn), K(2 * nn);
+  for (size_t i = 0; i < nn; ++i) {
+    Dt[i] = Da[i] + Db[i];
+    DK[i] = Da[i];
+    DK[nn + i] = Db[i];
+  }
+  int rc = hfgpu_jk(h, Dt.data(), 2, DK.data(), J.data(), K.data(), precision);
+  if (rc) return rc;
+  for (size_t i = 0; i < nn; ++i) {
+    Fa[i] = H[i] + J[i] - K[i];
+    Fb[i] = H[i] + J[i] - K[nn + i];
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_fock_delta(hfgpu_handle* h, const double* dD, double* F, int precision) {
+  if (!h || !dD || !F) return HFGPU_ERR_INVALID;
+  const size_t nn = (size_t)h->n * h->n;
+  std::vector<double> J(nn), K(nn);
+  int rc = hfgpu_jk(h, dD, 1, dD, J.data(), K.data(), precision);
+  if (rc) return rc;
+  for (size_t i = 0; i < nn; ++i) F[i] += 2.0 * J[i] - K[i];
+  return HFGPU_OK;
+}
+
+int hfgpu_energy_forward(hfgpu_handle* h, const double* D, double* E2, int precision) {
+  if (!h || !D || !E2) return HFGPU_ERR_INVALID;
+  const size_t nn = (size_t)h->n * h->n;
+  std::vector<double> J(nn), K(nn);
+  int rc = hfgpu_jk(h, D, 1, D, J.data(), K.data(), precision);
+  if (rc) return rc;
+  double e = 0.0;
+  for (size_t i = 0; i < nn; ++i) e += D[i] * (2.0 * J[i] - K[i]);
+  *E2 = e;
+  return std::isfinite(e) ? HFGPU_OK : fail(h, HFGPU_ERR_NONFINITE, "non-finite energy");
+}
+
+int hfgpu_grad2e_device(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
+                        double* grad, int precision) {
+  if (!h || !grad) return HFGPU_ERR_INVALID;
+  int rc = set_device(h);
+  if (rc) return rc;
+  return grad_device_impl(h, DJ, cJ, nK, DK, cK, grad, precision);
+}
+
+static int grad_host(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* const* DKs, double cK,
+                     double scale, double* dE_dR, int precision) {
+  int rc = set_device(h);
+  if (rc) return rc;
+  const size_t nn = (size_t)h->n * h->n;
+  HF_CUDA(h, h->d_mats.ensure(sizeof(double) * nn * (1 + nK)));
+  HF_CUDA(h, h->d_grad.ensure(sizeof(double) * 3 * h->natoms));
+  double* dDJ = h->d_mats.as<double>();
+  double* dDK = dDJ + nn;
+  HF_CUDA(h, cudaMemcpyAsync(dDJ, DJ, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream));
+  for (int m = 0; m < nK; ++m)
+    HF_CUDA(h, cudaMemcpyAsync(dDK + m * nn, DKs[m], sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream));
+  HF_CUDA(h, cudaMemsetAsync(h->d_grad.p, 0, sizeof(double) * 3 * h->natoms, h->stream));
+  if ((rc = grad_device_impl(h, dDJ, cJ, nK, dDK, cK, h->d_grad.as<double>(), precision))) return rc;
+  std::vector<double> g(3 * h->natoms);
+  HF_CUDA(h, cudaMemcpyAsync(g.data(), h->d_grad.p, sizeof(double) * g.size(), cudaMemcpyDeviceToHost, h->stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (size_t i = 0; i < g.size(); ++i) {
+    if (!std::isfinite(g[i])) return fail(h, HFGPU_ERR_NONFINITE, "non-finite gradient");
+    dE_dR[i] += scale * g[i];
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_grad2e_backward(hfgpu_handle* h, const double* D, double scale, double* dE_dR, int precision) {
+  if (!h || !D || !dE_dR) return HFGPU_ERR_INVALID;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  const double* dk[1] = {D};
+  return grad_host(h, D, 2.0, 1, dk, 1.0, scale, dE_dR, precision);
+}
+
+int hfgpu_grad2e_uhf_backward(hfgpu_handle* h, const double* Da, const double* Db, double scale, double* dE_dR,
+                              int precision) {
+  if (!h || !Da || !Db || !dE_dR) return HFGPU_ERR_INVALID;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  const size_t nn = (size_t)h->n * h->n;
+  std::vector<double> Dt(nn);
+  for (size_t i = 0; i < nn; ++i) Dt[i] = Da[i] + Db[i];
+  const double* dk[2] = {Da, Db};
+  return grad_host(h, Dt.data(), 0.5, 2, dk, 0.5, scale, dE_dR, precision);
+}
+
+// Host-only basis view for the one-electron code (normalised coefficients).
+struct OneEHost {
+  std::vector<int> off, first;
+  std::vector<double> coefs;
+  OneEBasis b{};
+};
+
+static int onee_basis(const hfgpu_basis* in, OneEHost& o) {
+  if (!in || in->nshell <= 0 || !in->L || !in->shell_atom || !in->nprim || !in->exps || !in->coefs)
+    return HFGPU_ERR_INVALID;
+  const int ns = in->nshell;
+  o.off.assign(ns + 1, 0);
+  o.first.assign(ns + 1, 0);
+  for (int s = 0; s < ns; ++s) {
+    if (in->L[s] < 0 || in->L[s] > 2 || in->nprim[s] < 1) return HFGPU_ERR_INVALID;
+    o.off[s + 1] = o.off[s] + in->nprim[s];
+    o.first[s + 1] = o.first[s] + (in->pure ? 2 * in->L[s] + 1 : (in->L[s] + 1) * (in->L[s] + 2) / 2);
+  }
+  o.coefs.resize(o.off[ns]);
+  for (int s = 0; s < ns; ++s)
+    normalise(in->L[s], in->nprim[s], &in->exps[o.off[s]], &in->coefs[o.off[s]], &o.coefs[o.off[s]]);
+  o.b.nshell = ns;
+  o.b.n = o.first[ns];
+  o.b.pure = in->pure ? 1 : 0;
+  o.b.L = in->L;
+  o.b.atom = in->shell_atom;
+  o.b.nprim = in->nprim;
+  o.b.off = o.off.data();
+  o.b.first = o.first.data();
+  o.b.exps = in->exps;
+  o.b.coefs = o.coefs.data();
+  return HFGPU_OK;
+}
+
+int hfgpu_one_electron(const hfgpu_basis* basis, const double* xyz, const double* Z, double* S, double* T, double* V) {
+  OneEHost o;
+  if (!xyz || !Z || !S || !T || !V || onee_basis(basis, o)) return HFGPU_ERR_INVALID;
+  hfgpu_onee_matrices(o.b, Z, xyz, basis->natoms, S, T, V);
+  return HFGPU_OK;
+}
+
+int hfgpu_one_electron_grad(const hfgpu_basis* basis, const double* xyz, const double* Z, const double* D,
+                            const double* W, double cH, double cS, double* grad) {
+  OneEHost o;
+  if (!xyz || !Z || !D || !W || !grad || onee_basis(basis, o)) return HFGPU_ERR_INVALID;
+  hfgpu_onee_gradient(o.b, Z, xyz, basis->natoms, D, W, cH, cS, grad);
+  return HFGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,455 @@
+// Two-electron kernels, templated on the shell-quartet class.
+//
+// One thread owns one unique shell quartet (ab|cd) (a b and c d canonical pairs,
+// pair(ab) <= pair(cd) in the sorted pair order) and
+//   * computes its contracted block with the class's generated VRR/HRR code,
+//   * transforms it to spherical functions when the basis is pure,
+//   * digests it straight into J and K (FP64 atomics into half-matrices that are
+//     symmetrised afterwards), or contracts it with density weights for the
+//     adjoint gradient.
+// Quartets are listed per class (one launch per class), grouped by primitive
+// counts so that a warp's threads run loops of equal length.
+#pragma once
+#include "hfgpu_common.cuh"
+#include "generated/common.cuh"
+
+// Arguments shared by every J/K launch.
+template <typename R>
+struct JKArgs {
+  const PairInfo* __restrict__ pairs;
+  const PrimPair<R>* __restrict__ prims;
+  BoysTable<R> boys;
+  int n;                             // basis functions
+  int nshell;
+  const double* __restrict__ DJ;     // density for J (n x n) or nullptr
+  int nK;                            // densities for K
+  const double* __restrict__ DK;     // nK x n x n
+  double* __restrict__ Jh;           // n x n half accumulator (symmetrised later)
+  double* __restrict__ Kh;           // nK x n x n
+  const float* __restrict__ dmax;    // nshell x nshell max |D| over all densities, or nullptr
+  double dtol;                       // density-weighted screening threshold
+  unsigned long long* __restrict__ counters;  // [0] quartets computed, [1] skipped by density
+};
+
+template <typename R>
+struct GradArgs {
+  const PairInfo* __restrict__ pairs;
+  const PrimPair<R>* __restrict__ prims;
+  const R* __restrict__ alpha_a;     // per primitive pair: exponent of shell a
+  const R* __restrict__ alpha_b;     // per primitive pair: exponent of shell b
+  BoysTable<R> boys;
+  int n;
+  const double* __restrict__ DJ;
+  double cJ;
+  int nK;
+  const double* __restrict__ DK;
+  double cK;
+  double* __restrict__ grad;         // natoms x 3
+  R* __restrict__ scratch;           // thread-interleaved scratch (table-mode classes)
+  int scratch_threads;               // threads sharing the scratch (stride)
+};
+
+template <int NA, int NB, int NC, int ND>
+__device__ __forceinline__ void load_block(const double* __restrict__ D, int n, int f0, int f1, int n0, int n1,
+                                           double* out) {
+#pragma unroll
+  for (int i = 0; i < n0; ++i)
+#pragma unroll
+    for (int j = 0; j < n1; ++j) out[i * n1 + j] = __ldg(D + (size_t)(f0 + i) * n + f1 + j);
+}
+
+// J/K digestion of one block V[a][b][c][d] (final basis), scaled by the quartet's
+// degeneracy s: Jh_ab += 2s sum_cd D_cd V, Jh_cd += 2s sum_ab D_ab V,
+// Kh_ac += s sum_bd D_bd V, Kh_ad += s D_bc V, Kh_bc += s D_ad V, Kh_bd += s D_ac V.
+template <int NA, int NB, int NC, int ND>
+__device__ __forceinline__ void digest_jk(const double* V, int fa, int fb, int fc, int fd, double s,
+                                          const double* __restrict__ DJ,
+                                          int nK, const double* __restrict__ DK, double* Jh, double* Kh, int n) {
+  constexpr int NV = NA * NB * NC * ND;
+  constexpr bool SMALL = NV <= 81;
+  if (DJ != nullptr) {
+    double dcd[NC * ND], dab[NA * NB];
+    load_block<NA, NB, NC, ND>(DJ, n, fc, fd, NC, ND, dcd);
+    load_block<NA, NB, NC, ND>(DJ, n, fa, fb, NA, NB, dab);
+    double jcd[NC * ND];
+#pragma unroll
+    for (int x = 0; x < NC * ND; ++x) jcd[x] = 0.0;
+#pragma unroll(SMALL ? NA * NB : 1)
+    for (int ab = 0; ab < NA * NB; ++ab) {
+      double jab = 0.0;
+      const double dv = dab[ab];
+#pragma unroll
+      for (int cd = 0; cd < NC * ND; ++cd) {
+        const double v = V[ab * NC * ND + cd];
+        jab += dcd[cd] * v;
+        jcd[cd] += dv * v;
+      }
+      atomicAdd(Jh + (size_t)(fa + ab / NB) * n + fb + ab % NB, 2.0 * s * jab);
+    }
+#pragma unroll
+    for (int cd = 0; cd < NC * ND; ++cd) atomicAdd(Jh + (size_t)(fc + cd / ND) * n + fd + cd % ND, 2.0 * s * jcd[cd]);
+  }
+  for (int m = 0; m < nK; ++m) {
+    const double* D = DK + (size_t)m * n * n;
+    double* K = Kh + (size_t)m * n * n;
+    double dbd[NB * ND], dbc[NB * NC], dad[NA * ND], dac[NA * NC];
+    load_block<NA, NB, NC, ND>(D, n, fb, fd, NB, ND, dbd);
+    load_block<NA, NB, NC, ND>(D, n, fb, fc, NB, NC, dbc);
+    load_block<NA, NB, NC, ND>(D, n, fa, fd, NA, ND, dad);
+    load_block<NA, NB, NC, ND>(D, n, fa, fc, NA, NC, dac);
+    double kbc[NB * NC], kbd[NB * ND];
+#pragma unroll
+    for (int x = 0; x < NB * NC; ++x) kbc[x] = 0.0;
+#pragma unroll
+    for (int x = 0; x < NB * ND; ++x) kbd[x] = 0.0;
+#pragma unroll(SMALL ? NA : 1)
+    for (int i = 0; i < NA; ++i) {
+      double kac[NC], kad[ND];
+#pragma unroll
+      for (int x = 0; x < NC; ++x) kac[x] = 0.0;
+#pragma unroll
+      for (int x = 0; x < ND; ++x) kad[x] = 0.0;
+#pragma unroll
+      for (int j = 0; j < NB; ++j)
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+#pragma unroll
+          for (int l = 0; l < ND; ++l) {
+            const double v = V[((i * NB + j) * NC + k) * ND + l];
+            kac[k] += dbd[j * ND + l] * v;
+            kad[l] += dbc[j * NC + k] * v;
+            kbc[j * NC + k] += dad[i * ND + l] * v;
+            kbd[j * ND + l] += dac[i * NC + k] * v;
+          }
+#pragma unroll
+      for (int k = 0; k < NC; ++k) atomicAdd(K + (size_t)(fa + i) * n + fc + k, s * kac[k]);
+#pragma unroll
+      for (int l = 0; l < ND; ++l) atomicAdd(K + (size_t)(fa + i) * n + fd + l, s * kad[l]);
+    }
+#pragma unroll
+    for (int x = 0; x < NB * NC; ++x) atomicAdd(K + (size_t)(fb + x / NC) * n + fc + x % NC, s * kbc[x]);
+#pragma unroll
+    for (int x = 0; x < NB * ND; ++x) atomicAdd(K + (size_t)(fb + x / ND) * n + fd + x % ND, s * kbd[x]);
+  }
+}
+
+template <int LA, int LB, int LC, int LD, bool PURE>
+struct BlockDims {
+  static constexpr int CA = ncart_of(LA), CB = ncart_of(LB), CC = ncart_of(LC), CD = ncart_of(LD);
+  static constexpr int NA = PURE ? npure_of(LA) : CA, NB = PURE ? npure_of(LB) : CB;
+  static constexpr int NC = PURE ? npure_of(LC) : CC, ND = PURE ? npure_of(LD) : CD;
+  static constexpr int NCART = CA * CB * CC * CD;
+  static constexpr int NOUT = NA * NB * NC * ND;
+};
+
+// Contracted block of quartet (P|Q) in the final basis, as doubles.
+template <int LA, int LB, int LC, int LD, typename R, bool PURE>
+__device__ __forceinline__ void finish_block(const R* cart, double* V) {
+  using Dm = BlockDims<LA, LB, LC, LD, PURE>;
+  if constexpr (PURE) {
+    R pure[Dm::NOUT];
+    ClassCode<LA, LB, LC, LD>::template to_pure<R>(cart, pure);
+#pragma unroll
+    for (int x = 0; x < Dm::NOUT; ++x) V[x] = double(pure[x]);
+  } else {
+#pragma unroll
+    for (int x = 0; x < Dm::NOUT; ++x) V[x] = double(cart[x]);
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename R>
+__device__ __forceinline__ void cart_block(const PairInfo& P, const PairInfo& Q, const PrimPair<R>* prims,
+                                           const BoysTable<R>& boys, R* cart) {
+  ClassCode<LA, LB, LC, LD>::template eri<R>(prims + P.prim_off, P.nprim, prims + Q.prim_off, Q.nprim,
+                                              R(P.ABx), R(P.ABy), R(P.ABz), R(Q.ABx), R(Q.ABy), R(Q.ABz), boys, cart);
+}
+
+__device__ __forceinline__ long long packed_index(long long i, long long j, long long k, long long l) {
+  const long long ij = i > j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i;
+  const long long kl = k > l ? k * (k + 1) / 2 + l : l * (l + 1) / 2 + k;
+  return ij > kl ? ij * (ij + 1) / 2 + kl : kl * (kl + 1) / 2 + ij;
+}
+
+enum : int { QMODE_JK = 0, QMODE_PACKED = 1, QMODE_SCHWARZ = 2 };
+
+// What one thread does with its block, by mode:
+//   JK      digest into J/K;
+//   PACKED  write the unique ERIs into the reference's packed 8-fold vector
+//           (hfscfmath::index_ijkl, src/math/hfscf_math.hpp:90-101);
+//   SCHWARZ (P|P) only: store sqrt(max |(ab|ab)|) into the pair.
+template <int LA, int LB, int LC, int LD, bool PURE>
+__device__ __forceinline__ void use_block(const double* V, int mode, const int2 pq, const PairInfo& P,
+                                          const PairInfo& Q, double s, const double* __restrict__ DJ, int nK,
+                                          const double* __restrict__ DK, double* Jh, double* Kh, int n, double* eri,
+                                          PairInfo* pairs_rw) {
+  using Dm = BlockDims<LA, LB, LC, LD, PURE>;
+  if (mode == QMODE_JK) {
+    digest_jk<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(V, P.fa, P.fb, Q.fa, Q.fb, s, DJ, nK, DK, Jh, Kh, n);
+  } else if (mode == QMODE_PACKED) {
+    for (int i = 0; i < Dm::NA; ++i)
+      for (int j = 0; j < Dm::NB; ++j)
+        for (int k = 0; k < Dm::NC; ++k)
+          for (int l = 0; l < Dm::ND; ++l)
+            eri[packed_index(P.fa + i, P.fb + j, Q.fa + k, Q.fb + l)] = V[((i * Dm::NB + j) * Dm::NC + k) * Dm::ND + l];
+  } else {
+    double m = 0.0;
+    for (int i = 0; i < Dm::NA; ++i)
+      for (int j = 0; j < Dm::NB; ++j) m = fmax(m, fabs(V[((i * Dm::NB + j) * Dm::NC + i) * Dm::ND + j]));
+    pairs_rw[pq.x].schwarz = sqrt(m);
+  }
+}
+
+template <typename R>
+struct QuartetArgs {
+  JKArgs<R> jk;
+  int mode;
+  int pure;
+  double* eri;          // PACKED output
+  PairInfo* pairs_rw;   // SCHWARZ output
+};
+
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets, int nq) {
+  const JKArgs<R>& a = qa.jk;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nq) return;
+  const int2 pq = quartets[t];
+  const PairInfo P = a.pairs[pq.x];
+  const PairInfo Q = a.pairs[pq.y];
+  if (qa.mode == QMODE_JK && a.dmax != nullptr) {
+    // density-weighted Schwarz bound: Q_ab Q_cd max(4|D_ab|, 4|D_cd|, |D_ac|, |D_ad|, |D_bc|, |D_bd|)
+    const float* dm = a.dmax;
+    const int ns = a.nshell;
+    float m = 4.f * fmaxf(dm[P.sa * ns + P.sb], dm[Q.sa * ns + Q.sb]);
+    m = fmaxf(m, fmaxf(fmaxf(dm[P.sa * ns + Q.sa], dm[P.sa * ns + Q.sb]), fmaxf(dm[P.sb * ns + Q.sa], dm[P.sb * ns + Q.sb])));
+    if (P.schwarz * Q.schwarz * double(m) < a.dtol) {
+      if (a.counters) atomicAdd(a.counters + 1, 1ull);
+      return;
+    }
+  }
+  using Dc = BlockDims<LA, LB, LC, LD, false>;
+  R cart[Dc::NCART];
+  cart_block<LA, LB, LC, LD, R>(P, Q, a.prims, a.boys, cart);
+  double s = 1.0;
+  if (P.sa == P.sb) s *= 0.5;
+  if (Q.sa == Q.sb) s *= 0.5;
+  if (pq.x == pq.y) s *= 0.5;
+  if (qa.pure) {
+    using Dp = BlockDims<LA, LB, LC, LD, true>;
+    double V[Dp::NOUT];
+    finish_block<LA, LB, LC, LD, R, true>(cart, V);
+    use_block<LA, LB, LC, LD, true>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri, qa.pairs_rw);
+  } else {
+    double V[Dc::NOUT];
+    finish_block<LA, LB, LC, LD, R, false>(cart, V);
+    use_block<LA, LB, LC, LD, false>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri, qa.pairs_rw);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint gradient.
+// ---------------------------------------------------------------------------
+template <typename R>
+struct Strided {
+  R* base;
+  int stride;
+  __device__ __forceinline__ R& operator[](int i) const { return base[(size_t)i * stride]; }
+};
+
+
+// Executor of a table-mode gradient class (ops generated by gen_eri.py).
+template <typename R, typename Tab>
+__device__ void grad_table(const PrimPair<R>* __restrict__ bp, const R* __restrict__ ea, const R* __restrict__ eb,
+                           int nbp, const PrimPair<R>* __restrict__ kp, const R* __restrict__ ec, int nkp, R ABx,
+                           R ABy, R ABz, R CDx, R CDy, R CDz, const BoysTable<R>& boys, Strided<R> W, Strided<R> vs,
+                           Strided<R> hs, R* g) {
+  vs[0] = R(0);
+  hs[0] = R(0);
+  for (int x = 1; x <= Tab::NACC; ++x) hs[x] = R(0);
+  const int(*vo)[10] = Tab::vrr();
+  const int(*ho)[8] = Tab::hrr();
+  for (int ib = 0; ib < nbp; ++ib) {
+    const R p = bp[ib].p, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;
+    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].K;
+    const R wa = R(2) * ea[ib], wb = R(2) * eb[ib];
+    for (int ik = 0; ik < nkp; ++ik) {
+      const R q = kp[ik].p, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;
+      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].K;
+      const R wc = R(2) * ec[ik];
+      const R pq = p + q;
+      const R ipq = R(1) / pq;
+      const R rho = p * q * ipq;
+      const R rp = q * ipq, rq = p * ipq;
+      const R inv2p = R(0.5) / p, inv2q = R(0.5) / q, inv2pq = R(0.5) * ipq;
+      const R PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+      const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+      const R pre = Kab * Kcd * R(PI_2_5) / (p * q * sqrt_t(pq));
+      R F[Tab::L + 1];
+      boys.template eval<Tab::L>(T, pre, F);
+#pragma unroll
+      for (int m = 0; m <= Tab::L; ++m) vs[1 + m] = F[m];
+      for (int o = 0; o < Tab::NVOPS; ++o) {
+        const int kind = __ldg(&vo[o][0]), dir = __ldg(&vo[o][1]), dst = __ldg(&vo[o][2]);
+        const int sa = __ldg(&vo[o][3]), sb = __ldg(&vo[o][4]), sc = __ldg(&vo[o][5]), sd = __ldg(&vo[o][6]);
+        if (kind == 2) {
+          const R w = dir == 0 ? R(1) : (dir == 1 ? wa : (dir == 2 ? wb : wc));
+          hs[1 + dst] += w * vs[sa];
+          continue;
+        }
+        const R PQd = dir == 0 ? PQx : (dir == 1 ? PQy : PQz);
+        const int k1 = __ldg(&vo[o][8]);
+        if (kind == 0) {
+          const R PA = dir == 0 ? PAx : (dir == 1 ? PAy : PAz);
+          vs[dst] = PA * vs[sa] - rp * PQd * vs[sb] + R(k1) * inv2p * (vs[sc] - rp * vs[sd]);
+        } else {
+          const R QC = dir == 0 ? QCx : (dir == 1 ? QCy : QCz);
+          const int sg = __ldg(&vo[o][7]), k2 = __ldg(&vo[o][9]);
+          vs[dst] = QC * vs[sa] + rq * PQd * vs[sb] + R(k1) * inv2q * (vs[sc] - rq * vs[sd]) + R(k2) * inv2pq * vs[sg];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int x = 0; x < 9; ++x) g[x] = R(0);
+  for (int o = 0; o < Tab::NHOPS; ++o) {
+    const int kind = __ldg(&ho[o][0]), dir = __ldg(&ho[o][1]), dst = __ldg(&ho[o][2]);
+    const int sx = __ldg(&ho[o][3]), sy = __ldg(&ho[o][4]);
+    if (kind == 2) {
+      const int k = __ldg(&ho[o][5]);
+      const R v = W[dst] * (hs[sx] - R(k) * hs[sy]);
+#pragma unroll
+      for (int x = 0; x < 9; ++x)
+        if (x == dir) g[x] += v;
+    } else {
+      const R d = kind == 0 ? (dir == 0 ? ABx : (dir == 1 ? ABy : ABz)) : (dir == 0 ? CDx : (dir == 1 ? CDy : CDz));
+      hs[dst] = hs[sx] + d * hs[sy];
+    }
+  }
+}
+
+// Weight block of a unique quartet in the final basis:
+// W_abcd = 8 s [cJ DJ_ab DJ_cd - (cK/2) sum_m (DK_ac DK_bd + DK_ad DK_bc)],
+// the average of cJ DJ_pq DJ_rs - cK DK_pr DK_qs over the quartet's 8 index images.
+template <int NA, int NB, int NC, int ND, typename Out>
+__device__ __forceinline__ void grad_weights(const double* __restrict__ DJ, double cJ,
+                                             int nK, const double* __restrict__ DK, double cK, int n, int fa, int fb,
+                                             int fc, int fd, double s8, Out W) {
+  for (int i = 0; i < NA; ++i)
+    for (int j = 0; j < NB; ++j) {
+      const double dab = DJ ? __ldg(DJ + (size_t)(fa + i) * n + fb + j) : 0.0;
+      for (int k = 0; k < NC; ++k)
+        for (int l = 0; l < ND; ++l) {
+          double w = DJ ? cJ * dab * __ldg(DJ + (size_t)(fc + k) * n + fd + l) : 0.0;
+          for (int m = 0; m < nK; ++m) {
+            const double* D = DK + (size_t)m * n * n;
+            w -= 0.5 * cK *
+                 (__ldg(D + (size_t)(fa + i) * n + fc + k) * __ldg(D + (size_t)(fb + j) * n + fd + l) +
+                  __ldg(D + (size_t)(fa + i) * n + fd + l) * __ldg(D + (size_t)(fb + j) * n + fc + k));
+          }
+          W[((i * NB + j) * NC + k) * ND + l] = s8 * w;
+        }
+    }
+}
+
+template <int LA, int LB, int LC, int LD, typename R, bool PURE>
+__device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, const int2 pq) {
+  using Dm = BlockDims<LA, LB, LC, LD, PURE>;
+  using CC = ClassCode<LA, LB, LC, LD>;
+  {
+    const PairInfo P = a.pairs[pq.x];
+    const PairInfo Q = a.pairs[pq.y];
+    double s = 8.0;
+    if (P.sa == P.sb) s *= 0.5;
+    if (Q.sa == Q.sb) s *= 0.5;
+    if (pq.x == pq.y) s *= 0.5;
+    R g[9];
+    if constexpr (CC::kGradTable) {
+      using Tab = typename CC::GradTab;
+      // scratch layout per thread: [VRR slots | HRR slots | W cart | 2 transform buffers]
+      R* base = a.scratch + tid;
+      Strided<R> vs{base, a.scratch_threads};
+      Strided<R> hs{base + (size_t)Tab::NVSLOT * a.scratch_threads, a.scratch_threads};
+      Strided<R> Wc{base + (size_t)(Tab::NVSLOT + Tab::NHSLOT) * a.scratch_threads, a.scratch_threads};
+      Strided<R> t0{base + (size_t)(Tab::NVSLOT + Tab::NHSLOT + Dm::NCART) * a.scratch_threads, a.scratch_threads};
+      Strided<R> t1{base + (size_t)(Tab::NVSLOT + Tab::NHSLOT + 2 * Dm::NCART) * a.scratch_threads, a.scratch_threads};
+      if constexpr (PURE) {
+        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb,
+                                                     Q.fa, Q.fb, s, t0);
+        // pure -> Cartesian weights, one index at a time: t0 -> t1 -> t0 -> t1 -> Wc
+        const int Ls[4] = {LA, LB, LC, LD};
+        int dims[4] = {Dm::NA, Dm::NB, Dm::NC, Dm::ND};
+        Strided<R> src = t0, dst = t1;
+        for (int st = 0; st < 4; ++st) {
+          const int nc = ncart_of(Ls[st]), np = npure_of(Ls[st]);
+          int nd[4] = {dims[0], dims[1], dims[2], dims[3]};
+          nd[st] = nc;
+          Strided<R> out = (st == 3) ? Wc : dst;
+          const int tot = nd[0] * nd[1] * nd[2] * nd[3];
+          for (int e = 0; e < tot; ++e) {
+            int id[4];
+            int r = e;
+            for (int q = 3; q >= 0; --q) {
+              id[q] = r % nd[q];
+              r /= nd[q];
+            }
+            R v = R(0);
+            for (int c = 0; c < np; ++c) {
+              const double y = c_ylm[Ls[st]][id[st] * np + c];
+              if (y == 0.0) continue;
+              int jd[4] = {id[0], id[1], id[2], id[3]};
+              jd[st] = c;
+              v += R(y) * src[((jd[0] * dims[1] + jd[1]) * dims[2] + jd[2]) * dims[3] + jd[3]];
+            }
+            out[e] = v;
+          }
+          for (int q = 0; q < 4; ++q) dims[q] = nd[q];
+          Strided<R> tmp = src;
+          src = dst;
+          dst = tmp;
+        }
+      } else {
+        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb,
+                                                     Q.fa, Q.fb, s, Wc);
+      }
+      grad_table<R, Tab>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
+                         a.prims + Q.prim_off, a.alpha_a + Q.prim_off, Q.nprim, R(P.ABx), R(P.ABy), R(P.ABz),
+                         R(Q.ABx), R(Q.ABy), R(Q.ABz), a.boys, Wc, vs, hs, g);
+    } else {
+      R Wc[Dm::NCART];
+      if constexpr (PURE) {
+        R Wp[Dm::NOUT];
+        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb,
+                                                     Q.fa, Q.fb, s, Wp);
+        CC::template from_pure<R>(Wp, Wc);
+      } else {
+        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb,
+                                                     Q.fa, Q.fb, s, Wc);
+      }
+      CC::template grad<R>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
+                           a.prims + Q.prim_off, a.alpha_a + Q.prim_off, Q.nprim, R(P.ABx), R(P.ABy), R(P.ABz),
+                           R(Q.ABx), R(Q.ABy), R(Q.ABz), a.boys, Wc, g, g + 3, g + 6);
+    }
+    const int at[3] = {P.atom_a, P.atom_b, Q.atom_a};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double gA = double(g[d]), gB = double(g[3 + d]), gC = double(g[6 + d]);
+      atomicAdd(a.grad + 3 * at[0] + d, gA);
+      atomicAdd(a.grad + 3 * at[1] + d, gB);
+      atomicAdd(a.grad + 3 * at[2] + d, gC);
+      atomicAdd(a.grad + 3 * Q.atom_b + d, -(gA + gB + gC));
+    }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(128) grad_kernel(GradArgs<R> a, int pure, const int2* __restrict__ quartets, int nq) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthr = gridDim.x * blockDim.x;
+  for (int t = tid; t < nq; t += nthr) {
+    if (pure)
+      grad_quartet<LA, LB, LC, LD, R, true>(a, tid, quartets[t]);
+    else
+      grad_quartet<LA, LB, LC, LD, R, false>(a, tid, quartets[t]);
+  }
+}
+

@@ -1,0 +1,24 @@
+// Host-visible launchers of the per-class kernels (one translation unit per class).
+#pragma once
+#include <cuda_runtime.h>
+
+template <typename R>
+struct QuartetArgs;
+template <typename R>
+struct GradArgs;
+
+namespace hfgpu {
+
+struct ClassLaunchers {
+  int la, lb, lc, ld;
+  void (*quartet_d)(const QuartetArgs<double>&, const int2*, int, cudaStream_t);
+  void (*quartet_f)(const QuartetArgs<float>&, const int2*, int, cudaStream_t);
+  void (*grad_d)(const GradArgs<double>&, int pure, const int2*, int, int grid, cudaStream_t);
+  void (*grad_f)(const GradArgs<float>&, int pure, const int2*, int, int grid, cudaStream_t);
+  int (*grad_scratch_slots)(int pure);  // per-thread scratch of table-mode gradient classes (0 otherwise)
+};
+
+extern const ClassLaunchers* const kClassLaunchers[];
+extern const int kNumClasses;
+
+}  // namespace hfgpu

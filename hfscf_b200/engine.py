@@ -1,0 +1,252 @@
+"""Python mirror of the engine's C ABI (include/hfgpu.h).
+
+``Erios`` mirrors the reference's integral-engine interface
+(ERIOS::Erios, src/integrals/hfscf_oseri.hpp:27-123) and ``FockBuilder`` the
+Fock hooks of Mol::hf_solver / Mol::uhf_solver
+(src/scfsolver/hfscf_hf_solver.cpp:254-286, hfscf_uhf_solver.cpp:155-191).  Both
+sit on one ``Engine`` handle.  Every call goes to the CUDA library
+``libhfgpu.so``; there is no CPU fallback, and a missing library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .basis import Basis
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhfgpu.so")
+
+FP64, MIXED = 0, 1
+STATUS = {0: "ok", 1: "invalid argument", 2: "out of memory", 3: "CUDA error", 4: "bad call order",
+          5: "non-finite result", 6: "unsupported"}
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class HfgpuError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"hfgpu error {code} ({STATUS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class _Basis(ctypes.Structure):
+    _fields_ = [("nshell", ctypes.c_int), ("natoms", ctypes.c_int), ("pure", ctypes.c_int),
+                ("L", _ip), ("shell_atom", _ip), ("nprim", _ip), ("exps", _dp), ("coefs", _dp)]
+
+
+class _Opts(ctypes.Structure):
+    _fields_ = [("schwarz_tol", ctypes.c_double), ("density_tol", ctypes.c_double),
+                ("mixed_fp32_bound", ctypes.c_double), ("device", ctypes.c_int),
+                ("reserved", ctypes.c_int * 7)]
+
+
+def lib():
+    """The CUDA engine library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m hfscf_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.hfgpu_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names declared in include/hfgpu.h (checked against the library by the tests)."""
+    import re
+    hdr = os.path.join(os.path.dirname(HERE), "include", "hfgpu.h")
+    text = open(hdr).read()
+    return sorted(set(re.findall(r"\b(hfgpu_[a-z0-9_]+)\s*\(", text)))
+
+
+def _p(a, ct=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+def _c(a, dtype=np.float64):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class _BasisView:
+    """Keeps the flat basis arrays alive while the C struct points at them."""
+
+    def __init__(self, basis: Basis):
+        f = basis.flat()
+        self.L = _c(f["L"], np.int32)
+        self.atom = _c(f["atom"], np.int32)
+        self.nprim = _c(f["nprim"], np.int32)
+        self.exps = _c(f["exps"])
+        self.coefs = _c(f["coefs"])
+        self.s = _Basis(basis.nshell, basis.natoms, int(basis.pure), _p(self.L, ctypes.c_int),
+                        _p(self.atom, ctypes.c_int), _p(self.nprim, ctypes.c_int), _p(self.exps), _p(self.coefs))
+
+
+class Engine:
+    """One engine handle: a basis on one GPU, with the current geometry."""
+
+    def __init__(self, basis: Basis, schwarz_tol=1e-12, density_tol=1e-12, mixed_fp32_bound=1e-4, device=0):
+        self.basis = basis
+        self.n = basis.nbf
+        self._bv = _BasisView(basis)
+        o = _Opts()
+        lib().hfgpu_default_opts(ctypes.byref(o))
+        o.schwarz_tol, o.density_tol, o.mixed_fp32_bound, o.device = schwarz_tol, density_tol, mixed_fp32_bound, device
+        self._opts = o
+        h = ctypes.c_void_p()
+        self._check(lib().hfgpu_create(ctypes.byref(self._bv.s), ctypes.byref(o), ctypes.byref(h)), None)
+        self.h = h
+        self.coords = None
+        self.set_geometry(basis.coords)
+
+    def _check(self, rc, h="self"):
+        if rc != 0:
+            msg = ""
+            hh = self.h if h == "self" else h
+            if hh is not None:
+                msg = lib().hfgpu_last_error(hh).decode()
+            raise HfgpuError(rc, msg)
+
+    def close(self):
+        if getattr(self, "h", None) is not None:
+            lib().hfgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- geometry / integrals -------------------------------------------------
+    def set_geometry(self, coords_bohr):
+        c = _c(coords_bohr).reshape(-1, 3)
+        self._check(lib().hfgpu_set_geometry(self.h, _p(c), ctypes.c_int(len(c))))
+        self.coords = c.copy()
+        self.basis = self.basis.with_coords(c)
+
+    def schwarz(self) -> np.ndarray:
+        ns = self.basis.nshell
+        Q = np.zeros((ns, ns))
+        self._check(lib().hfgpu_schwarz(self.h, _p(Q)))
+        return Q
+
+    def eri_packed(self) -> np.ndarray:
+        n = self.n
+        ln = n * (n + 1) * (n * n + n + 2) // 8
+        out = np.zeros(ln)
+        self._check(lib().hfgpu_eri_packed(self.h, _p(out), ctypes.c_longlong(ln)))
+        return out
+
+    # --- Fock builds -----------------------------------------------------------
+    def jk(self, DJ=None, DKs=(), precision=FP64):
+        n = self.n
+        DJc = _c(DJ) if DJ is not None else None
+        DK = _c(np.stack(DKs)) if len(DKs) else np.zeros((0, n, n))
+        J = np.zeros((n, n))
+        K = np.zeros((len(DKs), n, n))
+        self._check(lib().hfgpu_jk(self.h, _p(DJc) if DJc is not None else None, ctypes.c_int(len(DKs)),
+                                   _p(DK) if len(DKs) else None, _p(J), _p(K) if len(DKs) else None,
+                                   ctypes.c_int(precision)))
+        return (J if DJ is not None else None), K
+
+    def fock_rhf(self, D, H, precision=FP64) -> np.ndarray:
+        F = np.zeros((self.n, self.n))
+        self._check(lib().hfgpu_fock_rhf(self.h, _p(_c(D)), _p(_c(H)), _p(F), ctypes.c_int(precision)))
+        return F
+
+    def fock_uhf(self, Da, Db, H, precision=FP64):
+        Fa, Fb = np.zeros((self.n, self.n)), np.zeros((self.n, self.n))
+        self._check(lib().hfgpu_fock_uhf(self.h, _p(_c(Da)), _p(_c(Db)), _p(_c(H)), _p(Fa), _p(Fb),
+                                         ctypes.c_int(precision)))
+        return Fa, Fb
+
+    def fock_delta(self, dD, F, precision=FP64) -> np.ndarray:
+        F = _c(F).copy()
+        self._check(lib().hfgpu_fock_delta(self.h, _p(_c(dD)), _p(F), ctypes.c_int(precision)))
+        return F
+
+    def last_counts(self):
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(lib().hfgpu_last_counts(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    # --- autograd-shaped pair ---------------------------------------------------
+    def energy2e(self, D, precision=FP64) -> float:
+        e = ctypes.c_double()
+        self._check(lib().hfgpu_energy_forward(self.h, _p(_c(D)), ctypes.byref(e), ctypes.c_int(precision)))
+        return e.value
+
+    def grad2e(self, D, scale=1.0, precision=FP64) -> np.ndarray:
+        g = np.zeros((self.basis.natoms, 3))
+        self._check(lib().hfgpu_grad2e_backward(self.h, _p(_c(D)), ctypes.c_double(scale), _p(g),
+                                                ctypes.c_int(precision)))
+        return g
+
+    def grad2e_uhf(self, Da, Db, scale=1.0, precision=FP64) -> np.ndarray:
+        g = np.zeros((self.basis.natoms, 3))
+        self._check(lib().hfgpu_grad2e_uhf_backward(self.h, _p(_c(Da)), _p(_c(Db)), ctypes.c_double(scale), _p(g),
+                                                    ctypes.c_int(precision)))
+        return g
+
+
+# --- one-electron integrals (host CPU, no handle) ---------------------------------
+def one_electron(basis: Basis):
+    bv = _BasisView(basis)
+    n = basis.nbf
+    S, T, V = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
+    Z = _c(basis.Z)
+    xyz = _c(basis.coords)
+    rc = lib().hfgpu_one_electron(ctypes.byref(bv.s), _p(xyz), _p(Z), _p(S), _p(T), _p(V))
+    if rc:
+        raise HfgpuError(rc)
+    return S, T, V
+
+
+def one_electron_grad(basis: Basis, D, W, cH, cS) -> np.ndarray:
+    bv = _BasisView(basis)
+    g = np.zeros((basis.natoms, 3))
+    rc = lib().hfgpu_one_electron_grad(ctypes.byref(bv.s), _p(_c(basis.coords)), _p(_c(basis.Z)), _p(_c(D)),
+                                       _p(_c(W)), ctypes.c_double(cH), ctypes.c_double(cS), _p(g))
+    if rc:
+        raise HfgpuError(rc)
+    return g
+
+
+class Erios:
+    """Interface of the reference's ERIOS::Erios over the GPU engine
+    (src/integrals/hfscf_oseri.hpp:27-123): packed ERIs and the Schwarz diagonal."""
+
+    def __init__(self, engine: Engine):
+        self.engine = engine
+
+    def compute_repulsion_packed(self):
+        return self.engine.eri_packed()
+
+    def compute_screen_matrix(self):
+        return self.engine.schwarz()
+
+
+class FockBuilder:
+    """The Fock hooks of Mol::hf_solver / Mol::uhf_solver over the GPU engine."""
+
+    def __init__(self, engine: Engine, precision=FP64):
+        self.engine = engine
+        self.precision = precision
+
+    def update_fock_matrix(self, D, H):
+        return self.engine.fock_rhf(D, H, self.precision)
+
+    def update_fock_matrix_uhf(self, Da, Db, H):
+        return self.engine.fock_uhf(Da, Db, H, self.precision)

@@ -1,0 +1,142 @@
+/* hfgpu: B200 two-electron engine for hfscf -- C ABI.
+ *
+ * The entry points replace the reference's two-electron hot path:
+ *   - ERIOS::Erios (src/integrals/hfscf_oseri.hpp:27-123): Obara-Saika ERIs,
+ *     Schwarz diagonal, first-derivative ERIs;
+ *   - Mol::hf_solver::update_fock_matrix (src/scfsolver/hfscf_hf_solver.cpp:254-286)
+ *     and Mol::uhf_solver::update_fock_matrix (src/scfsolver/hfscf_uhf_solver.cpp:155-191);
+ *   - the two-electron term of Mol::scf_gradient::calc_scf_gradient_rhf/uhf
+ *     (src/gradient/hfscf_grad_rhf.cpp:76-141, src/gradient/hfscf_grad_uhf.cpp:124-150).
+ *
+ * Conventions (all as in the reference):
+ *   - matrices are n x n, row-major, FP64; n = number of pure or Cartesian functions;
+ *   - function order: atoms in input order, shells in basis-file order, Cartesian
+ *     components l = L-i, m = i-j, n = j, pure components m = -L..L;
+ *   - densities carry no factor 2 (RHF D = C_occ C_occ^T), F = H + 2J[D] - K[D];
+ *   - J[D]_ij = sum_kl D_kl (ij|kl), K[D]_ij = sum_kl D_kl (ik|jl).
+ *
+ * Every call returns an hfgpu_status (0 = success) and never exits the process.
+ * A handle is not thread-safe: serialise calls on one handle.  Host-pointer entry
+ * points copy inputs to the device and results back, synchronising the handle's
+ * stream; *_device entry points take device pointers and enqueue on that stream.
+ */
+#ifndef HFGPU_H
+#define HFGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hfgpu_handle hfgpu_handle;
+
+typedef enum {
+  HFGPU_OK = 0,
+  HFGPU_ERR_INVALID = 1,     /* bad argument or basis (e.g. L > 2, non-finite exponent) */
+  HFGPU_ERR_NOMEM = 2,       /* device or host allocation failed */
+  HFGPU_ERR_CUDA = 3,        /* CUDA runtime error; see hfgpu_last_error */
+  HFGPU_ERR_STATE = 4,       /* call out of order (e.g. no geometry set) */
+  HFGPU_ERR_NONFINITE = 5,   /* a result was NaN or Inf */
+  HFGPU_ERR_UNSUPPORTED = 6  /* feature not available in this build */
+} hfgpu_status;
+
+typedef enum { HFGPU_FP64 = 0, HFGPU_MIXED = 1 } hfgpu_precision;
+
+/* Basis description: flat arrays, as BASIS::Shell takes them
+ * (src/integrals/hfscf_shell.hpp:21-57).  Coefficients are the UNNORMALISED
+ * values of the basis file; the engine normalises them as the reference's
+ * Shell constructor does (src/integrals/hfscf_shell.cpp:44-54). */
+typedef struct {
+  int nshell;
+  int natoms;
+  int pure;                /* 1 = spherical functions, 0 = Cartesian */
+  const int* L;            /* [nshell] angular momentum, 0..2 */
+  const int* shell_atom;   /* [nshell] atom of each shell */
+  const int* nprim;        /* [nshell] primitives per shell */
+  const double* exps;      /* [sum nprim] exponents */
+  const double* coefs;     /* [sum nprim] contraction coefficients */
+} hfgpu_basis;
+
+typedef struct {
+  double schwarz_tol;      /* quartets with Q_ab Q_cd below this are never computed (default 1e-12,
+                              the reference's screen_tol = 100 * integral_tol, hfscf_oseri.hpp:31-32) */
+  double density_tol;      /* J/K: skip quartets whose density-weighted bound is below this (default 1e-12; 0 = off) */
+  double mixed_fp32_bound; /* mixed precision: quartets with Q_ab Q_cd below this run in FP32 (default 1e-4) */
+  int device;              /* CUDA device ordinal (default 0) */
+  int reserved[7];
+} hfgpu_opts;
+
+int hfgpu_default_opts(hfgpu_opts* opts);
+
+/* Replaces constructing Erios + Molecule::create_shell_pairs
+ * (src/integrals/hfscf_oseri.hpp:30-32, src/molecule/hfscf_molecule.cpp:661-669). */
+int hfgpu_create(const hfgpu_basis* basis, const hfgpu_opts* opts, hfgpu_handle** out);
+int hfgpu_destroy(hfgpu_handle* h);
+const char* hfgpu_last_error(const hfgpu_handle* h);
+int hfgpu_nbf(const hfgpu_handle* h, int* nbf);
+/* Stream for all device work of this handle (cudaStream_t passed as void*; NULL = handle's own). */
+int hfgpu_set_stream(hfgpu_handle* h, void* stream);
+
+/* Atom coordinates in bohr, natoms x 3.  Rebuilds primitive-pair data, the Schwarz
+ * factors and the screened quartet lists (replaces ShellPair::set_params,
+ * src/integrals/hfscf_shellpair.cpp:33-61, and Erios::compute_screen_matrix,
+ * src/integrals/hfscf_oseri_screen.cpp:22-181). */
+int hfgpu_set_geometry(hfgpu_handle* h, const double* xyz_bohr, int natoms);
+
+/* Shell-pair Schwarz factors sqrt(max |(ab|ab)|), nshell x nshell (symmetric). */
+int hfgpu_schwarz(hfgpu_handle* h, double* Q_out);
+
+/* Every unique ERI into the reference's packed 8-fold vector of length
+ * n(n+1)(n^2+n+2)/8, indexed by hfscfmath::index_ijkl (src/math/hfscf_math.hpp:90-101).
+ * Replaces Mol::hf_solver::create_repulsion_matrix (src/scfsolver/hfscf_hf_hamiltonian.cpp:67-112).
+ * No screening is applied. */
+int hfgpu_eri_packed(hfgpu_handle* h, double* eri_out, long long eri_len);
+
+/* J[DJ] (if DJ != NULL) and K[DK[m]] for m < nK.  J: n x n, K: nK x n x n. */
+int hfgpu_jk(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* J, double* K, int precision);
+
+/* RHF: F = H + 2 J[D] - K[D] (src/scfsolver/hfscf_hf_solver.cpp:261-278). */
+int hfgpu_fock_rhf(hfgpu_handle* h, const double* D, const double* H, double* F, int precision);
+
+/* UHF: F_a = H + J[Da+Db] - K[Da], F_b = H + J[Da+Db] - K[Db]
+ * (src/scfsolver/hfscf_uhf_solver.cpp:160-180). */
+int hfgpu_fock_uhf(hfgpu_handle* h, const double* Da, const double* Db, const double* H, double* Fa, double* Fb,
+                   int precision);
+
+/* Incremental RHF build: F_inout += 2 J[dD] - K[dD], with density screening on |dD|. */
+int hfgpu_fock_delta(hfgpu_handle* h, const double* dD, double* F_inout, int precision);
+
+/* Autograd-shaped pair for the two-electron energy E2 = sum_ij D_ij (2J[D] - K[D])_ij.
+ * forward: E2 at the current geometry.
+ * backward: dE_dR (natoms x 3) += scale * dE2/dR at fixed D, contracting first-derivative
+ * ERIs with the density on the fly; derivative integrals are recomputed, never stored. */
+int hfgpu_energy_forward(hfgpu_handle* h, const double* D, double* E2, int precision);
+int hfgpu_grad2e_backward(hfgpu_handle* h, const double* D, double scale, double* dE_dR, int precision);
+/* UHF: E2 = 1/2 [sum Dt J[Dt] - sum Da K[Da] - sum Db K[Db]], Dt = Da + Db. */
+int hfgpu_grad2e_uhf_backward(hfgpu_handle* h, const double* Da, const double* Db, double scale, double* dE_dR,
+                              int precision);
+
+/* Device-pointer variants (enqueue on the handle's stream, no host synchronisation). */
+int hfgpu_jk_device(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* J, double* K,
+                    int precision);
+int hfgpu_grad2e_device(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
+                        double* grad, int precision);
+
+/* One-electron matrices S, T, V (n x n) for the basis at xyz (bohr), on the host CPU.
+ * Z: nuclear charges per atom.  Needs no handle and no GPU: these O(N^2) integrals
+ * stay on the CPU here (the reference's OSOverlap/OSKinetic/OSNuclear,
+ * src/integrals/hfscf_osoverlap.cpp:10, hfscf_osnuclear.cpp:17). */
+int hfgpu_one_electron(const hfgpu_basis* basis, const double* xyz_bohr, const double* Z, double* S, double* T,
+                       double* V);
+/* grad (natoms x 3) += cH sum D_ij d(T+V)_ij/dX + cS sum W_ij dS_ij/dX, including the
+ * Hellmann-Feynman term of every nucleus.  The reference's RHF gradient
+ * (src/gradient/hfscf_grad_rhf.cpp:140-167) is cH = 2 with D and cS = -2 with Q = D F D. */
+int hfgpu_one_electron_grad(const hfgpu_basis* basis, const double* xyz_bohr, const double* Z, const double* D,
+                            const double* W, double cH, double cS, double* grad);
+
+/* Counters of the last J/K build: quartets launched and quartets skipped by density screening. */
+int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* skipped);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

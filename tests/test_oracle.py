@@ -1,0 +1,88 @@
+"""CPU tests of the oracle: the C restatement against the reference's own code
+(oracle/_ref, when the reference sources were present at build time) and against
+the committed golden fixtures."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from hfscf_b200 import basis as B
+from hfscf_b200 import molecules as M
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
+
+
+def _gold(name):
+    g = np.load(os.path.join(GOLD, name), allow_pickle=False)
+    return B.build_basis(str(g["basis"]), g["Z"], g["coords"], pure=bool(g["pure"])), g
+
+
+@pytest.mark.parametrize("fixture", ["h2o_ccpvdz_eri.npz", "ch4_ccpvdz_eri.npz"])
+def test_oracle_eris_match_golden(fixture):
+    bs, g = _gold(fixture)
+    assert np.max(np.abs(oracle.eri_packed(bs) - g["eri"])) < 1e-13
+
+
+def test_oracle_grad2e_matches_golden():
+    bs, g = _gold("h2o_631gs_grad2e.npz")
+    assert np.max(np.abs(oracle.grad2e_rhf(bs, g["D"]) - g["grad"])) < 1e-12
+
+
+@needs_ref
+@pytest.mark.parametrize("name,pure", [("6-31g**", False), ("6-31g*", True), ("sto-3g", True)])
+def test_oracle_eris_match_reference(name, pure):
+    Z, x = M.water(np.random.default_rng(3))
+    bs = B.build_basis(name, Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=pure)
+    assert np.max(np.abs(oracle.eri_packed(bs) - oracle.ref_eri_packed(bs))) < 1e-13
+
+
+@needs_ref
+def test_oracle_grad2e_matches_reference_deriv_tensors():
+    Z, x = M.water(np.random.default_rng(4))
+    bs = B.build_basis("cc-pvdz", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=True)
+    rng = np.random.default_rng(1)
+    A = rng.normal(size=(bs.nbf, bs.nbf))
+    D = (A + A.T) / bs.nbf
+    g_ref = oracle.grad2e_from_deriv1(oracle.ref_deriv1(bs), bs.bf_atom(), bs.natoms, D)
+    assert np.max(np.abs(oracle.grad2e_rhf(bs, D) - g_ref)) < 1e-12
+
+
+@needs_ref
+def test_oracle_pieces_match_reference():
+    for L in range(4):
+        assert np.max(np.abs(oracle.ylm(L) - oracle.ref_ylm(L))) < 1e-15
+    for m in range(12):
+        for T in (1e-7, 0.05, 0.7, 3.3, 11.0, 29.5, 36.5, 80.0, 500.0):
+            r = oracle.ref_boys(m, T)
+            assert abs(oracle.boys(m, T) - r) <= 1e-13 * r
+    rng = np.random.default_rng(0)
+    for L in range(3):
+        a = np.sort(rng.uniform(0.1, 50, size=4))[::-1]
+        c = rng.uniform(-1, 1, size=4)
+        assert np.allclose(oracle.shell_norm(L, a, c), oracle.ref_shell_coefs(L, a, c), rtol=1e-14, atol=0)
+
+
+def test_boys_against_high_precision_series():
+    """Oracle Boys values against an independent mpmath evaluation (50 digits).
+    T starts at 1e-6: below 1e-8 the oracle keeps the reference's clamp of T
+    (src/math/gamma.cpp:20-21)."""
+    mp = pytest.importorskip("mpmath")
+    mp.mp.dps = 50
+    for m in (0, 3, 8, 13):
+        for T in (1e-6, 0.4, 2.5, 9.0, 20.0, 35.9, 60.0):
+            exact = mp.quad(lambda t: t ** (2 * m) * mp.e ** (-T * t * t), [0, 1])
+            assert abs(oracle.boys(m, T) - float(exact)) <= 2e-14 * float(exact) + 1e-300
+
+
+def test_packed_index_and_unpack_roundtrip():
+    n = 5
+    r = np.arange(n)
+    i, j, k, l = np.meshgrid(r, r, r, r, indexing="ij")
+    idx = oracle.index_ijkl(i, j, k, l)
+    assert idx.max() == oracle.packed_len(n) - 1
+    # 8-fold symmetry
+    assert np.array_equal(idx, oracle.index_ijkl(j, i, k, l))
+    assert np.array_equal(idx, oracle.index_ijkl(k, l, i, j))
+    assert len(np.unique(idx)) == oracle.packed_len(n)
