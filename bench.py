@@ -1,0 +1,337 @@
+"""Benchmark: direct RHF Fock builds/s on one B200 (per GPU, replicas for N > 1).
+
+Workload (the headline configuration): n-octane C8H18, RHF/6-31G** with
+Cartesian d (210 basis functions), FP64 direct Fock builds, Schwarz 1e-12,
+density screening 1e-12, at the converged SCF density.  Geometry: idealised
+all-trans chain rotated by a seeded quaternion (synthetic; no dataset).
+
+A step is one full Fock build F = H + 2J[D] - K[D] over every screened shell
+quartet.  `value` times the device-resident build (CUDA events on the engine's
+stream, L2 flushed between steps); `e2e` times the reference-facing C ABI call
+hfgpu_fock_rhf with pinned host D, H and F (copies inside the timed region).
+
+`--impl reference` times the reference's own CPU code for the same build
+(oracle/_ref: the reference's integral translation units compiled in place) on a
+bounded sample, with all host threads.
+
+Launch: python bench.py [--gpus N --steps K --warmup W] (torchrun for N > 1).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = ("n-octane C8H18 RHF/6-31G** (Cartesian d, 210 basis functions), FP64 direct Fock build, "
+            "Schwarz 1e-12, density screening 1e-12, converged SCF density")
+METRIC = "direct RHF Fock builds/s"
+UNIT = "Fock builds/s"
+N_ITER_AMORTISE = 15  # SCF iterations the reference's one-off ERI generation is spread over
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload_basis():
+    from hfscf_b200 import basis as B, molecules as M
+    Z, x, name, pure = M.workload(2)
+    return B.build_basis(name, Z, x, pure=pure)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own code on a bounded sample
+# ---------------------------------------------------------------------------
+def reference_fock_build_seconds(bs, eri_stride=20, fock_rows=10):
+    import oracle
+    if not oracle.ref_available():
+        return None
+    L = oracle.ref()
+    L.hfref_time_eri_sample.restype = ctypes.c_double
+    L.hfref_time_fock_sample.restype = ctypes.c_double
+    args, keep = oracle._flat(bs)
+    s, t = ctypes.c_longlong(), ctypes.c_longlong()
+    sec = L.hfref_time_eri_sample(*args, ctypes.c_double(1e-14), ctypes.c_longlong(eri_stride), ctypes.byref(s),
+                                  ctypes.byref(t))
+    t_eri = sec * t.value / max(s.value, 1)
+    c = ctypes.c_double()
+    n = bs.nbf
+    sec2 = L.hfref_time_fock_sample(ctypes.c_longlong(n), ctypes.c_longlong(fock_rows), ctypes.byref(c))
+    frac = sum(n - i for i in range(fock_rows)) / (n * (n + 1) / 2)
+    t_con = sec2 / frac
+    build = t_eri / N_ITER_AMORTISE + t_con
+    sample = (f"reference Erios over every {eri_stride}th unique shell quartet ({s.value} of {t.value}) "
+              f"scaled to all; update_fock_matrix contraction over rows 0..{fock_rows - 1} scaled to N(N+1)/2 rows; "
+              f"build = t_eri/{N_ITER_AMORTISE} + t_contract")
+    return {"seconds_per_build": build, "t_eri_s": t_eri, "t_contract_s": t_con, "sample": sample,
+            "sample_wall_s": sec + sec2}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    import oracle
+    bs = workload_basis()
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/libhfref.so not built"}))
+        return 0
+    # warm-up and timed steps: each step is one bounded sample of a reference Fock build
+    for _ in range(args.warmup):
+        reference_fock_build_seconds(bs, eri_stride=4000, fock_rows=1)
+    times = []
+    last = None
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        last = reference_fock_build_seconds(bs, eri_stride=2000, fock_rows=2)
+        times.append(last["seconds_per_build"])
+    wall = time.perf_counter() - t0
+    per = statistics.mean(times)
+    v = 1.0 / per
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nbf": bs.nbf, "amortised_over_scf_iterations": N_ITER_AMORTISE},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": last["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "sample_wall_s": wall}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from hfscf_b200 import engine as E
+    from hfscf_b200 import flopmodel, scf
+    from hfscf_b200.basis import nuclear_repulsion
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    bs = workload_basis()
+    n = bs.nbf
+    stream = torch.cuda.current_stream()
+    eng = E.Engine(bs, device=local)
+    eng.set_stream(stream.cuda_stream)
+    # --- untimed set-up: converged SCF (FP64), gradient, mixed-precision SCF -----------------
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    res = scf.rhf(bs, engine=eng)
+    scf_wall = time.perf_counter() - t
+    t = time.perf_counter()
+    grad = scf.rhf_gradient(bs, res, eng)
+    grad_wall = time.perf_counter() - t
+    t = time.perf_counter()
+    res_mx = scf.rhf(bs, engine=eng, precision=E.MIXED, incremental=True)
+    mixed_wall = time.perf_counter() - t
+    S, T, V = E.one_electron(bs)
+    H = T + V
+    dev = torch.device("cuda", local)
+    D = torch.from_numpy(np.ascontiguousarray(res.D)).to(dev)
+    Hd = torch.from_numpy(np.ascontiguousarray(H)).to(dev)
+    J = torch.empty((n, n), dtype=torch.float64, device=dev)
+    K = torch.empty((n, n), dtype=torch.float64, device=dev)
+    F = torch.empty((n, n), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+
+    def step():
+        eng.jk_device(D.data_ptr(), 1, D.data_ptr(), J.data_ptr(), K.data_ptr())
+        torch.add(Hd, J, alpha=2.0, out=F)
+        F.sub_(K)
+
+    for _ in range(args.warmup):
+        step()
+    eng.set_timing(True)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    class_ms = np.zeros(E.NUM_CLASSES)
+    class_work = [None] * E.NUM_CLASSES
+    launches = 0
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()  # ncu --profile-from-start off captures only the timed steps
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        starts[k].record(stream)
+        step()
+        ends[k].record(stream)
+        launches += eng.last_launches() + 2  # + the two elementwise ops of F
+        for c in range(E.NUM_CLASSES):
+            class_ms[c] += eng.class_time_ms(c)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    if pg:
+        pg.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    clk = clocks.stop()
+    eng.set_timing(False)
+    for c in range(E.NUM_CLASSES):
+        class_work[c] = eng.class_stats(c)
+    total_s = sum(step_ms) / 1e3
+    if pg:
+        tt = torch.tensor([total_s], device=dev, dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        total_s = float(tt.item())
+    value = world * args.steps / total_s
+
+    # --- end to end through the reference-facing C ABI, pinned host buffers -----------------
+    Dh = torch.from_numpy(np.ascontiguousarray(res.D)).pin_memory()
+    Hh = torch.from_numpy(np.ascontiguousarray(H)).pin_memory()
+    Fh = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        eng.fock_rhf_ptr(Dh.data_ptr(), Hh.data_ptr(), Fh.data_ptr())
+    e2e_s = 0.0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        eng.fock_rhf_ptr(Dh.data_ptr(), Hh.data_ptr(), Fh.data_ptr())
+        torch.cuda.synchronize()
+        e2e_s += time.perf_counter() - t
+    if pg:
+        tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * n * n * 8,
+           "d2h_bytes_per_step": n * n * 8, "api": "hfgpu_fock_rhf (host D, H -> host F)"}
+    err_f = float(np.max(np.abs(Fh.numpy() - F.cpu().numpy())))
+
+    # --- roofline of the dominant kernel ------------------------------------------------------
+    dom = int(np.argmax(class_ms))
+    st = class_work[dom]
+    avg_ms = class_ms[dom] / args.steps
+    flops = flopmodel.class_flops(dom, st["computed"], st["prim_quartets"], bs.pure)
+    peak = E.fp64_peak_tflops(local)
+    achieved = flops / (avg_ms * 1e-3) / 1e12
+    total_flops = sum(flopmodel.class_flops(c, class_work[c]["computed"], class_work[c]["prim_quartets"], bs.pure)
+                      for c in range(E.NUM_CLASSES))
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        tr = json.load(open(tpath))
+        traffic = tr.get(flopmodel.class_name(dom))
+    roof = {"bound": "fp64", "kernel": f"quartet_kernel {flopmodel.class_name(dom)} FP64",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+            "peak_source": "measured in this run: register-only FP64 FMA kernel (hfgpu_fp64_peak); "
+                           "MEASURED_PEAKS.json has no FP64 figure",
+            "flops_per_launch": flops, "avg_launch_ms": avg_ms,
+            "build_fp64_tflops": total_flops / (sum(step_ms) / args.steps * 1e-3) / 1e12,
+            "share_of_step": class_ms[dom] / max(sum(step_ms), 1e-9)}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sum(step_ms) / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometry)",
+            "config": {"workload": WORKLOAD, "nbf": n, "parallelism": f"replicas x{world}",
+                       "l2": "flushed between steps (256 MiB write)",
+                       "quartets_screened": int(sum(class_work[c]["screened"] for c in range(E.NUM_CLASSES))),
+                       "quartets_computed_per_build": int(sum(class_work[c]["computed"] for c in range(E.NUM_CLASSES))) // args.steps},
+            "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            "scf": {"energy": res.energy, "iterations": res.iterations, "converged": res.converged,
+                    "wall_s": scf_wall, "grad_wall_s": grad_wall, "grad_max": float(np.max(np.abs(grad))),
+                    "mixed_incremental_energy": res_mx.energy, "mixed_dE": res_mx.energy - res.energy,
+                    "mixed_wall_s": mixed_wall, "e_nuc": nuclear_repulsion(bs.Z, bs.coords)},
+            "check": {"max_abs_F_device_vs_api": err_f}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        ref = reference_fock_build_seconds(bs)
+        if ref is not None:
+            line["cpu_baseline"] = {"value": 1.0 / ref["seconds_per_build"], "unit": UNIT,
+                                    "cores": os.cpu_count(), "kind": "reference", "sample": ref["sample"],
+                                    "t_eri_s": ref["t_eri_s"], "t_contract_s": ref["t_contract_s"]}
+    if rank == 0:
+        print(json.dumps(line))
+    eng.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

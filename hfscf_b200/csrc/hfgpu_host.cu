@@ -89,6 +89,10 @@ struct hfgpu_handle {
   DevBuf d_pairs, d_prim_d, d_prim_f, d_alpha_d, d_alpha_f, d_boys_d, d_boys_f, d_quart;
   DevBuf d_mats, d_half, d_dmax, d_counters, d_grad, d_scratch, d_eri, d_eriq;
   long long last_launched = 0, last_skipped = 0;
+  int last_kernels = 0;                 // kernel launches of the last J/K build
+  bool timing = false;                  // record CUDA events around every class launch
+  cudaEvent_t ev[2 * 21 + 2] = {};
+  bool ev_used[21] = {};
 
   hfgpu_handle() : q_beg(21), q_mid(21), q_end(21) {}
 };
@@ -337,7 +341,41 @@ __global__ void symmetrise_kernel(const double* __restrict__ h, double* __restri
   out[idx] = h[(size_t)m * tot + i * n + j] + h[(size_t)m * tot + j * n + i];
 }
 
+// F = H + 2J - K (F may alias J).
+__global__ void fock_combine_kernel(double* F, const double* __restrict__ H, const double* J,
+                                    const double* __restrict__ K, int tot) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < tot) F[i] = H[i] + 2.0 * J[i] - K[i];
+}
+
+// FP64 FMA throughput probe: 8 independent FMA chains per thread.
+__global__ void fp64_peak_kernel(double* out, int iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3 + k;
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+  double s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == 12345.678) out[0] = s;  // keeps the loop alive, never true in practice
+}
+
 }  // namespace
+
+static int read_counters(hfgpu_handle* h, long long* computed, long long* skipped) {
+  std::vector<unsigned long long> c(3 * hfgpu::kNumClasses);
+  HF_CUDA(h, cudaMemcpy(c.data(), h->d_counters.p, sizeof(unsigned long long) * c.size(), cudaMemcpyDeviceToHost));
+  long long a = 0, b = 0;
+  for (int k = 0; k < hfgpu::kNumClasses; ++k) {
+    a += (long long)c[3 * k];
+    b += (long long)c[3 * k + 1];
+  }
+  if (computed) *computed = a;
+  if (skipped) *skipped = b;
+  return HFGPU_OK;
+}
 
 // Device J/K: all pointers on the device.  Jout/Kout may be null to skip.
 static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* Jout, double* Kout,
@@ -347,11 +385,12 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   const int n = h->n, ns = h->nshell;
   const size_t nn = (size_t)n * n;
   HF_CUDA(h, h->d_half.ensure(sizeof(double) * nn * (1 + std::max(nK, 1))));
-  HF_CUDA(h, h->d_counters.ensure(sizeof(unsigned long long) * 2));
+  HF_CUDA(h, h->d_counters.ensure(sizeof(unsigned long long) * 3 * hfgpu::kNumClasses));
   double* Jh = h->d_half.as<double>();
   double* Kh = Jh + nn;
   HF_CUDA(h, cudaMemsetAsync(Jh, 0, sizeof(double) * nn * (1 + nK), h->stream));
-  HF_CUDA(h, cudaMemsetAsync(h->d_counters.p, 0, sizeof(unsigned long long) * 2, h->stream));
+  HF_CUDA(h, cudaMemsetAsync(h->d_counters.p, 0, sizeof(unsigned long long) * 3 * hfgpu::kNumClasses, h->stream));
+  int kernels = 0;
   const float* dmax = nullptr;
   if (h->opts.density_tol > 0.0) {
     HF_CUDA(h, h->d_dmax.ensure(sizeof(float) * ns * ns + sizeof(int) * (ns + 1)));
@@ -359,6 +398,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     HF_CUDA(h, cudaMemcpyAsync(dfirst, h->first.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, h->stream));
     dmax_kernel<<<(ns * ns + 127) / 128, 128, 0, h->stream>>>(dfirst, ns, n, DJ, nK, DK, h->d_dmax.as<float>());
     HF_CHECK_LAUNCH(h, "dmax kernel");
+    ++kernels;
     dmax = h->d_dmax.as<float>();
   }
   QuartetArgs<double> qd{};
@@ -376,20 +416,32 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   const int2* q = h->d_quart.as<int2>();
   long long launched = 0;
   // largest classes first so that they overlap the tail of the smaller ones
+  unsigned long long* cnt = h->d_counters.as<unsigned long long>();
   for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
     const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
+    qd.jk.counters = cnt + 3 * c;
+    qf.jk.counters = cnt + 3 * c;
+    h->ev_used[c] = false;
+    if (e <= b) continue;
+    if (h->timing) HF_CUDA(h, cudaEventRecord(h->ev[2 * c], h->stream));
     if (precision == HFGPU_MIXED) {
-      if (m > b) L->quartet_d(qd, q + b, (int)(m - b), h->stream);
-      if (e > m) L->quartet_f(qf, q + m, (int)(e - m), h->stream);
-    } else if (e > b) {
+      if (m > b) { L->quartet_d(qd, q + b, (int)(m - b), h->stream); ++kernels; }
+      if (e > m) { L->quartet_f(qf, q + m, (int)(e - m), h->stream); ++kernels; }
+    } else {
       L->quartet_d(qd, q + b, (int)(e - b), h->stream);
+      ++kernels;
     }
     HF_CHECK_LAUNCH(h, "quartet kernel");
+    if (h->timing) {
+      HF_CUDA(h, cudaEventRecord(h->ev[2 * c + 1], h->stream));
+      h->ev_used[c] = true;
+    }
     launched += e - b;
   }
   h->last_launched = launched;
   const int tot = (int)nn;
+  h->last_kernels = kernels + ((Jout && DJ) ? 1 : 0) + ((Kout && nK > 0) ? 1 : 0);
   if (Jout && DJ) {
     symmetrise_kernel<<<(tot + 255) / 256, 256, 0, h->stream>>>(Jh, Jout, n, 1);
     HF_CHECK_LAUNCH(h, "symmetrise J");
@@ -555,6 +607,8 @@ int hfgpu_destroy(hfgpu_handle* h) {
                     &h->d_quart, &h->d_mats, &h->d_half, &h->d_dmax, &h->d_counters, &h->d_grad, &h->d_scratch,
                     &h->d_eri, &h->d_eriq})
     d->release();
+  if (h->ev[0])
+    for (auto& e : h->ev) cudaEventDestroy(e);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return HFGPU_OK;
@@ -656,10 +710,10 @@ int hfgpu_jk(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double
   if ((rc = jk_device_impl(h, DJ ? dDJ : nullptr, nK, dDK, dJ, dK, precision))) return rc;
   if (DJ) HF_CUDA(h, cudaMemcpyAsync(J, dJ, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->stream));
   if (nK) HF_CUDA(h, cudaMemcpyAsync(K, dK, sizeof(double) * nn * nK, cudaMemcpyDeviceToHost, h->stream));
-  unsigned long long cnt[2] = {0, 0};
-  HF_CUDA(h, cudaMemcpyAsync(cnt, h->d_counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, h->stream));
   HF_CUDA(h, cudaStreamSynchronize(h->stream));
-  h->last_skipped = (long long)cnt[1];
+  long long sk = 0;
+  if ((rc = read_counters(h, nullptr, &sk))) return rc;
+  h->last_skipped = sk;
   return HFGPU_OK;
 }
 
@@ -672,11 +726,23 @@ int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* ski
 
 int hfgpu_fock_rhf(hfgpu_handle* h, const double* D, const double* H, double* F, int precision) {
   if (!h || !D || !H || !F) return HFGPU_ERR_INVALID;
-  const size_t nn = (size_t)h->n * h->n;
-  std::vector<double> J(nn), K(nn);
-  int rc = hfgpu_jk(h, D, 1, D, J.data(), K.data(), precision);
+  int rc = set_device(h);
   if (rc) return rc;
-  for (size_t i = 0; i < nn; ++i) F[i] = H[i] + 2.0 * J[i] - K[i];
+  const size_t nn = (size_t)h->n * h->n;
+  // device layout: [D | H | J | K]; only D and H go up, only F comes back
+  HF_CUDA(h, h->d_mats.ensure(sizeof(double) * nn * 4));
+  double* dD = h->d_mats.as<double>();
+  double* dH = dD + nn;
+  double* dJ = dH + nn;
+  double* dK = dJ + nn;
+  HF_CUDA(h, cudaMemcpyAsync(dD, D, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream));
+  HF_CUDA(h, cudaMemcpyAsync(dH, H, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream));
+  if ((rc = jk_device_impl(h, dD, 1, dD, dJ, dK, precision))) return rc;
+  fock_combine_kernel<<<(int)((nn + 255) / 256), 256, 0, h->stream>>>(dJ, dH, dJ, dK, (int)nn);
+  HF_CHECK_LAUNCH(h, "fock combine");
+  ++h->last_kernels;
+  HF_CUDA(h, cudaMemcpyAsync(F, dJ, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->stream));
   return HFGPU_OK;
 }
 
@@ -818,6 +884,82 @@ int hfgpu_one_electron_grad(const hfgpu_basis* basis, const double* xyz, const d
   if (!xyz || !Z || !D || !W || !grad || onee_basis(basis, o)) return HFGPU_ERR_INVALID;
   hfgpu_onee_gradient(o.b, Z, xyz, basis->natoms, D, W, cH, cS, grad);
   return HFGPU_OK;
+}
+
+int hfgpu_set_timing(hfgpu_handle* h, int on) {
+  if (!h) return HFGPU_ERR_INVALID;
+  int rc = set_device(h);
+  if (rc) return rc;
+  if (on && !h->ev[0])
+    for (auto& e : h->ev) HF_CUDA(h, cudaEventCreate(&e));
+  h->timing = on != 0;
+  return HFGPU_OK;
+}
+
+int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out) {
+  if (!h || !out || cls < 0 || cls >= hfgpu::kNumClasses) return HFGPU_ERR_INVALID;
+  const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[cls];
+  out[0] = L->la;
+  out[1] = L->lb;
+  out[2] = L->lc;
+  out[3] = L->ld;
+  out[4] = h->q_end[cls] - h->q_beg[cls];
+  out[5] = h->q_mid[cls] - h->q_beg[cls];
+  out[6] = out[7] = out[8] = 0;
+  if (h->d_counters.p) {
+    unsigned long long c[3];
+    HF_CUDA(h, cudaStreamSynchronize(h->stream));
+    HF_CUDA(h, cudaMemcpy(c, h->d_counters.as<unsigned long long>() + 3 * cls, sizeof(c), cudaMemcpyDeviceToHost));
+    out[6] = (long long)c[0];
+    out[7] = (long long)c[1];
+    out[8] = (long long)c[2];
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms) {
+  if (!h || !ms || cls < 0 || cls >= hfgpu::kNumClasses) return HFGPU_ERR_INVALID;
+  *ms = 0.f;
+  if (!h->timing || !h->ev_used[cls]) return HFGPU_OK;
+  HF_CUDA(h, cudaEventSynchronize(h->ev[2 * cls + 1]));
+  HF_CUDA(h, cudaEventElapsedTime(ms, h->ev[2 * cls], h->ev[2 * cls + 1]));
+  return HFGPU_OK;
+}
+
+int hfgpu_last_launches(const hfgpu_handle* h, int* kernels) {
+  if (!h || !kernels) return HFGPU_ERR_INVALID;
+  *kernels = h->last_kernels;
+  return HFGPU_OK;
+}
+
+int hfgpu_fp64_peak(int device, double* tflops) {
+  if (!tflops) return HFGPU_ERR_INVALID;
+  if (cudaSetDevice(device) != cudaSuccess) return HFGPU_ERR_CUDA;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  double* out = nullptr;
+  if (cudaMalloc(&out, sizeof(double)) != cudaSuccess) return HFGPU_ERR_NOMEM;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int iters = 20000, blocks = sms * 8, threads = 256;
+  fp64_peak_kernel<<<blocks, threads>>>(out, 100, 1.0000001, 1e-7);
+  double best = 0.0;
+  for (int r = 0; r < 3; ++r) {
+    cudaEventRecord(a);
+    fp64_peak_kernel<<<blocks, threads>>>(out, iters, 1.0000001, 1e-7);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    const double fl = 2.0 * 8.0 * iters * (double)blocks * threads;
+    best = std::max(best, fl / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  *tflops = best;
+  return cudaGetLastError() == cudaSuccess ? HFGPU_OK : HFGPU_ERR_CUDA;
 }
 
 }  // extern "C"

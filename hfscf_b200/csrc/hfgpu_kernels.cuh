@@ -28,7 +28,7 @@ struct JKArgs {
   double* __restrict__ Kh;           // nK x n x n
   const float* __restrict__ dmax;    // nshell x nshell max |D| over all densities, or nullptr
   double dtol;                       // density-weighted screening threshold
-  unsigned long long* __restrict__ counters;  // [0] quartets computed, [1] skipped by density
+  unsigned long long* __restrict__ counters;  // per class: computed, skipped by density, primitive quartets
 };
 
 template <typename R>
@@ -216,17 +216,28 @@ __global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const i
   const int2 pq = quartets[t];
   const PairInfo P = a.pairs[pq.x];
   const PairInfo Q = a.pairs[pq.y];
+  bool skip = false;
   if (qa.mode == QMODE_JK && a.dmax != nullptr) {
     // density-weighted Schwarz bound: Q_ab Q_cd max(4|D_ab|, 4|D_cd|, |D_ac|, |D_ad|, |D_bc|, |D_bd|)
     const float* dm = a.dmax;
     const int ns = a.nshell;
     float m = 4.f * fmaxf(dm[P.sa * ns + P.sb], dm[Q.sa * ns + Q.sb]);
     m = fmaxf(m, fmaxf(fmaxf(dm[P.sa * ns + Q.sa], dm[P.sa * ns + Q.sb]), fmaxf(dm[P.sb * ns + Q.sa], dm[P.sb * ns + Q.sb])));
-    if (P.schwarz * Q.schwarz * double(m) < a.dtol) {
-      if (a.counters) atomicAdd(a.counters + 1, 1ull);
-      return;
+    skip = P.schwarz * Q.schwarz * double(m) < a.dtol;
+  }
+  if (a.counters != nullptr) {
+    // per-class work counters, one atomic per warp: [0] quartets computed,
+    // [1] quartets skipped by the density bound, [2] primitive quartets computed
+    const unsigned mask = __activemask();
+    const unsigned nskip = __popc(__ballot_sync(mask, skip));
+    const unsigned prims = __reduce_add_sync(mask, skip ? 0u : unsigned(P.nprim * Q.nprim));
+    if ((threadIdx.x & 31) == __ffs(mask) - 1) {
+      atomicAdd(a.counters + 0, (unsigned long long)(__popc(mask) - nskip));
+      atomicAdd(a.counters + 1, (unsigned long long)nskip);
+      atomicAdd(a.counters + 2, (unsigned long long)prims);
     }
   }
+  if (skip) return;
   using Dc = BlockDims<LA, LB, LC, LD, false>;
   R cart[Dc::NCART];
   cart_block<LA, LB, LC, LD, R>(P, Q, a.prims, a.boys, cart);

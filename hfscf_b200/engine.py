@@ -62,7 +62,7 @@ def exported_symbols():
     import re
     hdr = os.path.join(os.path.dirname(HERE), "include", "hfgpu.h")
     text = open(hdr).read()
-    return sorted(set(re.findall(r"\b(hfgpu_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"^(?:int|const char\*)\s+(hfgpu_[a-z0-9_]+)\s*\(", text, re.M)))
 
 
 def _p(a, ct=ctypes.c_double):
@@ -177,6 +177,44 @@ class Engine:
         self._check(lib().hfgpu_fock_delta(self.h, _p(_c(dD)), _p(F), ctypes.c_int(precision)))
         return F
 
+    # --- device-pointer calls (torch tensors or raw addresses) -----------------
+    def set_stream(self, stream_ptr: int | None):
+        self._check(lib().hfgpu_set_stream(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def jk_device(self, DJ_ptr, nK, DK_ptr, J_ptr, K_ptr, precision=FP64):
+        self._check(lib().hfgpu_jk_device(self.h, ctypes.c_void_p(DJ_ptr), ctypes.c_int(nK), ctypes.c_void_p(DK_ptr),
+                                          ctypes.c_void_p(J_ptr), ctypes.c_void_p(K_ptr), ctypes.c_int(precision)))
+
+    def grad2e_device(self, DJ_ptr, cJ, nK, DK_ptr, cK, grad_ptr, precision=FP64):
+        self._check(lib().hfgpu_grad2e_device(self.h, ctypes.c_void_p(DJ_ptr), ctypes.c_double(cJ), ctypes.c_int(nK),
+                                              ctypes.c_void_p(DK_ptr), ctypes.c_double(cK), ctypes.c_void_p(grad_ptr),
+                                              ctypes.c_int(precision)))
+
+    def fock_rhf_ptr(self, D_ptr, H_ptr, F_ptr, precision=FP64):
+        """hfgpu_fock_rhf on raw host pointers (e.g. pinned buffers)."""
+        self._check(lib().hfgpu_fock_rhf(self.h, ctypes.c_void_p(D_ptr), ctypes.c_void_p(H_ptr),
+                                         ctypes.c_void_p(F_ptr), ctypes.c_int(precision)))
+
+    # --- measurement hooks ------------------------------------------------------
+    def set_timing(self, on: bool):
+        self._check(lib().hfgpu_set_timing(self.h, ctypes.c_int(int(on))))
+
+    def class_stats(self, cls: int):
+        out = (ctypes.c_longlong * 9)()
+        self._check(lib().hfgpu_class_stats(self.h, ctypes.c_int(cls), out))
+        keys = ("la", "lb", "lc", "ld", "screened", "high_bound", "computed", "skipped", "prim_quartets")
+        return dict(zip(keys, list(out)))
+
+    def class_time_ms(self, cls: int) -> float:
+        ms = ctypes.c_float()
+        self._check(lib().hfgpu_class_time(self.h, ctypes.c_int(cls), ctypes.byref(ms)))
+        return ms.value
+
+    def last_launches(self) -> int:
+        k = ctypes.c_int()
+        self._check(lib().hfgpu_last_launches(self.h, ctypes.byref(k)))
+        return k.value
+
     def last_counts(self):
         a, b = ctypes.c_longlong(), ctypes.c_longlong()
         self._check(lib().hfgpu_last_counts(self.h, ctypes.byref(a), ctypes.byref(b)))
@@ -199,6 +237,17 @@ class Engine:
         self._check(lib().hfgpu_grad2e_uhf_backward(self.h, _p(_c(Da)), _p(_c(Db)), ctypes.c_double(scale), _p(g),
                                                     ctypes.c_int(precision)))
         return g
+
+
+NUM_CLASSES = 21
+
+
+def fp64_peak_tflops(device=0) -> float:
+    t = ctypes.c_double()
+    rc = lib().hfgpu_fp64_peak(ctypes.c_int(device), ctypes.byref(t))
+    if rc:
+        raise HfgpuError(rc)
+    return t.value
 
 
 # --- one-electron integrals (host CPU, no handle) ---------------------------------

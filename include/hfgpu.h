@@ -136,6 +136,19 @@ int hfgpu_one_electron_grad(const hfgpu_basis* basis, const double* xyz_bohr, co
 /* Counters of the last J/K build: quartets launched and quartets skipped by density screening. */
 int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* skipped);
 
+/* Measurement hooks (no counterpart in the reference, which has no GPU path).
+ * set_timing: record CUDA events around every per-class kernel of later J/K builds.
+ * class_stats(cls, out[9]): la lb lc ld, screened quartets, quartets at/above the mixed-precision
+ *   bound, and from the last J/K build: quartets computed, skipped by density, primitive quartets computed.
+ * class_time: event time (ms) of that class's kernels in the last J/K build.
+ * last_launches: kernel launches of the last J/K (or Fock) build.
+ * fp64_peak: FP64 FMA throughput of the device in TFLOP/s, from a register-only FMA kernel. */
+int hfgpu_set_timing(hfgpu_handle* h, int on);
+int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out);
+int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms);
+int hfgpu_last_launches(const hfgpu_handle* h, int* kernels);
+int hfgpu_fp64_peak(int device, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,6 +16,8 @@
 #include <memory>
 #include <vector>
 
+#include <omp.h>
+
 #include "integrals/hfscf_oseri.hpp"
 #include "math/gamma.hpp"
 #include "math/solid_harmonics.hpp"
@@ -152,6 +154,65 @@ int hfref_deriv1(int nshell, const int* L, const double* xyz, const int* nprim, 
     for (Eigen::Index p = 0; p < len; ++p) out9[q * len + p] = t[q][p];
   }
   return 0;
+}
+
+// Timing sample of the reference's ERI generation: runs
+// Erios::compute_contracted_shell_quartet over every `stride`-th unique shell
+// quartet of create_repulsion_matrix's loop (hfscf_hf_hamiltonian.cpp:95-111), with
+// the reference's default eri_screen = true (screen matrix first, :77-89), on all
+// OpenMP threads.  Returns seconds; *sampled / *total give the scale factor.
+double hfref_time_eri_sample(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
+                             const double* coef, int pure, double cutoff, long long stride, long long* sampled,
+                             long long* total) {
+  auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, pure);
+  const Eigen::Index n = pure ? b->npure : b->ncart;
+  const Eigen::Index len = n * (n + 1) * (n * n + n + 2) / 8;
+  EigenVector<double> eri(len);
+  ERIOS::Erios os(pure != 0, cutoff);
+  std::vector<std::pair<int, int>> quartets;
+  for (int i = 0; i < nshell; ++i)
+    for (int j = i; j < nshell; ++j)
+      for (int k = 0; k < nshell; ++k)
+        for (int l = k; l < nshell; ++l)
+          if (hfscfmath::index_ij(i, j) <= hfscfmath::index_ij(k, l)) quartets.emplace_back(i * nshell + j, k * nshell + l);
+  std::vector<std::pair<int, int>> pick;
+  for (size_t q = 0; q < quartets.size(); q += (size_t)stride) pick.push_back(quartets[q]);
+  const double t0 = omp_get_wtime();
+  os.init_screen(b->ncart);
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < nshell; ++i)
+    for (int j = i; j < nshell; ++j) os.compute_screen_matrix(b->pairs[i * nshell + j]);
+#pragma omp parallel for schedule(dynamic)
+  for (long long q = 0; q < (long long)pick.size(); ++q)
+    os.compute_contracted_shell_quartet(eri, b->pairs[pick[q].first], b->pairs[pick[q].second], true);
+  const double t1 = omp_get_wtime();
+  *sampled = (long long)pick.size();
+  *total = (long long)quartets.size();
+  return t1 - t0;
+}
+
+// Timing sample of the reference's per-iteration Fock contraction
+// (Mol::hf_solver::update_fock_matrix, src/scfsolver/hfscf_hf_solver.cpp:258-279),
+// restated: rows i in [0, rows) over a packed ERI vector of the full length.
+// Returns seconds; the caller scales by the share of the N^3(N+1)/2 inner iterations.
+double hfref_time_fock_sample(long long n, long long rows, double* checksum) {
+  const long long len = n * (n + 1) * (n * n + n + 2) / 8;
+  std::vector<double> eri((size_t)len, 1e-3), D((size_t)(n * n), 1e-2), F((size_t)(n * n), 0.0);
+  const double t0 = omp_get_wtime();
+#pragma omp parallel for schedule(dynamic)
+  for (long long i = 0; i < rows; ++i)
+    for (long long j = i; j < n; ++j) {
+      double f = 0.0;
+      for (long long k = 0; k < n; ++k)
+        for (long long l = 0; l < n; ++l)
+          f += D[k * n + l] * (2.0 * eri[hfscfmath::index_ijkl(i, j, k, l)] - eri[hfscfmath::index_ijkl(i, k, j, l)]);
+      F[i * n + j] = F[j * n + i] = f;
+    }
+  const double t1 = omp_get_wtime();
+  double c = 0.0;
+  for (double v : F) c += v;
+  *checksum = c;
+  return t1 - t0;
 }
 
 }  // extern "C"

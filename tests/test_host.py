@@ -1,0 +1,145 @@
+"""CPU tests of the host side: the C-ABI library, basis handling, molecules."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from hfscf_b200 import basis as B
+from hfscf_b200 import engine as E
+from hfscf_b200 import molecules as M
+
+
+def test_library_exports_every_declared_symbol():
+    lib = E.lib()
+    names = E.exported_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_default_options():
+    o = E._Opts()
+    assert E.lib().hfgpu_default_opts(ctypes.byref(o)) == 0
+    assert o.schwarz_tol == 1e-12 and o.mixed_fp32_bound == 1e-4
+
+
+def test_basis_sizes_of_the_workloads():
+    sizes = {}
+    for w in (1, 2, 3, 4):
+        Z, x, name, pure = M.workload(w)
+        sizes[w] = B.build_basis(name, Z, x, pure=pure).nbf
+    assert sizes == {1: 24, 2: 210, 3: 246, 4: 152}
+
+
+def test_shell_order_and_offsets_follow_the_reference():
+    bs = B.build_basis("6-31g*", [8, 1], [[0, 0, 0], [0, 0, 1.8]], pure=False)
+    Ls = [s.L for s in bs.shells]
+    assert Ls == [0, 0, 1, 0, 1, 2, 0, 0]  # O: S, SP->S,P, SP->S,P, D ; H: S, S
+    assert [s.idx for s in bs.shells] == [0, 1, 2, 5, 6, 9, 15, 16]
+
+
+def test_batch_molecules_are_seeded_and_mixed():
+    a = M.batch_molecules(64)
+    b = M.batch_molecules(64)
+    assert all(np.array_equal(x[1], y[1]) for x, y in zip(a, b))
+    assert {m[2] for m in a} == {"sto-3g", "6-31g*"}
+
+
+def _md_overlap_kinetic(bs):
+    """Independent S and T by numerical quadrature-free closed forms for s/p/d (MD Hermite E)."""
+    from math import comb, factorial
+    shells = bs.shells
+
+    def norm_c(sh):
+        import oracle
+        return oracle.shell_norm(sh.L, sh.exps, sh.coefs)
+
+    def E1(i, j, t, Qx, a, b):
+        p = a + b
+        q = a * b / p
+        if t < 0 or t > i + j:
+            return 0.0
+        if i == j == t == 0:
+            return np.exp(-q * Qx * Qx)
+        if j == 0:
+            return (1 / (2 * p)) * E1(i - 1, j, t - 1, Qx, a, b) - (q * Qx / a) * E1(i - 1, j, t, Qx, a, b) + \
+                (t + 1) * E1(i - 1, j, t + 1, Qx, a, b)
+        return (1 / (2 * p)) * E1(i, j - 1, t - 1, Qx, a, b) + (q * Qx / b) * E1(i, j - 1, t, Qx, a, b) + \
+            (t + 1) * E1(i, j - 1, t + 1, Qx, a, b)
+
+    def s1(i, j, A, Bc, a, b):
+        return E1(i, j, 0, A - Bc, a, b) * np.sqrt(np.pi / (a + b))
+
+    def comps(L):
+        return [(L - i, i - j, j) for i in range(L + 1) for j in range(i + 1)]
+
+    n = bs.ncart
+    S = np.zeros((n, n))
+    T = np.zeros((n, n))
+    for sa in shells:
+        ca = norm_c(sa)
+        for sb in shells:
+            cb = norm_c(sb)
+            for x, la in enumerate(comps(sa.L)):
+                for y, lb in enumerate(comps(sb.L)):
+                    sv = tv = 0.0
+                    for a, c1 in zip(sa.exps, ca):
+                        for b, c2 in zip(sb.exps, cb):
+                            s = [s1(la[d], lb[d], sa.center[d], sb.center[d], a, b) for d in range(3)]
+                            t = 0.0
+                            for d in range(3):
+                                l2 = lb[d]
+                                td = -2 * b * b * s1(la[d], l2 + 2, sa.center[d], sb.center[d], a, b) + \
+                                    b * (2 * l2 + 1) * s1(la[d], l2, sa.center[d], sb.center[d], a, b)
+                                if l2 > 1:
+                                    td -= 0.5 * l2 * (l2 - 1) * s1(la[d], l2 - 2, sa.center[d], sb.center[d], a, b)
+                                others = [s[e] for e in range(3) if e != d]
+                                t += td * others[0] * others[1]
+                            sv += c1 * c2 * s[0] * s[1] * s[2]
+                            tv += c1 * c2 * t
+                    S[sa.idx + x, sb.idx + y] = sv
+                    T[sa.idx + x, sb.idx + y] = tv
+    return S, T
+
+
+def test_one_electron_overlap_kinetic_against_independent_hermite_forms():
+    Z, x = M.water(np.random.default_rng(2))
+    bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    S, T, V = E.one_electron(bs)
+    S0, T0 = _md_overlap_kinetic(bs)
+    assert np.max(np.abs(S - S0)) < 1e-12 and np.max(np.abs(T - T0)) < 1e-11
+    assert np.allclose(V, V.T) and np.all(np.diag(V) < 0)
+
+
+def test_one_electron_gradient_translational_invariance():
+    Z, x = M.water(np.random.default_rng(3))
+    bs = B.build_basis("cc-pvdz", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=True)
+    n = bs.nbf
+    rng = np.random.default_rng(0)
+    A = rng.normal(size=(n, n))
+    D = (A + A.T) / n
+    g = E.one_electron_grad(bs, D, D, 2.0, -2.0)
+    assert np.max(np.abs(g.sum(axis=0))) < 1e-10
+
+
+def test_one_electron_gradient_matches_finite_differences():
+    Z, x = M.water(np.random.default_rng(4))
+    x = np.asarray(x) * B.ANGSTROM_TO_BOHR
+    bs = B.build_basis("6-31g*", Z, x, pure=False)
+    n = bs.nbf
+    rng = np.random.default_rng(1)
+    A = rng.normal(size=(n, n))
+    D = (A + A.T) / n
+    W = D @ D
+    g = E.one_electron_grad(bs, D, W, 2.0, -2.0)
+    h = 1e-5
+    for a in range(3):
+        for d in range(3):
+            vals = []
+            for s in (1, -1):
+                xx = x.copy()
+                xx[a, d] += s * h
+                S, T, V = E.one_electron(bs.with_coords(xx))
+                vals.append(2 * np.sum(D * (T + V)) - 2 * np.sum(W * S))
+            assert abs((vals[0] - vals[1]) / (2 * h) - g[a, d]) < 1e-6
