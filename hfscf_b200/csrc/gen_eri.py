@@ -237,21 +237,21 @@ class HRR:
 PRIM_HEADER = """\
       // primitive-quartet scalars
       const R pq = p + q;
-      const R ipq = R(1) / pq;
+      const R rs = rsqrt_t(pq);      // 1 / sqrt(p + q)
+      const R ipq = rs * rs;
       const R rho = p * q * ipq;
       const R rp = q * ipq;          // rho / p
       const R rq = p * ipq;          // rho / q
-      const R inv2p = R(0.5) / p;
-      const R inv2q = R(0.5) / q;
+      const R inv2p = R(0.5) * ip;
+      const R inv2q = R(0.5) * iq;
       const R inv2pq = R(0.5) * ipq;
       const R PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
       const R WPx = -rp * PQx, WPy = -rp * PQy, WPz = -rp * PQz;
       const R WQx = rq * PQx, WQy = rq * PQy, WQz = rq * PQz;
       const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-      const R pre = Kab * Kcd * R(PI_2_5) / (p * q * sqrt_t(pq));
+      const R pre = Kab * Kcd * rs;
 """
-PRIM_HEADER_FLOPS = 1 + 1 + 2 + 1 + 1 + 1 + 1 + 1 + 3 + 3 + 3 + 6 + 5
-
+PRIM_HEADER_FLOPS = 1 + 1 + 1 + 2 + 1 + 1 + 1 + 1 + 1 + 3 + 3 + 3 + 6 + 2
 
 def ncart(L):
     return (L + 1) * (L + 2) // 2
@@ -288,11 +288,11 @@ def gen_eri_class(la, lb, lc, ld):
     s.append(f"#pragma unroll")
     s.append(f"  for (int t = 0; t < {len(targets)}; ++t) acc[t] = R(0);")
     s.append("  for (int ib = 0; ib < nbp; ++ib) {")
-    s.append("    const R p = bp[ib].p, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
-    s.append("    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].K;")
+    s.append("    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
+    s.append("    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;")
     s.append("    for (int ik = 0; ik < nkp; ++ik) {")
-    s.append("      const R q = kp[ik].p, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
-    s.append("      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].K;")
+    s.append("      const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
+    s.append("      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;")
     s.append(PRIM_HEADER.rstrip("\n"))
     s.append(f"      R F[{L + 1}];")
     s.append(f"      boys.template eval<{L}>(T, pre, F);")
@@ -533,12 +533,12 @@ def gen_grad_class(la, lb, lc, ld):
     s.append("#pragma unroll")
     s.append(f"  for (int t = 0; t < {nacc}; ++t) acc[t] = R(0);")
     s.append("  for (int ib = 0; ib < nbp; ++ib) {")
-    s.append("    const R p = bp[ib].p, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
-    s.append("    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].K;")
+    s.append("    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
+    s.append("    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;")
     s.append("    const R wa = R(2) * ea[ib], wb = R(2) * eb[ib];")
     s.append("    for (int ik = 0; ik < nkp; ++ik) {")
-    s.append("      const R q = kp[ik].p, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
-    s.append("      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].K;")
+    s.append("      const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
+    s.append("      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;")
     s.append("      const R wc = R(2) * ec[ik];")
     s.append(PRIM_HEADER.rstrip("\n"))
     s.append(f"      R F[{L + 1}];")
@@ -645,7 +645,7 @@ namespace hfgpu {{
 template <typename R>
 static void launch_quartet(const QuartetArgs<R>& a, const int2* q, int nq, cudaStream_t s) {{
   if (nq <= 0) return;
-  quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 127) / 128, 128, 0, s>>>(a, q, nq);
+  quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 63) / 64, 64, 0, s>>>(a, q, nq);
 }}
 template <typename R>
 static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, int grid, cudaStream_t s) {{

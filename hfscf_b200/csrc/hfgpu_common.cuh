@@ -6,13 +6,15 @@
 #define PI_2_5 34.986836655249725  // 2 pi^(5/2), hfscfmath::PI_25 (src/math/hfscf_math.hpp:25)
 
 // ---------------------------------------------------------------------------
-// Primitive pair of a shell pair (a b): p = alpha_a + alpha_b, P, PA = P - A,
-// K = exp(-alpha_a alpha_b / p |AB|^2) c_a c_b -- BASIS::ShellPair::set_params
-// (src/integrals/hfscf_shellpair.cpp:33-61).  64 bytes in FP64, one cache-line half.
+// Primitive pair of a shell pair (a b): p = alpha_a + alpha_b, ip = 1/p, P,
+// PA = P - A and Kp = K sqrt(2 pi^2.5) / p with K = exp(-alpha_a alpha_b / p |AB|^2) c_a c_b
+// (BASIS::ShellPair::set_params, src/integrals/hfscf_shellpair.cpp:33-61).  Kp is
+// scaled so that the [00|00] prefactor K_ab K_cd 2 pi^2.5 / (p q sqrt(p+q)) is
+// Kp_ab Kp_cd / sqrt(p+q).  80 bytes in FP64 (five 16-byte loads).
 // ---------------------------------------------------------------------------
 template <typename R>
-struct __align__(sizeof(R) * 8) PrimPair {
-  R p, Px, Py, Pz, PAx, PAy, PAz, K;
+struct __align__(sizeof(R) * 2) PrimPair {
+  R p, ip, Px, Py, Pz, PAx, PAy, PAz, Kp, pad;
 };
 
 // One canonical shell pair (La >= Lb after an optional swap of the two shells).
@@ -43,6 +45,12 @@ template <>
 __device__ __forceinline__ double exp_t<double>(double x) { return exp(x); }
 template <>
 __device__ __forceinline__ float exp_t<float>(float x) { return expf(x); }
+template <typename R>
+__device__ __forceinline__ R rsqrt_t(R x);
+template <>
+__device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt(x); }
+template <>
+__device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
 
 // ---------------------------------------------------------------------------
 // Boys function F_m(T), m = 0..M, scaled by `pre`.
@@ -96,8 +104,9 @@ struct BoysTable {
         for (int m = M; m > 0; --m) F[m - 1] = (t2 * F[m] + e) * R(1.0 / (2 * m - 1));
       }
     } else {
-      const R it = R(1) / T;
-      F[0] = R(0.88622692545275801365) * sqrt_t<R>(it);  // sqrt(pi)/2 / sqrt(T)
+      const R rt = rsqrt_t<R>(T);
+      const R it = rt * rt;
+      F[0] = R(0.88622692545275801365) * rt;  // sqrt(pi)/2 / sqrt(T)
       if constexpr (M > 0) {
         const R e = exp_t<R>(-T);
         const R h = R(0.5) * it;

@@ -90,6 +90,10 @@ struct hfgpu_handle {
   DevBuf d_mats, d_half, d_dmax, d_counters, d_grad, d_scratch, d_eri, d_eriq;
   long long last_launched = 0, last_skipped = 0;
   int last_kernels = 0;                 // kernel launches of the last J/K build
+  // class kernels run concurrently on auxiliary streams (fork/join with events)
+  static constexpr int kAux = 6;
+  cudaStream_t aux[kAux] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[kAux] = {};
   bool timing = false;                  // record CUDA events around every class launch
   cudaEvent_t ev[2 * 21 + 2] = {};
   bool ev_used[21] = {};
@@ -189,13 +193,15 @@ int build_pairs(hfgpu_handle* h) {
         if (std::fabs(K) < kPrimPairCut) continue;
         PrimPair<double> q;
         q.p = p;
+        q.ip = 1.0 / p;
+        q.pad = 0.0;
         q.Px = (a1 * A[0] + a2 * B[0]) / p;
         q.Py = (a1 * A[1] + a2 * B[1]) / p;
         q.Pz = (a1 * A[2] + a2 * B[2]) / p;
         q.PAx = q.Px - A[0];
         q.PAy = q.Py - A[1];
         q.PAz = q.Pz - A[2];
-        q.K = K;
+        q.Kp = K * std::sqrt(PI_2_5) / p;
         pd.push_back(q);
         aa.push_back(a1);
         ab.push_back(a2);
@@ -210,8 +216,8 @@ int build_pairs(hfgpu_handle* h) {
   std::vector<PrimPair<float>> pf(np);
   std::vector<float> aaf(np), abf(np);
   for (size_t i = 0; i < pd.size(); ++i) {
-    pf[i] = {(float)pd[i].p, (float)pd[i].Px, (float)pd[i].Py, (float)pd[i].Pz,
-             (float)pd[i].PAx, (float)pd[i].PAy, (float)pd[i].PAz, (float)pd[i].K};
+    pf[i] = {(float)pd[i].p, (float)pd[i].ip, (float)pd[i].Px, (float)pd[i].Py, (float)pd[i].Pz,
+             (float)pd[i].PAx, (float)pd[i].PAy, (float)pd[i].PAz, (float)pd[i].Kp, 0.f};
     aaf[i] = (float)aa[i];
     abf[i] = (float)ab[i];
   }
@@ -364,6 +370,44 @@ __global__ void fp64_peak_kernel(double* out, int iters, double a, double b) {
 
 }  // namespace
 
+static int ensure_aux(hfgpu_handle* h) {
+  if (h->aux[0]) return HFGPU_OK;
+  for (int i = 0; i < hfgpu_handle::kAux; ++i) {
+    HF_CUDA(h, cudaStreamCreateWithFlags(&h->aux[i], cudaStreamNonBlocking));
+    HF_CUDA(h, cudaEventCreateWithFlags(&h->join_ev[i], cudaEventDisableTiming));
+  }
+  HF_CUDA(h, cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
+  return HFGPU_OK;
+}
+
+// Fork: every auxiliary stream waits for the work already queued on the handle's stream.
+static int fork_streams(hfgpu_handle* h) {
+  int rc = ensure_aux(h);
+  if (rc) return rc;
+  HF_CUDA(h, cudaEventRecord(h->fork_ev, h->stream));
+  for (int i = 0; i < hfgpu_handle::kAux; ++i) HF_CUDA(h, cudaStreamWaitEvent(h->aux[i], h->fork_ev, 0));
+  return HFGPU_OK;
+}
+
+// Join: the handle's stream waits for all auxiliary streams.
+static int join_streams(hfgpu_handle* h) {
+  for (int i = 0; i < hfgpu_handle::kAux; ++i) {
+    HF_CUDA(h, cudaEventRecord(h->join_ev[i], h->aux[i]));
+    HF_CUDA(h, cudaStreamWaitEvent(h->stream, h->join_ev[i], 0));
+  }
+  return HFGPU_OK;
+}
+
+// Largest classes first, each of the first kAux on its own stream, the rest
+// round-robin: the few-quartet, long-latency d classes then overlap the
+// many-quartet s/p classes instead of running alone on a handful of SMs.
+static void class_schedule(int* order, int* stream_of) {
+  for (int i = 0; i < hfgpu::kNumClasses; ++i) {
+    order[i] = hfgpu::kNumClasses - 1 - i;
+    stream_of[i] = i % hfgpu_handle::kAux;
+  }
+}
+
 static int read_counters(hfgpu_handle* h, long long* computed, long long* skipped) {
   std::vector<unsigned long long> c(3 * hfgpu::kNumClasses);
   HF_CUDA(h, cudaMemcpy(c.data(), h->d_counters.p, sizeof(unsigned long long) * c.size(), cudaMemcpyDeviceToHost));
@@ -417,28 +461,35 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   long long launched = 0;
   // largest classes first so that they overlap the tail of the smaller ones
   unsigned long long* cnt = h->d_counters.as<unsigned long long>();
-  for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
+  int rc0 = fork_streams(h);
+  if (rc0) return rc0;
+  int order[32], sidx[32];
+  class_schedule(order, sidx);
+  for (int i = 0; i < hfgpu::kNumClasses; ++i) {
+    const int c = order[i];
+    cudaStream_t st = h->aux[sidx[i]];
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
     const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
     qd.jk.counters = cnt + 3 * c;
     qf.jk.counters = cnt + 3 * c;
     h->ev_used[c] = false;
     if (e <= b) continue;
-    if (h->timing) HF_CUDA(h, cudaEventRecord(h->ev[2 * c], h->stream));
+    if (h->timing) HF_CUDA(h, cudaEventRecord(h->ev[2 * c], st));
     if (precision == HFGPU_MIXED) {
-      if (m > b) { L->quartet_d(qd, q + b, (int)(m - b), h->stream); ++kernels; }
-      if (e > m) { L->quartet_f(qf, q + m, (int)(e - m), h->stream); ++kernels; }
+      if (m > b) { L->quartet_d(qd, q + b, (int)(m - b), st); ++kernels; }
+      if (e > m) { L->quartet_f(qf, q + m, (int)(e - m), st); ++kernels; }
     } else {
-      L->quartet_d(qd, q + b, (int)(e - b), h->stream);
+      L->quartet_d(qd, q + b, (int)(e - b), st);
       ++kernels;
     }
     HF_CHECK_LAUNCH(h, "quartet kernel");
     if (h->timing) {
-      HF_CUDA(h, cudaEventRecord(h->ev[2 * c + 1], h->stream));
+      HF_CUDA(h, cudaEventRecord(h->ev[2 * c + 1], st));
       h->ev_used[c] = true;
     }
     launched += e - b;
   }
+  if ((rc0 = join_streams(h))) return rc0;
   h->last_launched = launched;
   const int tot = (int)nn;
   h->last_kernels = kernels + ((Jout && DJ) ? 1 : 0) + ((Kout && nK > 0) ? 1 : 0);
@@ -475,37 +526,51 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   gf.DJ = DJ; gf.cJ = cJ; gf.nK = nK; gf.DK = DK; gf.cK = cK; gf.grad = grad;
   const int2* q = h->d_quart.as<int2>();
   const size_t budget = (size_t)1 << 30;  // scratch bytes for table-mode classes
+  // Table-mode classes share one scratch buffer, so they run in order on aux[0];
+  // straight-line classes spread over the other auxiliary streams.
+  size_t need_max = 0;
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    const int slots = hfgpu::kClassLaunchers[c]->grad_scratch_slots(h->pure);
+    const long long nq = h->q_end[c] - h->q_beg[c];
+    if (slots <= 0 || nq <= 0) continue;
+    long long thr = std::max<long long>((long long)(budget / ((size_t)slots * sizeof(double))), 4736);
+    thr = std::min<long long>(thr, ((nq + 127) / 128) * 128);
+    need_max = std::max(need_max, (size_t)slots * sizeof(double) * (size_t)thr);
+  }
+  if (need_max) HF_CUDA(h, h->d_scratch.ensure(need_max));
+  int rc = fork_streams(h);
+  if (rc) return rc;
+  int rr = 1;
   for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
     const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
     if (e <= b) continue;
     const int slots = L->grad_scratch_slots(h->pure);
+    cudaStream_t st = slots > 0 ? h->aux[0] : h->aux[1 + (rr++ % (hfgpu_handle::kAux - 1))];
     auto run = [&](bool fp32, long long lo, long long hi) -> int {
       const int nq = (int)(hi - lo);
       if (nq <= 0) return HFGPU_OK;
       int grid = (nq + 127) / 128;
       if (slots > 0) {
         const size_t rb = fp32 ? sizeof(float) : sizeof(double);
-        long long thr = (long long)(budget / ((size_t)slots * rb));
-        thr = std::max<long long>(thr, 4736);
+        long long thr = std::max<long long>((long long)(budget / ((size_t)slots * sizeof(double))), 4736);
         thr = std::min<long long>(thr, (long long)grid * 128);
         grid = (int)((thr + 127) / 128);
-        const size_t need = (size_t)slots * rb * (size_t)grid * 128;
-        HF_CUDA(h, h->d_scratch.ensure(need));
+        if ((size_t)slots * rb * (size_t)grid * 128 > h->d_scratch.bytes)
+          return fail(h, HFGPU_ERR_NOMEM, "gradient scratch too small");
       }
       if (fp32) {
         gf.scratch = h->d_scratch.as<float>();
         gf.scratch_threads = grid * 128;
-        L->grad_f(gf, h->pure, q + lo, nq, grid, h->stream);
+        L->grad_f(gf, h->pure, q + lo, nq, grid, st);
       } else {
         gd.scratch = h->d_scratch.as<double>();
         gd.scratch_threads = grid * 128;
-        L->grad_d(gd, h->pure, q + lo, nq, grid, h->stream);
+        L->grad_d(gd, h->pure, q + lo, nq, grid, st);
       }
       HF_CHECK_LAUNCH(h, "grad kernel");
       return HFGPU_OK;
     };
-    int rc;
     if (precision == HFGPU_MIXED) {
       if ((rc = run(false, b, m))) return rc;
       if ((rc = run(true, m, e))) return rc;
@@ -513,7 +578,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
       return rc;
     }
   }
-  return HFGPU_OK;
+  return join_streams(h);
 }
 
 extern "C" {
@@ -609,6 +674,11 @@ int hfgpu_destroy(hfgpu_handle* h) {
     d->release();
   if (h->ev[0])
     for (auto& e : h->ev) cudaEventDestroy(e);
+  for (int i = 0; i < hfgpu_handle::kAux; ++i) {
+    if (h->aux[i]) cudaStreamDestroy(h->aux[i]);
+    if (h->join_ev[i]) cudaEventDestroy(h->join_ev[i]);
+  }
+  if (h->fork_ev) cudaEventDestroy(h->fork_ev);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return HFGPU_OK;

@@ -280,21 +280,22 @@ __device__ void grad_table(const PrimPair<R>* __restrict__ bp, const R* __restri
   const int(*vo)[10] = Tab::vrr();
   const int(*ho)[8] = Tab::hrr();
   for (int ib = 0; ib < nbp; ++ib) {
-    const R p = bp[ib].p, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;
-    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].K;
+    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;
+    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;
     const R wa = R(2) * ea[ib], wb = R(2) * eb[ib];
     for (int ik = 0; ik < nkp; ++ik) {
-      const R q = kp[ik].p, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;
-      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].K;
+      const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;
+      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;
       const R wc = R(2) * ec[ik];
       const R pq = p + q;
-      const R ipq = R(1) / pq;
+      const R rsq = rsqrt_t(pq);
+      const R ipq = rsq * rsq;
       const R rho = p * q * ipq;
       const R rp = q * ipq, rq = p * ipq;
-      const R inv2p = R(0.5) / p, inv2q = R(0.5) / q, inv2pq = R(0.5) * ipq;
+      const R inv2p = R(0.5) * ip, inv2q = R(0.5) * iq, inv2pq = R(0.5) * ipq;
       const R PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
       const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-      const R pre = Kab * Kcd * R(PI_2_5) / (p * q * sqrt_t(pq));
+      const R pre = Kab * Kcd * rsq;
       R F[Tab::L + 1];
       boys.template eval<Tab::L>(T, pre, F);
 #pragma unroll
