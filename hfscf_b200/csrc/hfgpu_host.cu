@@ -526,6 +526,13 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   gf.DJ = DJ; gf.cJ = cJ; gf.nK = nK; gf.DK = DK; gf.cK = cK; gf.grad = grad;
   const int2* q = h->d_quart.as<int2>();
   const size_t budget = (size_t)1 << 30;  // scratch bytes for table-mode classes
+  // threads of a table-mode launch: as many as the budget allows (at least 4736),
+  // at most one per quartet, a whole number of 128-thread blocks
+  auto table_threads = [&](int slots, long long nq) -> long long {
+    long long thr = std::max<long long>((long long)(budget / ((size_t)slots * sizeof(double))), 4736);
+    thr = std::min<long long>(thr, ((nq + 127) / 128) * 128);
+    return ((thr + 127) / 128) * 128;
+  };
   // Table-mode classes share one scratch buffer, so they run in order on aux[0];
   // straight-line classes spread over the other auxiliary streams.
   size_t need_max = 0;
@@ -533,9 +540,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     const int slots = hfgpu::kClassLaunchers[c]->grad_scratch_slots(h->pure);
     const long long nq = h->q_end[c] - h->q_beg[c];
     if (slots <= 0 || nq <= 0) continue;
-    long long thr = std::max<long long>((long long)(budget / ((size_t)slots * sizeof(double))), 4736);
-    thr = std::min<long long>(thr, ((nq + 127) / 128) * 128);
-    need_max = std::max(need_max, (size_t)slots * sizeof(double) * (size_t)thr);
+    need_max = std::max(need_max, (size_t)slots * sizeof(double) * (size_t)table_threads(slots, nq));
   }
   if (need_max) HF_CUDA(h, h->d_scratch.ensure(need_max));
   int rc = fork_streams(h);
@@ -553,9 +558,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
       int grid = (nq + 127) / 128;
       if (slots > 0) {
         const size_t rb = fp32 ? sizeof(float) : sizeof(double);
-        long long thr = std::max<long long>((long long)(budget / ((size_t)slots * sizeof(double))), 4736);
-        thr = std::min<long long>(thr, (long long)grid * 128);
-        grid = (int)((thr + 127) / 128);
+        grid = (int)(table_threads(slots, nq) / 128);
         if ((size_t)slots * rb * (size_t)grid * 128 > h->d_scratch.bytes)
           return fail(h, HFGPU_ERR_NOMEM, "gradient scratch too small");
       }
