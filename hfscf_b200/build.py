@@ -75,6 +75,7 @@ def build(jobs: int | None = None, verbose: bool = False) -> str:
     generate()
     srcs = sorted(glob.glob(os.path.join(GEN, "inst_*.cu"))) + [os.path.join(GEN, "dispatch.cu"),
                                                                  os.path.join(CSRC, "hfgpu_host.cu"),
+                                                                 os.path.join(CSRC, "hfgpu_noalloc.cu"),
                                                                  os.path.join(CSRC, "hfgpu_onee.cpp")]
     # largest classes first so they do not finish last
     srcs.sort(key=lambda s: -os.path.getsize(os.path.join(GEN, "class_" + os.path.basename(s)[5:-3] + ".cuh"))

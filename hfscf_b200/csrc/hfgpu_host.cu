@@ -584,6 +584,72 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   return join_streams(h);
 }
 
+// Gradient with caller-provided scratch of fixed capacity, on the handle's stream
+// only.  Allocates nothing: table-mode classes get as many threads as the scratch
+// holds (whole 128-thread blocks); a class that cannot fit one block is rejected.
+int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
+                             double* grad, int precision, void* scratch, size_t scratch_bytes) {
+  if (!h || !grad || !scratch) return HFGPU_ERR_INVALID;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  int rc = set_device(h);
+  if (rc) return rc;
+  GradArgs<double> gd{};
+  gd.pairs = h->d_pairs.as<PairInfo>();
+  gd.prims = h->d_prim_d.as<PrimPair<double>>();
+  const size_t np = std::max<size_t>(h->nprimpairs, 1);
+  gd.alpha_a = h->d_alpha_d.as<double>();
+  gd.alpha_b = h->d_alpha_d.as<double>() + np;
+  gd.boys.tab = h->d_boys_d.as<double>();
+  gd.n = h->n;
+  gd.DJ = DJ; gd.cJ = cJ; gd.nK = nK; gd.DK = DK; gd.cK = cK; gd.grad = grad;
+  gd.scratch = static_cast<double*>(scratch);
+  GradArgs<float> gf{};
+  gf.pairs = gd.pairs;
+  gf.prims = h->d_prim_f.as<PrimPair<float>>();
+  gf.alpha_a = h->d_alpha_f.as<float>();
+  gf.alpha_b = h->d_alpha_f.as<float>() + np;
+  gf.boys.tab = h->d_boys_f.as<float>();
+  gf.n = h->n;
+  gf.DJ = DJ; gf.cJ = cJ; gf.nK = nK; gf.DK = DK; gf.cK = cK; gf.grad = grad;
+  gf.scratch = static_cast<float*>(scratch);
+  const int2* q = h->d_quart.as<int2>();
+  for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
+    const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
+    const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
+    if (e <= b) continue;
+    const int slots = L->grad_scratch_slots(h->pure);
+    for (int part = 0; part < 2; ++part) {
+      const bool fp32 = precision == HFGPU_MIXED && part == 1;
+      const long long lo = (precision == HFGPU_MIXED) ? (part == 0 ? b : m) : (part == 0 ? b : e);
+      const long long hi = (precision == HFGPU_MIXED) ? (part == 0 ? m : e) : e;
+      const int nq = (int)(hi - lo);
+      if (nq <= 0) continue;
+      int grid = (nq + 127) / 128;
+      if (slots > 0) {
+        const size_t per_thread = (size_t)slots * (fp32 ? sizeof(float) : sizeof(double));
+        const long long fit = (long long)(scratch_bytes / per_thread) / 128 * 128;
+        if (fit < 128)
+          return fail(h, HFGPU_ERR_INVALID,
+                      "gradient class needs " + std::to_string(per_thread * 128) +
+                          " bytes of scratch for one 128-thread block, more than the fixed scratch of " +
+                          std::to_string(scratch_bytes) + " bytes");
+        grid = (int)(std::min<long long>(fit, (long long)grid * 128) / 128);
+      }
+      if (fp32) {
+        gf.scratch_threads = grid * 128;
+        L->grad_f(gf, h->pure, q + lo, nq, grid, h->stream);
+      } else {
+        gd.scratch_threads = grid * 128;
+        L->grad_d(gd, h->pure, q + lo, nq, grid, h->stream);
+      }
+      HF_CHECK_LAUNCH(h, "grad kernel (fixed scratch)");
+    }
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_device_of(const hfgpu_handle* h) { return h ? h->device : -1; }
+
 extern "C" {
 
 int hfgpu_default_opts(hfgpu_opts* o) {

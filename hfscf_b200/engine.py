@@ -62,7 +62,7 @@ def exported_symbols():
     import re
     hdr = os.path.join(os.path.dirname(HERE), "include", "hfgpu.h")
     text = open(hdr).read()
-    return sorted(set(re.findall(r"^(?:int|const char\*)\s+(hfgpu_[a-z0-9_]+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^(?:int|long long|const char\*)\s+(hfgpu_[a-z0-9_]+)\s*\(", text, re.M)))
 
 
 def _p(a, ct=ctypes.c_double):

@@ -121,6 +121,19 @@ int hfgpu_jk_device(hfgpu_handle* h, const double* DJ, int nK, const double* DK,
 int hfgpu_grad2e_device(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
                         double* grad, int precision);
 
+/* Same result as hfgpu_grad2e_device, for callers that cannot allocate device memory
+ * while they run (their allocator owns the device, or allocation is forbidden after
+ * start-up).  No counterpart in the reference.  Allocates nothing: the scratch of the
+ * large gradient classes comes from a fixed array of hfgpu_noalloc_scratch_bytes()
+ * (32 MiB) inside the library, held on every device that loads it until exit; a
+ * class whose smallest launch does not fit returns HFGPU_ERR_INVALID.  The first call
+ * on a device looks up the array's address (make it before any stream capture); all
+ * calls share the array, so calls that overlap on the GPU race.  Runs on the handle's
+ * stream; grad is accumulated into, as in hfgpu_grad2e_device. */
+int hfgpu_grad2e_device_noalloc(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
+                                double* grad, int precision);
+long long hfgpu_noalloc_scratch_bytes(void);
+
 /* One-electron matrices S, T, V (n x n) for the basis at xyz (bohr), on the host CPU.
  * Z: nuclear charges per atom.  Needs no handle and no GPU: these O(N^2) integrals
  * stay on the CPU here (the reference's OSOverlap/OSKinetic/OSNuclear,
