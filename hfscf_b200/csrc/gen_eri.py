@@ -600,12 +600,22 @@ def common_header():
     return "\n".join(out) + "\n"
 
 
+WARP_MIN_VRR = 270   # energy classes with at least this many VRR values run one warp per quartet
+
+
 def class_header(c):
     la, lb, lc, ld = c
     t = f"{la}{lb}{lc}{ld}"
     parts = ["// GENERATED by gen_eri.py -- do not edit.", "#pragma once", '#include "common.cuh"', ""]
     code, m = gen_eri_class(*c)
-    parts += [code, ""]
+    warp = m["vrr_values"] >= WARP_MIN_VRR
+    m["warp"] = warp
+    if warp:
+        wcode, wm = gen_warp_class(*c)
+        parts += [wcode, ""]
+        m.update({"warp_" + k: v for k, v in wm.items() if k != "class"})
+    else:
+        parts += [code, ""]
     pc, pf = gen_pure(*c)
     parts += [pc, ""]
     parts += [gen_pure_T(*c), ""]
@@ -620,11 +630,14 @@ def class_header(c):
     parts.append(f"template <>")
     parts.append(f"struct ClassCode<{la}, {lb}, {lc}, {ld}> {{")
     parts.append(f"  static constexpr bool kGradTable = {'false' if straight else 'true'};")
+    parts.append(f"  static constexpr bool kWarp = {'true' if warp else 'false'};")
+    parts.append(f"  using WarpTab = {'WarpTab' + t if warp else 'void'};")
     parts.append(f"  using GradTab = {'void' if straight else 'GradTable' + t};")
-    parts.append(f"  template <typename R>")
-    parts.append(f"  static __device__ __forceinline__ void eri({class_args_sig()}) {{")
-    parts.append(f"    eri_{t}<R>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out);")
-    parts.append("  }")
+    if not warp:
+        parts.append(f"  template <typename R>")
+        parts.append(f"  static __device__ __forceinline__ void eri({class_args_sig()}) {{")
+        parts.append(f"    eri_{t}<R>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out);")
+        parts.append("  }")
     parts.append("  template <typename R>")
     parts.append(f"  static __device__ __forceinline__ void to_pure(const R* __restrict__ in, R* __restrict__ out) {{ to_pure_{t}<R>(in, out); }}")
     parts.append("  template <typename R>")
@@ -642,10 +655,23 @@ INST_TEMPLATE = """// GENERATED by gen_eri.py -- do not edit.
 #include "../hfgpu_launch.h"
 
 namespace hfgpu {{
+template <typename CC, typename R>
+static void launch_quartet_impl(const QuartetArgs<R>& a, const int2* q, int nq, cudaStream_t s) {{
+  if constexpr (CC::kWarp) {{
+    using Tab = typename CC::WarpTab;
+    constexpr int per = warp_slots<Tab, R>();
+    const int bytes = 4 * per * (int)sizeof(R);
+    auto k = quartet_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    k<<<(nq + 3) / 4, 128, bytes, s>>>(a, q, nq);
+  }} else {{
+    quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 63) / 64, 64, 0, s>>>(a, q, nq);
+  }}
+}}
 template <typename R>
 static void launch_quartet(const QuartetArgs<R>& a, const int2* q, int nq, cudaStream_t s) {{
   if (nq <= 0) return;
-  quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 63) / 64, 64, 0, s>>>(a, q, nq);
+  launch_quartet_impl<ClassCode<{la}, {lb}, {lc}, {ld}>, R>(a, q, nq, s);
 }}
 template <typename R>
 static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, int grid, cudaStream_t s) {{
@@ -935,6 +961,174 @@ def gen_grad_table(la, lb, lc, ld):
     meta = {"class": [la, lb, lc, ld], "table": True, "vrr_ops": len(vrr_rows), "vrr_slots": nvslot,
             "accumulators": nacc, "hrr_ops": len(hrows), "hrr_slots": nhslot,
             "prim_flops": flops + PRIM_HEADER_FLOPS, "hrr_flops": hfl, "boys_m": L}
+    return "\n".join(s), meta
+
+
+
+
+# ---------------------------------------------------------------------------
+# Warp mode: the large energy classes run one warp per quartet.  The VRR and
+# HRR are levelised (an op's inputs come from earlier levels only), so the 32
+# lanes execute one level's ops in parallel out of shared memory, with a
+# __syncwarp between levels.  Slots are reused once their last reader's level
+# has completed.
+# ---------------------------------------------------------------------------
+def _levelise(nodes_deps, n_pre):
+    """nodes_deps: list of (node id, [dep ids]) in topological order; ids < n_pre are inputs (level 0)."""
+    lev = {i: 0 for i in range(n_pre)}
+    for nid, deps in nodes_deps:
+        lev[nid] = 1 + max([lev[d] for d in deps] + [0])
+    return lev
+
+
+def _alloc_levels(order_by_level, deps_of, lev, pre_slots, live_to_end):
+    """Slot allocation with level granularity.  Returns (slot map, number of slots)."""
+    last = {}
+    for nid in order_by_level:
+        for d in deps_of[nid]:
+            last[d] = max(last.get(d, -1), lev[nid])
+    END = 10 ** 9
+    for v in live_to_end:
+        last[v] = END
+    slot = dict(pre_slots)
+    top = max(list(pre_slots.values()) + [-1]) + 1
+    free = []
+    # inputs never read are free from the start
+    for v, s in pre_slots.items():
+        if v not in last:
+            free.append(s)
+    maxlev = max([lev[n] for n in order_by_level] + [0])
+    by_level = {}
+    for nid in order_by_level:
+        by_level.setdefault(lev[nid], []).append(nid)
+    freed_at = {}
+    for v, l in last.items():
+        if l != END:
+            freed_at.setdefault(l, []).append(v)
+    for v in pre_slots:
+        if v in last and last[v] == 0:
+            pass
+    for l in range(1, maxlev + 1):
+        for nid in by_level.get(l, []):
+            if free:
+                slot[nid] = free.pop()
+            else:
+                slot[nid] = top
+                top += 1
+        for v in freed_at.get(l, []):
+            if v in slot:
+                free.append(slot[v])
+    return slot, top
+
+
+def gen_warp_class(la, lb, lc, ld):
+    L = la + lb + lc + ld
+    dag = Dag(L)
+    targets = vrr_targets(la, la + lb, lc, lc + ld)
+    tnodes = [dag.get(e, f, 0) for e, f in targets]
+    ops = [(nid, nd) for nid, nd in enumerate(dag.nodes) if nd[0] != "F"]
+    deps = {nid: [x for x in nd[2:7] if x >= 0] for nid, nd in ops}
+    lev = _levelise([(nid, deps[nid]) for nid, _ in ops], L + 1)
+    order = sorted([nid for nid, _ in ops], key=lambda n: (lev[n], n))
+    pre = {m: m for m in range(L + 1)}
+    slot, nvs = _alloc_levels(order, deps, lev, pre, set(tnodes))
+    ZV = nvs  # zero slot
+    nodes = dict(ops)
+    vrows, vlev = [], [0]
+    cur = 1
+    for nid in order:
+        while lev[nid] > cur:
+            vlev.append(len(vrows))
+            cur += 1
+        kind, i, a, b, c, d, g, k1, k2 = nodes[nid]
+        s_ = lambda x: slot[x] if x >= 0 else ZV
+        vrows.append(((1 if kind == "K" else 0) | (i << 2), slot[nid], s_(a), s_(b), s_(c), s_(d), s_(g),
+                      k1 | (k2 << 8)))
+    vlev.append(len(vrows))
+    acc_rows = [slot[n] for n in tnodes]
+    nacc = len(targets)
+    # HRR DAG on the accumulators
+    acc_of = {t: j for j, t in enumerate(targets)}
+    hnodes, hdeps, hinfo = {}, {}, {}
+    counter = [nacc]
+
+    def ket(e, c, d):
+        key = ("k", e, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(d) == 0:
+            v = acc_of[(e, c)]
+        else:
+            i = max(range(3), key=lambda q: (d[q], -q))
+            d1 = add(d, i, -1)
+            x = ket(e, add(c, i), d1)
+            y = ket(e, c, d1)
+            v = counter[0]
+            counter[0] += 1
+            hdeps[v] = [x, y]
+            hinfo[v] = (1, i, x, y)
+        hnodes[key] = v
+        return v
+
+    def bra(a, b, c, d):
+        key = ("b", a, b, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(b) == 0:
+            v = ket(a, c, d)
+        else:
+            i = max(range(3), key=lambda q: (b[q], -q))
+            b1 = add(b, i, -1)
+            x = bra(add(a, i), b1, c, d)
+            y = bra(a, b1, c, d)
+            v = counter[0]
+            counter[0] += 1
+            hdeps[v] = [x, y]
+            hinfo[v] = (0, i, x, y)
+        hnodes[key] = v
+        return v
+
+    outs = [bra(a, b, c, d) for a in cart(la) for b in cart(lb) for c in cart(lc) for d in cart(ld)]
+    hord = sorted(hinfo, key=lambda v: v)
+    hlev = _levelise([(v, hdeps[v]) for v in hord], nacc)
+    hord = sorted(hord, key=lambda v: (hlev[v], v))
+    hpre = {j: j for j in range(nacc)}
+    hslot, nhs = _alloc_levels(hord, hdeps, hlev, hpre, set(outs))
+    hrows, hlv = [], [0]
+    cur = 1
+    for v in hord:
+        while hlev[v] > cur:
+            hlv.append(len(hrows))
+            cur += 1
+        kind, i, x, y = hinfo[v]
+        hrows.append((kind | (i << 2), hslot[v], hslot[x], hslot[y]))
+    hlv.append(len(hrows))
+    wout = [hslot[o] for o in outs]
+    t = f"{la}{lb}{lc}{ld}"
+    ncart_blk = len(outs)
+    s = [f"// warp-mode J/K of class {t}: {len(vrows)} VRR ops in {len(vlev) - 1} levels over {nvs} slots, "
+         f"{nacc} accumulators, {len(hrows)} HRR ops in {len(hlv) - 1} levels over {nhs} slots"]
+    s.append(f"__device__ const int wvrr_{t}[{max(len(vrows), 1)}][8] = {{")
+    s += ["  {" + ",".join(map(str, r)) + "}," for r in vrows]
+    s.append("};")
+    s.append(f"__device__ const int wvrr_lv_{t}[{len(vlev)}] = {{{','.join(map(str, vlev))}}};")
+    s.append(f"__device__ const int wacc_{t}[{nacc}] = {{{','.join(map(str, acc_rows))}}};")
+    s.append(f"__device__ const int whrr_{t}[{max(len(hrows), 1)}][4] = {{")
+    s += ["  {" + ",".join(map(str, r)) + "}," for r in hrows] or ["  {0,0,0,0},"]
+    s.append("};")
+    s.append(f"__device__ const int whrr_lv_{t}[{len(hlv)}] = {{{','.join(map(str, hlv))}}};")
+    s.append(f"__device__ const int wout_{t}[{ncart_blk}] = {{{','.join(map(str, wout))}}};")
+    s.append(f"struct WarpTab{t} {{ static constexpr int L = {L}, NVLEV = {len(vlev) - 1}, NVSLOT = {nvs}, "
+             f"NACC = {nacc}, NHLEV = {len(hlv) - 1}, NHSLOT = {nhs}, NCART = {ncart_blk}; "
+             f"static __device__ const int (*vrr())[8] {{ return wvrr_{t}; }} "
+             f"static __device__ const int* vlev() {{ return wvrr_lv_{t}; }} "
+             f"static __device__ const int* acc() {{ return wacc_{t}; }} "
+             f"static __device__ const int (*hrr())[4] {{ return whrr_{t}; }} "
+             f"static __device__ const int* hlev() {{ return whrr_lv_{t}; }} "
+             f"static __device__ const int* out() {{ return wout_{t}; }} }};")
+    meta = {"class": [la, lb, lc, ld], "vrr_ops": len(vrows), "vrr_levels": len(vlev) - 1, "vrr_slots": nvs,
+            "acc": nacc, "hrr_ops": len(hrows), "hrr_levels": len(hlv) - 1, "hrr_slots": nhs,
+            "smem_doubles_per_warp": nvs + 1 + nhs + 1 + 2 * ncart_blk}
     return "\n".join(s), meta
 
 

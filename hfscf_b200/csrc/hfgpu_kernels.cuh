@@ -465,3 +465,235 @@ __global__ void __launch_bounds__(128) grad_kernel(GradArgs<R> a, int pure, cons
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Warp-per-quartet kernel for the large classes (generated levelised tables).
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void warp_to_pure(const R* src, R* dst0, R* dst1, const int* Ls, int lane, const R** out) {
+  // one index at a time, ping-pong between dst0 and dst1
+  int dims[4] = {ncart_of(Ls[0]), ncart_of(Ls[1]), ncart_of(Ls[2]), ncart_of(Ls[3])};
+  const R* in = src;
+  R* bufs[2] = {dst0, dst1};
+  for (int st = 0; st < 4; ++st) {
+    const int nc = ncart_of(Ls[st]), np = npure_of(Ls[st]);
+    int nd[4] = {dims[0], dims[1], dims[2], dims[3]};
+    nd[st] = np;
+    R* o = bufs[st & 1];
+    const int tot = nd[0] * nd[1] * nd[2] * nd[3];
+    for (int e = lane; e < tot; e += 32) {
+      int id[4];
+      int r = e;
+      for (int q = 3; q >= 0; --q) {
+        id[q] = r % nd[q];
+        r /= nd[q];
+      }
+      R v = R(0);
+      for (int c = 0; c < nc; ++c) {
+        const double y = c_ylm[Ls[st]][c * np + id[st]];
+        if (y == 0.0) continue;
+        int jd[4] = {id[0], id[1], id[2], id[3]};
+        jd[st] = c;
+        v += R(y) * in[((jd[0] * dims[1] + jd[1]) * dims[2] + jd[2]) * dims[3] + jd[3]];
+      }
+      o[e] = v;
+    }
+    __syncwarp();
+    for (int q = 0; q < 4; ++q) dims[q] = nd[q];
+    in = o;
+  }
+  *out = in;
+}
+
+template <typename R>
+__device__ __forceinline__ void warp_digest(const R* V, int NA, int NB, int NC, int ND, int fa, int fb, int fc, int fd,
+                                            double s, const double* __restrict__ DJ, int nK,
+                                            const double* __restrict__ DK, double* Jh, double* Kh, int n, int lane) {
+  const int NCD = NC * ND;
+  if (DJ != nullptr) {
+    for (int x = lane; x < NA * NB; x += 32) {
+      double acc = 0.0;
+      for (int c = 0; c < NC; ++c)
+        for (int d = 0; d < ND; ++d) acc += __ldg(DJ + (size_t)(fc + c) * n + fd + d) * double(V[x * NCD + c * ND + d]);
+      atomicAdd(Jh + (size_t)(fa + x / NB) * n + fb + x % NB, 2.0 * s * acc);
+    }
+    for (int y = lane; y < NCD; y += 32) {
+      double acc = 0.0;
+      for (int a = 0; a < NA; ++a)
+        for (int b = 0; b < NB; ++b) acc += __ldg(DJ + (size_t)(fa + a) * n + fb + b) * double(V[(a * NB + b) * NCD + y]);
+      atomicAdd(Jh + (size_t)(fc + y / ND) * n + fd + y % ND, 2.0 * s * acc);
+    }
+  }
+  for (int m = 0; m < nK; ++m) {
+    const double* D = DK + (size_t)m * n * n;
+    double* K = Kh + (size_t)m * n * n;
+    for (int x = lane; x < NA * NC; x += 32) {  // K_ac += D_bd V
+      const int a = x / NC, c = x % NC;
+      double acc = 0.0;
+      for (int b = 0; b < NB; ++b)
+        for (int d = 0; d < ND; ++d) acc += __ldg(D + (size_t)(fb + b) * n + fd + d) * double(V[((a * NB + b) * NC + c) * ND + d]);
+      atomicAdd(K + (size_t)(fa + a) * n + fc + c, s * acc);
+    }
+    for (int x = lane; x < NA * ND; x += 32) {  // K_ad += D_bc V
+      const int a = x / ND, d = x % ND;
+      double acc = 0.0;
+      for (int b = 0; b < NB; ++b)
+        for (int c = 0; c < NC; ++c) acc += __ldg(D + (size_t)(fb + b) * n + fc + c) * double(V[((a * NB + b) * NC + c) * ND + d]);
+      atomicAdd(K + (size_t)(fa + a) * n + fd + d, s * acc);
+    }
+    for (int x = lane; x < NB * NC; x += 32) {  // K_bc += D_ad V
+      const int b = x / NC, c = x % NC;
+      double acc = 0.0;
+      for (int a = 0; a < NA; ++a)
+        for (int d = 0; d < ND; ++d) acc += __ldg(D + (size_t)(fa + a) * n + fd + d) * double(V[((a * NB + b) * NC + c) * ND + d]);
+      atomicAdd(K + (size_t)(fb + b) * n + fc + c, s * acc);
+    }
+    for (int x = lane; x < NB * ND; x += 32) {  // K_bd += D_ac V
+      const int b = x / ND, d = x % ND;
+      double acc = 0.0;
+      for (int a = 0; a < NA; ++a)
+        for (int c = 0; c < NC; ++c) acc += __ldg(D + (size_t)(fa + a) * n + fc + c) * double(V[((a * NB + b) * NC + c) * ND + d]);
+      atomicAdd(K + (size_t)(fb + b) * n + fd + d, s * acc);
+    }
+  }
+}
+
+template <typename Tab, typename R>
+constexpr int warp_slots() {
+  return Tab::NVSLOT + 1 + Tab::NHSLOT + 1 + 2 * Tab::NCART;
+}
+
+// One warp per unique quartet: the levelised VRR and HRR run lane-parallel out
+// of shared memory; transform and digestion are lane-parallel over the block.
+template <int LA, int LB, int LC, int LD, typename R, typename Tab>
+__global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets,
+                                                           int nq) {
+  extern __shared__ __align__(16) unsigned char wsmem[];
+  constexpr int PER = warp_slots<Tab, R>();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int qi = blockIdx.x * (blockDim.x >> 5) + w;
+  if (qi >= nq) return;  // whole warp
+  R* vs = reinterpret_cast<R*>(wsmem) + (size_t)w * PER;
+  R* hs = vs + Tab::NVSLOT + 1;
+  R* A = hs + Tab::NHSLOT + 1;
+  R* Bb = A + Tab::NCART;
+  const JKArgs<R>& a = qa.jk;
+  const int2 pq = quartets[qi];
+  const PairInfo P = a.pairs[pq.x];
+  const PairInfo Q = a.pairs[pq.y];
+  bool skip = false;
+  if (qa.mode == QMODE_JK && a.dmax != nullptr) {
+    const float* dm = a.dmax;
+    const int ns = a.nshell;
+    float m = 4.f * fmaxf(dm[P.sa * ns + P.sb], dm[Q.sa * ns + Q.sb]);
+    m = fmaxf(m, fmaxf(fmaxf(dm[P.sa * ns + Q.sa], dm[P.sa * ns + Q.sb]), fmaxf(dm[P.sb * ns + Q.sa], dm[P.sb * ns + Q.sb])));
+    skip = P.schwarz * Q.schwarz * double(m) < a.dtol;
+  }
+  if (a.counters != nullptr && lane == 0) {
+    atomicAdd(a.counters + (skip ? 1 : 0), 1ull);
+    if (!skip) atomicAdd(a.counters + 2, (unsigned long long)(P.nprim * Q.nprim));
+  }
+  if (skip) return;
+  if (lane == 0) {
+    vs[Tab::NVSLOT] = R(0);
+    hs[Tab::NHSLOT] = R(0);
+  }
+  for (int t = lane; t < Tab::NACC; t += 32) hs[t] = R(0);
+  __syncwarp();
+  const PrimPair<R>* bp = a.prims + P.prim_off;
+  const PrimPair<R>* kp = a.prims + Q.prim_off;
+  const int(*vo)[8] = Tab::vrr();
+  const int* vl = Tab::vlev();
+  const int* accs = Tab::acc();
+  for (int ib = 0; ib < P.nprim; ++ib) {
+    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;
+    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;
+    for (int ik = 0; ik < Q.nprim; ++ik) {
+      const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;
+      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;
+      const R pqs = p + q;
+      const R rs = rsqrt_t(pqs);
+      const R ipq = rs * rs;
+      const R rho = p * q * ipq;
+      const R rp = q * ipq, rq = p * ipq;
+      const R inv2p = R(0.5) * ip, inv2q = R(0.5) * iq, inv2pq = R(0.5) * ipq;
+      const R PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+      const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+      R F[Tab::L + 1];
+      a.boys.template eval<Tab::L>(T, Kab * Kcd * rs, F);
+#pragma unroll
+      for (int m = 0; m <= Tab::L; ++m)
+        if (lane == m) vs[m] = F[m];
+      __syncwarp();
+      for (int l = 0; l < Tab::NVLEV; ++l) {
+        const int e = __ldg(vl + l + 1);
+        for (int o = __ldg(vl + l) + lane; o < e; o += 32) {
+          const int kd = __ldg(&vo[o][0]), dst = __ldg(&vo[o][1]);
+          const int sa = __ldg(&vo[o][2]), sb = __ldg(&vo[o][3]), sc = __ldg(&vo[o][4]), sd = __ldg(&vo[o][5]);
+          const int k12 = __ldg(&vo[o][7]);
+          const int dir = kd >> 2;
+          const R PQd = dir == 0 ? PQx : (dir == 1 ? PQy : PQz);
+          const R k1 = R(k12 & 255);
+          R v;
+          if ((kd & 1) == 0) {
+            const R PA = dir == 0 ? PAx : (dir == 1 ? PAy : PAz);
+            v = PA * vs[sa] - rp * PQd * vs[sb] + k1 * inv2p * (vs[sc] - rp * vs[sd]);
+          } else {
+            const R QC = dir == 0 ? QCx : (dir == 1 ? QCy : QCz);
+            const int sg = __ldg(&vo[o][6]);
+            v = QC * vs[sa] + rq * PQd * vs[sb] + k1 * inv2q * (vs[sc] - rq * vs[sd]) + R(k12 >> 8) * inv2pq * vs[sg];
+          }
+          vs[dst] = v;
+        }
+        __syncwarp();
+      }
+      for (int t = lane; t < Tab::NACC; t += 32) hs[t] += vs[__ldg(accs + t)];
+      __syncwarp();
+    }
+  }
+  const int(*ho)[4] = Tab::hrr();
+  const int* hl = Tab::hlev();
+  const R ABx = R(P.ABx), ABy = R(P.ABy), ABz = R(P.ABz), CDx = R(Q.ABx), CDy = R(Q.ABy), CDz = R(Q.ABz);
+  for (int l = 0; l < Tab::NHLEV; ++l) {
+    const int e = __ldg(hl + l + 1);
+    for (int o = __ldg(hl + l) + lane; o < e; o += 32) {
+      const int kd = __ldg(&ho[o][0]), dir = kd >> 2;
+      const R d = (kd & 1) ? (dir == 0 ? CDx : (dir == 1 ? CDy : CDz)) : (dir == 0 ? ABx : (dir == 1 ? ABy : ABz));
+      hs[__ldg(&ho[o][1])] = hs[__ldg(&ho[o][2])] + d * hs[__ldg(&ho[o][3])];
+    }
+    __syncwarp();
+  }
+  const int* outs = Tab::out();
+  for (int o = lane; o < Tab::NCART; o += 32) A[o] = hs[__ldg(outs + o)];
+  __syncwarp();
+  const R* V = A;
+  int NA = ncart_of(LA), NB = ncart_of(LB), NC = ncart_of(LC), ND = ncart_of(LD);
+  if (qa.pure) {
+    const int Ls[4] = {LA, LB, LC, LD};
+    warp_to_pure<R>(A, Bb, A, Ls, lane, &V);
+    NA = npure_of(LA);
+    NB = npure_of(LB);
+    NC = npure_of(LC);
+    ND = npure_of(LD);
+  }
+  double s = 1.0;
+  if (P.sa == P.sb) s *= 0.5;
+  if (Q.sa == Q.sb) s *= 0.5;
+  if (pq.x == pq.y) s *= 0.5;
+  if (qa.mode == QMODE_JK) {
+    warp_digest<R>(V, NA, NB, NC, ND, P.fa, P.fb, Q.fa, Q.fb, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, lane);
+  } else if (qa.mode == QMODE_PACKED) {
+    for (int e = lane; e < NA * NB * NC * ND; e += 32) {
+      const int l = e % ND, k = (e / ND) % NC, j = (e / (ND * NC)) % NB, i = e / (ND * NC * NB);
+      qa.eri[packed_index(P.fa + i, P.fb + j, Q.fa + k, Q.fb + l)] = double(V[e]);
+    }
+  } else {
+    double m = 0.0;
+    for (int x = lane; x < NA * NB; x += 32) {
+      const int i = x / NB, j = x % NB;
+      m = fmax(m, fabs(double(V[((i * NB + j) * NC + i) * ND + j])));
+    }
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if (lane == 0) qa.pairs_rw[pq.x].schwarz = sqrt(m);
+  }
+}
