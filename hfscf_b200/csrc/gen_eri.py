@@ -610,12 +610,11 @@ def class_header(c):
     code, m = gen_eri_class(*c)
     warp = m["vrr_values"] >= WARP_MIN_VRR
     m["warp"] = warp
+    parts += [code, ""]
     if warp:
         wcode, wm = gen_warp_class(*c)
         parts += [wcode, ""]
         m.update({"warp_" + k: v for k, v in wm.items() if k != "class"})
-    else:
-        parts += [code, ""]
     pc, pf = gen_pure(*c)
     parts += [pc, ""]
     parts += [gen_pure_T(*c), ""]
@@ -633,11 +632,10 @@ def class_header(c):
     parts.append(f"  static constexpr bool kWarp = {'true' if warp else 'false'};")
     parts.append(f"  using WarpTab = {'WarpTab' + t if warp else 'void'};")
     parts.append(f"  using GradTab = {'void' if straight else 'GradTable' + t};")
-    if not warp:
-        parts.append(f"  template <typename R>")
-        parts.append(f"  static __device__ __forceinline__ void eri({class_args_sig()}) {{")
-        parts.append(f"    eri_{t}<R>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out);")
-        parts.append("  }")
+    parts.append(f"  template <typename R>")
+    parts.append(f"  static __device__ __forceinline__ void eri({class_args_sig()}) {{")
+    parts.append(f"    eri_{t}<R>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out);")
+    parts.append("  }")
     parts.append("  template <typename R>")
     parts.append(f"  static __device__ __forceinline__ void to_pure(const R* __restrict__ in, R* __restrict__ out) {{ to_pure_{t}<R>(in, out); }}")
     parts.append("  template <typename R>")
@@ -655,8 +653,17 @@ INST_TEMPLATE = """// GENERATED by gen_eri.py -- do not edit.
 #include "../hfgpu_launch.h"
 
 namespace hfgpu {{
+// Large classes: one warp per quartet when the class has too few quartets to keep
+// the GPU busy with one (spilling, latency-bound) thread per quartet; one thread
+// per quartet otherwise.
 template <typename CC, typename R>
 static void launch_quartet_impl(const QuartetArgs<R>& a, const int2* q, int nq, cudaStream_t s) {{
+  bool warp = false;
+  if constexpr (CC::kWarp) warp = nq <= a.warp_max;
+  if (!warp) {{
+    quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 63) / 64, 64, 0, s>>>(a, q, nq);
+    return;
+  }}
   if constexpr (CC::kWarp) {{
     using Tab = typename CC::WarpTab;
     constexpr int per = warp_slots<Tab, R>();
@@ -664,8 +671,6 @@ static void launch_quartet_impl(const QuartetArgs<R>& a, const int2* q, int nq, 
     auto k = quartet_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     k<<<(nq + 3) / 4, 128, bytes, s>>>(a, q, nq);
-  }} else {{
-    quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 63) / 64, 64, 0, s>>>(a, q, nq);
   }}
 }}
 template <typename R>

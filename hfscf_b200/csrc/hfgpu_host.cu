@@ -270,6 +270,7 @@ int compute_schwarz(hfgpu_handle* h) {
   QuartetArgs<double> qa{};
   qa.jk = jk_args_d(h);
   qa.mode = QMODE_SCHWARZ;
+  qa.warp_max = h->opts.warp_max_quartets;
   qa.pure = h->pure;
   qa.pairs_rw = h->d_pairs.as<PairInfo>();
   for (int c = 0; c < kPairClasses; ++c) {
@@ -456,6 +457,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   qf.jk.DJ = DJ; qf.jk.nK = nK; qf.jk.DK = DK; qf.jk.Jh = Jh; qf.jk.Kh = Kh; qf.jk.dmax = dmax;
   qf.jk.dtol = h->opts.density_tol; qf.jk.counters = h->d_counters.as<unsigned long long>();
   qd.mode = qf.mode = QMODE_JK;
+  qd.warp_max = qf.warp_max = h->opts.warp_max_quartets;
   qd.pure = qf.pure = h->pure;
   const int2* q = h->d_quart.as<int2>();
   long long launched = 0;
@@ -659,6 +661,7 @@ int hfgpu_default_opts(hfgpu_opts* o) {
   o->density_tol = 1e-12;
   o->mixed_fp32_bound = 1e-4;
   o->device = 0;
+  o->warp_max_quartets = 16384;
   return HFGPU_OK;
 }
 
@@ -806,6 +809,7 @@ int hfgpu_eri_packed(hfgpu_handle* h, double* eri_out, long long eri_len) {
   QuartetArgs<double> qa{};
   qa.jk = jk_args_d(h);
   qa.mode = QMODE_PACKED;
+  qa.warp_max = h->opts.warp_max_quartets;
   qa.pure = h->pure;
   qa.eri = h->d_eri.as<double>();
   for (int cp = 0; cp < kPairClasses; ++cp)

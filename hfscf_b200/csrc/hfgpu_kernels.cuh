@@ -206,6 +206,7 @@ struct QuartetArgs {
   int pure;
   double* eri;          // PACKED output
   PairInfo* pairs_rw;   // SCHWARZ output
+  int warp_max;         // large classes: warp per quartet up to this many quartets
 };
 
 template <int LA, int LB, int LC, int LD, typename R>

@@ -42,7 +42,7 @@ class _Basis(ctypes.Structure):
 class _Opts(ctypes.Structure):
     _fields_ = [("schwarz_tol", ctypes.c_double), ("density_tol", ctypes.c_double),
                 ("mixed_fp32_bound", ctypes.c_double), ("device", ctypes.c_int),
-                ("reserved", ctypes.c_int * 7)]
+                ("warp_max_quartets", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
 def lib():
@@ -90,13 +90,16 @@ class _BasisView:
 class Engine:
     """One engine handle: a basis on one GPU, with the current geometry."""
 
-    def __init__(self, basis: Basis, schwarz_tol=1e-12, density_tol=1e-12, mixed_fp32_bound=1e-4, device=0):
+    def __init__(self, basis: Basis, schwarz_tol=1e-12, density_tol=1e-12, mixed_fp32_bound=1e-4, device=0,
+                 warp_max_quartets=None):
         self.basis = basis
         self.n = basis.nbf
         self._bv = _BasisView(basis)
         o = _Opts()
         lib().hfgpu_default_opts(ctypes.byref(o))
         o.schwarz_tol, o.density_tol, o.mixed_fp32_bound, o.device = schwarz_tol, density_tol, mixed_fp32_bound, device
+        if warp_max_quartets is not None:
+            o.warp_max_quartets = warp_max_quartets
         self._opts = o
         h = ctypes.c_void_p()
         self._check(lib().hfgpu_create(ctypes.byref(self._bv.s), ctypes.byref(o), ctypes.byref(h)), None)

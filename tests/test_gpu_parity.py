@@ -89,6 +89,23 @@ def test_jk_and_fock_match_oracle(name, bs):
     assert np.max(np.abs(Fa - Fa0)) < MAT_TOL and np.max(np.abs(Fb - Fb0)) < MAT_TOL
 
 
+@pytest.mark.parametrize("warp_max", [-1, 1 << 30], ids=["thread-per-quartet", "warp-per-quartet"])
+@pytest.mark.parametrize("idx", [0, 4], ids=["h2o-631gss-cart", "ch4-ccpvdz-pure"])
+def test_large_classes_both_kernel_forms_match_oracle(warp_max, idx):
+    """The large classes have a thread-per-quartet and a warp-per-quartet kernel;
+    each is forced in turn and checked (ERIs, J, K)."""
+    name, bs = SMALL[idx]
+    rng = np.random.default_rng(17)
+    D = _sym(rng, bs.nbf)
+    eri0 = oracle.eri_packed(bs)
+    J0, K0 = oracle.jk(eri0, D)
+    with E.Engine(bs, density_tol=0.0, warp_max_quartets=warp_max) as eng:
+        eri = eng.eri_packed()
+        J, K = eng.jk(D, [D])
+    assert np.max(np.abs(eri - eri0)) < ERI_TOL
+    assert np.max(np.abs(J - J0)) < MAT_TOL and np.max(np.abs(K[0] - K0)) < MAT_TOL
+
+
 def test_density_screened_jk_stays_within_threshold():
     bs = SMALL[0][1]
     rng = np.random.default_rng(3)
