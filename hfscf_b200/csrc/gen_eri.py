@@ -257,6 +257,9 @@ def ncart(L):
     return (L + 1) * (L + 2) // 2
 
 
+UNROLL2_MAX_VRR = 50
+
+
 def gen_eri_class(la, lb, lc, ld):
     """Device function computing the contracted Cartesian block of class (la lb|lc ld)."""
     L = la + lb + lc + ld
@@ -290,6 +293,9 @@ def gen_eri_class(la, lb, lc, ld):
     s.append("  for (int ib = 0; ib < nbp; ++ib) {")
     s.append("    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
     s.append("    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;")
+    if len(vrr.memo) <= UNROLL2_MAX_VRR:
+        # small classes: two primitive quartets in flight hide the load latency
+        s.append("#pragma unroll 2")
     s.append("    for (int ik = 0; ik < nkp; ++ik) {")
     s.append("      const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
     s.append("      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;")
