@@ -258,6 +258,52 @@ def ncart(L):
 
 
 UNROLL2_MAX_VRR = 50
+PRIMWARP_MAX_VRR = 150   # classes that also get a warp-over-primitives variant
+
+
+def gen_eri_primwarp(la, lb, lc, ld):
+    """Same integral block as gen_eri_class, for one warp: the lanes split the
+    primitive quartets, then the accumulators are summed with warp shuffles and
+    every lane runs the HRR (the block is valid in all lanes)."""
+    L = la + lb + lc + ld
+    em = Emitter("    ")
+    vrr = VRR(em)
+    targets = vrr_targets(la, la + lb, lc, lc + ld)
+    names = [vrr.get(e, f, 0) for e, f in targets]
+    prim_body = list(em.lines)
+    acc_index = {t: n for n, t in enumerate(targets)}
+    em2 = Emitter("  ")
+    hrr = HRR(em2, lambda e, f: f"acc[{acc_index[(e, f)]}]")
+    outs = [hrr.bra(a, b, c, d) for a in cart(la) for b in cart(lb) for c in cart(lc) for d in cart(ld)]
+    nt = len(targets)
+    s = [f"template <typename R>",
+         f"__device__ __forceinline__ void eri_{la}{lb}{lc}{ld}_pw(const PrimPair<R>* __restrict__ bp, int nbp, "
+         f"const PrimPair<R>* __restrict__ kp, int nkp, R ABx, R ABy, R ABz, R CDx, R CDy, R CDz, "
+         f"const BoysTable<R>& boys, R* __restrict__ out, int lane) {{",
+         f"  R acc[{nt}];", "#pragma unroll", f"  for (int t = 0; t < {nt}; ++t) acc[t] = R(0);",
+         "  const int npq = nbp * nkp;",
+         "  for (int x = lane; x < npq; x += 32) {",
+         "    const int ib = x / nkp, ik = x - ib * nkp;",
+         "    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;",
+         "    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;",
+         "    const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;",
+         "    const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;"]
+    s.append("\n".join("  " + l[6:] if l.startswith("      ") else l for l in PRIM_HEADER.rstrip("\n").split("\n")))
+    s.append(f"    R F[{L + 1}];")
+    s.append(f"    boys.template eval<{L}>(T, pre, F);")
+    s += prim_body
+    for t, nme in enumerate(names):
+        s.append(f"    acc[{t}] += {nme};")
+    s.append("  }")
+    s.append("#pragma unroll")
+    s.append(f"  for (int t = 0; t < {nt}; ++t)")
+    s.append("#pragma unroll")
+    s.append("    for (int off = 16; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);")
+    s += em2.lines
+    for o, nme in enumerate(outs):
+        s.append(f"  out[{o}] = {nme};")
+    s.append("}")
+    return "\n".join(s)
 
 
 def gen_eri_class(la, lb, lc, ld):
@@ -617,6 +663,10 @@ def class_header(c):
     warp = m["vrr_values"] >= WARP_MIN_VRR
     m["warp"] = warp
     parts += [code, ""]
+    primwarp = m["vrr_values"] <= PRIMWARP_MAX_VRR
+    m["primwarp"] = primwarp
+    if primwarp:
+        parts += [gen_eri_primwarp(*c), ""]
     if warp:
         wcode, wm = gen_warp_class(*c)
         parts += [wcode, ""]
@@ -638,6 +688,12 @@ def class_header(c):
     parts.append(f"  static constexpr bool kWarp = {'true' if warp else 'false'};")
     parts.append(f"  using WarpTab = {'WarpTab' + t if warp else 'void'};")
     parts.append(f"  using GradTab = {'void' if straight else 'GradTable' + t};")
+    parts.append(f"  static constexpr bool kPrimWarp = {'true' if primwarp else 'false'};")
+    if primwarp:
+        parts.append(f"  template <typename R>")
+        parts.append(f"  static __device__ __forceinline__ void eri_pw({class_args_sig()}, int lane) {{")
+        parts.append(f"    eri_{t}_pw<R>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out, lane);")
+        parts.append("  }")
     parts.append(f"  template <typename R>")
     parts.append(f"  static __device__ __forceinline__ void eri({class_args_sig()}) {{")
     parts.append(f"    eri_{t}<R>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out);")
@@ -684,6 +740,20 @@ static void launch_quartet(const QuartetArgs<R>& a, const int2* q, int nq, cudaS
   if (nq <= 0) return;
   launch_quartet_impl<ClassCode<{la}, {lb}, {lc}, {ld}>, R>(a, q, nq, s);
 }}
+template <typename CC, typename R>
+static bool launch_primwarp_impl(const QuartetArgs<R>& a, const int2* q, int nq, cudaStream_t s) {{
+  if constexpr (CC::kPrimWarp) {{
+    quartet_primwarp_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 3) / 4, 128, 0, s>>>(a, q, nq);
+    return true;
+  }} else {{
+    return false;
+  }}
+}}
+template <typename R>
+static bool launch_primwarp(const QuartetArgs<R>& a, const int2* q, int nq, cudaStream_t s) {{
+  if (nq <= 0) return true;
+  return launch_primwarp_impl<ClassCode<{la}, {lb}, {lc}, {ld}>, R>(a, q, nq, s);
+}}
 template <typename R>
 static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, int grid, cudaStream_t s) {{
   if (nq <= 0) return;
@@ -703,7 +773,9 @@ static int grad_scratch_slots(int) {{
 }}
 extern const ClassLaunchers launchers_{t};
 const ClassLaunchers launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_quartet<double>, &launch_quartet<float>,
-                                      &launch_grad<double>, &launch_grad<float>, &grad_scratch_slots}};
+                                      &launch_grad<double>, &launch_grad<float>, &grad_scratch_slots,
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kPrimWarp,
+                                      &launch_primwarp<double>, &launch_primwarp<float>}};
 }}  // namespace hfgpu
 """
 

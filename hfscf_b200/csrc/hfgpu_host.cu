@@ -82,8 +82,10 @@ struct hfgpu_handle {
   int class_begin[kPairClasses + 1] = {0};
   int nprimpairs = 0;
 
-  // quartet lists per class: [beg, mid) high bound (FP64 always), [mid, end) low bound
-  std::vector<long long> q_beg, q_mid, q_end;
+  // quartet lists per class: [beg, mid) high bound (FP64 always), [mid, end) low bound;
+  // inside each part the quartets with many primitive quartets come first:
+  // [beg, hik1) and [mid, hik2) run the warp-over-primitives kernel where the class has one
+  std::vector<long long> q_beg, q_mid, q_end, q_hik1, q_hik2;
   long long nquartets = 0;
 
   DevBuf d_pairs, d_prim_d, d_prim_f, d_alpha_d, d_alpha_f, d_boys_d, d_boys_f, d_quart;
@@ -98,7 +100,7 @@ struct hfgpu_handle {
   cudaEvent_t ev[2 * 21 + 2] = {};
   bool ev_used[21] = {};
 
-  hfgpu_handle() : q_beg(21), q_mid(21), q_end(21) {}
+  hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21) {}
 };
 
 namespace {
@@ -287,33 +289,39 @@ int compute_schwarz(hfgpu_handle* h) {
   return HFGPU_OK;
 }
 
+constexpr int kPrimWarpMinPrims = 64;  // primitive quartets per quartet for the warp-over-primitives kernel
+
 // Screened unique quartets (P <= Q within a class; bra class >= ket class), per class.
 int build_quartets(hfgpu_handle* h) {
   const double tol = h->opts.schwarz_tol, mix = h->opts.mixed_fp32_bound;
   std::vector<int2> all;
-  std::vector<int2> low;
+  std::vector<int2> parts[4];  // high bound many-prim, high bound few-prim, low bound many, low bound few
   h->nquartets = 0;
   for (int cp = 0; cp < kPairClasses; ++cp)
     for (int cq = 0; cq <= cp; ++cq) {
       const int qc = quartet_class(cp, cq);
-      low.clear();
-      h->q_beg[qc] = (long long)all.size();
+      for (auto& v : parts) v.clear();
       const int pb = h->class_begin[cp], pe = h->class_begin[cp + 1];
       const int kb = h->class_begin[cq], ke = h->class_begin[cq + 1];
       for (int P = pb; P < pe; ++P) {
         const double qp = h->pairs[P].schwarz;
+        const int np = h->pairs[P].nprim;
         const int k0 = (cp == cq) ? P : kb;
         for (int Q = k0; Q < ke; ++Q) {
           const double b = qp * h->pairs[Q].schwarz;
           if (b < tol) continue;
-          if (b >= mix)
-            all.push_back(make_int2(P, Q));
-          else
-            low.push_back(make_int2(P, Q));
+          const bool many = np * h->pairs[Q].nprim >= kPrimWarpMinPrims;
+          parts[(b >= mix ? 0 : 2) + (many ? 0 : 1)].push_back(make_int2(P, Q));
         }
       }
+      h->q_beg[qc] = (long long)all.size();
+      all.insert(all.end(), parts[0].begin(), parts[0].end());
+      h->q_hik1[qc] = (long long)all.size();
+      all.insert(all.end(), parts[1].begin(), parts[1].end());
       h->q_mid[qc] = (long long)all.size();
-      all.insert(all.end(), low.begin(), low.end());
+      all.insert(all.end(), parts[2].begin(), parts[2].end());
+      h->q_hik2[qc] = (long long)all.size();
+      all.insert(all.end(), parts[3].begin(), parts[3].end());
       h->q_end[qc] = (long long)all.size();
     }
   h->nquartets = (long long)all.size();
@@ -477,11 +485,20 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     h->ev_used[c] = false;
     if (e <= b) continue;
     if (h->timing) HF_CUDA(h, cudaEventRecord(h->ev[2 * c], st));
-    if (precision == HFGPU_MIXED) {
-      if (m > b) { L->quartet_d(qd, q + b, (int)(m - b), st); ++kernels; }
-      if (e > m) { L->quartet_f(qf, q + m, (int)(e - m), st); ++kernels; }
-    } else {
-      L->quartet_d(qd, q + b, (int)(e - b), st);
+    const long long h1 = h->q_hik1[c], h2 = h->q_hik2[c];
+    // four segments: [b,h1) [h1,m) high bound, [m,h2) [h2,e) low bound; many-primitive first
+    const long long seg[5] = {b, h1, m, h2, e};
+    for (int sg = 0; sg < 4; ++sg) {
+      const int nseg = (int)(seg[sg + 1] - seg[sg]);
+      if (nseg <= 0) continue;
+      const bool fp32 = precision == HFGPU_MIXED && sg >= 2;
+      const bool many = (sg % 2) == 0 && L->has_primwarp;
+      const int2* qs = q + seg[sg];
+      if (fp32) {
+        if (!(many && L->primwarp_f(qf, qs, nseg, st))) L->quartet_f(qf, qs, nseg, st);
+      } else {
+        if (!(many && L->primwarp_d(qd, qs, nseg, st))) L->quartet_d(qd, qs, nseg, st);
+      }
       ++kernels;
     }
     HF_CHECK_LAUNCH(h, "quartet kernel");

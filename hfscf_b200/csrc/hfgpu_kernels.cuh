@@ -258,6 +258,55 @@ __global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const i
   }
 }
 
+// One warp per quartet of a small class with many primitive quartets: the lanes
+// split the primitive quartets (consecutive ket primitives, one bra primitive per
+// lane group: coalesced and broadcast loads), the accumulators are reduced with
+// shuffles, and lane 0 transforms and digests the block.
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(128) quartet_primwarp_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets,
+                                                               int nq) {
+  const JKArgs<R>& a = qa.jk;
+  const int lane = threadIdx.x & 31;
+  const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (qi >= nq) return;  // whole warp
+  const int2 pq = quartets[qi];
+  const PairInfo P = a.pairs[pq.x];
+  const PairInfo Q = a.pairs[pq.y];
+  bool skip = false;
+  if (qa.mode == QMODE_JK && a.dmax != nullptr) {
+    const float* dm = a.dmax;
+    const int ns = a.nshell;
+    float m = 4.f * fmaxf(dm[P.sa * ns + P.sb], dm[Q.sa * ns + Q.sb]);
+    m = fmaxf(m, fmaxf(fmaxf(dm[P.sa * ns + Q.sa], dm[P.sa * ns + Q.sb]), fmaxf(dm[P.sb * ns + Q.sa], dm[P.sb * ns + Q.sb])));
+    skip = P.schwarz * Q.schwarz * double(m) < a.dtol;
+  }
+  if (a.counters != nullptr && lane == 0) {
+    atomicAdd(a.counters + (skip ? 1 : 0), 1ull);
+    if (!skip) atomicAdd(a.counters + 2, (unsigned long long)(P.nprim * Q.nprim));
+  }
+  if (skip) return;
+  using Dc = BlockDims<LA, LB, LC, LD, false>;
+  R cart[Dc::NCART];
+  ClassCode<LA, LB, LC, LD>::template eri_pw<R>(a.prims + P.prim_off, P.nprim, a.prims + Q.prim_off, Q.nprim,
+                                                 R(P.ABx), R(P.ABy), R(P.ABz), R(Q.ABx), R(Q.ABy), R(Q.ABz), a.boys,
+                                                 cart, lane);
+  if (lane != 0) return;
+  double s = 1.0;
+  if (P.sa == P.sb) s *= 0.5;
+  if (Q.sa == Q.sb) s *= 0.5;
+  if (pq.x == pq.y) s *= 0.5;
+  if (qa.pure) {
+    using Dp = BlockDims<LA, LB, LC, LD, true>;
+    double V[Dp::NOUT];
+    finish_block<LA, LB, LC, LD, R, true>(cart, V);
+    use_block<LA, LB, LC, LD, true>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri, qa.pairs_rw);
+  } else {
+    double V[Dc::NOUT];
+    finish_block<LA, LB, LC, LD, R, false>(cart, V);
+    use_block<LA, LB, LC, LD, false>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri, qa.pairs_rw);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Adjoint gradient.
 // ---------------------------------------------------------------------------

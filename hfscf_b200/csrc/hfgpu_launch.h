@@ -16,6 +16,9 @@ struct ClassLaunchers {
   void (*grad_d)(const GradArgs<double>&, int pure, const int2*, int, int grid, cudaStream_t);
   void (*grad_f)(const GradArgs<float>&, int pure, const int2*, int, int grid, cudaStream_t);
   int (*grad_scratch_slots)(int pure);  // per-thread scratch of table-mode gradient classes (0 otherwise)
+  bool has_primwarp;                     // warp-over-primitives kernel for high-contraction quartets
+  bool (*primwarp_d)(const QuartetArgs<double>&, const int2*, int, cudaStream_t);
+  bool (*primwarp_f)(const QuartetArgs<float>&, const int2*, int, cudaStream_t);
 };
 
 extern const ClassLaunchers* const kClassLaunchers[];
