@@ -289,7 +289,7 @@ int compute_schwarz(hfgpu_handle* h) {
   return HFGPU_OK;
 }
 
-constexpr int kPrimWarpMinPrims = 64;  // primitive quartets per quartet for the warp-over-primitives kernel
+constexpr int kPrimWarpMinPrims = 32;  // primitive quartets per quartet for the warp-over-primitives kernel
 
 // Screened unique quartets (P <= Q within a class; bra class >= ket class), per class.
 int build_quartets(hfgpu_handle* h) {
@@ -487,7 +487,8 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     if (h->timing) HF_CUDA(h, cudaEventRecord(h->ev[2 * c], st));
     const long long h1 = h->q_hik1[c], h2 = h->q_hik2[c];
     // four segments: [b,h1) [h1,m) high bound, [m,h2) [h2,e) low bound; many-primitive first
-    const long long seg[5] = {b, h1, m, h2, e};
+    // classes without the warp-over-primitives kernel launch each precision part whole
+    const long long seg[5] = {b, L->has_primwarp ? h1 : b, m, L->has_primwarp ? h2 : m, e};
     for (int sg = 0; sg < 4; ++sg) {
       const int nseg = (int)(seg[sg + 1] - seg[sg]);
       if (nseg <= 0) continue;

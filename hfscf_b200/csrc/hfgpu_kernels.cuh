@@ -61,10 +61,12 @@ __device__ __forceinline__ void load_block(const double* __restrict__ D, int n, 
 // J/K digestion of one block V[a][b][c][d] (final basis), scaled by the quartet's
 // degeneracy s: Jh_ab += 2s sum_cd D_cd V, Jh_cd += 2s sum_ab D_ab V,
 // Kh_ac += s sum_bd D_bd V, Kh_ad += s D_bc V, Kh_bc += s D_ad V, Kh_bd += s D_ac V.
+// coop: all 32 lanes of the warp call this with valid quartets of the same bra pair.
 template <int NA, int NB, int NC, int ND>
 __device__ __forceinline__ void digest_jk(const double* V, int fa, int fb, int fc, int fd, double s,
                                           const double* __restrict__ DJ,
-                                          int nK, const double* __restrict__ DK, double* Jh, double* Kh, int n) {
+                                          int nK, const double* __restrict__ DK, double* Jh, double* Kh, int n,
+                                          bool coop = false) {
   constexpr int NV = NA * NB * NC * ND;
   constexpr bool SMALL = NV <= 81;
   if (DJ != nullptr) {
@@ -84,7 +86,15 @@ __device__ __forceinline__ void digest_jk(const double* V, int fa, int fb, int f
         jab += dcd[cd] * v;
         jcd[cd] += dv * v;
       }
-      atomicAdd(Jh + (size_t)(fa + ab / NB) * n + fb + ab % NB, 2.0 * s * jab);
+      if (coop) {
+        // the whole warp shares this bra pair: one atomic per J_ab element
+        double v = 2.0 * s * jab;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if ((threadIdx.x & 31) == 0) atomicAdd(Jh + (size_t)(fa + ab / NB) * n + fb + ab % NB, v);
+      } else {
+        atomicAdd(Jh + (size_t)(fa + ab / NB) * n + fb + ab % NB, 2.0 * s * jab);
+      }
     }
 #pragma unroll
     for (int cd = 0; cd < NC * ND; ++cd) atomicAdd(Jh + (size_t)(fc + cd / ND) * n + fd + cd % ND, 2.0 * s * jcd[cd]);
@@ -181,10 +191,10 @@ template <int LA, int LB, int LC, int LD, bool PURE>
 __device__ __forceinline__ void use_block(const double* V, int mode, const int2 pq, const PairInfo& P,
                                           const PairInfo& Q, double s, const double* __restrict__ DJ, int nK,
                                           const double* __restrict__ DK, double* Jh, double* Kh, int n, double* eri,
-                                          PairInfo* pairs_rw) {
+                                          PairInfo* pairs_rw, bool coop = false) {
   using Dm = BlockDims<LA, LB, LC, LD, PURE>;
   if (mode == QMODE_JK) {
-    digest_jk<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(V, P.fa, P.fb, Q.fa, Q.fb, s, DJ, nK, DK, Jh, Kh, n);
+    digest_jk<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(V, P.fa, P.fb, Q.fa, Q.fb, s, DJ, nK, DK, Jh, Kh, n, coop);
   } else if (mode == QMODE_PACKED) {
     for (int i = 0; i < Dm::NA; ++i)
       for (int j = 0; j < Dm::NB; ++j)
@@ -213,12 +223,14 @@ template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets, int nq) {
   const JKArgs<R>& a = qa.jk;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nq) return;
-  const int2 pq = quartets[t];
+  // every lane stays to the end (lanes without work carry valid = false), so
+  // that the digestion can use whole-warp shuffles
+  const bool in_range = t < nq;
+  const int2 pq = in_range ? quartets[t] : make_int2(0, 0);
   const PairInfo P = a.pairs[pq.x];
   const PairInfo Q = a.pairs[pq.y];
-  bool skip = false;
-  if (qa.mode == QMODE_JK && a.dmax != nullptr) {
+  bool skip = !in_range;
+  if (in_range && qa.mode == QMODE_JK && a.dmax != nullptr) {
     // density-weighted Schwarz bound: Q_ab Q_cd max(4|D_ab|, 4|D_cd|, |D_ac|, |D_ad|, |D_bc|, |D_bd|)
     const float* dm = a.dmax;
     const int ns = a.nshell;
@@ -226,22 +238,25 @@ __global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const i
     m = fmaxf(m, fmaxf(fmaxf(dm[P.sa * ns + Q.sa], dm[P.sa * ns + Q.sb]), fmaxf(dm[P.sb * ns + Q.sa], dm[P.sb * ns + Q.sb])));
     skip = P.schwarz * Q.schwarz * double(m) < a.dtol;
   }
+  const bool valid = !skip;
   if (a.counters != nullptr) {
     // per-class work counters, one atomic per warp: [0] quartets computed,
     // [1] quartets skipped by the density bound, [2] primitive quartets computed
-    const unsigned mask = __activemask();
-    const unsigned nskip = __popc(__ballot_sync(mask, skip));
-    const unsigned prims = __reduce_add_sync(mask, skip ? 0u : unsigned(P.nprim * Q.nprim));
-    if ((threadIdx.x & 31) == __ffs(mask) - 1) {
-      atomicAdd(a.counters + 0, (unsigned long long)(__popc(mask) - nskip));
-      atomicAdd(a.counters + 1, (unsigned long long)nskip);
+    const unsigned nvalid = __popc(__ballot_sync(0xffffffffu, valid));
+    const unsigned nin = __popc(__ballot_sync(0xffffffffu, in_range));
+    const unsigned prims = __reduce_add_sync(0xffffffffu, valid ? unsigned(P.nprim * Q.nprim) : 0u);
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(a.counters + 0, (unsigned long long)nvalid);
+      atomicAdd(a.counters + 1, (unsigned long long)(nin - nvalid));
       atomicAdd(a.counters + 2, (unsigned long long)prims);
     }
   }
-  if (skip) return;
+  if (!__any_sync(0xffffffffu, valid)) return;  // whole warp leaves together
+  // J_ab contributions can be summed across the warp when every lane works on the same bra pair
+  const bool coop = qa.mode == QMODE_JK && __all_sync(0xffffffffu, valid && pq.x == __shfl_sync(0xffffffffu, pq.x, 0));
   using Dc = BlockDims<LA, LB, LC, LD, false>;
   R cart[Dc::NCART];
-  cart_block<LA, LB, LC, LD, R>(P, Q, a.prims, a.boys, cart);
+  if (valid) cart_block<LA, LB, LC, LD, R>(P, Q, a.prims, a.boys, cart);
   double s = 1.0;
   if (P.sa == P.sb) s *= 0.5;
   if (Q.sa == Q.sb) s *= 0.5;
@@ -249,12 +264,16 @@ __global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const i
   if (qa.pure) {
     using Dp = BlockDims<LA, LB, LC, LD, true>;
     double V[Dp::NOUT];
-    finish_block<LA, LB, LC, LD, R, true>(cart, V);
-    use_block<LA, LB, LC, LD, true>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri, qa.pairs_rw);
+    if (valid) finish_block<LA, LB, LC, LD, R, true>(cart, V);
+    if (valid || coop)
+      use_block<LA, LB, LC, LD, true>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri,
+                                      qa.pairs_rw, coop);
   } else {
     double V[Dc::NOUT];
-    finish_block<LA, LB, LC, LD, R, false>(cart, V);
-    use_block<LA, LB, LC, LD, false>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri, qa.pairs_rw);
+    if (valid) finish_block<LA, LB, LC, LD, R, false>(cart, V);
+    if (valid || coop)
+      use_block<LA, LB, LC, LD, false>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri,
+                                       qa.pairs_rw, coop);
   }
 }
 
