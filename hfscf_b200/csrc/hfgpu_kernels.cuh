@@ -252,8 +252,12 @@ __global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const i
     }
   }
   if (!__any_sync(0xffffffffu, valid)) return;  // whole warp leaves together
-  // J_ab contributions can be summed across the warp when every lane works on the same bra pair
-  const bool coop = qa.mode == QMODE_JK && __all_sync(0xffffffffu, valid && pq.x == __shfl_sync(0xffffffffu, pq.x, 0));
+  // J_ab contributions can be summed across the warp when every lane works on the same bra pair.
+  // The shuffle is taken by all 32 lanes before any predicate (a shuffle skipped by some
+  // lanes, e.g. through && short-circuiting, would leave the others waiting).
+  const int px0 = __shfl_sync(0xffffffffu, pq.x, 0);
+  const bool same_bra = valid && pq.x == px0;
+  const bool coop = __all_sync(0xffffffffu, same_bra) && qa.mode == QMODE_JK;
   using Dc = BlockDims<LA, LB, LC, LD, false>;
   R cart[Dc::NCART];
   if (valid) cart_block<LA, LB, LC, LD, R>(P, Q, a.prims, a.boys, cart);
