@@ -652,7 +652,7 @@ def common_header():
     return "\n".join(out) + "\n"
 
 
-WARP_MIN_VRR = 270   # energy classes with at least this many VRR values run one warp per quartet
+WARP_MIN_VRR = 1000  # (dd|dp) and (dd|dd): measured faster as one warp per quartet than one thread
 
 
 def class_header(c):

@@ -488,7 +488,10 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     const long long h1 = h->q_hik1[c], h2 = h->q_hik2[c];
     // four segments: [b,h1) [h1,m) high bound, [m,h2) [h2,e) low bound; many-primitive first
     // classes without the warp-over-primitives kernel launch each precision part whole
-    const long long seg[5] = {b, L->has_primwarp ? h1 : b, m, L->has_primwarp ? h2 : m, e};
+    // (in FP64 both parts as one launch)
+    const bool mixed = precision == HFGPU_MIXED;
+    const long long seg[5] = {b, L->has_primwarp ? h1 : b, (L->has_primwarp || mixed) ? m : e,
+                              L->has_primwarp ? h2 : ((L->has_primwarp || mixed) ? m : e), e};
     for (int sg = 0; sg < 4; ++sg) {
       const int nseg = (int)(seg[sg + 1] - seg[sg]);
       if (nseg <= 0) continue;
@@ -679,7 +682,7 @@ int hfgpu_default_opts(hfgpu_opts* o) {
   o->density_tol = 1e-12;
   o->mixed_fp32_bound = 1e-4;
   o->device = 0;
-  o->warp_max_quartets = 16384;
+  o->warp_max_quartets = 1 << 30;
   return HFGPU_OK;
 }
 

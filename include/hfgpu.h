@@ -62,8 +62,8 @@ typedef struct {
   double density_tol;      /* J/K: skip quartets whose density-weighted bound is below this (default 1e-12; 0 = off) */
   double mixed_fp32_bound; /* mixed precision: quartets with Q_ab Q_cd below this run in FP32 (default 1e-4) */
   int device;              /* CUDA device ordinal (default 0) */
-  int warp_max_quartets;   /* large classes run one warp per quartet when they have at most this many
-                              quartets, one thread per quartet otherwise (default 16384; -1 = never) */
+  int warp_max_quartets;   /* (dd|dp), (dd|dd): one warp per quartet when the class has at most this many
+                              quartets, one thread per quartet otherwise (default 2^30 = always; -1 = never) */
   int reserved[6];
 } hfgpu_opts;
 
