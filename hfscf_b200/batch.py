@@ -1,0 +1,250 @@
+"""Batched RHF: hundreds of small molecules solved together on one GPU.
+
+One batched engine handle holds every molecule (hfgpu_batch_create).  Each SCF
+iteration is one J/K build for all molecules at once -- the per-class kernels
+cover every molecule's quartets -- and the N x N work (orthogonalisation,
+DIIS, diagonalisation) runs batched on the GPU in torch over matrices padded to
+the largest molecule.  The J/K build and the Fock assembly can be captured once
+as a CUDA graph and replayed every iteration.  After convergence, the
+two-electron gradient of every molecule comes from one batched adjoint launch
+(hfgpu_batch_grad2e_device); one-electron and nuclear terms are added per
+molecule on the host.
+
+The SCF is the caller side, as in scf.py: symmetric orthogonalisation, D =
+C_occ C_occ^T (no factor 2), E = sum D (H + F), DIIS on the orthogonalised
+commutator.  Here DIIS keeps the last 6 vectors per molecule.
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import engine as eng
+from .basis import Basis, build_basis, nuclear_repulsion, nuclear_repulsion_gradient
+
+PAD_DIAG = 1.0e3  # padded diagonal of F: far above every occupied orbital energy
+
+
+class BatchEngine:
+    """A batched engine handle over many Cartesian molecules."""
+
+    def __init__(self, bases: list[Basis], device: int = 0, schwarz_tol: float = 1e-12):
+        self.bases = bases
+        self.nmol = len(bases)
+        self._views = [eng._BasisView(b) for b in bases]
+        arr = (eng._Basis * self.nmol)(*[v.s for v in self._views])
+        self._xyz = [np.ascontiguousarray(b.coords, dtype=np.float64) for b in bases]
+        ptrs = (ctypes.POINTER(ctypes.c_double) * self.nmol)(*[eng._p(x) for x in self._xyz])
+        o = eng._Opts()
+        eng.lib().hfgpu_default_opts(ctypes.byref(o))
+        o.schwarz_tol, o.device = schwarz_tol, device
+        h = ctypes.c_void_p()
+        rc = eng.lib().hfgpu_batch_create(ctypes.c_int(self.nmol), arr, ptrs, ctypes.byref(o), ctypes.byref(h))
+        if rc:
+            raise eng.HfgpuError(rc, "hfgpu_batch_create")
+        self.h = h
+        nbf = (ctypes.c_int * self.nmol)()
+        off = (ctypes.c_longlong * self.nmol)()
+        tot = ctypes.c_longlong()
+        eng.lib().hfgpu_batch_layout(h, nbf, off, ctypes.byref(tot))
+        self.nbf = np.array(list(nbf), dtype=np.int64)
+        self.mat_off = np.array(list(off), dtype=np.int64)
+        self.mat_total = int(tot.value)
+        self.natoms = np.array([b.natoms for b in bases], dtype=np.int64)
+        self.atom_off = np.concatenate([[0], np.cumsum(self.natoms)])
+
+    def _check(self, rc):
+        if rc:
+            raise eng.HfgpuError(rc, eng.lib().hfgpu_last_error(self.h).decode())
+
+    def set_stream(self, stream_ptr):
+        self._check(eng.lib().hfgpu_set_stream(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def jk_device(self, D, J, K, precision=eng.FP64):
+        self._check(eng.lib().hfgpu_batch_jk_device(self.h, ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(J.data_ptr()),
+                                                    ctypes.c_void_p(K.data_ptr()), ctypes.c_int(precision)))
+
+    def grad2e_device(self, D, grad, precision=eng.FP64):
+        self._check(eng.lib().hfgpu_batch_grad2e_device(self.h, ctypes.c_void_p(D.data_ptr()),
+                                                        ctypes.c_void_p(grad.data_ptr()), ctypes.c_int(precision)))
+
+    def close(self):
+        if getattr(self, "h", None) is not None:
+            eng.lib().hfgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Layout:
+    """Index maps between block storage (molecule m: n_m x n_m at mat_off[m]) and
+    padded batched matrices [nmol, nmax, nmax]."""
+
+    def __init__(self, nbf, mat_off, device):
+        self.nmol = len(nbf)
+        self.nmax = int(nbf.max())
+        idx = []
+        for m, (n, off) in enumerate(zip(nbf, mat_off)):
+            i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+            idx.append(m * self.nmax * self.nmax + i.ravel() * self.nmax + j.ravel())
+        self.pad_index = torch.from_numpy(np.concatenate(idx)).to(device)
+        mask = np.zeros((self.nmol, self.nmax), dtype=bool)
+        for m, n in enumerate(nbf):
+            mask[m, :n] = True
+        self.mask = torch.from_numpy(mask).to(device)
+
+    def to_block(self, Mp):
+        return Mp.reshape(-1)[self.pad_index]
+
+    def to_pad(self, Mb, fill_diag=0.0):
+        out = torch.zeros((self.nmol * self.nmax * self.nmax,), dtype=Mb.dtype, device=Mb.device)
+        out[self.pad_index] = Mb
+        out = out.view(self.nmol, self.nmax, self.nmax)
+        if fill_diag:
+            d = torch.diagonal(out, dim1=1, dim2=2)
+            d += (~self.mask).to(out.dtype) * fill_diag
+        return out
+
+
+def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-10, rms_tol=1e-8,
+              max_iter=60, use_graph=True, gradient=True):
+    """Converged RHF energies (and gradients) of every molecule of the batch."""
+    dev = torch.device("cuda", device)
+    t0 = time.perf_counter()
+    be = BatchEngine(bases, device)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    be.set_stream(stream.cuda_stream)
+    lay = _Layout(be.nbf, be.mat_off, dev)
+    nmol, nmax = lay.nmol, lay.nmax
+    # one-electron matrices (host) into block storage
+    Sb, Hb = [], []
+    for b in bases:
+        S, T, V = eng.one_electron(b)
+        Sb.append(S.ravel())
+        Hb.append((T + V).ravel())
+    Sblk = torch.from_numpy(np.concatenate(Sb)).to(dev)
+    Hblk = torch.from_numpy(np.concatenate(Hb)).to(dev)
+    S = lay.to_pad(Sblk, fill_diag=1.0)
+    H = lay.to_pad(Hblk, fill_diag=PAD_DIAG)
+    w, U = torch.linalg.eigh(S)
+    X = (U / torch.sqrt(w).unsqueeze(1)) @ U.transpose(1, 2)
+    nocc = torch.tensor([int(np.sum(b.Z)) // 2 for b in bases], device=dev)
+    occ = (torch.arange(nmax, device=dev).unsqueeze(0) < nocc.unsqueeze(1)).to(torch.float64)
+
+    def density(F):
+        e, Cp = torch.linalg.eigh(X.transpose(1, 2) @ F @ X)
+        C = X @ Cp
+        return (C * occ.unsqueeze(1)) @ C.transpose(1, 2)
+
+    D = density(H)
+    Dblk = lay.to_block(D).contiguous()
+    Jblk = torch.zeros_like(Dblk)
+    Kblk = torch.zeros_like(Dblk)
+    Fblk = torch.zeros_like(Dblk)
+
+    def build():
+        be.jk_device(Dblk, Jblk, Kblk, precision)
+        torch.add(Hblk, Jblk, alpha=2.0, out=Fblk)
+        Fblk.sub_(Kblk)
+
+    build()  # warm-up: loads every kernel before any capture
+    torch.cuda.synchronize()
+    graph = None
+    if use_graph:
+        try:
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=stream):
+                build()
+            torch.cuda.synchronize()
+        except Exception:
+            graph = None
+            torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    hist_F, hist_E = [], []
+    E_prev = torch.zeros(nmol, dtype=torch.float64, device=dev)
+    converged = torch.zeros(nmol, dtype=torch.bool, device=dev)
+    n_per = torch.from_numpy(be.nbf).to(dev).to(torch.float64)
+    it = 0
+    build_times = []
+    t1 = time.perf_counter()
+    while it < max_iter:
+        it += 1
+        Dblk.copy_(lay.to_block(D))
+        ta = time.perf_counter()
+        if graph is not None:
+            graph.replay()
+        else:
+            build()
+        build_times.append(time.perf_counter() - ta)
+        F = lay.to_pad(Fblk, fill_diag=PAD_DIAG)
+        FDS = F @ D @ S
+        err = X.transpose(1, 2) @ (FDS - FDS.transpose(1, 2)) @ X
+        rms = torch.sqrt((err * err).sum(dim=(1, 2)) / (n_per * n_per))
+        hist_F.append(F)
+        hist_E.append(err.reshape(nmol, -1))
+        if len(hist_F) > 6:
+            hist_F.pop(0)
+            hist_E.pop(0)
+        m = len(hist_F)
+        if m > 1:
+            Es = torch.stack(hist_E, dim=1)  # [nmol, m, n*n]
+            B = -torch.ones((nmol, m + 1, m + 1), dtype=torch.float64, device=dev)
+            B[:, :m, :m] = Es @ Es.transpose(1, 2)
+            B[:, m, m] = 0.0
+            rhs = torch.zeros((nmol, m + 1), dtype=torch.float64, device=dev)
+            rhs[:, m] = -1.0
+            c = torch.linalg.solve(B, rhs)[:, :m]
+            F = torch.einsum("bk,bkij->bij", c, torch.stack(hist_F, dim=1))
+        D = density(F)
+        E = ((D * (H + F)).sum(dim=(1, 2)) - PAD_DIAG * 0)  # padded entries of D are zero
+        conv = (rms < rms_tol) & ((E - E_prev).abs() < e_tol)
+        converged |= conv
+        E_prev = E
+        if bool(converged.all()):
+            break
+    torch.cuda.synchronize()
+    t_scf = time.perf_counter() - t1
+    # final Fock matrices at the converged densities
+    Dblk.copy_(lay.to_block(D))
+    build()
+    F = lay.to_pad(Fblk, fill_diag=0.0)
+    Dz = D
+    E_el = (Dz * (lay.to_pad(Hblk) + F)).sum(dim=(1, 2)).cpu().numpy()
+    enuc = np.array([nuclear_repulsion(b.Z, b.coords) for b in bases])
+    out = {"energies": E_el + enuc, "iterations": it, "converged": converged.cpu().numpy(),
+           "setup_s": t_setup, "scf_s": t_scf, "graph": graph is not None,
+           "build_ms_mean": 1e3 * float(np.mean(build_times)), "nmol": nmol}
+    if gradient:
+        t2 = time.perf_counter()
+        g = torch.zeros((int(be.atom_off[-1]), 3), dtype=torch.float64, device=dev)
+        be.grad2e_device(Dblk, g, precision)
+        torch.cuda.synchronize()
+        g2 = g.cpu().numpy()
+        Dn = D.cpu().numpy()
+        Fn = F.cpu().numpy()
+        grads = []
+        for k, b in enumerate(bases):
+            n = b.nbf
+            Dk, Fk = Dn[k, :n, :n], Fn[k, :n, :n]
+            gk = g2[be.atom_off[k]:be.atom_off[k + 1]].copy()
+            gk += eng.one_electron_grad(b, Dk, Dk @ Fk @ Dk, 2.0, -2.0)
+            gk += nuclear_repulsion_gradient(b.Z, b.coords)
+            grads.append(gk)
+        out["gradients"] = grads
+        out["grad_s"] = time.perf_counter() - t2
+    be.close()
+    torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    return out
+
+
+def batch_bases(molecules):
+    """Cartesian bases for (Z, coords_bohr, basis_name, pure) tuples (s/p pure == Cartesian)."""
+    return [build_basis(name, Z, x, pure=False) for Z, x, name, _ in molecules]

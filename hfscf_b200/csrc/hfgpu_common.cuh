@@ -25,7 +25,7 @@ struct PairInfo {
   int nprim;         // primitive pairs kept
   int cls;           // pair class: 0 ss, 1 ps, 2 pp, 3 ds, 4 dp, 5 dd
   int atom_a, atom_b;
-  int pad;
+  int mol;           // molecule of a batched handle (0 otherwise); fa, fb are local to it
   double ABx, ABy, ABz;  // A - B
   double schwarz;        // sqrt(max |(ab|ab)|) over the pair's functions
 };

@@ -77,9 +77,19 @@ struct hfgpu_handle {
   bool own_stream = false;
   std::string err;
 
-  // pair data (host mirror) and class ranges
+  // batched handles: several molecules; shells of molecule m are [mol_shell[m], mol_shell[m+1]),
+  // its matrices the n_m x n_m block at mol_off[m] of the block storage (mat_total doubles)
+  int nmol = 1;
+  bool batched = false;
+  std::vector<int> mol_shell, mol_n, mol_atom;
+  std::vector<long long> mol_off;
+  long long mat_total = 0;
+  DevBuf d_mol;
+
+  // pair data (host mirror) and class ranges; cm_begin[c * (nmol+1) + m]: first pair of class c, molecule m
   std::vector<PairInfo> pairs;
   int class_begin[kPairClasses + 1] = {0};
+  std::vector<int> cm_begin;
   int nprimpairs = 0;
 
   // quartet lists per class: [beg, mid) high bound (FP64 always), [mid, end) low bound;
@@ -147,22 +157,32 @@ int set_device(hfgpu_handle* h) {
 // Primitive pairs of every canonical shell pair; pairs sorted by class, then by
 // primitive count (descending) so that quartet lists group equal loop lengths.
 int build_pairs(hfgpu_handle* h) {
-  const int ns = h->nshell;
   struct Tmp {
-    int sa, sb, cls, np;
+    int sa, sb, cls, np, mol;
   };
   std::vector<Tmp> tmp;
-  tmp.reserve((size_t)ns * (ns + 1) / 2);
-  for (int i = 0; i < ns; ++i)
-    for (int j = i; j < ns; ++j) {
-      int sa = i, sb = j;
-      if (h->L[sa] < h->L[sb]) std::swap(sa, sb);
-      tmp.push_back({sa, sb, pair_class(h->L[sa], h->L[sb]), h->nprim[sa] * h->nprim[sb]});
-    }
+  for (int m = 0; m < h->nmol; ++m)
+    for (int i = h->mol_shell[m]; i < h->mol_shell[m + 1]; ++i)
+      for (int j = i; j < h->mol_shell[m + 1]; ++j) {
+        int sa = i, sb = j;
+        if (h->L[sa] < h->L[sb]) std::swap(sa, sb);
+        tmp.push_back({sa, sb, pair_class(h->L[sa], h->L[sb]), h->nprim[sa] * h->nprim[sb], m});
+      }
   std::stable_sort(tmp.begin(), tmp.end(), [](const Tmp& x, const Tmp& y) {
     if (x.cls != y.cls) return x.cls < y.cls;
+    if (x.mol != y.mol) return x.mol < y.mol;
     return x.np > y.np;
   });
+  const int nm1 = h->nmol + 1;
+  h->cm_begin.assign((size_t)kPairClasses * nm1, 0);
+  for (int c = 0; c < kPairClasses; ++c)
+    for (int m = 0; m <= h->nmol; ++m) {
+      // first pair at or after (class c, molecule m) in the (class, molecule) order
+      const auto it = std::lower_bound(tmp.begin(), tmp.end(), std::make_pair(c, m), [](const Tmp& x, const std::pair<int, int>& k) {
+        return x.cls < k.first || (x.cls == k.first && x.mol < k.second);
+      });
+      h->cm_begin[(size_t)c * nm1 + m] = (int)(it - tmp.begin());
+    }
   h->pairs.assign(tmp.size(), PairInfo{});
   std::vector<PrimPair<double>> pd;
   std::vector<double> aa, ab;
@@ -177,6 +197,7 @@ int build_pairs(hfgpu_handle* h) {
     P.fa = h->first[t.sa];
     P.fb = h->first[t.sb];
     P.cls = t.cls;
+    P.mol = t.mol;
     P.atom_a = h->shell_atom[t.sa];
     P.atom_b = h->shell_atom[t.sb];
     const double* A = &h->xyz[3 * P.atom_a];
@@ -301,8 +322,10 @@ int build_quartets(hfgpu_handle* h) {
     for (int cq = 0; cq <= cp; ++cq) {
       const int qc = quartet_class(cp, cq);
       for (auto& v : parts) v.clear();
-      const int pb = h->class_begin[cp], pe = h->class_begin[cp + 1];
-      const int kb = h->class_begin[cq], ke = h->class_begin[cq + 1];
+      const int nm1 = h->nmol + 1;
+      for (int mol = 0; mol < h->nmol; ++mol) {
+      const int pb = h->cm_begin[(size_t)cp * nm1 + mol], pe = h->cm_begin[(size_t)cp * nm1 + mol + 1];
+      const int kb = h->cm_begin[(size_t)cq * nm1 + mol], ke = h->cm_begin[(size_t)cq * nm1 + mol + 1];
       for (int P = pb; P < pe; ++P) {
         const double qp = h->pairs[P].schwarz;
         const int np = h->pairs[P].nprim;
@@ -313,6 +336,7 @@ int build_quartets(hfgpu_handle* h) {
           const bool many = np * h->pairs[Q].nprim >= kPrimWarpMinPrims;
           parts[(b >= mix ? 0 : 2) + (many ? 0 : 1)].push_back(make_int2(P, Q));
         }
+      }
       }
       h->q_beg[qc] = (long long)all.size();
       all.insert(all.end(), parts[0].begin(), parts[0].end());
@@ -347,6 +371,24 @@ __global__ void dmax_kernel(const int* __restrict__ first, int nshell, int n, co
 }
 
 // J = Jh + Jh^T, K = Kh + Kh^T (in place into J/K outputs).
+// J = Jh + Jh^T inside every molecule's block of a batched handle.
+__global__ void batch_symmetrise_kernel(const double* __restrict__ h, double* __restrict__ out, long long tot,
+                                        const long long* __restrict__ mol_off, const int* __restrict__ mol_n,
+                                        int nmol) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= tot) return;
+  int lo = 0, hi = nmol - 1;  // last molecule whose block starts at or before e
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (mol_off[mid] <= e) lo = mid; else hi = mid - 1;
+  }
+  const long long b = mol_off[lo];
+  const int nm = mol_n[lo];
+  const long long r = e - b;
+  const long long i = r / nm, j = r % nm;
+  out[e] = h[e] + h[b + j * nm + i];
+}
+
 __global__ void symmetrise_kernel(const double* __restrict__ h, double* __restrict__ out, int n, int nmat) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   const int tot = n * n;
@@ -436,7 +478,8 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
   if (nK < 0 || nK > 8) return fail(h, HFGPU_ERR_INVALID, "nK out of range");
   const int n = h->n, ns = h->nshell;
-  const size_t nn = (size_t)n * n;
+  const size_t nn = (size_t)h->mat_total;  // n*n, or the block storage of a batched handle
+  if (h->batched && nK > 1) return fail(h, HFGPU_ERR_UNSUPPORTED, "batched handles build RHF J/K (one density)");
   HF_CUDA(h, h->d_half.ensure(sizeof(double) * nn * (1 + std::max(nK, 1))));
   HF_CUDA(h, h->d_counters.ensure(sizeof(unsigned long long) * 3 * hfgpu::kNumClasses));
   double* Jh = h->d_half.as<double>();
@@ -445,7 +488,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   HF_CUDA(h, cudaMemsetAsync(h->d_counters.p, 0, sizeof(unsigned long long) * 3 * hfgpu::kNumClasses, h->stream));
   int kernels = 0;
   const float* dmax = nullptr;
-  if (h->opts.density_tol > 0.0) {
+  if (h->opts.density_tol > 0.0 && !h->batched) {
     HF_CUDA(h, h->d_dmax.ensure(sizeof(float) * ns * ns + sizeof(int) * (ns + 1)));
     int* dfirst = reinterpret_cast<int*>(h->d_dmax.as<float>() + (size_t)ns * ns);
     HF_CUDA(h, cudaMemcpyAsync(dfirst, h->first.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, h->stream));
@@ -464,6 +507,12 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   }
   qf.jk.DJ = DJ; qf.jk.nK = nK; qf.jk.DK = DK; qf.jk.Jh = Jh; qf.jk.Kh = Kh; qf.jk.dmax = dmax;
   qf.jk.dtol = h->opts.density_tol; qf.jk.counters = h->d_counters.as<unsigned long long>();
+  if (h->batched) {
+    const long long* mo = h->d_mol.as<long long>();
+    const int* mn = reinterpret_cast<const int*>(mo + h->nmol);
+    qd.jk.mol_off = qf.jk.mol_off = mo;
+    qd.jk.mol_n = qf.jk.mol_n = mn;
+  }
   qd.mode = qf.mode = QMODE_JK;
   qd.warp_max = qf.warp_max = h->opts.warp_max_quartets;
   qd.pure = qf.pure = h->pure;
@@ -516,13 +565,22 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   h->last_launched = launched;
   const int tot = (int)nn;
   h->last_kernels = kernels + ((Jout && DJ) ? 1 : 0) + ((Kout && nK > 0) ? 1 : 0);
-  if (Jout && DJ) {
-    symmetrise_kernel<<<(tot + 255) / 256, 256, 0, h->stream>>>(Jh, Jout, n, 1);
-    HF_CHECK_LAUNCH(h, "symmetrise J");
-  }
-  if (Kout && nK > 0) {
-    symmetrise_kernel<<<(tot * nK + 255) / 256, 256, 0, h->stream>>>(Kh, Kout, n, nK);
-    HF_CHECK_LAUNCH(h, "symmetrise K");
+  if (h->batched) {
+    const long long* mo = h->d_mol.as<long long>();
+    const int* mn = reinterpret_cast<const int*>(mo + h->nmol);
+    const int nb = (int)((nn + 255) / 256);
+    if (Jout && DJ) batch_symmetrise_kernel<<<nb, 256, 0, h->stream>>>(Jh, Jout, (long long)nn, mo, mn, h->nmol);
+    if (Kout && nK > 0) batch_symmetrise_kernel<<<nb, 256, 0, h->stream>>>(Kh, Kout, (long long)nn, mo, mn, h->nmol);
+    HF_CHECK_LAUNCH(h, "symmetrise blocks");
+  } else {
+    if (Jout && DJ) {
+      symmetrise_kernel<<<(tot + 255) / 256, 256, 0, h->stream>>>(Jh, Jout, n, 1);
+      HF_CHECK_LAUNCH(h, "symmetrise J");
+    }
+    if (Kout && nK > 0) {
+      symmetrise_kernel<<<(tot * nK + 255) / 256, 256, 0, h->stream>>>(Kh, Kout, n, nK);
+      HF_CHECK_LAUNCH(h, "symmetrise K");
+    }
   }
   return HFGPU_OK;
 }
@@ -539,6 +597,11 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   gd.boys.tab = h->d_boys_d.as<double>();
   gd.n = h->n;
   gd.DJ = DJ; gd.cJ = cJ; gd.nK = nK; gd.DK = DK; gd.cK = cK; gd.grad = grad;
+  if (h->batched) {
+    if (nK > 1) return fail(h, HFGPU_ERR_UNSUPPORTED, "batched handles take one density");
+    gd.mol_off = h->d_mol.as<long long>();
+    gd.mol_n = reinterpret_cast<const int*>(gd.mol_off + h->nmol);
+  }
   GradArgs<float> gf{};
   gf.pairs = gd.pairs;
   gf.prims = h->d_prim_f.as<PrimPair<float>>();
@@ -547,6 +610,8 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   gf.boys.tab = h->d_boys_f.as<float>();
   gf.n = h->n;
   gf.DJ = DJ; gf.cJ = cJ; gf.nK = nK; gf.DK = DK; gf.cK = cK; gf.grad = grad;
+  gf.mol_off = gd.mol_off;
+  gf.mol_n = gd.mol_n;
   const int2* q = h->d_quart.as<int2>();
   const size_t budget = (size_t)1 << 30;  // scratch bytes for table-mode classes
   // threads of a table-mode launch: as many as the budget allows (at least 4736),
@@ -734,6 +799,12 @@ int hfgpu_create(const hfgpu_basis* b, const hfgpu_opts* opts, hfgpu_handle** ou
   for (int s = 0; s < b->nshell; ++s)
     normalise(h->L[s], h->nprim[s], &b->exps[h->prim_off[s]], &b->coefs[h->prim_off[s]], &h->coefs[h->prim_off[s]]);
   h->n = h->first[b->nshell];
+  h->nmol = 1;
+  h->mol_shell = {0, b->nshell};
+  h->mol_n = {h->n};
+  h->mol_off = {0};
+  h->mol_atom = {0, b->natoms};
+  h->mat_total = (long long)h->n * h->n;
   int rc = set_device(h);
   if (rc) {
     delete h;
@@ -765,6 +836,7 @@ int hfgpu_destroy(hfgpu_handle* h) {
                     &h->d_quart, &h->d_mats, &h->d_half, &h->d_dmax, &h->d_counters, &h->d_grad, &h->d_scratch,
                     &h->d_eri, &h->d_eriq})
     d->release();
+  h->d_mol.release();
   if (h->ev[0])
     for (auto& e : h->ev) cudaEventDestroy(e);
   for (int i = 0; i < hfgpu_handle::kAux; ++i) {
@@ -1124,6 +1196,101 @@ int hfgpu_fp64_peak(int device, double* tflops) {
   cudaFree(out);
   *tflops = best;
   return cudaGetLastError() == cudaSuccess ? HFGPU_OK : HFGPU_ERR_CUDA;
+}
+
+int hfgpu_batch_create(int nmol, const hfgpu_basis* bases, const double* const* xyz, const hfgpu_opts* opts,
+                       hfgpu_handle** out) {
+  if (nmol <= 0 || !bases || !xyz || !out) return HFGPU_ERR_INVALID;
+  *out = nullptr;
+  // concatenate the molecules into one basis; function indices stay local to each molecule
+  std::vector<int> L, atom, nprim;
+  std::vector<double> exps, coefs;
+  std::vector<int> mol_shell(1, 0), mol_atom(1, 0);
+  int natoms = 0;
+  for (int m = 0; m < nmol; ++m) {
+    const hfgpu_basis& b = bases[m];
+    if (b.nshell <= 0 || b.natoms <= 0 || !b.L || !b.shell_atom || !b.nprim || !b.exps || !b.coefs || !xyz[m] ||
+        b.pure)
+      return HFGPU_ERR_INVALID;  // batched handles are Cartesian (s and p are identical either way)
+    int np = 0;
+    for (int s = 0; s < b.nshell; ++s) {
+      L.push_back(b.L[s]);
+      atom.push_back(b.shell_atom[s] + natoms);
+      nprim.push_back(b.nprim[s]);
+      np += b.nprim[s];
+    }
+    exps.insert(exps.end(), b.exps, b.exps + np);
+    coefs.insert(coefs.end(), b.coefs, b.coefs + np);
+    natoms += b.natoms;
+    mol_shell.push_back((int)L.size());
+    mol_atom.push_back(natoms);
+  }
+  hfgpu_opts o;
+  if (opts) o = *opts; else hfgpu_default_opts(&o);
+  o.density_tol = 0.0;  // the density bound is per molecule pair data; not used in batches
+  hfgpu_basis all{(int)L.size(), natoms, 0, L.data(), atom.data(), nprim.data(), exps.data(), coefs.data()};
+  hfgpu_handle* h = nullptr;
+  int rc = hfgpu_create(&all, &o, &h);
+  if (rc) return rc;
+  h->batched = true;
+  h->nmol = nmol;
+  h->mol_shell = mol_shell;
+  h->mol_atom = mol_atom;
+  h->mol_n.assign(nmol, 0);
+  h->mol_off.assign(nmol, 0);
+  long long off = 0;
+  for (int m = 0; m < nmol; ++m) {
+    int f = 0;
+    for (int s = mol_shell[m]; s < mol_shell[m + 1]; ++s) {
+      h->first[s] = f;
+      f += (L[s] + 1) * (L[s] + 2) / 2;
+    }
+    h->mol_n[m] = f;
+    h->mol_off[m] = off;
+    off += (long long)f * f;
+  }
+  h->first[h->nshell] = h->mol_n[nmol - 1];
+  h->mat_total = off;
+  h->n = *std::max_element(h->mol_n.begin(), h->mol_n.end());
+  std::vector<unsigned char> mol_dev(sizeof(long long) * nmol + sizeof(int) * nmol);
+  std::memcpy(mol_dev.data(), h->mol_off.data(), sizeof(long long) * nmol);
+  std::memcpy(mol_dev.data() + sizeof(long long) * nmol, h->mol_n.data(), sizeof(int) * nmol);
+  if (h->d_mol.ensure(mol_dev.size()) || cudaMemcpy(h->d_mol.p, mol_dev.data(), mol_dev.size(), cudaMemcpyHostToDevice)) {
+    hfgpu_destroy(h);
+    return HFGPU_ERR_CUDA;
+  }
+  std::vector<double> x;
+  for (int m = 0; m < nmol; ++m) x.insert(x.end(), xyz[m], xyz[m] + 3 * bases[m].natoms);
+  if ((rc = hfgpu_set_geometry(h, x.data(), natoms))) {
+    hfgpu_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return HFGPU_OK;
+}
+
+int hfgpu_batch_layout(const hfgpu_handle* h, int* nbf, long long* mat_off, long long* mat_total) {
+  if (!h) return HFGPU_ERR_INVALID;
+  for (int m = 0; m < h->nmol; ++m) {
+    if (nbf) nbf[m] = h->mol_n[m];
+    if (mat_off) mat_off[m] = h->mol_off[m];
+  }
+  if (mat_total) *mat_total = h->mat_total;
+  return HFGPU_OK;
+}
+
+int hfgpu_batch_jk_device(hfgpu_handle* h, const double* D, double* J, double* K, int precision) {
+  if (!h || !D || !J || !K) return HFGPU_ERR_INVALID;
+  int rc = set_device(h);
+  if (rc) return rc;
+  return jk_device_impl(h, D, 1, D, J, K, precision);
+}
+
+int hfgpu_batch_grad2e_device(hfgpu_handle* h, const double* D, double* grad, int precision) {
+  if (!h || !D || !grad) return HFGPU_ERR_INVALID;
+  int rc = set_device(h);
+  if (rc) return rc;
+  return grad_device_impl(h, D, 2.0, 1, D, 1.0, grad, precision);
 }
 
 }  // extern "C"

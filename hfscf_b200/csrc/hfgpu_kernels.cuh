@@ -28,6 +28,8 @@ struct JKArgs {
   double* __restrict__ Kh;           // nK x n x n
   const float* __restrict__ dmax;    // nshell x nshell max |D| over all densities, or nullptr
   double dtol;                       // density-weighted screening threshold
+  const long long* __restrict__ mol_off;  // batched handle: start of each molecule's n_m x n_m block, else nullptr
+  const int* __restrict__ mol_n;          // batched handle: n_m
   unsigned long long* __restrict__ counters;  // per class: computed, skipped by density, primitive quartets
 };
 
@@ -45,6 +47,8 @@ struct GradArgs {
   const double* __restrict__ DK;
   double cK;
   double* __restrict__ grad;         // natoms x 3
+  const long long* __restrict__ mol_off;  // batched handle (see JKArgs)
+  const int* __restrict__ mol_n;
   R* __restrict__ scratch;           // thread-interleaved scratch (table-mode classes)
   int scratch_threads;               // threads sharing the scratch (stride)
 };
@@ -182,6 +186,21 @@ __device__ __forceinline__ long long packed_index(long long i, long long j, long
 
 enum : int { QMODE_JK = 0, QMODE_PACKED = 1, QMODE_SCHWARZ = 2 };
 
+// Matrix block of the quartet's molecule: offset into D/J/K storage and its leading dimension.
+__device__ __forceinline__ void mol_block(const long long* mol_off, const int* mol_n, int mol, int n, long long& blk,
+                                          int& nm) {
+  if (mol_off != nullptr) {
+    blk = mol_off[mol];
+    nm = mol_n[mol];
+  } else {
+    blk = 0;
+    nm = n;
+  }
+}
+
+__device__ __forceinline__ const double* off_ptr(const double* p, long long b) { return p ? p + b : p; }
+__device__ __forceinline__ double* off_ptr(double* p, long long b) { return p ? p + b : p; }
+
 // What one thread does with its block, by mode:
 //   JK      digest into J/K;
 //   PACKED  write the unique ERIs into the reference's packed 8-fold vector
@@ -265,19 +284,22 @@ __global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const i
   if (P.sa == P.sb) s *= 0.5;
   if (Q.sa == Q.sb) s *= 0.5;
   if (pq.x == pq.y) s *= 0.5;
+  long long blk;
+  int nm;
+  mol_block(a.mol_off, a.mol_n, P.mol, a.n, blk, nm);
   if (qa.pure) {
     using Dp = BlockDims<LA, LB, LC, LD, true>;
     double V[Dp::NOUT];
     if (valid) finish_block<LA, LB, LC, LD, R, true>(cart, V);
     if (valid || coop)
-      use_block<LA, LB, LC, LD, true>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri,
-                                      qa.pairs_rw, coop);
+      use_block<LA, LB, LC, LD, true>(V, qa.mode, pq, P, Q, s, off_ptr(a.DJ, blk), a.nK, off_ptr(a.DK, blk),
+                                      off_ptr(a.Jh, blk), off_ptr(a.Kh, blk), nm, qa.eri, qa.pairs_rw, coop);
   } else {
     double V[Dc::NOUT];
     if (valid) finish_block<LA, LB, LC, LD, R, false>(cart, V);
     if (valid || coop)
-      use_block<LA, LB, LC, LD, false>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri,
-                                       qa.pairs_rw, coop);
+      use_block<LA, LB, LC, LD, false>(V, qa.mode, pq, P, Q, s, off_ptr(a.DJ, blk), a.nK, off_ptr(a.DK, blk),
+                                       off_ptr(a.Jh, blk), off_ptr(a.Kh, blk), nm, qa.eri, qa.pairs_rw, coop);
   }
 }
 
@@ -318,15 +340,20 @@ __global__ void __launch_bounds__(128) quartet_primwarp_kernel(QuartetArgs<R> qa
   if (P.sa == P.sb) s *= 0.5;
   if (Q.sa == Q.sb) s *= 0.5;
   if (pq.x == pq.y) s *= 0.5;
+  long long blk;
+  int nm;
+  mol_block(a.mol_off, a.mol_n, P.mol, a.n, blk, nm);
   if (qa.pure) {
     using Dp = BlockDims<LA, LB, LC, LD, true>;
     double V[Dp::NOUT];
     finish_block<LA, LB, LC, LD, R, true>(cart, V);
-    use_block<LA, LB, LC, LD, true>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri, qa.pairs_rw);
+    use_block<LA, LB, LC, LD, true>(V, qa.mode, pq, P, Q, s, off_ptr(a.DJ, blk), a.nK, off_ptr(a.DK, blk),
+                                    off_ptr(a.Jh, blk), off_ptr(a.Kh, blk), nm, qa.eri, qa.pairs_rw);
   } else {
     double V[Dc::NOUT];
     finish_block<LA, LB, LC, LD, R, false>(cart, V);
-    use_block<LA, LB, LC, LD, false>(V, qa.mode, pq, P, Q, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, qa.eri, qa.pairs_rw);
+    use_block<LA, LB, LC, LD, false>(V, qa.mode, pq, P, Q, s, off_ptr(a.DJ, blk), a.nK, off_ptr(a.DK, blk),
+                                     off_ptr(a.Jh, blk), off_ptr(a.Kh, blk), nm, qa.eri, qa.pairs_rw);
   }
 }
 
@@ -447,6 +474,9 @@ __device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, cons
     if (P.sa == P.sb) s *= 0.5;
     if (Q.sa == Q.sb) s *= 0.5;
     if (pq.x == pq.y) s *= 0.5;
+    long long gblk;
+    int gnm;
+    mol_block(a.mol_off, a.mol_n, P.mol, a.n, gblk, gnm);
     R g[9];
     if constexpr (CC::kGradTable) {
       using Tab = typename CC::GradTab;
@@ -458,7 +488,7 @@ __device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, cons
       Strided<R> t0{base + (size_t)(Tab::NVSLOT + Tab::NHSLOT + Dm::NCART) * a.scratch_threads, a.scratch_threads};
       Strided<R> t1{base + (size_t)(Tab::NVSLOT + Tab::NHSLOT + 2 * Dm::NCART) * a.scratch_threads, a.scratch_threads};
       if constexpr (PURE) {
-        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb,
+        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(off_ptr(a.DJ, gblk), a.cJ, a.nK, off_ptr(a.DK, gblk), a.cK, gnm, P.fa, P.fb,
                                                      Q.fa, Q.fb, s, t0);
         // pure -> Cartesian weights, one index at a time: t0 -> t1 -> t0 -> t1 -> Wc
         const int Ls[4] = {LA, LB, LC, LD};
@@ -493,7 +523,7 @@ __device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, cons
           dst = tmp;
         }
       } else {
-        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb,
+        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(off_ptr(a.DJ, gblk), a.cJ, a.nK, off_ptr(a.DK, gblk), a.cK, gnm, P.fa, P.fb,
                                                      Q.fa, Q.fb, s, Wc);
       }
       grad_table<R, Tab>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
@@ -503,11 +533,11 @@ __device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, cons
       R Wc[Dm::NCART];
       if constexpr (PURE) {
         R Wp[Dm::NOUT];
-        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb,
+        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(off_ptr(a.DJ, gblk), a.cJ, a.nK, off_ptr(a.DK, gblk), a.cK, gnm, P.fa, P.fb,
                                                      Q.fa, Q.fb, s, Wp);
         CC::template from_pure<R>(Wp, Wc);
       } else {
-        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb,
+        grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(off_ptr(a.DJ, gblk), a.cJ, a.nK, off_ptr(a.DK, gblk), a.cK, gnm, P.fa, P.fb,
                                                      Q.fa, Q.fb, s, Wc);
       }
       CC::template grad<R>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
@@ -754,7 +784,11 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
   if (Q.sa == Q.sb) s *= 0.5;
   if (pq.x == pq.y) s *= 0.5;
   if (qa.mode == QMODE_JK) {
-    warp_digest<R>(V, NA, NB, NC, ND, P.fa, P.fb, Q.fa, Q.fb, s, a.DJ, a.nK, a.DK, a.Jh, a.Kh, a.n, lane);
+    long long blk;
+    int nm;
+    mol_block(a.mol_off, a.mol_n, P.mol, a.n, blk, nm);
+    warp_digest<R>(V, NA, NB, NC, ND, P.fa, P.fb, Q.fa, Q.fb, s, off_ptr(a.DJ, blk), a.nK, off_ptr(a.DK, blk),
+                   off_ptr(a.Jh, blk), off_ptr(a.Kh, blk), nm, lane);
   } else if (qa.mode == QMODE_PACKED) {
     for (int e = lane; e < NA * NB * NC * ND; e += 32) {
       const int l = e % ND, k = (e / ND) % NC, j = (e / (ND * NC)) % NB, i = e / (ND * NC * NB);

@@ -136,6 +136,21 @@ int hfgpu_grad2e_device_noalloc(hfgpu_handle* h, const double* DJ, double cJ, in
                                 double* grad, int precision);
 long long hfgpu_noalloc_scratch_bytes(void);
 
+/* Batched handles: many independent molecules in one handle (hundreds of
+ * small molecules).  No counterpart in the reference, which runs one molecule per process.
+ * Shell pairs and quartets are formed within each molecule only; every per-class kernel
+ * launch covers all molecules.  Matrices live in a block storage: molecule m's n_m x n_m
+ * row-major block starts at mat_off[m].  Molecules must be Cartesian (pure = 0); for s and
+ * p shells the two are the same functions.  RHF only (one density).  Atoms are numbered
+ * consecutively over the molecules for the gradient. */
+int hfgpu_batch_create(int nmol, const hfgpu_basis* bases, const double* const* xyz_bohr, const hfgpu_opts* opts,
+                       hfgpu_handle** out);
+int hfgpu_batch_layout(const hfgpu_handle* h, int* nbf, long long* mat_off, long long* mat_total);
+/* J[D], K[D] for every molecule; D, J, K device pointers to block storage. */
+int hfgpu_batch_jk_device(hfgpu_handle* h, const double* D, double* J, double* K, int precision);
+/* grad (device, total atoms x 3) += two-electron RHF gradient of every molecule. */
+int hfgpu_batch_grad2e_device(hfgpu_handle* h, const double* D, double* grad, int precision);
+
 /* One-electron matrices S, T, V (n x n) for the basis at xyz (bohr), on the host CPU.
  * Z: nuclear charges per atom.  Needs no handle and no GPU: these O(N^2) integrals
  * stay on the CPU here (the reference's OSOverlap/OSKinetic/OSNuclear,
