@@ -2,9 +2,9 @@
 
 One batched engine handle holds every molecule (hfgpu_batch_create).  Each SCF
 iteration is one J/K build for all molecules at once -- the per-class kernels
-cover every molecule's quartets -- and the N x N work (orthogonalisation,
-DIIS, diagonalisation) runs batched on the GPU in torch over matrices padded to
-the largest molecule.  The J/K build and the Fock assembly can be captured once
+cover every molecule's quartets.  DIIS and the Fock assembly run batched on the
+GPU in torch over matrices padded to the largest molecule; the per-molecule
+diagonalisations run on a host thread pool over the unpadded blocks.  The J/K build and the Fock assembly can be captured once
 as a CUDA graph and replayed every iteration.  After convergence, the
 two-electron gradient of every molecule comes from one batched adjoint launch
 (hfgpu_batch_grad2e_device); one-electron and nuclear terms are added per
@@ -16,7 +16,9 @@ commutator.  Here DIIS keeps the last 6 vectors per molecule.
 """
 from __future__ import annotations
 
+import concurrent.futures as cf
 import ctypes
+import os
 import time
 
 import numpy as np
@@ -134,15 +136,33 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     Hblk = torch.from_numpy(np.concatenate(Hb)).to(dev)
     S = lay.to_pad(Sblk, fill_diag=1.0)
     H = lay.to_pad(Hblk, fill_diag=PAD_DIAG)
-    w, U = torch.linalg.eigh(S)
-    X = (U / torch.sqrt(w).unsqueeze(1)) @ U.transpose(1, 2)
-    nocc = torch.tensor([int(np.sum(b.Z)) // 2 for b in bases], device=dev)
-    occ = (torch.arange(nmax, device=dev).unsqueeze(0) < nocc.unsqueeze(1)).to(torch.float64)
+    # per-molecule orthogonalisers on the host; the diagonalisations run there too, on a
+    # thread pool over the unpadded blocks (LAPACK releases the GIL), because batched
+    # eigh of padded matrices on the GPU loops over the batch
+    Xh, Xpad = [], np.zeros((nmol, nmax, nmax))
+    for k, b in enumerate(bases):
+        n = b.nbf
+        w, U = np.linalg.eigh(Sb[k].reshape(n, n))
+        Xh.append((U / np.sqrt(w)) @ U.T)
+        Xpad[k, :n, :n] = Xh[-1]
+        Xpad[k, np.arange(n, nmax), np.arange(n, nmax)] = 1.0
+    X = torch.from_numpy(Xpad).to(dev)
+    nocc_h = [int(np.sum(b.Z)) // 2 for b in bases]
+    pool = cf.ThreadPoolExecutor(max_workers=max(1, min(32, os.cpu_count() or 1)))
+    Dh = np.zeros(be.mat_total)
 
     def density(F):
-        e, Cp = torch.linalg.eigh(X.transpose(1, 2) @ F @ X)
-        C = X @ Cp
-        return (C * occ.unsqueeze(1)) @ C.transpose(1, 2)
+        Fh = lay.to_block(F).cpu().numpy()
+
+        def one(k):
+            n, off = int(be.nbf[k]), int(be.mat_off[k])
+            Fk = Fh[off:off + n * n].reshape(n, n)
+            _, Cp = np.linalg.eigh(Xh[k].T @ Fk @ Xh[k])
+            C = Xh[k] @ Cp[:, :nocc_h[k]]
+            Dh[off:off + n * n] = (C @ C.T).ravel()
+
+        list(pool.map(one, range(nmol)))
+        return lay.to_pad(torch.from_numpy(Dh).to(dev))
 
     D = density(H)
     Dblk = lay.to_block(D).contiguous()
@@ -240,6 +260,7 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
             grads.append(gk)
         out["gradients"] = grads
         out["grad_s"] = time.perf_counter() - t2
+    pool.shutdown()
     be.close()
     torch.cuda.set_stream(torch.cuda.default_stream(dev))
     return out
