@@ -250,14 +250,16 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
         g2 = g.cpu().numpy()
         Dn = D.cpu().numpy()
         Fn = F.cpu().numpy()
-        grads = []
-        for k, b in enumerate(bases):
+        def one_grad(k):
+            b = bases[k]
             n = b.nbf
             Dk, Fk = Dn[k, :n, :n], Fn[k, :n, :n]
             gk = g2[be.atom_off[k]:be.atom_off[k + 1]].copy()
             gk += eng.one_electron_grad(b, Dk, Dk @ Fk @ Dk, 2.0, -2.0)
             gk += nuclear_repulsion_gradient(b.Z, b.coords)
-            grads.append(gk)
+            return gk
+
+        grads = list(pool.map(one_grad, range(nmol)))
         out["gradients"] = grads
         out["grad_s"] = time.perf_counter() - t2
     pool.shutdown()

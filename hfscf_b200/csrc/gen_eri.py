@@ -620,7 +620,7 @@ def classes():
     return pairs, out
 
 
-GRAD_STRAIGHT_MAX_VRR = 250   # larger gradient classes run in table mode
+GRAD_STRAIGHT_MAX_VRR = 900   # larger gradient classes run in table mode
 
 
 def class_args_sig():

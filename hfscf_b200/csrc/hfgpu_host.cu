@@ -613,7 +613,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   gf.mol_off = gd.mol_off;
   gf.mol_n = gd.mol_n;
   const int2* q = h->d_quart.as<int2>();
-  const size_t budget = (size_t)1 << 30;  // scratch bytes for table-mode classes
+  const size_t budget = (size_t)256 << 20;  // scratch bytes per table-mode class
   // threads of a table-mode launch: as many as the budget allows (at least 4736),
   // at most one per quartet, a whole number of 128-thread blocks
   auto table_threads = [&](int slots, long long nq) -> long long {
@@ -621,16 +621,19 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     thr = std::min<long long>(thr, ((nq + 127) / 128) * 128);
     return ((thr + 127) / 128) * 128;
   };
-  // Table-mode classes share one scratch buffer, so they run in order on aux[0];
-  // straight-line classes spread over the other auxiliary streams.
-  size_t need_max = 0;
+  // Every table-mode class gets its own slice of the scratch buffer, so the classes run
+  // concurrently on the auxiliary streams like the straight-line ones.
+  size_t slice_off[32] = {0};
+  size_t need_total = 0;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     const int slots = hfgpu::kClassLaunchers[c]->grad_scratch_slots(h->pure);
     const long long nq = h->q_end[c] - h->q_beg[c];
+    slice_off[c] = need_total;
     if (slots <= 0 || nq <= 0) continue;
-    need_max = std::max(need_max, (size_t)slots * sizeof(double) * (size_t)table_threads(slots, nq));
+    need_total += (size_t)slots * sizeof(double) * (size_t)table_threads(slots, nq);
+    need_total = (need_total + 255) / 256 * 256;
   }
-  if (need_max) HF_CUDA(h, h->d_scratch.ensure(need_max));
+  if (need_total) HF_CUDA(h, h->d_scratch.ensure(need_total));
   int rc = fork_streams(h);
   if (rc) return rc;
   int rr = 1;
@@ -639,7 +642,8 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
     if (e <= b) continue;
     const int slots = L->grad_scratch_slots(h->pure);
-    cudaStream_t st = slots > 0 ? h->aux[0] : h->aux[1 + (rr++ % (hfgpu_handle::kAux - 1))];
+    cudaStream_t st = h->aux[rr++ % hfgpu_handle::kAux];
+    unsigned char* slice = h->d_scratch.as<unsigned char>() + slice_off[c];
     auto run = [&](bool fp32, long long lo, long long hi) -> int {
       const int nq = (int)(hi - lo);
       if (nq <= 0) return HFGPU_OK;
@@ -647,15 +651,15 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
       if (slots > 0) {
         const size_t rb = fp32 ? sizeof(float) : sizeof(double);
         grid = (int)(table_threads(slots, nq) / 128);
-        if ((size_t)slots * rb * (size_t)grid * 128 > h->d_scratch.bytes)
+        if (slice_off[c] + (size_t)slots * rb * (size_t)grid * 128 > h->d_scratch.bytes)
           return fail(h, HFGPU_ERR_NOMEM, "gradient scratch too small");
       }
       if (fp32) {
-        gf.scratch = h->d_scratch.as<float>();
+        gf.scratch = reinterpret_cast<float*>(slice);
         gf.scratch_threads = grid * 128;
         L->grad_f(gf, h->pure, q + lo, nq, grid, st);
       } else {
-        gd.scratch = h->d_scratch.as<double>();
+        gd.scratch = reinterpret_cast<double*>(slice);
         gd.scratch_threads = grid * 128;
         L->grad_d(gd, h->pure, q + lo, nq, grid, st);
       }

@@ -230,7 +230,7 @@ void hfgpu_onee_matrices(const OneEBasis& b, const double* Zc, const double* xyz
   std::memset(S, 0, sizeof(double) * n * n);
   std::memset(T, 0, sizeof(double) * n * n);
   std::memset(V, 0, sizeof(double) * n * n);
-#pragma omp parallel for schedule(dynamic)
+#pragma omp parallel for schedule(dynamic) if (ns >= 24)
   for (int s = 0; s < ns; ++s)
     for (int t = s; t < ns; ++t) {
       const int la = b.L[s], lb = b.L[t], ca = ncart(la), cb = ncart(lb);
@@ -304,7 +304,7 @@ void hfgpu_onee_gradient(const OneEBasis& b, const double* Zc, const double* xyz
                          const double* W, double cH, double cS, double* grad) {
   const int ns = b.nshell, n = b.n;
   std::vector<double> g(3 * natoms, 0.0);
-#pragma omp parallel
+#pragma omp parallel if (ns >= 24)
   {
     std::vector<double> gl(3 * natoms, 0.0);
 #pragma omp for schedule(dynamic)
