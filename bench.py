@@ -319,11 +319,13 @@ def run_ours(args, world, rank, local):
         # 512 seeded small molecules, SCF + gradient each, in one batched handle
         from hfscf_b200 import batch as BT
         from hfscf_b200 import molecules as MM
-        bb = BT.batch_bases(MM.batch_molecules(512))
+        from hfscf_b200 import dist as DI
+        allm = MM.batch_molecules(512)
+        bb = BT.batch_bases([allm[i] for i in DI.shard(len(allm), rank, world)])  # replicas: molecules split
         torch.cuda.synchronize()
         tb = time.perf_counter()
         rb = BT.batch_rhf(bb, device=local)
-        wall = time.perf_counter() - tb
+        wall = DI.max_over_ranks(time.perf_counter() - tb, dev)
         torch.cuda.set_stream(stream)
         line["batch"] = {"workload": "512 seeded molecules ((H2O)1-6, CH4, C2H6, NH3; STO-3G or 6-31G*), "
                                      "RHF to convergence + RHF gradient each, one batched handle",
