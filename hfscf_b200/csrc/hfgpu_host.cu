@@ -16,7 +16,10 @@ namespace {
 
 constexpr int kPairClasses = 6;
 constexpr double kPi = 3.14159265358979323846;
-constexpr double kPrimPairCut = 1e-24;  // |K_ab| below this cannot reach 1e-14 in any integral
+// A primitive quartet contributes at most |Kp_ab Kp_cd| / sqrt(p + q) (times F_m <= 1 and
+// the recurrence factors) to any integral; primitive pairs whose bound against the
+// largest pair of the molecule is below kPrimQuartetCut are dropped.
+constexpr double kPrimQuartetCut = 1e-16;
 
 int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }  // la >= lb: ss ps pp ds dp dd
 int quartet_class(int cp, int cq) { return cp * (cp + 1) / 2 + cq; }  // cp >= cq
@@ -183,6 +186,23 @@ int build_pairs(hfgpu_handle* h) {
       });
       h->cm_begin[(size_t)c * nm1 + m] = (int)(it - tmp.begin());
     }
+  // largest |Kp| and smallest p over all primitive pairs, for the primitive-pair cut
+  double kp_max = 0.0, p_min = 1e300;
+  for (const Tmp& t : tmp) {
+    const double* A = &h->xyz[3 * h->shell_atom[t.sa]];
+    const double* B = &h->xyz[3 * h->shell_atom[t.sb]];
+    const double R2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
+    for (int i = 0; i < h->nprim[t.sa]; ++i)
+      for (int j = 0; j < h->nprim[t.sb]; ++j) {
+        const double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
+        const double p = a1 + a2;
+        const double kp = std::fabs(std::exp(-a1 * a2 / p * R2) * h->coefs[h->prim_off[t.sa] + i] *
+                                    h->coefs[h->prim_off[t.sb] + j]) * std::sqrt(PI_2_5) / p;
+        kp_max = std::max(kp_max, kp);
+        p_min = std::min(p_min, p);
+      }
+  }
+  const double kp_cut = kPrimQuartetCut * std::sqrt(2.0 * p_min) / std::max(kp_max, 1e-300);
   h->pairs.assign(tmp.size(), PairInfo{});
   std::vector<PrimPair<double>> pd;
   std::vector<double> aa, ab;
@@ -213,7 +233,7 @@ int build_pairs(hfgpu_handle* h) {
         const double c1 = h->coefs[h->prim_off[t.sa] + i], c2 = h->coefs[h->prim_off[t.sb] + j];
         const double p = a1 + a2;
         const double K = std::exp(-a1 * a2 / p * R2) * c1 * c2;
-        if (std::fabs(K) < kPrimPairCut) continue;
+        if (std::fabs(K) * std::sqrt(PI_2_5) / p < kp_cut) continue;
         PrimPair<double> q;
         q.p = p;
         q.ip = 1.0 / p;
