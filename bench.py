@@ -313,7 +313,10 @@ def run_ours(args, world, rank, local):
             "scf": {"energy": res.energy, "iterations": res.iterations, "converged": res.converged,
                     "wall_s": scf_wall, "grad_wall_s": grad_wall, "grad_max": float(np.max(np.abs(grad))),
                     "mixed_incremental_energy": res_mx.energy, "mixed_dE": res_mx.energy - res.energy,
-                    "mixed_wall_s": mixed_wall, "e_nuc": nuclear_repulsion(bs.Z, bs.coords)},
+                    "mixed_wall_s": mixed_wall, "e_nuc": nuclear_repulsion(bs.Z, bs.coords),
+                    "fp64_fock_ms": [round(1e3 * t, 3) for t in res.fock_times],
+                    "mixed_incremental_fock_ms": [round(1e3 * t, 3) for t in res_mx.fock_times],
+                    "time_to_solution_ratio_fp64_over_mixed": scf_wall / mixed_wall},
             "check": {"max_abs_F_device_vs_api": err_f}}
     if not args.no_batch:
         # 512 seeded small molecules, SCF + gradient each, in one batched handle

@@ -99,6 +99,11 @@ struct hfgpu_handle {
   // inside each part the quartets with many primitive quartets come first:
   // [beg, hik1) and [mid, hik2) run the warp-over-primitives kernel where the class has one
   std::vector<long long> q_beg, q_mid, q_end, q_hik1, q_hik2;
+  // inside each of the four segments quartets are ordered by Schwarz-bound decade
+  // (largest first, bra-major inside a decade): bucket_end[(c * 4 + seg) * kBuckets + e] is the
+  // end of decade e (bound in [10^-e, 10^(1-e)), e = 0 collects bounds >= 1)
+  std::vector<long long> bucket_end;
+  DevBuf d_gmax;
   long long nquartets = 0;
 
   DevBuf d_pairs, d_prim_d, d_prim_f, d_alpha_d, d_alpha_f, d_boys_d, d_boys_f, d_quart;
@@ -331,6 +336,13 @@ int compute_schwarz(hfgpu_handle* h) {
 }
 
 constexpr int kPrimWarpMinPrims = 32;  // primitive quartets per quartet for the warp-over-primitives kernel
+constexpr int kBuckets = 18;           // Schwarz-bound decades of the quartet lists
+
+int bound_decade(double b) {
+  if (b >= 1.0) return 0;
+  const int e = (int)std::ceil(-std::log10(b));  // b in [10^-e, 10^(1-e))
+  return std::min(std::max(e, 1), kBuckets - 1);
+}
 
 // Screened unique quartets (P <= Q within a class; bra class >= ket class), per class.
 int build_quartets(hfgpu_handle* h) {
@@ -338,6 +350,7 @@ int build_quartets(hfgpu_handle* h) {
   std::vector<int2> all;
   std::vector<int2> parts[4];  // high bound many-prim, high bound few-prim, low bound many, low bound few
   h->nquartets = 0;
+  h->bucket_end.assign((size_t)hfgpu::kNumClasses * 4 * kBuckets, 0);
   for (int cp = 0; cp < kPairClasses; ++cp)
     for (int cq = 0; cq <= cp; ++cq) {
       const int qc = quartet_class(cp, cq);
@@ -358,14 +371,27 @@ int build_quartets(hfgpu_handle* h) {
         }
       }
       }
-      h->q_beg[qc] = (long long)all.size();
-      all.insert(all.end(), parts[0].begin(), parts[0].end());
-      h->q_hik1[qc] = (long long)all.size();
-      all.insert(all.end(), parts[1].begin(), parts[1].end());
-      h->q_mid[qc] = (long long)all.size();
-      all.insert(all.end(), parts[2].begin(), parts[2].end());
-      h->q_hik2[qc] = (long long)all.size();
-      all.insert(all.end(), parts[3].begin(), parts[3].end());
+      long long* seg_start[4] = {&h->q_beg[qc], &h->q_hik1[qc], &h->q_mid[qc], &h->q_hik2[qc]};
+      for (int sg = 0; sg < 4; ++sg) {
+        *seg_start[sg] = (long long)all.size();
+        // stable counting sort by bound decade
+        std::vector<int> dec(parts[sg].size());
+        long long cnt[kBuckets] = {0};
+        for (size_t x = 0; x < parts[sg].size(); ++x) {
+          const int2 pqv = parts[sg][x];
+          dec[x] = bound_decade(h->pairs[pqv.x].schwarz * h->pairs[pqv.y].schwarz);
+          ++cnt[dec[x]];
+        }
+        long long pos[kBuckets];
+        long long acc = (long long)all.size();
+        for (int e = 0; e < kBuckets; ++e) {
+          pos[e] = acc;
+          acc += cnt[e];
+          h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e] = acc;
+        }
+        all.resize(acc);
+        for (size_t x = 0; x < parts[sg].size(); ++x) all[pos[dec[x]]++] = parts[sg][x];
+      }
       h->q_end[qc] = (long long)all.size();
     }
   h->nquartets = (long long)all.size();
@@ -391,6 +417,15 @@ __global__ void dmax_kernel(const int* __restrict__ first, int nshell, int n, co
 }
 
 // J = Jh + Jh^T, K = Kh + Kh^T (in place into J/K outputs).
+// Largest entry of the shell-pair density maxima (non-negative floats compare as ints).
+__global__ void gmax_kernel(const float* __restrict__ dmax, int n, unsigned int* out) {
+  unsigned int m = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    m = max(m, __float_as_uint(dmax[i]));
+  for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 // J = Jh + Jh^T inside every molecule's block of a batched handle.
 __global__ void batch_symmetrise_kernel(const double* __restrict__ h, double* __restrict__ out, long long tot,
                                         const long long* __restrict__ mol_off, const int* __restrict__ mol_n,
@@ -517,6 +552,29 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     ++kernels;
     dmax = h->d_dmax.as<float>();
   }
+  // Quartets whose Schwarz bound times 4 max|D| is below the threshold cannot survive the
+  // per-quartet density test: with the lists ordered by bound decade, only a prefix of
+  // every segment is launched.
+  int keep_decades = kBuckets;
+  if (dmax != nullptr) {
+    HF_CUDA(h, h->d_gmax.ensure(sizeof(unsigned int)));
+    HF_CUDA(h, cudaMemsetAsync(h->d_gmax.p, 0, sizeof(unsigned int), h->stream));
+    gmax_kernel<<<std::min((ns * ns + 255) / 256, 1024), 256, 0, h->stream>>>(h->d_dmax.as<float>(), ns * ns,
+                                                                            h->d_gmax.as<unsigned int>());
+    HF_CHECK_LAUNCH(h, "gmax kernel");
+    ++kernels;
+    unsigned int gm_bits = 0;
+    HF_CUDA(h, cudaMemcpyAsync(&gm_bits, h->d_gmax.p, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->stream));
+    HF_CUDA(h, cudaStreamSynchronize(h->stream));
+    float gm;
+    std::memcpy(&gm, &gm_bits, sizeof(float));
+    const double dm4 = 4.0 * (double)gm;
+    keep_decades = 0;
+    for (int e = 0; e < kBuckets; ++e) {
+      const double upper = e == 0 ? 1e300 : std::pow(10.0, 1 - e);  // largest bound of decade e
+      if (upper * dm4 >= h->opts.density_tol) keep_decades = e + 1;
+    }
+  }
   QuartetArgs<double> qd{};
   qd.jk = jk_args_d(h);
   QuartetArgs<float> qf{};
@@ -554,23 +612,34 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     h->ev_used[c] = false;
     if (e <= b) continue;
     if (h->timing) HF_CUDA(h, cudaEventRecord(h->ev[2 * c], st));
-    const long long h1 = h->q_hik1[c], h2 = h->q_hik2[c];
-    // four segments: [b,h1) [h1,m) high bound, [m,h2) [h2,e) low bound; many-primitive first
-    // classes without the warp-over-primitives kernel launch each precision part whole
-    // (in FP64 both parts as one launch)
-    const bool mixed = precision == HFGPU_MIXED;
-    const long long seg[5] = {b, L->has_primwarp ? h1 : b, (L->has_primwarp || mixed) ? m : e,
-                              L->has_primwarp ? h2 : ((L->has_primwarp || mixed) ? m : e), e};
-    for (int sg = 0; sg < 4; ++sg) {
-      const int nseg = (int)(seg[sg + 1] - seg[sg]);
-      if (nseg <= 0) continue;
-      const bool fp32 = precision == HFGPU_MIXED && sg >= 2;
-      const bool many = (sg % 2) == 0 && L->has_primwarp;
-      const int2* qs = q + seg[sg];
-      if (fp32) {
-        if (!(many && L->primwarp_f(qf, qs, nseg, st))) L->quartet_f(qf, qs, nseg, st);
+    // Four parts in list order: [beg,hik1) many-primitive / [hik1,mid) few-primitive (high
+    // bound, FP64), [mid,hik2) / [hik2,end) (low bound, FP32 in mixed mode).  Each part keeps
+    // the prefix of bound decades that can survive the density test; adjacent ranges that
+    // run the same kernel are launched together.
+    const long long pstart[5] = {b, h->q_hik1[c], m, h->q_hik2[c], e};
+    struct Range { long long lo, hi; bool fp32, many; };
+    Range rg[4];
+    int nr = 0;
+    for (int part = 0; part < 4; ++part) {
+      long long lo = pstart[part], hi = pstart[part + 1];
+      if (keep_decades < kBuckets)
+        hi = keep_decades > 0 ? std::min(hi, h->bucket_end[((size_t)c * 4 + part) * kBuckets + keep_decades - 1]) : lo;
+      const bool fp32 = precision == HFGPU_MIXED && part >= 2;
+      const bool many = (part % 2) == 0 && L->has_primwarp;
+      if (nr > 0 && rg[nr - 1].hi == lo && rg[nr - 1].fp32 == fp32 && rg[nr - 1].many == many) {
+        rg[nr - 1].hi = hi;  // contiguous and the same kernel: extend
       } else {
-        if (!(many && L->primwarp_d(qd, qs, nseg, st))) L->quartet_d(qd, qs, nseg, st);
+        rg[nr++] = {lo, hi, fp32, many};
+      }
+    }
+    for (int r = 0; r < nr; ++r) {
+      const int nseg = (int)(rg[r].hi - rg[r].lo);
+      if (nseg <= 0) continue;
+      const int2* qs = q + rg[r].lo;
+      if (rg[r].fp32) {
+        if (!(rg[r].many && L->primwarp_f(qf, qs, nseg, st))) L->quartet_f(qf, qs, nseg, st);
+      } else {
+        if (!(rg[r].many && L->primwarp_d(qd, qs, nseg, st))) L->quartet_d(qd, qs, nseg, st);
       }
       ++kernels;
     }
