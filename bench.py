@@ -204,6 +204,9 @@ def run_ours(args, world, rank, local):
     t = time.perf_counter()
     res_mx = scf.rhf(bs, engine=eng, precision=E.MIXED, incremental=True)
     mixed_wall = time.perf_counter() - t
+    t = time.perf_counter()
+    grad_mx = scf.rhf_gradient(bs, res_mx, eng, E.MIXED)
+    grad_mx_wall = time.perf_counter() - t
     S, T, V = E.one_electron(bs)
     H = T + V
     dev = torch.device("cuda", local)
@@ -316,7 +319,11 @@ def run_ours(args, world, rank, local):
                     "mixed_wall_s": mixed_wall, "e_nuc": nuclear_repulsion(bs.Z, bs.coords),
                     "fp64_fock_ms": [round(1e3 * t, 3) for t in res.fock_times],
                     "mixed_incremental_fock_ms": [round(1e3 * t, 3) for t in res_mx.fock_times],
-                    "time_to_solution_ratio_fp64_over_mixed": scf_wall / mixed_wall},
+                    "time_to_solution_ratio_fp64_over_mixed": scf_wall / mixed_wall,
+                    "fock_time_ratio_fp64_over_mixed": sum(res.fock_times) / sum(res_mx.fock_times),
+                    "mixed_grad_wall_s": grad_mx_wall,
+                    "mixed_grad_max_abs_diff": float(np.max(np.abs(grad_mx - grad))),
+                    "scf_plus_grad_ratio_fp64_over_mixed": (scf_wall + grad_wall) / (mixed_wall + grad_mx_wall)},
             "check": {"max_abs_F_device_vs_api": err_f}}
     if not args.no_batch:
         # 512 seeded small molecules, SCF + gradient each, in one batched handle

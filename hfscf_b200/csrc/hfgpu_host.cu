@@ -529,7 +529,7 @@ static int read_counters(hfgpu_handle* h, long long* computed, long long* skippe
 
 // Device J/K: all pointers on the device.  Jout/Kout may be null to skip.
 static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* Jout, double* Kout,
-                          int precision) {
+                          int precision, bool delta = false) {
   if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
   if (nK < 0 || nK > 8) return fail(h, HFGPU_ERR_INVALID, "nK out of range");
   const int n = h->n, ns = h->nshell;
@@ -542,8 +542,10 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   HF_CUDA(h, cudaMemsetAsync(Jh, 0, sizeof(double) * nn * (1 + nK), h->stream));
   HF_CUDA(h, cudaMemsetAsync(h->d_counters.p, 0, sizeof(unsigned long long) * 3 * hfgpu::kNumClasses, h->stream));
   int kernels = 0;
+  // mixed-precision Delta-D builds screen at their own (looser) threshold; full builds never do
+  const double dtol = delta && precision == HFGPU_MIXED ? h->opts.mixed_density_tol : h->opts.density_tol;
   const float* dmax = nullptr;
-  if (h->opts.density_tol > 0.0 && !h->batched) {
+  if (dtol > 0.0 && !h->batched) {
     HF_CUDA(h, h->d_dmax.ensure(sizeof(float) * ns * ns + sizeof(int) * (ns + 1)));
     int* dfirst = reinterpret_cast<int*>(h->d_dmax.as<float>() + (size_t)ns * ns);
     HF_CUDA(h, cudaMemcpyAsync(dfirst, h->first.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, h->stream));
@@ -572,7 +574,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     keep_decades = 0;
     for (int e = 0; e < kBuckets; ++e) {
       const double upper = e == 0 ? 1e300 : std::pow(10.0, 1 - e);  // largest bound of decade e
-      if (upper * dm4 >= h->opts.density_tol) keep_decades = e + 1;
+      if (upper * dm4 >= dtol) keep_decades = e + 1;
     }
   }
   QuartetArgs<double> qd{};
@@ -580,11 +582,11 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   QuartetArgs<float> qf{};
   qf.jk = jk_args_f(h);
   for (JKArgs<double>* a : {&qd.jk}) {
-    a->DJ = DJ; a->nK = nK; a->DK = DK; a->Jh = Jh; a->Kh = Kh; a->dmax = dmax; a->dtol = h->opts.density_tol;
+    a->DJ = DJ; a->nK = nK; a->DK = DK; a->Jh = Jh; a->Kh = Kh; a->dmax = dmax; a->dtol = dtol;
     a->counters = h->d_counters.as<unsigned long long>();
   }
   qf.jk.DJ = DJ; qf.jk.nK = nK; qf.jk.DK = DK; qf.jk.Jh = Jh; qf.jk.Kh = Kh; qf.jk.dmax = dmax;
-  qf.jk.dtol = h->opts.density_tol; qf.jk.counters = h->d_counters.as<unsigned long long>();
+  qf.jk.dtol = dtol; qf.jk.counters = h->d_counters.as<unsigned long long>();
   if (h->batched) {
     const long long* mo = h->d_mol.as<long long>();
     const int* mn = reinterpret_cast<const int*>(mo + h->nmol);
@@ -839,6 +841,7 @@ int hfgpu_default_opts(hfgpu_opts* o) {
   o->schwarz_tol = 1e-12;
   o->density_tol = 1e-12;
   o->mixed_fp32_bound = 1e-4;
+  o->mixed_density_tol = 1e-10;
   o->device = 0;
   o->warp_max_quartets = 1 << 30;
   return HFGPU_OK;
@@ -1096,11 +1099,23 @@ int hfgpu_fock_uhf(hfgpu_handle* h, const double* Da, const double* Db, const do
 
 int hfgpu_fock_delta(hfgpu_handle* h, const double* dD, double* F, int precision) {
   if (!h || !dD || !F) return HFGPU_ERR_INVALID;
-  const size_t nn = (size_t)h->n * h->n;
-  std::vector<double> J(nn), K(nn);
-  int rc = hfgpu_jk(h, dD, 1, dD, J.data(), K.data(), precision);
+  int rc = set_device(h);
   if (rc) return rc;
-  for (size_t i = 0; i < nn; ++i) F[i] += 2.0 * J[i] - K[i];
+  const size_t nn = (size_t)h->n * h->n;
+  // same device layout as hfgpu_fock_rhf, with F_in in place of H
+  HF_CUDA(h, h->d_mats.ensure(sizeof(double) * nn * 4));
+  double* ddD = h->d_mats.as<double>();
+  double* dF = ddD + nn;
+  double* dJ = dF + nn;
+  double* dK = dJ + nn;
+  HF_CUDA(h, cudaMemcpyAsync(ddD, dD, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream));
+  HF_CUDA(h, cudaMemcpyAsync(dF, F, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream));
+  if ((rc = jk_device_impl(h, ddD, 1, ddD, dJ, dK, precision, true))) return rc;
+  fock_combine_kernel<<<(int)((nn + 255) / 256), 256, 0, h->stream>>>(dJ, dF, dJ, dK, (int)nn);
+  HF_CHECK_LAUNCH(h, "fock combine");
+  ++h->last_kernels;
+  HF_CUDA(h, cudaMemcpyAsync(F, dJ, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->stream));
   return HFGPU_OK;
 }
 

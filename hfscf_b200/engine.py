@@ -41,7 +41,7 @@ class _Basis(ctypes.Structure):
 
 class _Opts(ctypes.Structure):
     _fields_ = [("schwarz_tol", ctypes.c_double), ("density_tol", ctypes.c_double),
-                ("mixed_fp32_bound", ctypes.c_double), ("device", ctypes.c_int),
+                ("mixed_fp32_bound", ctypes.c_double), ("mixed_density_tol", ctypes.c_double), ("device", ctypes.c_int),
                 ("warp_max_quartets", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 

@@ -61,6 +61,9 @@ typedef struct {
                               the reference's screen_tol = 100 * integral_tol, hfscf_oseri.hpp:31-32) */
   double density_tol;      /* J/K: skip quartets whose density-weighted bound is below this (default 1e-12; 0 = off) */
   double mixed_fp32_bound; /* mixed precision: quartets with Q_ab Q_cd below this run in FP32 (default 1e-4) */
+  double mixed_density_tol;/* density-weighted threshold of mixed-precision builds (default 1e-10; they are
+                              used for incremental SCF builds whose error the final FP64-accumulated build
+                              and the variational energy absorb) */
   int device;              /* CUDA device ordinal (default 0) */
   int warp_max_quartets;   /* (dd|dp), (dd|dd): one warp per quartet when the class has at most this many
                               quartets, one thread per quartet otherwise (default 2^30 = always; -1 = never) */
