@@ -652,7 +652,8 @@ def common_header():
     return "\n".join(out) + "\n"
 
 
-WARP_MIN_VRR = 1000  # (dd|dp) and (dd|dd): measured faster as one warp per quartet than one thread
+WARP_MIN_VRR = 250        # classes that also get a warp-per-quartet form (hfgpu_autotune picks)
+WARP_DEFAULT_MIN_VRR = 1000  # (dd|dp) and (dd|dd): measured faster as one warp per quartet by default
 
 
 def class_header(c):
@@ -686,6 +687,7 @@ def class_header(c):
     parts.append(f"struct ClassCode<{la}, {lb}, {lc}, {ld}> {{")
     parts.append(f"  static constexpr bool kGradTable = {'false' if straight else 'true'};")
     parts.append(f"  static constexpr bool kWarp = {'true' if warp else 'false'};")
+    parts.append(f"  static constexpr bool kWarpDefault = {'true' if m['vrr_values'] >= WARP_DEFAULT_MIN_VRR else 'false'};")
     parts.append(f"  using WarpTab = {'WarpTab' + t if warp else 'void'};")
     parts.append(f"  using GradTab = {'void' if straight else 'GradTable' + t};")
     parts.append(f"  static constexpr bool kPrimWarp = {'true' if primwarp else 'false'};")
@@ -723,7 +725,8 @@ static void launch_quartet_impl(const QuartetArgs<R>& a, const int2* q, int nq, 
   bool warp = false;
   if constexpr (CC::kWarp) warp = nq <= a.warp_max;
   if (!warp) {{
-    quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 63) / 64, 64, 0, s>>>(a, q, nq);
+    const int bs = a.block > 0 ? a.block : 64;
+    quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + bs - 1) / bs, bs, 0, s>>>(a, q, nq);
     return;
   }}
   if constexpr (CC::kWarp) {{
@@ -775,7 +778,9 @@ extern const ClassLaunchers launchers_{t};
 const ClassLaunchers launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_quartet<double>, &launch_quartet<float>,
                                       &launch_grad<double>, &launch_grad<float>, &grad_scratch_slots,
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kPrimWarp,
-                                      &launch_primwarp<double>, &launch_primwarp<float>}};
+                                      &launch_primwarp<double>, &launch_primwarp<float>,
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kWarp,
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kWarpDefault}};
 }}  // namespace hfgpu
 """
 

@@ -1,6 +1,7 @@
 // Host side of the hfgpu engine: basis set-up, primitive-pair data, Schwarz
 // factors, screened quartet lists, and the C ABI of include/hfgpu.h.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -117,8 +118,19 @@ struct hfgpu_handle {
   bool timing = false;                  // record CUDA events around every class launch
   cudaEvent_t ev[2 * 21 + 2] = {};
   bool ev_used[21] = {};
+  // per-class launch schedule (hfgpu_autotune / hfgpu_set_schedule): threads per block of
+  // the thread-per-quartet form, warp-over-primitives form for the many-primitive parts,
+  // warp-per-quartet form (-1 = follow opts.warp_max_quartets)
+  int sched_block[21], sched_primwarp[21], sched_warp[21];
+  unsigned class_mask = ~0u;            // classes a J/K build launches (autotuning runs one at a time)
 
-  hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21) {}
+  hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21) {
+    for (int c = 0; c < 21; ++c) {
+      sched_block[c] = 64;
+      sched_primwarp[c] = 1;
+      sched_warp[c] = c < hfgpu::kNumClasses && hfgpu::kClassLaunchers[c]->warp_default ? -1 : 0;
+    }
+  }
 };
 
 namespace {
@@ -126,6 +138,12 @@ namespace {
 int fail(hfgpu_handle* h, int code, const std::string& msg) {
   if (h) h->err = msg;
   return code;
+}
+
+// warp_max of QuartetArgs for class c under the handle's schedule
+int class_warp_max(const hfgpu_handle* h, int c) {
+  const int w = h->sched_warp[c];
+  return w < 0 ? h->opts.warp_max_quartets : (w ? INT_MAX : -1);
 }
 
 int cuda_fail(hfgpu_handle* h, cudaError_t e, const char* where) {
@@ -318,12 +336,13 @@ int compute_schwarz(hfgpu_handle* h) {
   QuartetArgs<double> qa{};
   qa.jk = jk_args_d(h);
   qa.mode = QMODE_SCHWARZ;
-  qa.warp_max = h->opts.warp_max_quartets;
   qa.pure = h->pure;
   qa.pairs_rw = h->d_pairs.as<PairInfo>();
   for (int c = 0; c < kPairClasses; ++c) {
     const int b = h->class_begin[c], e = h->class_begin[c + 1];
     if (e <= b) continue;
+    qa.warp_max = class_warp_max(h, quartet_class(c, c));
+    qa.block = h->sched_block[quartet_class(c, c)];
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[quartet_class(c, c)];
     L->quartet_d(qa, h->d_quart.as<int2>() + b, e - b, h->stream);
     HF_CHECK_LAUNCH(h, "schwarz kernel");
@@ -594,7 +613,6 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     qd.jk.mol_n = qf.jk.mol_n = mn;
   }
   qd.mode = qf.mode = QMODE_JK;
-  qd.warp_max = qf.warp_max = h->opts.warp_max_quartets;
   qd.pure = qf.pure = h->pure;
   const int2* q = h->d_quart.as<int2>();
   long long launched = 0;
@@ -611,8 +629,10 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
     qd.jk.counters = cnt + 3 * c;
     qf.jk.counters = cnt + 3 * c;
+    qd.block = qf.block = h->sched_block[c];
+    qd.warp_max = qf.warp_max = class_warp_max(h, c);
     h->ev_used[c] = false;
-    if (e <= b) continue;
+    if (e <= b || !((h->class_mask >> c) & 1u)) continue;
     if (h->timing) HF_CUDA(h, cudaEventRecord(h->ev[2 * c], st));
     // Four parts in list order: [beg,hik1) many-primitive / [hik1,mid) few-primitive (high
     // bound, FP64), [mid,hik2) / [hik2,end) (low bound, FP32 in mixed mode).  Each part keeps
@@ -627,7 +647,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
       if (keep_decades < kBuckets)
         hi = keep_decades > 0 ? std::min(hi, h->bucket_end[((size_t)c * 4 + part) * kBuckets + keep_decades - 1]) : lo;
       const bool fp32 = precision == HFGPU_MIXED && part >= 2;
-      const bool many = (part % 2) == 0 && L->has_primwarp;
+      const bool many = (part % 2) == 0 && L->has_primwarp && h->sched_primwarp[c];
       if (nr > 0 && rg[nr - 1].hi == lo && rg[nr - 1].fp32 == fp32 && rg[nr - 1].many == many) {
         rg[nr - 1].hi = hi;  // contiguous and the same kernel: extend
       } else {
@@ -841,7 +861,7 @@ int hfgpu_default_opts(hfgpu_opts* o) {
   o->schwarz_tol = 1e-12;
   o->density_tol = 1e-12;
   o->mixed_fp32_bound = 1e-4;
-  o->mixed_density_tol = 1e-10;
+  o->mixed_density_tol = 1e-12;
   o->device = 0;
   o->warp_max_quartets = 1 << 30;
   return HFGPU_OK;
@@ -998,7 +1018,6 @@ int hfgpu_eri_packed(hfgpu_handle* h, double* eri_out, long long eri_len) {
   QuartetArgs<double> qa{};
   qa.jk = jk_args_d(h);
   qa.mode = QMODE_PACKED;
-  qa.warp_max = h->opts.warp_max_quartets;
   qa.pure = h->pure;
   qa.eri = h->d_eri.as<double>();
   for (int cp = 0; cp < kPairClasses; ++cp)
@@ -1010,6 +1029,8 @@ int hfgpu_eri_packed(hfgpu_handle* h, double* eri_out, long long eri_len) {
       if (list.empty()) continue;
       HF_CUDA(h, h->d_eriq.ensure(sizeof(int2) * list.size()));
       HF_CUDA(h, cudaMemcpyAsync(h->d_eriq.p, list.data(), sizeof(int2) * list.size(), cudaMemcpyHostToDevice, h->stream));
+      qa.warp_max = class_warp_max(h, quartet_class(cp, cq));
+      qa.block = h->sched_block[quartet_class(cp, cq)];
       hfgpu::kClassLaunchers[quartet_class(cp, cq)]->quartet_d(qa, h->d_eriq.as<int2>(), (int)list.size(), h->stream);
       HF_CHECK_LAUNCH(h, "packed eri kernel");
       HF_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1268,6 +1289,94 @@ int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms) {
   HF_CUDA(h, cudaEventSynchronize(h->ev[2 * cls + 1]));
   HF_CUDA(h, cudaEventElapsedTime(ms, h->ev[2 * cls], h->ev[2 * cls + 1]));
   return HFGPU_OK;
+}
+
+int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule) {
+  if (!h || !schedule) return HFGPU_ERR_INVALID;
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    const int bs = schedule[3 * c], pw = schedule[3 * c + 1], wp = schedule[3 * c + 2];
+    if ((bs != 32 && bs != 64 && bs != 128) || (pw != 0 && pw != 1) || wp < -1 || wp > 1)
+      return fail(h, HFGPU_ERR_INVALID, "schedule entry out of range");
+  }
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    h->sched_block[c] = schedule[3 * c];
+    h->sched_primwarp[c] = schedule[3 * c + 1];
+    h->sched_warp[c] = schedule[3 * c + 2];
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule) {
+  if (!h || !schedule) return HFGPU_ERR_INVALID;
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    schedule[3 * c] = h->sched_block[c];
+    schedule[3 * c + 1] = h->sched_primwarp[c];
+    schedule[3 * c + 2] = h->sched_warp[c];
+  }
+  return HFGPU_OK;
+}
+
+// Per class, times every launch form the class has on the handle's current quartet lists
+// and the given density, one class at a time on the handle's stream, and keeps the fastest.
+int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule) {
+  if (!h || !D) return HFGPU_ERR_INVALID;
+  int rc = set_device(h);
+  if (rc) return rc;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  repeats = std::max(1, std::min(repeats, 100));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  HF_CUDA(h, cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(h, HFGPU_ERR_CUDA, "cudaEventCreate");
+  }
+  struct Restore {  // the mask goes back on every exit path
+    hfgpu_handle* h;
+    unsigned mask;
+    cudaEvent_t a, b;
+    ~Restore() {
+      h->class_mask = mask;
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } restore{h, h->class_mask, e0, e1};
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    if (h->q_end[c] <= h->q_beg[c]) continue;
+    const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
+    h->class_mask = 1u << c;
+    float best = 1e30f;
+    int bb = h->sched_block[c], bp = h->sched_primwarp[c], bw = h->sched_warp[c];
+    const int warps[2] = {1, 0};
+    for (int wi = 0; wi < (L->has_warp ? 2 : 1); ++wi) {
+      const int wp = L->has_warp ? warps[wi] : -1;
+      for (int pw = (L->has_primwarp ? 1 : 0); pw >= 0; --pw) {
+        for (int bs : {32, 64, 128}) {
+          if (wp == 1 && bs != 64) continue;  // the warp form has its own block shape
+          h->sched_block[c] = bs;
+          h->sched_primwarp[c] = L->has_primwarp ? pw : 1;
+          h->sched_warp[c] = wp;
+          if ((rc = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return rc;  // warm-up
+          HF_CUDA(h, cudaEventRecord(e0, h->stream));
+          for (int r = 0; r < repeats; ++r)
+            if ((rc = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return rc;
+          HF_CUDA(h, cudaEventRecord(e1, h->stream));
+          HF_CUDA(h, cudaEventSynchronize(e1));
+          float ms = 0.f;
+          HF_CUDA(h, cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < best) {
+            best = ms;
+            bb = bs;
+            bp = h->sched_primwarp[c];
+            bw = wp;
+          }
+        }
+      }
+    }
+    h->sched_block[c] = bb;
+    h->sched_primwarp[c] = bp;
+    h->sched_warp[c] = bw;
+  }
+  return schedule ? hfgpu_get_schedule(h, schedule) : HFGPU_OK;
 }
 
 int hfgpu_last_launches(const hfgpu_handle* h, int* kernels) {

@@ -236,6 +236,7 @@ struct QuartetArgs {
   double* eri;          // PACKED output
   PairInfo* pairs_rw;   // SCHWARZ output
   int warp_max;         // large classes: warp per quartet up to this many quartets
+  int block;            // threads per block of the thread-per-quartet form (32, 64 or 128; 0 = 64)
 };
 
 template <int LA, int LB, int LC, int LD, typename R>

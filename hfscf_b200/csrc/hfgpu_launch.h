@@ -19,6 +19,8 @@ struct ClassLaunchers {
   bool has_primwarp;                     // warp-over-primitives kernel for high-contraction quartets
   bool (*primwarp_d)(const QuartetArgs<double>&, const int2*, int, cudaStream_t);
   bool (*primwarp_f)(const QuartetArgs<float>&, const int2*, int, cudaStream_t);
+  bool has_warp;                         // warp-per-quartet form with levelised tables
+  bool warp_default;                     // ... used unless the schedule or opts say otherwise
 };
 
 extern const ClassLaunchers* const kClassLaunchers[];

@@ -61,9 +61,9 @@ typedef struct {
                               the reference's screen_tol = 100 * integral_tol, hfscf_oseri.hpp:31-32) */
   double density_tol;      /* J/K: skip quartets whose density-weighted bound is below this (default 1e-12; 0 = off) */
   double mixed_fp32_bound; /* mixed precision: quartets with Q_ab Q_cd below this run in FP32 (default 1e-4) */
-  double mixed_density_tol;/* density-weighted threshold of mixed-precision builds (default 1e-10; they are
-                              used for incremental SCF builds whose error the final FP64-accumulated build
-                              and the variational energy absorb) */
+  double mixed_density_tol;/* density-weighted threshold of mixed-precision Delta-D builds (hfgpu_fock_delta
+                              with HFGPU_MIXED; default 1e-12 as for full builds: a looser 1e-10 made the
+                              incremental SCF of n-octane take 44 iterations instead of 24) */
   int device;              /* CUDA device ordinal (default 0) */
   int warp_max_quartets;   /* (dd|dp), (dd|dd): one warp per quartet when the class has at most this many
                               quartets, one thread per quartet otherwise (default 2^30 = always; -1 = never) */
@@ -181,6 +181,22 @@ int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out);
 int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms);
 int hfgpu_last_launches(const hfgpu_handle* h, int* kernels);
 int hfgpu_fp64_peak(int device, double* tflops);
+
+/* Launch schedule of the J/K build (no reference counterpart: the reference has one CPU
+ * code path).  Three ints per quartet class, HFGPU_NUM_CLASSES classes in the order of
+ * hfgpu_class_stats: threads per block of the thread-per-quartet form (32, 64, 128),
+ * 1/0 = warp-over-primitives form for quartets with many primitive quartets (classes
+ * without that form ignore it), 1/0/-1 = warp-per-quartet form for the classes that have
+ * one, (dp|pp) (dp|ds) (dp|dp) (dd|pp) (dd|ds) (dd|dp) (dd|dd) (-1 = follow
+ * opts.warp_max_quartets).  Default: 64, 1, and -1 for (dd|dp), (dd|dd), 0 otherwise.
+ * autotune: times every form of every class on the current geometry with device density D
+ * (n x n; `repeats` builds per candidate, one class at a time on the handle's stream),
+ * keeps the fastest and returns the schedule in `schedule` (may be NULL).  Results of later
+ * builds do not depend on the schedule beyond FP64 summation order. */
+#define HFGPU_NUM_CLASSES 21
+int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule);
+int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule);
+int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,84 @@
+"""Launch schedule and autotuner: every launch form of every quartet class gives the
+oracle's ERIs, J and K, and an autotuned schedule changes nothing but speed.
+
+Tolerances as in test_gpu_parity: ERIs 1e-11, J/K 1e-10 absolute (FP64).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from hfscf_b200 import basis as B
+from hfscf_b200 import engine as E
+from hfscf_b200 import molecules as M
+
+pytestmark = pytest.mark.gpu
+
+ERI_TOL = 1e-11
+MAT_TOL = 1e-10
+
+
+def _sym(rng, n):
+    A = rng.normal(size=(n, n))
+    return (A + A.T) / n
+
+
+def _molecules():
+    rng = np.random.default_rng(23)
+    Z, x = M.water(rng)
+    h2o = B.build_basis("6-31g**", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    Z, x = M.methane()
+    x = np.asarray(x) * B.ANGSTROM_TO_BOHR + rng.normal(scale=0.05, size=(5, 3))
+    ch4 = B.build_basis("cc-pvdz", Z, x, pure=True)
+    return [("h2o-631gss-cart", h2o), ("ch4-ccpvdz-pure", ch4)]
+
+
+MOLS = _molecules()
+# (block, primwarp, warp) applied to every class
+FORMS = [(32, 0, 0), (64, 1, 0), (128, 0, 1), (64, 1, 1)]
+
+
+@pytest.mark.parametrize("form", FORMS, ids=[f"b{f[0]}-pw{f[1]}-w{f[2]}" for f in FORMS])
+@pytest.mark.parametrize("name,bs", MOLS, ids=[m[0] for m in MOLS])
+def test_every_launch_form_matches_oracle(name, bs, form):
+    rng = np.random.default_rng(29)
+    D = _sym(rng, bs.nbf)
+    eri0 = oracle.eri_packed(bs)
+    J0, K0 = oracle.jk(eri0, D)
+    with E.Engine(bs, density_tol=0.0) as eng:
+        eng.set_schedule(np.tile(np.array(form, dtype=np.int32), (E.NUM_CLASSES, 1)))
+        assert (eng.get_schedule() == np.array(form)).all()
+        eri = eng.eri_packed()
+        J, K = eng.jk(D, [D])
+    assert np.max(np.abs(eri - eri0)) < ERI_TOL
+    assert np.max(np.abs(J - J0)) < MAT_TOL and np.max(np.abs(K[0] - K0)) < MAT_TOL
+
+
+def test_set_schedule_rejects_bad_entries():
+    bs = MOLS[0][1]
+    with E.Engine(bs) as eng:
+        before = eng.get_schedule()
+        bad = before.copy()
+        bad[3, 0] = 48
+        with pytest.raises(E.HfgpuError):
+            eng.set_schedule(bad)
+        assert (eng.get_schedule() == before).all()
+
+
+def test_autotuned_schedule_gives_the_same_fock_build():
+    Z, x = M.water_cluster(2, 2.9, np.random.default_rng(31), 0.1)
+    bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    rng = np.random.default_rng(37)
+    D = _sym(rng, bs.nbf)
+    H = _sym(rng, bs.nbf)
+    with E.Engine(bs) as eng:
+        F0 = eng.fock_rhf(D, H)
+        Fm0 = eng.fock_rhf(D, H, E.MIXED)
+        sched = eng.autotune(D, repeats=2)
+        assert sched.shape == (E.NUM_CLASSES, 3)
+        assert set(np.unique(sched[:, 0])) <= {32, 64, 128}
+        assert set(np.unique(sched[:, 1])) <= {0, 1} and set(np.unique(sched[:, 2])) <= {-1, 0, 1}
+        assert (eng.get_schedule() == sched).all()
+        F1 = eng.fock_rhf(D, H)
+        Fm1 = eng.fock_rhf(D, H, E.MIXED)
+    assert np.max(np.abs(F1 - F0)) < 1e-11
+    assert np.max(np.abs(Fm1 - Fm0)) < 1e-6
