@@ -8,7 +8,8 @@ diagonalisations run on a host thread pool over the unpadded blocks.  The J/K bu
 as a CUDA graph and replayed every iteration.  After convergence, the
 two-electron gradient of every molecule comes from one batched adjoint launch
 (hfgpu_batch_grad2e_device); one-electron and nuclear terms are added per
-molecule on the host.
+molecule on the host.  Before the graph is captured, hfgpu_autotune picks each
+quartet class's launch form on the batch's first density.
 
 The SCF is the caller side, as in scf.py: symmetric orthogonalisation, D =
 C_occ C_occ^T (no factor 2), E = sum D (H + F), DIIS on the orthogonalised
@@ -69,6 +70,13 @@ class BatchEngine:
         self._check(eng.lib().hfgpu_batch_jk_device(self.h, ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(J.data_ptr()),
                                                     ctypes.c_void_p(K.data_ptr()), ctypes.c_int(precision)))
 
+    def autotune(self, D, precision=eng.FP64, repeats=2):
+        """hfgpu_autotune on the batched handle (D in block storage, on the device)."""
+        out = np.zeros((eng.NUM_CLASSES, 3), dtype=np.int32)
+        self._check(eng.lib().hfgpu_autotune(self.h, ctypes.c_void_p(D.data_ptr()), ctypes.c_int(precision),
+                                             ctypes.c_int(repeats), out.ctypes.data_as(eng._ip)))
+        return out
+
     def grad2e_device(self, D, grad, precision=eng.FP64):
         self._check(eng.lib().hfgpu_batch_grad2e_device(self.h, ctypes.c_void_p(D.data_ptr()),
                                                         ctypes.c_void_p(grad.data_ptr()), ctypes.c_int(precision)))
@@ -116,7 +124,7 @@ class _Layout:
 
 
 def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-10, rms_tol=1e-8,
-              max_iter=60, use_graph=True, gradient=True):
+              max_iter=60, use_graph=True, gradient=True, autotune=True):
     """Converged RHF energies (and gradients) of every molecule of the batch."""
     dev = torch.device("cuda", device)
     t0 = time.perf_counter()
@@ -177,6 +185,7 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
 
     build()  # warm-up: loads every kernel before any capture
     torch.cuda.synchronize()
+    schedule = be.autotune(Dblk, precision) if autotune else None
     graph = None
     if use_graph:
         try:
@@ -240,7 +249,7 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     E_el = (Dz * (lay.to_pad(Hblk) + F)).sum(dim=(1, 2)).cpu().numpy()
     enuc = np.array([nuclear_repulsion(b.Z, b.coords) for b in bases])
     out = {"energies": E_el + enuc, "iterations": it, "converged": converged.cpu().numpy(),
-           "setup_s": t_setup, "scf_s": t_scf, "graph": graph is not None,
+           "setup_s": t_setup, "scf_s": t_scf, "graph": graph is not None, "autotuned": schedule is not None,
            "build_ms_mean": 1e3 * float(np.mean(build_times)), "nmol": nmol}
     if gradient:
         t2 = time.perf_counter()

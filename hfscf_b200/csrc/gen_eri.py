@@ -913,6 +913,43 @@ def linear_scan(n_values, uses_per_op, defs_per_op, preassigned):
     return slot, top
 
 
+def _u16(x):
+    assert 0 <= x < 65536, x
+    return x
+
+
+def _i32(u):
+    """A 32-bit pattern as a C int literal."""
+    u &= 0xFFFFFFFF
+    return u - (1 << 32) if u >= (1 << 31) else u
+
+
+def pack_grad_vrr(r):
+    kind, i, dst, sa, sb, sc, sd, sg, k1, k2 = r
+    assert 0 <= kind < 16 and 0 <= i < 16 and 0 <= k1 < 256 and 0 <= k2 < 256
+    return (_i32(_u16(dst) | _u16(sa) << 16), _i32(_u16(sb) | _u16(sc) << 16), _i32(_u16(sd) | _u16(sg) << 16),
+            _i32(kind | i << 4 | k1 << 8 | k2 << 16))
+
+
+def pack_grad_hrr(r):
+    kind, i, dst, x, y, kk = r[:6]
+    assert 0 <= kind < 16 and 0 <= i < 16 and 0 <= kk < 128 and y < 65536
+    return (_i32(_u16(dst) | _u16(x) << 16), _i32(_u16(y) | kind << 16 | i << 20 | kk << 24))
+
+
+def pack_warp_vrr(r):
+    kd, dst, sa, sb, sc, sd, sg, k12 = r
+    assert 0 <= kd < 256 and 0 <= k12 < (1 << 16)
+    return (_i32(_u16(dst) | _u16(sa) << 16), _i32(_u16(sb) | _u16(sc) << 16), _i32(_u16(sd) | _u16(sg) << 16),
+            _i32(kd | k12 << 8))
+
+
+def pack_warp_hrr(r):
+    kd, dst, x, y = r
+    assert 0 <= kd < (1 << 15)
+    return (_i32(_u16(dst) | _u16(x) << 16), _i32(_u16(y) | kd << 16))
+
+
 def gen_grad_table(la, lb, lc, ld):
     L = la + lb + lc + ld + 1
     order = grad_sets(la, lb, lc, ld)
@@ -1033,16 +1070,19 @@ def gen_grad_table(la, lb, lc, ld):
     tagc = f"{la}{lb}{lc}{ld}"
     s = [f"// table-mode adjoint gradient of class {tagc}: {len(vrr_rows)} VRR ops over {nvslot} slots, "
          f"{nacc} accumulators, {len(hrows)} HRR/contraction ops over {nhslot} slots"]
-    s.append(f"__device__ const int gvrr_{tagc}[{len(vrr_rows)}][10] = {{")
-    s += ["  {" + ",".join(map(str, r)) + "}," for r in vrr_rows]
+    # one 16-byte row per VRR op and one 8-byte row per HRR op (a single vector load each):
+    # VRR {dst | sa<<16, sb | sc<<16, sd | sg<<16, kind | dir<<4 | k1<<8 | k2<<16}
+    # HRR {dst | x<<16, y | kind<<16 | dir<<20 | k<<24}
+    s.append(f"__device__ const int4 gvrr_{tagc}[{len(vrr_rows)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_grad_vrr(r))) + "}," for r in vrr_rows]
     s.append("};")
-    s.append(f"__device__ const int ghrr_{tagc}[{len(hrows)}][8] = {{")
-    s += ["  {" + ",".join(map(str, r)) + "}," for r in hrows]
+    s.append(f"__device__ const int2 ghrr_{tagc}[{len(hrows)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_grad_hrr(r))) + "}," for r in hrows]
     s.append("};")
     s.append(f"struct GradTable{tagc} {{ static constexpr int L = {L}, NVOPS = {len(vrr_rows)}, NVSLOT = {nvslot}, "
              f"NACC = {nacc}, NHOPS = {len(hrows)}, NHSLOT = {nhslot}; "
-             f"static __device__ const int (*vrr())[10] {{ return gvrr_{tagc}; }} "
-             f"static __device__ const int (*hrr())[8] {{ return ghrr_{tagc}; }} }};")
+             f"static __device__ const int4* vrr() {{ return gvrr_{tagc}; }} "
+             f"static __device__ const int2* hrr() {{ return ghrr_{tagc}; }} }};")
     flops = sum(3 + (3 if r[8] else 0) + (2 if r[9] else 0) for r in vrr_rows if r[0] < 2) + \
         2 * sum(1 for r in vrr_rows if r[0] == 2)
     hfl = sum(2 if r[0] < 2 else 4 for r in hrows)
@@ -1196,22 +1236,23 @@ def gen_warp_class(la, lb, lc, ld):
     ncart_blk = len(outs)
     s = [f"// warp-mode J/K of class {t}: {len(vrows)} VRR ops in {len(vlev) - 1} levels over {nvs} slots, "
          f"{nacc} accumulators, {len(hrows)} HRR ops in {len(hlv) - 1} levels over {nhs} slots"]
-    s.append(f"__device__ const int wvrr_{t}[{max(len(vrows), 1)}][8] = {{")
-    s += ["  {" + ",".join(map(str, r)) + "}," for r in vrows]
+    # VRR row {dst | sa<<16, sb | sc<<16, sd | sg<<16, kd | k12<<8}; HRR row {dst | x<<16, y | kd<<16}
+    s.append(f"__device__ const int4 wvrr_{t}[{max(len(vrows), 1)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_warp_vrr(r))) + "}," for r in vrows]
     s.append("};")
     s.append(f"__device__ const int wvrr_lv_{t}[{len(vlev)}] = {{{','.join(map(str, vlev))}}};")
     s.append(f"__device__ const int wacc_{t}[{nacc}] = {{{','.join(map(str, acc_rows))}}};")
-    s.append(f"__device__ const int whrr_{t}[{max(len(hrows), 1)}][4] = {{")
-    s += ["  {" + ",".join(map(str, r)) + "}," for r in hrows] or ["  {0,0,0,0},"]
+    s.append(f"__device__ const int2 whrr_{t}[{max(len(hrows), 1)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_warp_hrr(r))) + "}," for r in hrows] or ["  {0,0},"]
     s.append("};")
     s.append(f"__device__ const int whrr_lv_{t}[{len(hlv)}] = {{{','.join(map(str, hlv))}}};")
     s.append(f"__device__ const int wout_{t}[{ncart_blk}] = {{{','.join(map(str, wout))}}};")
     s.append(f"struct WarpTab{t} {{ static constexpr int L = {L}, NVLEV = {len(vlev) - 1}, NVSLOT = {nvs}, "
              f"NACC = {nacc}, NHLEV = {len(hlv) - 1}, NHSLOT = {nhs}, NCART = {ncart_blk}; "
-             f"static __device__ const int (*vrr())[8] {{ return wvrr_{t}; }} "
+             f"static __device__ const int4* vrr() {{ return wvrr_{t}; }} "
              f"static __device__ const int* vlev() {{ return wvrr_lv_{t}; }} "
              f"static __device__ const int* acc() {{ return wacc_{t}; }} "
-             f"static __device__ const int (*hrr())[4] {{ return whrr_{t}; }} "
+             f"static __device__ const int2* hrr() {{ return whrr_{t}; }} "
              f"static __device__ const int* hlev() {{ return whrr_lv_{t}; }} "
              f"static __device__ const int* out() {{ return wout_{t}; }} }};")
     meta = {"class": [la, lb, lc, ld], "vrr_ops": len(vrows), "vrr_levels": len(vlev) - 1, "vrr_slots": nvs,

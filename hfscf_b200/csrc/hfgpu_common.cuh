@@ -60,7 +60,9 @@ __device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
 //   T <  BOYS_TMAX: six-term Taylor expansion of F_M about the nearest grid point
 //                  T_k = k h (h = 0.1), F_M(T) = sum_j F_{M+j}(T_k) (-dT)^j / j!,
 //                  then the stable downward recursion
-//                  F_{m-1} = (2T F_m + e^-T) / (2m - 1);
+//                  F_{m-1} = (2T F_m + e^-T) / (2m - 1), where (FP64) e^-T = e^-T_k e^(T_k - T)
+//                  with e^-T_k tabulated and e^d, |d| <= h/2, from its degree-8 Taylor
+//                  polynomial (remainder below (h/2)^9 / 9! = 5e-18 relative);
 //   T >= BOYS_TMAX: F_0 = sqrt(pi/T)/2 (erf(sqrt T) = 1 to double precision there)
 //                  and the upward recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T).
 // The table F_m(T_k) is computed on the host from the convergent series
@@ -73,7 +75,7 @@ __device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
 
 template <typename R>
 struct BoysTable {
-  const R* __restrict__ tab;  // [BOYS_NGRID][BOYS_NM]
+  const R* __restrict__ tab;  // [BOYS_NGRID][BOYS_NM], then e^-T_k [BOYS_NGRID]
 
   template <int M>
   __device__ __forceinline__ void eval(R T, R pre, R* F) const {
@@ -98,7 +100,21 @@ struct BoysTable {
       }
       F[M] = f;
       if constexpr (M > 0) {
-        const R e = exp_t<R>(-T);
+        R e;
+        if constexpr (sizeof(R) == 8) {
+          R x = R(1.0 / 40320.0);
+          x = R(1.0 / 5040.0) + d * x;
+          x = R(1.0 / 720.0) + d * x;
+          x = R(1.0 / 120.0) + d * x;
+          x = R(1.0 / 24.0) + d * x;
+          x = R(1.0 / 6.0) + d * x;
+          x = R(0.5) + d * x;
+          x = R(1.0) + d * x;
+          x = R(1.0) + d * x;
+          e = tab[BOYS_NGRID * BOYS_NM + k] * x;
+        } else {
+          e = exp_t<R>(-T);
+        }
         const R t2 = T + T;
 #pragma unroll
         for (int m = M; m > 0; --m) F[m - 1] = (t2 * F[m] + e) * R(1.0 / (2 * m - 1));

@@ -26,8 +26,9 @@ int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }  // la >= lb: 
 int quartet_class(int cp, int cq) { return cp * (cp + 1) / 2 + cq; }  // cp >= cq
 
 // Boys table F_m(k h), m < BOYS_NM, from the series e^-T sum_i (2T)^i / (2m+1)(2m+3)...(2m+2i+1).
+// After the table: e^-T_k for k < BOYS_NGRID.
 std::vector<double> boys_table() {
-  std::vector<double> t((size_t)BOYS_NGRID * BOYS_NM);
+  std::vector<double> t((size_t)BOYS_NGRID * BOYS_NM + BOYS_NGRID);
   for (int k = 0; k < BOYS_NGRID; ++k) {
     const long double T = (long double)k * (long double)BOYS_H;
     for (int m = 0; m < BOYS_NM; ++m) {
@@ -39,6 +40,7 @@ std::vector<double> boys_table() {
       }
       t[(size_t)k * BOYS_NM + m] = (double)(expl(-T) * sum);
     }
+    t[(size_t)BOYS_NGRID * BOYS_NM + k] = (double)expl(-T);
   }
   return t;
 }
@@ -219,8 +221,9 @@ int build_pairs(hfgpu_handle* h) {
       for (int j = 0; j < h->nprim[t.sb]; ++j) {
         const double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
         const double p = a1 + a2;
-        const double kp = std::fabs(std::exp(-a1 * a2 / p * R2) * h->coefs[h->prim_off[t.sa] + i] *
-                                    h->coefs[h->prim_off[t.sb] + j]) * std::sqrt(PI_2_5) / p;
+        const double fold = (t.sa == t.sb && i != j) ? 2.0 : 1.0;  // see the folding below
+        const double kp = fold * std::fabs(std::exp(-a1 * a2 / p * R2) * h->coefs[h->prim_off[t.sa] + i] *
+                                           h->coefs[h->prim_off[t.sb] + j]) * std::sqrt(PI_2_5) / p;
         kp_max = std::max(kp_max, kp);
         p_min = std::min(p_min, p);
       }
@@ -250,12 +253,18 @@ int build_pairs(hfgpu_handle* h) {
     P.ABz = A[2] - B[2];
     const double R2 = P.ABx * P.ABx + P.ABy * P.ABy + P.ABz * P.ABz;
     P.prim_off = (int)pd.size();
+    // A pair of a shell with itself has A = B, so primitive pairs (i, j) and (j, i) have the
+    // same p, P, PA and K: they are stored once, j >= i, with K doubled for j > i.  For the
+    // gradient both exponent weights become (a_i + a_j)/2: the A and B derivatives then
+    // have the right sum, which is all that reaches the atom the two centres share.
+    const bool self = t.sa == t.sb;
     for (int i = 0; i < h->nprim[t.sa]; ++i)
-      for (int j = 0; j < h->nprim[t.sb]; ++j) {
-        const double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
+      for (int j = self ? i : 0; j < h->nprim[t.sb]; ++j) {
+        double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
         const double c1 = h->coefs[h->prim_off[t.sa] + i], c2 = h->coefs[h->prim_off[t.sb] + j];
         const double p = a1 + a2;
-        const double K = std::exp(-a1 * a2 / p * R2) * c1 * c2;
+        const double K = std::exp(-a1 * a2 / p * R2) * c1 * c2 * (self && j > i ? 2.0 : 1.0);
+        if (self && j > i) a1 = a2 = 0.5 * p;
         if (std::fabs(K) * std::sqrt(PI_2_5) / p < kp_cut) continue;
         PrimPair<double> q;
         q.p = p;
@@ -1340,6 +1349,8 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
       cudaEventDestroy(b);
     }
   } restore{h, h->class_mask, e0, e1};
+  int start[3 * 21];
+  hfgpu_get_schedule(h, start);
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     if (h->q_end[c] <= h->q_beg[c]) continue;
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
@@ -1376,6 +1387,26 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
     h->sched_primwarp[c] = bp;
     h->sched_warp[c] = bw;
   }
+  // Classes were timed one at a time; in a build they run concurrently.  Keep the tuned
+  // schedule only if a whole build with it beats one with the schedule we started from.
+  h->class_mask = restore.mask;
+  int tuned[3 * 21];
+  hfgpu_get_schedule(h, tuned);
+  float t_tuned = 0.f, t_start = 0.f;
+  for (int round = 0; round < 2; ++round)
+    for (int which = 0; which < 2; ++which) {
+      if ((rc = hfgpu_set_schedule(h, which ? start : tuned))) return rc;
+      if ((rc = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return rc;  // warm-up
+      HF_CUDA(h, cudaEventRecord(e0, h->stream));
+      for (int r = 0; r < repeats; ++r)
+        if ((rc = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return rc;
+      HF_CUDA(h, cudaEventRecord(e1, h->stream));
+      HF_CUDA(h, cudaEventSynchronize(e1));
+      float ms = 0.f;
+      HF_CUDA(h, cudaEventElapsedTime(&ms, e0, e1));
+      (which ? t_start : t_tuned) += ms;
+    }
+  if ((rc = hfgpu_set_schedule(h, t_tuned <= t_start ? tuned : start))) return rc;
   return schedule ? hfgpu_get_schedule(h, schedule) : HFGPU_OK;
 }
 

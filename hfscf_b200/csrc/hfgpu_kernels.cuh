@@ -378,8 +378,8 @@ __device__ void grad_table(const PrimPair<R>* __restrict__ bp, const R* __restri
   vs[0] = R(0);
   hs[0] = R(0);
   for (int x = 1; x <= Tab::NACC; ++x) hs[x] = R(0);
-  const int(*vo)[10] = Tab::vrr();
-  const int(*ho)[8] = Tab::hrr();
+  const int4* vo = Tab::vrr();  // packed rows, see gen_eri.py pack_grad_vrr / pack_grad_hrr
+  const int2* ho = Tab::hrr();
   for (int ib = 0; ib < nbp; ++ib) {
     const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;
     const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;
@@ -402,21 +402,22 @@ __device__ void grad_table(const PrimPair<R>* __restrict__ bp, const R* __restri
 #pragma unroll
       for (int m = 0; m <= Tab::L; ++m) vs[1 + m] = F[m];
       for (int o = 0; o < Tab::NVOPS; ++o) {
-        const int kind = __ldg(&vo[o][0]), dir = __ldg(&vo[o][1]), dst = __ldg(&vo[o][2]);
-        const int sa = __ldg(&vo[o][3]), sb = __ldg(&vo[o][4]), sc = __ldg(&vo[o][5]), sd = __ldg(&vo[o][6]);
+        const int4 op = __ldg(vo + o);
+        const int kind = op.w & 15, dir = (op.w >> 4) & 15, dst = op.x & 0xffff;
+        const int sa = (unsigned)op.x >> 16, sb = op.y & 0xffff, sc = (unsigned)op.y >> 16, sd = op.z & 0xffff;
         if (kind == 2) {
           const R w = dir == 0 ? R(1) : (dir == 1 ? wa : (dir == 2 ? wb : wc));
           hs[1 + dst] += w * vs[sa];
           continue;
         }
         const R PQd = dir == 0 ? PQx : (dir == 1 ? PQy : PQz);
-        const int k1 = __ldg(&vo[o][8]);
+        const int k1 = (op.w >> 8) & 255;
         if (kind == 0) {
           const R PA = dir == 0 ? PAx : (dir == 1 ? PAy : PAz);
           vs[dst] = PA * vs[sa] - rp * PQd * vs[sb] + R(k1) * inv2p * (vs[sc] - rp * vs[sd]);
         } else {
           const R QC = dir == 0 ? QCx : (dir == 1 ? QCy : QCz);
-          const int sg = __ldg(&vo[o][7]), k2 = __ldg(&vo[o][9]);
+          const int sg = (unsigned)op.z >> 16, k2 = (unsigned)op.w >> 16;
           vs[dst] = QC * vs[sa] + rq * PQd * vs[sb] + R(k1) * inv2q * (vs[sc] - rq * vs[sd]) + R(k2) * inv2pq * vs[sg];
         }
       }
@@ -425,10 +426,11 @@ __device__ void grad_table(const PrimPair<R>* __restrict__ bp, const R* __restri
 #pragma unroll
   for (int x = 0; x < 9; ++x) g[x] = R(0);
   for (int o = 0; o < Tab::NHOPS; ++o) {
-    const int kind = __ldg(&ho[o][0]), dir = __ldg(&ho[o][1]), dst = __ldg(&ho[o][2]);
-    const int sx = __ldg(&ho[o][3]), sy = __ldg(&ho[o][4]);
+    const int2 op = __ldg(ho + o);
+    const int dst = op.x & 0xffff, sx = (unsigned)op.x >> 16, sy = op.y & 0xffff;
+    const int kind = (op.y >> 16) & 15, dir = (op.y >> 20) & 15;
     if (kind == 2) {
-      const int k = __ldg(&ho[o][5]);
+      const int k = (op.y >> 24) & 127;
       const R v = W[dst] * (hs[sx] - R(k) * hs[sy]);
 #pragma unroll
       for (int x = 0; x < 9; ++x)
@@ -706,7 +708,7 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
   __syncwarp();
   const PrimPair<R>* bp = a.prims + P.prim_off;
   const PrimPair<R>* kp = a.prims + Q.prim_off;
-  const int(*vo)[8] = Tab::vrr();
+  const int4* vo = Tab::vrr();  // packed rows, see gen_eri.py pack_warp_vrr / pack_warp_hrr
   const int* vl = Tab::vlev();
   const int* accs = Tab::acc();
   for (int ib = 0; ib < P.nprim; ++ib) {
@@ -732,9 +734,9 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
       for (int l = 0; l < Tab::NVLEV; ++l) {
         const int e = __ldg(vl + l + 1);
         for (int o = __ldg(vl + l) + lane; o < e; o += 32) {
-          const int kd = __ldg(&vo[o][0]), dst = __ldg(&vo[o][1]);
-          const int sa = __ldg(&vo[o][2]), sb = __ldg(&vo[o][3]), sc = __ldg(&vo[o][4]), sd = __ldg(&vo[o][5]);
-          const int k12 = __ldg(&vo[o][7]);
+          const int4 op = __ldg(vo + o);
+          const int dst = op.x & 0xffff, sa = (unsigned)op.x >> 16, sb = op.y & 0xffff, sc = (unsigned)op.y >> 16;
+          const int sd = op.z & 0xffff, kd = op.w & 255, k12 = (unsigned)op.w >> 8;
           const int dir = kd >> 2;
           const R PQd = dir == 0 ? PQx : (dir == 1 ? PQy : PQz);
           const R k1 = R(k12 & 255);
@@ -744,7 +746,7 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
             v = PA * vs[sa] - rp * PQd * vs[sb] + k1 * inv2p * (vs[sc] - rp * vs[sd]);
           } else {
             const R QC = dir == 0 ? QCx : (dir == 1 ? QCy : QCz);
-            const int sg = __ldg(&vo[o][6]);
+            const int sg = (unsigned)op.z >> 16;
             v = QC * vs[sa] + rq * PQd * vs[sb] + k1 * inv2q * (vs[sc] - rq * vs[sd]) + R(k12 >> 8) * inv2pq * vs[sg];
           }
           vs[dst] = v;
@@ -755,15 +757,16 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
       __syncwarp();
     }
   }
-  const int(*ho)[4] = Tab::hrr();
+  const int2* ho = Tab::hrr();
   const int* hl = Tab::hlev();
   const R ABx = R(P.ABx), ABy = R(P.ABy), ABz = R(P.ABz), CDx = R(Q.ABx), CDy = R(Q.ABy), CDz = R(Q.ABz);
   for (int l = 0; l < Tab::NHLEV; ++l) {
     const int e = __ldg(hl + l + 1);
     for (int o = __ldg(hl + l) + lane; o < e; o += 32) {
-      const int kd = __ldg(&ho[o][0]), dir = kd >> 2;
+      const int2 op = __ldg(ho + o);
+      const int kd = (unsigned)op.y >> 16, dir = kd >> 2;
       const R d = (kd & 1) ? (dir == 0 ? CDx : (dir == 1 ? CDy : CDz)) : (dir == 0 ? ABx : (dir == 1 ? ABy : ABz));
-      hs[__ldg(&ho[o][1])] = hs[__ldg(&ho[o][2])] + d * hs[__ldg(&ho[o][3])];
+      hs[op.x & 0xffff] = hs[(unsigned)op.x >> 16] + d * hs[op.y & 0xffff];
     }
     __syncwarp();
   }

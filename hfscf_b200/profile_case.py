@@ -5,7 +5,8 @@
 
 Builds the named workload's basis (``molecules.workload``: 1 = H2O/cc-pVDZ,
 2 = n-octane/6-31G**, 3 = anthracene/cc-pVDZ, 4 = (H2O)8/6-31G*), forms the
-core-guess density, runs one untimed warm-up of the operation and then
+core-guess density (and with ``--autotune`` tunes the launch schedule on it),
+runs one untimed warm-up of the operation and then
 ``--repeat`` timed ones between ``cudaProfilerStart``/``cudaProfilerStop`` (so
 ``ncu --profile-from-start off`` sees exactly those launches).  Prints one JSON
 line with the per-call device time and the kernel count of each call.
@@ -39,6 +40,7 @@ def main(argv=None):
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--autotune", action="store_true", help="hfgpu_autotune first (as bench.py does)")
     a = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("profile_case needs a CUDA device")
@@ -53,6 +55,8 @@ def main(argv=None):
     with E.Engine(bs, device=a.device) as eng:
         eng.set_stream(stream.cuda_stream)
         Dd = torch.from_numpy(np.ascontiguousarray(D)).to(dev)
+        if a.autotune:
+            eng.autotune(Dd, E.FP64, 3)
         n = bs.nbf
         J = torch.empty((n, n), dtype=torch.float64, device=dev)
         K = torch.empty((n, n), dtype=torch.float64, device=dev)

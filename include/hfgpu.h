@@ -191,7 +191,8 @@ int hfgpu_fp64_peak(int device, double* tflops);
  * opts.warp_max_quartets).  Default: 64, 1, and -1 for (dd|dp), (dd|dd), 0 otherwise.
  * autotune: times every form of every class on the current geometry with device density D
  * (n x n; `repeats` builds per candidate, one class at a time on the handle's stream),
- * keeps the fastest and returns the schedule in `schedule` (may be NULL).  Results of later
+ * keeps the fastest, then keeps the result only if whole builds with it beat whole builds
+ * with the schedule it started from, and returns the schedule in `schedule` (may be NULL).  Results of later
  * builds do not depend on the schedule beyond FP64 summation order. */
 #define HFGPU_NUM_CLASSES 21
 int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule);
