@@ -103,7 +103,8 @@ struct hfgpu_handle {
   // [beg, hik1) and [mid, hik2) run the warp-over-primitives kernel where the class has one
   std::vector<long long> q_beg, q_mid, q_end, q_hik1, q_hik2;
   // inside each of the four segments quartets are ordered by Schwarz-bound decade
-  // (largest first, bra-major inside a decade): bucket_end[(c * 4 + seg) * kBuckets + e] is the
+  // (largest first; inside a decade by primitive-quartet count, then bra-major):
+  // bucket_end[(c * 4 + seg) * kBuckets + e] is the
   // end of decade e (bound in [10^-e, 10^(1-e)), e = 0 collects bounds >= 1)
   std::vector<long long> bucket_end;
   DevBuf d_gmax;
@@ -419,6 +420,16 @@ int build_quartets(hfgpu_handle* h) {
         }
         all.resize(acc);
         for (size_t x = 0; x < parts[sg].size(); ++x) all[pos[dec[x]]++] = parts[sg][x];
+        // inside a decade: by primitive-quartet count, largest first (stable, so bra-major
+        // within equal counts), so that the 32 lanes of a warp loop over similar counts
+        for (int e = 0; e < kBuckets; ++e) {
+          const long long lo = e == 0 ? *seg_start[sg] : h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e - 1];
+          const long long hi = h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e];
+          if (hi - lo > 1)
+            std::stable_sort(all.begin() + lo, all.begin() + hi, [h](const int2& u, const int2& v) {
+              return h->pairs[u.x].nprim * h->pairs[u.y].nprim > h->pairs[v.x].nprim * h->pairs[v.y].nprim;
+            });
+        }
       }
       h->q_end[qc] = (long long)all.size();
     }
