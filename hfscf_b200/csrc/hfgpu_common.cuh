@@ -39,6 +39,20 @@ template <>
 __device__ __forceinline__ double sqrt_t<double>(double x) { return sqrt(x); }
 template <>
 __device__ __forceinline__ float sqrt_t<float>(float x) { return sqrtf(x); }
+// Exact value of a small non-negative int (0 <= k < 2^22) without an int -> float
+// conversion instruction (those issue on the narrow XU pipe): k is written into the low
+// mantissa bits of 1.5 * 2^52 (1.5 * 2^23 in FP32) and the offset subtracted.
+template <typename R>
+__device__ __forceinline__ R small_int(int k);
+template <>
+__device__ __forceinline__ double small_int<double>(int k) {
+  return __hiloint2double(0x43380000, k) - 6755399441055744.0;
+}
+template <>
+__device__ __forceinline__ float small_int<float>(int k) {
+  return __int_as_float(0x4B400000 | k) - 12582912.0f;
+}
+
 template <typename R>
 __device__ __forceinline__ R exp_t(R x);
 template <>
@@ -80,8 +94,18 @@ struct BoysTable {
   template <int M>
   __device__ __forceinline__ void eval(R T, R pre, R* F) const {
     if (T < R(BOYS_TMAX)) {
-      const int k = __float2int_rn(float(T * R(10)));
-      const R d = R(k) * R(BOYS_H) - T;  // -(T - T_k)
+      int k;
+      R d;  // -(T - T_k)
+      if constexpr (sizeof(R) == 8) {
+        // nearest grid index without int/float conversions (they go through the narrow XU
+        // pipe): adding 1.5 * 2^52 leaves round(T / h) in the low mantissa bits
+        const double sh = T * 10.0 + 6755399441055744.0;
+        k = __double2loint(sh);
+        d = (sh - 6755399441055744.0) * BOYS_H - T;
+      } else {
+        k = __float2int_rn(T * R(10));
+        d = R(k) * R(BOYS_H) - T;
+      }
       const R* row = tab + k * BOYS_NM + M;
       R f;
       if constexpr (sizeof(R) == 8) {

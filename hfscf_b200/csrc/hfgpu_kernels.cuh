@@ -414,11 +414,12 @@ __device__ void grad_table(const PrimPair<R>* __restrict__ bp, const R* __restri
         const int k1 = (op.w >> 8) & 255;
         if (kind == 0) {
           const R PA = dir == 0 ? PAx : (dir == 1 ? PAy : PAz);
-          vs[dst] = PA * vs[sa] - rp * PQd * vs[sb] + R(k1) * inv2p * (vs[sc] - rp * vs[sd]);
+          vs[dst] = PA * vs[sa] - rp * PQd * vs[sb] + small_int<R>(k1) * inv2p * (vs[sc] - rp * vs[sd]);
         } else {
           const R QC = dir == 0 ? QCx : (dir == 1 ? QCy : QCz);
           const int sg = (unsigned)op.z >> 16, k2 = (unsigned)op.w >> 16;
-          vs[dst] = QC * vs[sa] + rq * PQd * vs[sb] + R(k1) * inv2q * (vs[sc] - rq * vs[sd]) + R(k2) * inv2pq * vs[sg];
+          vs[dst] = QC * vs[sa] + rq * PQd * vs[sb] + small_int<R>(k1) * inv2q * (vs[sc] - rq * vs[sd]) +
+                    small_int<R>(k2) * inv2pq * vs[sg];
         }
       }
     }
@@ -431,7 +432,7 @@ __device__ void grad_table(const PrimPair<R>* __restrict__ bp, const R* __restri
     const int kind = (op.y >> 16) & 15, dir = (op.y >> 20) & 15;
     if (kind == 2) {
       const int k = (op.y >> 24) & 127;
-      const R v = W[dst] * (hs[sx] - R(k) * hs[sy]);
+      const R v = W[dst] * (hs[sx] - small_int<R>(k) * hs[sy]);
 #pragma unroll
       for (int x = 0; x < 9; ++x)
         if (x == dir) g[x] += v;
@@ -739,7 +740,7 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
           const int sd = op.z & 0xffff, kd = op.w & 255, k12 = (unsigned)op.w >> 8;
           const int dir = kd >> 2;
           const R PQd = dir == 0 ? PQx : (dir == 1 ? PQy : PQz);
-          const R k1 = R(k12 & 255);
+          const R k1 = small_int<R>(k12 & 255);
           R v;
           if ((kd & 1) == 0) {
             const R PA = dir == 0 ? PAx : (dir == 1 ? PAy : PAz);
@@ -747,7 +748,7 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
           } else {
             const R QC = dir == 0 ? QCx : (dir == 1 ? QCy : QCz);
             const int sg = (unsigned)op.z >> 16;
-            v = QC * vs[sa] + rq * PQd * vs[sb] + k1 * inv2q * (vs[sc] - rq * vs[sd]) + R(k12 >> 8) * inv2pq * vs[sg];
+            v = QC * vs[sa] + rq * PQd * vs[sb] + k1 * inv2q * (vs[sc] - rq * vs[sd]) + small_int<R>(k12 >> 8) * inv2pq * vs[sg];
           }
           vs[dst] = v;
         }
