@@ -262,9 +262,10 @@ PRIMWARP_MAX_VRR = 150   # classes that also get a warp-over-primitives variant
 
 
 def gen_eri_primwarp(la, lb, lc, ld):
-    """Same integral block as gen_eri_class, for one warp: the lanes split the
-    primitive quartets, then the accumulators are summed with warp shuffles and
-    every lane runs the HRR (the block is valid in all lanes)."""
+    """Same integral block as gen_eri_class, for a group of G lanes (G = 4 ... 32, aligned
+    inside the warp): the lanes split the primitive quartets, then the accumulators are
+    summed with shuffles inside the group and every lane of it runs the HRR (the block is
+    valid in all G lanes).  Every lane of the warp must call it (full-mask shuffles)."""
     L = la + lb + lc + ld
     em = Emitter("    ")
     vrr = VRR(em)
@@ -276,13 +277,13 @@ def gen_eri_primwarp(la, lb, lc, ld):
     hrr = HRR(em2, lambda e, f: f"acc[{acc_index[(e, f)]}]")
     outs = [hrr.bra(a, b, c, d) for a in cart(la) for b in cart(lb) for c in cart(lc) for d in cart(ld)]
     nt = len(targets)
-    s = [f"template <typename R>",
+    s = [f"template <typename R, int G>",
          f"__device__ __forceinline__ void eri_{la}{lb}{lc}{ld}_pw(const PrimPair<R>* __restrict__ bp, int nbp, "
          f"const PrimPair<R>* __restrict__ kp, int nkp, R ABx, R ABy, R ABz, R CDx, R CDy, R CDz, "
          f"const BoysTable<R>& boys, R* __restrict__ out, int lane) {{",
          f"  R acc[{nt}];", "#pragma unroll", f"  for (int t = 0; t < {nt}; ++t) acc[t] = R(0);",
          "  const int npq = nbp * nkp;",
-         "  for (int x = lane; x < npq; x += 32) {",
+         "  for (int x = lane; x < npq; x += G) {",
          "    const int ib = x / nkp, ik = x - ib * nkp;",
          "    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;",
          "    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;",
@@ -298,7 +299,7 @@ def gen_eri_primwarp(la, lb, lc, ld):
     s.append("#pragma unroll")
     s.append(f"  for (int t = 0; t < {nt}; ++t)")
     s.append("#pragma unroll")
-    s.append("    for (int off = 16; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off);")
+    s.append("    for (int off = G / 2; off > 0; off >>= 1) acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], off, G);")
     s += em2.lines
     for o, nme in enumerate(outs):
         s.append(f"  out[{o}] = {nme};")
@@ -692,9 +693,9 @@ def class_header(c):
     parts.append(f"  using GradTab = {'void' if straight else 'GradTable' + t};")
     parts.append(f"  static constexpr bool kPrimWarp = {'true' if primwarp else 'false'};")
     if primwarp:
-        parts.append(f"  template <typename R>")
+        parts.append(f"  template <typename R, int G>")
         parts.append(f"  static __device__ __forceinline__ void eri_pw({class_args_sig()}, int lane) {{")
-        parts.append(f"    eri_{t}_pw<R>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out, lane);")
+        parts.append(f"    eri_{t}_pw<R, G>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out, lane);")
         parts.append("  }")
     parts.append(f"  template <typename R>")
     parts.append(f"  static __device__ __forceinline__ void eri({class_args_sig()}) {{")
@@ -746,7 +747,13 @@ static void launch_quartet(const QuartetArgs<R>& a, const int2* q, int nq, cudaS
 template <typename CC, typename R>
 static bool launch_primwarp_impl(const QuartetArgs<R>& a, const int2* q, int nq, cudaStream_t s) {{
   if constexpr (CC::kPrimWarp) {{
-    quartet_primwarp_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + 3) / 4, 128, 0, s>>>(a, q, nq);
+    // a.group lanes per quartet, 128-thread blocks
+    switch (a.group) {{
+      case 4: quartet_primwarp_kernel<{la}, {lb}, {lc}, {ld}, R, 4><<<(nq + 31) / 32, 128, 0, s>>>(a, q, nq); break;
+      case 8: quartet_primwarp_kernel<{la}, {lb}, {lc}, {ld}, R, 8><<<(nq + 15) / 16, 128, 0, s>>>(a, q, nq); break;
+      case 16: quartet_primwarp_kernel<{la}, {lb}, {lc}, {ld}, R, 16><<<(nq + 7) / 8, 128, 0, s>>>(a, q, nq); break;
+      default: quartet_primwarp_kernel<{la}, {lb}, {lc}, {ld}, R, 32><<<(nq + 3) / 4, 128, 0, s>>>(a, q, nq); break;
+    }}
     return true;
   }} else {{
     return false;

@@ -130,7 +130,7 @@ struct hfgpu_handle {
   hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21) {
     for (int c = 0; c < 21; ++c) {
       sched_block[c] = 64;
-      sched_primwarp[c] = 1;
+      sched_primwarp[c] = 0;
       sched_warp[c] = c < hfgpu::kNumClasses && hfgpu::kClassLaunchers[c]->warp_default ? -1 : 0;
     }
   }
@@ -364,7 +364,7 @@ int compute_schwarz(hfgpu_handle* h) {
   return HFGPU_OK;
 }
 
-constexpr int kPrimWarpMinPrims = 32;  // primitive quartets per quartet for the warp-over-primitives kernel
+constexpr int kPrimWarpMinPrims = 16;  // primitive quartets per quartet for the primitive-split kernel
 constexpr int kBuckets = 18;           // Schwarz-bound decades of the quartet lists
 
 int bound_decade(double b) {
@@ -650,6 +650,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     qd.jk.counters = cnt + 3 * c;
     qf.jk.counters = cnt + 3 * c;
     qd.block = qf.block = h->sched_block[c];
+    qd.group = qf.group = h->sched_primwarp[c] == 1 ? 32 : h->sched_primwarp[c];
     qd.warp_max = qf.warp_max = class_warp_max(h, c);
     h->ev_used[c] = false;
     if (e <= b || !((h->class_mask >> c) & 1u)) continue;
@@ -1315,7 +1316,8 @@ int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule) {
   if (!h || !schedule) return HFGPU_ERR_INVALID;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     const int bs = schedule[3 * c], pw = schedule[3 * c + 1], wp = schedule[3 * c + 2];
-    if ((bs != 32 && bs != 64 && bs != 128) || (pw != 0 && pw != 1) || wp < -1 || wp > 1)
+    if ((bs != 32 && bs != 64 && bs != 128) || (pw != 0 && pw != 1 && pw != 4 && pw != 8 && pw != 16 && pw != 32) ||
+        wp < -1 || wp > 1)
       return fail(h, HFGPU_ERR_INVALID, "schedule entry out of range");
   }
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
@@ -1371,7 +1373,9 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
     const int warps[2] = {1, 0};
     for (int wi = 0; wi < (L->has_warp ? 2 : 1); ++wi) {
       const int wp = L->has_warp ? warps[wi] : -1;
-      for (int pw = (L->has_primwarp ? 1 : 0); pw >= 0; --pw) {
+      const int pws[5] = {32, 16, 8, 4, 0};
+      for (int pi = (L->has_primwarp ? 0 : 4); pi < 5; ++pi) {
+        const int pw = pws[pi];
         for (int bs : {32, 64, 128}) {
           if (wp == 1 && bs != 64) continue;  // the warp form has its own block shape
           h->sched_block[c] = bs;

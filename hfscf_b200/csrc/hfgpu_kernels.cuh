@@ -237,6 +237,7 @@ struct QuartetArgs {
   PairInfo* pairs_rw;   // SCHWARZ output
   int warp_max;         // large classes: warp per quartet up to this many quartets
   int block;            // threads per block of the thread-per-quartet form (32, 64 or 128; 0 = 64)
+  int group;            // lanes per quartet of the primitive-split form (4, 8, 16 or 32; 0 = 32)
 };
 
 template <int LA, int LB, int LC, int LD, typename R>
@@ -304,39 +305,51 @@ __global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const i
   }
 }
 
-// One warp per quartet of a small class with many primitive quartets: the lanes
-// split the primitive quartets (consecutive ket primitives, one bra primitive per
-// lane group: coalesced and broadcast loads), the accumulators are reduced with
-// shuffles, and lane 0 transforms and digests the block.
-template <int LA, int LB, int LC, int LD, typename R>
+// G lanes per quartet (G = 4, 8, 16 or 32) for small classes and quartets with many
+// primitive quartets: the lanes of a group split the primitive quartets (consecutive ket
+// primitives, one bra primitive per run: coalesced and broadcast loads), the
+// accumulators are reduced with shuffles inside the group, and the group's first lane
+// transforms and digests the block.  Every lane stays to the end: the shuffles take the
+// whole warp.
+template <int LA, int LB, int LC, int LD, typename R, int G>
 __global__ void __launch_bounds__(128) quartet_primwarp_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets,
                                                                int nq) {
+  static_assert(G == 4 || G == 8 || G == 16 || G == 32, "group size");
   const JKArgs<R>& a = qa.jk;
-  const int lane = threadIdx.x & 31;
-  const int qi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (qi >= nq) return;  // whole warp
-  const int2 pq = quartets[qi];
+  const int sub = threadIdx.x & (G - 1);
+  const int qi = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+  const bool in_range = qi < nq;
+  if (!__any_sync(0xffffffffu, in_range)) return;  // whole warp leaves together
+  const int2 pq = in_range ? quartets[qi] : make_int2(0, 0);
   const PairInfo P = a.pairs[pq.x];
   const PairInfo Q = a.pairs[pq.y];
-  bool skip = false;
-  if (qa.mode == QMODE_JK && a.dmax != nullptr) {
+  bool skip = !in_range;
+  if (in_range && qa.mode == QMODE_JK && a.dmax != nullptr) {
     const float* dm = a.dmax;
     const int ns = a.nshell;
     float m = 4.f * fmaxf(dm[P.sa * ns + P.sb], dm[Q.sa * ns + Q.sb]);
     m = fmaxf(m, fmaxf(fmaxf(dm[P.sa * ns + Q.sa], dm[P.sa * ns + Q.sb]), fmaxf(dm[P.sb * ns + Q.sa], dm[P.sb * ns + Q.sb])));
     skip = P.schwarz * Q.schwarz * double(m) < a.dtol;
   }
-  if (a.counters != nullptr && lane == 0) {
-    atomicAdd(a.counters + (skip ? 1 : 0), 1ull);
-    if (!skip) atomicAdd(a.counters + 2, (unsigned long long)(P.nprim * Q.nprim));
+  if (a.counters != nullptr) {
+    // per-class work counters, one atomic per warp (see quartet_kernel)
+    const bool lead = sub == 0;
+    const unsigned nvalid = __popc(__ballot_sync(0xffffffffu, lead && !skip));
+    const unsigned nin = __popc(__ballot_sync(0xffffffffu, lead && in_range));
+    const unsigned prims = __reduce_add_sync(0xffffffffu, (lead && !skip) ? unsigned(P.nprim * Q.nprim) : 0u);
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(a.counters + 0, (unsigned long long)nvalid);
+      atomicAdd(a.counters + 1, (unsigned long long)(nin - nvalid));
+      atomicAdd(a.counters + 2, (unsigned long long)prims);
+    }
   }
-  if (skip) return;
   using Dc = BlockDims<LA, LB, LC, LD, false>;
   R cart[Dc::NCART];
-  ClassCode<LA, LB, LC, LD>::template eri_pw<R>(a.prims + P.prim_off, P.nprim, a.prims + Q.prim_off, Q.nprim,
-                                                 R(P.ABx), R(P.ABy), R(P.ABz), R(Q.ABx), R(Q.ABy), R(Q.ABz), a.boys,
-                                                 cart, lane);
-  if (lane != 0) return;
+  // skipped and out-of-range groups run an empty primitive loop but still take the shuffles
+  ClassCode<LA, LB, LC, LD>::template eri_pw<R, G>(a.prims + P.prim_off, skip ? 0 : P.nprim,
+                                                    a.prims + Q.prim_off, Q.nprim, R(P.ABx), R(P.ABy), R(P.ABz),
+                                                    R(Q.ABx), R(Q.ABy), R(Q.ABz), a.boys, cart, sub);
+  if (skip || sub != 0) return;
   double s = 1.0;
   if (P.sa == P.sb) s *= 0.5;
   if (Q.sa == Q.sb) s *= 0.5;

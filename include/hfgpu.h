@@ -185,10 +185,12 @@ int hfgpu_fp64_peak(int device, double* tflops);
 /* Launch schedule of the J/K build (no reference counterpart: the reference has one CPU
  * code path).  Three ints per quartet class, HFGPU_NUM_CLASSES classes in the order of
  * hfgpu_class_stats: threads per block of the thread-per-quartet form (32, 64, 128),
- * 1/0 = warp-over-primitives form for quartets with many primitive quartets (classes
- * without that form ignore it), 1/0/-1 = warp-per-quartet form for the classes that have
+ * lanes per quartet of the primitive-split form used for quartets with many primitive
+ * quartets (4, 8, 16, 32; 1 = 32; 0 = thread form; classes without that form ignore it),
+ * 1/0/-1 = warp-per-quartet form for the classes that have
  * one, (dp|pp) (dp|ds) (dp|dp) (dd|pp) (dd|ds) (dd|dp) (dd|dd) (-1 = follow
- * opts.warp_max_quartets).  Default: 64, 1, and -1 for (dd|dp), (dd|dd), 0 otherwise.
+ * opts.warp_max_quartets).  Default: 64, 0, and -1 for (dd|dp), (dd|dd), 0 otherwise.
+ * "Many" primitive quartets means at least 16 for the quartet.
  * autotune: times every form of every class on the current geometry with device density D
  * (n x n; `repeats` builds per candidate, one class at a time on the handle's stream),
  * keeps the fastest, then keeps the result only if whole builds with it beat whole builds
