@@ -7,8 +7,9 @@ GPU in torch over matrices padded to the largest molecule; the per-molecule
 diagonalisations run on a host thread pool over the unpadded blocks.  The J/K build and the Fock assembly can be captured once
 as a CUDA graph and replayed every iteration.  After convergence, the
 two-electron gradient of every molecule comes from one batched adjoint launch
-(hfgpu_batch_grad2e_device); one-electron and nuclear terms are added per
-molecule on the host.  Before the graph is captured, hfgpu_autotune picks each
+(hfgpu_batch_grad2e_device) and one for the one-electron part
+(hfgpu_one_electron_grad_device); only the nuclear repulsion term is added on the host.
+S, T and V of every molecule also come from one device launch.  Before the graph is captured, hfgpu_autotune picks each
 quartet class's launch form on the batch's first density.
 
 The SCF is the caller side, as in scf.py: symmetric orthogonalisation, D =
@@ -69,6 +70,19 @@ class BatchEngine:
     def jk_device(self, D, J, K, precision=eng.FP64):
         self._check(eng.lib().hfgpu_batch_jk_device(self.h, ctypes.c_void_p(D.data_ptr()), ctypes.c_void_p(J.data_ptr()),
                                                     ctypes.c_void_p(K.data_ptr()), ctypes.c_int(precision)))
+
+    def one_electron_device(self, S, T, V):
+        """S, T, V of every molecule into block storage (device tensors), on the GPU."""
+        Z = np.ascontiguousarray(np.concatenate([np.asarray(b.Z, dtype=np.float64) for b in self.bases]))
+        self._check(eng.lib().hfgpu_one_electron_device(self.h, eng._p(Z), ctypes.c_void_p(S.data_ptr()),
+                                                        ctypes.c_void_p(T.data_ptr()), ctypes.c_void_p(V.data_ptr())))
+
+    def one_electron_grad_device(self, D, W, cH, cS, grad):
+        """grad (device, total atoms x 3) += cH sum D d(T+V)/dX + cS sum W dS/dX, every molecule."""
+        Z = np.ascontiguousarray(np.concatenate([np.asarray(b.Z, dtype=np.float64) for b in self.bases]))
+        self._check(eng.lib().hfgpu_one_electron_grad_device(self.h, eng._p(Z), ctypes.c_void_p(D.data_ptr()),
+                                                             ctypes.c_void_p(W.data_ptr()), ctypes.c_double(cH),
+                                                             ctypes.c_double(cS), ctypes.c_void_p(grad.data_ptr())))
 
     def autotune(self, D, precision=eng.FP64, repeats=2):
         """hfgpu_autotune on the batched handle (D in block storage, on the device)."""
@@ -134,14 +148,15 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     be.set_stream(stream.cuda_stream)
     lay = _Layout(be.nbf, be.mat_off, dev)
     nmol, nmax = lay.nmol, lay.nmax
-    # one-electron matrices (host) into block storage
-    Sb, Hb = [], []
-    for b in bases:
-        S, T, V = eng.one_electron(b)
-        Sb.append(S.ravel())
-        Hb.append((T + V).ravel())
-    Sblk = torch.from_numpy(np.concatenate(Sb)).to(dev)
-    Hblk = torch.from_numpy(np.concatenate(Hb)).to(dev)
+    # one-electron matrices of every molecule, on the GPU, into block storage
+    Sblk = torch.empty(be.mat_total, dtype=torch.float64, device=dev)
+    Tblk = torch.empty_like(Sblk)
+    Vblk = torch.empty_like(Sblk)
+    be.one_electron_device(Sblk, Tblk, Vblk)
+    Hblk = Tblk + Vblk
+    del Tblk, Vblk
+    Sh_all = Sblk.cpu().numpy()
+    Sb = [Sh_all[int(o):int(o) + int(n) * int(n)] for o, n in zip(be.mat_off, be.nbf)]
     S = lay.to_pad(Sblk, fill_diag=1.0)
     H = lay.to_pad(Hblk, fill_diag=PAD_DIAG)
     # per-molecule orthogonalisers on the host; the diagonalisations run there too, on a
@@ -255,20 +270,13 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
         t2 = time.perf_counter()
         g = torch.zeros((int(be.atom_off[-1]), 3), dtype=torch.float64, device=dev)
         be.grad2e_device(Dblk, g, precision)
+        # one-electron part on the GPU: 2 sum D d(T+V)/dX - 2 sum Q dS/dX with Q = D F D
+        Qblk = lay.to_block(D @ F @ D).contiguous()
+        be.one_electron_grad_device(Dblk, Qblk, 2.0, -2.0, g)
         torch.cuda.synchronize()
         g2 = g.cpu().numpy()
-        Dn = D.cpu().numpy()
-        Fn = F.cpu().numpy()
-        def one_grad(k):
-            b = bases[k]
-            n = b.nbf
-            Dk, Fk = Dn[k, :n, :n], Fn[k, :n, :n]
-            gk = g2[be.atom_off[k]:be.atom_off[k + 1]].copy()
-            gk += eng.one_electron_grad(b, Dk, Dk @ Fk @ Dk, 2.0, -2.0)
-            gk += nuclear_repulsion_gradient(b.Z, b.coords)
-            return gk
-
-        grads = list(pool.map(one_grad, range(nmol)))
+        grads = [g2[be.atom_off[k]:be.atom_off[k + 1]] + nuclear_repulsion_gradient(b.Z, b.coords)
+                 for k, b in enumerate(bases)]
         out["gradients"] = grads
         out["grad_s"] = time.perf_counter() - t2
     pool.shutdown()

@@ -54,6 +54,8 @@ def _compile(src, verbose):
     deps = [src] + _common_headers() + [os.path.join(CSRC, "hfgpu_onee.h")]
     if base.startswith("inst_"):
         deps.append(os.path.join(GEN, "class_" + base[5:] + ".cuh"))
+    else:  # hand-written sources: every hand-written header counts
+        deps += sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")))
     stamp = obj + ".sha1"
     key = _hash_files(deps) + " ".join(FLAGS + ARCH)
     if os.path.exists(obj) and os.path.exists(stamp) and open(stamp).read() == key:

@@ -10,11 +10,13 @@
 // PA = P - A and Kp = K sqrt(2 pi^2.5) / p with K = exp(-alpha_a alpha_b / p |AB|^2) c_a c_b
 // (BASIS::ShellPair::set_params, src/integrals/hfscf_shellpair.cpp:33-61).  Kp is
 // scaled so that the [00|00] prefactor K_ab K_cd 2 pi^2.5 / (p q sqrt(p+q)) is
-// Kp_ab Kp_cd / sqrt(p+q).  80 bytes in FP64 (five 16-byte loads).
+// Kp_ab Kp_cd / sqrt(p+q).  eb2 is the square of the ket exponent, used only by the
+// kinetic-energy integrals (for a folded self pair, the mean over (i, j) and (j, i)).
+// 80 bytes in FP64 (five 16-byte loads).
 // ---------------------------------------------------------------------------
 template <typename R>
 struct __align__(sizeof(R) * 2) PrimPair {
-  R p, ip, Px, Py, Pz, PAx, PAy, PAz, Kp, pad;
+  R p, ip, Px, Py, Pz, PAx, PAy, PAz, Kp, eb2;
 };
 
 // One canonical shell pair (La >= Lb after an optional swap of the two shells).

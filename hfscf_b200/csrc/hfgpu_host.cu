@@ -12,6 +12,7 @@
 #include "hfgpu_kernels.cuh"
 #include "hfgpu_launch.h"
 #include "hfgpu_onee.h"
+#include "hfgpu_onee_kernels.cuh"
 
 namespace {
 
@@ -111,6 +112,7 @@ struct hfgpu_handle {
   long long nquartets = 0;
 
   DevBuf d_pairs, d_prim_d, d_prim_f, d_alpha_d, d_alpha_f, d_boys_d, d_boys_f, d_quart;
+  DevBuf d_onee;  // one-electron kernels: atoms (x, y, z, Z), molecule atom ranges, Cartesian -> pure tables
   DevBuf d_mats, d_half, d_dmax, d_counters, d_grad, d_scratch, d_eri, d_eriq;
   long long last_launched = 0, last_skipped = 0;
   int last_kernels = 0;                 // kernel launches of the last J/K build
@@ -265,12 +267,16 @@ int build_pairs(hfgpu_handle* h) {
         const double c1 = h->coefs[h->prim_off[t.sa] + i], c2 = h->coefs[h->prim_off[t.sb] + j];
         const double p = a1 + a2;
         const double K = std::exp(-a1 * a2 / p * R2) * c1 * c2 * (self && j > i ? 2.0 : 1.0);
-        if (self && j > i) a1 = a2 = 0.5 * p;
+        double eb2 = a2 * a2;  // the kinetic integral is quadratic in the ket exponent
+        if (self && j > i) {
+          eb2 = 0.5 * (a1 * a1 + a2 * a2);
+          a1 = a2 = 0.5 * p;
+        }
         if (std::fabs(K) * std::sqrt(PI_2_5) / p < kp_cut) continue;
         PrimPair<double> q;
         q.p = p;
         q.ip = 1.0 / p;
-        q.pad = 0.0;
+        q.eb2 = eb2;
         q.Px = (a1 * A[0] + a2 * B[0]) / p;
         q.Py = (a1 * A[1] + a2 * B[1]) / p;
         q.Pz = (a1 * A[2] + a2 * B[2]) / p;
@@ -293,7 +299,7 @@ int build_pairs(hfgpu_handle* h) {
   std::vector<float> aaf(np), abf(np);
   for (size_t i = 0; i < pd.size(); ++i) {
     pf[i] = {(float)pd[i].p, (float)pd[i].ip, (float)pd[i].Px, (float)pd[i].Py, (float)pd[i].Pz,
-             (float)pd[i].PAx, (float)pd[i].PAy, (float)pd[i].PAz, (float)pd[i].Kp, 0.f};
+             (float)pd[i].PAx, (float)pd[i].PAy, (float)pd[i].PAz, (float)pd[i].Kp, (float)pd[i].eb2};
     aaf[i] = (float)aa[i];
     abf[i] = (float)ab[i];
   }
@@ -969,7 +975,7 @@ int hfgpu_destroy(hfgpu_handle* h) {
   if (!h) return HFGPU_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (DevBuf* d : {&h->d_pairs, &h->d_prim_d, &h->d_prim_f, &h->d_alpha_d, &h->d_alpha_f, &h->d_boys_d, &h->d_boys_f,
+  for (DevBuf* d : {&h->d_onee, &h->d_pairs, &h->d_prim_d, &h->d_prim_f, &h->d_alpha_d, &h->d_alpha_f, &h->d_boys_d, &h->d_boys_f,
                     &h->d_quart, &h->d_mats, &h->d_half, &h->d_dmax, &h->d_counters, &h->d_grad, &h->d_scratch,
                     &h->d_eri, &h->d_eriq})
     d->release();
@@ -1269,6 +1275,82 @@ int hfgpu_one_electron_grad(const hfgpu_basis* basis, const double* xyz, const d
   OneEHost o;
   if (!xyz || !Z || !D || !W || !grad || onee_basis(basis, o)) return HFGPU_ERR_INVALID;
   hfgpu_onee_gradient(o.b, Z, xyz, basis->natoms, D, W, cH, cS, grad);
+  return HFGPU_OK;
+}
+
+// Kernel arguments of the device one-electron kernels; uploads atoms and charges.
+static int onee_setup(hfgpu_handle* h, const double* Z, onee::Args& a, long long& nitems) {
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  const int na = h->natoms, nm = h->nmol;
+  std::vector<int> mol_atom = h->batched ? h->mol_atom : std::vector<int>{0, na};
+  int slots = 0;
+  for (int m = 0; m < nm; ++m) slots = std::max(slots, mol_atom[m + 1] - mol_atom[m]);
+  slots += 1;
+  // layout: ylm [3][30] | atoms [na][4] | mol_atom [nm + 1] (ints)
+  const size_t bytes = sizeof(double) * (90 + 4 * (size_t)na) + sizeof(int) * (nm + 1);
+  std::vector<unsigned char> host(bytes, 0);
+  double* y = reinterpret_cast<double*>(host.data());
+  for (int L = 0; L <= 2; ++L) hfgpu_onee_ylm(L, y + 30 * L);
+  double* at = y + 90;
+  for (int i = 0; i < na; ++i) {
+    if (!std::isfinite(Z[i])) return fail(h, HFGPU_ERR_INVALID, "non-finite nuclear charge");
+    for (int d = 0; d < 3; ++d) at[4 * i + d] = h->xyz[3 * i + d];
+    at[4 * i + 3] = Z[i];
+  }
+  std::memcpy(at + 4 * na, mol_atom.data(), sizeof(int) * (nm + 1));
+  HF_CUDA(h, h->d_onee.ensure(bytes));
+  HF_CUDA(h, cudaMemcpyAsync(h->d_onee.p, host.data(), bytes, cudaMemcpyHostToDevice, h->stream));
+  const double* dy = h->d_onee.as<double>();
+  const size_t np = std::max<size_t>(h->nprimpairs, 1);
+  a = onee::Args{};
+  a.pairs = h->d_pairs.as<PairInfo>();
+  a.prims = h->d_prim_d.as<PrimPair<double>>();
+  a.alpha_a = h->d_alpha_d.as<double>();
+  a.alpha_b = h->d_alpha_d.as<double>() + np;
+  a.npairs = (int)h->pairs.size();
+  a.boys.tab = h->d_boys_d.as<double>();
+  a.atoms.xyzZ = dy + 90;
+  a.atoms.mol_atom = reinterpret_cast<const int*>(dy + 90 + 4 * na);
+  a.atoms.slots = slots;
+  a.ylm = dy;
+  a.pure = h->pure;
+  a.n = h->n;
+  if (h->batched) {
+    a.mol_off = h->d_mol.as<long long>();
+    a.mol_n = reinterpret_cast<const int*>(a.mol_off + h->nmol);
+  }
+  nitems = (long long)a.npairs * slots;
+  return HFGPU_OK;
+}
+
+int hfgpu_one_electron_device(hfgpu_handle* h, const double* Z, double* S, double* T, double* V) {
+  if (!h || !Z || !S || !T || !V) return HFGPU_ERR_INVALID;
+  int rc = set_device(h);
+  if (rc) return rc;
+  onee::Args a;
+  long long nitems = 0;
+  if ((rc = onee_setup(h, Z, a, nitems))) return rc;
+  const size_t nn = h->batched ? (size_t)h->mat_total : (size_t)h->n * h->n;
+  HF_CUDA(h, cudaMemsetAsync(V, 0, sizeof(double) * nn, h->stream));
+  if (nitems > 0) {
+    onee_matrices_kernel<<<(unsigned)((nitems + 127) / 128), 128, 0, h->stream>>>(a, nitems, S, T, V);
+    HF_CHECK_LAUNCH(h, "one-electron matrices");
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_one_electron_grad_device(hfgpu_handle* h, const double* Z, const double* D, const double* W, double cH,
+                                   double cS, double* grad) {
+  if (!h || !Z || !D || !W || !grad) return HFGPU_ERR_INVALID;
+  int rc = set_device(h);
+  if (rc) return rc;
+  onee::Args a;
+  long long nitems = 0;
+  if ((rc = onee_setup(h, Z, a, nitems))) return rc;
+  if (nitems > 0) {
+    onee_grad_kernel<<<(unsigned)((nitems + 127) / 128), 128, 0, h->stream>>>(a, nitems, D, W, cH, cS, grad);
+    HF_CHECK_LAUNCH(h, "one-electron gradient");
+  }
   return HFGPU_OK;
 }
 

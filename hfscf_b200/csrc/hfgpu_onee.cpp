@@ -429,3 +429,6 @@ void hfgpu_onee_gradient(const OneEBasis& b, const double* Zc, const double* xyz
   }
   for (int x = 0; x < 3 * natoms; ++x) grad[x] += g[x];
 }
+
+// Cartesian -> pure coefficients of shell L (the table the device one-electron kernels use).
+void hfgpu_onee_ylm(int L, double* out) { ylm(L, out); }

@@ -16,3 +16,5 @@ void hfgpu_onee_matrices(const OneEBasis& b, const double* Zc, const double* xyz
                          double* V);
 void hfgpu_onee_gradient(const OneEBasis& b, const double* Zc, const double* xyz, int natoms, const double* D,
                          const double* W, double cH, double cS, double* grad);
+// Cartesian -> pure coefficients, (L+1)(L+2)/2 x (2L+1) row-major (the reference's Ylm_transmat).
+void hfgpu_onee_ylm(int L, double* out);

@@ -213,6 +213,44 @@ class Engine:
         self._check(lib().hfgpu_class_time(self.h, ctypes.c_int(cls), ctypes.byref(ms)))
         return ms.value
 
+    # --- one-electron integrals on the device -----------------------------------------
+    def one_electron_device(self, S_ptr, T_ptr, V_ptr):
+        """hfgpu_one_electron_device into device buffers (n x n each)."""
+        Z = _c(self.basis.Z)
+        self._check(lib().hfgpu_one_electron_device(self.h, _p(Z), ctypes.c_void_p(S_ptr), ctypes.c_void_p(T_ptr),
+                                                    ctypes.c_void_p(V_ptr)))
+
+    def one_electron_grad_device(self, D_ptr, W_ptr, cH, cS, grad_ptr):
+        """grad (device, natoms x 3) += cH sum D d(T+V)/dX + cS sum W dS/dX."""
+        Z = _c(self.basis.Z)
+        self._check(lib().hfgpu_one_electron_grad_device(self.h, _p(Z), ctypes.c_void_p(D_ptr), ctypes.c_void_p(W_ptr),
+                                                         ctypes.c_double(cH), ctypes.c_double(cS),
+                                                         ctypes.c_void_p(grad_ptr)))
+
+    def one_electron(self):
+        """S, T, V (host arrays) computed on the GPU."""
+        import torch
+        dev = torch.device("cuda", self._opts.device)
+        n = self.n
+        M = torch.empty((3, n, n), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)  # the handle's stream need not be torch's
+        self.one_electron_device(M[0].data_ptr(), M[1].data_ptr(), M[2].data_ptr())
+        torch.cuda.synchronize(dev)
+        out = M.cpu().numpy()
+        return out[0], out[1], out[2]
+
+    def one_electron_grad(self, D, W, cH, cS) -> np.ndarray:
+        """cH sum D d(T+V)/dX + cS sum W dS/dX (natoms x 3, host) computed on the GPU."""
+        import torch
+        dev = torch.device("cuda", self._opts.device)
+        Dd = torch.from_numpy(_c(D)).to(dev)
+        Wd = torch.from_numpy(_c(W)).to(dev)
+        g = torch.zeros((self.basis.natoms, 3), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        self.one_electron_grad_device(Dd.data_ptr(), Wd.data_ptr(), cH, cS, g.data_ptr())
+        torch.cuda.synchronize(dev)
+        return g.cpu().numpy()
+
     # --- launch schedule ----------------------------------------------------------
     def autotune(self, D, precision=FP64, repeats=3) -> np.ndarray:
         """hfgpu_autotune: per class, the fastest launch form on this geometry and density.

@@ -95,12 +95,13 @@ def rhf(basis: Basis, fock=None, *, H=None, S=None, e_tol=1e-10, rms_tol=1e-8, d
     if nel % 2:
         raise ValueError("RHF needs an even electron count")
     nocc = nel // 2
-    if H is None or S is None:
-        S_, T_, V_ = eng.one_electron(basis)
-        S, H = S_, T_ + V_
     if fock is None:
         engine = engine or eng.Engine(basis)
         fock = lambda D, H_: engine.fock_rhf(D, H_, precision)  # noqa: E731
+    if H is None or S is None:
+        # one-electron matrices on the GPU when there is an engine, on the host otherwise
+        S_, T_, V_ = engine.one_electron() if engine is not None else eng.one_electron(basis)
+        S, H = S_, T_ + V_
     X = sym_orth(S)
     # CORE guess (deterministic): diagonalise X^T H X
     if D0 is None:
@@ -151,7 +152,7 @@ def rhf_gradient(basis: Basis, res: ScfResult, engine, precision=eng.FP64):
     D, F = res.D, res.F
     Q = D @ F @ D
     g = engine.grad2e(D, 1.0, precision)
-    g += eng.one_electron_grad(basis, D, Q, 2.0, -2.0)
+    g += engine.one_electron_grad(D, Q, 2.0, -2.0)
     g += nuclear_repulsion_gradient(basis.Z, basis.coords)
     return g
 
@@ -162,7 +163,7 @@ def uhf(basis: Basis, engine, *, multiplicity=1, e_tol=1e-10, rms_tol=1e-8, max_
     nel = int(np.sum(basis.Z))
     na = (nel + multiplicity - 1) // 2
     nb = nel - na
-    S, T, V = eng.one_electron(basis)
+    S, T, V = engine.one_electron()
     H = T + V
     X = sym_orth(S)
     eps, Cp = np.linalg.eigh(X.T @ H @ X)
@@ -216,6 +217,6 @@ def uhf_gradient(basis: Basis, r, engine, precision=eng.FP64):
     Da, Db, Fa, Fb = r["Da"], r["Db"], r["Fa"], r["Fb"]
     W = Da @ Fa @ Da + Db @ Fb @ Db
     g = engine.grad2e_uhf(Da, Db, 1.0, precision)
-    g += eng.one_electron_grad(basis, Da + Db, W, 1.0, -1.0)
+    g += engine.one_electron_grad(Da + Db, W, 1.0, -1.0)
     g += nuclear_repulsion_gradient(basis.Z, basis.coords)
     return g

@@ -155,9 +155,9 @@ int hfgpu_batch_jk_device(hfgpu_handle* h, const double* D, double* J, double* K
 int hfgpu_batch_grad2e_device(hfgpu_handle* h, const double* D, double* grad, int precision);
 
 /* One-electron matrices S, T, V (n x n) for the basis at xyz (bohr), on the host CPU.
- * Z: nuclear charges per atom.  Needs no handle and no GPU: these O(N^2) integrals
- * stay on the CPU here (the reference's OSOverlap/OSKinetic/OSNuclear,
- * src/integrals/hfscf_osoverlap.cpp:10, hfscf_osnuclear.cpp:17). */
+ * Z: nuclear charges per atom.  Needs no handle and no GPU (the reference's
+ * OSOverlap/OSKinetic/OSNuclear, src/integrals/hfscf_osoverlap.cpp:10, hfscf_osnuclear.cpp:17);
+ * the handle-based device versions follow below. */
 int hfgpu_one_electron(const hfgpu_basis* basis, const double* xyz_bohr, const double* Z, double* S, double* T,
                        double* V);
 /* grad (natoms x 3) += cH sum D_ij d(T+V)_ij/dX + cS sum W_ij dS_ij/dX, including the
@@ -165,6 +165,16 @@ int hfgpu_one_electron(const hfgpu_basis* basis, const double* xyz_bohr, const d
  * (src/gradient/hfscf_grad_rhf.cpp:140-167) is cH = 2 with D and cS = -2 with Q = D F D. */
 int hfgpu_one_electron_grad(const hfgpu_basis* basis, const double* xyz_bohr, const double* Z, const double* D,
                             const double* W, double cH, double cS, double* grad);
+
+/* The same one-electron matrices and gradient on the GPU, for the handle's basis and current
+ * geometry (reference routines as above, and the per-atom assembly of
+ * src/gradient/hfscf_grad_ints.cpp:14-77,153-199).  Z: nuclear charge per atom (host array;
+ * a batched handle takes every molecule's atoms in order).  S, T, V, D, W and grad are device
+ * pointers: n x n matrices (block storage for a batched handle) and natoms x 3; V is
+ * overwritten, grad accumulated.  Enqueued on the handle's stream. */
+int hfgpu_one_electron_device(hfgpu_handle* h, const double* Z, double* S, double* T, double* V);
+int hfgpu_one_electron_grad_device(hfgpu_handle* h, const double* Z, const double* D, const double* W, double cH,
+                                   double cS, double* grad);
 
 /* Counters of the last J/K build: quartets launched and quartets skipped by density screening. */
 int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* skipped);

@@ -172,6 +172,35 @@ def ref_deriv1(basis, coords=(1, 1, 1), cutoff=1e-14) -> np.ndarray:
     return out
 
 
+def ref_onee(basis):
+    """S, T, V from the reference's one-electron shell routines (hfscf_osoverlap.cpp,
+    hfscf_osnuclear.cpp) over the driver loop of hfscf_hf_hamiltonian.cpp:14-37."""
+    args, f = _flat(basis)
+    n = basis.nbf
+    Z = np.ascontiguousarray(np.asarray(basis.Z), dtype=np.int32)
+    xyz = np.ascontiguousarray(basis.coords, dtype=np.float64)
+    S, T, V = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
+    rc = ref().hfref_onee(*args, ctypes.c_int(basis.natoms), _p(Z, ctypes.c_int), _p(xyz), _p(S), _p(T), _p(V))
+    assert rc == 0
+    return S, T, V
+
+
+def ref_onee_grad(basis, D, Q, cD=2.0, cQ=-2.0) -> np.ndarray:
+    """cD sum D.(dT + dV) + cQ sum Q.dS per atom and direction, from the reference's
+    first-derivative shell routines and its per-atom assembly (hfscf_grad_ints.cpp:14-77,153-199)."""
+    args, f = _flat(basis)
+    Z = np.ascontiguousarray(np.asarray(basis.Z), dtype=np.int32)
+    xyz = np.ascontiguousarray(basis.coords, dtype=np.float64)
+    Dc = np.ascontiguousarray(D, dtype=np.float64)
+    Qc = np.ascontiguousarray(Q, dtype=np.float64)
+    g = np.zeros((basis.natoms, 3))
+    rc = ref().hfref_onee_grad(*args, ctypes.c_int(basis.natoms), _p(Z, ctypes.c_int), _p(xyz),
+                               _p(f["atom"], ctypes.c_int), _p(Dc), _p(Qc), ctypes.c_double(cD),
+                               ctypes.c_double(cQ), _p(g))
+    assert rc == 0
+    return g
+
+
 def ref_boys(m, T) -> float:
     return ref().hfref_boys(float(m), float(T))
 

@@ -4,7 +4,14 @@
 // TEST INFRASTRUCTURE ONLY.  Nothing in the product links or loads this
 // library; tests and the CPU-baseline leg of bench.py use it as the checker.
 //
-// The shell-quartet loops below restate the reference's drivers:
+// The shell-pair and shell-quartet loops below restate the reference's drivers:
+//   - hfref_onee: Mol::hf_solver::create_one_electron_hamiltonian
+//       (src/scfsolver/hfscf_hf_hamiltonian.cpp:14-37)
+//   - hfref_onee_grad: the one-electron part of Mol::scf_gradient::calc_scf_gradient_rhf
+//       (src/gradient/hfscf_grad_rhf.cpp:78-81,99-102,144-146,164) with
+//       calc_overlap_centers / calc_kinetic_centers / calc_nuclear_potential_centers and
+//       calc_overlap_kinetic_gradient / calc_potential_gradient
+//       (src/gradient/hfscf_grad_ints.cpp:14-77,153-199)
 //   - hfref_eri_packed: Mol::hf_solver::create_repulsion_matrix
 //       (src/scfsolver/hfscf_hf_hamiltonian.cpp:67-112)
 //   - hfref_deriv1: Mol::scf_gradient::calc_coulomb_exchange_integral_centers
@@ -19,6 +26,10 @@
 #include <omp.h>
 
 #include "integrals/hfscf_oseri.hpp"
+#include "integrals/hfscf_oskinetic.hpp"
+#include "integrals/hfscf_osnuclear.hpp"
+#include "integrals/hfscf_osoverlap.hpp"
+#include "molecule/hfscf_atom.hpp"
 #include "math/gamma.hpp"
 #include "math/solid_harmonics.hpp"
 
@@ -153,6 +164,94 @@ int hfref_deriv1(int nshell, const int* L, const double* xyz, const int* nprim, 
     }
     for (Eigen::Index p = 0; p < len; ++p) out9[q * len + p] = t[q][p];
   }
+  return 0;
+}
+
+// S, T, V (n x n each, row-major) from OSOverlap::compute_contracted_shell and
+// OSNuclear::compute_contracted_shell over all shell pairs i <= j.  Atoms: natoms
+// charges Z and positions atom_xyz (bohr); shell centres in xyz.
+int hfref_onee(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
+               const double* coef, int pure, int natoms, const int* Z, const double* atom_xyz, double* S_out,
+               double* T_out, double* V_out) {
+  auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, pure);
+  const Eigen::Index n = pure ? b->npure : b->ncart;
+  std::vector<MOLEC::Atom> atoms;
+  for (int a = 0; a < natoms; ++a) atoms.emplace_back(Z[a], Vec3D(atom_xyz[3 * a], atom_xyz[3 * a + 1], atom_xyz[3 * a + 2]));
+  EigenMatrix<double> S = EigenMatrix<double>::Zero(n, n), T = S, V = S;
+  OSOVERLAP::OSOverlap os(pure != 0);
+  OSNUCLEAR::OSNuclear on(pure != 0);
+  for (int i = 0; i < nshell; ++i)
+    for (int j = i; j < nshell; ++j) {
+      os.compute_contracted_shell(S, T, b->pairs[i * nshell + j]);
+      on.compute_contracted_shell(V, b->pairs[i * nshell + j], atoms);
+    }
+  for (Eigen::Index i = 0; i < n; ++i)
+    for (Eigen::Index j = 0; j < n; ++j) {
+      S_out[i * n + j] = S(i, j);
+      T_out[i * n + j] = T(i, j);
+      V_out[i * n + j] = V(i, j);
+    }
+  return 0;
+}
+
+// One-electron gradient grad (natoms x 3) = cD sum D.(dT/dX + dV/dX) + cQ sum Q.dS/dX, from the
+// reference's first-derivative shell routines and its per-atom assembly (cD = 2, cQ = -2 is
+// the RHF gradient's one-electron part with Q = D F D).  shell_atom maps shells to atoms.
+int hfref_onee_grad(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
+                    const double* coef, int pure, int natoms, const int* Z, const double* atom_xyz,
+                    const int* shell_atom, const double* D, const double* Q, double cD, double cQ, double* grad) {
+  auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, pure);
+  const Eigen::Index n = pure ? b->npure : b->ncart;
+  std::vector<MOLEC::Atom> atoms;
+  for (int a = 0; a < natoms; ++a) atoms.emplace_back(Z[a], Vec3D(atom_xyz[3 * a], atom_xyz[3 * a + 1], atom_xyz[3 * a + 2]));
+  tensor3d<double> dSdq(3, n, n), dTdq(3, n, n), dVdqa(3 * natoms, n, n), dVdqb(3 * natoms, n, n);
+  OSOVERLAP::OSOverlap os(pure != 0);
+  OSKINETIC::OSKinetic ok(pure != 0);
+  OSNUCLEAR::OSNuclear on(pure != 0);
+  const std::vector<bool> coords = {true, true, true};
+  for (int i = 0; i < nshell; ++i)
+    for (int j = i; j < nshell; ++j) {
+      os.compute_contracted_shell_deriv1(dSdq, b->pairs[i * nshell + j]);
+      ok.compute_contracted_shell_deriv1(dTdq, b->pairs[i * nshell + j]);
+      on.compute_contracted_shell_deriv1(dVdqa, dVdqb, b->pairs[i * nshell + j], atoms, coords);
+    }
+  // function -> atom
+  std::vector<int> fatom;
+  for (int s = 0; s < nshell; ++s)
+    for (int k = 0; k < (pure ? 2 * L[s] + 1 : (L[s] + 1) * (L[s] + 2) / 2); ++k) fatom.push_back(shell_atom[s]);
+  for (int dir = 0; dir < 3; ++dir)
+    for (int atom = 0; atom < natoms; ++atom) {
+      double g = 0.0;
+      for (Eigen::Index i = 0; i < n; ++i) {
+        const bool mi = fatom[i] == atom;
+        // overlap and kinetic: A-derivative with the B term by translational invariance
+        for (Eigen::Index j = i + 1; j < n; ++j) {
+          const bool mj = fatom[j] == atom;
+          double ds = 0.0, dt = 0.0;
+          if (mi) {
+            ds = dSdq(dir, i, j);
+            dt = dTdq(dir, i, j);
+          }
+          if (mj) {
+            ds -= dSdq(dir, i, j);
+            dt -= dTdq(dir, i, j);
+          }
+          g += 2.0 * (cQ * Q[i * n + j] * ds + cD * D[i * n + j] * dt);  // (i, j) and (j, i)
+        }
+        // nuclear attraction, upper triangle with the diagonal
+        for (Eigen::Index j = i; j < n; ++j) {
+          const bool mj = fatom[j] == atom;
+          double dv = 0.0;
+          for (int k = 0; k < natoms; ++k) {
+            if (mi) dv -= dVdqa(natoms * dir + k, i, j);
+            if (mj) dv -= dVdqb(natoms * dir + k, i, j);
+            if (k == atom) dv += dVdqa(natoms * dir + atom, i, j) + dVdqb(natoms * dir + atom, i, j);
+          }
+          g += (j == i ? 1.0 : 2.0) * cD * D[i * n + j] * dv;
+        }
+      }
+      grad[3 * atom + dir] = g;
+    }
   return 0;
 }
 

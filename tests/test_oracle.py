@@ -9,6 +9,7 @@ import pytest
 import oracle
 from hfscf_b200 import basis as B
 from hfscf_b200 import molecules as M
+from hfscf_b200 import engine as E
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="reference library not built here")
@@ -86,3 +87,25 @@ def test_packed_index_and_unpack_roundtrip():
     assert np.array_equal(idx, oracle.index_ijkl(j, i, k, l))
     assert np.array_equal(idx, oracle.index_ijkl(k, l, i, j))
     assert len(np.unique(idx)) == oracle.packed_len(n)
+
+
+@pytest.mark.parametrize("name,pure", [("6-31g**", False), ("cc-pvdz", True), ("sto-3g", False)])
+def test_host_one_electron_matches_reference(name, pure):
+    """Host S, T, V and one-electron gradient against the reference's own one-electron
+    routines (hfscf_osoverlap.cpp, hfscf_osnuclear.cpp and their _deriv1 forms)."""
+    if not oracle.ref_available():
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(13)
+    Z, x = M.water(rng)
+    bs = B.build_basis(name, Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=pure)
+    S0, T0, V0 = oracle.ref_onee(bs)
+    S, T, V = E.one_electron(bs)
+    assert max(np.abs(S - S0).max(), np.abs(T - T0).max(), np.abs(V - V0).max()) < 1e-12
+    n = bs.nbf
+    A = rng.normal(size=(n, n))
+    D = (A + A.T) / n
+    A = rng.normal(size=(n, n))
+    Q = (A + A.T) / n
+    g0 = oracle.ref_onee_grad(bs, D, Q, 2.0, -2.0)
+    g = E.one_electron_grad(bs, D, Q, 2.0, -2.0)
+    assert np.abs(g - g0).max() < 1e-11
