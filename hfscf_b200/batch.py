@@ -2,15 +2,16 @@
 
 One batched engine handle holds every molecule (hfgpu_batch_create).  Each SCF
 iteration is one J/K build for all molecules at once -- the per-class kernels
-cover every molecule's quartets.  DIIS and the Fock assembly run batched on the
-GPU in torch over matrices padded to the largest molecule; the per-molecule
-diagonalisations run on a host thread pool over the unpadded blocks.  The J/K build and the Fock assembly can be captured once
-as a CUDA graph and replayed every iteration.  After convergence, the
-two-electron gradient of every molecule comes from one batched adjoint launch
-(hfgpu_batch_grad2e_device) and one for the one-electron part
-(hfgpu_one_electron_grad_device); only the nuclear repulsion term is added on the host.
-S, T and V of every molecule also come from one device launch.  Before the graph is captured, hfgpu_autotune picks each
-quartet class's launch form on the batch's first density.
+cover every molecule's quartets -- captured once as a CUDA graph and replayed.
+DIIS and the Fock assembly run batched on the GPU in torch over matrices padded to
+the largest molecule, and every molecule's Fock matrix is diagonalised in one launch
+of the batched Jacobi eigensolver (hfgpu_batch_eigh), which also gives the
+orthogonalisers S^-1/2.  S, T and V of every molecule come from one device launch.
+After convergence, the two-electron gradient of every molecule comes from one
+batched adjoint launch (hfgpu_batch_grad2e_device) and the one-electron part from
+one more (hfgpu_one_electron_grad_device); only the nuclear repulsion term is added
+on the host.  With diag="host" the diagonalisations run per molecule on a host
+thread pool instead.
 
 The SCF is the caller side, as in scf.py: symmetric orthogonalisation, D =
 C_occ C_occ^T (no factor 2), E = sum D (H + F), DIIS on the orthogonalised
@@ -91,6 +92,13 @@ class BatchEngine:
                                              ctypes.c_int(repeats), out.ctypes.data_as(eng._ip)))
         return out
 
+    def eigh(self, A, W, V, sweeps=None):
+        """hfgpu_batch_eigh: eigenvalues (ascending) and eigenvectors of every molecule's block of
+        the padded batch A [nmol, nmax, nmax] (device tensors)."""
+        self._check(eng.lib().hfgpu_batch_eigh(self.h, ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(W.data_ptr()),
+                                               ctypes.c_void_p(V.data_ptr()),
+                                               ctypes.c_void_p(sweeps.data_ptr() if sweeps is not None else 0)))
+
     def grad2e_device(self, D, grad, precision=eng.FP64):
         self._check(eng.lib().hfgpu_batch_grad2e_device(self.h, ctypes.c_void_p(D.data_ptr()),
                                                         ctypes.c_void_p(grad.data_ptr()), ctypes.c_int(precision)))
@@ -138,11 +146,24 @@ class _Layout:
 
 
 def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-10, rms_tol=1e-8,
-              max_iter=60, use_graph=True, gradient=True, autotune=True):
-    """Converged RHF energies (and gradients) of every molecule of the batch."""
+              max_iter=60, use_graph=True, gradient=True, autotune=False, diag="gpu"):
+    """Converged RHF energies (and gradients) of every molecule of the batch.  ``diag``:
+    "gpu" diagonalises every molecule's Fock matrix in one launch of the batched Jacobi
+    kernel (hfgpu_batch_eigh, molecules of up to 118 functions); "host" runs LAPACK per
+    molecule on a host thread pool.  ``autotune`` runs hfgpu_autotune on the first density
+    before the graph is captured (off by default: for 512 small molecules it cost 2.4 s and
+    bought nothing over the default schedule)."""
     dev = torch.device("cuda", device)
     t0 = time.perf_counter()
+    stages = {}
+
+    def stage(name, t_start):
+        torch.cuda.synchronize()
+        stages[name] = time.perf_counter() - t_start
+        return time.perf_counter()
+
     be = BatchEngine(bases, device)
+    tt = stage("handle", t0)
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
     be.set_stream(stream.cuda_stream)
@@ -155,26 +176,46 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     be.one_electron_device(Sblk, Tblk, Vblk)
     Hblk = Tblk + Vblk
     del Tblk, Vblk
-    Sh_all = Sblk.cpu().numpy()
-    Sb = [Sh_all[int(o):int(o) + int(n) * int(n)] for o, n in zip(be.mat_off, be.nbf)]
     S = lay.to_pad(Sblk, fill_diag=1.0)
     H = lay.to_pad(Hblk, fill_diag=PAD_DIAG)
-    # per-molecule orthogonalisers on the host; the diagonalisations run there too, on a
-    # thread pool over the unpadded blocks (LAPACK releases the GIL), because batched
-    # eigh of padded matrices on the GPU loops over the batch
-    Xh, Xpad = [], np.zeros((nmol, nmax, nmax))
-    for k, b in enumerate(bases):
-        n = b.nbf
-        w, U = np.linalg.eigh(Sb[k].reshape(n, n))
-        Xh.append((U / np.sqrt(w)) @ U.T)
-        Xpad[k, :n, :n] = Xh[-1]
-        Xpad[k, np.arange(n, nmax), np.arange(n, nmax)] = 1.0
-    X = torch.from_numpy(Xpad).to(dev)
+    tt = stage("one_electron", tt)
+    Wev = torch.empty((nmol, nmax), dtype=torch.float64, device=dev)
+    Vev = torch.empty((nmol, nmax, nmax), dtype=torch.float64, device=dev)
+    # symmetric orthogonalisers X = S^-1/2 (padding: identity)
+    Xh = []
+    if diag == "gpu":
+        be.eigh(S, Wev, Vev)
+        X = (Vev * Wev.rsqrt()[:, None, :]) @ Vev.transpose(1, 2)
+    else:
+        # per-molecule LAPACK on the host; the diagonalisations of the SCF run there too,
+        # on a thread pool over the unpadded blocks (LAPACK releases the GIL)
+        Sh_all = Sblk.cpu().numpy()
+        Xpad = np.zeros((nmol, nmax, nmax))
+        for k, b in enumerate(bases):
+            n, o = b.nbf, int(be.mat_off[k])
+            w, U = np.linalg.eigh(Sh_all[o:o + n * n].reshape(n, n))
+            Xh.append((U / np.sqrt(w)) @ U.T)
+            Xpad[k, :n, :n] = Xh[-1]
+            Xpad[k, np.arange(n, nmax), np.arange(n, nmax)] = 1.0
+        X = torch.from_numpy(Xpad).to(dev)
     nocc_h = [int(np.sum(b.Z)) // 2 for b in bases]
     pool = cf.ThreadPoolExecutor(max_workers=max(1, min(32, os.cpu_count() or 1)))
     Dh = np.zeros(be.mat_total)
 
+    occ = (torch.arange(nmax, device=dev)[None, :] <
+           torch.tensor(nocc_h, device=dev)[:, None]).to(torch.float64)
+    tt = stage("orthogonaliser", tt)
+
+    def density_gpu(F):
+        Fp = X.transpose(1, 2) @ F @ X
+        Fp = 0.5 * (Fp + Fp.transpose(1, 2))
+        be.eigh(Fp, Wev, Vev)
+        C = X @ Vev
+        return (C * occ[:, None, :]) @ C.transpose(1, 2)
+
     def density(F):
+        if diag == "gpu":
+            return density_gpu(F)
         Fh = lay.to_block(F).cpu().numpy()
 
         def one(k):
@@ -199,8 +240,9 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
         Fblk.sub_(Kblk)
 
     build()  # warm-up: loads every kernel before any capture
-    torch.cuda.synchronize()
+    tt = stage("guess_and_first_build", tt)
     schedule = be.autotune(Dblk, precision) if autotune else None
+    tt = stage("autotune", tt)
     graph = None
     if use_graph:
         try:
@@ -211,6 +253,7 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
         except Exception:
             graph = None
             torch.cuda.synchronize()
+    tt = stage("graph_capture", tt)
     t_setup = time.perf_counter() - t0
     hist_F, hist_E = [], []
     E_prev = torch.zeros(nmol, dtype=torch.float64, device=dev)
@@ -264,7 +307,8 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     E_el = (Dz * (lay.to_pad(Hblk) + F)).sum(dim=(1, 2)).cpu().numpy()
     enuc = np.array([nuclear_repulsion(b.Z, b.coords) for b in bases])
     out = {"energies": E_el + enuc, "iterations": it, "converged": converged.cpu().numpy(),
-           "setup_s": t_setup, "scf_s": t_scf, "graph": graph is not None, "autotuned": schedule is not None,
+           "setup_s": t_setup, "setup_stages_s": stages, "scf_s": t_scf, "graph": graph is not None,
+           "autotuned": schedule is not None,
            "build_ms_mean": 1e3 * float(np.mean(build_times)), "nmol": nmol}
     if gradient:
         t2 = time.perf_counter()

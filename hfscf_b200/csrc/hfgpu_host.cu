@@ -13,6 +13,7 @@
 #include "hfgpu_launch.h"
 #include "hfgpu_onee.h"
 #include "hfgpu_onee_kernels.cuh"
+#include "hfgpu_batch_eigh.cuh"
 
 namespace {
 
@@ -409,33 +410,28 @@ int build_quartets(hfgpu_handle* h) {
       long long* seg_start[4] = {&h->q_beg[qc], &h->q_hik1[qc], &h->q_mid[qc], &h->q_hik2[qc]};
       for (int sg = 0; sg < 4; ++sg) {
         *seg_start[sg] = (long long)all.size();
-        // stable counting sort by bound decade
-        std::vector<int> dec(parts[sg].size());
-        long long cnt[kBuckets] = {0};
+        // one stable counting sort on (bound decade, largest primitive-quartet count first):
+        // the decades make the prefix launches of density-screened builds possible, the
+        // counts let the 32 lanes of a warp loop over similar numbers of primitive quartets
+        std::vector<int> key(parts[sg].size());
+        int maxprod = 0;
+        for (const int2& pqv : parts[sg])
+          maxprod = std::max(maxprod, h->pairs[pqv.x].nprim * h->pairs[pqv.y].nprim);
+        const int nk = kBuckets * (maxprod + 1);
+        std::vector<long long> cnt((size_t)nk + 1, 0);
         for (size_t x = 0; x < parts[sg].size(); ++x) {
           const int2 pqv = parts[sg][x];
-          dec[x] = bound_decade(h->pairs[pqv.x].schwarz * h->pairs[pqv.y].schwarz);
-          ++cnt[dec[x]];
+          const int dec = bound_decade(h->pairs[pqv.x].schwarz * h->pairs[pqv.y].schwarz);
+          const int prod = h->pairs[pqv.x].nprim * h->pairs[pqv.y].nprim;
+          key[x] = dec * (maxprod + 1) + (maxprod - prod);
+          ++cnt[(size_t)key[x] + 1];
         }
-        long long pos[kBuckets];
-        long long acc = (long long)all.size();
-        for (int e = 0; e < kBuckets; ++e) {
-          pos[e] = acc;
-          acc += cnt[e];
-          h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e] = acc;
-        }
-        all.resize(acc);
-        for (size_t x = 0; x < parts[sg].size(); ++x) all[pos[dec[x]]++] = parts[sg][x];
-        // inside a decade: by primitive-quartet count, largest first (stable, so bra-major
-        // within equal counts), so that the 32 lanes of a warp loop over similar counts
-        for (int e = 0; e < kBuckets; ++e) {
-          const long long lo = e == 0 ? *seg_start[sg] : h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e - 1];
-          const long long hi = h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e];
-          if (hi - lo > 1)
-            std::stable_sort(all.begin() + lo, all.begin() + hi, [h](const int2& u, const int2& v) {
-              return h->pairs[u.x].nprim * h->pairs[u.y].nprim > h->pairs[v.x].nprim * h->pairs[v.y].nprim;
-            });
-        }
+        const long long base = (long long)all.size();
+        for (int k = 0; k < nk; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];  // cnt[k] = first slot of key k
+        for (int e = 0; e < kBuckets; ++e)
+          h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e] = base + cnt[(size_t)(e + 1) * (maxprod + 1)];
+        all.resize((size_t)base + parts[sg].size());
+        for (size_t x = 0; x < parts[sg].size(); ++x) all[(size_t)base + (size_t)cnt[(size_t)key[x]]++] = parts[sg][x];
       }
       h->q_end[qc] = (long long)all.size();
     }
@@ -1351,6 +1347,21 @@ int hfgpu_one_electron_grad_device(hfgpu_handle* h, const double* Z, const doubl
     onee_grad_kernel<<<(unsigned)((nitems + 127) / 128), 128, 0, h->stream>>>(a, nitems, D, W, cH, cS, grad);
     HF_CHECK_LAUNCH(h, "one-electron gradient");
   }
+  return HFGPU_OK;
+}
+
+int hfgpu_batch_eigh(hfgpu_handle* h, const double* A, double* W, double* V, int* sweeps) {
+  if (!h || !A || !W || !V) return HFGPU_ERR_INVALID;
+  if (!h->batched) return fail(h, HFGPU_ERR_UNSUPPORTED, "hfgpu_batch_eigh needs a batched handle");
+  const int nmax = h->n;
+  if (nmax > kJacobiMaxN) return fail(h, HFGPU_ERR_UNSUPPORTED, "batched eigensolver: a molecule has more than 118 functions");
+  int rc = set_device(h);
+  if (rc) return rc;
+  const size_t smem = jacobi_smem_bytes(nmax);
+  HF_CUDA(h, cudaFuncSetAttribute(batch_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int* mol_n = reinterpret_cast<const int*>(h->d_mol.as<long long>() + h->nmol);
+  batch_jacobi_kernel<<<h->nmol, kJacobiThreads, smem, h->stream>>>(A, nmax, mol_n, W, V, 30, sweeps);
+  HF_CHECK_LAUNCH(h, "batched eigensolver");
   return HFGPU_OK;
 }
 

@@ -153,6 +153,14 @@ int hfgpu_batch_layout(const hfgpu_handle* h, int* nbf, long long* mat_off, long
 int hfgpu_batch_jk_device(hfgpu_handle* h, const double* D, double* J, double* K, int precision);
 /* grad (device, total atoms x 3) += two-electron RHF gradient of every molecule. */
 int hfgpu_batch_grad2e_device(hfgpu_handle* h, const double* D, double* grad, int precision);
+/* Eigenvalues W (nmol x nmax, ascending) and eigenvectors V (nmol x nmax x nmax, columns) of
+ * every molecule's symmetric matrix in A (nmol x nmax x nmax, padded; nmax = the largest
+ * molecule's function count, at most 118), for the batched SCF's diagonalisation step; the
+ * reference diagonalises one molecule with Eigen (src/scfsolver/hfscf_hf_solver.cpp:206-242).
+ * Cyclic Jacobi, one thread block per molecule; entries outside a molecule's block pass
+ * through as identity eigenvectors.  sweeps (device, nmol ints, may be NULL) receives the
+ * Jacobi sweeps each molecule took.  Device pointers, enqueued on the handle's stream. */
+int hfgpu_batch_eigh(hfgpu_handle* h, const double* A, double* W, double* V, int* sweeps);
 
 /* One-electron matrices S, T, V (n x n) for the basis at xyz (bohr), on the host CPU.
  * Z: nuclear charges per atom.  Needs no handle and no GPU (the reference's

@@ -40,10 +40,11 @@ def test_batch_jk_matches_single_molecule_engine():
     be.close()
 
 
-@pytest.mark.parametrize("use_graph", [True, False], ids=["cuda-graph", "eager"])
-def test_batch_scf_and_gradients_match_single_molecule_runs(use_graph):
+@pytest.mark.parametrize("use_graph,diag", [(True, "gpu"), (False, "gpu"), (True, "host")],
+                         ids=["cuda-graph", "eager", "host-diag"])
+def test_batch_scf_and_gradients_match_single_molecule_runs(use_graph, diag):
     bases = _mols(10)
-    out = batch.batch_rhf(bases, use_graph=use_graph, e_tol=1e-11, rms_tol=1e-9)
+    out = batch.batch_rhf(bases, use_graph=use_graph, e_tol=1e-11, rms_tol=1e-9, diag=diag)
     assert out["converged"].all()
     for m, b in enumerate(bases):
         with E.Engine(b) as e1:
@@ -51,3 +52,36 @@ def test_batch_scf_and_gradients_match_single_molecule_runs(use_graph):
             g = scf.rhf_gradient(b, r, e1)
         assert abs(out["energies"][m] - r.energy) < 1e-8
         assert np.max(np.abs(out["gradients"][m] - g)) < 1e-6
+
+
+def test_batched_eigensolver_matches_lapack():
+    """hfgpu_batch_eigh against numpy's LAPACK eigh on random symmetric blocks of uneven size."""
+    import torch
+    bases = _mols(9, seed=7)
+    be = batch.BatchEngine(bases)
+    nmol, nmax = len(bases), int(be.nbf.max())
+    rng = np.random.default_rng(5)
+    A = np.zeros((nmol, nmax, nmax))
+    for k in range(nmol):
+        n = int(be.nbf[k])
+        R = rng.normal(size=(n, n))
+        A[k, :n, :n] = (R + R.T) / 2
+        A[k, np.arange(n, nmax), np.arange(n, nmax)] = 1e3
+    dev = torch.device("cuda", 0)
+    Ad = torch.from_numpy(A).to(dev)
+    W = torch.empty((nmol, nmax), dtype=torch.float64, device=dev)
+    V = torch.empty((nmol, nmax, nmax), dtype=torch.float64, device=dev)
+    sw = torch.zeros(nmol, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    be.eigh(Ad, W, V, sw)
+    torch.cuda.synchronize()
+    Wn, Vn, swn = W.cpu().numpy(), V.cpu().numpy(), sw.cpu().numpy()
+    be.close()
+    for k in range(nmol):
+        n = int(be.nbf[k])
+        w0 = np.linalg.eigvalsh(A[k, :n, :n])
+        assert np.abs(Wn[k, :n] - w0).max() < 1e-11 * max(1.0, np.abs(w0).max())
+        Vk = Vn[k, :n, :n]
+        assert np.abs(Vk.T @ Vk - np.eye(n)).max() < 1e-12
+        assert np.abs(A[k, :n, :n] @ Vk - Vk * Wn[k, :n]).max() < 1e-11
+        assert (Wn[k, n:] == 1e3).all() and swn[k] < 30
