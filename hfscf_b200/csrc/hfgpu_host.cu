@@ -1,6 +1,8 @@
 // Host side of the hfgpu engine: basis set-up, primitive-pair data, Schwarz
 // factors, screened quartet lists, and the C ABI of include/hfgpu.h.
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -381,61 +383,96 @@ int bound_decade(double b) {
 }
 
 // Screened unique quartets (P <= Q within a class; bra class >= ket class), per class.
-int build_quartets(hfgpu_handle* h) {
+// Quartet list of one class (pair classes cp >= cq), in four segments, each ordered by one
+// stable counting sort on (bound decade, largest primitive-quartet count first): the decades
+// make the prefix launches of density-screened builds possible, the counts let the 32 lanes
+// of a warp loop over similar numbers of primitive quartets.  Offsets are relative to the
+// start of the class's list.
+struct ClassList {
+  std::vector<int2> q;
+  long long seg[5] = {0, 0, 0, 0, 0};
+  long long bend[4 * kBuckets] = {0};
+};
+
+static void build_class_list(const hfgpu_handle* h, int cp, int cq, ClassList& out) {
   const double tol = h->opts.schwarz_tol, mix = h->opts.mixed_fp32_bound;
-  std::vector<int2> all;
   std::vector<int2> parts[4];  // high bound many-prim, high bound few-prim, low bound many, low bound few
-  h->nquartets = 0;
-  h->bucket_end.assign((size_t)hfgpu::kNumClasses * 4 * kBuckets, 0);
-  for (int cp = 0; cp < kPairClasses; ++cp)
-    for (int cq = 0; cq <= cp; ++cq) {
-      const int qc = quartet_class(cp, cq);
-      for (auto& v : parts) v.clear();
-      const int nm1 = h->nmol + 1;
-      for (int mol = 0; mol < h->nmol; ++mol) {
-      const int pb = h->cm_begin[(size_t)cp * nm1 + mol], pe = h->cm_begin[(size_t)cp * nm1 + mol + 1];
-      const int kb = h->cm_begin[(size_t)cq * nm1 + mol], ke = h->cm_begin[(size_t)cq * nm1 + mol + 1];
-      for (int P = pb; P < pe; ++P) {
-        const double qp = h->pairs[P].schwarz;
-        const int np = h->pairs[P].nprim;
-        const int k0 = (cp == cq) ? P : kb;
-        for (int Q = k0; Q < ke; ++Q) {
-          const double b = qp * h->pairs[Q].schwarz;
-          if (b < tol) continue;
-          const bool many = np * h->pairs[Q].nprim >= kPrimWarpMinPrims;
-          parts[(b >= mix ? 0 : 2) + (many ? 0 : 1)].push_back(make_int2(P, Q));
-        }
+  const int nm1 = h->nmol + 1;
+  for (int mol = 0; mol < h->nmol; ++mol) {
+    const int pb = h->cm_begin[(size_t)cp * nm1 + mol], pe = h->cm_begin[(size_t)cp * nm1 + mol + 1];
+    const int kb = h->cm_begin[(size_t)cq * nm1 + mol], ke = h->cm_begin[(size_t)cq * nm1 + mol + 1];
+    for (int P = pb; P < pe; ++P) {
+      const double qp = h->pairs[P].schwarz;
+      const int np = h->pairs[P].nprim;
+      const int k0 = (cp == cq) ? P : kb;
+      for (int Q = k0; Q < ke; ++Q) {
+        const double b = qp * h->pairs[Q].schwarz;
+        if (b < tol) continue;
+        const bool many = np * h->pairs[Q].nprim >= kPrimWarpMinPrims;
+        parts[(b >= mix ? 0 : 2) + (many ? 0 : 1)].push_back(make_int2(P, Q));
       }
-      }
-      long long* seg_start[4] = {&h->q_beg[qc], &h->q_hik1[qc], &h->q_mid[qc], &h->q_hik2[qc]};
-      for (int sg = 0; sg < 4; ++sg) {
-        *seg_start[sg] = (long long)all.size();
-        // one stable counting sort on (bound decade, largest primitive-quartet count first):
-        // the decades make the prefix launches of density-screened builds possible, the
-        // counts let the 32 lanes of a warp loop over similar numbers of primitive quartets
-        std::vector<int> key(parts[sg].size());
-        int maxprod = 0;
-        for (const int2& pqv : parts[sg])
-          maxprod = std::max(maxprod, h->pairs[pqv.x].nprim * h->pairs[pqv.y].nprim);
-        const int nk = kBuckets * (maxprod + 1);
-        std::vector<long long> cnt((size_t)nk + 1, 0);
-        for (size_t x = 0; x < parts[sg].size(); ++x) {
-          const int2 pqv = parts[sg][x];
-          const int dec = bound_decade(h->pairs[pqv.x].schwarz * h->pairs[pqv.y].schwarz);
-          const int prod = h->pairs[pqv.x].nprim * h->pairs[pqv.y].nprim;
-          key[x] = dec * (maxprod + 1) + (maxprod - prod);
-          ++cnt[(size_t)key[x] + 1];
-        }
-        const long long base = (long long)all.size();
-        for (int k = 0; k < nk; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];  // cnt[k] = first slot of key k
-        for (int e = 0; e < kBuckets; ++e)
-          h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e] = base + cnt[(size_t)(e + 1) * (maxprod + 1)];
-        all.resize((size_t)base + parts[sg].size());
-        for (size_t x = 0; x < parts[sg].size(); ++x) all[(size_t)base + (size_t)cnt[(size_t)key[x]]++] = parts[sg][x];
-      }
-      h->q_end[qc] = (long long)all.size();
     }
-  h->nquartets = (long long)all.size();
+  }
+  size_t total = 0;
+  for (auto& v : parts) total += v.size();
+  out.q.resize(total);
+  long long base = 0;
+  for (int sg = 0; sg < 4; ++sg) {
+    out.seg[sg] = base;
+    const std::vector<int2>& in = parts[sg];
+    std::vector<int> key(in.size());
+    int maxprod = 0;
+    for (const int2& pqv : in) maxprod = std::max(maxprod, h->pairs[pqv.x].nprim * h->pairs[pqv.y].nprim);
+    const int nk = kBuckets * (maxprod + 1);
+    std::vector<long long> cnt((size_t)nk + 1, 0);
+    for (size_t x = 0; x < in.size(); ++x) {
+      const int2 pqv = in[x];
+      const int dec = bound_decade(h->pairs[pqv.x].schwarz * h->pairs[pqv.y].schwarz);
+      const int prod = h->pairs[pqv.x].nprim * h->pairs[pqv.y].nprim;
+      key[x] = dec * (maxprod + 1) + (maxprod - prod);
+      ++cnt[(size_t)key[x] + 1];
+    }
+    for (int k = 0; k < nk; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];  // cnt[k] = first slot of key k
+    for (int e = 0; e < kBuckets; ++e) out.bend[sg * kBuckets + e] = base + cnt[(size_t)(e + 1) * (maxprod + 1)];
+    for (size_t x = 0; x < in.size(); ++x) out.q[(size_t)base + (size_t)cnt[(size_t)key[x]]++] = in[x];
+    base += (long long)in.size();
+  }
+  out.seg[4] = base;
+}
+
+int build_quartets(hfgpu_handle* h) {
+  // the 21 classes are independent: built on host threads, then concatenated in class order
+  std::vector<std::pair<int, int>> cls;
+  for (int cp = 0; cp < kPairClasses; ++cp)
+    for (int cq = 0; cq <= cp; ++cq) cls.emplace_back(cp, cq);
+  std::vector<ClassList> lists(cls.size());
+  std::atomic<int> next{0};
+  auto work = [&]() {
+    for (int i = next++; i < (int)cls.size(); i = next++) build_class_list(h, cls[i].first, cls[i].second, lists[i]);
+  };
+  const int nthr = (int)std::min<size_t>(cls.size(), std::max(1u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  h->bucket_end.assign((size_t)hfgpu::kNumClasses * 4 * kBuckets, 0);
+  long long total = 0;
+  for (const ClassList& l : lists) total += (long long)l.q.size();
+  std::vector<int2> all((size_t)total);
+  long long base = 0;
+  for (size_t i = 0; i < cls.size(); ++i) {
+    const int qc = quartet_class(cls[i].first, cls[i].second);
+    const ClassList& l = lists[i];
+    h->q_beg[qc] = base + l.seg[0];
+    h->q_hik1[qc] = base + l.seg[1];
+    h->q_mid[qc] = base + l.seg[2];
+    h->q_hik2[qc] = base + l.seg[3];
+    h->q_end[qc] = base + l.seg[4];
+    for (int x = 0; x < 4 * kBuckets; ++x) h->bucket_end[(size_t)qc * 4 * kBuckets + x] = base + l.bend[x];
+    std::copy(l.q.begin(), l.q.end(), all.begin() + base);
+    base += (long long)l.q.size();
+  }
+  h->nquartets = total;
   HF_CUDA(h, h->d_quart.ensure(sizeof(int2) * std::max<size_t>(all.size(), 1)));
   if (!all.empty())
     HF_CUDA(h, cudaMemcpyAsync(h->d_quart.p, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, h->stream));
