@@ -204,13 +204,13 @@ def run_ours(args, world, rank, local):
         tune_s = time.perf_counter() - t
     torch.cuda.synchronize()
     t = time.perf_counter()
-    res = scf.rhf(bs, engine=eng)
+    res = scf.rhf(bs, engine=eng, guess="sad")  # the reference's default guess
     scf_wall = time.perf_counter() - t
     t = time.perf_counter()
     grad = scf.rhf_gradient(bs, res, eng)
     grad_wall = time.perf_counter() - t
     t = time.perf_counter()
-    res_mx = scf.rhf(bs, engine=eng, precision=E.MIXED, incremental=True)
+    res_mx = scf.rhf(bs, engine=eng, precision=E.MIXED, incremental=True, guess="sad")
     mixed_wall = time.perf_counter() - t
     t = time.perf_counter()
     grad_mx = scf.rhf_gradient(bs, res_mx, eng, E.MIXED)
@@ -323,7 +323,8 @@ def run_ours(args, world, rank, local):
                        "quartets_screened": int(sum(class_work[c]["screened"] for c in range(E.NUM_CLASSES))),
                        "quartets_computed_last_build": int(sum(class_work[c]["computed"] for c in range(E.NUM_CLASSES)))},
             "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
-            "scf": {"energy": res.energy, "iterations": res.iterations, "converged": res.converged,
+            "scf": {"guess": "SAD", "energy": res.energy, "iterations": res.iterations, "converged": res.converged,
+                    "mixed_iterations": res_mx.iterations,
                     "wall_s": scf_wall, "grad_wall_s": grad_wall, "grad_max": float(np.max(np.abs(grad))),
                     "mixed_incremental_energy": res_mx.energy, "mixed_dE": res_mx.energy - res.energy,
                     "mixed_wall_s": mixed_wall, "e_nuc": nuclear_repulsion(bs.Z, bs.coords),

@@ -80,13 +80,152 @@ class ScfResult:
     energies: list = field(default_factory=list)
 
 
+class DiisUhf:
+    """Restatement of the two-spin DIIS_SOLVER::diis_solver::diis_extrapolate
+    (src/scfsolver/hfscf_diis.cpp:126-260): error vectors of both spins concatenated, the
+    largest-error entry dropped when over the limit, rms per spin 0.5 sqrt(mean(e^2))."""
+
+    def __init__(self, nvec=6):
+        self.nvec = nvec
+        self.Fa, self.Fb, self.E, self.rms_list = [], [], [], []
+        self.rms_a = self.rms_b = np.inf
+
+    def extrapolate(self, Fa, Fb, S, Da, Db, X):
+        if len(self.rms_list) > self.nvec:
+            pos = int(np.argmax(self.rms_list))
+            del self.Fa[pos], self.Fb[pos], self.E[pos], self.rms_list[pos]
+        ga = X.T @ (Fa @ Da @ S - (Fa @ Da @ S).T) @ X
+        gb = X.T @ (Fb @ Db @ S - (Fb @ Db @ S).T) @ X
+        self.rms_a = 0.5 * float(np.sqrt(np.mean(ga * ga)))
+        self.rms_b = 0.5 * float(np.sqrt(np.mean(gb * gb)))
+        self.E.append(np.concatenate([ga.ravel(), gb.ravel()]))
+        self.Fa.append(Fa.copy())
+        self.Fb.append(Fb.copy())
+        self.rms_list.append(self.rms_a + self.rms_b)
+        if len(self.rms_list) > 1:
+            m = len(self.E)
+            B = np.empty((m + 1, m + 1))
+            for i in range(m):
+                for j in range(m):
+                    B[i, j] = float(self.E[i] @ self.E[j])
+            if np.abs(B[:m, :m]).sum() < DIIS_EPS:
+                B[:m, :m] /= B[:m, :m].max()
+            B[m, :] = -1.0
+            B[:, m] = -1.0
+            B[m, m] = 0.0
+            rhs = np.zeros(m + 1)
+            rhs[m] = -1.0
+            q, r = np.linalg.qr(B)
+            c = np.linalg.solve(r, q.T @ rhs)
+            Fa = sum(c[k] * self.Fa[k] for k in range(m))
+            Fb = sum(c[k] * self.Fb[k] for k in range(m))
+        return Fa, Fb
+
+
+def sad_populations(Z: int, norb: int):
+    """Frozen-core and fractional valence occupations of the SAD atom
+    (Mol::sad_uhf_solver::get_pop_numbers, src/scfsolver/hfscf_sad.cpp:198-245): the noble-gas
+    core below Z is frozen (weight 1), the next shell's orbitals share the remaining electrons
+    (weight sqrt(n_valence / 2 n_active) on the MO coefficients).  Returns (weights, n_occupied)."""
+    zvalues = [0, 2, 10, 18, 36, 54, 86, 118]
+    k = next(i for i, z in enumerate(zvalues) if z >= Z)
+    if zvalues[k] > Z:
+        k -= 1
+    if zvalues[k] == Z:
+        nfrozen, nactive = 0, zvalues[k] // 2
+    else:
+        nfrozen = zvalues[k] // 2
+        nactive = zvalues[k + 1] // 2 - nfrozen
+    nactive = min(nactive, norb - nfrozen)
+    w = np.zeros(norb)
+    w[:nfrozen] = 1.0
+    w[nfrozen:nfrozen + nactive] = np.sqrt((Z - 2.0 * nfrozen) / (2.0 * nactive))
+    return w, nfrozen + nactive
+
+
+def sad_atom_density(Z: int, S, T, V, jk, rms_tol=1e-6, e_tol=1e-5, max_iter=25):
+    """Spin-averaged density of one atom from the SAD atomic UHF
+    (Mol::sad_uhf_solver, src/scfsolver/hfscf_sad.cpp:13-476): H = T + V of the atom's own
+    nucleus, S^-1/2 orthogonalisation, fractional occupations (sad_populations), Fock
+    F_a = H + J[Da + Db] - K[Da] (and b) from ``jk(DJ, DK_list) -> (J, [K...])``, two-spin
+    DIIS over 6 vectors, converged when both rms < rms_tol and |dE| < e_tol (or the rms sum
+    < 1e-14).  Returns 0.5 (Da + Db)."""
+    H = T + V
+    w, U = np.linalg.eigh(S)
+    X = U @ np.diag(1.0 / np.sqrt(w)) @ U.T
+    pop, occ = sad_populations(Z, S.shape[0])
+
+    def density(Fp):
+        _, C = np.linalg.eigh(Fp)
+        mo = X @ C * pop[None, :]
+        return mo[:, :occ] @ mo[:, :occ].T
+
+    Da = density(X.T @ H @ X)
+    Db = Da.copy()
+    E = float(np.sum(Da * H))
+    diis = DiisUhf(6)
+    it = 0
+    while True:
+        it += 1
+        J, K = jk(Da + Db, [Da, Db])
+        Fa = H + J - K[0]
+        Fb = H + J - K[1]
+        Fa, Fb = diis.extrapolate(Fa, Fb, S, Da, Db, X)
+        Da, Db = density(X.T @ Fa @ X), density(X.T @ Fb @ X)
+        E_prev, E = E, 0.5 * float(np.sum(Da * (H + Fa)) + np.sum(Db * (H + Fb)))
+        if diis.rms_a < rms_tol and diis.rms_b < rms_tol and abs(E - E_prev) < e_tol:
+            break
+        if diis.rms_a + diis.rms_b < 1e-14:
+            break
+        if it >= max_iter:
+            raise RuntimeError(f"SAD atom Z={Z} did not converge in {max_iter} iterations")
+    return 0.5 * (Da + Db)
+
+
+def atom_basis(basis: Basis, atom: int) -> Basis:
+    """The shells of one atom as a basis of their own (the atom's block of the molecule's basis)."""
+    shells, idx, ids = [], 0, 0
+    for s in basis.shells:
+        if s.atom != atom:
+            continue
+        shells.append(type(s)(L=s.L, atom=0, center=s.center, exps=s.exps, coefs=s.coefs, idx=idx, ids=ids))
+        idx += (s.L + 1) * (s.L + 2) // 2
+        ids += 2 * s.L + 1
+    return Basis(name=basis.name, pure=basis.pure, Z=np.asarray([basis.Z[atom]]),
+                 coords=np.asarray(basis.coords[atom]).reshape(1, 3), shells=shells)
+
+
+def sad_guess(basis: Basis, engine_factory=None) -> np.ndarray:
+    """Superposition-of-atomic-densities guess (Mol::hf_solver::get_sad_guess,
+    src/scfsolver/hfscf_hf_solver.cpp:478-553): one atomic UHF per element (first atom of
+    that element), its spin-averaged density copied onto the diagonal block of every atom of
+    the element.  The atomic J/K builds run on the GPU engine of the atom's basis."""
+    n = basis.nbf
+    D = np.zeros((n, n))
+    first = {}
+    bf_atom = basis.bf_atom()
+    for a, Zc in enumerate(basis.Z):
+        first.setdefault(int(Zc), a)
+    for Zc, a0 in first.items():
+        ab = atom_basis(basis, a0)
+        with (engine_factory or eng.Engine)(ab) as e:
+            S, T, V = e.one_electron()
+            Dat = sad_atom_density(Zc, S, T, V, lambda DJ, DKs: e.jk(DJ, DKs))
+        for a, Za in enumerate(basis.Z):
+            if int(Za) != Zc:
+                continue
+            f = np.nonzero(bf_atom == a)[0]
+            D[np.ix_(f, f)] = Dat
+    return D
+
+
 def sym_orth(S):
     w, U = np.linalg.eigh(S)
     return (U / np.sqrt(w)) @ U.T
 
 
 def rhf(basis: Basis, fock=None, *, H=None, S=None, e_tol=1e-10, rms_tol=1e-8, diis_range=5, max_iter=50,
-        precision=eng.FP64, incremental=False, engine=None, D0=None) -> ScfResult:
+        precision=eng.FP64, incremental=False, engine=None, D0=None, guess="core") -> ScfResult:
     """Restricted HF to convergence.  ``fock(D, H) -> F`` builds the Fock matrix;
     by default the GPU engine's RHF Fock build.  With ``incremental`` the engine
     builds F_k = F_{k-1} + 2J[dD] - K[dD] (density screening on |dD|), with a full
@@ -103,6 +242,8 @@ def rhf(basis: Basis, fock=None, *, H=None, S=None, e_tol=1e-10, rms_tol=1e-8, d
         S_, T_, V_ = engine.one_electron() if engine is not None else eng.one_electron(basis)
         S, H = S_, T_ + V_
     X = sym_orth(S)
+    if D0 is None and guess == "sad":
+        D0 = sad_guess(basis)
     # CORE guess (deterministic): diagonalise X^T H X
     if D0 is None:
         eps, Cp = np.linalg.eigh(X.T @ H @ X)

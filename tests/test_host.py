@@ -143,3 +143,36 @@ def test_one_electron_gradient_matches_finite_differences():
                 S, T, V = E.one_electron(bs.with_coords(xx))
                 vals.append(2 * np.sum(D * (T + V)) - 2 * np.sum(W * S))
             assert abs((vals[0] - vals[1]) / (2 * h) - g[a, d]) < 1e-6
+
+
+def test_sad_populations_follow_the_reference():
+    """Frozen-core / fractional valence weights of get_pop_numbers (hfscf_sad.cpp:198-245)."""
+    from hfscf_b200 import scf
+    w, occ = scf.sad_populations(1, 2)
+    assert occ == 1 and np.allclose(w, [np.sqrt(0.5), 0.0])
+    w, occ = scf.sad_populations(6, 14)
+    assert occ == 5 and w[0] == 1.0 and np.allclose(w[1:5], np.sqrt(0.5)) and (w[5:] == 0).all()
+    w, occ = scf.sad_populations(8, 14)
+    assert occ == 5 and np.allclose(w[1:5], np.sqrt(6 / 8))
+    w, occ = scf.sad_populations(2, 5)
+    assert occ == 1 and w[0] == 1.0
+
+
+def test_sad_atom_density_with_oracle_jk_holds_the_atom_electrons():
+    """The SAD atomic UHF run with the oracle's J/K (CPU): the spin-averaged density
+    carries Z/2 electrons in the atom's overlap metric."""
+    import oracle
+    from hfscf_b200 import scf
+    Z, x = M.water(np.random.default_rng(2))
+    bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    for a in (0, 1):
+        ab = scf.atom_basis(bs, a)
+        S, T, V = E.one_electron(ab)
+        eri = oracle.eri_packed(ab)
+
+        def jk(DJ, DKs):
+            J = oracle.jk(eri, DJ)[0]
+            return J, [oracle.jk(eri, Dk)[1] for Dk in DKs]
+
+        D = scf.sad_atom_density(int(ab.Z[0]), S, T, V, jk)
+        assert abs(np.sum(D * S) - ab.Z[0] / 2) < 1e-10
