@@ -195,11 +195,12 @@ def atom_basis(basis: Basis, atom: int) -> Basis:
                  coords=np.asarray(basis.coords[atom]).reshape(1, 3), shells=shells)
 
 
-def sad_guess(basis: Basis, engine_factory=None) -> np.ndarray:
+def sad_guess(basis: Basis, engine_factory=None, rms_tol=1e-6, e_tol=1e-5, max_iter=25) -> np.ndarray:
     """Superposition-of-atomic-densities guess (Mol::hf_solver::get_sad_guess,
     src/scfsolver/hfscf_hf_solver.cpp:478-553): one atomic UHF per element (first atom of
     that element), its spin-averaged density copied onto the diagonal block of every atom of
-    the element.  The atomic J/K builds run on the GPU engine of the atom's basis."""
+    the element.  The atomic J/K builds run on the GPU engine of the atom's basis.  The
+    tolerances default to the reference's SAD settings (src/settings/hfscf_settings.hpp:35-50)."""
     n = basis.nbf
     D = np.zeros((n, n))
     first = {}
@@ -210,7 +211,7 @@ def sad_guess(basis: Basis, engine_factory=None) -> np.ndarray:
         ab = atom_basis(basis, a0)
         with (engine_factory or eng.Engine)(ab) as e:
             S, T, V = e.one_electron()
-            Dat = sad_atom_density(Zc, S, T, V, lambda DJ, DKs: e.jk(DJ, DKs))
+            Dat = sad_atom_density(Zc, S, T, V, lambda DJ, DKs: e.jk(DJ, DKs), rms_tol, e_tol, max_iter)
         for a, Za in enumerate(basis.Z):
             if int(Za) != Zc:
                 continue
