@@ -202,19 +202,23 @@ def run_ours(args, world, rank, local):
         t = time.perf_counter()
         eng.autotune(core_guess_density(bs, S0, T0 + V0), E.FP64, 3)
         tune_s = time.perf_counter() - t
-    torch.cuda.synchronize()
-    t = time.perf_counter()
-    res = scf.rhf(bs, engine=eng, guess="sad")  # the reference's default guess
-    scf_wall = time.perf_counter() - t
-    t = time.perf_counter()
-    grad = scf.rhf_gradient(bs, res, eng)
-    grad_wall = time.perf_counter() - t
-    t = time.perf_counter()
-    res_mx = scf.rhf(bs, engine=eng, precision=E.MIXED, incremental=True, guess="sad")
-    mixed_wall = time.perf_counter() - t
-    t = time.perf_counter()
-    grad_mx = scf.rhf_gradient(bs, res_mx, eng, E.MIXED)
-    grad_mx_wall = time.perf_counter() - t
+    # SCF + gradient time-to-solution, FP64 and mixed, each from the SAD guess (the
+    # reference's default).  The whole sequence runs twice and the second pass is kept, so
+    # neither mode pays the first launch of any kernel.
+    for _pass in range(2):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        res = scf.rhf(bs, engine=eng, guess="sad")
+        scf_wall = time.perf_counter() - t
+        t = time.perf_counter()
+        grad = scf.rhf_gradient(bs, res, eng)
+        grad_wall = time.perf_counter() - t
+        t = time.perf_counter()
+        res_mx = scf.rhf(bs, engine=eng, precision=E.MIXED, incremental=True, guess="sad")
+        mixed_wall = time.perf_counter() - t
+        t = time.perf_counter()
+        grad_mx = scf.rhf_gradient(bs, res_mx, eng, E.MIXED)
+        grad_mx_wall = time.perf_counter() - t
     S, T, V = E.one_electron(bs)
     H = T + V
     dev = torch.device("cuda", local)
