@@ -237,6 +237,9 @@ def rhf(basis: Basis, fock=None, *, H=None, S=None, e_tol=1e-10, rms_tol=1e-8, d
     nocc = nel // 2
     if fock is None:
         engine = engine or eng.Engine(basis)
+        if H is None and S is None:
+            return _rhf_device(basis, engine, e_tol=e_tol, rms_tol=rms_tol, diis_range=diis_range,
+                               max_iter=max_iter, precision=precision, incremental=incremental, D0=D0, guess=guess)
         fock = lambda D, H_: engine.fock_rhf(D, H_, precision)  # noqa: E731
     if H is None or S is None:
         # one-electron matrices on the GPU when there is an engine, on the host otherwise
@@ -285,6 +288,125 @@ def rhf(basis: Basis, fock=None, *, H=None, S=None, e_tol=1e-10, rms_tol=1e-8, d
     enuc = nuclear_repulsion(basis.Z, basis.coords)
     res.energy, res.e_elec, res.e_nuc = E + enuc, E, enuc
     res.D, res.F, res.C, res.eps, res.iterations = D, F, C, eps, it
+    return res
+
+
+def _rhf_device(basis: Basis, engine, *, e_tol, rms_tol, diis_range, max_iter, precision, incremental, D0,
+                guess) -> ScfResult:
+    """The loop of rhf() with every matrix on the GPU: J/K through hfgpu_jk_device, the
+    one-electron matrices through hfgpu_one_electron_device, DIIS (as Diis) and the
+    diagonalisations in torch on the device; per iteration only the DIIS matrix and two
+    scalars come back to the host.  Same steps, order and convergence test as the host loop."""
+    import torch
+    dev = torch.device("cuda", engine._opts.device)
+    cur = torch.cuda.current_stream(dev)
+    # the engine's kernels and torch's ops must share one stream: the caller's, unless that is
+    # the legacy default stream (which the engine's non-blocking stream does not wait for)
+    private = cur.cuda_stream == 0
+    stream = torch.cuda.Stream(dev) if private else cur
+    engine.set_stream(stream.cuda_stream)
+    try:
+        with torch.cuda.stream(stream):
+            return _rhf_device_loop(basis, engine, dev, e_tol=e_tol, rms_tol=rms_tol, diis_range=diis_range,
+                                    max_iter=max_iter, precision=precision, incremental=incremental, D0=D0,
+                                    guess=guess)
+    finally:
+        if private:
+            torch.cuda.synchronize(dev)
+            engine.set_stream(None)
+
+
+def _rhf_device_loop(basis, engine, dev, *, e_tol, rms_tol, diis_range, max_iter, precision, incremental, D0,
+                     guess) -> ScfResult:
+    import torch
+    n = basis.nbf
+    nocc = int(np.sum(basis.Z)) // 2
+    f64 = dict(dtype=torch.float64, device=dev)
+    M = torch.empty((3, n, n), **f64)
+    engine.one_electron_device(M[0].data_ptr(), M[1].data_ptr(), M[2].data_ptr())
+    S = M[0]
+    H = M[1] + M[2]
+    w, U = torch.linalg.eigh(S)
+    X = (U * w.rsqrt()) @ U.T
+    J = torch.empty((n, n), **f64)
+    K = torch.empty((n, n), **f64)
+
+    def two_e(Dm):
+        Dm = Dm.contiguous()
+        engine.jk_device(Dm.data_ptr(), 1, Dm.data_ptr(), J.data_ptr(), K.data_ptr(), precision)
+        return 2.0 * J - K
+
+    if D0 is None and guess == "sad":
+        D0 = sad_guess(basis)
+    if D0 is None:
+        eps, Cp = torch.linalg.eigh(X.T @ H @ X)
+        C = X @ Cp
+        D = C[:, :nocc] @ C[:, :nocc].T
+    else:
+        D = torch.from_numpy(np.ascontiguousarray(D0)).to(dev)
+        C = eps = None
+    E = float((D * (H + H)).sum())
+    res = ScfResult(0, 0, 0, None, None, None, None, 0, False)
+    Fs, Es, rms_list = [], [], []  # DIIS history
+    F_last = D_last = None
+    it = 0
+    while True:
+        it += 1
+        t = time.perf_counter()
+        if incremental and F_last is not None and (it % 8) != 0:
+            F = F_last + two_e(D - D_last)
+        else:
+            F = H + two_e(D)
+        torch.cuda.synchronize(dev)
+        res.fock_times.append(time.perf_counter() - t)
+        F_last, D_last = F, D
+        # DIIS (Diis.extrapolate on the device)
+        if len(rms_list) > diis_range:
+            pos = int(np.argmax(rms_list))
+            del Fs[pos], Es[pos], rms_list[pos]
+        FDS = F @ D @ S
+        err = X.T @ (FDS - FDS.T) @ X
+        Fs.append(F)
+        Es.append(err)
+        m = len(Es)
+        Bd = torch.stack([e.reshape(-1) for e in Es]) if m > 1 else None
+        Bm = (Bd @ Bd.T) if m > 1 else None
+        rms_t = err.square().mean().sqrt()
+        if Bm is not None:
+            vals = torch.cat([rms_t.reshape(1), Bm.reshape(-1)]).cpu().numpy()
+        else:
+            vals = rms_t.reshape(1).cpu().numpy()
+        rms = float(vals[0])
+        rms_list.append(rms)
+        if m > 1:
+            B = np.empty((m + 1, m + 1))
+            B[:m, :m] = vals[1:].reshape(m, m)
+            if np.abs(B[:m, :m]).sum() < DIIS_EPS:
+                B[:m, :m] /= B[:m, :m].max()
+            B[m, :] = -1.0
+            B[:, m] = -1.0
+            B[m, m] = 0.0
+            rhs = np.zeros(m + 1)
+            rhs[m] = -1.0
+            q, r = np.linalg.qr(B)
+            cvec = np.linalg.solve(r, q.T @ rhs)[:m]
+            F = torch.einsum("k,kij->ij", torch.from_numpy(cvec).to(dev), torch.stack(Fs))
+        eps, Cp = torch.linalg.eigh(X.T @ F @ X)
+        C = X @ Cp
+        D = C[:, :nocc] @ C[:, :nocc].T
+        E_prev, E = E, float((D * (H + F)).sum())
+        res.energies.append(E)
+        if rms < rms_tol and abs(E - E_prev) < e_tol:
+            res.converged = True
+            break
+        if it >= max_iter:
+            break
+    F = H + two_e(D)
+    E = float((D * (H + F)).sum())
+    enuc = nuclear_repulsion(basis.Z, basis.coords)
+    res.energy, res.e_elec, res.e_nuc = E + enuc, E, enuc
+    res.D, res.F, res.C, res.eps = D.cpu().numpy(), F.cpu().numpy(), C.cpu().numpy(), eps.cpu().numpy()
+    res.iterations = it
     return res
 
 
