@@ -784,7 +784,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   gf.mol_off = gd.mol_off;
   gf.mol_n = gd.mol_n;
   const int2* q = h->d_quart.as<int2>();
-  const size_t budget = (size_t)256 << 20;  // scratch bytes per table-mode class
+  const size_t budget = (size_t)1 << 30;  // scratch bytes per table-mode class and precision
   // threads of a table-mode launch: as many as the budget allows (at least 4736),
   // at most one per quartet, a whole number of 128-thread blocks
   auto table_threads = [&](int slots, long long nq) -> long long {
@@ -794,15 +794,21 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   };
   // Every table-mode class gets its own slice of the scratch buffer, so the classes run
   // concurrently on the auxiliary streams like the straight-line ones.
-  size_t slice_off[32] = {0};
+  // In mixed mode the FP32 part of a class gets a second slice and its own stream, so the two
+  // parts of a class run concurrently too.
+  size_t slice_off[32] = {0}, slice_off_f[32] = {0};
   size_t need_total = 0;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     const int slots = hfgpu::kClassLaunchers[c]->grad_scratch_slots(h->pure);
     const long long nq = h->q_end[c] - h->q_beg[c];
-    slice_off[c] = need_total;
+    slice_off[c] = slice_off_f[c] = need_total;
     if (slots <= 0 || nq <= 0) continue;
-    need_total += (size_t)slots * sizeof(double) * (size_t)table_threads(slots, nq);
-    need_total = (need_total + 255) / 256 * 256;
+    const size_t one = (size_t)slots * sizeof(double) * (size_t)table_threads(slots, nq);
+    need_total += (one + 255) / 256 * 256;
+    if (precision == HFGPU_MIXED) {
+      slice_off_f[c] = need_total;
+      need_total += (one + 255) / 256 * 256;
+    }
   }
   if (need_total) HF_CUDA(h, h->d_scratch.ensure(need_total));
   int rc = fork_streams(h);
@@ -813,16 +819,19 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
     if (e <= b) continue;
     const int slots = L->grad_scratch_slots(h->pure);
-    cudaStream_t st = h->aux[rr++ % hfgpu_handle::kAux];
-    unsigned char* slice = h->d_scratch.as<unsigned char>() + slice_off[c];
+    cudaStream_t st_d = h->aux[rr++ % hfgpu_handle::kAux];
+    cudaStream_t st_f = precision == HFGPU_MIXED ? h->aux[rr++ % hfgpu_handle::kAux] : st_d;
     auto run = [&](bool fp32, long long lo, long long hi) -> int {
       const int nq = (int)(hi - lo);
       if (nq <= 0) return HFGPU_OK;
+      const size_t off = fp32 ? slice_off_f[c] : slice_off[c];
+      unsigned char* slice = h->d_scratch.as<unsigned char>() + off;
+      cudaStream_t st = fp32 ? st_f : st_d;
       int grid = (nq + 127) / 128;
       if (slots > 0) {
         const size_t rb = fp32 ? sizeof(float) : sizeof(double);
         grid = (int)(table_threads(slots, nq) / 128);
-        if (slice_off[c] + (size_t)slots * rb * (size_t)grid * 128 > h->d_scratch.bytes)
+        if (off + (size_t)slots * rb * (size_t)grid * 128 > h->d_scratch.bytes)
           return fail(h, HFGPU_ERR_NOMEM, "gradient scratch too small");
       }
       if (fp32) {
