@@ -684,6 +684,13 @@ def class_header(c):
         code_g, mg = gen_grad_table(*c)
     parts += [code_g, ""]
     mg["table"] = not straight
+    # the op-table classes also get the warp-per-quartet form (measured faster than one thread
+    # per quartet on global scratch for every one of them; the straight-line classes stay threads)
+    gwarp = not straight
+    if gwarp:
+        gwcode, gwmeta = gen_grad_warp(*c)
+        parts += [gwcode, ""]
+        mg["grad_warp"] = gwmeta
     parts.append(f"template <>")
     parts.append(f"struct ClassCode<{la}, {lb}, {lc}, {ld}> {{")
     parts.append(f"  static constexpr bool kGradTable = {'false' if straight else 'true'};")
@@ -691,6 +698,8 @@ def class_header(c):
     parts.append(f"  static constexpr bool kWarpDefault = {'true' if m['vrr_values'] >= WARP_DEFAULT_MIN_VRR else 'false'};")
     parts.append(f"  using WarpTab = {'WarpTab' + t if warp else 'void'};")
     parts.append(f"  using GradTab = {'void' if straight else 'GradTable' + t};")
+    parts.append(f"  static constexpr bool kGradWarp = {'true' if gwarp else 'false'};")
+    parts.append(f"  using GradWarpTab = {'GradWarpTab' + t if gwarp else 'void'};")
     parts.append(f"  static constexpr bool kPrimWarp = {'true' if primwarp else 'false'};")
     if primwarp:
         parts.append(f"  template <typename R, int G>")
@@ -769,6 +778,37 @@ static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, i
   if (nq <= 0) return;
   grad_kernel<{la}, {lb}, {lc}, {ld}, R><<<grid, 128, 0, s>>>(a, pure, q, nq);
 }}
+template <typename CC, typename R>
+static bool launch_grad_warp_impl(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{
+  if constexpr (CC::kGradWarp) {{
+    using Tab = typename CC::GradWarpTab;
+    constexpr size_t bytes = sizeof(R) * (size_t)grad_warp_slots<Tab, R>();
+    if (bytes > 232448) return false;  // more shared memory than one block may have
+    auto k = grad_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    k<<<nq, 32, bytes, s>>>(a, pure, q, nq);
+    return true;
+  }} else {{
+    return false;
+  }}
+}}
+template <typename CC, typename R>
+static int grad_warp_bytes_impl() {{
+  if constexpr (CC::kGradWarp) {{
+    return (int)(sizeof(R) * (size_t)grad_warp_slots<typename CC::GradWarpTab, R>());
+  }} else {{
+    return 0;
+  }}
+}}
+static int grad_warp_bytes(int fp32) {{
+  return fp32 ? grad_warp_bytes_impl<ClassCode<{la}, {lb}, {lc}, {ld}>, float>()
+              : grad_warp_bytes_impl<ClassCode<{la}, {lb}, {lc}, {ld}>, double>();
+}}
+template <typename R>
+static bool launch_grad_warp(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{
+  if (nq <= 0) return true;
+  return launch_grad_warp_impl<ClassCode<{la}, {lb}, {lc}, {ld}>, R>(a, pure, q, nq, s);
+}}
 template <typename CC, int NCART>
 static int grad_scratch_slots_impl() {{
   if constexpr (CC::kGradTable) {{
@@ -787,7 +827,9 @@ const ClassLaunchers launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_quartet<d
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kPrimWarp,
                                       &launch_primwarp<double>, &launch_primwarp<float>,
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kWarp,
-                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kWarpDefault}};
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kWarpDefault,
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kGradWarp,
+                                      &launch_grad_warp<double>, &launch_grad_warp<float>, &grad_warp_bytes}};
 }}  // namespace hfgpu
 """
 
@@ -1154,6 +1196,175 @@ def _alloc_levels(order_by_level, deps_of, lev, pre_slots, live_to_end):
             if v in slot:
                 free.append(slot[v])
     return slot, top
+
+
+def _alloc_levels_with_readers(order_by_level, deps_of, lev, pre_slots, live_to_end, readers):
+    """_alloc_levels where `readers` (level, [dep ids]) read values but produce none."""
+    last = {}
+    for nid in order_by_level:
+        for d in deps_of[nid]:
+            last[d] = max(last.get(d, -1), lev[nid])
+    for l, deps in readers:
+        for d in deps:
+            last[d] = max(last.get(d, -1), l)
+    END = 10 ** 9
+    for v in live_to_end:
+        last[v] = END
+    slot = dict(pre_slots)
+    top = max(list(pre_slots.values()) + [-1]) + 1
+    free = [s for v, s in pre_slots.items() if v not in last]
+    maxlev = max([lev[n] for n in order_by_level] + [l for l, _ in readers] + [0])
+    by_level = {}
+    for nid in order_by_level:
+        by_level.setdefault(lev[nid], []).append(nid)
+    freed_at = {}
+    for v, l in last.items():
+        if l != END:
+            freed_at.setdefault(l, []).append(v)
+    for l in range(1, maxlev + 1):
+        for nid in by_level.get(l, []):
+            if free:
+                slot[nid] = free.pop()
+            else:
+                slot[nid] = top
+                top += 1
+        for v in freed_at.get(l, []):
+            if v in slot:
+                free.append(slot[v])
+    return slot, top
+
+
+def gen_grad_warp(la, lb, lc, ld):
+    """Adjoint gradient of one quartet by one warp: the VRR one order higher and the HRR of
+    the four weighted sets are levelised (an op's inputs come from earlier levels), so the
+    32 lanes run one level's ops in parallel out of shared memory; the contractions with
+    the weight block W are ops of the HRR levels that only read."""
+    L = la + lb + lc + ld + 1
+    order = grad_sets(la, lb, lc, ld)
+    dag = Dag(L)
+    setoff, nacc = {}, 0
+    for k in ("U", "A", "B", "C"):
+        setoff[k] = nacc
+        nacc += len(order[k])
+    acc_src, acc_set = [], []
+    for si, k in enumerate(("U", "A", "B", "C")):
+        for (e, f) in order[k]:
+            acc_src.append(dag.get(e, f, 0))
+            acc_set.append(si)
+    ops = [(nid, nd) for nid, nd in enumerate(dag.nodes) if nd[0] != "F"]
+    deps = {nid: [x for x in nd[2:7] if x >= 0] for nid, nd in ops}
+    lev = _levelise([(nid, deps[nid]) for nid, _ in ops], L + 1)
+    vorder = sorted([nid for nid, _ in ops], key=lambda n: (lev[n], n))
+    pre = {m: m for m in range(L + 1)}
+    slot, nvs = _alloc_levels(vorder, deps, lev, pre, set(acc_src))
+    ZV = nvs
+    nodes = dict(ops)
+    vrows, vlev, cur = [], [0], 1
+    for nid in vorder:
+        while lev[nid] > cur:
+            vlev.append(len(vrows))
+            cur += 1
+        kind, i, a, b, c, d, g, k1, k2 = nodes[nid]
+        s_ = lambda x: slot[x] if x >= 0 else ZV
+        vrows.append(((1 if kind == "K" else 0) | (i << 2), slot[nid], s_(a), s_(b), s_(c), s_(d), s_(g),
+                      k1 | (k2 << 8)))
+    vlev.append(len(vrows))
+    # HRR of the four sets (accumulator j is value j) and the contractions
+    hnodes, hinfo, hdeps = {}, {}, {}
+    counter = [nacc]
+
+    def new_id():
+        counter[0] += 1
+        return counter[0] - 1
+
+    def ket(k, e, c, d):
+        key = ("k", k, e, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(d) == 0:
+            v = setoff[k] + order[k].index((e, c))
+        else:
+            i = max(range(3), key=lambda q: (d[q], -q))
+            d1 = add(d, i, -1)
+            x, y = ket(k, e, add(c, i), d1), ket(k, e, c, d1)
+            v = new_id()
+            hinfo[v], hdeps[v] = (1, i, x, y), [x, y]
+        hnodes[key] = v
+        return v
+
+    def bra(k, a, b, c, d):
+        key = ("b", k, a, b, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(b) == 0:
+            v = ket(k, a, c, d)
+        else:
+            i = max(range(3), key=lambda q: (b[q], -q))
+            b1 = add(b, i, -1)
+            x, y = bra(k, add(a, i), b1, c, d), bra(k, a, b1, c, d)
+            v = new_id()
+            hinfo[v], hdeps[v] = (0, i, x, y), [x, y]
+        hnodes[key] = v
+        return v
+
+    cops = []
+    for (cen, dr), items in grad_terms(la, lb, lc, ld).items():
+        gi = "ABC".index(cen) * 3 + dr
+        for wi, terms in items:
+            x = bra(terms[0][1], *terms[0][2:])
+            if len(terms) > 1:
+                y, kk = bra("U", *terms[1][2:]), -terms[1][0]
+            else:
+                y, kk = -1, 0
+            cops.append((gi, wi, x, y, kk))
+    hord = sorted(hinfo)
+    hlev = _levelise([(v, hdeps[v]) for v in hord], nacc)
+    clev = [1 + max(hlev[x], hlev[y] if y >= 0 else 0) for (_, _, x, y, _) in cops]
+    readers = [(l, [x] + ([y] if y >= 0 else [])) for l, (_, _, x, y, _) in zip(clev, cops)]
+    hpre = {j: j for j in range(nacc)}
+    hslot, nhs = _alloc_levels_with_readers(sorted(hord, key=lambda v: (hlev[v], v)), hdeps, hlev, hpre, set(),
+                                            readers)
+    ZH = nhs
+    items = [(hlev[v], 0, v) for v in hord] + [(l, 1, j) for j, l in enumerate(clev)]
+    items.sort()
+    hrows, hlv, cur = [], [0], 1
+    for l, is_c, v in items:
+        while l > cur:
+            hlv.append(len(hrows))
+            cur += 1
+        if is_c:
+            gi, wi, x, y, kk = cops[v]
+            hrows.append((2 | (gi << 2) | (kk << 6), wi, hslot[x], hslot[y] if y >= 0 else ZH))
+        else:
+            kind, i, x, y = hinfo[v]
+            hrows.append((kind | (i << 2), hslot[v], hslot[x], hslot[y]))
+    hlv.append(len(hrows))
+    t = f"{la}{lb}{lc}{ld}"
+    ncart_blk = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
+    s = [f"// warp-mode adjoint gradient of class {t}: {len(vrows)} VRR ops in {len(vlev) - 1} levels over "
+         f"{nvs} slots, {nacc} accumulators, {len(hrows)} HRR/contraction ops in {len(hlv) - 1} levels over "
+         f"{nhs} slots"]
+    s.append(f"__device__ const int4 gwv_{t}[{max(len(vrows), 1)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_warp_vrr(r))) + "}," for r in vrows]
+    s.append("};")
+    s.append(f"__device__ const int gwv_lv_{t}[{len(vlev)}] = {{{','.join(map(str, vlev))}}};")
+    s.append(f"__device__ const int2 gwa_{t}[{nacc}] = {{" +
+             ",".join("{%d,%d}" % (slot[n], k) for n, k in zip(acc_src, acc_set)) + "};")
+    s.append(f"__device__ const int2 gwh_{t}[{max(len(hrows), 1)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_warp_hrr(r))) + "}," for r in hrows]
+    s.append("};")
+    s.append(f"__device__ const int gwh_lv_{t}[{len(hlv)}] = {{{','.join(map(str, hlv))}}};")
+    s.append(f"struct GradWarpTab{t} {{ static constexpr int L = {L}, NVLEV = {len(vlev) - 1}, NVSLOT = {nvs}, "
+             f"NACC = {nacc}, NHLEV = {len(hlv) - 1}, NHSLOT = {nhs}, NCART = {ncart_blk}; "
+             f"static __device__ const int4* vrr() {{ return gwv_{t}; }} "
+             f"static __device__ const int* vlev() {{ return gwv_lv_{t}; }} "
+             f"static __device__ const int2* acc() {{ return gwa_{t}; }} "
+             f"static __device__ const int2* hrr() {{ return gwh_{t}; }} "
+             f"static __device__ const int* hlev() {{ return gwh_lv_{t}; }} }};")
+    meta = {"class": [la, lb, lc, ld], "grad_warp": True, "vrr_ops": len(vrows), "vrr_levels": len(vlev) - 1,
+            "vrr_slots": nvs, "acc": nacc, "hrr_ops": len(hrows), "hrr_levels": len(hlv) - 1, "hrr_slots": nhs,
+            "smem_doubles_per_warp": nvs + 1 + nhs + 1 + 3 * ncart_blk}
+    return "\n".join(s), meta
 
 
 def gen_warp_class(la, lb, lc, ld):

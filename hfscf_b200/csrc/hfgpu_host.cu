@@ -756,6 +756,19 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   return HFGPU_OK;
 }
 
+// Warp form for a gradient launch of nq quartets of class c: when the class has one and the
+// launch fills at most opts.grad_warp_max_waves waves of the blocks all SMs hold at once.
+static bool grad_use_warp(const hfgpu_handle* h, int c, long long nq, bool fp32) {
+  const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
+  if (!L->has_grad_warp || h->opts.grad_warp_max_waves <= 0) return false;
+  const int bytes = L->grad_warp_bytes(fp32 ? 1 : 0);
+  if (bytes <= 0 || bytes > 232448) return false;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+  const long long per_sm = std::min(32, 233472 / (bytes + 1024));  // 228 KB per SM, 1 KB reserved per block
+  return nq <= (long long)h->opts.grad_warp_max_waves * per_sm * sms;
+}
+
 static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
                             double* grad, int precision) {
   if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
@@ -803,6 +816,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     const long long nq = h->q_end[c] - h->q_beg[c];
     slice_off[c] = slice_off_f[c] = need_total;
     if (slots <= 0 || nq <= 0) continue;
+    if (grad_use_warp(h, c, nq, false) && grad_use_warp(h, c, nq, true)) continue;  // warp form: no scratch
     const size_t one = (size_t)slots * sizeof(double) * (size_t)table_threads(slots, nq);
     need_total += (one + 255) / 256 * 256;
     if (precision == HFGPU_MIXED) {
@@ -824,6 +838,14 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     auto run = [&](bool fp32, long long lo, long long hi) -> int {
       const int nq = (int)(hi - lo);
       if (nq <= 0) return HFGPU_OK;
+      if (grad_use_warp(h, c, e - b, fp32)) {
+        const bool done = fp32 ? L->grad_warp_f(gf, h->pure, q + lo, nq, fp32 ? st_f : st_d)
+                               : L->grad_warp_d(gd, h->pure, q + lo, nq, st_d);
+        if (done) {
+          HF_CHECK_LAUNCH(h, "grad warp kernel");
+          return HFGPU_OK;
+        }
+      }
       const size_t off = fp32 ? slice_off_f[c] : slice_off[c];
       unsigned char* slice = h->d_scratch.as<unsigned char>() + off;
       cudaStream_t st = fp32 ? st_f : st_d;
@@ -933,6 +955,7 @@ int hfgpu_default_opts(hfgpu_opts* o) {
   o->mixed_density_tol = 1e-12;
   o->device = 0;
   o->warp_max_quartets = 1 << 30;
+  o->grad_warp_max_waves = 24;
   return HFGPU_OK;
 }
 

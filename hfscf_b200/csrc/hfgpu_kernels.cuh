@@ -822,3 +822,202 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
     if (lane == 0) qa.pairs_rw[pq.x].schwarz = sqrt(m);
   }
 }
+
+// ---------------------------------------------------------------------------
+// Warp-per-quartet adjoint gradient for the large classes: the weight block, the VRR one
+// order higher with its four weighted accumulations, and the HRR of the four sets with
+// the contractions against W all run lane-parallel out of shared memory, level by level
+// (generated tables, gen_eri.py gen_grad_warp).  One warp per block, one block per quartet.
+// ---------------------------------------------------------------------------
+template <typename Tab, typename R>
+__host__ __device__ constexpr int grad_warp_slots() {
+  return Tab::NVSLOT + 1 + Tab::NHSLOT + 1 + 3 * Tab::NCART;
+}
+
+template <int LA, int LB, int LC, int LD, typename R, typename Tab>
+__global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, const int2* __restrict__ quartets,
+                                                       int nq) {
+  extern __shared__ __align__(16) unsigned char gwsm[];
+  const int lane = threadIdx.x;
+  const int qi = blockIdx.x;
+  if (qi >= nq) return;
+  R* vs = reinterpret_cast<R*>(gwsm);
+  R* hs = vs + Tab::NVSLOT + 1;
+  R* W = hs + Tab::NHSLOT + 1;
+  R* t0 = W + Tab::NCART;
+  R* t1 = t0 + Tab::NCART;
+  const int2 pq = quartets[qi];
+  const PairInfo P = a.pairs[pq.x];
+  const PairInfo Q = a.pairs[pq.y];
+  double s8 = 8.0;
+  if (P.sa == P.sb) s8 *= 0.5;
+  if (Q.sa == Q.sb) s8 *= 0.5;
+  if (pq.x == pq.y) s8 *= 0.5;
+  long long blk;
+  int nm;
+  mol_block(a.mol_off, a.mol_n, P.mol, a.n, blk, nm);
+  const double* DJ = off_ptr(a.DJ, blk);
+  const double* DK = off_ptr(a.DK, blk);
+  // weight block W_abcd = s8 [cJ DJ_ab DJ_cd - cK/2 sum_m (DK_ac DK_bd + DK_ad DK_bc)] in the final
+  // basis (t0), then (pure) back to Cartesian one index at a time
+  const int Ls[4] = {LA, LB, LC, LD};
+  int dims[4];
+  for (int q = 0; q < 4; ++q) dims[q] = pure ? npure_of(Ls[q]) : ncart_of(Ls[q]);
+  {
+    const int tot = dims[0] * dims[1] * dims[2] * dims[3];
+    R* dstw = pure ? t0 : W;
+    for (int e = lane; e < tot; e += 32) {
+      const int l = e % dims[3], k = (e / dims[3]) % dims[2], j = (e / (dims[3] * dims[2])) % dims[1];
+      const int i = e / (dims[3] * dims[2] * dims[1]);
+      const int ia = P.fa + i, jb = P.fb + j, kc = Q.fa + k, ld = Q.fb + l;
+      double w = DJ ? a.cJ * __ldg(DJ + (size_t)ia * nm + jb) * __ldg(DJ + (size_t)kc * nm + ld) : 0.0;
+      for (int m = 0; m < a.nK; ++m) {
+        const double* D = DK + (size_t)m * nm * nm;
+        w -= 0.5 * a.cK *
+             (__ldg(D + (size_t)ia * nm + kc) * __ldg(D + (size_t)jb * nm + ld) +
+              __ldg(D + (size_t)ia * nm + ld) * __ldg(D + (size_t)jb * nm + kc));
+      }
+      dstw[e] = R(s8 * w);
+    }
+    __syncwarp();
+  }
+  if (pure) {
+    R* bufs[2] = {t1, t0};
+    const R* in = t0;
+    for (int st = 0; st < 4; ++st) {
+      const int nc = ncart_of(Ls[st]), np = npure_of(Ls[st]);
+      int nd[4] = {dims[0], dims[1], dims[2], dims[3]};
+      nd[st] = nc;
+      R* o = st == 3 ? W : bufs[st & 1];
+      const int tot = nd[0] * nd[1] * nd[2] * nd[3];
+      for (int e = lane; e < tot; e += 32) {
+        int id[4];
+        int r = e;
+        for (int q = 3; q >= 0; --q) {
+          id[q] = r % nd[q];
+          r /= nd[q];
+        }
+        R v = R(0);
+        for (int c = 0; c < np; ++c) {
+          const double y = c_ylm[Ls[st]][id[st] * np + c];
+          if (y == 0.0) continue;
+          int jd[4] = {id[0], id[1], id[2], id[3]};
+          jd[st] = c;
+          v += R(y) * in[((jd[0] * dims[1] + jd[1]) * dims[2] + jd[2]) * dims[3] + jd[3]];
+        }
+        o[e] = v;
+      }
+      __syncwarp();
+      for (int q = 0; q < 4; ++q) dims[q] = nd[q];
+      in = o;
+    }
+  }
+  for (int t = lane; t < Tab::NACC; t += 32) hs[t] = R(0);
+  if (lane == 0) {
+    vs[Tab::NVSLOT] = R(0);
+    hs[Tab::NHSLOT] = R(0);
+  }
+  __syncwarp();
+  const PrimPair<R>* bp = a.prims + P.prim_off;
+  const PrimPair<R>* kp = a.prims + Q.prim_off;
+  const R* eA = a.alpha_a + P.prim_off;
+  const R* eB = a.alpha_b + P.prim_off;
+  const R* eC = a.alpha_a + Q.prim_off;
+  const int4* vo = Tab::vrr();
+  const int* vl = Tab::vlev();
+  const int2* acc = Tab::acc();
+  for (int ib = 0; ib < P.nprim; ++ib) {
+    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;
+    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;
+    const R wa = R(2) * eA[ib], wb = R(2) * eB[ib];
+    for (int ik = 0; ik < Q.nprim; ++ik) {
+      const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;
+      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;
+      const R wc = R(2) * eC[ik];
+      const R pqs = p + q;
+      const R rs = rsqrt_t(pqs);
+      const R ipq = rs * rs;
+      const R rho = p * q * ipq;
+      const R rp = q * ipq, rq = p * ipq;
+      const R inv2p = R(0.5) * ip, inv2q = R(0.5) * iq, inv2pq = R(0.5) * ipq;
+      const R PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+      const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+      R F[Tab::L + 1];
+      a.boys.template eval<Tab::L>(T, Kab * Kcd * rs, F);
+#pragma unroll
+      for (int m = 0; m <= Tab::L; ++m)
+        if (lane == m) vs[m] = F[m];
+      __syncwarp();
+      for (int l = 0; l < Tab::NVLEV; ++l) {
+        const int e = __ldg(vl + l + 1);
+        for (int o = __ldg(vl + l) + lane; o < e; o += 32) {
+          const int4 op = __ldg(vo + o);
+          const int dst = op.x & 0xffff, sa = (unsigned)op.x >> 16, sb = op.y & 0xffff, sc = (unsigned)op.y >> 16;
+          const int sd = op.z & 0xffff, kd = op.w & 255, k12 = (unsigned)op.w >> 8;
+          const int dir = kd >> 2;
+          const R PQd = dir == 0 ? PQx : (dir == 1 ? PQy : PQz);
+          const R k1 = small_int<R>(k12 & 255);
+          R v;
+          if ((kd & 1) == 0) {
+            const R PA = dir == 0 ? PAx : (dir == 1 ? PAy : PAz);
+            v = PA * vs[sa] - rp * PQd * vs[sb] + k1 * inv2p * (vs[sc] - rp * vs[sd]);
+          } else {
+            const R QC = dir == 0 ? QCx : (dir == 1 ? QCy : QCz);
+            const int sg = (unsigned)op.z >> 16;
+            v = QC * vs[sa] + rq * PQd * vs[sb] + k1 * inv2q * (vs[sc] - rq * vs[sd]) +
+                small_int<R>(k12 >> 8) * inv2pq * vs[sg];
+          }
+          vs[dst] = v;
+        }
+        __syncwarp();
+      }
+      for (int t = lane; t < Tab::NACC; t += 32) {
+        const int2 ac = __ldg(acc + t);
+        const R w = ac.y == 0 ? R(1) : (ac.y == 1 ? wa : (ac.y == 2 ? wb : wc));
+        hs[t] += w * vs[ac.x];
+      }
+      __syncwarp();
+    }
+  }
+  // HRR of the four sets and the contractions with W, per lane into nine partial sums
+  R g[9];
+#pragma unroll
+  for (int x = 0; x < 9; ++x) g[x] = R(0);
+  const int2* ho = Tab::hrr();
+  const int* hl = Tab::hlev();
+  const R ABx = R(P.ABx), ABy = R(P.ABy), ABz = R(P.ABz), CDx = R(Q.ABx), CDy = R(Q.ABy), CDz = R(Q.ABz);
+  for (int l = 0; l < Tab::NHLEV; ++l) {
+    const int e = __ldg(hl + l + 1);
+    for (int o = __ldg(hl + l) + lane; o < e; o += 32) {
+      const int2 op = __ldg(ho + o);
+      const int kd = (unsigned)op.y >> 16;
+      const int x = (unsigned)op.x >> 16, y = op.y & 0xffff;
+      if ((kd & 3) == 2) {
+        const int gi = (kd >> 2) & 15;
+        const R v = W[op.x & 0xffff] * (hs[x] - small_int<R>(kd >> 6) * hs[y]);
+#pragma unroll
+        for (int c = 0; c < 9; ++c)
+          if (c == gi) g[c] += v;
+      } else {
+        const int dir = kd >> 2;
+        const R d = (kd & 1) ? (dir == 0 ? CDx : (dir == 1 ? CDy : CDz)) : (dir == 0 ? ABx : (dir == 1 ? ABy : ABz));
+        hs[op.x & 0xffff] = hs[x] + d * hs[y];
+      }
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c)
+    for (int off = 16; off > 0; off >>= 1) g[c] += __shfl_xor_sync(0xffffffffu, g[c], off);
+  if (lane == 0) {
+    const int at[3] = {P.atom_a, P.atom_b, Q.atom_a};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double gA = double(g[d]), gB = double(g[3 + d]), gC = double(g[6 + d]);
+      atomicAdd(a.grad + 3 * at[0] + d, gA);
+      atomicAdd(a.grad + 3 * at[1] + d, gB);
+      atomicAdd(a.grad + 3 * at[2] + d, gC);
+      atomicAdd(a.grad + 3 * Q.atom_b + d, -(gA + gB + gC));
+    }
+  }
+}

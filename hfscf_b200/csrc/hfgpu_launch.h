@@ -21,6 +21,10 @@ struct ClassLaunchers {
   bool (*primwarp_f)(const QuartetArgs<float>&, const int2*, int, cudaStream_t);
   bool has_warp;                         // warp-per-quartet form with levelised tables
   bool warp_default;                     // ... used unless the schedule or opts say otherwise
+  bool has_grad_warp;                    // warp-per-quartet adjoint gradient (shared memory, no scratch)
+  bool (*grad_warp_d)(const GradArgs<double>&, int pure, const int2*, int, cudaStream_t);
+  bool (*grad_warp_f)(const GradArgs<float>&, int pure, const int2*, int, cudaStream_t);
+  int (*grad_warp_bytes)(int fp32);      // shared memory of one warp-form block (0: no warp form)
 };
 
 extern const ClassLaunchers* const kClassLaunchers[];

@@ -42,7 +42,8 @@ class _Basis(ctypes.Structure):
 class _Opts(ctypes.Structure):
     _fields_ = [("schwarz_tol", ctypes.c_double), ("density_tol", ctypes.c_double),
                 ("mixed_fp32_bound", ctypes.c_double), ("mixed_density_tol", ctypes.c_double), ("device", ctypes.c_int),
-                ("warp_max_quartets", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+                ("warp_max_quartets", ctypes.c_int), ("grad_warp_max_waves", ctypes.c_int),
+                ("reserved", ctypes.c_int * 5)]
 
 
 def lib():
@@ -91,7 +92,7 @@ class Engine:
     """One engine handle: a basis on one GPU, with the current geometry."""
 
     def __init__(self, basis: Basis, schwarz_tol=1e-12, density_tol=1e-12, mixed_fp32_bound=1e-4, device=0,
-                 warp_max_quartets=None):
+                 warp_max_quartets=None, grad_warp_max_waves=None):
         self.basis = basis
         self.n = basis.nbf
         self._bv = _BasisView(basis)
@@ -100,6 +101,8 @@ class Engine:
         o.schwarz_tol, o.density_tol, o.mixed_fp32_bound, o.device = schwarz_tol, density_tol, mixed_fp32_bound, device
         if warp_max_quartets is not None:
             o.warp_max_quartets = warp_max_quartets
+        if grad_warp_max_waves is not None:
+            o.grad_warp_max_waves = grad_warp_max_waves
         self._opts = o
         h = ctypes.c_void_p()
         self._check(lib().hfgpu_create(ctypes.byref(self._bv.s), ctypes.byref(o), ctypes.byref(h)), None)

@@ -67,7 +67,12 @@ typedef struct {
   int device;              /* CUDA device ordinal (default 0) */
   int warp_max_quartets;   /* (dd|dp), (dd|dd): one warp per quartet when the class has at most this many
                               quartets, one thread per quartet otherwise (default 2^30 = always; -1 = never) */
-  int reserved[6];
+  int grad_warp_max_waves;    /* gradient of (dp|dp) (dd|pp) (dd|ds) (dd|dp) (dd|dd): one warp per quartet
+                                 (shared memory) when the class's quartets fill at most this many waves of
+                                 the blocks the GPU holds at once, else one thread per quartet on global
+                                 scratch (default 24: longer warp-form launches hold the shared memory of
+                                 every SM and stop the other classes' kernels from overlapping; 0 = never) */
+  int reserved[5];
 } hfgpu_opts;
 
 int hfgpu_default_opts(hfgpu_opts* opts);

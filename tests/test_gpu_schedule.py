@@ -82,3 +82,18 @@ def test_autotuned_schedule_gives_the_same_fock_build():
         Fm1 = eng.fock_rhf(D, H, E.MIXED)
     assert np.max(np.abs(F1 - F0)) < 1e-11
     assert np.max(np.abs(Fm1 - Fm0)) < 1e-6
+
+
+@pytest.mark.parametrize("gmax", [0, 1 << 20], ids=["thread-per-quartet", "warp-per-quartet"])
+@pytest.mark.parametrize("name,bs", MOLS, ids=[m[0] for m in MOLS])
+def test_gradient_launch_forms_match_oracle(name, bs, gmax):
+    """The large gradient classes have a thread-per-quartet and a warp-per-quartet kernel;
+    each is forced in turn (FP64, tolerance 1e-10 as in test_gpu_parity)."""
+    rng = np.random.default_rng(31)
+    D = _sym(rng, bs.nbf)
+    g0 = oracle.grad2e_rhf(bs, D)
+    with E.Engine(bs, grad_warp_max_waves=gmax) as eng:
+        g = eng.grad2e(D)
+        gm = eng.grad2e(D, precision=E.MIXED)
+    assert np.max(np.abs(g - g0)) < 1e-10
+    assert np.max(np.abs(gm - g0)) < 1e-6
