@@ -747,8 +747,8 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
       __syncwarp();
       for (int l = 0; l < Tab::NVLEV; ++l) {
         const int e = __ldg(vl + l + 1);
-        for (int o = __ldg(vl + l) + lane; o < e; o += 32) {
-          const int4 op = __ldg(vo + o);
+        // two op rows in flight per lane: the rows of one level are independent
+        auto body = [&](const int4 op) {
           const int dst = op.x & 0xffff, sa = (unsigned)op.x >> 16, sb = op.y & 0xffff, sc = (unsigned)op.y >> 16;
           const int sd = op.z & 0xffff, kd = op.w & 255, k12 = (unsigned)op.w >> 8;
           const int dir = kd >> 2;
@@ -764,6 +764,13 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
             v = QC * vs[sa] + rq * PQd * vs[sb] + k1 * inv2q * (vs[sc] - rq * vs[sd]) + small_int<R>(k12 >> 8) * inv2pq * vs[sg];
           }
           vs[dst] = v;
+        };
+        for (int o = __ldg(vl + l) + lane; o < e; o += 64) {
+          const int4 opa = __ldg(vo + o);
+          const bool two = o + 32 < e;
+          const int4 opb = two ? __ldg(vo + o + 32) : opa;
+          body(opa);
+          if (two) body(opb);
         }
         __syncwarp();
       }
@@ -776,11 +783,18 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
   const R ABx = R(P.ABx), ABy = R(P.ABy), ABz = R(P.ABz), CDx = R(Q.ABx), CDy = R(Q.ABy), CDz = R(Q.ABz);
   for (int l = 0; l < Tab::NHLEV; ++l) {
     const int e = __ldg(hl + l + 1);
-    for (int o = __ldg(hl + l) + lane; o < e; o += 32) {
-      const int2 op = __ldg(ho + o);
+    // two op rows in flight per lane: the rows of one level are independent
+    auto body = [&](const int2 op) {
       const int kd = (unsigned)op.y >> 16, dir = kd >> 2;
       const R d = (kd & 1) ? (dir == 0 ? CDx : (dir == 1 ? CDy : CDz)) : (dir == 0 ? ABx : (dir == 1 ? ABy : ABz));
       hs[op.x & 0xffff] = hs[(unsigned)op.x >> 16] + d * hs[op.y & 0xffff];
+    };
+    for (int o = __ldg(hl + l) + lane; o < e; o += 64) {
+      const int2 opa = __ldg(ho + o);
+      const bool two = o + 32 < e;
+      const int2 opb = two ? __ldg(ho + o + 32) : opa;
+      body(opa);
+      if (two) body(opb);
     }
     __syncwarp();
   }
@@ -950,8 +964,8 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
       __syncwarp();
       for (int l = 0; l < Tab::NVLEV; ++l) {
         const int e = __ldg(vl + l + 1);
-        for (int o = __ldg(vl + l) + lane; o < e; o += 32) {
-          const int4 op = __ldg(vo + o);
+        // two op rows in flight per lane: the rows of one level are independent
+        auto body = [&](const int4 op) {
           const int dst = op.x & 0xffff, sa = (unsigned)op.x >> 16, sb = op.y & 0xffff, sc = (unsigned)op.y >> 16;
           const int sd = op.z & 0xffff, kd = op.w & 255, k12 = (unsigned)op.w >> 8;
           const int dir = kd >> 2;
@@ -968,6 +982,13 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
                 small_int<R>(k12 >> 8) * inv2pq * vs[sg];
           }
           vs[dst] = v;
+        };
+        for (int o = __ldg(vl + l) + lane; o < e; o += 64) {
+          const int4 opa = __ldg(vo + o);
+          const bool two = o + 32 < e;
+          const int4 opb = two ? __ldg(vo + o + 32) : opa;
+          body(opa);
+          if (two) body(opb);
         }
         __syncwarp();
       }
@@ -988,8 +1009,8 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
   const R ABx = R(P.ABx), ABy = R(P.ABy), ABz = R(P.ABz), CDx = R(Q.ABx), CDy = R(Q.ABy), CDz = R(Q.ABz);
   for (int l = 0; l < Tab::NHLEV; ++l) {
     const int e = __ldg(hl + l + 1);
-    for (int o = __ldg(hl + l) + lane; o < e; o += 32) {
-      const int2 op = __ldg(ho + o);
+    // two op rows in flight per lane: the rows of one level are independent
+    auto body = [&](const int2 op) {
       const int kd = (unsigned)op.y >> 16;
       const int x = (unsigned)op.x >> 16, y = op.y & 0xffff;
       if ((kd & 3) == 2) {
@@ -1003,6 +1024,13 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
         const R d = (kd & 1) ? (dir == 0 ? CDx : (dir == 1 ? CDy : CDz)) : (dir == 0 ? ABx : (dir == 1 ? ABy : ABz));
         hs[op.x & 0xffff] = hs[x] + d * hs[y];
       }
+    };
+    for (int o = __ldg(hl + l) + lane; o < e; o += 64) {
+      const int2 opa = __ldg(ho + o);
+      const bool two = o + 32 < e;
+      const int2 opb = two ? __ldg(ho + o + 32) : opa;
+      body(opa);
+      if (two) body(opb);
     }
     __syncwarp();
   }
