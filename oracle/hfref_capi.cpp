@@ -259,15 +259,25 @@ int hfref_onee_grad(int nshell, const int* L, const double* xyz, const int* npri
 // Erios::compute_contracted_shell_quartet over every `stride`-th unique shell
 // quartet of create_repulsion_matrix's loop (hfscf_hf_hamiltonian.cpp:95-111), with
 // the reference's default eri_screen = true (screen matrix first, :77-89), on all
-// OpenMP threads.  Returns seconds; *sampled / *total give the scale factor.
+// OpenMP threads.  Returns the seconds of the sampled quartets (*sampled / *total give the
+// scale factor); *fixed_s is the unscaled once-per-geometry part.
 double hfref_time_eri_sample(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
                              const double* coef, int pure, double cutoff, long long stride, long long* sampled,
-                             long long* total) {
+                             long long* total, double* fixed_s) {
   auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, pure);
   const Eigen::Index n = pure ? b->npure : b->ncart;
   const Eigen::Index len = n * (n + 1) * (n * n + n + 2) / 8;
   EigenVector<double> eri(len);
   ERIOS::Erios os(pure != 0, cutoff);
+  // Once-per-geometry work that does not scale with the sample: the first touch of the whole
+  // packed ERI vector and the Schwarz screen matrix.  Timed apart and reported in *fixed_s.
+  const double f0 = omp_get_wtime();
+  eri.setZero();
+  os.init_screen(b->ncart);
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < nshell; ++i)
+    for (int j = i; j < nshell; ++j) os.compute_screen_matrix(b->pairs[i * nshell + j]);
+  *fixed_s = omp_get_wtime() - f0;
   std::vector<std::pair<int, int>> quartets;
   for (int i = 0; i < nshell; ++i)
     for (int j = i; j < nshell; ++j)
@@ -277,10 +287,6 @@ double hfref_time_eri_sample(int nshell, const int* L, const double* xyz, const 
   std::vector<std::pair<int, int>> pick;
   for (size_t q = 0; q < quartets.size(); q += (size_t)stride) pick.push_back(quartets[q]);
   const double t0 = omp_get_wtime();
-  os.init_screen(b->ncart);
-#pragma omp parallel for schedule(dynamic)
-  for (int i = 0; i < nshell; ++i)
-    for (int j = i; j < nshell; ++j) os.compute_screen_matrix(b->pairs[i * nshell + j]);
 #pragma omp parallel for schedule(dynamic)
   for (long long q = 0; q < (long long)pick.size(); ++q)
     os.compute_contracted_shell_quartet(eri, b->pairs[pick[q].first], b->pairs[pick[q].second], true);
@@ -297,16 +303,21 @@ double hfref_time_eri_sample(int nshell, const int* L, const double* xyz, const 
 double hfref_time_fock_sample(long long n, long long rows, double* checksum) {
   const long long len = n * (n + 1) * (n * n + n + 2) / 8;
   std::vector<double> eri((size_t)len, 1e-3), D((size_t)(n * n), 1e-2), F((size_t)(n * n), 0.0);
+  // the sampled (i, j) elements are spread over all threads, as the reference's loop over every
+  // row spreads them (a sample of a few rows parallelised by row would leave threads idle)
+  std::vector<std::pair<long long, long long>> ij;
+  for (long long i = 0; i < rows; ++i)
+    for (long long j = i; j < n; ++j) ij.emplace_back(i, j);
   const double t0 = omp_get_wtime();
 #pragma omp parallel for schedule(dynamic)
-  for (long long i = 0; i < rows; ++i)
-    for (long long j = i; j < n; ++j) {
-      double f = 0.0;
-      for (long long k = 0; k < n; ++k)
-        for (long long l = 0; l < n; ++l)
-          f += D[k * n + l] * (2.0 * eri[hfscfmath::index_ijkl(i, j, k, l)] - eri[hfscfmath::index_ijkl(i, k, j, l)]);
-      F[i * n + j] = F[j * n + i] = f;
-    }
+  for (long long x = 0; x < (long long)ij.size(); ++x) {
+    const long long i = ij[(size_t)x].first, j = ij[(size_t)x].second;
+    double f = 0.0;
+    for (long long k = 0; k < n; ++k)
+      for (long long l = 0; l < n; ++l)
+        f += D[k * n + l] * (2.0 * eri[hfscfmath::index_ijkl(i, j, k, l)] - eri[hfscfmath::index_ijkl(i, k, j, l)]);
+    F[i * n + j] = F[j * n + i] = f;
+  }
   const double t1 = omp_get_wtime();
   double c = 0.0;
   for (double v : F) c += v;
