@@ -87,7 +87,7 @@ class BatchEngine:
 
     def autotune(self, D, precision=eng.FP64, repeats=2):
         """hfgpu_autotune on the batched handle (D in block storage, on the device)."""
-        out = np.zeros((eng.NUM_CLASSES, 3), dtype=np.int32)
+        out = np.zeros((eng.NUM_CLASSES, 4), dtype=np.int32)
         self._check(eng.lib().hfgpu_autotune(self.h, ctypes.c_void_p(D.data_ptr()), ctypes.c_int(precision),
                                              ctypes.c_int(repeats), out.ctypes.data_as(eng._ip)))
         return out

@@ -653,6 +653,18 @@ def common_header():
     return "\n".join(out) + "\n"
 
 
+def cap_blocks(vrr_values):
+    """Blocks of 128 threads per SM the register-capped thread variant asks for (0: no such
+    variant): 8 (64 registers) for the smallest classes, 5 (about 100) for the next ones."""
+    if vrr_values <= 1:
+        return 0  # (ss|ss) already fits in 64 registers
+    if vrr_values <= 20:
+        return 8
+    if vrr_values <= 60:
+        return 5
+    return 0
+
+
 WARP_MIN_VRR = 250        # classes that also get a warp-per-quartet form (hfgpu_autotune picks)
 WARP_DEFAULT_MIN_VRR = 1000  # (dd|dp) and (dd|dd): measured faster as one warp per quartet by default
 
@@ -701,6 +713,7 @@ def class_header(c):
     parts.append(f"  static constexpr bool kGradWarp = {'true' if gwarp else 'false'};")
     parts.append(f"  using GradWarpTab = {'GradWarpTab' + t if gwarp else 'void'};")
     parts.append(f"  static constexpr bool kPrimWarp = {'true' if primwarp else 'false'};")
+    parts.append(f"  static constexpr int kCapBlocks = {cap_blocks(m['vrr_values'])};")
     if primwarp:
         parts.append(f"  template <typename R, int G>")
         parts.append(f"  static __device__ __forceinline__ void eri_pw({class_args_sig()}, int lane) {{")
@@ -736,6 +749,12 @@ static void launch_quartet_impl(const QuartetArgs<R>& a, const int2* q, int nq, 
   if constexpr (CC::kWarp) warp = nq <= a.warp_max;
   if (!warp) {{
     const int bs = a.block > 0 ? a.block : 64;
+    if constexpr (CC::kCapBlocks > 0) {{
+      if (a.capped) {{
+        quartet_kernel<{la}, {lb}, {lc}, {ld}, R, CC::kCapBlocks><<<(nq + bs - 1) / bs, bs, 0, s>>>(a, q, nq);
+        return;
+      }}
+    }}
     quartet_kernel<{la}, {lb}, {lc}, {ld}, R><<<(nq + bs - 1) / bs, bs, 0, s>>>(a, q, nq);
     return;
   }}
@@ -829,7 +848,8 @@ const ClassLaunchers launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_quartet<d
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kWarp,
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kWarpDefault,
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kGradWarp,
-                                      &launch_grad_warp<double>, &launch_grad_warp<float>, &grad_warp_bytes}};
+                                      &launch_grad_warp<double>, &launch_grad_warp<float>, &grad_warp_bytes,
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kCapBlocks > 0}};
 }}  // namespace hfgpu
 """
 

@@ -129,7 +129,7 @@ struct hfgpu_handle {
   // per-class launch schedule (hfgpu_autotune / hfgpu_set_schedule): threads per block of
   // the thread-per-quartet form, warp-over-primitives form for the many-primitive parts,
   // warp-per-quartet form (-1 = follow opts.warp_max_quartets)
-  int sched_block[21], sched_primwarp[21], sched_warp[21];
+  int sched_block[21], sched_primwarp[21], sched_warp[21], sched_cap[21];
   unsigned class_mask = ~0u;            // classes a J/K build launches (autotuning runs one at a time)
 
   hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21) {
@@ -137,6 +137,7 @@ struct hfgpu_handle {
       sched_block[c] = 64;
       sched_primwarp[c] = 0;
       sched_warp[c] = c < hfgpu::kNumClasses && hfgpu::kClassLaunchers[c]->warp_default ? -1 : 0;
+      sched_cap[c] = 0;
     }
   }
 };
@@ -362,6 +363,7 @@ int compute_schwarz(hfgpu_handle* h) {
     if (e <= b) continue;
     qa.warp_max = class_warp_max(h, quartet_class(c, c));
     qa.block = h->sched_block[quartet_class(c, c)];
+    qa.capped = h->sched_cap[quartet_class(c, c)];
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[quartet_class(c, c)];
     L->quartet_d(qa, h->d_quart.as<int2>() + b, e - b, h->stream);
     HF_CHECK_LAUNCH(h, "schwarz kernel");
@@ -689,6 +691,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     qd.jk.counters = cnt + 3 * c;
     qf.jk.counters = cnt + 3 * c;
     qd.block = qf.block = h->sched_block[c];
+    qd.capped = qf.capped = h->sched_cap[c];
     qd.group = qf.group = h->sched_primwarp[c] == 1 ? 32 : h->sched_primwarp[c];
     qd.warp_max = qf.warp_max = class_warp_max(h, c);
     h->ev_used[c] = false;
@@ -1123,6 +1126,7 @@ int hfgpu_eri_packed(hfgpu_handle* h, double* eri_out, long long eri_len) {
       HF_CUDA(h, cudaMemcpyAsync(h->d_eriq.p, list.data(), sizeof(int2) * list.size(), cudaMemcpyHostToDevice, h->stream));
       qa.warp_max = class_warp_max(h, quartet_class(cp, cq));
       qa.block = h->sched_block[quartet_class(cp, cq)];
+      qa.capped = h->sched_cap[quartet_class(cp, cq)];
       hfgpu::kClassLaunchers[quartet_class(cp, cq)]->quartet_d(qa, h->d_eriq.as<int2>(), (int)list.size(), h->stream);
       HF_CHECK_LAUNCH(h, "packed eri kernel");
       HF_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1477,15 +1481,16 @@ int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms) {
 int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule) {
   if (!h || !schedule) return HFGPU_ERR_INVALID;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
-    const int bs = schedule[3 * c], pw = schedule[3 * c + 1], wp = schedule[3 * c + 2];
+    const int bs = schedule[4 * c], pw = schedule[4 * c + 1], wp = schedule[4 * c + 2], cp = schedule[4 * c + 3];
     if ((bs != 32 && bs != 64 && bs != 128) || (pw != 0 && pw != 1 && pw != 4 && pw != 8 && pw != 16 && pw != 32) ||
-        wp < -1 || wp > 1)
+        wp < -1 || wp > 1 || (cp != 0 && cp != 1))
       return fail(h, HFGPU_ERR_INVALID, "schedule entry out of range");
   }
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
-    h->sched_block[c] = schedule[3 * c];
-    h->sched_primwarp[c] = schedule[3 * c + 1];
-    h->sched_warp[c] = schedule[3 * c + 2];
+    h->sched_block[c] = schedule[4 * c];
+    h->sched_primwarp[c] = schedule[4 * c + 1];
+    h->sched_warp[c] = schedule[4 * c + 2];
+    h->sched_cap[c] = schedule[4 * c + 3];
   }
   return HFGPU_OK;
 }
@@ -1493,9 +1498,10 @@ int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule) {
 int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule) {
   if (!h || !schedule) return HFGPU_ERR_INVALID;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
-    schedule[3 * c] = h->sched_block[c];
-    schedule[3 * c + 1] = h->sched_primwarp[c];
-    schedule[3 * c + 2] = h->sched_warp[c];
+    schedule[4 * c] = h->sched_block[c];
+    schedule[4 * c + 1] = h->sched_primwarp[c];
+    schedule[4 * c + 2] = h->sched_warp[c];
+    schedule[4 * c + 3] = h->sched_cap[c];
   }
   return HFGPU_OK;
 }
@@ -1524,25 +1530,27 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
       cudaEventDestroy(b);
     }
   } restore{h, h->class_mask, e0, e1};
-  int start[3 * 21];
+  int start[4 * 21];
   hfgpu_get_schedule(h, start);
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     if (h->q_end[c] <= h->q_beg[c]) continue;
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
     h->class_mask = 1u << c;
     float best = 1e30f;
-    int bb = h->sched_block[c], bp = h->sched_primwarp[c], bw = h->sched_warp[c];
+    int bb = h->sched_block[c], bp = h->sched_primwarp[c], bw = h->sched_warp[c], bc = h->sched_cap[c];
     const int warps[2] = {1, 0};
     for (int wi = 0; wi < (L->has_warp ? 2 : 1); ++wi) {
       const int wp = L->has_warp ? warps[wi] : -1;
       const int pws[5] = {32, 16, 8, 4, 0};
       for (int pi = (L->has_primwarp ? 0 : 4); pi < 5; ++pi) {
         const int pw = pws[pi];
-        for (int bs : {32, 64, 128}) {
-          if (wp == 1 && bs != 64) continue;  // the warp form has its own block shape
+        for (int cand = 0; cand < (L->has_capped ? 6 : 3); ++cand) {
+          const int bs = 32 << (cand % 3), cap = cand / 3;
+          if (wp == 1 && (bs != 64 || cap)) continue;  // the warp form has its own block shape
           h->sched_block[c] = bs;
           h->sched_primwarp[c] = L->has_primwarp ? pw : 1;
           h->sched_warp[c] = wp;
+          h->sched_cap[c] = cap;
           if ((rc = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return rc;  // warm-up
           HF_CUDA(h, cudaEventRecord(e0, h->stream));
           for (int r = 0; r < repeats; ++r)
@@ -1556,6 +1564,7 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
             bb = bs;
             bp = h->sched_primwarp[c];
             bw = wp;
+            bc = cap;
           }
         }
       }
@@ -1563,11 +1572,12 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
     h->sched_block[c] = bb;
     h->sched_primwarp[c] = bp;
     h->sched_warp[c] = bw;
+    h->sched_cap[c] = bc;
   }
   // Classes were timed one at a time; in a build they run concurrently.  Keep the tuned
   // schedule only if a whole build with it beats one with the schedule we started from.
   h->class_mask = restore.mask;
-  int tuned[3 * 21];
+  int tuned[4 * 21];
   hfgpu_get_schedule(h, tuned);
   float t_tuned = 0.f, t_start = 0.f;
   for (int round = 0; round < 2; ++round)

@@ -238,10 +238,14 @@ struct QuartetArgs {
   int warp_max;         // large classes: warp per quartet up to this many quartets
   int block;            // threads per block of the thread-per-quartet form (32, 64 or 128; 0 = 64)
   int group;            // lanes per quartet of the primitive-split form (4, 8, 16 or 32; 0 = 32)
+  int capped;           // 1: the register-capped variant of the thread form (classes that have one)
 };
 
-template <int LA, int LB, int LC, int LD, typename R>
-__global__ void __launch_bounds__(128) quartet_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets, int nq) {
+// MINB > 1: the register-capped variant (at least MINB blocks of 128 threads per SM) of the
+// small classes, for more warps in flight.
+template <int LA, int LB, int LC, int LD, typename R, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) quartet_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets,
+                                                            int nq) {
   const JKArgs<R>& a = qa.jk;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   // every lane stays to the end (lanes without work carry valid = false), so

@@ -25,6 +25,7 @@ struct ClassLaunchers {
   bool (*grad_warp_d)(const GradArgs<double>&, int pure, const int2*, int, cudaStream_t);
   bool (*grad_warp_f)(const GradArgs<float>&, int pure, const int2*, int, cudaStream_t);
   int (*grad_warp_bytes)(int fp32);      // shared memory of one warp-form block (0: no warp form)
+  bool has_capped;                       // register-capped variant of the thread-per-quartet form
 };
 
 extern const ClassLaunchers* const kClassLaunchers[];

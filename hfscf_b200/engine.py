@@ -258,24 +258,24 @@ class Engine:
     def autotune(self, D, precision=FP64, repeats=3) -> np.ndarray:
         """hfgpu_autotune: per class, the fastest launch form on this geometry and density.
         ``D`` is a CUDA tensor (n x n, float64) or a host array (copied to the device).
-        Returns the schedule, HFGPU_NUM_CLASSES x 3 ints (block, primwarp, warp)."""
+        Returns the schedule, HFGPU_NUM_CLASSES x 4 ints (block, primwarp, warp, capped)."""
         import torch
         if isinstance(D, torch.Tensor) and D.is_cuda:
             Dd = D.contiguous()
         else:
             Dd = torch.from_numpy(_c(D)).to(torch.device("cuda", self._opts.device))
-        out = np.zeros((NUM_CLASSES, 3), dtype=np.int32)
+        out = np.zeros((NUM_CLASSES, 4), dtype=np.int32)
         self._check(lib().hfgpu_autotune(self.h, ctypes.c_void_p(Dd.data_ptr()), ctypes.c_int(precision),
                                          ctypes.c_int(repeats), out.ctypes.data_as(_ip)))
         return out
 
     def get_schedule(self) -> np.ndarray:
-        out = np.zeros((NUM_CLASSES, 3), dtype=np.int32)
+        out = np.zeros((NUM_CLASSES, 4), dtype=np.int32)
         self._check(lib().hfgpu_get_schedule(self.h, out.ctypes.data_as(_ip)))
         return out
 
     def set_schedule(self, sched):
-        s = np.ascontiguousarray(np.asarray(sched, dtype=np.int32).reshape(NUM_CLASSES, 3))
+        s = np.ascontiguousarray(np.asarray(sched, dtype=np.int32).reshape(NUM_CLASSES, 4))
         self._check(lib().hfgpu_set_schedule(self.h, s.ctypes.data_as(_ip)))
 
     def last_launches(self) -> int:

@@ -206,19 +206,22 @@ int hfgpu_last_launches(const hfgpu_handle* h, int* kernels);
 int hfgpu_fp64_peak(int device, double* tflops);
 
 /* Launch schedule of the J/K build (no reference counterpart: the reference has one CPU
- * code path).  Three ints per quartet class, HFGPU_NUM_CLASSES classes in the order of
- * hfgpu_class_stats: threads per block of the thread-per-quartet form (32, 64, 128),
- * lanes per quartet of the primitive-split form used for quartets with many primitive
- * quartets (4, 8, 16, 32; 1 = 32; 0 = thread form; classes without that form ignore it),
- * 1/0/-1 = warp-per-quartet form for the classes that have
- * one, (dp|pp) (dp|ds) (dp|dp) (dd|pp) (dd|ds) (dd|dp) (dd|dd) (-1 = follow
- * opts.warp_max_quartets).  Default: 64, 0, and -1 for (dd|dp), (dd|dd), 0 otherwise.
- * "Many" primitive quartets means at least 16 for the quartet.
+ * code path).  Four ints per quartet class, HFGPU_NUM_CLASSES classes in the order of
+ * hfgpu_class_stats:
+ *   [0] threads per block of the thread-per-quartet form (32, 64, 128);
+ *   [1] lanes per quartet of the primitive-split form used for quartets with at least 16
+ *       primitive quartets (4, 8, 16, 32; 1 = 32; 0 = thread form; classes without that
+ *       form ignore it);
+ *   [2] 1/0/-1 = warp-per-quartet form for the classes that have one, (dp|pp) (dp|ds) (dp|dp)
+ *       (dd|pp) (dd|ds) (dd|dp) (dd|dd) (-1 = follow opts.warp_max_quartets);
+ *   [3] 1/0 = register-capped variant of the thread form, for more warps per SM (the small
+ *       classes (ps|ss) ... (dp|ss) have one; others ignore it).
+ * Default: 64, 0, -1 for (dd|dp) and (dd|dd) else 0, 0.
  * autotune: times every form of every class on the current geometry with device density D
  * (n x n; `repeats` builds per candidate, one class at a time on the handle's stream),
  * keeps the fastest, then keeps the result only if whole builds with it beat whole builds
- * with the schedule it started from, and returns the schedule in `schedule` (may be NULL).  Results of later
- * builds do not depend on the schedule beyond FP64 summation order. */
+ * with the schedule it started from, and returns the schedule in `schedule` (may be NULL).
+ * Results of later builds do not depend on the schedule beyond FP64 summation order. */
 #define HFGPU_NUM_CLASSES 21
 int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule);
 int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule);

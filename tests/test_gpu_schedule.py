@@ -33,11 +33,11 @@ def _molecules():
 
 
 MOLS = _molecules()
-# (block, primwarp, warp) applied to every class
-FORMS = [(32, 0, 0), (64, 1, 0), (128, 0, 1), (64, 1, 1), (64, 4, 0), (32, 8, 1), (128, 16, 0)]
+# (block, primwarp, warp, capped) applied to every class
+FORMS = [(32, 0, 0, 0), (64, 1, 0, 1), (128, 0, 1, 0), (64, 1, 1, 0), (64, 4, 0, 1), (32, 8, 1, 1), (128, 16, 0, 0)]
 
 
-@pytest.mark.parametrize("form", FORMS, ids=[f"b{f[0]}-pw{f[1]}-w{f[2]}" for f in FORMS])
+@pytest.mark.parametrize("form", FORMS, ids=[f"b{f[0]}-pw{f[1]}-w{f[2]}-c{f[3]}" for f in FORMS])
 @pytest.mark.parametrize("name,bs", MOLS, ids=[m[0] for m in MOLS])
 def test_every_launch_form_matches_oracle(name, bs, form):
     rng = np.random.default_rng(29)
@@ -74,9 +74,10 @@ def test_autotuned_schedule_gives_the_same_fock_build():
         F0 = eng.fock_rhf(D, H)
         Fm0 = eng.fock_rhf(D, H, E.MIXED)
         sched = eng.autotune(D, repeats=2)
-        assert sched.shape == (E.NUM_CLASSES, 3)
+        assert sched.shape == (E.NUM_CLASSES, 4)
         assert set(np.unique(sched[:, 0])) <= {32, 64, 128}
         assert set(np.unique(sched[:, 1])) <= {0, 1, 4, 8, 16, 32} and set(np.unique(sched[:, 2])) <= {-1, 0, 1}
+        assert set(np.unique(sched[:, 3])) <= {0, 1}
         assert (eng.get_schedule() == sched).all()
         F1 = eng.fock_rhf(D, H)
         Fm1 = eng.fock_rhf(D, H, E.MIXED)
