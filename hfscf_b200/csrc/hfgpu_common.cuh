@@ -73,28 +73,34 @@ __device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
 //
 // Method (Gill, Johnson & Pople, Int. J. Quantum Chem. 40, 745 (1991); Helgaker,
 // Jorgensen & Olsen, "Molecular Electronic-Structure Theory", sec. 9.8.2):
-//   T <  BOYS_TMAX: six-term Taylor expansion of F_M about the nearest grid point
-//                  T_k = k h (h = 0.1), F_M(T) = sum_j F_{M+j}(T_k) (-dT)^j / j!,
-//                  then the stable downward recursion
+//   T <  BOYS_TMAX: Taylor expansion of F_M about the nearest grid point T_k = k h
+//                  (h = 0.1), F_M(T) = sum_j F_{M+j}(T_k) (-dT)^j / j!, j = 0..6 in FP64
+//                  (0..3 in FP32), then the stable downward recursion
 //                  F_{m-1} = (2T F_m + e^-T) / (2m - 1), where (FP64) e^-T = e^-T_k e^(T_k - T)
 //                  with e^-T_k tabulated and e^d, |d| <= h/2, from its degree-8 Taylor
 //                  polynomial (remainder below (h/2)^9 / 9! = 5e-18 relative);
 //   T >= BOYS_TMAX: F_0 = sqrt(pi/T)/2 (erf(sqrt T) = 1 to double precision there)
 //                  and the upward recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T).
-// The table F_m(T_k) is computed on the host from the convergent series
-// F_m(T) = e^-T sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)) in long double.
+// Table layout: one row of 8 values per (order M, grid point k), rows of one order
+// contiguous.  FP64 row: F_{M+j}(T_k) / j!, j = 0..6, then e^-T_k (64 bytes, four 16-byte
+// loads give the whole expansion); FP32 row: F_{M+j}(T_k) / j!, j = 0..3, then e^-T_k and
+// padding (32 bytes).  The values F_m(T_k) are computed on the host from the convergent
+// series F_m(T) = e^-T sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)) in long double.
 // ---------------------------------------------------------------------------
 #define BOYS_H 0.1
 #define BOYS_NGRID 361           // T_k = 0 .. 36
 #define BOYS_TMAX 36.0
-#define BOYS_NM 18               // m = 0 .. 17 tabulated (m <= 10 used + 7 Taylor terms)
+#define BOYS_MMAX 10             // orders M = 0 .. 10 have rows
+#define BOYS_NM 18               // m = 0 .. 17 computed on the host (M <= 10 plus 7 Taylor terms)
+#define BOYS_ROW 8               // values per row
 
 template <typename R>
 struct BoysTable {
-  const R* __restrict__ tab;  // [BOYS_NGRID][BOYS_NM], then e^-T_k [BOYS_NGRID]
+  const R* __restrict__ tab;  // [BOYS_MMAX + 1][BOYS_NGRID][BOYS_ROW]
 
   template <int M>
   __device__ __forceinline__ void eval(R T, R pre, R* F) const {
+    static_assert(M <= BOYS_MMAX, "Boys order beyond the table");
     if (T < R(BOYS_TMAX)) {
       int k;
       R d;  // -(T - T_k)
@@ -108,21 +114,28 @@ struct BoysTable {
         k = __float2int_rn(T * R(10));
         d = R(k) * R(BOYS_H) - T;
       }
-      const R* row = tab + k * BOYS_NM + M;
+      const R* row = tab + ((size_t)M * BOYS_NGRID + k) * BOYS_ROW;
       R f;
+      R ek;  // e^-T_k
       if constexpr (sizeof(R) == 8) {
-        f = row[6];
-        f = row[5] + f * d * R(1.0 / 6.0);
-        f = row[4] + f * d * R(1.0 / 5.0);
-        f = row[3] + f * d * R(1.0 / 4.0);
-        f = row[2] + f * d * R(1.0 / 3.0);
-        f = row[1] + f * d * R(1.0 / 2.0);
-        f = row[0] + f * d;
+        const double2* r = reinterpret_cast<const double2*>(row);
+        const double2 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+        f = r3.x;
+        f = r2.y + f * d;
+        f = r2.x + f * d;
+        f = r1.y + f * d;
+        f = r1.x + f * d;
+        f = r0.y + f * d;
+        f = r0.x + f * d;
+        ek = r3.y;
       } else {
-        f = row[3];
-        f = row[2] + f * d * R(1.0 / 3.0);
-        f = row[1] + f * d * R(1.0 / 2.0);
-        f = row[0] + f * d;
+        const float4* r = reinterpret_cast<const float4*>(row);
+        const float4 r0 = r[0];
+        f = r0.w;
+        f = r0.z + f * d;
+        f = r0.y + f * d;
+        f = r0.x + f * d;
+        ek = R(0);
       }
       F[M] = f;
       if constexpr (M > 0) {
@@ -137,8 +150,9 @@ struct BoysTable {
           x = R(0.5) + d * x;
           x = R(1.0) + d * x;
           x = R(1.0) + d * x;
-          e = tab[BOYS_NGRID * BOYS_NM + k] * x;
+          e = ek * x;
         } else {
+          (void)ek;
           e = exp_t<R>(-T);
         }
         const R t2 = T + T;

@@ -29,10 +29,12 @@ constexpr double kPrimQuartetCut = 1e-16;
 int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }  // la >= lb: ss ps pp ds dp dd
 int quartet_class(int cp, int cq) { return cp * (cp + 1) / 2 + cq; }  // cp >= cq
 
-// Boys table F_m(k h), m < BOYS_NM, from the series e^-T sum_i (2T)^i / (2m+1)(2m+3)...(2m+2i+1).
-// After the table: e^-T_k for k < BOYS_NGRID.
-std::vector<double> boys_table() {
-  std::vector<double> t((size_t)BOYS_NGRID * BOYS_NM + BOYS_NGRID);
+// Boys table rows (layout in hfgpu_common.cuh): F_m(k h), m < BOYS_NM, from the series
+// e^-T sum_i (2T)^i / (2m+1)(2m+3)...(2m+2i+1) in long double, divided by j! for the j-th
+// Taylor term, and e^-T_k.  `terms` = 7 (FP64 rows) or 4 (FP32 rows).
+template <typename R>
+std::vector<R> boys_table(int terms) {
+  std::vector<long double> F((size_t)BOYS_NGRID * BOYS_NM), ek(BOYS_NGRID);
   for (int k = 0; k < BOYS_NGRID; ++k) {
     const long double T = (long double)k * (long double)BOYS_H;
     for (int m = 0; m < BOYS_NM; ++m) {
@@ -42,10 +44,21 @@ std::vector<double> boys_table() {
         sum += term;
         if (term < sum * 1e-21L) break;
       }
-      t[(size_t)k * BOYS_NM + m] = (double)(expl(-T) * sum);
+      F[(size_t)k * BOYS_NM + m] = expl(-T) * sum;
     }
-    t[(size_t)BOYS_NGRID * BOYS_NM + k] = (double)expl(-T);
+    ek[k] = expl(-T);
   }
+  std::vector<R> t((size_t)(BOYS_MMAX + 1) * BOYS_NGRID * BOYS_ROW, R(0));
+  for (int M = 0; M <= BOYS_MMAX; ++M)
+    for (int k = 0; k < BOYS_NGRID; ++k) {
+      R* row = &t[((size_t)M * BOYS_NGRID + k) * BOYS_ROW];
+      long double fact = 1.0L;
+      for (int j = 0; j < terms; ++j) {
+        if (j > 0) fact *= j;
+        row[j] = (R)(F[(size_t)k * BOYS_NM + M + j] / fact);
+      }
+      row[terms] = (R)ek[k];
+    }
   return t;
 }
 
@@ -1026,12 +1039,11 @@ int hfgpu_create(const hfgpu_basis* b, const hfgpu_opts* opts, hfgpu_handle** ou
     return HFGPU_ERR_CUDA;
   }
   h->own_stream = true;
-  std::vector<double> bt = boys_table();
-  std::vector<float> btf(bt.size());
-  for (size_t i = 0; i < bt.size(); ++i) btf[i] = (float)bt[i];
-  if (h->d_boys_d.ensure(sizeof(double) * bt.size()) || h->d_boys_f.ensure(sizeof(float) * bt.size()) ||
+  const std::vector<double> bt = boys_table<double>(7);
+  const std::vector<float> btf = boys_table<float>(4);
+  if (h->d_boys_d.ensure(sizeof(double) * bt.size()) || h->d_boys_f.ensure(sizeof(float) * btf.size()) ||
       cudaMemcpy(h->d_boys_d.p, bt.data(), sizeof(double) * bt.size(), cudaMemcpyHostToDevice) ||
-      cudaMemcpy(h->d_boys_f.p, btf.data(), sizeof(float) * bt.size(), cudaMemcpyHostToDevice)) {
+      cudaMemcpy(h->d_boys_f.p, btf.data(), sizeof(float) * btf.size(), cudaMemcpyHostToDevice)) {
     hfgpu_destroy(h);
     return HFGPU_ERR_CUDA;
   }
