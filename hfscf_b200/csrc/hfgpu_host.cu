@@ -1544,6 +1544,16 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
   } restore{h, h->class_mask, e0, e1};
   int start[4 * 21];
   hfgpu_get_schedule(h, start);
+  // best candidate per class and kind of form: 0 thread per quartet, 1 primitive-split for
+  // the many-primitive segments, 2 warp per quartet
+  struct Cand {
+    float ms;
+    int b, p, w, c;
+  };
+  std::vector<Cand> kind_best((size_t)3 * hfgpu::kNumClasses, Cand{1e30f, 0, 0, 0, 0});
+  auto kind_of = [&](int c, int pw, int wp) {
+    return wp == 1 ? 2 : (hfgpu::kClassLaunchers[c]->has_primwarp && pw > 0 ? 1 : 0);
+  };
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     if (h->q_end[c] <= h->q_beg[c]) continue;
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
@@ -1578,6 +1588,8 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
             bw = wp;
             bc = cap;
           }
+          Cand& kb = kind_best[(size_t)3 * c + kind_of(c, pw, wp)];
+          if (ms < kb.ms) kb = Cand{ms, bs, h->sched_primwarp[c], wp, cap};
         }
       }
     }
@@ -1586,9 +1598,48 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
     h->sched_warp[c] = bw;
     h->sched_cap[c] = bc;
   }
-  // Classes were timed one at a time; in a build they run concurrently.  Keep the tuned
-  // schedule only if a whole build with it beats one with the schedule we started from.
+  // Classes were timed one at a time; in a build they run concurrently on several streams,
+  // where a slower form that overlaps better can win.  Refinement on whole builds: per
+  // class, the best candidate of each other kind replaces the current form if the build
+  // gets at least 1% faster.
   h->class_mask = restore.mask;
+  auto time_builds = [&](float* ms) -> int {
+    int r0;
+    if ((r0 = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return r0;  // warm-up
+    HF_CUDA(h, cudaEventRecord(e0, h->stream));
+    for (int r = 0; r < repeats; ++r)
+      if ((r0 = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return r0;
+    HF_CUDA(h, cudaEventRecord(e1, h->stream));
+    HF_CUDA(h, cudaEventSynchronize(e1));
+    HF_CUDA(h, cudaEventElapsedTime(ms, e0, e1));
+    return HFGPU_OK;
+  };
+  float cur = 0.f;
+  if ((rc = time_builds(&cur))) return rc;
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    if (h->q_end[c] <= h->q_beg[c]) continue;
+    for (int k = 0; k < 3; ++k) {
+      const Cand& cd = kind_best[(size_t)3 * c + k];
+      if (cd.ms >= 1e30f || k == kind_of(c, h->sched_primwarp[c], h->sched_warp[c])) continue;
+      const Cand keep{0.f, h->sched_block[c], h->sched_primwarp[c], h->sched_warp[c], h->sched_cap[c]};
+      h->sched_block[c] = cd.b;
+      h->sched_primwarp[c] = cd.p;
+      h->sched_warp[c] = cd.w;
+      h->sched_cap[c] = cd.c;
+      float ms = 0.f;
+      if ((rc = time_builds(&ms))) return rc;
+      if (ms < 0.99f * cur) {
+        cur = ms;
+      } else {
+        h->sched_block[c] = keep.b;
+        h->sched_primwarp[c] = keep.p;
+        h->sched_warp[c] = keep.w;
+        h->sched_cap[c] = keep.c;
+      }
+    }
+  }
+  // Keep the tuned schedule only if whole builds with it beat whole builds with the schedule
+  // we started from.
   int tuned[4 * 21];
   hfgpu_get_schedule(h, tuned);
   float t_tuned = 0.f, t_start = 0.f;

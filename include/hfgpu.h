@@ -219,8 +219,10 @@ int hfgpu_fp64_peak(int device, double* tflops);
  * Default: 64, 0, -1 for (dd|dp) and (dd|dd) else 0, 0.
  * autotune: times every form of every class on the current geometry with device density D
  * (n x n; `repeats` builds per candidate, one class at a time on the handle's stream),
- * keeps the fastest, then keeps the result only if whole builds with it beat whole builds
- * with the schedule it started from, and returns the schedule in `schedule` (may be NULL).
+ * keeps the fastest; then, on whole builds, tries per class the best candidate of each other
+ * kind of form (thread, primitive-split, warp) and keeps it where the build gets at least 1%
+ * faster; keeps the result only if whole builds with it beat whole builds with the schedule
+ * it started from, and returns the schedule in `schedule` (may be NULL).
  * Results of later builds do not depend on the schedule beyond FP64 summation order. */
 #define HFGPU_NUM_CLASSES 21
 int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule);
