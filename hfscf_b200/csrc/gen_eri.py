@@ -795,7 +795,7 @@ static bool launch_primwarp(const QuartetArgs<R>& a, const int2* q, int nq, cuda
 template <typename R>
 static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, int grid, cudaStream_t s) {{
   if (nq <= 0) return;
-  grad_kernel<{la}, {lb}, {lc}, {ld}, R><<<grid, 128, 0, s>>>(a, pure, q, nq);
+  grad_kernel<{la}, {lb}, {lc}, {ld}, R><<<grid, 128, sizeof(double) * 3 * a.smem_atoms, s>>>(a, pure, q, nq);
 }}
 template <typename CC, typename R>
 static bool launch_grad_warp_impl(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{

@@ -774,6 +774,16 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
 
 // Warp form for a gradient launch of nq quartets of class c: when the class has one and the
 // launch fills at most opts.grad_warp_max_waves waves of the blocks all SMs hold at once.
+// Gradient accumulation of grad_kernel: per block in shared memory when the natoms x 3
+// totals fit in kGradSmemBytes, and then no more than kGradMaxBlocks blocks for the
+// straight-line classes (their grid-stride loop takes the rest), so that the flush at the
+// end of each block stays a small number of atomics.
+constexpr int kGradSmemBytes = 24 * 1024;
+constexpr int kGradMaxBlocks = 2048;
+int grad_smem_atoms(const hfgpu_handle* h) {
+  return (size_t)h->natoms * 3 * sizeof(double) <= (size_t)kGradSmemBytes ? h->natoms : 0;
+}
+
 static bool grad_use_warp(const hfgpu_handle* h, int c, long long nq, bool fp32) {
   const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
   if (!L->has_grad_warp || h->opts.grad_warp_max_waves <= 0) return false;
@@ -812,6 +822,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   gf.DJ = DJ; gf.cJ = cJ; gf.nK = nK; gf.DK = DK; gf.cK = cK; gf.grad = grad;
   gf.mol_off = gd.mol_off;
   gf.mol_n = gd.mol_n;
+  gd.smem_atoms = gf.smem_atoms = grad_smem_atoms(h);
   const int2* q = h->d_quart.as<int2>();
   const size_t budget = (size_t)1 << 30;  // scratch bytes per table-mode class and precision
   // threads of a table-mode launch: as many as the budget allows (at least 4736),
@@ -866,6 +877,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
       unsigned char* slice = h->d_scratch.as<unsigned char>() + off;
       cudaStream_t st = fp32 ? st_f : st_d;
       int grid = (nq + 127) / 128;
+      if (slots == 0 && gd.smem_atoms > 0) grid = std::min(grid, kGradMaxBlocks);
       if (slots > 0) {
         const size_t rb = fp32 ? sizeof(float) : sizeof(double);
         grid = (int)(table_threads(slots, nq) / 128);
@@ -913,6 +925,11 @@ int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int n
   gd.n = h->n;
   gd.DJ = DJ; gd.cJ = cJ; gd.nK = nK; gd.DK = DK; gd.cK = cK; gd.grad = grad;
   gd.scratch = static_cast<double*>(scratch);
+  if (h->batched) {
+    if (nK > 1) return fail(h, HFGPU_ERR_UNSUPPORTED, "batched handles take one density");
+    gd.mol_off = h->d_mol.as<long long>();
+    gd.mol_n = reinterpret_cast<const int*>(gd.mol_off + h->nmol);
+  }
   GradArgs<float> gf{};
   gf.pairs = gd.pairs;
   gf.prims = h->d_prim_f.as<PrimPair<float>>();
@@ -922,6 +939,9 @@ int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int n
   gf.n = h->n;
   gf.DJ = DJ; gf.cJ = cJ; gf.nK = nK; gf.DK = DK; gf.cK = cK; gf.grad = grad;
   gf.scratch = static_cast<float*>(scratch);
+  gf.mol_off = gd.mol_off;
+  gf.mol_n = gd.mol_n;
+  gd.smem_atoms = gf.smem_atoms = grad_smem_atoms(h);
   const int2* q = h->d_quart.as<int2>();
   for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
@@ -935,6 +955,7 @@ int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int n
       const int nq = (int)(hi - lo);
       if (nq <= 0) continue;
       int grid = (nq + 127) / 128;
+      if (slots == 0 && gd.smem_atoms > 0) grid = std::min(grid, kGradMaxBlocks);
       if (slots > 0) {
         const size_t per_thread = (size_t)slots * (fp32 ? sizeof(float) : sizeof(double));
         const long long fit = (long long)(scratch_bytes / per_thread) / 128 * 128;

@@ -51,6 +51,8 @@ struct GradArgs {
   const int* __restrict__ mol_n;
   R* __restrict__ scratch;           // thread-interleaved scratch (table-mode classes)
   int scratch_threads;               // threads sharing the scratch (stride)
+  int smem_atoms;                    // grad_kernel: > 0 = accumulate 3 x smem_atoms entries per block in
+                                     // shared memory, then one atomic per entry (0: atomics into grad)
 };
 
 template <int NA, int NB, int NC, int ND>
@@ -485,7 +487,7 @@ __device__ __forceinline__ void grad_weights(const double* __restrict__ DJ, doub
 }
 
 template <int LA, int LB, int LC, int LD, typename R, bool PURE>
-__device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, const int2 pq) {
+__device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, const int2 pq, double* gout) {
   using Dm = BlockDims<LA, LB, LC, LD, PURE>;
   using CC = ClassCode<LA, LB, LC, LD>;
   {
@@ -569,23 +571,40 @@ __device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, cons
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double gA = double(g[d]), gB = double(g[3 + d]), gC = double(g[6 + d]);
-      atomicAdd(a.grad + 3 * at[0] + d, gA);
-      atomicAdd(a.grad + 3 * at[1] + d, gB);
-      atomicAdd(a.grad + 3 * at[2] + d, gC);
-      atomicAdd(a.grad + 3 * Q.atom_b + d, -(gA + gB + gC));
+      atomicAdd(gout + 3 * at[0] + d, gA);
+      atomicAdd(gout + 3 * at[1] + d, gB);
+      atomicAdd(gout + 3 * at[2] + d, gC);
+      atomicAdd(gout + 3 * Q.atom_b + d, -(gA + gB + gC));
     }
   }
 }
 
+// Every quartet adds 12 values into the natoms x 3 gradient.  Straight into global memory
+// those are millions of atomics on a few dozen addresses, serialised in L2; with
+// a.smem_atoms > 0 each block sums into shared memory first and adds its 3 natoms totals
+// once at the end.
 template <int LA, int LB, int LC, int LD, typename R>
 __global__ void __launch_bounds__(128) grad_kernel(GradArgs<R> a, int pure, const int2* __restrict__ quartets, int nq) {
+  extern __shared__ double grad_sh[];
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int nthr = gridDim.x * blockDim.x;
+  const int nsh = 3 * a.smem_atoms;
+  double* gout = a.grad;
+  if (nsh > 0) {
+    for (int i = threadIdx.x; i < nsh; i += blockDim.x) grad_sh[i] = 0.0;
+    __syncthreads();
+    gout = grad_sh;
+  }
   for (int t = tid; t < nq; t += nthr) {
     if (pure)
-      grad_quartet<LA, LB, LC, LD, R, true>(a, tid, quartets[t]);
+      grad_quartet<LA, LB, LC, LD, R, true>(a, tid, quartets[t], gout);
     else
-      grad_quartet<LA, LB, LC, LD, R, false>(a, tid, quartets[t]);
+      grad_quartet<LA, LB, LC, LD, R, false>(a, tid, quartets[t], gout);
+  }
+  if (nsh > 0) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < nsh; i += blockDim.x)
+      if (grad_sh[i] != 0.0) atomicAdd(a.grad + i, grad_sh[i]);
   }
 }
 

@@ -61,3 +61,44 @@ def test_noalloc_gradient_matches_allocating_entry_point_on_two_calls(case):
             assert rc == 0, lib.hfgpu_last_error(eng.h)
             torch.cuda.synchronize()
             assert np.max(np.abs(out.cpu().numpy() - g_ref)) < TOL
+
+
+def test_noalloc_gradient_of_a_batched_handle():
+    """A batched handle (one water hexamer and two single waters) through the scratch-free
+    entry point: every molecule's block of the concatenated density is read at its own
+    offset, as in hfgpu_batch_grad2e_device."""
+    import torch
+
+    from hfscf_b200 import basis as B
+    from hfscf_b200 import batch
+    from hfscf_b200 import engine as E
+    from hfscf_b200 import molecules as M
+    rng = np.random.default_rng(5)
+    mols = []
+    for k in (6, 1, 1):
+        Z, x = M.water_cluster(k, 3.0, rng, 0.05)
+        mols.append((np.asarray(Z), np.asarray(x) * B.ANGSTROM_TO_BOHR, "6-31g*", False))
+    bases = batch.batch_bases(mols)
+    be = batch.BatchEngine(bases)
+    dev = torch.device("cuda", 0)
+    blocks = []
+    for b in bases:
+        A = rng.normal(size=(b.nbf, b.nbf))
+        blocks.append(((A + A.T) / b.nbf).ravel())
+    D = torch.from_numpy(np.concatenate(blocks)).to(dev)
+    natoms = sum(b.natoms for b in bases)
+    ref = torch.zeros((natoms, 3), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    be.grad2e_device(D, ref)
+    torch.cuda.synchronize()
+    lib = E.lib()
+    for _ in range(2):
+        out = torch.zeros_like(ref)
+        torch.cuda.synchronize()
+        rc = lib.hfgpu_grad2e_device_noalloc(be.h, ctypes.c_void_p(D.data_ptr()), ctypes.c_double(2.0),
+                                             ctypes.c_int(1), ctypes.c_void_p(D.data_ptr()), ctypes.c_double(1.0),
+                                             ctypes.c_void_p(out.data_ptr()), ctypes.c_int(E.FP64))
+        assert rc == 0, lib.hfgpu_last_error(be.h)
+        torch.cuda.synchronize()
+        assert np.max(np.abs(out.cpu().numpy() - ref.cpu().numpy())) < TOL
+    be.close()
