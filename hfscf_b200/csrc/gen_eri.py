@@ -337,15 +337,18 @@ def gen_eri_class(la, lb, lc, ld):
     s.append(f"  R acc[{len(targets)}];")
     s.append(f"#pragma unroll")
     s.append(f"  for (int t = 0; t < {len(targets)}; ++t) acc[t] = R(0);")
-    s.append("  for (int ib = 0; ib < nbp; ++ib) {")
-    s.append("    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
-    s.append("    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;")
+    # Ket primitives outside, bra primitives inside: the lanes of a warp mostly hold
+    # quartets of one bra pair (the lists are bra-major), so the inner loads are broadcasts
+    # and the gathers of the lanes' different ket pairs happen once per ket primitive.
+    s.append("  for (int ik = 0; ik < nkp; ++ik) {")
+    s.append("    const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
+    s.append("    const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;")
     if len(vrr.memo) <= UNROLL2_MAX_VRR:
         # small classes: two primitive quartets in flight hide the load latency
         s.append("#pragma unroll 2")
-    s.append("    for (int ik = 0; ik < nkp; ++ik) {")
-    s.append("      const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
-    s.append("      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;")
+    s.append("    for (int ib = 0; ib < nbp; ++ib) {")
+    s.append("      const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
+    s.append("      const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;")
     s.append(PRIM_HEADER.rstrip("\n"))
     s.append(f"      R F[{L + 1}];")
     s.append(f"      boys.template eval<{L}>(T, pre, F);")
