@@ -357,9 +357,21 @@ def run_ours(args, world, rank, local):
         line["batch"] = {"workload": "512 seeded molecules ((H2O)1-6, CH4, C2H6, NH3; STO-3G or 6-31G*), "
                                      "RHF to convergence + RHF gradient each, one batched handle",
                          "molecules_per_s": 512 / wall, "wall_s": wall, "setup_s": rb["setup_s"],
-                         "scf_s": rb["scf_s"], "grad_s": rb["grad_s"], "iterations": rb["iterations"],
+                         "setup_stages_s": {k: round(v, 4) for k, v in rb["setup_stages_s"].items()},
+                         "scf_s": rb["scf_s"], "grad_s": rb["grad_s"], "final_s": rb["final_s"],
+                         "close_s": rb["close_s"], "iterations": rb["iterations"],
                          "converged": int(rb["converged"].sum()), "cuda_graph": rb["graph"], "autotuned": rb["autotuned"],
                          "jk_build_ms": rb["build_ms_mean"], "nbf_total": int(sum(b.nbf for b in bb))}
+        # the same batch in mixed precision (FP32 quartets below the Schwarz bound 1e-4)
+        torch.cuda.synchronize()
+        tb = time.perf_counter()
+        rbm = BT.batch_rhf(bb, device=local, precision=E.MIXED)
+        wall_m = DI.max_over_ranks(time.perf_counter() - tb, dev)
+        torch.cuda.set_stream(stream)
+        line["batch"]["mixed"] = {"molecules_per_s": 512 / wall_m, "wall_s": wall_m, "setup_s": rbm["setup_s"],
+                                  "scf_s": rbm["scf_s"], "grad_s": rbm["grad_s"], "iterations": rbm["iterations"],
+                                  "converged": int(rbm["converged"].sum()),
+                                  "max_abs_dE_vs_fp64": float(np.max(np.abs(rbm["energies"] - rb["energies"])))}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
         ref = reference_fock_build_seconds(bs)

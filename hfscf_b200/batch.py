@@ -65,6 +65,13 @@ class BatchEngine:
         if rc:
             raise eng.HfgpuError(rc, eng.lib().hfgpu_last_error(self.h).decode())
 
+    def setup_times(self):
+        """Host wall time (s) of the handle's set-up: primitive pairs, Schwarz factors,
+        quartet lists, list upload (hfgpu_setup_times)."""
+        ms = (ctypes.c_double * 4)()
+        self._check(eng.lib().hfgpu_setup_times(self.h, ms))
+        return dict(zip(("pairs", "schwarz", "lists", "upload"), [v / 1e3 for v in ms]))
+
     def set_stream(self, stream_ptr):
         self._check(eng.lib().hfgpu_set_stream(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
 
@@ -164,6 +171,8 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
 
     be = BatchEngine(bases, device)
     tt = stage("handle", t0)
+    for k, v in be.setup_times().items():
+        stages["handle_" + k] = v
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
     be.set_stream(stream.cuda_stream)
@@ -299,6 +308,7 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
             break
     torch.cuda.synchronize()
     t_scf = time.perf_counter() - t1
+    t_fin = time.perf_counter()
     # final Fock matrices at the converged densities
     Dblk.copy_(lay.to_block(D))
     build()
@@ -309,7 +319,8 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     out = {"energies": E_el + enuc, "iterations": it, "converged": converged.cpu().numpy(),
            "setup_s": t_setup, "setup_stages_s": stages, "scf_s": t_scf, "graph": graph is not None,
            "autotuned": schedule is not None,
-           "build_ms_mean": 1e3 * float(np.mean(build_times)), "nmol": nmol}
+           "build_ms_mean": 1e3 * float(np.mean(build_times)), "nmol": nmol,
+           "final_s": time.perf_counter() - t_fin}
     if gradient:
         t2 = time.perf_counter()
         g = torch.zeros((int(be.atom_off[-1]), 3), dtype=torch.float64, device=dev)
@@ -323,9 +334,11 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
                  for k, b in enumerate(bases)]
         out["gradients"] = grads
         out["grad_s"] = time.perf_counter() - t2
+    t3 = time.perf_counter()
     pool.shutdown()
     be.close()
     torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    out["close_s"] = time.perf_counter() - t3
     return out
 
 

@@ -2,6 +2,7 @@
 // factors, screened quartet lists, and the C ABI of include/hfgpu.h.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <thread>
 #include <climits>
 #include <cmath>
@@ -132,6 +133,7 @@ struct hfgpu_handle {
   DevBuf d_mats, d_half, d_dmax, d_counters, d_grad, d_scratch, d_eri, d_eriq;
   long long last_launched = 0, last_skipped = 0;
   int last_kernels = 0;                 // kernel launches of the last J/K build
+  double setup_ms[4] = {0, 0, 0, 0};    // last set_geometry: pairs, Schwarz, quartet lists (host), list upload
   // class kernels run concurrently on auxiliary streams (fork/join with events)
   static constexpr int kAux = 6;
   cudaStream_t aux[kAux] = {};
@@ -398,100 +400,152 @@ int bound_decade(double b) {
 }
 
 // Screened unique quartets (P <= Q within a class; bra class >= ket class), per class.
-// Quartet list of one class (pair classes cp >= cq), in four segments, each ordered by one
-// stable counting sort on (bound decade, largest primitive-quartet count first): the decades
-// make the prefix launches of density-screened builds possible, the counts let the 32 lanes
-// of a warp loop over similar numbers of primitive quartets.  Offsets are relative to the
-// start of the class's list.
-struct ClassList {
-  std::vector<int2> q;
-  long long seg[5] = {0, 0, 0, 0, 0};
-  long long bend[4 * kBuckets] = {0};
+// Quartet list of one class (pair classes cp >= cq), in four segments (Schwarz bound at or
+// above the mixed-precision bound / below, each split into quartets with at least
+// kPrimWarpMinPrims primitive quartets / fewer), each ordered by one stable counting sort
+// on (bound decade, largest primitive-quartet count first): the decades make the prefix
+// launches of density-screened builds possible, the counts let the 32 lanes of a warp loop
+// over similar numbers of primitive quartets.
+//
+// Built in two parallel phases on all host threads.  Phase 1 filters the candidates of
+// chunks of about kListChunkWork candidate quartets (consecutive bra pairs of one class) and
+// keeps each chunk's survivors in bra-pair order with their sort keys; phase 2 sorts every
+// (class, segment) with one counting sort over its chunks in order and writes it into place.
+// The lists are the same as those of one serial pass per class in bra-pair order.
+constexpr long long kListChunkWork = 1 << 20;
+constexpr int kProdSpan = 1 << 16;  // primitive-quartet counts above this share the last sort slot
+
+struct ListChunk {
+  int cls = 0;                  // index into the class table (cp, cq)
+  int P0 = 0, P1 = 0;           // bra pairs [P0, P1)
+  std::vector<int2> q[4];       // survivors per segment, in list order
+  std::vector<int> key[4];      // bound decade * kProdSpan + primitive-quartet count
+  int maxprod[4] = {0, 0, 0, 0};
 };
 
-static void build_class_list(const hfgpu_handle* h, int cp, int cq, ClassList& out) {
-  const double tol = h->opts.schwarz_tol, mix = h->opts.mixed_fp32_bound;
-  std::vector<int2> parts[4];  // high bound many-prim, high bound few-prim, low bound many, low bound few
-  const int nm1 = h->nmol + 1;
-  for (int mol = 0; mol < h->nmol; ++mol) {
-    const int pb = h->cm_begin[(size_t)cp * nm1 + mol], pe = h->cm_begin[(size_t)cp * nm1 + mol + 1];
-    const int kb = h->cm_begin[(size_t)cq * nm1 + mol], ke = h->cm_begin[(size_t)cq * nm1 + mol + 1];
-    for (int P = pb; P < pe; ++P) {
-      const double qp = h->pairs[P].schwarz;
-      const int np = h->pairs[P].nprim;
-      const int k0 = (cp == cq) ? P : kb;
-      for (int Q = k0; Q < ke; ++Q) {
-        const double b = qp * h->pairs[Q].schwarz;
-        if (b < tol) continue;
-        const bool many = np * h->pairs[Q].nprim >= kPrimWarpMinPrims;
-        parts[(b >= mix ? 0 : 2) + (many ? 0 : 1)].push_back(make_int2(P, Q));
-      }
-    }
-  }
-  size_t total = 0;
-  for (auto& v : parts) total += v.size();
-  out.q.resize(total);
-  long long base = 0;
-  for (int sg = 0; sg < 4; ++sg) {
-    out.seg[sg] = base;
-    const std::vector<int2>& in = parts[sg];
-    std::vector<int> key(in.size());
-    int maxprod = 0;
-    for (const int2& pqv : in) maxprod = std::max(maxprod, h->pairs[pqv.x].nprim * h->pairs[pqv.y].nprim);
-    const int nk = kBuckets * (maxprod + 1);
-    std::vector<long long> cnt((size_t)nk + 1, 0);
-    for (size_t x = 0; x < in.size(); ++x) {
-      const int2 pqv = in[x];
-      const int dec = bound_decade(h->pairs[pqv.x].schwarz * h->pairs[pqv.y].schwarz);
-      const int prod = h->pairs[pqv.x].nprim * h->pairs[pqv.y].nprim;
-      key[x] = dec * (maxprod + 1) + (maxprod - prod);
-      ++cnt[(size_t)key[x] + 1];
-    }
-    for (int k = 0; k < nk; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];  // cnt[k] = first slot of key k
-    for (int e = 0; e < kBuckets; ++e) out.bend[sg * kBuckets + e] = base + cnt[(size_t)(e + 1) * (maxprod + 1)];
-    for (size_t x = 0; x < in.size(); ++x) out.q[(size_t)base + (size_t)cnt[(size_t)key[x]]++] = in[x];
-    base += (long long)in.size();
-  }
-  out.seg[4] = base;
-}
-
-int build_quartets(hfgpu_handle* h) {
-  // the 21 classes are independent: built on host threads, then concatenated in class order
-  std::vector<std::pair<int, int>> cls;
-  for (int cp = 0; cp < kPairClasses; ++cp)
-    for (int cq = 0; cq <= cp; ++cq) cls.emplace_back(cp, cq);
-  std::vector<ClassList> lists(cls.size());
+template <typename F>
+void run_parallel(int ntask, F&& f) {
   std::atomic<int> next{0};
   auto work = [&]() {
-    for (int i = next++; i < (int)cls.size(); i = next++) build_class_list(h, cls[i].first, cls[i].second, lists[i]);
+    for (int i = next++; i < ntask; i = next++) f(i);
   };
-  const int nthr = (int)std::min<size_t>(cls.size(), std::max(1u, std::thread::hardware_concurrency()));
+  const int nthr = std::max(1, std::min<int>(ntask, (int)std::max(1u, std::thread::hardware_concurrency())));
   std::vector<std::thread> pool;
   for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
   work();
   for (auto& t : pool) t.join();
-  h->bucket_end.assign((size_t)hfgpu::kNumClasses * 4 * kBuckets, 0);
+}
+
+int build_quartets(hfgpu_handle* h) {
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  std::vector<std::pair<int, int>> cls;
+  for (int cp = 0; cp < kPairClasses; ++cp)
+    for (int cq = 0; cq <= cp; ++cq) cls.emplace_back(cp, cq);
+  const int ncls = (int)cls.size();
+  const int nm1 = h->nmol + 1;
+  // ket pair range [k0, ke) of bra pair P in class (cp, cq)
+  auto ket_range = [&](int cp, int cq, int P, int& k0, int& ke) {
+    const int mol = h->pairs[P].mol;
+    const int kb = h->cm_begin[(size_t)cq * nm1 + mol];
+    ke = h->cm_begin[(size_t)cq * nm1 + mol + 1];
+    k0 = (cp == cq) ? P : kb;
+  };
+  // chunks of consecutive bra pairs, about kListChunkWork candidates each
+  std::vector<ListChunk> chunks;
+  std::vector<int> cls_chunk0(ncls + 1, 0);
+  for (int i = 0; i < ncls; ++i) {
+    const int cp = cls[i].first, cq = cls[i].second;
+    cls_chunk0[i] = (int)chunks.size();
+    const int pb = h->class_begin[cp], pe = h->class_begin[cp + 1];
+    long long work = 0;
+    int start = pb;
+    for (int P = pb; P < pe; ++P) {
+      int k0, ke;
+      ket_range(cp, cq, P, k0, ke);
+      work += std::max(0, ke - k0);
+      if (work >= kListChunkWork || P + 1 == pe) {
+        ListChunk c;
+        c.cls = i;
+        c.P0 = start;
+        c.P1 = P + 1;
+        chunks.push_back(std::move(c));
+        start = P + 1;
+        work = 0;
+      }
+    }
+  }
+  cls_chunk0[ncls] = (int)chunks.size();
+  // phase 1: filter
+  const double tol = h->opts.schwarz_tol, mix = h->opts.mixed_fp32_bound;
+  run_parallel((int)chunks.size(), [&](int ci) {
+    ListChunk& c = chunks[ci];
+    const int cp = cls[c.cls].first, cq = cls[c.cls].second;
+    for (int P = c.P0; P < c.P1; ++P) {
+      const double qp = h->pairs[P].schwarz;
+      const int np = h->pairs[P].nprim;
+      int k0, ke;
+      ket_range(cp, cq, P, k0, ke);
+      for (int Q = k0; Q < ke; ++Q) {
+        const double b = qp * h->pairs[Q].schwarz;
+        if (b < tol) continue;
+        const int prod = std::min(np * h->pairs[Q].nprim, kProdSpan - 1);
+        const int sg = (b >= mix ? 0 : 2) + (prod >= kPrimWarpMinPrims ? 0 : 1);
+        c.q[sg].push_back(make_int2(P, Q));
+        c.key[sg].push_back(bound_decade(b) * kProdSpan + prod);
+        c.maxprod[sg] = std::max(c.maxprod[sg], prod);
+      }
+    }
+  });
+  // offsets: classes in class order, segments in order inside a class
+  std::vector<long long> seg_base((size_t)ncls * 5, 0);
   long long total = 0;
-  for (const ClassList& l : lists) total += (long long)l.q.size();
+  for (int i = 0; i < ncls; ++i) {
+    for (int sg = 0; sg < 4; ++sg) {
+      seg_base[(size_t)i * 5 + sg] = total;
+      for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci) total += (long long)chunks[ci].q[sg].size();
+    }
+    seg_base[(size_t)i * 5 + 4] = total;
+  }
   std::vector<int2> all((size_t)total);
-  long long base = 0;
-  for (size_t i = 0; i < cls.size(); ++i) {
+  h->bucket_end.assign((size_t)hfgpu::kNumClasses * 4 * kBuckets, 0);
+  // phase 2: one stable counting sort per (class, segment) on (decade, count descending)
+  run_parallel(ncls * 4, [&](int task) {
+    const int i = task / 4, sg = task % 4;
     const int qc = quartet_class(cls[i].first, cls[i].second);
-    const ClassList& l = lists[i];
-    h->q_beg[qc] = base + l.seg[0];
-    h->q_hik1[qc] = base + l.seg[1];
-    h->q_mid[qc] = base + l.seg[2];
-    h->q_hik2[qc] = base + l.seg[3];
-    h->q_end[qc] = base + l.seg[4];
-    for (int x = 0; x < 4 * kBuckets; ++x) h->bucket_end[(size_t)qc * 4 * kBuckets + x] = base + l.bend[x];
-    std::copy(l.q.begin(), l.q.end(), all.begin() + base);
-    base += (long long)l.q.size();
+    const long long base = seg_base[(size_t)i * 5 + sg];
+    int maxprod = 0;
+    for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci) maxprod = std::max(maxprod, chunks[ci].maxprod[sg]);
+    const int span = maxprod + 1;
+    const int nk = kBuckets * span;
+    auto key_of = [&](int raw) { return (raw / kProdSpan) * span + (maxprod - raw % kProdSpan); };
+    std::vector<long long> cnt((size_t)nk + 1, 0);
+    for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci)
+      for (const int raw : chunks[ci].key[sg]) ++cnt[(size_t)key_of(raw) + 1];
+    for (int k = 0; k < nk; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];  // cnt[k] = first slot of key k
+    for (int e = 0; e < kBuckets; ++e)
+      h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e] = base + cnt[(size_t)(e + 1) * span];
+    for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci) {
+      const ListChunk& c = chunks[ci];
+      for (size_t x = 0; x < c.q[sg].size(); ++x) all[(size_t)base + (size_t)cnt[(size_t)key_of(c.key[sg][x])]++] = c.q[sg][x];
+    }
+  });
+  for (int i = 0; i < ncls; ++i) {
+    const int qc = quartet_class(cls[i].first, cls[i].second);
+    h->q_beg[qc] = seg_base[(size_t)i * 5 + 0];
+    h->q_hik1[qc] = seg_base[(size_t)i * 5 + 1];
+    h->q_mid[qc] = seg_base[(size_t)i * 5 + 2];
+    h->q_hik2[qc] = seg_base[(size_t)i * 5 + 3];
+    h->q_end[qc] = seg_base[(size_t)i * 5 + 4];
   }
   h->nquartets = total;
+  const auto t1 = clk::now();
   HF_CUDA(h, h->d_quart.ensure(sizeof(int2) * std::max<size_t>(all.size(), 1)));
   if (!all.empty())
     HF_CUDA(h, cudaMemcpyAsync(h->d_quart.p, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, h->stream));
   HF_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->setup_ms[2] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  h->setup_ms[3] = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
   return HFGPU_OK;
 }
 
@@ -1116,9 +1170,15 @@ int hfgpu_set_geometry(hfgpu_handle* h, const double* xyz, int natoms) {
   if (rc) return rc;
   h->xyz.assign(xyz, xyz + 3 * natoms);
   h->have_geometry = false;
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
   if ((rc = build_pairs(h))) return rc;
+  const auto t1 = clk::now();
   if ((rc = compute_schwarz(h))) return rc;
-  if ((rc = build_quartets(h))) return rc;
+  const auto t2 = clk::now();
+  if ((rc = build_quartets(h))) return rc;  // sets setup_ms[2] and [3]
+  h->setup_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  h->setup_ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
   h->have_geometry = true;
   return HFGPU_OK;
 }
@@ -1499,6 +1559,12 @@ int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out) {
     out[7] = (long long)c[1];
     out[8] = (long long)c[2];
   }
+  return HFGPU_OK;
+}
+
+int hfgpu_setup_times(const hfgpu_handle* h, double* ms) {
+  if (!h || !ms) return HFGPU_ERR_INVALID;
+  for (int i = 0; i < 4; ++i) ms[i] = h->setup_ms[i];
   return HFGPU_OK;
 }
 

@@ -198,12 +198,15 @@ int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* ski
  *   bound, and from the last J/K build: quartets computed, skipped by density, primitive quartets computed.
  * class_time: event time (ms) of that class's kernels in the last J/K build.
  * last_launches: kernel launches of the last J/K (or Fock) build.
- * fp64_peak: FP64 FMA throughput of the device in TFLOP/s, from a register-only FMA kernel. */
+ * fp64_peak: FP64 FMA throughput of the device in TFLOP/s, from a register-only FMA kernel.
+ * setup_times(ms[4]): host wall time (ms) of the last hfgpu_set_geometry (or create): primitive
+ *   pairs, Schwarz factors, quartet lists built on the host, their upload to the device. */
 int hfgpu_set_timing(hfgpu_handle* h, int on);
 int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out);
 int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms);
 int hfgpu_last_launches(const hfgpu_handle* h, int* kernels);
 int hfgpu_fp64_peak(int device, double* tflops);
+int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
 
 /* Launch schedule of the J/K build (no reference counterpart: the reference has one CPU
  * code path).  Four ints per quartet class, HFGPU_NUM_CLASSES classes in the order of
