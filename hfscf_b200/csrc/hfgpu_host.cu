@@ -1046,7 +1046,7 @@ int hfgpu_default_opts(hfgpu_opts* o) {
   o->mixed_density_tol = 1e-12;
   o->device = 0;
   o->warp_max_quartets = 1 << 30;
-  o->grad_warp_max_waves = 24;
+  o->grad_warp_max_waves = 48;
   return HFGPU_OK;
 }
 

@@ -70,7 +70,7 @@ typedef struct {
   int grad_warp_max_waves;    /* gradient of (dp|dp) (dd|pp) (dd|ds) (dd|dp) (dd|dd): one warp per quartet
                                  (shared memory) when the class's quartets fill at most this many waves of
                                  the blocks the GPU holds at once, else one thread per quartet on global
-                                 scratch (default 24: longer warp-form launches hold the shared memory of
+                                 scratch (default 48: longer warp-form launches hold the shared memory of
                                  every SM and stop the other classes' kernels from overlapping; 0 = never) */
   int reserved[5];
 } hfgpu_opts;
