@@ -211,6 +211,13 @@ class Engine:
         keys = ("la", "lb", "lc", "ld", "screened", "high_bound", "computed", "skipped", "prim_quartets")
         return dict(zip(keys, list(out)))
 
+    def setup_times(self):
+        """Host wall time (s) of the last geometry set-up: primitive pairs, Schwarz factors,
+        quartet lists, list upload (hfgpu_setup_times)."""
+        ms = (ctypes.c_double * 4)()
+        self._check(lib().hfgpu_setup_times(self.h, ms))
+        return dict(zip(("pairs", "schwarz", "lists", "upload"), [v / 1e3 for v in ms]))
+
     def class_time_ms(self, cls: int) -> float:
         ms = ctypes.c_float()
         self._check(lib().hfgpu_class_time(self.h, ctypes.c_int(cls), ctypes.byref(ms)))

@@ -126,3 +126,25 @@ def test_batched_eigensolver_rejects_large_molecules():
         be.eigh(A, W, V)
     assert err.value.code == 6
     be.close()
+
+
+def test_setup_times_and_list_segments_cover_every_screened_quartet():
+    """hfgpu_setup_times reports the four set-up phases; the quartet lists built in parallel
+    chunks hold every quartet that passes the Schwarz test exactly once (class counts against
+    a host count of the screened quartets from the pair Schwarz factors)."""
+    rng = np.random.default_rng(12)
+    Z, x = M.water_cluster(3, 3.0, rng, 0.05)
+    bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    with E.Engine(bs) as eng:
+        t = eng.setup_times()
+        assert set(t) == {"pairs", "schwarz", "lists", "upload"}
+        assert all(v >= 0.0 for v in t.values()) and t["lists"] > 0.0
+        Q = eng.schwarz()
+        listed = sum(eng.class_stats(c)["screened"] for c in range(E.NUM_CLASSES))
+    # unique shell quartets (ab|cd), a >= b, c >= d, pair(ab) >= pair(cd) in the engine's
+    # canonical sense: count unordered pairs of unordered shell pairs with Q_ab Q_cd >= 1e-12
+    ns = len(bs.shells)
+    q = np.array([Q[i, j] for i in range(ns) for j in range(i + 1)])
+    prod = np.outer(q, q)
+    iu = np.triu_indices(len(q))
+    assert listed == int(np.count_nonzero(prod[iu] >= 1e-12))
