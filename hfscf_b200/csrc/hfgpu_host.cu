@@ -509,26 +509,56 @@ int build_quartets(hfgpu_handle* h) {
   }
   std::vector<int2> all((size_t)total);
   h->bucket_end.assign((size_t)hfgpu::kNumClasses * 4 * kBuckets, 0);
-  // phase 2: one stable counting sort per (class, segment) on (decade, count descending)
+  // phase 2: one stable counting sort per (class, segment) on (decade, count descending),
+  // itself parallel over the class's chunks: (a) per-chunk key histograms, (b) per (class,
+  // segment) the histograms become each chunk's first slot per key (keys in order, chunks in
+  // order inside a key), (c) every chunk scatters its quartets.
+  std::vector<int> seg_span((size_t)ncls * 4, 1);
+  for (int i = 0; i < ncls; ++i)
+    for (int sg = 0; sg < 4; ++sg) {
+      int maxprod = 0;
+      for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci) maxprod = std::max(maxprod, chunks[ci].maxprod[sg]);
+      seg_span[(size_t)i * 4 + sg] = maxprod + 1;
+    }
+  auto key_of = [&](int raw, int span) { return (raw / kProdSpan) * span + (span - 1 - raw % kProdSpan); };
+  std::vector<std::vector<long long>> slot(chunks.size() * 4);  // per (chunk, segment): next slot per key
+  run_parallel((int)chunks.size() * 4, [&](int task) {
+    const int ci = task / 4, sg = task % 4;
+    const ListChunk& c = chunks[ci];
+    if (c.key[sg].empty()) return;
+    const int span = seg_span[(size_t)c.cls * 4 + sg];
+    std::vector<long long>& hst = slot[task];
+    hst.assign((size_t)kBuckets * span, 0);
+    for (const int raw : c.key[sg]) ++hst[(size_t)key_of(raw, span)];
+  });
   run_parallel(ncls * 4, [&](int task) {
     const int i = task / 4, sg = task % 4;
     const int qc = quartet_class(cls[i].first, cls[i].second);
-    const long long base = seg_base[(size_t)i * 5 + sg];
-    int maxprod = 0;
-    for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci) maxprod = std::max(maxprod, chunks[ci].maxprod[sg]);
-    const int span = maxprod + 1;
+    const int span = seg_span[(size_t)task];
     const int nk = kBuckets * span;
-    auto key_of = [&](int raw) { return (raw / kProdSpan) * span + (maxprod - raw % kProdSpan); };
-    std::vector<long long> cnt((size_t)nk + 1, 0);
-    for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci)
-      for (const int raw : chunks[ci].key[sg]) ++cnt[(size_t)key_of(raw) + 1];
-    for (int k = 0; k < nk; ++k) cnt[(size_t)k + 1] += cnt[(size_t)k];  // cnt[k] = first slot of key k
-    for (int e = 0; e < kBuckets; ++e)
-      h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e] = base + cnt[(size_t)(e + 1) * span];
-    for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci) {
-      const ListChunk& c = chunks[ci];
-      for (size_t x = 0; x < c.q[sg].size(); ++x) all[(size_t)base + (size_t)cnt[(size_t)key_of(c.key[sg][x])]++] = c.q[sg][x];
+    long long next = seg_base[(size_t)i * 5 + sg];
+    for (int k = 0; k < nk; ++k) {
+      if (k % span == 0) {
+        const int e = k / span;  // decade e starts here; decade e-1 ends here
+        if (e > 0) h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + e - 1] = next;
+      }
+      for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci) {
+        std::vector<long long>& hst = slot[(size_t)ci * 4 + sg];
+        if (hst.empty()) continue;
+        const long long n = hst[(size_t)k];
+        hst[(size_t)k] = next;
+        next += n;
+      }
     }
+    h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + kBuckets - 1] = next;
+  });
+  run_parallel((int)chunks.size() * 4, [&](int task) {
+    const int ci = task / 4, sg = task % 4;
+    const ListChunk& c = chunks[ci];
+    if (c.key[sg].empty()) return;
+    const int span = seg_span[(size_t)c.cls * 4 + sg];
+    std::vector<long long>& nxt = slot[task];
+    for (size_t x = 0; x < c.q[sg].size(); ++x) all[(size_t)nxt[(size_t)key_of(c.key[sg][x], span)]++] = c.q[sg][x];
   });
   for (int i = 0; i < ncls; ++i) {
     const int qc = quartet_class(cls[i].first, cls[i].second);
