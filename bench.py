@@ -319,6 +319,7 @@ def run_ours(args, world, rank, local):
             "flops_per_build": total_flops, "build_ms": build_ms,
             "dominant_class": {"class": flopmodel.class_name(dom), "flop_share": flops_c[dom] / total_flops,
                                "event_ms_overlapped": class_ms[dom] / args.steps}}
+    eris_per_build = sum(flopmodel.class_integrals(c, class_work[c]["computed"], bs.pure) for c in range(E.NUM_CLASSES))
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sum(step_ms) / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometry)",
@@ -341,7 +342,13 @@ def run_ours(args, world, rank, local):
                     "mixed_grad_wall_s": grad_mx_wall,
                     "mixed_grad_max_abs_diff": float(np.max(np.abs(grad_mx - grad))),
                     "scf_plus_grad_ratio_fp64_over_mixed": (scf_wall + grad_wall) / (mixed_wall + grad_mx_wall)},
-            "check": {"max_abs_F_device_vs_api": err_f}}
+            "check": {"max_abs_F_device_vs_api": err_f},
+            # model-independent rates: contracted integrals (blocks x block size) per second of the
+            # timed builds, and whole RHF gradients (two-electron + one-electron + nuclear) per second
+            "throughput": {"eris_per_build": eris_per_build,
+                           "eris_per_s": eris_per_build / (build_ms * 1e-3),
+                           "gradients_per_s": 1.0 / grad_wall,
+                           "mixed_gradients_per_s": 1.0 / grad_mx_wall}}
     if not args.no_batch:
         # 512 seeded small molecules, SCF + gradient each, in one batched handle
         from hfscf_b200 import batch as BT

@@ -38,14 +38,23 @@ def _ops():
         return json.load(f)
 
 
+def class_block_size(cls_index: int, pure: bool) -> int:
+    """Integrals in one contracted block of the class in the final basis."""
+    la, lb, lc, ld = _ops()["eri"][cls_index]["class"]
+    if pure:
+        return (2 * la + 1) * (2 * lb + 1) * (2 * lc + 1) * (2 * ld + 1)
+    return ((la + 1) * (la + 2) // 2) * ((lb + 1) * (lb + 2) // 2) * ((lc + 1) * (lc + 2) // 2) * \
+        ((ld + 1) * (ld + 2) // 2)
+
+
+def class_integrals(cls_index: int, computed_quartets: int, pure: bool) -> int:
+    """Contracted integrals a launch computes (model-independent count: blocks x block size)."""
+    return int(computed_quartets) * class_block_size(cls_index, pure)
+
+
 def class_flops(cls_index: int, computed_quartets: int, prim_quartets: int, pure: bool) -> float:
     m = _ops()["eri"][cls_index]
-    la, lb, lc, ld = m["class"]
-    if pure:
-        nout = (2 * la + 1) * (2 * lb + 1) * (2 * lc + 1) * (2 * ld + 1)
-    else:
-        nout = ((la + 1) * (la + 2) // 2) * ((lb + 1) * (lb + 2) // 2) * ((lc + 1) * (lc + 2) // 2) * \
-            ((ld + 1) * (ld + 2) // 2)
+    nout = class_block_size(cls_index, pure)
     per_prim = m["prim_flops"] + c_boys(m["boys_m"])
     per_q = m["hrr_flops"] + (m["pure_flops"] if pure else 0) + C_DIG * nout
     return float(prim_quartets) * per_prim + float(computed_quartets) * per_q
