@@ -350,7 +350,7 @@ def run_ours(args, world, rank, local):
                            "gradients_per_s": 1.0 / grad_wall,
                            "mixed_gradients_per_s": 1.0 / grad_mx_wall}}
     if not args.no_batch:
-        # 512 seeded small molecules, SCF + gradient each, in one batched handle
+        # batched-mode workload: 512 seeded small molecules, SCF + gradient each, in one batched handle
         from hfscf_b200 import batch as BT
         from hfscf_b200 import molecules as MM
         from hfscf_b200 import dist as DI
