@@ -22,6 +22,26 @@ def test_default_options():
     o = E._Opts()
     assert E.lib().hfgpu_default_opts(ctypes.byref(o)) == 0
     assert o.schwarz_tol == 1e-12 and o.mixed_fp32_bound == 1e-4
+    assert o.density_tol == 1e-12 and o.mixed_density_tol == 1e-12
+    assert o.warp_max_quartets == 1 << 30 and o.grad_warp_max_waves == 48
+
+
+def test_flop_model_counts():
+    """The counting model of the roofline: block sizes in the final basis, FLOPs linear in the
+    computed quartets and primitive quartets, classes named in the order of hfgpu_class_stats."""
+    from hfscf_b200 import flopmodel as F
+    names = [F.class_name(c) for c in range(E.NUM_CLASSES)]
+    assert names[0] == "(ss|ss)" and names[-1] == "(dd|dd)" and len(set(names)) == E.NUM_CLASSES
+    assert F.class_block_size(E.NUM_CLASSES - 1, False) == 6 ** 4
+    assert F.class_block_size(E.NUM_CLASSES - 1, True) == 5 ** 4
+    assert F.class_block_size(0, False) == 1
+    assert F.class_integrals(E.NUM_CLASSES - 1, 7, True) == 7 * 625
+    for c in range(E.NUM_CLASSES):
+        f1 = F.class_flops(c, 10, 100, False)
+        assert F.class_flops(c, 20, 200, False) == pytest.approx(2 * f1)
+        assert F.class_flops(c, 0, 0, False) == 0.0
+        if c < 6:  # s and p only: the pure and Cartesian bases are the same
+            assert F.class_flops(c, 10, 100, True) == F.class_flops(c, 10, 100, False)
 
 
 def test_basis_sizes_of_the_workloads():
