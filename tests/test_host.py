@@ -196,3 +196,26 @@ def test_sad_atom_density_with_oracle_jk_holds_the_atom_electrons():
 
         D = scf.sad_atom_density(int(ab.Z[0]), S, T, V, jk)
         assert abs(np.sum(D * S) - ab.Z[0] / 2) < 1e-10
+
+
+def test_batched_layout_round_trip_and_padding():
+    """Block storage (molecule m: n_m x n_m at its offset) <-> padded [nmol, nmax, nmax]
+    matrices of the batched SCF: a round trip is exact, the padding is zero off the
+    diagonal and carries the fill value on it (it keeps padded orbitals out of the
+    occupied set)."""
+    import torch
+
+    from hfscf_b200.batch import _Layout
+    nbf = np.array([1, 4, 2])
+    off = np.concatenate([[0], np.cumsum(nbf * nbf)[:-1]])
+    lay = _Layout(nbf, off, torch.device("cpu"))
+    rng = np.random.default_rng(2)
+    blocks = torch.from_numpy(rng.normal(size=int((nbf * nbf).sum())))
+    P = lay.to_pad(blocks, fill_diag=7.0)
+    assert P.shape == (3, 4, 4)
+    assert torch.equal(lay.to_block(P), blocks)
+    for m, (n, o) in enumerate(zip(nbf, off)):
+        assert torch.equal(P[m, :n, :n].reshape(-1), blocks[o:o + n * n])
+        pad = P[m].clone()
+        pad[:n, :n] = 0.0
+        assert torch.equal(pad, torch.diag(torch.tensor([0.0] * n + [7.0] * (4 - n), dtype=pad.dtype)))
