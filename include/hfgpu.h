@@ -145,7 +145,8 @@ int hfgpu_grad2e_device_noalloc(hfgpu_handle* h, const double* DJ, double cJ, in
 long long hfgpu_noalloc_scratch_bytes(void);
 
 /* Batched handles: many independent molecules in one handle (hundreds of small molecules,
- * e.g. water clusters, methane, ethane and ammonia in STO-3G or 6-31G*).  No counterpart in the reference, which runs one molecule per process.
+ * e.g. water clusters, methane, ethane and ammonia in STO-3G or 6-31G*).  No counterpart in
+ * the reference, which runs one molecule per process.
  * Shell pairs and quartets are formed within each molecule only; every per-class kernel
  * launch covers all molecules.  Matrices live in a block storage: molecule m's n_m x n_m
  * row-major block starts at mat_off[m].  Molecules must be Cartesian (pure = 0); for s and
