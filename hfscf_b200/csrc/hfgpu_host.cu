@@ -423,13 +423,14 @@ struct ListChunk {
   int maxprod[4] = {0, 0, 0, 0};
 };
 
+// Runs f(0) ... f(ntask - 1) on up to max_threads threads (the caller's thread among them).
 template <typename F>
-void run_parallel(int ntask, F&& f) {
+void run_parallel(int ntask, int max_threads, F&& f) {
   std::atomic<int> next{0};
   auto work = [&]() {
     for (int i = next++; i < ntask; i = next++) f(i);
   };
-  const int nthr = std::max(1, std::min<int>(ntask, (int)std::max(1u, std::thread::hardware_concurrency())));
+  const int nthr = std::max(1, std::min(ntask, max_threads));
   std::vector<std::thread> pool;
   for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
   work();
@@ -454,6 +455,7 @@ int build_quartets(hfgpu_handle* h) {
   // chunks of consecutive bra pairs, about kListChunkWork candidates each
   std::vector<ListChunk> chunks;
   std::vector<int> cls_chunk0(ncls + 1, 0);
+  long long all_work = 0;  // candidate quartets of every class
   for (int i = 0; i < ncls; ++i) {
     const int cp = cls[i].first, cq = cls[i].second;
     cls_chunk0[i] = (int)chunks.size();
@@ -464,6 +466,7 @@ int build_quartets(hfgpu_handle* h) {
       int k0, ke;
       ket_range(cp, cq, P, k0, ke);
       work += std::max(0, ke - k0);
+      all_work += std::max(0, ke - k0);
       if (work >= kListChunkWork || P + 1 == pe) {
         ListChunk c;
         c.cls = i;
@@ -476,9 +479,11 @@ int build_quartets(hfgpu_handle* h) {
     }
   }
   cls_chunk0[ncls] = (int)chunks.size();
+  // small lists (fewer than two chunks' worth of candidates) are built on the calling thread
+  const int threads = all_work < 2 * kListChunkWork ? 1 : (int)std::max(1u, std::thread::hardware_concurrency());
   // phase 1: filter
   const double tol = h->opts.schwarz_tol, mix = h->opts.mixed_fp32_bound;
-  run_parallel((int)chunks.size(), [&](int ci) {
+  run_parallel((int)chunks.size(), threads, [&](int ci) {
     ListChunk& c = chunks[ci];
     const int cp = cls[c.cls].first, cq = cls[c.cls].second;
     for (int P = c.P0; P < c.P1; ++P) {
@@ -522,7 +527,7 @@ int build_quartets(hfgpu_handle* h) {
     }
   auto key_of = [&](int raw, int span) { return (raw / kProdSpan) * span + (span - 1 - raw % kProdSpan); };
   std::vector<std::vector<long long>> slot(chunks.size() * 4);  // per (chunk, segment): next slot per key
-  run_parallel((int)chunks.size() * 4, [&](int task) {
+  run_parallel((int)chunks.size() * 4, threads, [&](int task) {
     const int ci = task / 4, sg = task % 4;
     const ListChunk& c = chunks[ci];
     if (c.key[sg].empty()) return;
@@ -531,7 +536,7 @@ int build_quartets(hfgpu_handle* h) {
     hst.assign((size_t)kBuckets * span, 0);
     for (const int raw : c.key[sg]) ++hst[(size_t)key_of(raw, span)];
   });
-  run_parallel(ncls * 4, [&](int task) {
+  run_parallel(ncls * 4, threads, [&](int task) {
     const int i = task / 4, sg = task % 4;
     const int qc = quartet_class(cls[i].first, cls[i].second);
     const int span = seg_span[(size_t)task];
@@ -552,7 +557,7 @@ int build_quartets(hfgpu_handle* h) {
     }
     h->bucket_end[((size_t)qc * 4 + sg) * kBuckets + kBuckets - 1] = next;
   });
-  run_parallel((int)chunks.size() * 4, [&](int task) {
+  run_parallel((int)chunks.size() * 4, threads, [&](int task) {
     const int ci = task / 4, sg = task % 4;
     const ListChunk& c = chunks[ci];
     if (c.key[sg].empty()) return;
