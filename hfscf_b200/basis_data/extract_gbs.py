@@ -69,4 +69,8 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/basis")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HFSCF_BASIS_DIR")
+    if not src:
+        sys.exit("usage: extract_gbs.py BASIS_DIR  (the reference's basis/ folder of .gbs files; "
+                 "or set HFSCF_BASIS_DIR)")
+    main(src)

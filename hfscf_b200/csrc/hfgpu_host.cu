@@ -199,10 +199,27 @@ void normalise(int L, int np, const double* a, const double* c, double* out) {
   for (int j = 0; j < np; ++j) out[j] = c[j] * norm * std::pow(a[j], m2);
 }
 
-int set_device(hfgpu_handle* h) {
-  HF_CUDA(h, cudaSetDevice(h->device));
-  return HFGPU_OK;
-}
+// Makes the handle's device current for the duration of one entry point and restores the
+// caller's current device when the entry point returns (on every path).
+struct DeviceGuard {
+  int prev = -1;
+  int rc = HFGPU_OK;
+  explicit DeviceGuard(hfgpu_handle* h) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      (void)cudaGetLastError();
+      prev = -1;
+    }
+    if (prev != h->device) {
+      const cudaError_t e = cudaSetDevice(h->device);
+      if (e != cudaSuccess) rc = cuda_fail(h, e, "cudaSetDevice");
+    }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
 
 // Primitive pairs of every canonical shell pair; pairs sorted by class, then by
 // primitive count (descending) so that quartet lists group equal loop lengths.
@@ -1002,7 +1019,8 @@ int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int n
                              double* grad, int precision, void* scratch, size_t scratch_bytes) {
   if (!h || !grad || !scratch) return HFGPU_ERR_INVALID;
   if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   GradArgs<double> gd{};
   gd.pairs = h->d_pairs.as<PairInfo>();
@@ -1032,27 +1050,45 @@ int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int n
   gf.mol_n = gd.mol_n;
   gd.smem_atoms = gf.smem_atoms = grad_smem_atoms(h);
   const int2* q = h->d_quart.as<int2>();
+  // quartet range of part 0 / 1 of class c (FP64 and, in mixed mode, the FP32 low-bound part)
+  auto part_range = [&](int c, int part, long long& lo, long long& hi) {
+    const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
+    lo = (precision == HFGPU_MIXED) ? (part == 0 ? b : m) : (part == 0 ? b : e);
+    hi = (precision == HFGPU_MIXED) ? (part == 0 ? m : e) : e;
+  };
+  // First pass: every table-mode launch must fit one 128-thread block into the scratch.
+  // Checked before anything is enqueued, so that a rejected call leaves grad untouched.
+  for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
+    const int slots = hfgpu::kClassLaunchers[c]->grad_scratch_slots(h->pure);
+    if (slots <= 0) continue;
+    for (int part = 0; part < 2; ++part) {
+      long long lo, hi;
+      part_range(c, part, lo, hi);
+      if (hi <= lo) continue;
+      const bool fp32 = precision == HFGPU_MIXED && part == 1;
+      const size_t per_thread = (size_t)slots * (fp32 ? sizeof(float) : sizeof(double));
+      if (scratch_bytes / per_thread < 128)
+        return fail(h, HFGPU_ERR_INVALID,
+                    "gradient class needs " + std::to_string(per_thread * 128) +
+                        " bytes of scratch for one 128-thread block, more than the fixed scratch of " +
+                        std::to_string(scratch_bytes) + " bytes");
+    }
+  }
   for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
-    const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
-    if (e <= b) continue;
+    if (h->q_end[c] <= h->q_beg[c]) continue;
     const int slots = L->grad_scratch_slots(h->pure);
     for (int part = 0; part < 2; ++part) {
       const bool fp32 = precision == HFGPU_MIXED && part == 1;
-      const long long lo = (precision == HFGPU_MIXED) ? (part == 0 ? b : m) : (part == 0 ? b : e);
-      const long long hi = (precision == HFGPU_MIXED) ? (part == 0 ? m : e) : e;
+      long long lo, hi;
+      part_range(c, part, lo, hi);
       const int nq = (int)(hi - lo);
       if (nq <= 0) continue;
       int grid = (nq + 127) / 128;
       if (slots == 0 && gd.smem_atoms > 0) grid = std::min(grid, kGradMaxBlocks);
       if (slots > 0) {
         const size_t per_thread = (size_t)slots * (fp32 ? sizeof(float) : sizeof(double));
-        const long long fit = (long long)(scratch_bytes / per_thread) / 128 * 128;
-        if (fit < 128)
-          return fail(h, HFGPU_ERR_INVALID,
-                      "gradient class needs " + std::to_string(per_thread * 128) +
-                          " bytes of scratch for one 128-thread block, more than the fixed scratch of " +
-                          std::to_string(scratch_bytes) + " bytes");
+        const long long fit = (long long)(scratch_bytes / per_thread) / 128 * 128;  // >= 128 (first pass)
         grid = (int)(std::min<long long>(fit, (long long)grid * 128) / 128);
       }
       if (fp32) {
@@ -1069,6 +1105,13 @@ int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int n
 }
 
 int hfgpu_device_of(const hfgpu_handle* h) { return h ? h->device : -1; }
+
+// Records a CUDA failure on the handle (status and hfgpu_last_error message) and clears the
+// runtime's sticky last error, so that a later launch check on any handle does not report it.
+int hfgpu_cuda_error(hfgpu_handle* h, int cuda_code, const char* where) {
+  (void)cudaGetLastError();
+  return cuda_fail(h, static_cast<cudaError_t>(cuda_code), where);
+}
 
 extern "C" {
 
@@ -1139,7 +1182,8 @@ int hfgpu_create(const hfgpu_basis* b, const hfgpu_opts* opts, hfgpu_handle** ou
   h->mol_off = {0};
   h->mol_atom = {0, b->natoms};
   h->mat_total = (long long)h->n * h->n;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) {
     delete h;
     return rc;
@@ -1163,8 +1207,9 @@ int hfgpu_create(const hfgpu_basis* b, const hfgpu_opts* opts, hfgpu_handle** ou
 
 int hfgpu_destroy(hfgpu_handle* h) {
   if (!h) return HFGPU_OK;
-  cudaSetDevice(h->device);
-  if (h->stream) cudaStreamSynchronize(h->stream);
+  {
+    DeviceGuard dev_guard(h);
+    if (h->stream) cudaStreamSynchronize(h->stream);
   for (DevBuf* d : {&h->d_onee, &h->d_pairs, &h->d_prim_d, &h->d_prim_f, &h->d_alpha_d, &h->d_alpha_f, &h->d_boys_d, &h->d_boys_f,
                     &h->d_quart, &h->d_mats, &h->d_half, &h->d_dmax, &h->d_counters, &h->d_grad, &h->d_scratch,
                     &h->d_eri, &h->d_eriq})
@@ -1178,6 +1223,7 @@ int hfgpu_destroy(hfgpu_handle* h) {
   }
   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  }  // the caller's current device is restored here, before the handle goes
   delete h;
   return HFGPU_OK;
 }
@@ -1201,7 +1247,8 @@ int hfgpu_set_geometry(hfgpu_handle* h, const double* xyz, int natoms) {
   if (!h || !xyz || natoms != h->natoms) return fail(h, HFGPU_ERR_INVALID, "bad geometry arguments");
   for (int i = 0; i < 3 * natoms; ++i)
     if (!std::isfinite(xyz[i])) return fail(h, HFGPU_ERR_INVALID, "non-finite coordinate");
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   h->xyz.assign(xyz, xyz + 3 * natoms);
   h->have_geometry = false;
@@ -1234,7 +1281,8 @@ int hfgpu_eri_packed(hfgpu_handle* h, double* eri_out, long long eri_len) {
   if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
   const long long n = h->n, len = n * (n + 1) * (n * n + n + 2) / 8;
   if (eri_len != len) return fail(h, HFGPU_ERR_INVALID, "eri_len must be n(n+1)(n^2+n+2)/8");
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   HF_CUDA(h, h->d_eri.ensure(sizeof(double) * len));
   HF_CUDA(h, cudaMemsetAsync(h->d_eri.p, 0, sizeof(double) * len, h->stream));
@@ -1266,14 +1314,16 @@ int hfgpu_eri_packed(hfgpu_handle* h, double* eri_out, long long eri_len) {
 
 int hfgpu_jk_device(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* J, double* K, int precision) {
   if (!h) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   return jk_device_impl(h, DJ, nK, DK, J, K, precision);
 }
 
 int hfgpu_jk(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* J, double* K, int precision) {
   if (!h || (nK > 0 && (!DK || !K)) || (DJ && !J)) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   const size_t nn = (size_t)h->n * h->n;
   // device layout: [DJ | DK (nK) | J | K (nK)]
@@ -1303,7 +1353,8 @@ int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* ski
 
 int hfgpu_fock_rhf(hfgpu_handle* h, const double* D, const double* H, double* F, int precision) {
   if (!h || !D || !H || !F) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   const size_t nn = (size_t)h->n * h->n;
   // device layout: [D | H | J | K]; only D and H go up, only F comes back
@@ -1344,7 +1395,8 @@ int hfgpu_fock_uhf(hfgpu_handle* h, const double* Da, const double* Db, const do
 
 int hfgpu_fock_delta(hfgpu_handle* h, const double* dD, double* F, int precision) {
   if (!h || !dD || !F) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   const size_t nn = (size_t)h->n * h->n;
   // same device layout as hfgpu_fock_rhf, with F_in in place of H
@@ -1379,14 +1431,16 @@ int hfgpu_energy_forward(hfgpu_handle* h, const double* D, double* E2, int preci
 int hfgpu_grad2e_device(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
                         double* grad, int precision) {
   if (!h || !grad) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   return grad_device_impl(h, DJ, cJ, nK, DK, cK, grad, precision);
 }
 
 static int grad_host(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* const* DKs, double cK,
                      double scale, double* dE_dR, int precision) {
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   const size_t nn = (size_t)h->n * h->n;
   HF_CUDA(h, h->d_mats.ensure(sizeof(double) * nn * (1 + nK)));
@@ -1522,7 +1576,8 @@ static int onee_setup(hfgpu_handle* h, const double* Z, onee::Args& a, long long
 
 int hfgpu_one_electron_device(hfgpu_handle* h, const double* Z, double* S, double* T, double* V) {
   if (!h || !Z || !S || !T || !V) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   onee::Args a;
   long long nitems = 0;
@@ -1539,7 +1594,8 @@ int hfgpu_one_electron_device(hfgpu_handle* h, const double* Z, double* S, doubl
 int hfgpu_one_electron_grad_device(hfgpu_handle* h, const double* Z, const double* D, const double* W, double cH,
                                    double cS, double* grad) {
   if (!h || !Z || !D || !W || !grad) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   onee::Args a;
   long long nitems = 0;
@@ -1556,7 +1612,8 @@ int hfgpu_batch_eigh(hfgpu_handle* h, const double* A, double* W, double* V, int
   if (!h->batched) return fail(h, HFGPU_ERR_UNSUPPORTED, "hfgpu_batch_eigh needs a batched handle");
   const int nmax = h->n;
   if (nmax > kJacobiMaxN) return fail(h, HFGPU_ERR_UNSUPPORTED, "batched eigensolver: a molecule has more than 118 functions");
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   const size_t smem = jacobi_smem_bytes(nmax);
   HF_CUDA(h, cudaFuncSetAttribute(batch_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1568,7 +1625,8 @@ int hfgpu_batch_eigh(hfgpu_handle* h, const double* A, double* W, double* V, int
 
 int hfgpu_set_timing(hfgpu_handle* h, int on) {
   if (!h) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   if (on && !h->ev[0])
     for (auto& e : h->ev) HF_CUDA(h, cudaEventCreate(&e));
@@ -1644,7 +1702,8 @@ int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule) {
 // and the given density, one class at a time on the handle's stream, and keeps the fastest.
 int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule) {
   if (!h || !D) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
   repeats = std::max(1, std::min(repeats, 100));
@@ -1790,6 +1849,14 @@ int hfgpu_last_launches(const hfgpu_handle* h, int* kernels) {
 
 int hfgpu_fp64_peak(int device, double* tflops) {
   if (!tflops) return HFGPU_ERR_INVALID;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  struct Restore {
+    int d;
+    ~Restore() {
+      if (d >= 0) cudaSetDevice(d);
+    }
+  } restore{prev};
   if (cudaSetDevice(device) != cudaSuccess) return HFGPU_ERR_CUDA;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -1901,14 +1968,16 @@ int hfgpu_batch_layout(const hfgpu_handle* h, int* nbf, long long* mat_off, long
 
 int hfgpu_batch_jk_device(hfgpu_handle* h, const double* D, double* J, double* K, int precision) {
   if (!h || !D || !J || !K) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   return jk_device_impl(h, D, 1, D, J, K, precision);
 }
 
 int hfgpu_batch_grad2e_device(hfgpu_handle* h, const double* D, double* grad, int precision) {
   if (!h || !D || !grad) return HFGPU_ERR_INVALID;
-  int rc = set_device(h);
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
   if (rc) return rc;
   return grad_device_impl(h, D, 2.0, 1, D, 1.0, grad, precision);
 }

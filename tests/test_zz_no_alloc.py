@@ -15,7 +15,8 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-10  # the two-electron gradient tolerance used by the other parity tests
+TOL = 1e-10  # the FP64 two-electron gradient tolerance used by the other parity tests
+TOL_MIXED = 1e-6  # the mixed-precision gradient tolerance of the launch-form tests
 
 
 def _case(workload, pure=None):
@@ -29,18 +30,21 @@ def _case(workload, pure=None):
     return B.build_basis(name, Z, x, pure=p if pure is None else pure)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("case", ["water-octamer-6-31g*", "methane-cc-pvdz"])
-def test_noalloc_gradient_matches_allocating_entry_point_on_two_calls(case):
+def test_noalloc_gradient_matches_allocating_entry_point_on_two_calls(case, precision):
+    """Two calls in a row against hfgpu_grad2e_device at the same precision.  In mixed
+    precision the FP32 part of every table-mode class reuses the same array as floats."""
     import torch
 
     from hfscf_b200 import engine as E
     bs = _case(4) if case.startswith("water") else _case("ch4")
+    prec, tol = (E.FP64, TOL) if precision == "fp64" else (E.MIXED, TOL_MIXED)
     n = bs.nbf
     rng = np.random.default_rng(21)
     A = rng.normal(size=(n, n))
     D = (A + A.T) / n
     lib = E.lib()
-    assert lib.hfgpu_noalloc_scratch_bytes.restype is not None or True
     lib.hfgpu_noalloc_scratch_bytes.restype = ctypes.c_longlong
     assert lib.hfgpu_noalloc_scratch_bytes() == 32 << 20
     with E.Engine(bs, device=0) as eng:
@@ -48,7 +52,7 @@ def test_noalloc_gradient_matches_allocating_entry_point_on_two_calls(case):
         Dd = torch.from_numpy(D).to(dev)
         ref = torch.zeros((bs.natoms, 3), dtype=torch.float64, device=dev)
         torch.cuda.synchronize()
-        eng.grad2e_device(Dd.data_ptr(), 2.0, 1, Dd.data_ptr(), 1.0, ref.data_ptr())
+        eng.grad2e_device(Dd.data_ptr(), 2.0, 1, Dd.data_ptr(), 1.0, ref.data_ptr(), prec)
         torch.cuda.synchronize()
         g_ref = ref.cpu().numpy()
         for _ in range(2):
@@ -57,10 +61,11 @@ def test_noalloc_gradient_matches_allocating_entry_point_on_two_calls(case):
             rc = lib.hfgpu_grad2e_device_noalloc(eng.h, ctypes.c_void_p(Dd.data_ptr()), ctypes.c_double(2.0),
                                                  ctypes.c_int(1), ctypes.c_void_p(Dd.data_ptr()),
                                                  ctypes.c_double(1.0), ctypes.c_void_p(out.data_ptr()),
-                                                 ctypes.c_int(E.FP64))
+                                                 ctypes.c_int(prec))
             assert rc == 0, lib.hfgpu_last_error(eng.h)
             torch.cuda.synchronize()
-            assert np.max(np.abs(out.cpu().numpy() - g_ref)) < TOL
+            assert np.max(np.abs(out.cpu().numpy() - g_ref)) < tol
+        assert torch.cuda.current_device() == 0
 
 
 def test_noalloc_gradient_of_a_batched_handle():
