@@ -659,6 +659,42 @@ __global__ void fock_combine_kernel(double* F, const double* __restrict__ H, con
   if (i < tot) F[i] = H[i] + 2.0 * J[i] - K[i];
 }
 
+// F_0 .. F_M at count points T through the engine's own Boys evaluation (BoysTable::eval, the
+// routine every quartet kernel calls), F[i * (M + 1) + m], for the direct Boys tests.
+template <typename R, int M>
+__global__ void boys_eval_kernel(BoysTable<R> bt, const double* __restrict__ T, long long count,
+                                 double* __restrict__ F) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  R f[M + 1];
+  bt.template eval<M>(R(T[i]), R(1), f);
+#pragma unroll
+  for (int m = 0; m <= M; ++m) F[i * (M + 1) + m] = double(f[m]);
+}
+
+template <typename R, int M>
+void launch_boys_eval(const R* tab, const double* T, long long count, double* F, cudaStream_t st) {
+  BoysTable<R> bt{tab};
+  boys_eval_kernel<R, M><<<(unsigned)((count + 127) / 128), 128, 0, st>>>(bt, T, count, F);
+}
+
+template <typename R>
+void boys_eval_dispatch(int m, const R* tab, const double* T, long long count, double* F, cudaStream_t st) {
+  switch (m) {
+    case 0: launch_boys_eval<R, 0>(tab, T, count, F, st); break;
+    case 1: launch_boys_eval<R, 1>(tab, T, count, F, st); break;
+    case 2: launch_boys_eval<R, 2>(tab, T, count, F, st); break;
+    case 3: launch_boys_eval<R, 3>(tab, T, count, F, st); break;
+    case 4: launch_boys_eval<R, 4>(tab, T, count, F, st); break;
+    case 5: launch_boys_eval<R, 5>(tab, T, count, F, st); break;
+    case 6: launch_boys_eval<R, 6>(tab, T, count, F, st); break;
+    case 7: launch_boys_eval<R, 7>(tab, T, count, F, st); break;
+    case 8: launch_boys_eval<R, 8>(tab, T, count, F, st); break;
+    case 9: launch_boys_eval<R, 9>(tab, T, count, F, st); break;
+    default: launch_boys_eval<R, 10>(tab, T, count, F, st); break;
+  }
+}
+
 // FP64 FMA throughput probe: 8 independent FMA chains per thread.
 __global__ void fp64_peak_kernel(double* out, int iters, double a, double b) {
   double x[8];
@@ -1845,6 +1881,35 @@ int hfgpu_last_launches(const hfgpu_handle* h, int* kernels) {
   if (!h || !kernels) return HFGPU_ERR_INVALID;
   *kernels = h->last_kernels;
   return HFGPU_OK;
+}
+
+int hfgpu_boys(hfgpu_handle* h, int precision, int m, const double* T, long long count, double* F) {
+  if (!h || !T || !F || count < 0 || m < 0 || m > BOYS_MMAX) return fail(h, HFGPU_ERR_INVALID, "bad Boys arguments");
+  if (precision != HFGPU_FP64 && precision != HFGPU_MIXED) return fail(h, HFGPU_ERR_INVALID, "bad precision");
+  for (long long i = 0; i < count; ++i)
+    if (!(T[i] >= 0.0) || !std::isfinite(T[i])) return fail(h, HFGPU_ERR_INVALID, "T must be finite and >= 0");
+  if (count == 0) return HFGPU_OK;
+  DeviceGuard dev_guard(h);
+  if (dev_guard.rc) return dev_guard.rc;
+  DevBuf buf;
+  const size_t nT = sizeof(double) * (size_t)count, nF = sizeof(double) * (size_t)count * (m + 1);
+  HF_CUDA(h, buf.ensure(nT + nF));
+  double* dT = buf.as<double>();
+  double* dF = dT + count;
+  int rc = HFGPU_OK;
+  cudaError_t e = cudaMemcpyAsync(dT, T, nT, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    if (precision == HFGPU_FP64)
+      boys_eval_dispatch<double>(m, h->d_boys_d.as<double>(), dT, count, dF, h->stream);
+    else
+      boys_eval_dispatch<float>(m, h->d_boys_f.as<float>(), dT, count, dF, h->stream);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(F, dF, nF, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) rc = cuda_fail(h, e, "Boys evaluation");
+  buf.release();
+  return rc;
 }
 
 int hfgpu_fp64_peak(int device, double* tflops) {

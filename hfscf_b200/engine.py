@@ -148,6 +148,15 @@ class Engine:
         self._check(lib().hfgpu_schwarz(self.h, _p(Q)))
         return Q
 
+    def boys(self, m, T, precision=FP64) -> np.ndarray:
+        """F_0..F_m at the points T through the engine's Boys evaluation (hfgpu_boys):
+        shape (len(T), m + 1)."""
+        T = _c(np.atleast_1d(T))
+        F = np.zeros((len(T), m + 1))
+        self._check(lib().hfgpu_boys(self.h, ctypes.c_int(precision), ctypes.c_int(m), _p(T),
+                                     ctypes.c_longlong(len(T)), _p(F)))
+        return F
+
     def eri_packed(self) -> np.ndarray:
         n = self.n
         ln = n * (n + 1) * (n * n + n + 2) // 8

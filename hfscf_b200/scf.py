@@ -421,9 +421,13 @@ def rhf_gradient(basis: Basis, res: ScfResult, engine, precision=eng.FP64):
     return g
 
 
-def uhf(basis: Basis, engine, *, multiplicity=1, e_tol=1e-10, rms_tol=1e-8, max_iter=100, precision=eng.FP64):
-    """Unrestricted HF with the GPU UHF Fock build (src/scfsolver/hfscf_uhf_solver.cpp:155-191),
-    DIIS on the stacked alpha/beta errors."""
+def uhf(basis: Basis, engine, *, multiplicity=1, e_tol=1e-10, rms_tol=1e-8, diis_range=5, max_iter=100,
+        precision=eng.FP64):
+    """Unrestricted HF with the GPU UHF Fock build, as Mol::uhf_solver runs it
+    (src/scfsolver/hfscf_uhf_solver.cpp:155-225): F_a = H + J[Da+Db] - K[Da] from the engine,
+    two-spin DIIS (DiisUhf, the reference's diis_extrapolate for UHF), core guess without
+    HOMO/LUMO mixing (the default), energy 1/2 sum[Da (H + Fa) + Db (H + Fb)], converged when
+    both spins' rms and |dE| are below the tolerances."""
     nel = int(np.sum(basis.Z))
     na = (nel + multiplicity - 1) // 2
     nb = nel - na
@@ -433,40 +437,21 @@ def uhf(basis: Basis, engine, *, multiplicity=1, e_tol=1e-10, rms_tol=1e-8, max_
     eps, Cp = np.linalg.eigh(X.T @ H @ X)
     C = X @ Cp
     Da, Db = C[:, :na] @ C[:, :na].T, C[:, :nb] @ C[:, :nb].T
-    E = 0.5 * float(np.sum((Da + Db) * (H + H)))
-    hist_F, hist_E = [], []
+    E = float(np.sum(Da * (H + H)))
+    diis = DiisUhf(diis_range)
     it = 0
     converged = False
     while True:
         it += 1
         Fa, Fb = engine.fock_uhf(Da, Db, H, precision)
-        ea = X.T @ (Fa @ Da @ S - S @ Da @ Fa) @ X
-        eb = X.T @ (Fb @ Db @ S - S @ Db @ Fb) @ X
-        rms = 0.5 * (np.sqrt(np.mean(ea ** 2)) + np.sqrt(np.mean(eb ** 2)))
-        hist_F.append((Fa.copy(), Fb.copy()))
-        hist_E.append(np.concatenate([ea.ravel(), eb.ravel()]))
-        if len(hist_F) > 6:
-            hist_F.pop(0)
-            hist_E.pop(0)
-        if len(hist_F) > 1:
-            m = len(hist_F)
-            B = -np.ones((m + 1, m + 1))
-            B[m, m] = 0
-            for i in range(m):
-                for j in range(m):
-                    B[i, j] = hist_E[i] @ hist_E[j]
-            rhs = np.zeros(m + 1)
-            rhs[m] = -1
-            c = np.linalg.solve(B, rhs)
-            Fa = sum(c[k] * hist_F[k][0] for k in range(m))
-            Fb = sum(c[k] * hist_F[k][1] for k in range(m))
+        Fa, Fb = diis.extrapolate(Fa, Fb, S, Da, Db, X)
         _, Ca = np.linalg.eigh(X.T @ Fa @ X)
         _, Cb = np.linalg.eigh(X.T @ Fb @ X)
         Ca, Cb = X @ Ca, X @ Cb
         Da, Db = Ca[:, :na] @ Ca[:, :na].T, Cb[:, :nb] @ Cb[:, :nb].T
         E_prev = E
-        E = 0.5 * float(np.sum((Da + Db) * H + Da * Fa + Db * Fb))
-        if rms < rms_tol and abs(E - E_prev) < e_tol:
+        E = 0.5 * float(np.sum(Da * (H + Fa)) + np.sum(Db * (H + Fb)))
+        if diis.rms_a < rms_tol and diis.rms_b < rms_tol and abs(E - E_prev) < e_tol:
             converged = True
             break
         if it >= max_iter:

@@ -207,6 +207,12 @@ int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out);
 int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms);
 int hfgpu_last_launches(const hfgpu_handle* h, int* kernels);
 int hfgpu_fp64_peak(int device, double* tflops);
+/* Boys function F_0..F_m (m <= 10) at count points T >= 0 (host arrays; F is count x (m+1)),
+ * through the same table and evaluation the quartet kernels use, in FP64 (HFGPU_FP64) or in
+ * the FP32 form of the mixed-precision kernels (HFGPU_MIXED; T is rounded to float first).
+ * The reference's counterpart is extramath::F_nu (src/math/gamma.cpp:18-24), which evaluates
+ * T < 1e-8 at T = 1e-8; this routine does not clamp. */
+int hfgpu_boys(hfgpu_handle* h, int precision, int m, const double* T, long long count, double* F);
 int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
 
 /* Launch schedule of the J/K build (no reference counterpart: the reference has one CPU

@@ -135,6 +135,18 @@ def jk(eri, D):
     return J, K
 
 
+def jk_packed(eri, Ds):
+    """J[D_m], K[D_m] for a list of densities, from the packed ERI vector in one pass over the
+    unique integrals (or_jk_packed): the sums of or_jk, fast enough for N = 250."""
+    Ds = [np.ascontiguousarray(D, dtype=np.float64) for D in Ds]
+    n = Ds[0].shape[0]
+    Dst = np.ascontiguousarray(np.stack(Ds))
+    J, K = np.zeros_like(Dst), np.zeros_like(Dst)
+    rc = lib().or_jk_packed(ctypes.c_longlong(n), _p(eri), ctypes.c_int(len(Ds)), _p(Dst), _p(J), _p(K))
+    assert rc == 0
+    return J, K
+
+
 def grad2e(basis, DJ, cJ, DKs, cK) -> np.ndarray:
     args, keep = _flat(basis)
     sa = keep["atom"]
@@ -201,6 +213,19 @@ def ref_onee_grad(basis, D, Q, cD=2.0, cQ=-2.0) -> np.ndarray:
     return g
 
 
+def ref_screen_diagonal(basis, cutoff=1e-14) -> np.ndarray:
+    """(pq|pq) over Cartesian functions as the reference's Schwarz screen matrix holds it
+    (Erios::compute_screen_matrix, src/integrals/hfscf_oseri_screen.cpp:22-181); entries of
+    shell pairs that the reference's block test skips are -1.  Cartesian bases only."""
+    assert not basis.pure
+    args, keep = _flat(basis)
+    n = basis.nbf
+    out = np.zeros((n, n))
+    rc = ref().hfref_screen_diagonal(*args[:6], ctypes.c_double(cutoff), _p(out))
+    assert rc == 0
+    return out
+
+
 def ref_boys(m, T) -> float:
     return ref().hfref_boys(float(m), float(T))
 
@@ -232,6 +257,21 @@ def unpack(packed, n) -> np.ndarray:
     r = np.arange(n)
     i, j, k, l = np.meshgrid(r, r, r, r, indexing="ij")
     return packed[index_ijkl(i, j, k, l)]
+
+
+def grad2e_packed_deriv1(deriv9, bf_atom, natoms, DJ, cJ, DKs, cK) -> np.ndarray:
+    """Two-electron gradient from the reference's nine packed derivative tensors in one pass
+    over the unique slots (or_grad2e_from_deriv1, C); RHF: DJ = D, cJ = 2, DKs = [D], cK = 1."""
+    n = DJ.shape[0]
+    d9 = np.ascontiguousarray(deriv9, dtype=np.float64)
+    at = np.ascontiguousarray(bf_atom, dtype=np.int32)
+    DK = np.ascontiguousarray(np.stack(DKs)) if len(DKs) else np.zeros((0,))
+    g = np.zeros((natoms, 3))
+    rc = lib().or_grad2e_from_deriv1(ctypes.c_longlong(n), _p(d9), _p(at, ctypes.c_int), ctypes.c_int(natoms),
+                                     _p(np.ascontiguousarray(DJ)), ctypes.c_double(cJ), ctypes.c_int(len(DKs)),
+                                     _p(DK), ctypes.c_double(cK), _p(g))
+    assert rc == 0
+    return g
 
 
 def grad2e_from_deriv1(deriv9, bf_atom, natoms, D) -> np.ndarray:

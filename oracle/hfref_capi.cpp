@@ -131,6 +131,35 @@ int hfref_eri_packed(int nshell, const int* L, const double* xyz, const int* npr
   return 0;
 }
 
+// The reference's Schwarz diagonal (pq|pq) over Cartesian functions, as its screen matrix
+// holds it.  Erios::init_screen and Erios::compute_screen_matrix over the shell pairs i <= j
+// (as create_repulsion_matrix calls them, src/scfsolver/hfscf_hf_hamiltonian.cpp:77-89), then
+// compute_contracted_shell_quartet(eri, s_ij, s_ij, do_screen = true) for every diagonal
+// shell quartet: with screening on, a Cartesian basis stores screen(p, q) into the slot of
+// (pq|pq) (src/integrals/hfscf_oseri.cpp:214-218), and the matrix itself is private.
+// out: ncart x ncart, row-major; entries of shell pairs whose whole block the reference's
+// block test skips (src/integrals/hfscf_oseri.cpp:36-46) are left at -1.
+int hfref_screen_diagonal(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
+                          const double* coef, double cutoff, double* out) {
+  auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, 0);
+  const Eigen::Index n = b->ncart;
+  const Eigen::Index len = n * (n + 1) * (n * n + n + 2) / 8;
+  EigenVector<double> eri(len);
+  for (Eigen::Index p = 0; p < len; ++p) eri(p) = -1.0;
+  ERIOS::Erios os(false, cutoff);
+  os.init_screen(n);
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < nshell; ++i)
+    for (int j = i; j < nshell; ++j) os.compute_screen_matrix(b->pairs[i * nshell + j]);
+#pragma omp parallel for schedule(dynamic)
+  for (int i = 0; i < nshell; ++i)
+    for (int j = i; j < nshell; ++j)
+      os.compute_contracted_shell_quartet(eri, b->pairs[i * nshell + j], b->pairs[i * nshell + j], true);
+  for (Eigen::Index p = 0; p < n; ++p)
+    for (Eigen::Index q = 0; q < n; ++q) out[p * n + q] = eri(hfscfmath::index_ijkl(p, q, p, q));
+  return 0;
+}
+
 // Nine packed derivative-ERI tensors (d/dXa, d/dXb, d/dXc, d/dYa, ..., d/dZc), each
 // of the packed 8-fold length, from Erios::compute_contracted_shell_quartet_deriv1.
 // coords[3] selects the Cartesian directions, as the reference's out_of_plane mask.

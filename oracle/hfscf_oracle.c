@@ -585,3 +585,115 @@ int or_grad2e(int nshell, const int* L, const double* xyz, const int* nprim, con
   or_basis_free(&b);
   return 0;
 }
+
+/* J[D_m] and K[D_m] for nd densities from the packed 8-fold ERI vector, visiting each
+ * unique integral once.  The same sums as the contraction of Mol::hf_solver::update_fock_matrix
+ * (src/scfsolver/hfscf_hf_solver.cpp:261-278): J_ij = sum_kl D_kl (ij|kl), K_ij = sum_kl D_kl (ik|jl),
+ * written as a scatter over the eight index images of (ij|kl) (i >= j, k >= l, ij >= kl) with
+ * each image weighted by 1 / (number of coinciding images), so that an N = 250 basis takes
+ * seconds instead of the N^4 gathers of the row-by-row form (or_jk, or_fock_rhf).
+ * Densities need not be symmetric; J and K are n x n, row-major. */
+int or_jk_packed(long long n, const double* eri, int nd, const double* D, double* J, double* K) {
+  const long long nn = n * n;
+  memset(J, 0, sizeof(double) * nn * nd);
+  memset(K, 0, sizeof(double) * nn * nd);
+#pragma omp parallel
+  {
+    double* Jt = (double*)calloc((size_t)(nn * nd), sizeof(double));
+    double* Kt = (double*)calloc((size_t)(nn * nd), sizeof(double));
+#pragma omp for schedule(dynamic, 1)
+    for (long long i = n - 1; i >= 0; --i)
+      for (long long j = 0; j <= i; ++j) {
+        const long long ij = i * (i + 1) / 2 + j;
+        for (long long k = 0; k <= i; ++k)
+          for (long long l = 0; l <= k; ++l) {
+            const long long kl = k * (k + 1) / 2 + l;
+            if (kl > ij) break;
+            const double v0 = eri[ij * (ij + 1) / 2 + kl];
+            if (v0 == 0.0) continue;
+            double w = v0;
+            if (i == j) w *= 0.5;
+            if (k == l) w *= 0.5;
+            if (ij == kl) w *= 0.5;
+            /* the eight images (p q | r s) of (i j | k l) */
+            const long long im[8][4] = {{i, j, k, l}, {j, i, k, l}, {i, j, l, k}, {j, i, l, k},
+                                        {k, l, i, j}, {l, k, i, j}, {k, l, j, i}, {l, k, j, i}};
+            for (int m = 0; m < nd; ++m) {
+              const double* Dm = D + m * nn;
+              double* Jm = Jt + m * nn;
+              double* Km = Kt + m * nn;
+              for (int x = 0; x < 8; ++x) {
+                const long long p = im[x][0], q = im[x][1], r = im[x][2], t = im[x][3];
+                Jm[p * n + q] += w * Dm[r * n + t];
+                Km[p * n + r] += w * Dm[q * n + t];
+              }
+            }
+          }
+      }
+#pragma omp critical
+    for (long long x = 0; x < nn * nd; ++x) {
+      J[x] += Jt[x];
+      K[x] += Kt[x];
+    }
+    free(Jt);
+    free(Kt);
+  }
+  return 0;
+}
+
+/* Two-electron gradient from the reference's nine packed first-derivative tensors
+ * (d/dXa, d/dXb, d/dXc, d/dYa, ..., d/dZc, each of the packed 8-fold length, from
+ * Erios::compute_contracted_shell_quartet_deriv1).  Restates the dV/dX assembly of
+ * Mol::scf_gradient::calc_coulomb_exchange_integrals (src/gradient/hfscf_grad_ints.cpp:79-108:
+ * over canonical slots i >= j, k >= l, ij <= kl, the derivative belongs to the atom of function
+ * i (A), j (B), k (C), and -(A + B + C) to the atom of l) and the contraction of
+ * calc_scf_gradient_rhf (src/gradient/hfscf_grad_rhf.cpp:121-141), summed over all atoms at
+ * once: every slot carries the sum, over its distinct index images (pq|rs), of
+ * cJ DJ_pq DJ_rs - cK sum_m DK_m,pr DK_m,qs (RHF: cJ = 2, DK = {D}, cK = 1). */
+int or_grad2e_from_deriv1(long long n, const double* deriv9, const int* bf_atom, int natoms, const double* DJ,
+                          double cJ, int nK, const double* DK, double cK, double* grad) {
+  const long long len = or_packed_len(n);
+  const long long nn = n * n;
+  memset(grad, 0, sizeof(double) * 3 * natoms);
+#pragma omp parallel
+  {
+    double* g = (double*)calloc((size_t)(3 * natoms), sizeof(double));
+#pragma omp for schedule(dynamic, 1)
+    for (long long i = n - 1; i >= 0; --i)
+      for (long long j = 0; j <= i; ++j) {
+        const long long ij = i * (i + 1) / 2 + j;
+        for (long long k = i; k < n; ++k)
+          for (long long l = 0; l <= k; ++l) {
+            const long long kl = k * (k + 1) / 2 + l;
+            if (kl < ij) continue;
+            const long long slot = kl * (kl + 1) / 2 + ij;
+            double f = 1.0;
+            if (i == j) f *= 0.5;
+            if (k == l) f *= 0.5;
+            if (ij == kl) f *= 0.5;
+            const long long im[8][4] = {{i, j, k, l}, {j, i, k, l}, {i, j, l, k}, {j, i, l, k},
+                                        {k, l, i, j}, {l, k, i, j}, {k, l, j, i}, {l, k, j, i}};
+            double w = 0.0;
+            for (int x = 0; x < 8; ++x) {
+              const long long p = im[x][0], q = im[x][1], r = im[x][2], t = im[x][3];
+              double v = cJ * DJ[p * n + q] * DJ[r * n + t];
+              for (int m = 0; m < nK; ++m) v -= cK * DK[m * nn + p * n + r] * DK[m * nn + q * n + t];
+              w += f * v;
+            }
+            if (w == 0.0) continue;
+            for (int d = 0; d < 3; ++d) {
+              const double A = deriv9[(3 * d + 0) * len + slot], B = deriv9[(3 * d + 1) * len + slot];
+              const double C = deriv9[(3 * d + 2) * len + slot];
+              g[3 * bf_atom[i] + d] += w * A;
+              g[3 * bf_atom[j] + d] += w * B;
+              g[3 * bf_atom[k] + d] += w * C;
+              g[3 * bf_atom[l] + d] -= w * (A + B + C);
+            }
+          }
+      }
+#pragma omp critical
+    for (int x = 0; x < 3 * natoms; ++x) grad[x] += g[x];
+    free(g);
+  }
+  return 0;
+}

@@ -34,6 +34,9 @@ int or_fock_rhf(long long n, const double* eri, const double* D, const double* H
 int or_fock_uhf(long long n, const double* eri, const double* Da, const double* Db, const double* H,
                 double* Fa, double* Fb);
 int or_jk(long long n, const double* eri, const double* D, double* J, double* K);
+int or_jk_packed(long long n, const double* eri, int nd, const double* D, double* J, double* K);
+int or_grad2e_from_deriv1(long long n, const double* deriv9, const int* bf_atom, int natoms, const double* DJ,
+                          double cJ, int nK, const double* DK, double cK, double* grad);
 int or_grad2e(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
               const double* coef, int pure, const int* shell_atom, int natoms, const double* DJ, double cJ,
               int nK, const double* DK, double cK, double* grad);

@@ -109,3 +109,62 @@ def test_host_one_electron_matches_reference(name, pure):
     g0 = oracle.ref_onee_grad(bs, D, Q, 2.0, -2.0)
     g = E.one_electron_grad(bs, D, Q, 2.0, -2.0)
     assert np.abs(g - g0).max() < 1e-11
+
+
+def test_packed_digest_matches_row_contraction():
+    """or_jk_packed (one pass over the unique ERIs, used for the oracle SCF at full size)
+    gives the sums of the row-by-row contraction or_jk, for symmetric and general densities."""
+    rng = np.random.default_rng(41)
+    Z, x = M.water(rng)
+    bs = B.build_basis("6-31g**", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    eri = oracle.eri_packed(bs)
+    n = bs.nbf
+    A = rng.normal(size=(n, n))
+    Ds = [(A + A.T) / n, rng.normal(size=(n, n)) / n]
+    J, K = oracle.jk_packed(eri, Ds)
+    for m, D in enumerate(Ds):
+        J0, K0 = oracle.jk(eri, D)
+        assert np.max(np.abs(J[m] - J0)) < 1e-13 and np.max(np.abs(K[m] - K0)) < 1e-13
+
+
+@needs_ref
+@pytest.mark.parametrize("name,pure", [("6-31g*", False), ("cc-pvdz", True)])
+def test_packed_derivative_digest_matches_restatement(name, pure):
+    """The gradient contracted from the reference's nine packed derivative tensors in one
+    pass (or_grad2e_from_deriv1, used for the (H2O)8 oracle gradient) equals the C
+    restatement over all ordered quartets (or_grad2e), RHF and UHF weights."""
+    rng = np.random.default_rng(43)
+    Z, x = M.water(rng)
+    bs = B.build_basis(name, Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=pure)
+    n = bs.nbf
+    sym = lambda: (lambda A: (A + A.T) / n)(rng.normal(size=(n, n)))  # noqa: E731
+    D, Da, Db = sym(), sym(), sym()
+    d9 = oracle.ref_deriv1(bs)
+    g = oracle.grad2e_packed_deriv1(d9, bs.bf_atom(), bs.natoms, D, 2.0, [D], 1.0)
+    assert np.max(np.abs(g - oracle.grad2e_rhf(bs, D))) < 1e-13
+    gu = oracle.grad2e_packed_deriv1(d9, bs.bf_atom(), bs.natoms, Da + Db, 0.5, [Da, Db], 0.5)
+    assert np.max(np.abs(gu - oracle.grad2e_uhf(bs, Da, Db))) < 1e-13
+
+
+@needs_ref
+def test_oracle_scf_converges_to_a_stationary_density():
+    """The oracle RHF driver (oracle/scf.py) on the reference's own integrals of H2O/cc-pVDZ:
+    converged, idempotent D S D = D with tr(DS) = nocc, and a vanishing commutator FDS - SDF."""
+    from oracle import scf as OS
+    Z, x, name, pure = M.workload(1)
+    bs = B.build_basis(name, Z, x, pure=pure)
+    S, T, V = oracle.ref_onee(bs)
+    eri = oracle.ref_eri_packed(bs)
+    nocc = int(sum(Z)) // 2
+
+    def jk(D):
+        J, K = oracle.jk_packed(eri, [D])
+        return J[0], K[0]
+
+    r = OS.rhf(S, T + V, nocc, jk, OS.nuclear_repulsion(Z, bs.coords))
+    D, F = r["D"], r["F"]
+    assert r["converged"]
+    assert np.max(np.abs(D @ S @ D - D)) < 1e-12
+    assert abs(np.trace(D @ S) - nocc) < 1e-12
+    assert np.max(np.abs(F @ D @ S - S @ D @ F)) < 1e-7
+    assert abs(OS.nuclear_repulsion(Z, bs.coords) - B.nuclear_repulsion(Z, bs.coords)) < 1e-12
