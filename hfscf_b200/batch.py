@@ -29,6 +29,7 @@ import torch
 
 from . import engine as eng
 from .basis import Basis, build_basis, nuclear_repulsion, nuclear_repulsion_gradient
+from .scf import DIIS_EPS
 
 PAD_DIAG = 1.0e3  # padded diagonal of F: far above every occupied orbital energy
 
@@ -153,7 +154,7 @@ class _Layout:
 
 
 def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-10, rms_tol=1e-8,
-              max_iter=60, use_graph=True, gradient=True, autotune=False, diag="gpu"):
+              max_iter=60, use_graph=True, gradient=True, autotune=False, diag="gpu", diis_range=5):
     """Converged RHF energies (and gradients) of every molecule of the batch.  ``diag``:
     "gpu" diagonalises every molecule's Fock matrix in one launch of the batched Jacobi
     kernel (hfgpu_batch_eigh, molecules of up to 118 functions); "host" runs LAPACK per
@@ -264,41 +265,55 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
             torch.cuda.synchronize()
     tt = stage("graph_capture", tt)
     t_setup = time.perf_counter() - t0
-    hist_F, hist_E = [], []
+    # DIIS history per molecule (the reference's diis_extrapolate, src/scfsolver/hfscf_diis.cpp:9-123):
+    # beyond diis_range vectors each molecule drops its own LARGEST-error entry before the new
+    # one is added; the B matrix is rescaled where sum|B| < 1e-14
+    hF = hE = hR = None  # [nmol, m, n, n], [nmol, m, n*n], [nmol, m]
     E_prev = torch.zeros(nmol, dtype=torch.float64, device=dev)
     converged = torch.zeros(nmol, dtype=torch.bool, device=dev)
     n_per = torch.from_numpy(be.nbf).to(dev).to(torch.float64)
     it = 0
-    build_times = []
+    build_events = []
     t1 = time.perf_counter()
     while it < max_iter:
         it += 1
         Dblk.copy_(lay.to_block(D))
-        ta = time.perf_counter()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
         if graph is not None:
             graph.replay()
         else:
             build()
-        build_times.append(time.perf_counter() - ta)
+        ev1.record(stream)
+        build_events.append((ev0, ev1))
         F = lay.to_pad(Fblk, fill_diag=PAD_DIAG)
         FDS = F @ D @ S
         err = X.transpose(1, 2) @ (FDS - FDS.transpose(1, 2)) @ X
         rms = torch.sqrt((err * err).sum(dim=(1, 2)) / (n_per * n_per))
-        hist_F.append(F)
-        hist_E.append(err.reshape(nmol, -1))
-        if len(hist_F) > 6:
-            hist_F.pop(0)
-            hist_E.pop(0)
-        m = len(hist_F)
+        if hF is not None and hF.shape[1] > diis_range:
+            keep = torch.arange(hF.shape[1], device=dev)[None, :] != hR.argmax(dim=1)[:, None]
+            m1 = hF.shape[1] - 1
+            hF = hF[keep].reshape(nmol, m1, *hF.shape[2:])
+            hE = hE[keep].reshape(nmol, m1, -1)
+            hR = hR[keep].reshape(nmol, m1)
+        if hF is None:
+            hF, hE, hR = F[:, None], err.reshape(nmol, 1, -1), rms[:, None]
+        else:
+            hF = torch.cat([hF, F[:, None]], dim=1)
+            hE = torch.cat([hE, err.reshape(nmol, 1, -1)], dim=1)
+            hR = torch.cat([hR, rms[:, None]], dim=1)
+        m = hF.shape[1]
         if m > 1:
-            Es = torch.stack(hist_E, dim=1)  # [nmol, m, n*n]
+            Bm = hE @ hE.transpose(1, 2)
+            small = Bm.abs().sum(dim=(1, 2)) < DIIS_EPS
+            Bm = torch.where(small[:, None, None], Bm / Bm.amax(dim=(1, 2), keepdim=True), Bm)
             B = -torch.ones((nmol, m + 1, m + 1), dtype=torch.float64, device=dev)
-            B[:, :m, :m] = Es @ Es.transpose(1, 2)
+            B[:, :m, :m] = Bm
             B[:, m, m] = 0.0
             rhs = torch.zeros((nmol, m + 1), dtype=torch.float64, device=dev)
             rhs[:, m] = -1.0
             c = torch.linalg.solve(B, rhs)[:, :m]
-            F = torch.einsum("bk,bkij->bij", c, torch.stack(hist_F, dim=1))
+            F = torch.einsum("bk,bkij->bij", c, hF)
         D = density(F)
         E = ((D * (H + F)).sum(dim=(1, 2)) - PAD_DIAG * 0)  # padded entries of D are zero
         conv = (rms < rms_tol) & ((E - E_prev).abs() < e_tol)
@@ -319,7 +334,7 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     out = {"energies": E_el + enuc, "iterations": it, "converged": converged.cpu().numpy(),
            "setup_s": t_setup, "setup_stages_s": stages, "scf_s": t_scf, "graph": graph is not None,
            "autotuned": schedule is not None,
-           "build_ms_mean": 1e3 * float(np.mean(build_times)), "nmol": nmol,
+           "build_ms_mean": float(np.mean([a.elapsed_time(b) for a, b in build_events])), "nmol": nmol,
            "final_s": time.perf_counter() - t_fin}
     if gradient:
         t2 = time.perf_counter()

@@ -355,3 +355,97 @@ double hfref_time_fock_sample(long long n, long long rows, double* checksum) {
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// Timing sample of the reference's RHF gradient two-electron part
+// (Mol::scf_gradient::calc_scf_gradient_rhf, src/gradient/hfscf_grad_rhf.cpp:76-141):
+//   *t_deriv_s   calc_coulomb_exchange_integral_centers (src/gradient/hfscf_grad_ints.cpp:110-151):
+//                Erios::compute_contracted_shell_quartet_deriv1 over every `stride`-th unique shell
+//                quartet of its loop, on all OpenMP threads, scaled to all quartets (the nine packed
+//                tensors are allocated and first touched outside the timed part, which is added in
+//                full to *t_fixed_s);
+//   *t_assemble_s  one call of calc_coulomb_exchange_integrals (:79-108) for atom 0, x, over all
+//                canonical slots (the reference makes 3 natoms of them);
+//   *t_contract_s  the dG/dX contraction of one (atom, direction) (hfscf_grad_rhf.cpp:121-134) over
+//                the rows i < rows, scaled to all N(N+1)/2 elements (3 natoms of them).
+// Returns 0.  Only the timings are of interest; the sums are kept in *checksum.
+int hfref_time_grad_sample(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
+                           const double* coef, int pure, double cutoff, long long stride, long long rows,
+                           double* t_deriv_s, double* t_fixed_s, double* t_assemble_s, double* t_contract_s,
+                           double* checksum) {
+  auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, pure);
+  const Eigen::Index n = pure ? b->npure : b->ncart;
+  const double f0 = omp_get_wtime();
+  std::vector<bool> mask = {true, true, true};
+  std::vector<tensor4dmath::symm4dTensor<double>> t(9);
+  for (int q = 0; q < 9; ++q) t[q] = tensor4dmath::symm4dTensor<double>(n);
+  *t_fixed_s = omp_get_wtime() - f0;
+  std::vector<std::pair<int, int>> quartets;
+  for (int i = 0; i < nshell; ++i)
+    for (int j = 0; j <= i; ++j)
+      for (int k = 0; k < nshell; ++k)
+        for (int l = 0; l <= k; ++l)
+          if (hfscfmath::index_ij(i, j) <= hfscfmath::index_ij(k, l)) quartets.emplace_back(i * nshell + j, k * nshell + l);
+  std::vector<std::pair<int, int>> pick;
+  for (size_t q = 0; q < quartets.size(); q += (size_t)stride) pick.push_back(quartets[q]);
+  ERIOS::Erios os(pure != 0, cutoff);
+  const double t0 = omp_get_wtime();
+#pragma omp parallel for schedule(dynamic)
+  for (long long q = 0; q < (long long)pick.size(); ++q)
+    os.compute_contracted_shell_quartet_deriv1(t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], t[8],
+                                               b->pairs[pick[q].first], b->pairs[pick[q].second], mask);
+  *t_deriv_s = (omp_get_wtime() - t0) * (double)quartets.size() / (double)std::max<size_t>(pick.size(), 1);
+  // function -> atom of shell, for the mask of atom 0
+  std::vector<char> m0((size_t)n, 0);
+  {
+    Eigen::Index f = 0;
+    for (int s = 0; s < nshell; ++s) {
+      const int nf = pure ? 2 * L[s] + 1 : (L[s] + 1) * (L[s] + 2) / 2;
+      const bool on0 = xyz[3 * s] == xyz[0] && xyz[3 * s + 1] == xyz[1] && xyz[3 * s + 2] == xyz[2];
+      for (int k = 0; k < nf; ++k) m0[(size_t)(f + k)] = on0;
+      f += nf;
+    }
+  }
+  tensor4dmath::symm4dTensor<double> dV(n);
+  const double t1 = omp_get_wtime();
+#pragma omp parallel for schedule(dynamic)
+  for (Eigen::Index i = 0; i < n; ++i)
+    for (Eigen::Index j = 0; j <= i; ++j) {
+      const Eigen::Index ij = hfscfmath::index_ij(i, j);
+      for (Eigen::Index k = 0; k < n; ++k)
+        for (Eigen::Index l = 0; l <= k; ++l) {
+          const Eigen::Index kl = hfscfmath::index_ij(k, l);
+          if (ij <= kl) {
+            if (m0[(size_t)i]) dV(i, j, k, l) += t[0](i, j, k, l);
+            if (m0[(size_t)j]) dV(i, j, k, l) += t[1](i, j, k, l);
+            if (m0[(size_t)k]) dV(i, j, k, l) += t[2](i, j, k, l);
+            if (m0[(size_t)l]) dV(i, j, k, l) += -t[0](i, j, k, l) - t[1](i, j, k, l) - t[2](i, j, k, l);
+          }
+        }
+    }
+  *t_assemble_s = omp_get_wtime() - t1;
+  std::vector<double> D((size_t)(n * n), 1e-2);
+  std::vector<std::pair<Eigen::Index, Eigen::Index>> ij;
+  for (Eigen::Index i = 0; i < std::min<Eigen::Index>(rows, n); ++i)
+    for (Eigen::Index j = i; j < n; ++j) ij.emplace_back(i, j);
+  double c = 0.0;
+  const double t2 = omp_get_wtime();
+#pragma omp parallel for schedule(dynamic) reduction(+ : c)
+  for (long long x = 0; x < (long long)ij.size(); ++x) {
+    const Eigen::Index i = ij[(size_t)x].first, j = ij[(size_t)x].second;
+    double gc = 0.0, ge = 0.0;
+    for (Eigen::Index k = 0; k < n; ++k)
+      for (Eigen::Index l = 0; l < n; ++l) {
+        gc += D[(size_t)(k * n + l)] * (2.0 * dV(i, j, k, l));
+        ge -= D[(size_t)(k * n + l)] * dV(i, k, j, l);
+      }
+    c += gc + ge;
+  }
+  const double frac = (double)ij.size() / (0.5 * (double)n * (double)(n + 1));
+  *t_contract_s = (omp_get_wtime() - t2) / frac;
+  *checksum = c;
+  return 0;
+}
+
+}  // extern "C"

@@ -12,7 +12,8 @@ m = 0..10 over T in [0, 1e3]:
   * below T = 1e-8 the reference evaluates F_m(1e-8) (src/math/gamma.cpp:20-21) and the
     GPU the exact F_m(T); the two differ by at most 1e-8 / (2m + 3).
 Schwarz factors (hfgpu_schwarz) against the reference's own screen matrix
-(Erios::compute_screen_matrix, src/integrals/hfscf_oseri_screen.cpp:22-181).
+(Erios::compute_screen_matrix, src/integrals/hfscf_oseri_screen.cpp:22-181), as (ab|ab) to
+1e-10 relative + 1e-13 absolute.
 """
 import os
 
@@ -66,7 +67,8 @@ def test_gpu_boys_below_the_reference_clamp():
         for m in range(11):
             r = oracle.ref_boys(m, t)
             if t < 1e-8:
-                assert abs(Fg[i, m] - r) <= 1e-8 / (2 * m + 3) + 1e-15
+                # F_m(0) - F_m(1e-8) = 1e-8 / (2m + 3) + O(1e-16); 1e-13 covers the reference's rounding
+                assert abs(Fg[i, m] - r) <= 1e-8 / (2 * m + 3) + 1e-13
             else:
                 assert abs(Fg[i, m] - r) <= 1e-13 * r
 
@@ -101,7 +103,10 @@ def test_schwarz_factors_match_reference_screen_matrix():
             if np.all(blk < 0):
                 assert Q[a, b] < 1e-5
                 continue
-            q0 = np.sqrt(np.max(np.abs(blk)))
-            assert abs(Q[a, b] - q0) <= 1e-10 * q0 + 1e-12, (a, b, Q[a, b], q0)
+            # compared as (ab|ab): the reference drops intermediates below 1e-12 while it builds
+            # the screen matrix (hfscf_oseri_screen.cpp:140,155), which moves the smallest diagonal
+            # integrals at the 1e-15 level
+            q2 = np.max(np.abs(blk))
+            assert abs(Q[a, b] ** 2 - q2) <= 1e-10 * q2 + 1e-13, (a, b, Q[a, b] ** 2, q2)
             checked += 1
     assert checked > ns * ns // 2
