@@ -330,10 +330,11 @@ def gen_eri_class(la, lb, lc, ld):
     fn = f"eri_{la}{lb}{lc}{ld}"
     s.append(f"// ({'spdf'[la]}{'spdf'[lb]}|{'spdf'[lc]}{'spdf'[ld]}): {len(targets)} contracted VRR targets, "
              f"{len(vrr.memo)} VRR values, {nout} outputs")
-    s.append("template <typename R>")
+    # BT: the Boys table in global memory (BoysTable) or staged in shared memory (BoysShared)
+    s.append("template <typename R, typename BT>")
     s.append(f"__device__ __forceinline__ void {fn}(const PrimPair<R>* __restrict__ bp, int nbp, "
              f"const PrimPair<R>* __restrict__ kp, int nkp, R ABx, R ABy, R ABz, R CDx, R CDy, R CDz, "
-             f"const BoysTable<R>& boys, R* __restrict__ out) {{")
+             f"const BT& boys, R* __restrict__ out) {{")
     s.append(f"  R acc[{len(targets)}];")
     s.append(f"#pragma unroll")
     s.append(f"  for (int t = 0; t < {len(targets)}; ++t) acc[t] = R(0);")
@@ -668,6 +669,7 @@ def cap_blocks(vrr_values):
     return 0
 
 
+STAGED_MAX_L = 4          # classes that also get the persistent form with the Boys table in shared memory
 WARP_MIN_VRR = 250        # classes that also get a warp-per-quartet form (hfgpu_autotune picks)
 WARP_DEFAULT_MIN_VRR = 1000  # (dd|dp) and (dd|dd): measured faster as one warp per quartet by default
 
@@ -717,14 +719,16 @@ def class_header(c):
     parts.append(f"  using GradWarpTab = {'GradWarpTab' + t if gwarp else 'void'};")
     parts.append(f"  static constexpr bool kPrimWarp = {'true' if primwarp else 'false'};")
     parts.append(f"  static constexpr int kCapBlocks = {cap_blocks(m['vrr_values'])};")
+    # the persistent form with the Boys table in shared memory: classes of total L <= STAGED_MAX_L
+    parts.append(f"  static constexpr bool kStaged = {'true' if la + lb + lc + ld <= STAGED_MAX_L else 'false'};")
     if primwarp:
         parts.append(f"  template <typename R, int G>")
         parts.append(f"  static __device__ __forceinline__ void eri_pw({class_args_sig()}, int lane) {{")
         parts.append(f"    eri_{t}_pw<R, G>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out, lane);")
         parts.append("  }")
-    parts.append(f"  template <typename R>")
-    parts.append(f"  static __device__ __forceinline__ void eri({class_args_sig()}) {{")
-    parts.append(f"    eri_{t}<R>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out);")
+    parts.append(f"  template <typename R, typename BT>")
+    parts.append(f"  static __device__ __forceinline__ void eri({class_args_sig().replace('const BoysTable<R>&', 'const BT&')}) {{")
+    parts.append(f"    eri_{t}<R, BT>(bp, nbp, kp, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, out);")
     parts.append("  }")
     parts.append("  template <typename R>")
     parts.append(f"  static __device__ __forceinline__ void to_pure(const R* __restrict__ in, R* __restrict__ out) {{ to_pure_{t}<R>(in, out); }}")
@@ -738,6 +742,8 @@ def class_header(c):
 
 
 INST_TEMPLATE = """// GENERATED by gen_eri.py -- do not edit.
+#include <algorithm>
+
 #include "../hfgpu_kernels.cuh"
 #include "class_{t}.cuh"
 #include "../hfgpu_launch.h"
@@ -748,6 +754,21 @@ namespace hfgpu {{
 // per quartet otherwise.
 template <typename CC, typename R>
 static void launch_quartet_impl(const QuartetArgs<R>& a, const int2* q, int nq, cudaStream_t s) {{
+  if constexpr (CC::kStaged) {{
+    if (a.staged) {{
+      // persistent: about as many blocks as the GPU holds at once (each stages the Boys table once)
+      auto k = quartet_staged_kernel<{la}, {lb}, {lc}, {ld}, R>;
+      const int bs = a.block > 0 ? a.block : 64;
+      const int smem = boys_plane_bytes<R>();
+      int dev = 0, sms = 148, per_sm = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, bs, smem);
+      const int grid = std::min((nq + bs - 1) / bs, std::max(per_sm, 1) * sms);
+      k<<<grid, bs, smem, s>>>(a, q, nq);
+      return;
+    }}
+  }}
   bool warp = false;
   if constexpr (CC::kWarp) warp = nq <= a.warp_max;
   if (!warp) {{
@@ -852,7 +873,8 @@ const ClassLaunchers launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_quartet<d
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kWarpDefault,
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kGradWarp,
                                       &launch_grad_warp<double>, &launch_grad_warp<float>, &grad_warp_bytes,
-                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kCapBlocks > 0}};
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kCapBlocks > 0,
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kStaged}};
 }}  // namespace hfgpu
 """
 

@@ -177,3 +177,158 @@ struct BoysTable {
 
 __host__ __device__ constexpr int ncart_of(int L) { return (L + 1) * (L + 2) / 2; }
 __host__ __device__ constexpr int npure_of(int L) { return 2 * L + 1; }
+
+// ---------------------------------------------------------------------------
+// Boys table of one order staged in shared memory.
+//
+// The same expansion as BoysTable::eval, reading the table of the kernel's single order MS
+// from shared memory, where a block puts it once with one bulk copy (stage_boys_table).  The
+// rows are stored as planes: FP64 plane j (j = 0..3) holds the 16-byte pair (value 2j, value
+// 2j+1) of every grid point, so the four 16-byte loads of one evaluation go to four planes and
+// the lanes of a warp, holding different T, spread over the banks by grid point instead of all
+// hitting the same four banks of their 64-byte rows; FP32 has one plane of float4 (values
+// 0..3).  Global layout: per order, the planes back to back (BOYS_PLANE_BYTES(R) bytes).
+// ---------------------------------------------------------------------------
+#define BOYS_PLANES_D 4
+#define BOYS_PLANE_BYTES_D (BOYS_PLANES_D * BOYS_NGRID * 16)  // 23104 bytes per FP64 order
+#define BOYS_PLANE_BYTES_F (BOYS_NGRID * 16)                  // 5776 bytes per FP32 order
+
+template <typename R>
+__host__ __device__ constexpr int boys_plane_bytes() {
+  return sizeof(R) == 8 ? BOYS_PLANE_BYTES_D : BOYS_PLANE_BYTES_F;
+}
+
+template <typename R, int MS>
+struct BoysShared {
+  const R* tab;  // shared memory: the planes of order MS
+
+  template <int M>
+  __device__ __forceinline__ void eval(R T, R pre, R* F) const {
+    static_assert(M == MS, "the staged table holds one order");
+    if (T < R(BOYS_TMAX)) {
+      int k;
+      R d;
+      if constexpr (sizeof(R) == 8) {
+        const double sh = T * 10.0 + 6755399441055744.0;
+        k = __double2loint(sh);
+        d = (sh - 6755399441055744.0) * BOYS_H - T;
+      } else {
+        k = __float2int_rn(T * R(10));
+        d = R(k) * R(BOYS_H) - T;
+      }
+      R f, ek;
+      if constexpr (sizeof(R) == 8) {
+        const double2* P = reinterpret_cast<const double2*>(tab);
+        const double2 r0 = P[k], r1 = P[BOYS_NGRID + k], r2 = P[2 * BOYS_NGRID + k], r3 = P[3 * BOYS_NGRID + k];
+        f = r3.x;
+        f = r2.y + f * d;
+        f = r2.x + f * d;
+        f = r1.y + f * d;
+        f = r1.x + f * d;
+        f = r0.y + f * d;
+        f = r0.x + f * d;
+        ek = r3.y;
+      } else {
+        const float4 r0 = reinterpret_cast<const float4*>(tab)[k];
+        f = r0.w;
+        f = r0.z + f * d;
+        f = r0.y + f * d;
+        f = r0.x + f * d;
+        ek = R(0);
+      }
+      F[M] = f;
+      if constexpr (M > 0) {
+        R e;
+        if constexpr (sizeof(R) == 8) {
+          R x = R(1.0 / 40320.0);
+          x = R(1.0 / 5040.0) + d * x;
+          x = R(1.0 / 720.0) + d * x;
+          x = R(1.0 / 120.0) + d * x;
+          x = R(1.0 / 24.0) + d * x;
+          x = R(1.0 / 6.0) + d * x;
+          x = R(0.5) + d * x;
+          x = R(1.0) + d * x;
+          x = R(1.0) + d * x;
+          e = ek * x;
+        } else {
+          (void)ek;
+          e = exp_t<R>(-T);
+        }
+        const R t2 = T + T;
+#pragma unroll
+        for (int m = M; m > 0; --m) F[m - 1] = (t2 * F[m] + e) * R(1.0 / (2 * m - 1));
+      }
+    } else {
+      const R rt = rsqrt_t<R>(T);
+      const R it = rt * rt;
+      F[0] = R(0.88622692545275801365) * rt;
+      if constexpr (M > 0) {
+        const R e = exp_t<R>(-T);
+        const R h = R(0.5) * it;
+#pragma unroll
+        for (int m = 0; m < M; ++m) F[m + 1] = (R(2 * m + 1) * F[m] - e) * h;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] *= pre;
+  }
+};
+
+// Status codes a kernel leaves in its status word (device int, 0 = fine).
+enum : int { HFGPU_DEV_STAGE_TIMEOUT = 2 };
+// Polls of a bounded mbarrier wait (each followed by a short sleep): about 0.1 s in all.
+#define HFGPU_STAGE_MAX_POLLS (1 << 20)
+
+// Copies `bytes` (a multiple of 16; both addresses 16-byte aligned) from global memory into
+// this block's shared memory with one bulk copy of the TMA unit (cp.async.bulk, completing on
+// the mbarrier `mbar` in shared memory), called by every thread of the block.  The wait for the
+// copy is bounded: after HFGPU_STAGE_MAX_POLLS polls the block records
+// HFGPU_DEV_STAGE_TIMEOUT in *status and the function returns false (every thread gets the same
+// answer).  issue = false arms the barrier for `bytes` without issuing any copy, so that the
+// wait runs out: the bounded-wait test, never used by a build.
+__device__ __forceinline__ bool stage_to_shared(void* smem_dst, const void* gmem_src, unsigned bytes,
+                                                unsigned long long* mbar, int* status, bool issue = true) {
+  const unsigned mb = (unsigned)__cvta_generic_to_shared(mbar);
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+    if (issue)
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                   "l"(gmem_src), "r"(bytes), "r"(mb)
+                   : "memory");
+  }
+  unsigned done = 0;
+  for (int i = 0; i < HFGPU_STAGE_MAX_POLLS; ++i) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(mb)
+        : "memory");
+    if (done) break;
+    __nanosleep(64);
+  }
+  const int ok = __syncthreads_and(done != 0);
+  if (!ok) {
+    if (threadIdx.x == 0 && status != nullptr) atomicExch(status, HFGPU_DEV_STAGE_TIMEOUT);
+    // a copy that was issued may still be in flight: give it one more bounded wait before the
+    // block leaves (and its shared memory goes to another block)
+    if (issue) {
+      for (int i = 0; i < HFGPU_STAGE_MAX_POLLS && !done; ++i) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(mb)
+            : "memory");
+        if (!done) __nanosleep(64);
+      }
+    }
+    __syncthreads();
+  }
+  return ok != 0;
+}

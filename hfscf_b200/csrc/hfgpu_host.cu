@@ -63,6 +63,28 @@ std::vector<R> boys_table(int terms) {
   return t;
 }
 
+// The same table in the plane layout of BoysShared (hfgpu_common.cuh): per order, FP64 planes
+// j = 0..3 of (row[2j], row[2j+1]) over the grid points; FP32 one plane of row[0..3].
+template <typename R>
+std::vector<R> boys_planes(const std::vector<R>& rows) {
+  const int per = boys_plane_bytes<R>() / (int)sizeof(R);  // values per order
+  std::vector<R> t((size_t)(BOYS_MMAX + 1) * per, R(0));
+  for (int M = 0; M <= BOYS_MMAX; ++M)
+    for (int k = 0; k < BOYS_NGRID; ++k) {
+      const R* row = &rows[((size_t)M * BOYS_NGRID + k) * BOYS_ROW];
+      R* o = &t[(size_t)M * per];
+      if (sizeof(R) == 8) {
+        for (int j = 0; j < BOYS_PLANES_D; ++j) {
+          o[((size_t)j * BOYS_NGRID + k) * 2 + 0] = row[2 * j];
+          o[((size_t)j * BOYS_NGRID + k) * 2 + 1] = row[2 * j + 1];
+        }
+      } else {
+        for (int j = 0; j < 4; ++j) o[(size_t)k * 4 + j] = row[j];
+      }
+    }
+  return t;
+}
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -126,6 +148,13 @@ struct hfgpu_handle {
   // end of decade e (bound in [10^-e, 10^(1-e)), e = 0 collects bounds >= 1)
   std::vector<long long> bucket_end;
   DevBuf d_gmax;
+  // per geometry, for density-screened builds without a host round trip: d_launch holds per
+  // (class, list segment) the segment's [lo, hi) and its decade ends (2 + kBuckets longs),
+  // d_dyn the counts a build's launches process, d_first the first function of every shell
+  DevBuf d_launch, d_dyn, d_first;
+  // the Boys table in the plane layout of the staged kernels, and the device status word
+  DevBuf d_boys_pd, d_boys_pf, d_status;
+  int status_host = 0;  // the status word as the last host-pointer entry point read it
   long long nquartets = 0;
 
   DevBuf d_pairs, d_prim_d, d_prim_f, d_alpha_d, d_alpha_f, d_boys_d, d_boys_f, d_quart;
@@ -595,6 +624,28 @@ int build_quartets(hfgpu_handle* h) {
   HF_CUDA(h, h->d_quart.ensure(sizeof(int2) * std::max<size_t>(all.size(), 1)));
   if (!all.empty())
     HF_CUDA(h, cudaMemcpyAsync(h->d_quart.p, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, h->stream));
+  {
+    // launch table of the density-screened builds (see launch_counts_kernel)
+    const int nslot = hfgpu::kNumClasses * 4;
+    std::vector<long long> lt((size_t)nslot * (2 + kBuckets), 0);
+    for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+      const long long pstart[5] = {h->q_beg[c], h->q_hik1[c], h->q_mid[c], h->q_hik2[c], h->q_end[c]};
+      for (int part = 0; part < 4; ++part) {
+        long long* row = lt.data() + (size_t)(c * 4 + part) * (2 + kBuckets);
+        row[0] = pstart[part];
+        row[1] = pstart[part + 1];
+        for (int e = 0; e < kBuckets; ++e) row[2 + e] = h->bucket_end[((size_t)c * 4 + part) * kBuckets + e];
+      }
+    }
+    HF_CUDA(h, h->d_launch.ensure(sizeof(long long) * lt.size()));
+    HF_CUDA(h, h->d_dyn.ensure(sizeof(int) * nslot));
+    HF_CUDA(h, h->d_first.ensure(sizeof(int) * h->first.size()));
+    HF_CUDA(h, cudaMemcpyAsync(h->d_launch.p, lt.data(), sizeof(long long) * lt.size(), cudaMemcpyHostToDevice,
+                               h->stream));
+    if (!h->first.empty())
+      HF_CUDA(h, cudaMemcpyAsync(h->d_first.p, h->first.data(), sizeof(int) * h->first.size(),
+                                 cudaMemcpyHostToDevice, h->stream));
+  }
   HF_CUDA(h, cudaStreamSynchronize(h->stream));
   h->setup_ms[2] = std::chrono::duration<double, std::milli>(t1 - t0).count();
   h->setup_ms[3] = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
@@ -623,6 +674,29 @@ __global__ void gmax_kernel(const float* __restrict__ dmax, int n, unsigned int*
     m = max(m, __float_as_uint(dmax[i]));
   for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// Per launch of a density-screened build: how many quartets of its list segment can pass the
+// per-quartet test.  A segment is ordered by Schwarz-bound decade, largest first; decade e holds
+// bounds below kDecadeUpper[e], so with 4 max|D| = dm4 only the decades with
+// kDecadeUpper[e] * dm4 >= dtol can hold a surviving quartet.  table: per slot (class * 4 +
+// segment) lo, hi and the end of every decade; dyn[slot] = quartets from lo to the end of the
+// last such decade.  Runs on the device, so the build needs no host round trip.
+__constant__ double kDecadeUpper[18] = {1e300, 1.0,   1e-1,  1e-2,  1e-3,  1e-4,  1e-5,  1e-6,  1e-7,
+                                        1e-8,  1e-9,  1e-10, 1e-11, 1e-12, 1e-13, 1e-14, 1e-15, 1e-16};
+__global__ void launch_counts_kernel(const unsigned int* __restrict__ gmax_bits, double dtol,
+                                     const long long* __restrict__ table, int nslot, int nbuckets,
+                                     int* __restrict__ dyn) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslot) return;
+  const double dm4 = 4.0 * (double)__uint_as_float(*gmax_bits);
+  int keep = 0;
+  for (int e = 0; e < nbuckets; ++e)
+    if (kDecadeUpper[e] * dm4 >= dtol) keep = e + 1;
+  const long long* row = table + (size_t)s * (2 + nbuckets);
+  const long long lo = row[0], hi = row[1];
+  const long long end = keep > 0 ? min(hi, row[2 + keep - 1]) : lo;
+  dyn[s] = (int)max(0LL, end - lo);
 }
 
 // J = Jh + Jh^T inside every molecule's block of a batched handle.
@@ -762,6 +836,21 @@ static int read_counters(hfgpu_handle* h, long long* computed, long long* skippe
   return HFGPU_OK;
 }
 
+// Host-pointer entry points read the device status word back with their results (in stream
+// order) and clear it; a staging wait that ran out fails the call.
+static int enqueue_status_read(hfgpu_handle* h) {
+  HF_CUDA(h, cudaMemcpyAsync(&h->status_host, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  HF_CUDA(h, cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
+  return HFGPU_OK;
+}
+static int status_after_sync(hfgpu_handle* h) {
+  const int st = h->status_host;
+  h->status_host = 0;
+  if (st == HFGPU_DEV_STAGE_TIMEOUT)
+    return fail(h, HFGPU_ERR_CUDA, "a shared-memory staging wait ran out (bounded wait); the build is incomplete");
+  return st == 0 ? HFGPU_OK : fail(h, HFGPU_ERR_CUDA, "device status " + std::to_string(st));
+}
+
 // Device J/K: all pointers on the device.  Jout/Kout may be null to skip.
 static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* Jout, double* Kout,
                           int precision, bool delta = false) {
@@ -781,36 +870,28 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   const double dtol = delta && precision == HFGPU_MIXED ? h->opts.mixed_density_tol : h->opts.density_tol;
   const float* dmax = nullptr;
   if (dtol > 0.0 && !h->batched) {
-    HF_CUDA(h, h->d_dmax.ensure(sizeof(float) * ns * ns + sizeof(int) * (ns + 1)));
-    int* dfirst = reinterpret_cast<int*>(h->d_dmax.as<float>() + (size_t)ns * ns);
-    HF_CUDA(h, cudaMemcpyAsync(dfirst, h->first.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, h->stream));
-    dmax_kernel<<<(ns * ns + 127) / 128, 128, 0, h->stream>>>(dfirst, ns, n, DJ, nK, DK, h->d_dmax.as<float>());
+    HF_CUDA(h, h->d_dmax.ensure(sizeof(float) * ns * ns));
+    dmax_kernel<<<(ns * ns + 127) / 128, 128, 0, h->stream>>>(h->d_first.as<int>(), ns, n, DJ, nK, DK,
+                                                              h->d_dmax.as<float>());
     HF_CHECK_LAUNCH(h, "dmax kernel");
     ++kernels;
     dmax = h->d_dmax.as<float>();
   }
   // Quartets whose Schwarz bound times 4 max|D| is below the threshold cannot survive the
-  // per-quartet density test: with the lists ordered by bound decade, only a prefix of
-  // every segment is launched.
-  int keep_decades = kBuckets;
+  // per-quartet density test: with the lists ordered by bound decade, only a prefix of every
+  // segment can.  The prefix lengths are computed on the device (launch_counts_kernel) and read
+  // by the class kernels, so a density-screened build never waits for the host.
+  const int nslot = hfgpu::kNumClasses * 4;
   if (dmax != nullptr) {
+    static_assert(kBuckets == 18, "launch_counts_kernel's decade table");
     HF_CUDA(h, h->d_gmax.ensure(sizeof(unsigned int)));
     HF_CUDA(h, cudaMemsetAsync(h->d_gmax.p, 0, sizeof(unsigned int), h->stream));
     gmax_kernel<<<std::min((ns * ns + 255) / 256, 1024), 256, 0, h->stream>>>(h->d_dmax.as<float>(), ns * ns,
                                                                             h->d_gmax.as<unsigned int>());
-    HF_CHECK_LAUNCH(h, "gmax kernel");
-    ++kernels;
-    unsigned int gm_bits = 0;
-    HF_CUDA(h, cudaMemcpyAsync(&gm_bits, h->d_gmax.p, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->stream));
-    HF_CUDA(h, cudaStreamSynchronize(h->stream));
-    float gm;
-    std::memcpy(&gm, &gm_bits, sizeof(float));
-    const double dm4 = 4.0 * (double)gm;
-    keep_decades = 0;
-    for (int e = 0; e < kBuckets; ++e) {
-      const double upper = e == 0 ? 1e300 : std::pow(10.0, 1 - e);  // largest bound of decade e
-      if (upper * dm4 >= dtol) keep_decades = e + 1;
-    }
+    launch_counts_kernel<<<1, 128, 0, h->stream>>>(h->d_gmax.as<unsigned int>(), dtol, h->d_launch.as<long long>(),
+                                                   nslot, kBuckets, h->d_dyn.as<int>());
+    HF_CHECK_LAUNCH(h, "launch counts");
+    kernels += 2;
   }
   QuartetArgs<double> qd{};
   qd.jk = jk_args_d(h);
@@ -830,6 +911,10 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   }
   qd.mode = qf.mode = QMODE_JK;
   qd.pure = qf.pure = h->pure;
+  qd.boys_planes = h->d_boys_pd.as<double>();
+  qf.boys_planes = h->d_boys_pf.as<float>();
+  qd.status = qf.status = h->d_status.as<int>();
+  qd.stage_test = qf.stage_test = h->opts.reserved[0] == 1 ? 1 : 0;
   const int2* q = h->d_quart.as<int2>();
   long long launched = 0;
   // largest classes first so that they overlap the tail of the smaller ones
@@ -849,36 +934,38 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     qd.capped = qf.capped = h->sched_cap[c];
     qd.group = qf.group = h->sched_primwarp[c] == 1 ? 32 : h->sched_primwarp[c];
     qd.warp_max = qf.warp_max = class_warp_max(h, c);
+    qd.staged = qf.staged = (h->sched_cap[c] == 2 && L->has_staged) ? 1 : 0;
     h->ev_used[c] = false;
     if (e <= b || !((h->class_mask >> c) & 1u)) continue;
     if (h->timing) HF_CUDA(h, cudaEventRecord(h->ev[2 * c], st));
     // Four parts in list order: [beg,hik1) many-primitive / [hik1,mid) few-primitive (high
-    // bound, FP64), [mid,hik2) / [hik2,end) (low bound, FP32 in mixed mode).  Each part keeps
-    // the prefix of bound decades that can survive the density test; adjacent ranges that
-    // run the same kernel are launched together.
+    // bound, FP64), [mid,hik2) / [hik2,end) (low bound, FP32 in mixed mode).  Without density
+    // screening adjacent parts that run the same kernel are launched together; with it every
+    // part is its own launch and processes the device-computed prefix of its decades.
     const long long pstart[5] = {b, h->q_hik1[c], m, h->q_hik2[c], e};
-    struct Range { long long lo, hi; bool fp32, many; };
+    struct Range { long long lo, hi; bool fp32, many; int slot; };
     Range rg[4];
     int nr = 0;
     for (int part = 0; part < 4; ++part) {
-      long long lo = pstart[part], hi = pstart[part + 1];
-      if (keep_decades < kBuckets)
-        hi = keep_decades > 0 ? std::min(hi, h->bucket_end[((size_t)c * 4 + part) * kBuckets + keep_decades - 1]) : lo;
+      const long long lo = pstart[part], hi = pstart[part + 1];
       const bool fp32 = precision == HFGPU_MIXED && part >= 2;
       const bool many = (part % 2) == 0 && L->has_primwarp && h->sched_primwarp[c];
-      if (nr > 0 && rg[nr - 1].hi == lo && rg[nr - 1].fp32 == fp32 && rg[nr - 1].many == many) {
+      if (dmax == nullptr && nr > 0 && rg[nr - 1].hi == lo && rg[nr - 1].fp32 == fp32 && rg[nr - 1].many == many) {
         rg[nr - 1].hi = hi;  // contiguous and the same kernel: extend
       } else {
-        rg[nr++] = {lo, hi, fp32, many};
+        rg[nr++] = {lo, hi, fp32, many, c * 4 + part};
       }
     }
     for (int r = 0; r < nr; ++r) {
       const int nseg = (int)(rg[r].hi - rg[r].lo);
       if (nseg <= 0) continue;
       const int2* qs = q + rg[r].lo;
+      const int* dyn = dmax != nullptr ? h->d_dyn.as<int>() + rg[r].slot : nullptr;
       if (rg[r].fp32) {
+        qf.dyn_nq = dyn;
         if (!(rg[r].many && L->primwarp_f(qf, qs, nseg, st))) L->quartet_f(qf, qs, nseg, st);
       } else {
+        qd.dyn_nq = dyn;
         if (!(rg[r].many && L->primwarp_d(qd, qs, nseg, st))) L->quartet_d(qd, qs, nseg, st);
       }
       ++kernels;
@@ -1231,9 +1318,16 @@ int hfgpu_create(const hfgpu_basis* b, const hfgpu_opts* opts, hfgpu_handle** ou
   h->own_stream = true;
   const std::vector<double> bt = boys_table<double>(7);
   const std::vector<float> btf = boys_table<float>(4);
+  const std::vector<double> bpd = boys_planes(bt);
+  const std::vector<float> bpf = boys_planes(btf);
   if (h->d_boys_d.ensure(sizeof(double) * bt.size()) || h->d_boys_f.ensure(sizeof(float) * btf.size()) ||
+      h->d_boys_pd.ensure(sizeof(double) * bpd.size()) || h->d_boys_pf.ensure(sizeof(float) * bpf.size()) ||
+      h->d_status.ensure(sizeof(int)) ||
       cudaMemcpy(h->d_boys_d.p, bt.data(), sizeof(double) * bt.size(), cudaMemcpyHostToDevice) ||
-      cudaMemcpy(h->d_boys_f.p, btf.data(), sizeof(float) * btf.size(), cudaMemcpyHostToDevice)) {
+      cudaMemcpy(h->d_boys_f.p, btf.data(), sizeof(float) * btf.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(h->d_boys_pd.p, bpd.data(), sizeof(double) * bpd.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(h->d_boys_pf.p, bpf.data(), sizeof(float) * bpf.size(), cudaMemcpyHostToDevice) ||
+      cudaMemset(h->d_status.p, 0, sizeof(int))) {
     hfgpu_destroy(h);
     return HFGPU_ERR_CUDA;
   }
@@ -1248,7 +1342,8 @@ int hfgpu_destroy(hfgpu_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
   for (DevBuf* d : {&h->d_onee, &h->d_pairs, &h->d_prim_d, &h->d_prim_f, &h->d_alpha_d, &h->d_alpha_f, &h->d_boys_d, &h->d_boys_f,
                     &h->d_quart, &h->d_mats, &h->d_half, &h->d_dmax, &h->d_counters, &h->d_grad, &h->d_scratch,
-                    &h->d_eri, &h->d_eriq})
+                    &h->d_eri, &h->d_eriq, &h->d_launch, &h->d_dyn, &h->d_first, &h->d_boys_pd,
+                    &h->d_boys_pf, &h->d_status})
     d->release();
   h->d_mol.release();
   if (h->ev[0])
@@ -1373,7 +1468,9 @@ int hfgpu_jk(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double
   if ((rc = jk_device_impl(h, DJ ? dDJ : nullptr, nK, dDK, dJ, dK, precision))) return rc;
   if (DJ) HF_CUDA(h, cudaMemcpyAsync(J, dJ, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->stream));
   if (nK) HF_CUDA(h, cudaMemcpyAsync(K, dK, sizeof(double) * nn * nK, cudaMemcpyDeviceToHost, h->stream));
+  if ((rc = enqueue_status_read(h))) return rc;
   HF_CUDA(h, cudaStreamSynchronize(h->stream));
+  if ((rc = status_after_sync(h))) return rc;
   long long sk = 0;
   if ((rc = read_counters(h, nullptr, &sk))) return rc;
   h->last_skipped = sk;
@@ -1406,8 +1503,9 @@ int hfgpu_fock_rhf(hfgpu_handle* h, const double* D, const double* H, double* F,
   HF_CHECK_LAUNCH(h, "fock combine");
   ++h->last_kernels;
   HF_CUDA(h, cudaMemcpyAsync(F, dJ, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->stream));
+  if ((rc = enqueue_status_read(h))) return rc;
   HF_CUDA(h, cudaStreamSynchronize(h->stream));
-  return HFGPU_OK;
+  return status_after_sync(h);
 }
 
 int hfgpu_fock_uhf(hfgpu_handle* h, const double* Da, const double* Db, const double* H, double* Fa, double* Fb,
@@ -1448,8 +1546,9 @@ int hfgpu_fock_delta(hfgpu_handle* h, const double* dD, double* F, int precision
   HF_CHECK_LAUNCH(h, "fock combine");
   ++h->last_kernels;
   HF_CUDA(h, cudaMemcpyAsync(F, dJ, sizeof(double) * nn, cudaMemcpyDeviceToHost, h->stream));
+  if ((rc = enqueue_status_read(h))) return rc;
   HF_CUDA(h, cudaStreamSynchronize(h->stream));
-  return HFGPU_OK;
+  return status_after_sync(h);
 }
 
 int hfgpu_energy_forward(hfgpu_handle* h, const double* D, double* E2, int precision) {
@@ -1711,7 +1810,7 @@ int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule) {
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     const int bs = schedule[4 * c], pw = schedule[4 * c + 1], wp = schedule[4 * c + 2], cp = schedule[4 * c + 3];
     if ((bs != 32 && bs != 64 && bs != 128) || (pw != 0 && pw != 1 && pw != 4 && pw != 8 && pw != 16 && pw != 32) ||
-        wp < -1 || wp > 1 || (cp != 0 && cp != 1))
+        wp < -1 || wp > 1 || cp < 0 || cp > 2)
       return fail(h, HFGPU_ERR_INVALID, "schedule entry out of range");
   }
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
@@ -1767,9 +1866,10 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
     float ms;
     int b, p, w, c;
   };
-  std::vector<Cand> kind_best((size_t)3 * hfgpu::kNumClasses, Cand{1e30f, 0, 0, 0, 0});
-  auto kind_of = [&](int c, int pw, int wp) {
-    return wp == 1 ? 2 : (hfgpu::kClassLaunchers[c]->has_primwarp && pw > 0 ? 1 : 0);
+  std::vector<Cand> kind_best((size_t)4 * hfgpu::kNumClasses, Cand{1e30f, 0, 0, 0, 0});
+  auto kind_of = [&](int c, int pw, int wp, int cap) {
+    const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
+    return wp == 1 ? 2 : (L->has_primwarp && pw > 0 ? 1 : (cap == 2 && L->has_staged ? 3 : 0));
   };
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     if (h->q_end[c] <= h->q_beg[c]) continue;
@@ -1783,8 +1883,11 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
       const int pws[5] = {32, 16, 8, 4, 0};
       for (int pi = (L->has_primwarp ? 0 : 4); pi < 5; ++pi) {
         const int pw = pws[pi];
-        for (int cand = 0; cand < (L->has_capped ? 6 : 3); ++cand) {
+        // thread-form variants: plain (0), register-capped (1), persistent with the Boys table
+        // staged in shared memory (2)
+        for (int cand = 0; cand < 9; ++cand) {
           const int bs = 32 << (cand % 3), cap = cand / 3;
+          if ((cap == 1 && !L->has_capped) || (cap == 2 && !L->has_staged)) continue;
           if (wp == 1 && (bs != 64 || cap)) continue;  // the warp form has its own block shape
           h->sched_block[c] = bs;
           h->sched_primwarp[c] = L->has_primwarp ? pw : 1;
@@ -1805,7 +1908,7 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
             bw = wp;
             bc = cap;
           }
-          Cand& kb = kind_best[(size_t)3 * c + kind_of(c, pw, wp)];
+          Cand& kb = kind_best[(size_t)4 * c + kind_of(c, pw, wp, cap)];
           if (ms < kb.ms) kb = Cand{ms, bs, h->sched_primwarp[c], wp, cap};
         }
       }
@@ -1835,9 +1938,9 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
   if ((rc = time_builds(&cur))) return rc;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     if (h->q_end[c] <= h->q_beg[c]) continue;
-    for (int k = 0; k < 3; ++k) {
-      const Cand& cd = kind_best[(size_t)3 * c + k];
-      if (cd.ms >= 1e30f || k == kind_of(c, h->sched_primwarp[c], h->sched_warp[c])) continue;
+    for (int k = 0; k < 4; ++k) {
+      const Cand& cd = kind_best[(size_t)4 * c + k];
+      if (cd.ms >= 1e30f || k == kind_of(c, h->sched_primwarp[c], h->sched_warp[c], h->sched_cap[c])) continue;
       const Cand keep{0.f, h->sched_block[c], h->sched_primwarp[c], h->sched_warp[c], h->sched_cap[c]};
       h->sched_block[c] = cd.b;
       h->sched_primwarp[c] = cd.p;
@@ -1875,6 +1978,18 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
     }
   if ((rc = hfgpu_set_schedule(h, t_tuned <= t_start ? tuned : start))) return rc;
   return schedule ? hfgpu_get_schedule(h, schedule) : HFGPU_OK;
+}
+
+int hfgpu_device_status(hfgpu_handle* h, int* status) {
+  if (!h || !status) return HFGPU_ERR_INVALID;
+  DeviceGuard dev_guard(h);
+  if (dev_guard.rc) return dev_guard.rc;
+  int v = 0;
+  HF_CUDA(h, cudaMemcpyAsync(&v, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  HF_CUDA(h, cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->stream));
+  *status = v;
+  return HFGPU_OK;
 }
 
 int hfgpu_last_launches(const hfgpu_handle* h, int* kernels) {

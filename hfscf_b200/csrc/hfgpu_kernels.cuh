@@ -241,15 +241,26 @@ struct QuartetArgs {
   int block;            // threads per block of the thread-per-quartet form (32, 64 or 128; 0 = 64)
   int group;            // lanes per quartet of the primitive-split form (4, 8, 16 or 32; 0 = 32)
   int capped;           // 1: the register-capped variant of the thread form (classes that have one)
+  const int* dyn_nq;    // device count of this launch's quartets (<= nq), written by an earlier kernel
+                        // of the same build (density-screened prefix); nullptr: all nq quartets
+  int staged;           // 1: the persistent form with the Boys table staged in shared memory (low L)
+  const R* boys_planes; // the Boys table in plane layout, one block of boys_plane_bytes<R>() per order
+  int* status;          // device status word (HFGPU_DEV_STAGE_TIMEOUT when a staging wait ran out)
+  int stage_test;       // 1: arm the staging barrier without a copy, so that its wait runs out (test only)
 };
 
-// MINB > 1: the register-capped variant (at least MINB blocks of 128 threads per SM) of the
-// small classes, for more warps in flight.
-template <int LA, int LB, int LC, int LD, typename R, int MINB = 1>
-__global__ void __launch_bounds__(128, MINB) quartet_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets,
-                                                            int nq) {
+// Quartets this launch processes: nq, or the device-side count of a density-screened build.
+template <typename R>
+__device__ __forceinline__ int launch_count(const QuartetArgs<R>& qa, int nq) {
+  return qa.dyn_nq != nullptr ? min(nq, __ldg(qa.dyn_nq)) : nq;
+}
+
+// One thread per quartet: quartet t of the launch's list (t >= nq: an idle lane that still
+// takes part in the warp's shuffles).  Called by all 32 lanes of a warp with consecutive t.
+template <int LA, int LB, int LC, int LD, typename R, typename BT>
+__device__ __forceinline__ void quartet_thread(const QuartetArgs<R>& qa, const BT& boys,
+                                               const int2* __restrict__ quartets, int nq, int t) {
   const JKArgs<R>& a = qa.jk;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   // every lane stays to the end (lanes without work carry valid = false), so
   // that the digestion can use whole-warp shuffles
   const bool in_range = t < nq;
@@ -287,7 +298,10 @@ __global__ void __launch_bounds__(128, MINB) quartet_kernel(QuartetArgs<R> qa, c
   const bool coop = __all_sync(0xffffffffu, same_bra) && qa.mode == QMODE_JK;
   using Dc = BlockDims<LA, LB, LC, LD, false>;
   R cart[Dc::NCART];
-  if (valid) cart_block<LA, LB, LC, LD, R>(P, Q, a.prims, a.boys, cart);
+  if (valid)
+    ClassCode<LA, LB, LC, LD>::template eri<R>(a.prims + P.prim_off, P.nprim, a.prims + Q.prim_off, Q.nprim,
+                                                R(P.ABx), R(P.ABy), R(P.ABz), R(Q.ABx), R(Q.ABy), R(Q.ABz), boys,
+                                                cart);
   double s = 1.0;
   if (P.sa == P.sb) s *= 0.5;
   if (Q.sa == Q.sb) s *= 0.5;
@@ -311,6 +325,36 @@ __global__ void __launch_bounds__(128, MINB) quartet_kernel(QuartetArgs<R> qa, c
   }
 }
 
+// MINB > 1: the register-capped variant (at least MINB blocks of 128 threads per SM) of the
+// small classes, for more warps in flight.
+template <int LA, int LB, int LC, int LD, typename R, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) quartet_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets,
+                                                            int nq) {
+  nq = launch_count(qa, nq);
+  quartet_thread<LA, LB, LC, LD, R>(qa, qa.jk.boys, quartets, nq, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The thread-per-quartet form as a persistent kernel with the class's Boys table in shared
+// memory, for the low-L classes whose time goes to the lanes' scattered Boys-row loads: every
+// block stages the table of the class's single order L = la+lb+lc+ld with one bulk copy
+// (stage_to_shared), then its warps take 32 quartets at a time, grid-stride.  Launched with
+// about as many blocks as the GPU holds at once, so the copy is made once per resident block.
+template <int LA, int LB, int LC, int LD, typename R>
+__global__ void __launch_bounds__(128) quartet_staged_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets,
+                                                             int nq) {
+  constexpr int L = LA + LB + LC + LD;
+  extern __shared__ __align__(16) unsigned char staged_smem[];
+  __shared__ unsigned long long stage_bar;
+  R* tab = reinterpret_cast<R*>(staged_smem);
+  const unsigned char* src = reinterpret_cast<const unsigned char*>(qa.boys_planes) + (size_t)L * boys_plane_bytes<R>();
+  if (!stage_to_shared(tab, src, boys_plane_bytes<R>(), &stage_bar, qa.status, qa.stage_test == 0)) return;
+  const BoysShared<R, L> boys{tab};
+  nq = launch_count(qa, nq);
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w * 32 < nq; w += warps)
+    quartet_thread<LA, LB, LC, LD, R>(qa, boys, quartets, nq, w * 32 + (threadIdx.x & 31));
+}
+
 // G lanes per quartet (G = 4, 8, 16 or 32) for small classes and quartets with many
 // primitive quartets: the lanes of a group split the primitive quartets (consecutive ket
 // primitives, one bra primitive per run: coalesced and broadcast loads), the
@@ -322,6 +366,7 @@ __global__ void __launch_bounds__(128) quartet_primwarp_kernel(QuartetArgs<R> qa
                                                                int nq) {
   static_assert(G == 4 || G == 8 || G == 16 || G == 32, "group size");
   const JKArgs<R>& a = qa.jk;
+  nq = launch_count(qa, nq);
   const int sub = threadIdx.x & (G - 1);
   const int qi = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool in_range = qi < nq;
@@ -715,7 +760,7 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
   constexpr int PER = warp_slots<Tab, R>();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int qi = blockIdx.x * (blockDim.x >> 5) + w;
-  if (qi >= nq) return;  // whole warp
+  if (qi >= launch_count(qa, nq)) return;  // whole warp
   R* vs = reinterpret_cast<R*>(wsmem) + (size_t)w * PER;
   R* hs = vs + Tab::NVSLOT + 1;
   R* A = hs + Tab::NHSLOT + 1;

@@ -26,6 +26,7 @@ struct ClassLaunchers {
   bool (*grad_warp_f)(const GradArgs<float>&, int pure, const int2*, int, cudaStream_t);
   int (*grad_warp_bytes)(int fp32);      // shared memory of one warp-form block (0: no warp form)
   bool has_capped;                       // register-capped variant of the thread-per-quartet form
+  bool has_staged;                       // persistent thread form with the Boys table in shared memory
 };
 
 extern const ClassLaunchers* const kClassLaunchers[];

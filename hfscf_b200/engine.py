@@ -92,7 +92,7 @@ class Engine:
     """One engine handle: a basis on one GPU, with the current geometry."""
 
     def __init__(self, basis: Basis, schwarz_tol=1e-12, density_tol=1e-12, mixed_fp32_bound=1e-4, device=0,
-                 warp_max_quartets=None, grad_warp_max_waves=None):
+                 warp_max_quartets=None, grad_warp_max_waves=None, stage_wait_test=False):
         self.basis = basis
         self.n = basis.nbf
         self._bv = _BasisView(basis)
@@ -103,6 +103,8 @@ class Engine:
             o.warp_max_quartets = warp_max_quartets
         if grad_warp_max_waves is not None:
             o.grad_warp_max_waves = grad_warp_max_waves
+        if stage_wait_test:
+            o.reserved[0] = 1  # staging waits run out on purpose (tests the bounded wait)
         self._opts = o
         h = ctypes.c_void_p()
         self._check(lib().hfgpu_create(ctypes.byref(self._bv.s), ctypes.byref(o), ctypes.byref(h)), None)
@@ -293,6 +295,12 @@ class Engine:
     def set_schedule(self, sched):
         s = np.ascontiguousarray(np.asarray(sched, dtype=np.int32).reshape(NUM_CLASSES, 4))
         self._check(lib().hfgpu_set_schedule(self.h, s.ctypes.data_as(_ip)))
+
+    def device_status(self) -> int:
+        """hfgpu_device_status: the kernels' status word since the last call (then cleared)."""
+        st = ctypes.c_int()
+        self._check(lib().hfgpu_device_status(self.h, ctypes.byref(st)))
+        return st.value
 
     def last_launches(self) -> int:
         k = ctypes.c_int()

@@ -72,7 +72,9 @@ typedef struct {
                                  the blocks the GPU holds at once, else one thread per quartet on global
                                  scratch (default 48: longer warp-form launches hold the shared memory of
                                  every SM and stop the other classes' kernels from overlapping; 0 = never) */
-  int reserved[5];
+  int reserved[5];          /* reserved[0] = 1: arm every shared-memory staging wait without issuing its copy,
+                              so that the bounded wait runs out (tests the timeout path; builds then report
+                              status 2); 0 otherwise.  reserved[1..4]: 0. */
 } hfgpu_opts;
 
 int hfgpu_default_opts(hfgpu_opts* opts);
@@ -206,6 +208,12 @@ int hfgpu_set_timing(hfgpu_handle* h, int on);
 int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out);
 int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms);
 int hfgpu_last_launches(const hfgpu_handle* h, int* kernels);
+/* Device status word of the handle's kernels since the last call, then cleared (synchronises
+ * the handle's stream): 0 = fine; 2 = a block's wait for its shared-memory staging copy ran
+ * out (bounded at about 0.1 s; the block skipped its quartets, so that build is incomplete).
+ * The host-pointer entry points check it themselves and return HFGPU_ERR_CUDA.  No reference
+ * counterpart (the reference has no device code). */
+int hfgpu_device_status(hfgpu_handle* h, int* status);
 int hfgpu_fp64_peak(int device, double* tflops);
 /* Boys function F_0..F_m (m <= 10) at count points T >= 0 (host arrays; F is count x (m+1)),
  * through the same table and evaluation the quartet kernels use, in FP64 (HFGPU_FP64) or in
@@ -224,8 +232,10 @@ int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
  *       form ignore it);
  *   [2] 1/0/-1 = warp-per-quartet form for the classes that have one, (dp|pp) (dp|ds) (dp|dp)
  *       (dd|pp) (dd|ds) (dd|dp) (dd|dd) (-1 = follow opts.warp_max_quartets);
- *   [3] 1/0 = register-capped variant of the thread form, for more warps per SM (the small
- *       classes (ps|ss) ... (dp|ss) have one; others ignore it).
+ *   [3] variant of the thread-per-quartet form: 0 plain; 1 register-capped, for more warps
+ *       per SM (the small classes (ps|ss) ... (dp|ss) have one); 2 persistent, with the
+ *       class's Boys table staged into shared memory by one bulk (TMA) copy per block (the
+ *       classes of total angular momentum <= 4 have one); classes without the variant ignore it.
  * Default: 64, 0, -1 for (dd|dp) and (dd|dd) else 0, 0.
  * autotune: times every form of every class on the current geometry with device density D
  * (n x n; `repeats` builds per candidate, one class at a time on the handle's stream),

@@ -34,7 +34,9 @@ def _molecules():
 
 MOLS = _molecules()
 # (block, primwarp, warp, capped) applied to every class
-FORMS = [(32, 0, 0, 0), (64, 1, 0, 1), (128, 0, 1, 0), (64, 1, 1, 0), (64, 4, 0, 1), (32, 8, 1, 1), (128, 16, 0, 0)]
+# capped = 2: the persistent form with the Boys table staged in shared memory (classes of L <= 4)
+FORMS = [(32, 0, 0, 0), (64, 1, 0, 1), (128, 0, 1, 0), (64, 1, 1, 0), (64, 4, 0, 1), (32, 8, 1, 1), (128, 16, 0, 0),
+         (64, 0, 0, 2), (128, 4, 0, 2), (32, 0, 1, 2)]
 
 
 @pytest.mark.parametrize("form", FORMS, ids=[f"b{f[0]}-pw{f[1]}-w{f[2]}-c{f[3]}" for f in FORMS])
@@ -77,7 +79,7 @@ def test_autotuned_schedule_gives_the_same_fock_build():
         assert sched.shape == (E.NUM_CLASSES, 4)
         assert set(np.unique(sched[:, 0])) <= {32, 64, 128}
         assert set(np.unique(sched[:, 1])) <= {0, 1, 4, 8, 16, 32} and set(np.unique(sched[:, 2])) <= {-1, 0, 1}
-        assert set(np.unique(sched[:, 3])) <= {0, 1}
+        assert set(np.unique(sched[:, 3])) <= {0, 1, 2}
         assert (eng.get_schedule() == sched).all()
         F1 = eng.fock_rhf(D, H)
         Fm1 = eng.fock_rhf(D, H, E.MIXED)
@@ -98,3 +100,57 @@ def test_gradient_launch_forms_match_oracle(name, bs, gmax):
         gm = eng.grad2e(D, precision=E.MIXED)
     assert np.max(np.abs(g - g0)) < 1e-10
     assert np.max(np.abs(gm - g0)) < 1e-6
+
+
+@pytest.mark.parametrize("precision", [E.FP64, E.MIXED], ids=["fp64", "mixed"])
+def test_staged_form_with_density_screening_matches_plain_form(precision):
+    """The staged persistent form under density screening (the counts of its launches come
+    from the device) gives the plain form's J and K."""
+    Z, x = M.water_cluster(3, 2.9, np.random.default_rng(33), 0.1)
+    bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    rng = np.random.default_rng(35)
+    D = 1e-3 * _sym(rng, bs.nbf)
+    with E.Engine(bs) as eng:
+        J0, K0 = eng.jk(D, [D], precision)
+        sched = eng.get_schedule()
+        sched[:, 3] = 2
+        sched[:, 1] = 0
+        eng.set_schedule(sched)
+        J1, K1 = eng.jk(D, [D], precision)
+    tol = 1e-12 if precision == E.FP64 else 1e-9
+    assert np.max(np.abs(J1 - J0)) < tol and np.max(np.abs(K1[0] - K0[0])) < tol
+
+
+def test_staging_wait_runs_out_and_reports():
+    """Bounded wait of the shared-memory staging: with the barrier armed and no copy issued
+    (the engine's wait test), every staged block gives up after its poll limit, records
+    status 2 and skips its quartets; the host-pointer build fails with HFGPU_ERR_CUDA, the
+    device build reports the status through hfgpu_device_status, and the context stays
+    usable for a normal engine afterwards.  No fault, no hang."""
+    import torch
+    rng = np.random.default_rng(37)
+    Z, x = M.water(rng)
+    bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    D = _sym(rng, bs.nbf)
+    staged = np.tile(np.array((64, 0, 0, 2), dtype=np.int32), (E.NUM_CLASSES, 1))
+    with E.Engine(bs, stage_wait_test=True) as eng:
+        eng.set_schedule(staged)
+        with pytest.raises(E.HfgpuError) as err:
+            eng.jk(D, [D])
+        assert err.value.code == 3 and "staging wait ran out" in str(err.value)
+        assert eng.device_status() == 0  # the failing call read and cleared it
+        dev = torch.device("cuda", 0)
+        Dd = torch.from_numpy(D).to(dev)
+        J = torch.zeros_like(Dd)
+        K = torch.zeros_like(Dd)
+        torch.cuda.synchronize()
+        eng.jk_device(Dd.data_ptr(), 1, Dd.data_ptr(), J.data_ptr(), K.data_ptr())
+        assert eng.device_status() == 2
+        assert eng.device_status() == 0
+    eri0 = oracle.eri_packed(bs)
+    J0, K0 = oracle.jk(eri0, D)
+    with E.Engine(bs, density_tol=0.0) as eng:
+        eng.set_schedule(staged)
+        J, K = eng.jk(D, [D])
+        assert eng.device_status() == 0
+    assert np.max(np.abs(J - J0)) < MAT_TOL and np.max(np.abs(K[0] - K0)) < MAT_TOL
