@@ -180,6 +180,31 @@ class VRR:
         return name
 
 
+def interleave_accumulation(body, adds):
+    """Places every accumulation statement right after the statement that defines its VRR value
+    (`adds`: (value name, statement) pairs), instead of after the whole recurrence: a target
+    value then dies as soon as its last use in the recurrence has passed, rather than living to
+    the end of the primitive-quartet body next to every accumulator.  Statements of values that
+    are not defined in `body` (the Boys values F[m]) go first."""
+    where = {}
+    for i, line in enumerate(body):
+        st = line.strip()
+        if st.startswith("const R "):
+            where[st[len("const R "):].split(" =", 1)[0]] = i
+    after = {}
+    head = []
+    for name, stmt in adds:
+        if name in where:
+            after.setdefault(where[name], []).append(stmt)
+        else:
+            head.append(stmt)
+    out = list(head)
+    for i, line in enumerate(body):
+        out.append(line)
+        out.extend(after.get(i, []))
+    return out
+
+
 def vrr_targets(lo_e, hi_e, lo_f, hi_f):
     out = []
     for le in range(lo_e, hi_e + 1):
@@ -292,9 +317,7 @@ def gen_eri_primwarp(la, lb, lc, ld):
     s.append("\n".join("  " + l[6:] if l.startswith("      ") else l for l in PRIM_HEADER.rstrip("\n").split("\n")))
     s.append(f"    R F[{L + 1}];")
     s.append(f"    boys.template eval<{L}>(T, pre, F);")
-    s += prim_body
-    for t, nme in enumerate(names):
-        s.append(f"    acc[{t}] += {nme};")
+    s += interleave_accumulation(prim_body, [(nme, f"    acc[{t}] += {nme};") for t, nme in enumerate(names)])
     s.append("  }")
     s.append("#pragma unroll")
     s.append(f"  for (int t = 0; t < {nt}; ++t)")
@@ -353,9 +376,7 @@ def gen_eri_class(la, lb, lc, ld):
     s.append(PRIM_HEADER.rstrip("\n"))
     s.append(f"      R F[{L + 1}];")
     s.append(f"      boys.template eval<{L}>(T, pre, F);")
-    s += prim_body
-    for t, n in enumerate(names):
-        s.append(f"      acc[{t}] += {n};")
+    s += interleave_accumulation(prim_body, [(n, f"      acc[{t}] += {n};") for t, n in enumerate(names)])
     s.append("    }")
     s.append("  }")
     s += em2.lines
@@ -600,12 +621,13 @@ def gen_grad_class(la, lb, lc, ld):
     s.append(PRIM_HEADER.rstrip("\n"))
     s.append(f"      R F[{L + 1}];")
     s.append(f"      boys.template eval<{L}>(T, pre, F);")
-    s += prim_body
+    adds = []
     for k, wname in (("U", None), ("A", "wa"), ("B", "wb"), ("C", "wc")):
         for t in order[k]:
             v = vals[t]
-            s.append(f"      acc[{idx[(k, t)]}] += {v};" if wname is None else
-                     f"      acc[{idx[(k, t)]}] += {wname} * {v};")
+            adds.append((v, f"      acc[{idx[(k, t)]}] += {v};" if wname is None else
+                         f"      acc[{idx[(k, t)]}] += {wname} * {v};"))
+    s += interleave_accumulation(prim_body, adds)
     s.append("    }")
     s.append("  }")
     s += em2.lines

@@ -1009,6 +1009,10 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
 // end of each block stays a small number of atomics.
 constexpr int kGradSmemBytes = 24 * 1024;
 constexpr int kGradMaxBlocks = 2048;
+// blocks of a straight-line gradient launch: opts.reserved[1] when set (> 0), else kGradMaxBlocks
+static int grad_max_blocks(const hfgpu_handle* h) {
+  return h->opts.reserved[1] > 0 ? h->opts.reserved[1] : kGradMaxBlocks;
+}
 int grad_smem_atoms(const hfgpu_handle* h) {
   return (size_t)h->natoms * 3 * sizeof(double) <= (size_t)kGradSmemBytes ? h->natoms : 0;
 }
@@ -1106,7 +1110,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
       unsigned char* slice = h->d_scratch.as<unsigned char>() + off;
       cudaStream_t st = fp32 ? st_f : st_d;
       int grid = (nq + 127) / 128;
-      if (slots == 0 && gd.smem_atoms > 0) grid = std::min(grid, kGradMaxBlocks);
+      if (slots == 0 && gd.smem_atoms > 0) grid = std::min(grid, grad_max_blocks(h));
       if (slots > 0) {
         const size_t rb = fp32 ? sizeof(float) : sizeof(double);
         grid = (int)(table_threads(slots, nq) / 128);
@@ -1208,7 +1212,7 @@ int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int n
       const int nq = (int)(hi - lo);
       if (nq <= 0) continue;
       int grid = (nq + 127) / 128;
-      if (slots == 0 && gd.smem_atoms > 0) grid = std::min(grid, kGradMaxBlocks);
+      if (slots == 0 && gd.smem_atoms > 0) grid = std::min(grid, grad_max_blocks(h));
       if (slots > 0) {
         const size_t per_thread = (size_t)slots * (fp32 ? sizeof(float) : sizeof(double));
         const long long fit = (long long)(scratch_bytes / per_thread) / 128 * 128;  // >= 128 (first pass)

@@ -92,7 +92,7 @@ class Engine:
     """One engine handle: a basis on one GPU, with the current geometry."""
 
     def __init__(self, basis: Basis, schwarz_tol=1e-12, density_tol=1e-12, mixed_fp32_bound=1e-4, device=0,
-                 warp_max_quartets=None, grad_warp_max_waves=None, stage_wait_test=False):
+                 warp_max_quartets=None, grad_warp_max_waves=None, stage_wait_test=False, grad_max_blocks=None):
         self.basis = basis
         self.n = basis.nbf
         self._bv = _BasisView(basis)
@@ -105,6 +105,8 @@ class Engine:
             o.grad_warp_max_waves = grad_warp_max_waves
         if stage_wait_test:
             o.reserved[0] = 1  # staging waits run out on purpose (tests the bounded wait)
+        if grad_max_blocks is not None:
+            o.reserved[1] = grad_max_blocks
         self._opts = o
         h = ctypes.c_void_p()
         self._check(lib().hfgpu_create(ctypes.byref(self._bv.s), ctypes.byref(o), ctypes.byref(h)), None)

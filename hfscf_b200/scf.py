@@ -347,60 +347,64 @@ def _rhf_device_loop(basis, engine, dev, *, e_tol, rms_tol, diis_range, max_iter
         C = eps = None
     E = float((D * (H + H)).sum())
     res = ScfResult(0, 0, 0, None, None, None, None, 0, False)
-    Fs, Es, rms_list = [], [], []  # DIIS history
+    # DIIS history in fixed device slots (no host round trip): diis_range + 1 slots; once all
+    # are used, the new vector replaces the slot of the LARGEST rms, which is the reference's
+    # "drop the largest-error entry, then append" (hfscf_diis.cpp:23-41) with the order of the
+    # stored vectors, which the extrapolation does not depend on, left free.
+    cap = diis_range + 1
+    Fs = torch.zeros((cap, n, n), **f64)
+    Es = torch.zeros((cap, n * n), **f64)
+    rms_d = torch.zeros(cap, **f64)
+    used = 0
     F_last = D_last = None
+    ev = []  # CUDA events around every Fock build, read once at the end
     it = 0
     while True:
         it += 1
-        t = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         if incremental and F_last is not None and (it % 8) != 0:
             F = F_last + two_e(D - D_last)
         else:
             F = H + two_e(D)
-        torch.cuda.synchronize(dev)
-        res.fock_times.append(time.perf_counter() - t)
+        e1.record()
+        ev.append((e0, e1))
         F_last, D_last = F, D
-        # DIIS (Diis.extrapolate on the device)
-        if len(rms_list) > diis_range:
-            pos = int(np.argmax(rms_list))
-            del Fs[pos], Es[pos], rms_list[pos]
         FDS = F @ D @ S
         err = X.T @ (FDS - FDS.T) @ X
-        Fs.append(F)
-        Es.append(err)
-        m = len(Es)
-        Bd = torch.stack([e.reshape(-1) for e in Es]) if m > 1 else None
-        Bm = (Bd @ Bd.T) if m > 1 else None
         rms_t = err.square().mean().sqrt()
-        if Bm is not None:
-            vals = torch.cat([rms_t.reshape(1), Bm.reshape(-1)]).cpu().numpy()
+        if used < cap:
+            slot = torch.tensor(used, device=dev)
+            used += 1
         else:
-            vals = rms_t.reshape(1).cpu().numpy()
-        rms = float(vals[0])
-        rms_list.append(rms)
+            slot = torch.argmax(rms_d)
+        Fs.index_copy_(0, slot.reshape(1), F.reshape(1, n, n))
+        Es.index_copy_(0, slot.reshape(1), err.reshape(1, -1))
+        rms_d.index_copy_(0, slot.reshape(1), rms_t.reshape(1))
+        m = used
         if m > 1:
-            B = np.empty((m + 1, m + 1))
-            B[:m, :m] = vals[1:].reshape(m, m)
-            if np.abs(B[:m, :m]).sum() < DIIS_EPS:
-                B[:m, :m] /= B[:m, :m].max()
-            B[m, :] = -1.0
-            B[:, m] = -1.0
+            Bm = Es[:m] @ Es[:m].T
+            Bm = torch.where(Bm.abs().sum() < DIIS_EPS, Bm / Bm.max(), Bm)
+            B = torch.full((m + 1, m + 1), -1.0, **f64)
+            B[:m, :m] = Bm
             B[m, m] = 0.0
-            rhs = np.zeros(m + 1)
+            rhs = torch.zeros(m + 1, **f64)
             rhs[m] = -1.0
-            q, r = np.linalg.qr(B)
-            cvec = np.linalg.solve(r, q.T @ rhs)[:m]
-            F = torch.einsum("k,kij->ij", torch.from_numpy(cvec).to(dev), torch.stack(Fs))
+            cvec = torch.linalg.solve(B, rhs)[:m]
+            F = torch.einsum("k,kij->ij", cvec, Fs[:m])
         eps, Cp = torch.linalg.eigh(X.T @ F @ X)
         C = X @ Cp
         D = C[:, :nocc] @ C[:, :nocc].T
-        E_prev, E = E, float((D * (H + F)).sum())
+        # one host round trip per iteration: the rms and the energy for the convergence test
+        rms, E_new = (float(v) for v in torch.stack([rms_t, (D * (H + F)).sum()]).cpu())
+        E_prev, E = E, E_new
         res.energies.append(E)
         if rms < rms_tol and abs(E - E_prev) < e_tol:
             res.converged = True
             break
         if it >= max_iter:
             break
+    res.fock_times = [a.elapsed_time(b) / 1e3 for a, b in ev]
     F = H + two_e(D)
     E = float((D * (H + F)).sum())
     enuc = nuclear_repulsion(basis.Z, basis.coords)

@@ -74,7 +74,9 @@ typedef struct {
                                  every SM and stop the other classes' kernels from overlapping; 0 = never) */
   int reserved[5];          /* reserved[0] = 1: arm every shared-memory staging wait without issuing its copy,
                               so that the bounded wait runs out (tests the timeout path; builds then report
-                              status 2); 0 otherwise.  reserved[1..4]: 0. */
+                              status 2); 0 otherwise.  reserved[1] > 0: at most this many blocks per
+                              straight-line gradient launch (default 2048; the launch loops over the rest).
+                              reserved[2..4]: 0. */
 } hfgpu_opts;
 
 int hfgpu_default_opts(hfgpu_opts* opts);
