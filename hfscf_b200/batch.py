@@ -100,6 +100,11 @@ class BatchEngine:
                                              ctypes.c_int(repeats), out.ctypes.data_as(eng._ip)))
         return out
 
+    def set_schedule(self, schedule):
+        """hfgpu_set_schedule on the batched handle (HFGPU_NUM_CLASSES x 4 ints)."""
+        sched = np.ascontiguousarray(schedule, dtype=np.int32)
+        self._check(eng.lib().hfgpu_set_schedule(self.h, sched.ctypes.data_as(eng._ip)))
+
     def eigh(self, A, W, V, sweeps=None):
         """hfgpu_batch_eigh: eigenvalues (ascending) and eigenvectors of every molecule's block of
         the padded batch A [nmol, nmax, nmax] (device tensors)."""
@@ -154,13 +159,16 @@ class _Layout:
 
 
 def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-10, rms_tol=1e-8,
-              max_iter=60, use_graph=True, gradient=True, autotune=False, diag="gpu", diis_range=5):
+              max_iter=60, use_graph=True, gradient=True, autotune=False, diag="gpu", diis_range=5,
+              schedule=None):
     """Converged RHF energies (and gradients) of every molecule of the batch.  ``diag``:
     "gpu" diagonalises every molecule's Fock matrix in one launch of the batched Jacobi
     kernel (hfgpu_batch_eigh, molecules of up to 118 functions); "host" runs LAPACK per
     molecule on a host thread pool.  ``autotune`` runs hfgpu_autotune on the first density
     before the graph is captured (off by default: for 512 small molecules it cost 2.4 s and
-    bought nothing over the default schedule)."""
+    bought nothing over the default schedule).  ``schedule``: a launch schedule to use instead
+    (e.g. one the autotuner returned for the same batch in an earlier, untimed run); the result
+    dict's "schedule" is the schedule the run used."""
     dev = torch.device("cuda", device)
     t0 = time.perf_counter()
     stages = {}
@@ -249,9 +257,15 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
         torch.add(Hblk, Jblk, alpha=2.0, out=Fblk)
         Fblk.sub_(Kblk)
 
+    tuned = False
+    if schedule is not None:
+        be.set_schedule(schedule)
+        tuned = True
     build()  # warm-up: loads every kernel before any capture
     tt = stage("guess_and_first_build", tt)
-    schedule = be.autotune(Dblk, precision) if autotune else None
+    if autotune:
+        schedule = be.autotune(Dblk, precision)
+        tuned = True
     tt = stage("autotune", tt)
     graph = None
     if use_graph:
@@ -333,7 +347,7 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     enuc = np.array([nuclear_repulsion(b.Z, b.coords) for b in bases])
     out = {"energies": E_el + enuc, "iterations": it, "converged": converged.cpu().numpy(),
            "setup_s": t_setup, "setup_stages_s": stages, "scf_s": t_scf, "graph": graph is not None,
-           "autotuned": schedule is not None,
+           "autotuned": tuned, "schedule": schedule,
            "build_ms_mean": float(np.mean([a.elapsed_time(b) for a, b in build_events])), "nmol": nmol,
            "final_s": time.perf_counter() - t_fin}
     if gradient:

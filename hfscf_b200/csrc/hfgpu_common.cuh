@@ -275,7 +275,7 @@ struct BoysShared {
 };
 
 // Status codes a kernel leaves in its status word (device int, 0 = fine).
-enum : int { HFGPU_DEV_STAGE_TIMEOUT = 2 };
+enum : int { HFGPU_DEV_STAGE_TIMEOUT = 2, HFGPU_DEV_ABORTED = 3 };
 // Polls of a bounded mbarrier wait (each followed by a short sleep): about 0.1 s in all.
 #define HFGPU_STAGE_MAX_POLLS (1 << 20)
 

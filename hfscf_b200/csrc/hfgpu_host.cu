@@ -153,7 +153,8 @@ struct hfgpu_handle {
   // d_dyn the counts a build's launches process, d_first the first function of every shell
   DevBuf d_launch, d_dyn, d_first;
   // the Boys table in the plane layout of the staged kernels, and the device status word
-  DevBuf d_boys_pd, d_boys_pf, d_status;
+  DevBuf d_boys_pd, d_boys_pf, d_status, d_abort;
+  cudaStream_t ctl_stream = nullptr;  // non-blocking stream of hfgpu_request_abort
   int status_host = 0;  // the status word as the last host-pointer entry point read it
   long long nquartets = 0;
 
@@ -848,6 +849,7 @@ static int status_after_sync(hfgpu_handle* h) {
   h->status_host = 0;
   if (st == HFGPU_DEV_STAGE_TIMEOUT)
     return fail(h, HFGPU_ERR_CUDA, "a shared-memory staging wait ran out (bounded wait); the build is incomplete");
+  if (st == HFGPU_DEV_ABORTED) return fail(h, HFGPU_ERR_STATE, "the build was stopped by hfgpu_request_abort");
   return st == 0 ? HFGPU_OK : fail(h, HFGPU_ERR_CUDA, "device status " + std::to_string(st));
 }
 
@@ -915,6 +917,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   qf.boys_planes = h->d_boys_pf.as<float>();
   qd.status = qf.status = h->d_status.as<int>();
   qd.stage_test = qf.stage_test = h->opts.reserved[0] == 1 ? 1 : 0;
+  qd.abort_flag = qf.abort_flag = h->d_abort.as<int>();
   const int2* q = h->d_quart.as<int2>();
   long long launched = 0;
   // largest classes first so that they overlap the tail of the smaller ones
@@ -1326,7 +1329,8 @@ int hfgpu_create(const hfgpu_basis* b, const hfgpu_opts* opts, hfgpu_handle** ou
   const std::vector<float> bpf = boys_planes(btf);
   if (h->d_boys_d.ensure(sizeof(double) * bt.size()) || h->d_boys_f.ensure(sizeof(float) * btf.size()) ||
       h->d_boys_pd.ensure(sizeof(double) * bpd.size()) || h->d_boys_pf.ensure(sizeof(float) * bpf.size()) ||
-      h->d_status.ensure(sizeof(int)) ||
+      h->d_status.ensure(sizeof(int)) || h->d_abort.ensure(sizeof(int)) ||
+      cudaMemset(h->d_abort.p, 0, sizeof(int)) ||
       cudaMemcpy(h->d_boys_d.p, bt.data(), sizeof(double) * bt.size(), cudaMemcpyHostToDevice) ||
       cudaMemcpy(h->d_boys_f.p, btf.data(), sizeof(float) * btf.size(), cudaMemcpyHostToDevice) ||
       cudaMemcpy(h->d_boys_pd.p, bpd.data(), sizeof(double) * bpd.size(), cudaMemcpyHostToDevice) ||
@@ -1347,7 +1351,7 @@ int hfgpu_destroy(hfgpu_handle* h) {
   for (DevBuf* d : {&h->d_onee, &h->d_pairs, &h->d_prim_d, &h->d_prim_f, &h->d_alpha_d, &h->d_alpha_f, &h->d_boys_d, &h->d_boys_f,
                     &h->d_quart, &h->d_mats, &h->d_half, &h->d_dmax, &h->d_counters, &h->d_grad, &h->d_scratch,
                     &h->d_eri, &h->d_eriq, &h->d_launch, &h->d_dyn, &h->d_first, &h->d_boys_pd,
-                    &h->d_boys_pf, &h->d_status})
+                    &h->d_boys_pf, &h->d_status, &h->d_abort})
     d->release();
   h->d_mol.release();
   if (h->ev[0])
@@ -1358,6 +1362,7 @@ int hfgpu_destroy(hfgpu_handle* h) {
   }
   if (h->fork_ev) cudaEventDestroy(h->fork_ev);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  if (h->ctl_stream) cudaStreamDestroy(h->ctl_stream);
   }  // the caller's current device is restored here, before the handle goes
   delete h;
   return HFGPU_OK;
@@ -1982,6 +1987,17 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
     }
   if ((rc = hfgpu_set_schedule(h, t_tuned <= t_start ? tuned : start))) return rc;
   return schedule ? hfgpu_get_schedule(h, schedule) : HFGPU_OK;
+}
+
+int hfgpu_request_abort(hfgpu_handle* h, int on) {
+  if (!h) return HFGPU_ERR_INVALID;
+  DeviceGuard dev_guard(h);
+  if (dev_guard.rc) return dev_guard.rc;
+  if (!h->ctl_stream) HF_CUDA(h, cudaStreamCreateWithFlags(&h->ctl_stream, cudaStreamNonBlocking));
+  // written on a stream of its own, so that it lands while the handle's stream is busy
+  HF_CUDA(h, cudaMemsetAsync(h->d_abort.p, on ? 0x01 : 0x00, 1, h->ctl_stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->ctl_stream));
+  return HFGPU_OK;
 }
 
 int hfgpu_device_status(hfgpu_handle* h, int* status) {

@@ -247,6 +247,7 @@ struct QuartetArgs {
   const R* boys_planes; // the Boys table in plane layout, one block of boys_plane_bytes<R>() per order
   int* status;          // device status word (HFGPU_DEV_STAGE_TIMEOUT when a staging wait ran out)
   int stage_test;       // 1: arm the staging barrier without a copy, so that its wait runs out (test only)
+  const int* abort_flag;  // device word the host sets to stop persistent launches early (nullptr: none)
 };
 
 // Quartets this launch processes: nq, or the device-side count of a density-screened build.
@@ -351,8 +352,14 @@ __global__ void __launch_bounds__(128) quartet_staged_kernel(QuartetArgs<R> qa, 
   const BoysShared<R, L> boys{tab};
   nq = launch_count(qa, nq);
   const int warps = gridDim.x * (blockDim.x >> 5);
-  for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w * 32 < nq; w += warps)
+  for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w * 32 < nq; w += warps) {
+    // a host request to stop (hfgpu_request_abort) ends the launch between two warp chunks
+    if (qa.abort_flag != nullptr && *reinterpret_cast<const volatile int*>(qa.abort_flag) != 0) {
+      if ((threadIdx.x & 31) == 0 && qa.status != nullptr) atomicExch(qa.status, HFGPU_DEV_ABORTED);
+      break;
+    }
     quartet_thread<LA, LB, LC, LD, R>(qa, boys, quartets, nq, w * 32 + (threadIdx.x & 31));
+  }
 }
 
 // G lanes per quartet (G = 4, 8, 16 or 32) for small classes and quartets with many

@@ -304,6 +304,10 @@ class Engine:
         self._check(lib().hfgpu_device_status(self.h, ctypes.byref(st)))
         return st.value
 
+    def request_abort(self, on=True):
+        """hfgpu_request_abort: set (or reset) the host abort flag of the persistent launches."""
+        self._check(lib().hfgpu_request_abort(self.h, ctypes.c_int(int(on))))
+
     def last_launches(self) -> int:
         k = ctypes.c_int()
         self._check(lib().hfgpu_last_launches(self.h, ctypes.byref(k)))

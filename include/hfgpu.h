@@ -212,10 +212,16 @@ int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms);
 int hfgpu_last_launches(const hfgpu_handle* h, int* kernels);
 /* Device status word of the handle's kernels since the last call, then cleared (synchronises
  * the handle's stream): 0 = fine; 2 = a block's wait for its shared-memory staging copy ran
- * out (bounded at about 0.1 s; the block skipped its quartets, so that build is incomplete).
- * The host-pointer entry points check it themselves and return HFGPU_ERR_CUDA.  No reference
- * counterpart (the reference has no device code). */
+ * out (bounded at about 0.1 s; the block skipped its quartets, so that build is incomplete);
+ * 3 = a persistent launch stopped at a host abort request.  The host-pointer entry points
+ * check it themselves and return HFGPU_ERR_CUDA (2) or HFGPU_ERR_STATE (3).  No reference
+ * counterpart (the reference has no device code and exits on errors). */
 int hfgpu_device_status(hfgpu_handle* h, int* status);
+/* Host abort flag (on = 1) or its reset (on = 0), written on a stream of its own so that it
+ * lands while builds run: the persistent launches (schedule variant 2) stop between two chunks
+ * of 32 quartets and record status 3; a build running then is incomplete.  The flag stays set
+ * until reset.  No reference counterpart. */
+int hfgpu_request_abort(hfgpu_handle* h, int on);
 int hfgpu_fp64_peak(int device, double* tflops);
 /* Boys function F_0..F_m (m <= 10) at count points T >= 0 (host arrays; F is count x (m+1)),
  * through the same table and evaluation the quartet kernels use, in FP64 (HFGPU_FP64) or in

@@ -85,3 +85,27 @@ def test_batched_eigensolver_matches_lapack():
         assert np.abs(Vk.T @ Vk - np.eye(n)).max() < 1e-12
         assert np.abs(A[k, :n, :n] @ Vk - Vk * Wn[k, :n]).max() < 1e-11
         assert (Wn[k, n:] == 1e3).all() and swn[k] < 30
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference library not built")
+def test_batch_energies_match_oracle_scf():
+    """Six molecules of the batched workload's mix (both basis sets), solved together in one
+    batched handle with the autotuned schedule, against an oracle SCF per molecule on the
+    reference's own integrals (1e-8 Eh)."""
+    import oracle
+    from oracle import scf as OS
+    bases = _mols(6, seed=1234)
+    first = batch.batch_rhf(bases, autotune=True, gradient=False, max_iter=2)
+    out = batch.batch_rhf(bases, e_tol=1e-11, rms_tol=1e-9, gradient=False, schedule=first["schedule"])
+    assert out["converged"].all() and out["autotuned"]
+    for m, b in enumerate(bases):
+        S, T, V = oracle.ref_onee(b)
+        eri = oracle.ref_eri_packed(b)
+
+        def jk(D):
+            J, K = oracle.jk_packed(eri, [D])
+            return J[0], K[0]
+
+        ref = OS.rhf(S, T + V, int(sum(b.Z)) // 2, jk, OS.nuclear_repulsion(b.Z, b.coords), rms_tol=1e-9)
+        assert ref["converged"]
+        assert abs(out["energies"][m] - ref["energy"]) < 1e-8, (m, out["energies"][m], ref["energy"])

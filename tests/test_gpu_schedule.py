@@ -154,3 +154,34 @@ def test_staging_wait_runs_out_and_reports():
         J, K = eng.jk(D, [D])
         assert eng.device_status() == 0
     assert np.max(np.abs(J - J0)) < MAT_TOL and np.max(np.abs(K[0] - K0)) < MAT_TOL
+
+
+def test_host_abort_flag_stops_persistent_builds():
+    """hfgpu_request_abort: with the flag set, the persistent launches stop at their first chunk
+    and record status 3 (the host-pointer build then fails with HFGPU_ERR_STATE, a device
+    build reports it through hfgpu_device_status); after the flag is reset the same handle
+    builds the full J and K again."""
+    import torch
+    Z, x = M.water_cluster(3, 2.9, np.random.default_rng(39), 0.1)
+    bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    rng = np.random.default_rng(41)
+    D = _sym(rng, bs.nbf)
+    staged = np.tile(np.array((64, 0, 0, 2), dtype=np.int32), (E.NUM_CLASSES, 1))
+    with E.Engine(bs) as eng:
+        eng.set_schedule(staged)
+        J0, K0 = eng.jk(D, [D])
+        eng.request_abort(True)
+        with pytest.raises(E.HfgpuError) as err:
+            eng.jk(D, [D])
+        assert err.value.code == 4 and "hfgpu_request_abort" in str(err.value)
+        dev = torch.device("cuda", 0)
+        Dd = torch.from_numpy(D).to(dev)
+        J = torch.zeros_like(Dd)
+        K = torch.zeros_like(Dd)
+        torch.cuda.synchronize()
+        eng.jk_device(Dd.data_ptr(), 1, Dd.data_ptr(), J.data_ptr(), K.data_ptr())
+        assert eng.device_status() == 3
+        eng.request_abort(False)
+        J1, K1 = eng.jk(D, [D])
+        assert eng.device_status() == 0
+    assert np.max(np.abs(J1 - J0)) < 1e-12 and np.max(np.abs(K1[0] - K0[0])) < 1e-12
