@@ -942,34 +942,42 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     if (e <= b || !((h->class_mask >> c) & 1u)) continue;
     if (h->timing) HF_CUDA(h, cudaEventRecord(h->ev[2 * c], st));
     // Four parts in list order: [beg,hik1) many-primitive / [hik1,mid) few-primitive (high
-    // bound, FP64), [mid,hik2) / [hik2,end) (low bound, FP32 in mixed mode).  Without density
-    // screening adjacent parts that run the same kernel are launched together; with it every
-    // part is its own launch and processes the device-computed prefix of its decades.
+    // bound, FP64), [mid,hik2) / [hik2,end) (low bound, FP32 in mixed mode).  Adjacent parts
+    // that run the same kernel are launched together.  In a density-screened build each part
+    // keeps the device-computed prefix of its bound decades: the launch gets the parts' offsets
+    // and their slots of the device counts (consecutive, one per part).
     const long long pstart[5] = {b, h->q_hik1[c], m, h->q_hik2[c], e};
-    struct Range { long long lo, hi; bool fp32, many; int slot; };
+    struct Range { long long lo, hi; bool fp32, many; int part0, nseg; long long off[4]; };
     Range rg[4];
     int nr = 0;
     for (int part = 0; part < 4; ++part) {
       const long long lo = pstart[part], hi = pstart[part + 1];
       const bool fp32 = precision == HFGPU_MIXED && part >= 2;
       const bool many = (part % 2) == 0 && L->has_primwarp && h->sched_primwarp[c];
-      if (dmax == nullptr && nr > 0 && rg[nr - 1].hi == lo && rg[nr - 1].fp32 == fp32 && rg[nr - 1].many == many) {
-        rg[nr - 1].hi = hi;  // contiguous and the same kernel: extend
+      if (nr > 0 && rg[nr - 1].hi == lo && rg[nr - 1].fp32 == fp32 && rg[nr - 1].many == many) {
+        Range& r = rg[nr - 1];  // contiguous and the same kernel: extend
+        r.off[r.nseg++] = lo - r.lo;
+        r.hi = hi;
       } else {
-        rg[nr++] = {lo, hi, fp32, many, c * 4 + part};
+        Range& r = rg[nr++];
+        r = Range{lo, hi, fp32, many, part, 1, {0, 0, 0, 0}};
       }
     }
     for (int r = 0; r < nr; ++r) {
-      const int nseg = (int)(rg[r].hi - rg[r].lo);
-      if (nseg <= 0) continue;
+      const int nq_max = (int)(rg[r].hi - rg[r].lo);  // the grid covers every quartet of the parts
+      if (nq_max <= 0) continue;
       const int2* qs = q + rg[r].lo;
-      const int* dyn = dmax != nullptr ? h->d_dyn.as<int>() + rg[r].slot : nullptr;
+      const int* dyn = dmax != nullptr ? h->d_dyn.as<int>() + c * 4 + rg[r].part0 : nullptr;
       if (rg[r].fp32) {
         qf.dyn_nq = dyn;
-        if (!(rg[r].many && L->primwarp_f(qf, qs, nseg, st))) L->quartet_f(qf, qs, nseg, st);
+        qf.nseg = rg[r].nseg;
+        for (int k = 0; k < 4; ++k) qf.seg_off[k] = (int)rg[r].off[k];
+        if (!(rg[r].many && L->primwarp_f(qf, qs, nq_max, st))) L->quartet_f(qf, qs, nq_max, st);
       } else {
         qd.dyn_nq = dyn;
-        if (!(rg[r].many && L->primwarp_d(qd, qs, nseg, st))) L->quartet_d(qd, qs, nseg, st);
+        qd.nseg = rg[r].nseg;
+        for (int k = 0; k < 4; ++k) qd.seg_off[k] = (int)rg[r].off[k];
+        if (!(rg[r].many && L->primwarp_d(qd, qs, nq_max, st))) L->quartet_d(qd, qs, nq_max, st);
       }
       ++kernels;
     }

@@ -241,8 +241,13 @@ struct QuartetArgs {
   int block;            // threads per block of the thread-per-quartet form (32, 64 or 128; 0 = 64)
   int group;            // lanes per quartet of the primitive-split form (4, 8, 16 or 32; 0 = 32)
   int capped;           // 1: the register-capped variant of the thread form (classes that have one)
-  const int* dyn_nq;    // device count of this launch's quartets (<= nq), written by an earlier kernel
-                        // of the same build (density-screened prefix); nullptr: all nq quartets
+  // Density-screened builds: a launch covers up to four consecutive list segments; segment k
+  // starts at seg_off[k] (relative to the launch's list pointer) and only its first dyn_nq[k]
+  // quartets (written on the device by an earlier kernel of the same build) are processed.
+  // dyn_nq == nullptr: all nq quartets.
+  const int* dyn_nq;
+  int nseg;
+  int seg_off[4];
   int staged;           // 1: the persistent form with the Boys table staged in shared memory (low L)
   const R* boys_planes; // the Boys table in plane layout, one block of boys_plane_bytes<R>() per order
   int* status;          // device status word (HFGPU_DEV_STAGE_TIMEOUT when a staging wait ran out)
@@ -250,10 +255,27 @@ struct QuartetArgs {
   const int* abort_flag;  // device word the host sets to stop persistent launches early (nullptr: none)
 };
 
-// Quartets this launch processes: nq, or the device-side count of a density-screened build.
+// Quartets this launch processes: nq, or the sum of the device-side segment counts of a
+// density-screened build.
 template <typename R>
 __device__ __forceinline__ int launch_count(const QuartetArgs<R>& qa, int nq) {
-  return qa.dyn_nq != nullptr ? min(nq, __ldg(qa.dyn_nq)) : nq;
+  if (qa.dyn_nq == nullptr) return nq;
+  int tot = 0;
+  for (int k = 0; k < qa.nseg; ++k) tot += __ldg(qa.dyn_nq + k);
+  return min(nq, tot);
+}
+
+// List position of the launch's t-th processed quartet (t < launch_count): t itself, or, in a
+// density-screened build, the t-th quartet of the segments' kept prefixes in segment order.
+template <typename R>
+__device__ __forceinline__ int quartet_slot(const QuartetArgs<R>& qa, int t) {
+  if (qa.dyn_nq == nullptr) return t;
+  for (int k = 0; k < qa.nseg - 1; ++k) {
+    const int c = __ldg(qa.dyn_nq + k);
+    if (t < c) return qa.seg_off[k] + t;
+    t -= c;
+  }
+  return qa.seg_off[qa.nseg - 1] + t;
 }
 
 // One thread per quartet: quartet t of the launch's list (t >= nq: an idle lane that still
@@ -265,7 +287,7 @@ __device__ __forceinline__ void quartet_thread(const QuartetArgs<R>& qa, const B
   // every lane stays to the end (lanes without work carry valid = false), so
   // that the digestion can use whole-warp shuffles
   const bool in_range = t < nq;
-  const int2 pq = in_range ? quartets[t] : make_int2(0, 0);
+  const int2 pq = in_range ? quartets[quartet_slot(qa, t)] : make_int2(0, 0);
   const PairInfo P = a.pairs[pq.x];
   const PairInfo Q = a.pairs[pq.y];
   bool skip = !in_range;
@@ -378,7 +400,7 @@ __global__ void __launch_bounds__(128) quartet_primwarp_kernel(QuartetArgs<R> qa
   const int qi = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool in_range = qi < nq;
   if (!__any_sync(0xffffffffu, in_range)) return;  // whole warp leaves together
-  const int2 pq = in_range ? quartets[qi] : make_int2(0, 0);
+  const int2 pq = in_range ? quartets[quartet_slot(qa, qi)] : make_int2(0, 0);
   const PairInfo P = a.pairs[pq.x];
   const PairInfo Q = a.pairs[pq.y];
   bool skip = !in_range;
@@ -773,7 +795,7 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
   R* A = hs + Tab::NHSLOT + 1;
   R* Bb = A + Tab::NCART;
   const JKArgs<R>& a = qa.jk;
-  const int2 pq = quartets[qi];
+  const int2 pq = quartets[quartet_slot(qa, qi)];
   const PairInfo P = a.pairs[pq.x];
   const PairInfo Q = a.pairs[pq.y];
   bool skip = false;

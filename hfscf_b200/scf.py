@@ -26,6 +26,7 @@ from . import engine as eng
 from .basis import Basis, nuclear_repulsion, nuclear_repulsion_gradient
 
 DIIS_EPS = 1.0e-14  # src/scfsolver/hfscf_diis.hpp:65
+PURIFY_TOL = 1e-11  # largest |P^2 - P| accepted from the purification before the diagonalisation is used
 
 
 class Diis:
@@ -78,6 +79,7 @@ class ScfResult:
     converged: bool
     fock_times: list = field(default_factory=list)
     energies: list = field(default_factory=list)
+    diag_fallbacks: int = 0  # device loop: iterations whose density came from the diagonalisation
 
 
 class DiisUhf:
@@ -291,6 +293,64 @@ def rhf(basis: Basis, fock=None, *, H=None, S=None, e_tol=1e-10, rms_tol=1e-8, d
     return res
 
 
+class Purifier:
+    """Density matrix of the nocc lowest orbitals of an orthonormal-basis Fock matrix Fo without
+    diagonalising it: trace-correcting purification (TC2; Niklasson, Phys. Rev. B 66, 155115
+    (2002)).  From P0 = (e_max - Fo) / (e_max - e_min) (Gershgorin bounds of the spectrum),
+    P <- P^2 when tr P > nocc, else 2P - P^2; the fixed point is the projector onto the nocc
+    lowest eigenvectors of Fo, i.e. C_occ C_occ^T of the diagonalisation
+    (src/scfsolver/hfscf_hf_solver.cpp:206-231) whenever there is a gap at nocc.  The
+    branch is taken on the device (both candidates formed, one kept), so a fixed number of
+    steps replays from one CUDA graph with no host round trip; the caller checks the
+    idempotency error |P^2 - P|_max once per SCF iteration and falls back to the
+    diagonalisation when it is not small (no gap, or too few steps)."""
+
+    STEPS = 56
+
+    def __init__(self, n, nocc, dev):
+        import torch
+        self.n, self.nocc = n, nocc
+        f64 = dict(dtype=torch.float64, device=dev)
+        self.Fo = torch.zeros((n, n), **f64)
+        self.P = torch.zeros((n, n), **f64)
+        self.err = torch.zeros((), **f64)
+        self.eye = torch.eye(n, **f64)
+        self.graph = None
+        self._run()  # loads every kernel before any capture
+        try:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=torch.cuda.current_stream(dev)):
+                self._run()
+            self.graph = g
+        except Exception:
+            self.graph = None
+
+    def _run(self):
+        import torch
+        Fo = self.Fo
+        r = Fo.abs().sum(dim=1) - Fo.diagonal().abs()
+        emax = (Fo.diagonal() + r).max()
+        emin = (Fo.diagonal() - r).min()
+        P = (emax * self.eye - Fo) / (emax - emin)
+        for _ in range(self.STEPS):
+            P2 = P @ P
+            P = torch.where(P.trace() > self.nocc, P2, 2.0 * P - P2)
+        self.P.copy_(P)
+        self.err.copy_((P @ P - P).abs().max())
+
+    def __call__(self, Fo):
+        """Copies Fo in, runs the steps; returns (P, idempotency error), both on the device."""
+        self.Fo.copy_(Fo)
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._run()
+        return self.P, self.err
+
+    def close(self):
+        self.graph = None
+
+
 def _rhf_device(basis: Basis, engine, *, e_tol, rms_tol, diis_range, max_iter, precision, incremental, D0,
                 guess) -> ScfResult:
     """The loop of rhf() with every matrix on the GPU: J/K through hfgpu_jk_device, the
@@ -351,6 +411,7 @@ def _rhf_device_loop(basis, engine, dev, *, e_tol, rms_tol, diis_range, max_iter
     # are used, the new vector replaces the slot of the LARGEST rms, which is the reference's
     # "drop the largest-error entry, then append" (hfscf_diis.cpp:23-41) with the order of the
     # stored vectors, which the extrapolation does not depend on, left free.
+    purifier = Purifier(n, nocc, dev)
     cap = diis_range + 1
     Fs = torch.zeros((cap, n, n), **f64)
     Es = torch.zeros((cap, n * n), **f64)
@@ -390,13 +451,20 @@ def _rhf_device_loop(basis, engine, dev, *, e_tol, rms_tol, diis_range, max_iter
             B[m, m] = 0.0
             rhs = torch.zeros(m + 1, **f64)
             rhs[m] = -1.0
-            cvec = torch.linalg.solve(B, rhs)[:m]
+            cvec = torch.linalg.solve_ex(B, rhs)[0][:m]  # no host check of the LU info
             F = torch.einsum("k,kij->ij", cvec, Fs[:m])
-        eps, Cp = torch.linalg.eigh(X.T @ F @ X)
-        C = X @ Cp
-        D = C[:, :nocc] @ C[:, :nocc].T
-        # one host round trip per iteration: the rms and the energy for the convergence test
-        rms, E_new = (float(v) for v in torch.stack([rms_t, (D * (H + F)).sum()]).cpu())
+        # the new density: purification of X^T F X (same projector as C_occ C_occ^T), with the
+        # diagonalisation as the fallback when the projector has not converged
+        Pq, perr = purifier(X.T @ F @ X)
+        D = X @ Pq @ X.T
+        # one host round trip per iteration: the rms, the energy and the purification error
+        rms, E_new, pe = (float(v) for v in torch.stack([rms_t, (D * (H + F)).sum(), perr]).cpu())
+        if not pe < PURIFY_TOL:
+            eps, Cp = torch.linalg.eigh(X.T @ F @ X)
+            C = X @ Cp
+            D = C[:, :nocc] @ C[:, :nocc].T
+            E_new = float((D * (H + F)).sum())
+            res.diag_fallbacks += 1
         E_prev, E = E, E_new
         res.energies.append(E)
         if rms < rms_tol and abs(E - E_prev) < e_tol:
@@ -405,8 +473,12 @@ def _rhf_device_loop(basis, engine, dev, *, e_tol, rms_tol, diis_range, max_iter
         if it >= max_iter:
             break
     res.fock_times = [a.elapsed_time(b) / 1e3 for a, b in ev]
+    purifier.close()
     F = H + two_e(D)
     E = float((D * (H + F)).sum())
+    # orbitals and orbital energies once, at the converged density's Fock matrix
+    eps, Cp = torch.linalg.eigh(X.T @ F @ X)
+    C = X @ Cp
     enuc = nuclear_repulsion(basis.Z, basis.coords)
     res.energy, res.e_elec, res.e_nuc = E + enuc, E, enuc
     res.D, res.F, res.C, res.eps = D.cpu().numpy(), F.cpu().numpy(), C.cpu().numpy(), eps.cpu().numpy()
