@@ -109,7 +109,11 @@ class Basis:
         }
 
     def with_coords(self, coords) -> "Basis":
-        return build_basis(self.name, self.Z, coords, pure=self.pure)
+        """The same shells on the atoms moved to `coords` (bohr)."""
+        coords = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
+        out = Basis(self.name, self.pure, self.Z, coords)
+        out.shells = [Shell(s.L, s.atom, coords[s.atom].copy(), s.exps, s.coefs, s.idx, s.ids) for s in self.shells]
+        return out
 
 
 def build_basis(name: str, Z, coords_bohr, pure: bool | None = None) -> Basis:

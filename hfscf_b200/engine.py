@@ -123,6 +123,9 @@ class Engine:
             raise HfgpuError(rc, msg)
 
     def close(self):
+        if getattr(self, "_purifier", None) is not None:
+            self._purifier.close()  # the SCF loop's captured purification graph
+            self._purifier = None
         if getattr(self, "h", None) is not None:
             lib().hfgpu_destroy(self.h)
             self.h = None

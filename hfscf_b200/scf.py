@@ -301,11 +301,13 @@ class Purifier:
     lowest eigenvectors of Fo, i.e. C_occ C_occ^T of the diagonalisation
     (src/scfsolver/hfscf_hf_solver.cpp:206-231) whenever there is a gap at nocc.  The
     branch is taken on the device (both candidates formed, one kept), so a fixed number of
-    steps replays from one CUDA graph with no host round trip; the caller checks the
-    idempotency error |P^2 - P|_max once per SCF iteration and falls back to the
+    steps replays from one CUDA graph with no host round trip.  Past convergence the
+    trace-correcting steps amplify rounding (each flip of the branch doubles it), so P is frozen
+    on the device once tr(P - P^2) = sum lambda (1 - lambda) falls below 1e-11.  The caller
+    checks the idempotency error |P^2 - P|_max once per SCF iteration and falls back to the
     diagonalisation when it is not small (no gap, or too few steps)."""
 
-    STEPS = 56
+    STEPS = 64
 
     def __init__(self, n, nocc, dev):
         import torch
@@ -332,9 +334,11 @@ class Purifier:
         emax = (Fo.diagonal() + r).max()
         emin = (Fo.diagonal() - r).min()
         P = (emax * self.eye - Fo) / (emax - emin)
+        frozen = torch.zeros((), dtype=torch.bool, device=Fo.device)
         for _ in range(self.STEPS):
             P2 = P @ P
-            P = torch.where(P.trace() > self.nocc, P2, 2.0 * P - P2)
+            frozen = frozen | ((P.trace() - P2.trace()) < 1e-11)
+            P = torch.where(frozen, P, torch.where(P.trace() > self.nocc, P2, 2.0 * P - P2))
         self.P.copy_(P)
         self.err.copy_((P @ P - P).abs().max())
 
@@ -411,7 +415,11 @@ def _rhf_device_loop(basis, engine, dev, *, e_tol, rms_tol, diis_range, max_iter
     # are used, the new vector replaces the slot of the LARGEST rms, which is the reference's
     # "drop the largest-error entry, then append" (hfscf_diis.cpp:23-41) with the order of the
     # stored vectors, which the extrapolation does not depend on, left free.
-    purifier = Purifier(n, nocc, dev)
+    # one purifier (and its captured graph) per engine and basis size, reused by later SCF runs
+    purifier = getattr(engine, "_purifier", None)
+    if purifier is None or (purifier.n, purifier.nocc) != (n, nocc):
+        purifier = Purifier(n, nocc, dev)
+        engine._purifier = purifier
     cap = diis_range + 1
     Fs = torch.zeros((cap, n, n), **f64)
     Es = torch.zeros((cap, n * n), **f64)
@@ -473,7 +481,6 @@ def _rhf_device_loop(basis, engine, dev, *, e_tol, rms_tol, diis_range, max_iter
         if it >= max_iter:
             break
     res.fock_times = [a.elapsed_time(b) / 1e3 for a, b in ev]
-    purifier.close()
     F = H + two_e(D)
     E = float((D * (H + F)).sum())
     # orbitals and orbital energies once, at the converged density's Fock matrix
