@@ -648,7 +648,6 @@ def classes():
 
 
 GRAD_STRAIGHT_MAX_VRR = 900   # larger gradient classes run in table mode
-GRAD_WARP_MIN_ACC = 150       # straight-line gradient classes with this many accumulators also get the warp form
 
 
 def class_args_sig():
@@ -726,9 +725,10 @@ def class_header(c):
     mg["table"] = not straight
     # the op-table classes also get the warp-per-quartet form (measured faster than one thread
     # per quartet on global scratch for every one of them; the straight-line classes stay threads)
-    # and so do the straight-line classes whose per-thread accumulators spill (GRAD_WARP_MIN_ACC);
-    # the host picks the form per launch (opts.grad_warp_max_waves)
-    gwarp = not straight or mg["accumulators"] >= GRAD_WARP_MIN_ACC
+    # (the straight-line classes keep one thread per quartet: warp forms generated for those with
+    # more than 150 accumulators measured slower at n-octane and anthracene sizes, 29.6 against
+    # 25.7 ms and 216 against 189 ms per gradient)
+    gwarp = not straight
     if gwarp:
         gwcode, gwmeta = gen_grad_warp(*c)
         parts += [gwcode, ""]

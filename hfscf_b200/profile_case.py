@@ -2,6 +2,7 @@
 
     python -m hfscf_b200.profile_case jk   --workload 2 [--precision mixed] [--repeat 3]
     python -m hfscf_b200.profile_case grad --workload 3 [--repeat 1]
+    python -m hfscf_b200.profile_case jk   --workload 2 --variant 2   (every class in the staged form)
 
 Builds the named workload's basis (``molecules.workload``: 1 = H2O/cc-pVDZ,
 2 = n-octane/6-31G**, 3 = anthracene/cc-pVDZ, 4 = (H2O)8/6-31G*), forms the
@@ -41,6 +42,9 @@ def main(argv=None):
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--autotune", action="store_true", help="hfgpu_autotune first (as bench.py does)")
+    ap.add_argument("--variant", type=int, choices=(0, 1, 2), default=None,
+                    help="thread-form variant for every class (schedule column 3: 0 plain, 1 capped, "
+                         "2 staged persistent)")
     a = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("profile_case needs a CUDA device")
@@ -57,6 +61,10 @@ def main(argv=None):
         Dd = torch.from_numpy(np.ascontiguousarray(D)).to(dev)
         if a.autotune:
             eng.autotune(Dd, E.FP64, 3)
+        if a.variant is not None:
+            sched = eng.get_schedule()
+            sched[:, 3] = a.variant
+            eng.set_schedule(sched)
         n = bs.nbf
         J = torch.empty((n, n), dtype=torch.float64, device=dev)
         K = torch.empty((n, n), dtype=torch.float64, device=dev)
