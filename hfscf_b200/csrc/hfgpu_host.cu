@@ -154,6 +154,7 @@ struct hfgpu_handle {
   DevBuf d_launch, d_dyn, d_first;
   // the Boys table in the plane layout of the staged kernels, and the device status word
   DevBuf d_boys_pd, d_boys_pf, d_status, d_abort;
+  DevBuf d_purify;  // workspace of hfgpu_purify_device
   cudaStream_t ctl_stream = nullptr;  // non-blocking stream of hfgpu_request_abort
   int status_host = 0;  // the status word as the last host-pointer entry point read it
   long long nquartets = 0;
@@ -770,6 +771,97 @@ void boys_eval_dispatch(int m, const R* tab, const double* T, long long count, d
   }
 }
 
+// ---------------------------------------------------------------------------
+// Density by trace-correcting purification (TC2; Niklasson, Phys. Rev. B 66, 155115 (2002)) of
+// an orthonormal-basis Fock matrix, for the SCF loop: the projector onto the nocc lowest
+// eigenvectors without a diagonalisation.  Workspace (doubles): A, C (n x n each), then per
+// step k: tr A_k, tr A_k^2, and a frozen flag f_k (as a double), then emin, emax.
+//   purify_bounds_kernel   Gershgorin bounds of Fo (one block), zeroes the per-step slots;
+//   purify_init_kernel     A_0 = (emax I - Fo) / (emax - emin);
+//   purify_square_kernel   C = A_k A_k (16 x 16 output tiles, shared-memory k tiles), and the
+//                          traces of A_k and C from the diagonal tiles; skipped once frozen;
+//   purify_update_kernel   frozen_{k+1} = frozen_k or tr A_k - tr A_k^2 < tol;
+//                          A_{k+1} = A_k if frozen, C if tr A_k > nocc, else 2 A_k - C.
+// Every step reads the slots of its own index only, so no kernel reads what it writes.
+// ---------------------------------------------------------------------------
+constexpr int kPurifyTile = 16;
+
+__global__ void purify_bounds_kernel(const double* __restrict__ F, int n, double* __restrict__ slots, int nslot,
+                                     double* __restrict__ bounds) {
+  __shared__ double smin[1024], smax[1024];
+  double lo = 1e300, hi = -1e300;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double r = 0.0;
+    for (int j = 0; j < n; ++j)
+      if (j != i) r += fabs(F[(size_t)i * n + j]);
+    lo = fmin(lo, F[(size_t)i * n + i] - r);
+    hi = fmax(hi, F[(size_t)i * n + i] + r);
+  }
+  smin[threadIdx.x] = lo;
+  smax[threadIdx.x] = hi;
+  for (int i = threadIdx.x; i < nslot; i += blockDim.x) slots[i] = 0.0;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off) {
+      smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + off]);
+      smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + off]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    bounds[0] = smin[0];
+    bounds[1] = smax[0];
+  }
+}
+
+__global__ void purify_init_kernel(const double* __restrict__ F, int n, const double* __restrict__ bounds,
+                                   double* __restrict__ A) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n * n) return;
+  const int i = (int)(e / n), j = (int)(e % n);
+  const double emin = bounds[0], emax = bounds[1];
+  A[e] = ((i == j ? emax : 0.0) - F[e]) / (emax - emin);
+}
+
+__global__ void __launch_bounds__(kPurifyTile * kPurifyTile) purify_square_kernel(const double* __restrict__ A, int n,
+                                                                                   double* __restrict__ C,
+                                                                                   double* __restrict__ step) {
+  if (step[2] != 0.0) return;  // frozen: nothing to compute
+  __shared__ double ta[kPurifyTile][kPurifyTile + 1], tb[kPurifyTile][kPurifyTile + 1];
+  const int tx = threadIdx.x % kPurifyTile, ty = threadIdx.x / kPurifyTile;
+  const int row = blockIdx.y * kPurifyTile + ty, col = blockIdx.x * kPurifyTile + tx;
+  double acc = 0.0;
+  for (int k0 = 0; k0 < n; k0 += kPurifyTile) {
+    ta[ty][tx] = (row < n && k0 + tx < n) ? A[(size_t)row * n + k0 + tx] : 0.0;
+    tb[ty][tx] = (k0 + ty < n && col < n) ? A[(size_t)(k0 + ty) * n + col] : 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kPurifyTile; ++k) acc = fma(ta[ty][k], tb[k][tx], acc);
+    __syncthreads();
+  }
+  if (row < n && col < n) {
+    C[(size_t)row * n + col] = acc;
+    if (row == col) {
+      atomicAdd(step + 0, A[(size_t)row * n + col]);
+      atomicAdd(step + 1, acc);
+    }
+  }
+}
+
+__global__ void purify_update_kernel(double* __restrict__ A, const double* __restrict__ C, int n, int nocc,
+                                     double tol, const double* __restrict__ step, double* __restrict__ next,
+                                     double* __restrict__ err) {
+  const bool frozen = step[2] != 0.0 || (step[0] - step[1]) < tol;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e == 0) {
+    next[2] = frozen ? 1.0 : 0.0;
+    // error report: tr A - tr A^2 (= sum lambda (1 - lambda)) of the step that froze, else 1
+    if (err != nullptr) *err = frozen ? (step[2] != 0.0 ? *err : step[0] - step[1]) : 1.0;
+  }
+  if (frozen || e >= (long long)n * n) return;
+  A[e] = step[0] > (double)nocc ? C[e] : 2.0 * A[e] - C[e];
+}
+
 // FP64 FMA throughput probe: 8 independent FMA chains per thread.
 __global__ void fp64_peak_kernel(double* out, int iters, double a, double b) {
   double x[8];
@@ -1359,7 +1451,7 @@ int hfgpu_destroy(hfgpu_handle* h) {
   for (DevBuf* d : {&h->d_onee, &h->d_pairs, &h->d_prim_d, &h->d_prim_f, &h->d_alpha_d, &h->d_alpha_f, &h->d_boys_d, &h->d_boys_f,
                     &h->d_quart, &h->d_mats, &h->d_half, &h->d_dmax, &h->d_counters, &h->d_grad, &h->d_scratch,
                     &h->d_eri, &h->d_eriq, &h->d_launch, &h->d_dyn, &h->d_first, &h->d_boys_pd,
-                    &h->d_boys_pf, &h->d_status, &h->d_abort})
+                    &h->d_boys_pf, &h->d_status, &h->d_abort, &h->d_purify})
     d->release();
   h->d_mol.release();
   if (h->ev[0])
@@ -2005,6 +2097,31 @@ int hfgpu_request_abort(hfgpu_handle* h, int on) {
   // written on a stream of its own, so that it lands while the handle's stream is busy
   HF_CUDA(h, cudaMemsetAsync(h->d_abort.p, on ? 0x01 : 0x00, 1, h->ctl_stream));
   HF_CUDA(h, cudaStreamSynchronize(h->ctl_stream));
+  return HFGPU_OK;
+}
+
+int hfgpu_purify_device(hfgpu_handle* h, const double* Fo, int n, int nocc, int max_steps, double* P,
+                        double* err) {
+  if (!h || !Fo || !P || !err || n <= 0 || nocc < 0 || nocc > n || max_steps <= 0 || max_steps > 256)
+    return fail(h, HFGPU_ERR_INVALID, "bad purification arguments");
+  if (n > 4096) return fail(h, HFGPU_ERR_UNSUPPORTED, "purification: n > 4096");
+  DeviceGuard dev_guard(h);
+  if (dev_guard.rc) return dev_guard.rc;
+  const size_t nn = (size_t)n * n;
+  const int nslot = 3 * (max_steps + 1);
+  HF_CUDA(h, h->d_purify.ensure(sizeof(double) * (nn + nslot + 2)));
+  double* C = h->d_purify.as<double>();
+  double* slots = C + nn;
+  double* bounds = slots + nslot;
+  purify_bounds_kernel<<<1, 1024, 0, h->stream>>>(Fo, n, slots, nslot, bounds);
+  const int eb = (int)((nn + 255) / 256);
+  purify_init_kernel<<<eb, 256, 0, h->stream>>>(Fo, n, bounds, P);
+  const dim3 tiles((n + kPurifyTile - 1) / kPurifyTile, (n + kPurifyTile - 1) / kPurifyTile);
+  for (int k = 0; k < max_steps; ++k) {
+    purify_square_kernel<<<tiles, kPurifyTile * kPurifyTile, 0, h->stream>>>(P, n, C, slots + 3 * k);
+    purify_update_kernel<<<eb, 256, 0, h->stream>>>(P, C, n, nocc, 1e-11, slots + 3 * k, slots + 3 * (k + 1), err);
+  }
+  HF_CHECK_LAUNCH(h, "purification");
   return HFGPU_OK;
 }
 

@@ -123,9 +123,6 @@ class Engine:
             raise HfgpuError(rc, msg)
 
     def close(self):
-        if getattr(self, "_purifier", None) is not None:
-            self._purifier.close()  # the SCF loop's captured purification graph
-            self._purifier = None
         if getattr(self, "h", None) is not None:
             lib().hfgpu_destroy(self.h)
             self.h = None
@@ -306,6 +303,12 @@ class Engine:
         st = ctypes.c_int()
         self._check(lib().hfgpu_device_status(self.h, ctypes.byref(st)))
         return st.value
+
+    def purify_device(self, Fo_ptr, n, nocc, max_steps, P_ptr, err_ptr):
+        """hfgpu_purify_device: P = projector onto the nocc lowest eigenvectors of Fo (device)."""
+        self._check(lib().hfgpu_purify_device(self.h, ctypes.c_void_p(Fo_ptr), ctypes.c_int(n), ctypes.c_int(nocc),
+                                              ctypes.c_int(max_steps), ctypes.c_void_p(P_ptr),
+                                              ctypes.c_void_p(err_ptr)))
 
     def request_abort(self, on=True):
         """hfgpu_request_abort: set (or reset) the host abort flag of the persistent launches."""

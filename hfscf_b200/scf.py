@@ -26,7 +26,8 @@ from . import engine as eng
 from .basis import Basis, nuclear_repulsion, nuclear_repulsion_gradient
 
 DIIS_EPS = 1.0e-14  # src/scfsolver/hfscf_diis.hpp:65
-PURIFY_TOL = 1e-11  # largest |P^2 - P| accepted from the purification before the diagonalisation is used
+PURIFY_TOL = 1e-10  # largest tr P - tr P^2 accepted from the purification before the diagonalisation is used
+PURIFY_STEPS = 64   # squarings of one purification (it stops changing P once converged)
 
 
 class Diis:
@@ -293,68 +294,6 @@ def rhf(basis: Basis, fock=None, *, H=None, S=None, e_tol=1e-10, rms_tol=1e-8, d
     return res
 
 
-class Purifier:
-    """Density matrix of the nocc lowest orbitals of an orthonormal-basis Fock matrix Fo without
-    diagonalising it: trace-correcting purification (TC2; Niklasson, Phys. Rev. B 66, 155115
-    (2002)).  From P0 = (e_max - Fo) / (e_max - e_min) (Gershgorin bounds of the spectrum),
-    P <- P^2 when tr P > nocc, else 2P - P^2; the fixed point is the projector onto the nocc
-    lowest eigenvectors of Fo, i.e. C_occ C_occ^T of the diagonalisation
-    (src/scfsolver/hfscf_hf_solver.cpp:206-231) whenever there is a gap at nocc.  The
-    branch is taken on the device (both candidates formed, one kept), so a fixed number of
-    steps replays from one CUDA graph with no host round trip.  Past convergence the
-    trace-correcting steps amplify rounding (each flip of the branch doubles it), so P is frozen
-    on the device once tr(P - P^2) = sum lambda (1 - lambda) falls below 1e-11.  The caller
-    checks the idempotency error |P^2 - P|_max once per SCF iteration and falls back to the
-    diagonalisation when it is not small (no gap, or too few steps)."""
-
-    STEPS = 64
-
-    def __init__(self, n, nocc, dev):
-        import torch
-        self.n, self.nocc = n, nocc
-        f64 = dict(dtype=torch.float64, device=dev)
-        self.Fo = torch.zeros((n, n), **f64)
-        self.P = torch.zeros((n, n), **f64)
-        self.err = torch.zeros((), **f64)
-        self.eye = torch.eye(n, **f64)
-        self.graph = None
-        self._run()  # loads every kernel before any capture
-        try:
-            g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g, stream=torch.cuda.current_stream(dev)):
-                self._run()
-            self.graph = g
-        except Exception:
-            self.graph = None
-
-    def _run(self):
-        import torch
-        Fo = self.Fo
-        r = Fo.abs().sum(dim=1) - Fo.diagonal().abs()
-        emax = (Fo.diagonal() + r).max()
-        emin = (Fo.diagonal() - r).min()
-        P = (emax * self.eye - Fo) / (emax - emin)
-        frozen = torch.zeros((), dtype=torch.bool, device=Fo.device)
-        for _ in range(self.STEPS):
-            P2 = P @ P
-            frozen = frozen | ((P.trace() - P2.trace()) < 1e-11)
-            P = torch.where(frozen, P, torch.where(P.trace() > self.nocc, P2, 2.0 * P - P2))
-        self.P.copy_(P)
-        self.err.copy_((P @ P - P).abs().max())
-
-    def __call__(self, Fo):
-        """Copies Fo in, runs the steps; returns (P, idempotency error), both on the device."""
-        self.Fo.copy_(Fo)
-        if self.graph is not None:
-            self.graph.replay()
-        else:
-            self._run()
-        return self.P, self.err
-
-    def close(self):
-        self.graph = None
-
-
 def _rhf_device(basis: Basis, engine, *, e_tol, rms_tol, diis_range, max_iter, precision, incremental, D0,
                 guess) -> ScfResult:
     """The loop of rhf() with every matrix on the GPU: J/K through hfgpu_jk_device, the
@@ -415,11 +354,8 @@ def _rhf_device_loop(basis, engine, dev, *, e_tol, rms_tol, diis_range, max_iter
     # are used, the new vector replaces the slot of the LARGEST rms, which is the reference's
     # "drop the largest-error entry, then append" (hfscf_diis.cpp:23-41) with the order of the
     # stored vectors, which the extrapolation does not depend on, left free.
-    # one purifier (and its captured graph) per engine and basis size, reused by later SCF runs
-    purifier = getattr(engine, "_purifier", None)
-    if purifier is None or (purifier.n, purifier.nocc) != (n, nocc):
-        purifier = Purifier(n, nocc, dev)
-        engine._purifier = purifier
+    Pq = torch.empty((n, n), **f64)
+    perr = torch.zeros((), **f64)
     cap = diis_range + 1
     Fs = torch.zeros((cap, n, n), **f64)
     Es = torch.zeros((cap, n * n), **f64)
@@ -461,9 +397,12 @@ def _rhf_device_loop(basis, engine, dev, *, e_tol, rms_tol, diis_range, max_iter
             rhs[m] = -1.0
             cvec = torch.linalg.solve_ex(B, rhs)[0][:m]  # no host check of the LU info
             F = torch.einsum("k,kij->ij", cvec, Fs[:m])
-        # the new density: purification of X^T F X (same projector as C_occ C_occ^T), with the
-        # diagonalisation as the fallback when the projector has not converged
-        Pq, perr = purifier(X.T @ F @ X)
+        # the new density: trace-correcting purification of X^T F X on the device
+        # (hfgpu_purify_device; the same projector as C_occ C_occ^T of the diagonalisation of
+        # src/scfsolver/hfscf_hf_solver.cpp:206-231), with the diagonalisation as the fallback
+        # when the projector has not converged (no gap at nocc)
+        Fo = (X.T @ F @ X).contiguous()
+        engine.purify_device(Fo.data_ptr(), n, nocc, PURIFY_STEPS, Pq.data_ptr(), perr.data_ptr())
         D = X @ Pq @ X.T
         # one host round trip per iteration: the rms, the energy and the purification error
         rms, E_new, pe = (float(v) for v in torch.stack([rms_t, (D * (H + F)).sum(), perr]).cpu())

@@ -194,6 +194,15 @@ int hfgpu_one_electron_device(hfgpu_handle* h, const double* Z, double* S, doubl
 int hfgpu_one_electron_grad_device(hfgpu_handle* h, const double* Z, const double* D, const double* W, double cH,
                                    double cS, double* grad);
 
+/* SCF density without a diagonalisation: P (n x n, device) = the projector onto the nocc lowest
+ * eigenvectors of the symmetric orthonormal-basis Fock matrix Fo (device), by trace-correcting
+ * purification (at most max_steps <= 256 squarings; it stops changing P once tr P - tr P^2 <
+ * 1e-11).  *err (device double) receives that tr P - tr P^2 at convergence, or 1 if it did not
+ * converge in max_steps (then diagonalise instead).  Replaces the diagonalisation of
+ * Mol::hf_solver::calc_density_matrix (src/scfsolver/hfscf_hf_solver.cpp:206-231) for a
+ * closed-shell density: C_occ C_occ^T is that projector.  Enqueued on the handle's stream. */
+int hfgpu_purify_device(hfgpu_handle* h, const double* Fo, int n, int nocc, int max_steps, double* P, double* err);
+
 /* Counters of the last J/K build: quartets launched and quartets skipped by density screening. */
 int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* skipped);
 

@@ -148,3 +148,50 @@ def test_setup_times_and_list_segments_cover_every_screened_quartet():
     prod = np.outer(q, q)
     iu = np.triu_indices(len(q))
     assert listed == int(np.count_nonzero(prod[iu] >= 1e-12))
+
+
+@pytest.mark.parametrize("n,nocc", [(7, 3), (152, 40), (210, 33)])
+def test_purification_matches_the_diagonalisation_projector(n, nocc):
+    """hfgpu_purify_device: the projector onto the nocc lowest eigenvectors of a symmetric matrix
+    with a gap, against numpy's eigh (1e-10), and a reported trace error below 1e-10."""
+    import torch
+    rng = np.random.default_rng(n)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    w = np.sort(np.concatenate([rng.uniform(-40.0, -0.3, nocc), rng.uniform(0.2, 6.0, n - nocc)]))
+    Fo = (Q * w) @ Q.T
+    Fo = 0.5 * (Fo + Fo.T)
+    P0 = Q[:, :nocc] @ Q[:, :nocc].T
+    Z, x = M.water(rng)
+    bs = B.build_basis("sto-3g", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR)
+    dev = torch.device("cuda", 0)
+    with E.Engine(bs) as eng:
+        F = torch.from_numpy(Fo).to(dev)
+        P = torch.empty_like(F)
+        err = torch.zeros((), dtype=torch.float64, device=dev)
+        eng.purify_device(F.data_ptr(), n, nocc, 64, P.data_ptr(), err.data_ptr())
+        torch.cuda.synchronize()
+        assert float(err) < 1e-10
+        assert np.max(np.abs(P.cpu().numpy() - P0)) < 1e-10
+
+
+def test_purification_reports_a_missing_gap():
+    """Two equal eigenvalues at the Fermi level: no projector separates them, the purification
+    does not converge and says so (err = 1), so the SCF diagonalises instead.  (24 steps: far
+    more would let rounding split the pair, 2^-53 doubling each step.)"""
+    import torch
+    n, nocc = 12, 5
+    rng = np.random.default_rng(3)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    w = np.array([-9.0, -7.0, -5.0, -3.0, -1.0, -1.0, 1.0, 2.0, 3.0, 4.0, 5.0, 6.0])
+    Fo = (Q * w) @ Q.T
+    Fo = 0.5 * (Fo + Fo.T)
+    Z, x = M.water(rng)
+    bs = B.build_basis("sto-3g", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR)
+    dev = torch.device("cuda", 0)
+    with E.Engine(bs) as eng:
+        F = torch.from_numpy(Fo).to(dev)
+        P = torch.empty_like(F)
+        err = torch.zeros((), dtype=torch.float64, device=dev)
+        eng.purify_device(F.data_ptr(), n, nocc, 24, P.data_ptr(), err.data_ptr())
+        torch.cuda.synchronize()
+        assert float(err) >= 1e-10
