@@ -637,6 +637,73 @@ def gen_grad_class(la, lb, lc, ld):
     return "\n".join(s), meta
 
 
+GRAD_SETS = ("U", "A", "B", "C")
+
+
+def gen_grad_class_pass(la, lb, lc, ld, pset):
+    """The part of gen_grad_class that one accumulator set carries: the VRR (one order higher)
+    of the set's targets only, the set's accumulation (weight 1, 2 alpha_a, 2 alpha_b or
+    2 alpha_c), its HRR, and the gradient terms that read it -- for A, B, C the
+    2 alpha (a+1_i b|cd)-type terms of that centre; for U the -a_i (a-1_i b|cd)-type terms of all
+    three centres.  The four passes add up to the whole gradient; each keeps about a quarter
+    of the accumulators of the one-pass form, at the price of recomputing the shared part of
+    the recurrence."""
+    L = la + lb + lc + ld + 1
+    em = Emitter("      ")
+    vrr = VRR(em)
+    order = grad_sets(la, lb, lc, ld)[pset]
+    vals = {t: vrr.get(t[0], t[1], 0) for t in order}
+    prim_body = list(em.lines)
+    idx = {t: i for i, t in enumerate(order)}
+    nacc = len(order)
+    em2 = Emitter("  ")
+    hr = HRR(em2, lambda e, f: f"acc[{idx[(e, f)]}]", prefix=f"h{pset}")
+    gt = grad_terms(la, lb, lc, ld)
+    outs = {}
+    for (cen, dr), items in gt.items():
+        terms = []
+        for wi, tl in items:
+            for coef, st, a, b, c, d in tl:
+                if st != pset:
+                    continue
+                v = hr.bra(a, b, c, d)
+                terms.append(f"W[{wi}] * {v}" if coef == 1 else f"{lit(coef)} * W[{wi}] * {v}")
+        outs[(cen, dr)] = terms
+    for (cen, dr), terms in outs.items():
+        em2.emit(f"g{cen}[{dr}] = " + (" + ".join(terms) if terms else "R(0)") + ";", 3 * len(terms))
+    wname = {"U": None, "A": "wa", "B": "wb", "C": "wc"}[pset]
+    fn = f"grad_{la}{lb}{lc}{ld}_{pset}"
+    s = [f"// adjoint gradient of ({'spdf'[la]}{'spdf'[lb]}|{'spdf'[lc]}{'spdf'[ld]}), set {pset} only: {nacc} "
+         f"accumulators, {len(vrr.memo)} VRR values"]
+    s.append("template <typename R>")
+    s.append(f"__device__ __forceinline__ void {fn}({GRAD_SIG}) {{")
+    s.append(f"  R acc[{nacc}];")
+    s.append("#pragma unroll")
+    s.append(f"  for (int t = 0; t < {nacc}; ++t) acc[t] = R(0);")
+    s.append("  for (int ib = 0; ib < nbp; ++ib) {")
+    s.append("    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
+    s.append("    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;")
+    s.append("    const R wa = R(2) * ea[ib], wb = R(2) * eb[ib];")
+    s.append("    (void)wa; (void)wb;")
+    s.append("    for (int ik = 0; ik < nkp; ++ik) {")
+    s.append("      const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
+    s.append("      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;")
+    s.append("      const R wc = R(2) * ec[ik];")
+    s.append("      (void)wc;")
+    s.append(PRIM_HEADER.rstrip("\n"))
+    s.append(f"      R F[{L + 1}];")
+    s.append(f"      boys.template eval<{L}>(T, pre, F);")
+    adds = [(vals[t], f"      acc[{idx[t]}] += {vals[t]};" if wname is None else
+             f"      acc[{idx[t]}] += {wname} * {vals[t]};") for t in order]
+    s += interleave_accumulation(prim_body, adds)
+    s.append("    }")
+    s.append("  }")
+    s += em2.lines
+    s.append("}")
+    return "\n".join(s), {"accumulators": nacc, "vrr_values": len(vrr.memo), "prim_flops": em.flops,
+                          "hrr_flops": em2.flops}
+
+
 def classes():
     pairs = [(a, b) for a in range(LMAX + 1) for b in range(a + 1)]  # ss ps pp ds dp dd
     out = []
@@ -648,6 +715,7 @@ def classes():
 
 
 GRAD_STRAIGHT_MAX_VRR = 900   # larger gradient classes run in table mode
+GRAD_SPLIT_MIN_ACC = 150      # straight-line gradient classes with this many accumulators run as 4 passes
 
 
 def class_args_sig():
@@ -759,9 +827,27 @@ def class_header(c):
     parts.append(f"  static __device__ __forceinline__ void to_pure(const R* __restrict__ in, R* __restrict__ out) {{ to_pure_{t}<R>(in, out); }}")
     parts.append("  template <typename R>")
     parts.append(f"  static __device__ __forceinline__ void from_pure(const R* __restrict__ in, R* __restrict__ out) {{ from_pure_{t}<R>(in, out); }}")
+    # the straight-line classes whose one-pass accumulators spill run as four passes, one
+    # accumulator set each (gen_grad_class_pass)
+    npass = 4 if straight and mg["accumulators"] >= GRAD_SPLIT_MIN_ACC else 1
+    mg["passes"] = npass
+    parts.append(f"  static constexpr int kGradPasses = {npass};")
     if straight:
         parts.append("  template <typename R>")
         parts.append(f"  static __device__ __forceinline__ void grad({GRAD_SIG}) {{ grad_{t}<R>({GRAD_ARGS}); }}")
+    if npass > 1:
+        pcodes = []
+        for pi, ps in enumerate(GRAD_SETS):
+            pcode, pm = gen_grad_class_pass(la, lb, lc, ld, ps)
+            pcodes += [pcode, ""]
+            mg[f"pass_{ps}"] = pm
+        at = parts.index("template <>")  # the pass functions go before the ClassCode specialisation
+        parts[at:at] = pcodes
+        parts.append("  template <typename R, int PASS>")
+        parts.append(f"  static __device__ __forceinline__ void grad_pass({GRAD_SIG}) {{")
+        for pi, ps in enumerate(GRAD_SETS):
+            parts.append(f"    if constexpr (PASS == {pi}) grad_{t}_{ps}<R>({GRAD_ARGS});")
+        parts.append("  }")
     parts.append("};")
     return "\n".join(parts) + "\n", m, mg
 
@@ -844,7 +930,16 @@ static bool launch_primwarp(const QuartetArgs<R>& a, const int2* q, int nq, cuda
 template <typename R>
 static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, int grid, cudaStream_t s) {{
   if (nq <= 0) return;
-  grad_kernel<{la}, {lb}, {lc}, {ld}, R><<<grid, 128, sizeof(double) * 3 * a.smem_atoms, s>>>(a, pure, q, nq);
+  const size_t sm = sizeof(double) * 3 * a.smem_atoms;
+  if constexpr (ClassCode<{la}, {lb}, {lc}, {ld}>::kGradPasses == 4) {{
+    // one launch per accumulator set, one after the other on the stream; each adds its part
+    grad_kernel<{la}, {lb}, {lc}, {ld}, R, 0><<<grid, 128, sm, s>>>(a, pure, q, nq);
+    grad_kernel<{la}, {lb}, {lc}, {ld}, R, 1><<<grid, 128, sm, s>>>(a, pure, q, nq);
+    grad_kernel<{la}, {lb}, {lc}, {ld}, R, 2><<<grid, 128, sm, s>>>(a, pure, q, nq);
+    grad_kernel<{la}, {lb}, {lc}, {ld}, R, 3><<<grid, 128, sm, s>>>(a, pure, q, nq);
+  }} else {{
+    grad_kernel<{la}, {lb}, {lc}, {ld}, R><<<grid, 128, sm, s>>>(a, pure, q, nq);
+  }}
 }}
 template <typename CC, typename R>
 static bool launch_grad_warp_impl(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{

@@ -560,7 +560,9 @@ __device__ __forceinline__ void grad_weights(const double* __restrict__ DJ, doub
     }
 }
 
-template <int LA, int LB, int LC, int LD, typename R, bool PURE>
+// PASS < 0: the whole gradient of the quartet; PASS = 0..3: the part that accumulator set
+// U, A, B or C carries (classes generated with kGradPasses = 4 run one launch per pass).
+template <int LA, int LB, int LC, int LD, typename R, bool PURE, int PASS = -1>
 __device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, const int2 pq, double* gout) {
   using Dm = BlockDims<LA, LB, LC, LD, PURE>;
   using CC = ClassCode<LA, LB, LC, LD>;
@@ -637,9 +639,16 @@ __device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, cons
         grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(off_ptr(a.DJ, gblk), a.cJ, a.nK, off_ptr(a.DK, gblk), a.cK, gnm, P.fa, P.fb,
                                                      Q.fa, Q.fb, s, Wc);
       }
-      CC::template grad<R>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
-                           a.prims + Q.prim_off, a.alpha_a + Q.prim_off, Q.nprim, R(P.ABx), R(P.ABy), R(P.ABz),
-                           R(Q.ABx), R(Q.ABy), R(Q.ABz), a.boys, Wc, g, g + 3, g + 6);
+      if constexpr (PASS >= 0) {
+        CC::template grad_pass<R, PASS>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off,
+                                        P.nprim, a.prims + Q.prim_off, a.alpha_a + Q.prim_off, Q.nprim, R(P.ABx),
+                                        R(P.ABy), R(P.ABz), R(Q.ABx), R(Q.ABy), R(Q.ABz), a.boys, Wc, g, g + 3,
+                                        g + 6);
+      } else {
+        CC::template grad<R>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
+                             a.prims + Q.prim_off, a.alpha_a + Q.prim_off, Q.nprim, R(P.ABx), R(P.ABy), R(P.ABz),
+                             R(Q.ABx), R(Q.ABy), R(Q.ABz), a.boys, Wc, g, g + 3, g + 6);
+      }
     }
     const int at[3] = {P.atom_a, P.atom_b, Q.atom_a};
 #pragma unroll
@@ -657,7 +666,7 @@ __device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, cons
 // those are millions of atomics on a few dozen addresses, serialised in L2; with
 // a.smem_atoms > 0 each block sums into shared memory first and adds its 3 natoms totals
 // once at the end.
-template <int LA, int LB, int LC, int LD, typename R>
+template <int LA, int LB, int LC, int LD, typename R, int PASS = -1>
 __global__ void __launch_bounds__(128) grad_kernel(GradArgs<R> a, int pure, const int2* __restrict__ quartets, int nq) {
   extern __shared__ double grad_sh[];
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -671,9 +680,9 @@ __global__ void __launch_bounds__(128) grad_kernel(GradArgs<R> a, int pure, cons
   }
   for (int t = tid; t < nq; t += nthr) {
     if (pure)
-      grad_quartet<LA, LB, LC, LD, R, true>(a, tid, quartets[t], gout);
+      grad_quartet<LA, LB, LC, LD, R, true, PASS>(a, tid, quartets[t], gout);
     else
-      grad_quartet<LA, LB, LC, LD, R, false>(a, tid, quartets[t], gout);
+      grad_quartet<LA, LB, LC, LD, R, false, PASS>(a, tid, quartets[t], gout);
   }
   if (nsh > 0) {
     __syncthreads();
