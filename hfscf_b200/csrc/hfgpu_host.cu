@@ -177,6 +177,10 @@ struct hfgpu_handle {
   // warp-per-quartet form (-1 = follow opts.warp_max_quartets)
   int sched_block[21], sched_primwarp[21], sched_warp[21], sched_cap[21];
   unsigned class_mask = ~0u;            // classes a J/K build launches (autotuning runs one at a time)
+  // gradient form per class (hfgpu_autotune_grad): 1 warp per quartet, 0 one thread per
+  // quartet, -1 the quartet-count rule of opts.grad_warp_max_waves
+  int grad_form[21];
+  unsigned grad_class_mask = ~0u;       // classes a gradient launches (autotuning runs one at a time)
 
   hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21) {
     for (int c = 0; c < 21; ++c) {
@@ -184,6 +188,7 @@ struct hfgpu_handle {
       sched_primwarp[c] = 0;
       sched_warp[c] = c < hfgpu::kNumClasses && hfgpu::kClassLaunchers[c]->warp_default ? -1 : 0;
       sched_cap[c] = 0;
+      grad_form[c] = -1;
     }
   }
 };
@@ -1122,9 +1127,11 @@ int grad_smem_atoms(const hfgpu_handle* h) {
 
 static bool grad_use_warp(const hfgpu_handle* h, int c, long long nq, bool fp32) {
   const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
-  if (!L->has_grad_warp || h->opts.grad_warp_max_waves <= 0) return false;
+  if (!L->has_grad_warp) return false;
   const int bytes = L->grad_warp_bytes(fp32 ? 1 : 0);
   if (bytes <= 0 || bytes > 232448) return false;
+  if (h->grad_form[c] >= 0) return h->grad_form[c] == 1;  // chosen by hfgpu_autotune_grad
+  if (h->opts.grad_warp_max_waves <= 0) return false;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
   const long long per_sm = std::min(32, 233472 / (bytes + 1024));  // 228 KB per SM, 1 KB reserved per block
@@ -1194,7 +1201,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
     const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
-    if (e <= b) continue;
+    if (e <= b || !((h->grad_class_mask >> c) & 1u)) continue;
     const int slots = L->grad_scratch_slots(h->pure);
     cudaStream_t st_d = h->aux[rr++ % hfgpu_handle::kAux];
     cudaStream_t st_f = precision == HFGPU_MIXED ? h->aux[rr++ % hfgpu_handle::kAux] : st_d;
@@ -2097,6 +2104,60 @@ int hfgpu_request_abort(hfgpu_handle* h, int on) {
   // written on a stream of its own, so that it lands while the handle's stream is busy
   HF_CUDA(h, cudaMemsetAsync(h->d_abort.p, on ? 0x01 : 0x00, 1, h->ctl_stream));
   HF_CUDA(h, cudaStreamSynchronize(h->ctl_stream));
+  return HFGPU_OK;
+}
+
+int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int repeats, int* forms) {
+  if (!h || !D) return HFGPU_ERR_INVALID;
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
+  if (rc) return rc;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  repeats = std::max(1, std::min(repeats, 100));
+  DevBuf g;
+  HF_CUDA(h, g.ensure(sizeof(double) * 3 * std::max(h->natoms, 1)));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  HF_CUDA(h, cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(h, HFGPU_ERR_CUDA, "cudaEventCreate");
+  }
+  struct Restore {  // the class mask goes back on every exit path
+    hfgpu_handle* h;
+    cudaEvent_t a, b;
+    ~Restore() {
+      h->grad_class_mask = ~0u;
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } restore{h, e0, e1};
+  // RHF weights (cJ = 2, cK = 1) on the given density, one class at a time, each form timed
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
+    if (!L->has_grad_warp || h->q_end[c] <= h->q_beg[c]) continue;
+    h->grad_class_mask = 1u << c;
+    float best = 1e30f;
+    int best_form = 0;
+    for (int form = 0; form < 2; ++form) {
+      h->grad_form[c] = form;
+      if ((rc = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return rc;  // warm-up
+      HF_CUDA(h, cudaEventRecord(e0, h->stream));
+      for (int r = 0; r < repeats; ++r)
+        if ((rc = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return rc;
+      HF_CUDA(h, cudaEventRecord(e1, h->stream));
+      HF_CUDA(h, cudaEventSynchronize(e1));
+      float ms = 0.f;
+      HF_CUDA(h, cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best) {
+        best = ms;
+        best_form = form;
+      }
+    }
+    h->grad_form[c] = best_form;
+  }
+  if (forms)
+    for (int c = 0; c < hfgpu::kNumClasses; ++c) forms[c] = h->grad_form[c];
+  g.release();
   return HFGPU_OK;
 }
 

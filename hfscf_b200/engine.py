@@ -289,6 +289,16 @@ class Engine:
                                          ctypes.c_int(repeats), out.ctypes.data_as(_ip)))
         return out
 
+    def autotune_grad(self, D, precision=FP64, repeats=2) -> np.ndarray:
+        """hfgpu_autotune_grad on density D (host array or device tensor): the gradient form per
+        class (1 warp, 0 thread, -1 no choice)."""
+        import torch
+        Dd = D if isinstance(D, torch.Tensor) else torch.from_numpy(_c(D)).to(torch.device("cuda", self._opts.device))
+        forms = np.zeros(NUM_CLASSES, dtype=np.int32)
+        self._check(lib().hfgpu_autotune_grad(self.h, ctypes.c_void_p(Dd.data_ptr()), ctypes.c_int(precision),
+                                              ctypes.c_int(repeats), forms.ctypes.data_as(_ip)))
+        return forms
+
     def get_schedule(self) -> np.ndarray:
         out = np.zeros((NUM_CLASSES, 4), dtype=np.int32)
         self._check(lib().hfgpu_get_schedule(self.h, out.ctypes.data_as(_ip)))

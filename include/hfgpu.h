@@ -264,6 +264,13 @@ int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
 #define HFGPU_NUM_CLASSES 21
 int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule);
 int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule);
+/* Gradient form per class for the classes that have both (the op-table classes (dp|dp) (dd|pp)
+ * (dd|ds) (dd|dp) (dd|dd)): times one warp per quartet against one thread per quartet for each
+ * class alone on the handle's lists and the given device density D (RHF weights), keeps the
+ * faster, and returns it in forms[HFGPU_NUM_CLASSES] (1 warp, 0 thread, -1 class without a
+ * choice; may be NULL).  Until it runs, opts.grad_warp_max_waves decides by quartet count.
+ * Results do not depend on the form beyond FP64 summation order. */
+int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int repeats, int* forms);
 int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule);
 
 #ifdef __cplusplus

@@ -185,3 +185,17 @@ def test_host_abort_flag_stops_persistent_builds():
         J1, K1 = eng.jk(D, [D])
         assert eng.device_status() == 0
     assert np.max(np.abs(J1 - J0)) < 1e-12 and np.max(np.abs(K1[0] - K0[0])) < 1e-12
+
+
+def test_gradient_form_autotuner_keeps_the_gradient():
+    """hfgpu_autotune_grad picks, per op-table class, warp or thread form; the gradient after
+    tuning equals the oracle's (FP64, 1e-10)."""
+    rng = np.random.default_rng(43)
+    bs = MOLS[1][1]  # methane cc-pVDZ: d shells, every op-table class present
+    D = _sym(rng, bs.nbf)
+    g0 = oracle.grad2e_rhf(bs, D)
+    with E.Engine(bs) as eng:
+        forms = eng.autotune_grad(D, repeats=1)
+        assert set(np.unique(forms)) <= {-1, 0, 1} and (forms >= 0).any()
+        g = eng.grad2e(D)
+    assert np.max(np.abs(g - g0)) < 1e-10
