@@ -760,6 +760,7 @@ def cap_blocks(vrr_values):
 
 
 STAGED_MAX_L = 4          # classes that also get the persistent form with the Boys table in shared memory
+LOWRES_MIN_VRR = 250      # classes that also get the low-residency thread variant (their registers spill)
 WARP_MIN_VRR = 250        # classes that also get a warp-per-quartet form (hfgpu_autotune picks)
 WARP_DEFAULT_MIN_VRR = 1000  # (dd|dp) and (dd|dd): measured faster as one warp per quartet by default
 
@@ -814,6 +815,8 @@ def class_header(c):
     parts.append(f"  static constexpr int kCapBlocks = {cap_blocks(m['vrr_values'])};")
     # the persistent form with the Boys table in shared memory: classes of total L <= STAGED_MAX_L
     parts.append(f"  static constexpr bool kStaged = {'true' if la + lb + lc + ld <= STAGED_MAX_L else 'false'};")
+    # the low-residency variant of the thread form: the classes whose register code spills
+    parts.append(f"  static constexpr bool kLowRes = {'true' if m['vrr_values'] >= LOWRES_MIN_VRR else 'false'};")
     if primwarp:
         parts.append(f"  template <typename R, int G>")
         parts.append(f"  static __device__ __forceinline__ void eri_pw({class_args_sig()}, int lane) {{")
@@ -882,6 +885,16 @@ static void launch_quartet_impl(const QuartetArgs<R>& a, const int2* q, int nq, 
   }}
   bool warp = false;
   if constexpr (CC::kWarp) warp = nq <= a.warp_max;
+  if (!warp && a.capped == 3) {{
+    // low residency: the launch reserves (unused) shared memory so that at most two blocks share
+    // an SM; the spilled stacks of the large-register classes then stay inside L2
+    const int bs = a.block > 0 ? a.block : 64;
+    const int pad = 100 * 1024;
+    auto k = quartet_kernel<{la}, {lb}, {lc}, {ld}, R>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, pad);
+    k<<<(nq + bs - 1) / bs, bs, pad, s>>>(a, q, nq);
+    return;
+  }}
   if (!warp) {{
     const int bs = a.block > 0 ? a.block : 64;
     if constexpr (CC::kCapBlocks > 0) {{
@@ -994,7 +1007,8 @@ const ClassLaunchers launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_quartet<d
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kGradWarp,
                                       &launch_grad_warp<double>, &launch_grad_warp<float>, &grad_warp_bytes,
                                       ClassCode<{la}, {lb}, {lc}, {ld}>::kCapBlocks > 0,
-                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kStaged}};
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kStaged,
+                                      ClassCode<{la}, {lb}, {lc}, {ld}>::kLowRes}};
 }}  // namespace hfgpu
 """
 

@@ -1926,7 +1926,7 @@ int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule) {
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     const int bs = schedule[4 * c], pw = schedule[4 * c + 1], wp = schedule[4 * c + 2], cp = schedule[4 * c + 3];
     if ((bs != 32 && bs != 64 && bs != 128) || (pw != 0 && pw != 1 && pw != 4 && pw != 8 && pw != 16 && pw != 32) ||
-        wp < -1 || wp > 1 || cp < 0 || cp > 2)
+        wp < -1 || wp > 1 || cp < 0 || cp > 3)
       return fail(h, HFGPU_ERR_INVALID, "schedule entry out of range");
   }
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
@@ -2000,10 +2000,11 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
       for (int pi = (L->has_primwarp ? 0 : 4); pi < 5; ++pi) {
         const int pw = pws[pi];
         // thread-form variants: plain (0), register-capped (1), persistent with the Boys table
-        // staged in shared memory (2)
-        for (int cand = 0; cand < 9; ++cand) {
+        // staged in shared memory (2), at most two blocks per SM (3, the classes that spill)
+        for (int cand = 0; cand < 12; ++cand) {
           const int bs = 32 << (cand % 3), cap = cand / 3;
-          if ((cap == 1 && !L->has_capped) || (cap == 2 && !L->has_staged)) continue;
+          if ((cap == 1 && !L->has_capped) || (cap == 2 && !L->has_staged) || (cap == 3 && !L->has_lowres))
+            continue;
           if (wp == 1 && (bs != 64 || cap)) continue;  // the warp form has its own block shape
           h->sched_block[c] = bs;
           h->sched_primwarp[c] = L->has_primwarp ? pw : 1;
@@ -2154,6 +2155,33 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
       }
     }
     h->grad_form[c] = best_form;
+  }
+  // Classes were timed alone; in a gradient they run concurrently on several streams, where the
+  // slower form of a class can overlap the others better.  Refinement on whole gradients: per
+  // class the other form replaces the chosen one if the whole gradient gets at least 1% faster.
+  h->grad_class_mask = ~0u;
+  auto time_all = [&](float* ms) -> int {
+    int r0;
+    if ((r0 = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return r0;  // warm-up
+    HF_CUDA(h, cudaEventRecord(e0, h->stream));
+    for (int r = 0; r < repeats; ++r)
+      if ((r0 = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return r0;
+    HF_CUDA(h, cudaEventRecord(e1, h->stream));
+    HF_CUDA(h, cudaEventSynchronize(e1));
+    HF_CUDA(h, cudaEventElapsedTime(ms, e0, e1));
+    return HFGPU_OK;
+  };
+  float cur = 0.f;
+  if ((rc = time_all(&cur))) return rc;
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    if (h->grad_form[c] < 0) continue;
+    h->grad_form[c] ^= 1;
+    float ms = 0.f;
+    if ((rc = time_all(&ms))) return rc;
+    if (ms < 0.99f * cur)
+      cur = ms;
+    else
+      h->grad_form[c] ^= 1;
   }
   if (forms)
     for (int c = 0; c < hfgpu::kNumClasses; ++c) forms[c] = h->grad_form[c];

@@ -27,6 +27,7 @@ struct ClassLaunchers {
   int (*grad_warp_bytes)(int fp32);      // shared memory of one warp-form block (0: no warp form)
   bool has_capped;                       // register-capped variant of the thread-per-quartet form
   bool has_staged;                       // persistent thread form with the Boys table in shared memory
+  bool has_lowres;                       // low-residency variant of the thread form (classes that spill)
 };
 
 extern const ClassLaunchers* const kClassLaunchers[];

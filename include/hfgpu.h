@@ -252,7 +252,9 @@ int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
  *   [3] variant of the thread-per-quartet form: 0 plain; 1 register-capped, for more warps
  *       per SM (the small classes (ps|ss) ... (dp|ss) have one); 2 persistent, with the
  *       class's Boys table staged into shared memory by one bulk (TMA) copy per block (the
- *       classes of total angular momentum <= 4 have one); classes without the variant ignore it.
+ *       classes of total angular momentum <= 4 have one); 3 at most two blocks per SM, so that
+ *       the spilled registers of the large classes stay in L2 (classes with 250 or more VRR
+ *       values have one); classes without the variant ignore it.
  * Default: 64, 0, -1 for (dd|dp) and (dd|dd) else 0, 0.
  * autotune: times every form of every class on the current geometry with device density D
  * (n x n; `repeats` builds per candidate, one class at a time on the handle's stream),
@@ -267,8 +269,9 @@ int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule);
 /* Gradient form per class for the classes that have both (the op-table classes (dp|dp) (dd|pp)
  * (dd|ds) (dd|dp) (dd|dd)): times one warp per quartet against one thread per quartet for each
  * class alone on the handle's lists and the given device density D (RHF weights), keeps the
- * faster, and returns it in forms[HFGPU_NUM_CLASSES] (1 warp, 0 thread, -1 class without a
- * choice; may be NULL).  Until it runs, opts.grad_warp_max_waves decides by quartet count.
+ * faster; then, on whole gradients, flips each class's form where that makes the gradient at
+ * least 1% faster (the classes run concurrently), and returns the forms in
+ * forms[HFGPU_NUM_CLASSES] (1 warp, 0 thread, -1 class without a choice; may be NULL).  Until it runs, opts.grad_warp_max_waves decides by quartet count.
  * Results do not depend on the form beyond FP64 summation order. */
 int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int repeats, int* forms);
 int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule);

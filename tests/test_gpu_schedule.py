@@ -36,7 +36,7 @@ MOLS = _molecules()
 # (block, primwarp, warp, capped) applied to every class
 # capped = 2: the persistent form with the Boys table staged in shared memory (classes of L <= 4)
 FORMS = [(32, 0, 0, 0), (64, 1, 0, 1), (128, 0, 1, 0), (64, 1, 1, 0), (64, 4, 0, 1), (32, 8, 1, 1), (128, 16, 0, 0),
-         (64, 0, 0, 2), (128, 4, 0, 2), (32, 0, 1, 2)]
+         (64, 0, 0, 2), (128, 4, 0, 2), (32, 0, 1, 2), (64, 0, 0, 3), (128, 0, -1, 3)]
 
 
 @pytest.mark.parametrize("form", FORMS, ids=[f"b{f[0]}-pw{f[1]}-w{f[2]}-c{f[3]}" for f in FORMS])
@@ -79,7 +79,7 @@ def test_autotuned_schedule_gives_the_same_fock_build():
         assert sched.shape == (E.NUM_CLASSES, 4)
         assert set(np.unique(sched[:, 0])) <= {32, 64, 128}
         assert set(np.unique(sched[:, 1])) <= {0, 1, 4, 8, 16, 32} and set(np.unique(sched[:, 2])) <= {-1, 0, 1}
-        assert set(np.unique(sched[:, 3])) <= {0, 1, 2}
+        assert set(np.unique(sched[:, 3])) <= {0, 1, 2, 3}
         assert (eng.get_schedule() == sched).all()
         F1 = eng.fock_rhf(D, H)
         Fm1 = eng.fock_rhf(D, H, E.MIXED)
