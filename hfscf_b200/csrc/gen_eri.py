@@ -802,6 +802,11 @@ def class_header(c):
         gwcode, gwmeta = gen_grad_warp(*c)
         parts += [gwcode, ""]
         mg["grad_warp"] = gwmeta
+        # and the per-set split of the warp form: four one-set tables, four launches
+        for ps in GRAD_SETS:
+            pcode, pmeta = gen_grad_warp(*c, sets=(ps,), suffix="_" + ps)
+            parts += [pcode, ""]
+            mg["grad_warp_" + ps] = pmeta
     parts.append(f"template <>")
     parts.append(f"struct ClassCode<{la}, {lb}, {lc}, {ld}> {{")
     parts.append(f"  static constexpr bool kGradTable = {'false' if straight else 'true'};")
@@ -811,6 +816,8 @@ def class_header(c):
     parts.append(f"  using GradTab = {'void' if straight else 'GradTable' + t};")
     parts.append(f"  static constexpr bool kGradWarp = {'true' if gwarp else 'false'};")
     parts.append(f"  using GradWarpTab = {'GradWarpTab' + t if gwarp else 'void'};")
+    for pi, ps in enumerate(GRAD_SETS):
+        parts.append(f"  using GradWarpTabP{pi} = {'GradWarpTab' + t + '_' + ps if gwarp else 'void'};")
     parts.append(f"  static constexpr bool kPrimWarp = {'true' if primwarp else 'false'};")
     parts.append(f"  static constexpr int kCapBlocks = {cap_blocks(m['vrr_values'])};")
     # the persistent form with the Boys table in shared memory: classes of total L <= STAGED_MAX_L
@@ -954,16 +961,26 @@ static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, i
     grad_kernel<{la}, {lb}, {lc}, {ld}, R><<<grid, 128, sm, s>>>(a, pure, q, nq);
   }}
 }}
+template <typename Tab, typename R>
+static bool launch_grad_warp_tab(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{
+  constexpr size_t bytes = sizeof(R) * (size_t)grad_warp_slots<Tab, R>();
+  if (bytes > 232448) return false;  // more shared memory than one block may have
+  auto k = grad_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  k<<<nq, 32, bytes, s>>>(a, pure, q, nq);
+  return true;
+}}
 template <typename CC, typename R>
 static bool launch_grad_warp_impl(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{
   if constexpr (CC::kGradWarp) {{
-    using Tab = typename CC::GradWarpTab;
-    constexpr size_t bytes = sizeof(R) * (size_t)grad_warp_slots<Tab, R>();
-    if (bytes > 232448) return false;  // more shared memory than one block may have
-    auto k = grad_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    k<<<nq, 32, bytes, s>>>(a, pure, q, nq);
-    return true;
+    if (a.warp_split) {{
+      // one launch per accumulator set (smaller tables: more warps per SM); each adds its part
+      return launch_grad_warp_tab<typename CC::GradWarpTabP0, R>(a, pure, q, nq, s) &&
+             launch_grad_warp_tab<typename CC::GradWarpTabP1, R>(a, pure, q, nq, s) &&
+             launch_grad_warp_tab<typename CC::GradWarpTabP2, R>(a, pure, q, nq, s) &&
+             launch_grad_warp_tab<typename CC::GradWarpTabP3, R>(a, pure, q, nq, s);
+    }}
+    return launch_grad_warp_tab<typename CC::GradWarpTab, R>(a, pure, q, nq, s);
   }} else {{
     return false;
   }}
@@ -1413,23 +1430,25 @@ def _alloc_levels_with_readers(order_by_level, deps_of, lev, pre_slots, live_to_
     return slot, top
 
 
-def gen_grad_warp(la, lb, lc, ld):
+def gen_grad_warp(la, lb, lc, ld, sets=("U", "A", "B", "C"), suffix=""):
     """Adjoint gradient of one quartet by one warp: the VRR one order higher and the HRR of
-    the four weighted sets are levelised (an op's inputs come from earlier levels), so the
+    the weighted sets are levelised (an op's inputs come from earlier levels), so the
     32 lanes run one level's ops in parallel out of shared memory; the contractions with
-    the weight block W are ops of the HRR levels that only read."""
+    the weight block W are ops of the HRR levels that only read.  `sets` restricts the table to
+    some of the four accumulator sets (one pass of the per-set split: the terms that read those
+    sets only, so the four one-set tables add up to the whole gradient)."""
     L = la + lb + lc + ld + 1
     order = grad_sets(la, lb, lc, ld)
     dag = Dag(L)
     setoff, nacc = {}, 0
-    for k in ("U", "A", "B", "C"):
+    for k in sets:
         setoff[k] = nacc
         nacc += len(order[k])
     acc_src, acc_set = [], []
-    for si, k in enumerate(("U", "A", "B", "C")):
+    for k in sets:
         for (e, f) in order[k]:
             acc_src.append(dag.get(e, f, 0))
-            acc_set.append(si)
+            acc_set.append(("U", "A", "B", "C").index(k))
     ops = [(nid, nd) for nid, nd in enumerate(dag.nodes) if nd[0] != "F"]
     deps = {nid: [x for x in nd[2:7] if x >= 0] for nid, nd in ops}
     lev = _levelise([(nid, deps[nid]) for nid, _ in ops], L + 1)
@@ -1490,16 +1509,18 @@ def gen_grad_warp(la, lb, lc, ld):
     for (cen, dr), items in grad_terms(la, lb, lc, ld).items():
         gi = "ABC".index(cen) * 3 + dr
         for wi, terms in items:
-            x = bra(terms[0][1], *terms[0][2:])
-            if len(terms) > 1:
+            x = bra(terms[0][1], *terms[0][2:]) if terms[0][1] in sets else -1
+            if len(terms) > 1 and "U" in sets:
                 y, kk = bra("U", *terms[1][2:]), -terms[1][0]
             else:
                 y, kk = -1, 0
+            if x < 0 and y < 0:
+                continue
             cops.append((gi, wi, x, y, kk))
     hord = sorted(hinfo)
     hlev = _levelise([(v, hdeps[v]) for v in hord], nacc)
-    clev = [1 + max(hlev[x], hlev[y] if y >= 0 else 0) for (_, _, x, y, _) in cops]
-    readers = [(l, [x] + ([y] if y >= 0 else [])) for l, (_, _, x, y, _) in zip(clev, cops)]
+    clev = [1 + max(hlev[x] if x >= 0 else 0, hlev[y] if y >= 0 else 0) for (_, _, x, y, _) in cops]
+    readers = [(l, ([x] if x >= 0 else []) + ([y] if y >= 0 else [])) for l, (_, _, x, y, _) in zip(clev, cops)]
     hpre = {j: j for j in range(nacc)}
     hslot, nhs = _alloc_levels_with_readers(sorted(hord, key=lambda v: (hlev[v], v)), hdeps, hlev, hpre, set(),
                                             readers)
@@ -1513,12 +1534,12 @@ def gen_grad_warp(la, lb, lc, ld):
             cur += 1
         if is_c:
             gi, wi, x, y, kk = cops[v]
-            hrows.append((2 | (gi << 2) | (kk << 6), wi, hslot[x], hslot[y] if y >= 0 else ZH))
+            hrows.append((2 | (gi << 2) | (kk << 6), wi, hslot[x] if x >= 0 else ZH, hslot[y] if y >= 0 else ZH))
         else:
             kind, i, x, y = hinfo[v]
             hrows.append((kind | (i << 2), hslot[v], hslot[x], hslot[y]))
     hlv.append(len(hrows))
-    t = f"{la}{lb}{lc}{ld}"
+    t = f"{la}{lb}{lc}{ld}{suffix}"
     ncart_blk = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
     s = [f"// warp-mode adjoint gradient of class {t}: {len(vrows)} VRR ops in {len(vlev) - 1} levels over "
          f"{nvs} slots, {nacc} accumulators, {len(hrows)} HRR/contraction ops in {len(hlv) - 1} levels over "

@@ -1130,7 +1130,7 @@ static bool grad_use_warp(const hfgpu_handle* h, int c, long long nq, bool fp32)
   if (!L->has_grad_warp) return false;
   const int bytes = L->grad_warp_bytes(fp32 ? 1 : 0);
   if (bytes <= 0 || bytes > 232448) return false;
-  if (h->grad_form[c] >= 0) return h->grad_form[c] == 1;  // chosen by hfgpu_autotune_grad
+  if (h->grad_form[c] >= 0) return h->grad_form[c] >= 1;  // chosen by hfgpu_autotune_grad
   if (h->opts.grad_warp_max_waves <= 0) return false;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
@@ -1208,6 +1208,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     auto run = [&](bool fp32, long long lo, long long hi) -> int {
       const int nq = (int)(hi - lo);
       if (nq <= 0) return HFGPU_OK;
+      gd.warp_split = gf.warp_split = h->grad_form[c] == 2 ? 1 : 0;
       if (grad_use_warp(h, c, e - b, fp32)) {
         const bool done = fp32 ? L->grad_warp_f(gf, h->pure, q + lo, nq, fp32 ? st_f : st_d)
                                : L->grad_warp_d(gd, h->pure, q + lo, nq, st_d);
@@ -2108,6 +2109,15 @@ int hfgpu_request_abort(hfgpu_handle* h, int on) {
   return HFGPU_OK;
 }
 
+int hfgpu_set_grad_forms(hfgpu_handle* h, const int* forms) {
+  if (!h || !forms) return HFGPU_ERR_INVALID;
+  for (int c = 0; c < hfgpu::kNumClasses; ++c)
+    if (forms[c] < -1 || forms[c] > 2) return fail(h, HFGPU_ERR_INVALID, "gradient form out of range");
+  for (int c = 0; c < hfgpu::kNumClasses; ++c)
+    h->grad_form[c] = hfgpu::kClassLaunchers[c]->has_grad_warp ? forms[c] : -1;
+  return HFGPU_OK;
+}
+
 int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int repeats, int* forms) {
   if (!h || !D) return HFGPU_ERR_INVALID;
   DeviceGuard dev_guard(h);
@@ -2139,7 +2149,7 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
     h->grad_class_mask = 1u << c;
     float best = 1e30f;
     int best_form = 0;
-    for (int form = 0; form < 2; ++form) {
+    for (int form = 0; form < 3; ++form) {  // thread, warp, warp split into four one-set passes
       h->grad_form[c] = form;
       if ((rc = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return rc;  // warm-up
       HF_CUDA(h, cudaEventRecord(e0, h->stream));
@@ -2175,13 +2185,18 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
   if ((rc = time_all(&cur))) return rc;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     if (h->grad_form[c] < 0) continue;
-    h->grad_form[c] ^= 1;
-    float ms = 0.f;
-    if ((rc = time_all(&ms))) return rc;
-    if (ms < 0.99f * cur)
-      cur = ms;
-    else
-      h->grad_form[c] ^= 1;
+    const int keep = h->grad_form[c];
+    for (int form = 0; form < 3; ++form) {
+      if (form == keep) continue;
+      const int before = h->grad_form[c];
+      h->grad_form[c] = form;
+      float ms = 0.f;
+      if ((rc = time_all(&ms))) return rc;
+      if (ms < 0.99f * cur)
+        cur = ms;
+      else
+        h->grad_form[c] = before;
+    }
   }
   if (forms)
     for (int c = 0; c < hfgpu::kNumClasses; ++c) forms[c] = h->grad_form[c];

@@ -53,6 +53,7 @@ struct GradArgs {
   int scratch_threads;               // threads sharing the scratch (stride)
   int smem_atoms;                    // grad_kernel: > 0 = accumulate 3 x smem_atoms entries per block in
                                      // shared memory, then one atomic per entry (0: atomics into grad)
+  int warp_split;                    // grad_warp_kernel: 1 = four launches, one accumulator set each
 };
 
 template <int NA, int NB, int NC, int ND>

@@ -291,13 +291,18 @@ class Engine:
 
     def autotune_grad(self, D, precision=FP64, repeats=2) -> np.ndarray:
         """hfgpu_autotune_grad on density D (host array or device tensor): the gradient form per
-        class (1 warp, 0 thread, -1 no choice)."""
+        class (0 thread, 1 warp, 2 warp split per accumulator set, -1 no choice)."""
         import torch
         Dd = D if isinstance(D, torch.Tensor) else torch.from_numpy(_c(D)).to(torch.device("cuda", self._opts.device))
         forms = np.zeros(NUM_CLASSES, dtype=np.int32)
         self._check(lib().hfgpu_autotune_grad(self.h, ctypes.c_void_p(Dd.data_ptr()), ctypes.c_int(precision),
                                               ctypes.c_int(repeats), forms.ctypes.data_as(_ip)))
         return forms
+
+    def set_grad_forms(self, forms):
+        """hfgpu_set_grad_forms: the gradient form per class (-1, 0 thread, 1 warp, 2 warp split)."""
+        f = np.ascontiguousarray(np.broadcast_to(np.asarray(forms, dtype=np.int32), (NUM_CLASSES,)))
+        self._check(lib().hfgpu_set_grad_forms(self.h, f.ctypes.data_as(_ip)))
 
     def get_schedule(self) -> np.ndarray:
         out = np.zeros((NUM_CLASSES, 4), dtype=np.int32)
