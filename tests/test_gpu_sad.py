@@ -1,5 +1,6 @@
 """SAD guess (Mol::hf_solver::get_sad_guess, src/scfsolver/hfscf_hf_solver.cpp:478-553)
-on the GPU engine against the same atomic UHF run with the oracle's J/K, and SCF from
+on the GPU engine against the oracle's restatement of the atomic UHF on the reference's own
+integrals, and SCF from
 it against SCF from the core guess.  The guess comparison converges both atomic UHF runs
 tightly (rms 1e-10): at the reference's loose SAD tolerance (rms 1e-6) the stopping point
 depends on last-digit differences between two J/K builds, which the DIIS solves amplify.
@@ -7,34 +8,13 @@ Tolerances: guess density 1e-8; SCF energy 1e-8 Eh."""
 import numpy as np
 import pytest
 
-import oracle
+import oracle.scf as OS
 from hfscf_b200 import basis as B
 from hfscf_b200 import engine as E
 from hfscf_b200 import molecules as M
 from hfscf_b200 import scf
 
 pytestmark = pytest.mark.gpu
-
-
-def _oracle_sad(bs):
-    n = bs.nbf
-    D = np.zeros((n, n))
-    bf_atom = bs.bf_atom()
-    done = {}
-    for a, Zc in enumerate(bs.Z):
-        Zc = int(Zc)
-        if Zc not in done:
-            ab = scf.atom_basis(bs, a)
-            S, T, V = oracle.ref_onee(ab)
-            eri = oracle.eri_packed(ab)
-
-            def jk(DJ, DKs):
-                return oracle.jk(eri, DJ)[0], [oracle.jk(eri, Dk)[1] for Dk in DKs]
-
-            done[Zc] = scf.sad_atom_density(Zc, S, T, V, jk, rms_tol=1e-10, e_tol=1e-12, max_iter=200)
-        f = np.nonzero(bf_atom == a)[0]
-        D[np.ix_(f, f)] = done[Zc]
-    return D
 
 
 @pytest.mark.parametrize("name,pure", [("6-31g*", False), ("cc-pvdz", True)])
@@ -44,7 +24,7 @@ def test_sad_guess_matches_oracle_restatement(name, pure):
     x = np.vstack([np.asarray(x), [[4.0, 4.0, 4.0]]])
     bs = B.build_basis(name, Z, x * B.ANGSTROM_TO_BOHR, pure=pure)
     D = scf.sad_guess(bs, rms_tol=1e-10, e_tol=1e-12, max_iter=200)
-    D0 = _oracle_sad(bs)
+    D0 = OS.sad_guess(bs, rms_tol=1e-10, e_tol=1e-12, max_iter=200)
     assert np.abs(D - D0).max() < 1e-8
 
 

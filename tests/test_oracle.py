@@ -168,3 +168,37 @@ def test_oracle_scf_converges_to_a_stationary_density():
     assert abs(np.trace(D @ S) - nocc) < 1e-12
     assert np.max(np.abs(F @ D @ S - S @ D @ F)) < 1e-7
     assert abs(OS.nuclear_repulsion(Z, bs.coords) - B.nuclear_repulsion(Z, bs.coords)) < 1e-12
+
+
+@needs_ref
+@pytest.mark.parametrize("name,pure", [("6-31g*", False), ("cc-pvdz", True)])
+def test_sad_host_logic_matches_oracle_sad(name, pure):
+    """The engine's SAD host logic (scf.sad_atom_density, scf.atom_basis, scf.sad_populations)
+    driven by the C restatement's J/K, against the oracle's SAD on the reference's integrals
+    (oracle/scf.py: sad_guess), for H, C and O; both atomic UHF runs converged to rms 1e-10."""
+    from oracle import scf as OS
+    from hfscf_b200 import scf
+    Z, x = M.water_cluster(2, 2.9, np.random.default_rng(8), 0.1)
+    Z = np.concatenate([Z, [6]])
+    x = np.vstack([np.asarray(x), [[4.0, 4.0, 4.0]]])
+    bs = B.build_basis(name, Z, x * B.ANGSTROM_TO_BOHR, pure=pure)
+    n = bs.nbf
+    D = np.zeros((n, n))
+    bf_atom = bs.bf_atom()
+    done = {}
+    for a, Zc in enumerate(bs.Z):
+        Zc = int(Zc)
+        if Zc not in done:
+            ab = scf.atom_basis(bs, a)
+            S, T, V = oracle.ref_onee(ab)
+            eri = oracle.eri_packed(ab)
+
+            def jk(DJ, DKs, eri=eri):
+                return oracle.jk(eri, DJ)[0], [oracle.jk(eri, Dk)[1] for Dk in DKs]
+
+            done[Zc] = scf.sad_atom_density(Zc, S, T, V, jk, rms_tol=1e-10, e_tol=1e-12, max_iter=200)
+        f = np.nonzero(bf_atom == a)[0]
+        D[np.ix_(f, f)] = done[Zc]
+    D0 = OS.sad_guess(bs, rms_tol=1e-10, e_tol=1e-12, max_iter=200)
+    assert np.abs(D - D0).max() < 1e-10
+    assert abs(np.trace(D0 @ oracle.ref_onee(bs)[0]) - float(np.sum(Z)) / 2) < 1e-8
