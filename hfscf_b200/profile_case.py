@@ -6,7 +6,8 @@
 
 Builds the named workload's basis (``molecules.workload``: 1 = H2O/cc-pVDZ,
 2 = n-octane/6-31G**, 3 = anthracene/cc-pVDZ, 4 = (H2O)8/6-31G*), forms the
-core-guess density (and with ``--autotune`` tunes the launch schedule on it),
+core-guess density (and with ``--autotune`` tunes the J/K launch schedule or the gradient
+forms on it),
 runs one untimed warm-up of the operation and then
 ``--repeat`` timed ones between ``cudaProfilerStart``/``cudaProfilerStop`` (so
 ``ncu --profile-from-start off`` sees exactly those launches).  Prints one JSON
@@ -41,7 +42,8 @@ def main(argv=None):
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--device", type=int, default=0)
-    ap.add_argument("--autotune", action="store_true", help="hfgpu_autotune first (as bench.py does)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="hfgpu_autotune (jk) or hfgpu_autotune_grad (grad) first, as bench.py does")
     ap.add_argument("--variant", type=int, choices=(0, 1, 2), default=None,
                     help="thread-form variant for every class (schedule column 3: 0 plain, 1 capped, "
                          "2 staged persistent)")
@@ -60,7 +62,10 @@ def main(argv=None):
         eng.set_stream(stream.cuda_stream)
         Dd = torch.from_numpy(np.ascontiguousarray(D)).to(dev)
         if a.autotune:
-            eng.autotune(Dd, E.FP64, 3)
+            if a.op == "jk":
+                eng.autotune(Dd, E.FP64, 3)
+            else:
+                eng.autotune_grad(Dd, prec, 3)
         if a.variant is not None:
             sched = eng.get_schedule()
             sched[:, 3] = a.variant
