@@ -142,6 +142,7 @@ struct hfgpu_handle {
   // inside each part the quartets with many primitive quartets come first:
   // [beg, hik1) and [mid, hik2) run the warp-over-primitives kernel where the class has one
   std::vector<long long> q_beg, q_mid, q_end, q_hik1, q_hik2;
+  std::vector<long long> q_prims;  // per class: primitive quartets of the Schwarz-screened quartets
   // inside each of the four segments quartets are ordered by Schwarz-bound decade
   // (largest first; inside a decade by primitive-quartet count, then bra-major):
   // bucket_end[(c * 4 + seg) * kBuckets + e] is the
@@ -182,7 +183,7 @@ struct hfgpu_handle {
   int grad_form[21];
   unsigned grad_class_mask = ~0u;       // classes a gradient launches (autotuning runs one at a time)
 
-  hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21) {
+  hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21), q_prims(21) {
     for (int c = 0; c < 21; ++c) {
       sched_block[c] = 64;
       sched_primwarp[c] = 0;
@@ -474,6 +475,7 @@ struct ListChunk {
   std::vector<int2> q[4];       // survivors per segment, in list order
   std::vector<int> key[4];      // bound decade * kProdSpan + primitive-quartet count
   int maxprod[4] = {0, 0, 0, 0};
+  long long prims = 0;          // primitive quartets of the survivors
 };
 
 // Runs f(0) ... f(ntask - 1) on up to max_threads threads (the caller's thread among them).
@@ -547,6 +549,7 @@ int build_quartets(hfgpu_handle* h) {
       for (int Q = k0; Q < ke; ++Q) {
         const double b = qp * h->pairs[Q].schwarz;
         if (b < tol) continue;
+        c.prims += (long long)np * h->pairs[Q].nprim;
         const int prod = std::min(np * h->pairs[Q].nprim, kProdSpan - 1);
         const int sg = (b >= mix ? 0 : 2) + (prod >= kPrimWarpMinPrims ? 0 : 1);
         c.q[sg].push_back(make_int2(P, Q));
@@ -625,6 +628,8 @@ int build_quartets(hfgpu_handle* h) {
     h->q_mid[qc] = seg_base[(size_t)i * 5 + 2];
     h->q_hik2[qc] = seg_base[(size_t)i * 5 + 3];
     h->q_end[qc] = seg_base[(size_t)i * 5 + 4];
+    h->q_prims[qc] = 0;
+    for (int ci = cls_chunk0[i]; ci < cls_chunk0[i + 1]; ++ci) h->q_prims[qc] += chunks[ci].prims;
   }
   h->nquartets = total;
   const auto t1 = clk::now();
@@ -1904,6 +1909,13 @@ int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out) {
     out[7] = (long long)c[1];
     out[8] = (long long)c[2];
   }
+  return HFGPU_OK;
+}
+
+int hfgpu_class_work(const hfgpu_handle* h, int cls, long long* out) {
+  if (!h || !out || cls < 0 || cls >= hfgpu::kNumClasses) return HFGPU_ERR_INVALID;
+  out[0] = h->q_end[cls] - h->q_beg[cls];
+  out[1] = h->q_prims[cls];
   return HFGPU_OK;
 }
 

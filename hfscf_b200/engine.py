@@ -224,6 +224,12 @@ class Engine:
         keys = ("la", "lb", "lc", "ld", "screened", "high_bound", "computed", "skipped", "prim_quartets")
         return dict(zip(keys, list(out)))
 
+    def class_work(self, cls: int):
+        """hfgpu_class_work: Schwarz-screened quartets of class cls and their primitive quartets."""
+        out = (ctypes.c_longlong * 2)()
+        self._check(lib().hfgpu_class_work(self.h, ctypes.c_int(cls), out))
+        return {"quartets": out[0], "prim_quartets": out[1]}
+
     def setup_times(self):
         """Host wall time (s) of the last geometry set-up: primitive pairs, Schwarz factors,
         quartet lists, list upload (hfgpu_setup_times)."""

@@ -26,6 +26,15 @@ one multiply or one add (an FMA is two).
   C_dig    J/K digestion: 12 per integral of the final basis (J_ab, J_cd and the four K
            blocks, one FMA each).
 
+Gradient (adjoint or not, the same frozen count): the derivative classes with L + 1 on three
+centres, d/dA_i (ab|cd) = 2 alpha (a+1_i b|cd) - a_i (a-1_i b|cd) and likewise for B and C
+(D by translational invariance), per primitive quartet the Boys function to order L + 1, the
+VRR of every [e0|f0] the raised and lowered classes need, one add per unweighted target and two
+(a product and an add) per exponent-weighted target (2 alpha, 2 beta, 2 gamma sets); per
+contracted quartet the HRR of the six raised and lowered classes, two flops per derivative
+integral that has a lowered term, the pure transform of the nine derivative blocks and
+C_DIG_GRAD = 4 per derivative integral per centre component (grad_class_flops).
+
 Classes are numbered as the engine numbers them (hfgpu_class_stats): pair classes
 ss ps pp ds dp dd = 0..5 (la >= lb), quartet class cp (cp + 1) / 2 + cq for cp >= cq.
 The count of the engine's own generated code (csrc/generated/ops.json) is kept as a second
@@ -43,6 +52,7 @@ OPS = os.path.join(HERE, "csrc", "generated", "ops.json")
 
 C_PRIM = 25
 C_DIG = 12
+C_DIG_GRAD = 4
 PAIRS = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
 
 
@@ -85,14 +95,22 @@ def _dec(v, i):
     return tuple(w)
 
 
+def _target_set(e_lo, e_hi, f_lo, f_hi):
+    return {(e, f) for le in range(max(e_lo, 0), e_hi + 1) for e in cart(le)
+            for lf in range(max(f_lo, 0), f_hi + 1) for f in cart(lf)}
+
+
 @lru_cache(maxsize=None)
 def _vrr_count(la, lb, lc, ld):
     """(flops, targets) of the vertical recurrence of one primitive quartet."""
+    return _vrr_enumerate(frozenset(_target_set(la, la + lb, lc, lc + ld)))
+
+
+def _vrr_enumerate(targets):
+    """(flops, number of targets) of building every [e0|f0]^(0) in targets by the VRR."""
     built = set()
     flops = 0
     stack = []
-    targets = [(e, f) for le in range(la, la + lb + 1) for e in cart(le)
-               for lf in range(lc, lc + ld + 1) for f in cart(lf)]
     for e, f in targets:
         stack.append((e, f, 0))
     while stack:
@@ -214,6 +232,62 @@ def class_flops(cls_index: int, computed_quartets: int, prim_quartets: int, pure
     primitive quartets."""
     return float(prim_quartets) * per_prim_flops(cls_index) + \
         float(computed_quartets) * per_quartet_flops(cls_index, pure)
+
+
+# ---- gradient ------------------------------------------------------------------------------
+@lru_cache(maxsize=None)
+def _grad_sets(la, lb, lc, ld):
+    """[e0|f0] target sets of the derivative classes: unweighted (lowered classes) and the
+    2 alpha, 2 beta, 2 gamma weighted sets (raised on A, B, C)."""
+    U = set()
+    if la > 0:
+        U |= _target_set(la - 1, la - 1 + lb, lc, lc + ld)
+    if lb > 0:
+        U |= _target_set(la, la + lb - 1, lc, lc + ld)
+    if lc > 0:
+        U |= _target_set(la, la + lb, lc - 1, lc - 1 + ld)
+    A = _target_set(la + 1, la + 1 + lb, lc, lc + ld)
+    B = _target_set(la, la + lb + 1, lc, lc + ld)
+    C = _target_set(la, la + lb, lc + 1, lc + 1 + ld)
+    return U, A, B, C
+
+
+def grad_per_prim_flops(cls_index: int) -> int:
+    la, lb, lc, ld = class_am(cls_index)
+    U, A, B, C = _grad_sets(la, lb, lc, ld)
+    v, _ = _vrr_enumerate(frozenset(U | A | B | C))
+    return C_PRIM + c_boys(la + lb + lc + ld + 1) + v + len(U) + 2 * (len(A) + len(B) + len(C))
+
+
+def _lowered_terms(la, lb, lc, ld) -> int:
+    """Derivative integrals (per Cartesian block, over the nine centre components) that have
+    a lowered term: sum over A, B, C and i of the Cartesian functions with a nonzero i index."""
+    blk = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
+    n = 0
+    for L in (la, lb, lc):
+        with_i = sum(1 for c in cart(L) for i in range(3) if c[i] > 0)
+        n += with_i * blk // ncart(L)
+    return n
+
+
+def grad_per_quartet_flops(cls_index: int, pure: bool) -> int:
+    la, lb, lc, ld = class_am(cls_index)
+    h = _hrr_count(la + 1, lb, lc, ld) + _hrr_count(la, lb + 1, lc, ld) + _hrr_count(la, lb, lc + 1, ld)
+    if la > 0:
+        h += _hrr_count(la - 1, lb, lc, ld)
+    if lb > 0:
+        h += _hrr_count(la, lb - 1, lc, ld)
+    if lc > 0:
+        h += _hrr_count(la, lb, lc - 1, ld)
+    sph = 9 * _sph_count(la, lb, lc, ld) if pure else 0
+    return h + 2 * _lowered_terms(la, lb, lc, ld) + sph + C_DIG_GRAD * 9 * class_block_size(cls_index, pure)
+
+
+def grad_class_flops(cls_index: int, quartets: int, prim_quartets: int, pure: bool) -> float:
+    """Frozen-model FLOPs of the first derivatives of `quartets` contracted quartets holding
+    `prim_quartets` primitive quartets, contracted with their density weights."""
+    return float(prim_quartets) * grad_per_prim_flops(cls_index) + \
+        float(quartets) * grad_per_quartet_flops(cls_index, pure)
 
 
 # ---- second number: the operation count of the engine's generated code ---------------------

