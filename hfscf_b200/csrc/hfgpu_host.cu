@@ -143,6 +143,7 @@ struct hfgpu_handle {
   // [beg, hik1) and [mid, hik2) run the warp-over-primitives kernel where the class has one
   std::vector<long long> q_beg, q_mid, q_end, q_hik1, q_hik2;
   std::vector<long long> q_prims;  // per class: primitive quartets of the Schwarz-screened quartets
+  int part = 0, nparts = 1;        // partition of every quartet list (hfgpu_set_partition)
   // inside each of the four segments quartets are ordered by Schwarz-bound decade
   // (largest first; inside a decade by primitive-quartet count, then bra-major):
   // bucket_end[(c * 4 + seg) * kBuckets + e] is the
@@ -1020,6 +1021,8 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   qd.status = qf.status = h->d_status.as<int>();
   qd.stage_test = qf.stage_test = h->opts.reserved[0] == 1 ? 1 : 0;
   qd.abort_flag = qf.abort_flag = h->d_abort.as<int>();
+  qd.part = qf.part = h->part;
+  qd.nparts = qf.nparts = h->nparts;
   const int2* q = h->d_quart.as<int2>();
   long long launched = 0;
   // largest classes first so that they overlap the tail of the smaller ones
@@ -1066,18 +1069,22 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
       }
     }
     for (int r = 0; r < nr; ++r) {
-      const int nq_max = (int)(rg[r].hi - rg[r].lo);  // the grid covers every quartet of the parts
-      if (nq_max <= 0) continue;
+      const int nq_all = (int)(rg[r].hi - rg[r].lo);
+      // the grid covers every quartet of the parts (this partition's share of them)
+      const int nq_max = (int)((nq_all + h->nparts - 1) / h->nparts);
+      if (nq_max <= 0 || (h->nparts > 1 && nq_all <= h->part)) continue;
       const int2* qs = q + rg[r].lo;
       const int* dyn = dmax != nullptr ? h->d_dyn.as<int>() + c * 4 + rg[r].part0 : nullptr;
       if (rg[r].fp32) {
         qf.dyn_nq = dyn;
         qf.nseg = rg[r].nseg;
+        qf.full_nq = nq_all;
         for (int k = 0; k < 4; ++k) qf.seg_off[k] = (int)rg[r].off[k];
         if (!(rg[r].many && L->primwarp_f(qf, qs, nq_max, st))) L->quartet_f(qf, qs, nq_max, st);
       } else {
         qd.dyn_nq = dyn;
         qd.nseg = rg[r].nseg;
+        qd.full_nq = nq_all;
         for (int k = 0; k < 4; ++k) qd.seg_off[k] = (int)rg[r].off[k];
         if (!(rg[r].many && L->primwarp_d(qd, qs, nq_max, st))) L->quartet_d(qd, qs, nq_max, st);
       }
@@ -1143,6 +1150,13 @@ static bool grad_use_warp(const hfgpu_handle* h, int c, long long nq, bool fp32)
   return nq <= (long long)h->opts.grad_warp_max_waves * per_sm * sms;
 }
 
+// Quartets of a list range of n that this handle's partition processes (every nparts-th,
+// starting at number part).
+static long long part_share(const hfgpu_handle* h, long long n) {
+  if (h->nparts <= 1) return n;
+  return n > h->part ? (n - h->part + h->nparts - 1) / h->nparts : 0;
+}
+
 static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
                             double* grad, int precision) {
   if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
@@ -1171,6 +1185,8 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
   gf.mol_off = gd.mol_off;
   gf.mol_n = gd.mol_n;
   gd.smem_atoms = gf.smem_atoms = grad_smem_atoms(h);
+  gd.part = gf.part = h->part;
+  gd.nparts = gf.nparts = h->nparts;
   const int2* q = h->d_quart.as<int2>();
   const size_t budget = (size_t)1 << 30;  // scratch bytes per table-mode class and precision
   // threads of a table-mode launch: as many as the budget allows (at least 4736),
@@ -1211,7 +1227,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     cudaStream_t st_d = h->aux[rr++ % hfgpu_handle::kAux];
     cudaStream_t st_f = precision == HFGPU_MIXED ? h->aux[rr++ % hfgpu_handle::kAux] : st_d;
     auto run = [&](bool fp32, long long lo, long long hi) -> int {
-      const int nq = (int)(hi - lo);
+      const int nq = (int)part_share(h, hi - lo);
       if (nq <= 0) return HFGPU_OK;
       gd.warp_split = gf.warp_split = h->grad_form[c] == 2 ? 1 : 0;
       if (grad_use_warp(h, c, e - b, fp32)) {
@@ -1292,6 +1308,8 @@ int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int n
   gf.mol_off = gd.mol_off;
   gf.mol_n = gd.mol_n;
   gd.smem_atoms = gf.smem_atoms = grad_smem_atoms(h);
+  gd.part = gf.part = h->part;
+  gd.nparts = gf.nparts = h->nparts;
   const int2* q = h->d_quart.as<int2>();
   // quartet range of part 0 / 1 of class c (FP64 and, in mixed mode, the FP32 low-bound part)
   auto part_range = [&](int c, int part, long long& lo, long long& hi) {
@@ -1325,7 +1343,7 @@ int hfgpu_grad_fixed_scratch(hfgpu_handle* h, const double* DJ, double cJ, int n
       const bool fp32 = precision == HFGPU_MIXED && part == 1;
       long long lo, hi;
       part_range(c, part, lo, hi);
-      const int nq = (int)(hi - lo);
+      const int nq = (int)part_share(h, hi - lo);
       if (nq <= 0) continue;
       int grid = (nq + 127) / 128;
       if (slots == 0 && gd.smem_atoms > 0) grid = std::min(grid, grad_max_blocks(h));
@@ -1608,6 +1626,7 @@ int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* ski
 
 int hfgpu_fock_rhf(hfgpu_handle* h, const double* D, const double* H, double* F, int precision) {
   if (!h || !D || !H || !F) return HFGPU_ERR_INVALID;
+  if (h->nparts > 1) return fail(h, HFGPU_ERR_STATE, "a partitioned handle builds partial J/K only: the Fock entry points add H and are refused");
   DeviceGuard dev_guard(h);
   int rc = dev_guard.rc;
   if (rc) return rc;
@@ -1633,6 +1652,7 @@ int hfgpu_fock_rhf(hfgpu_handle* h, const double* D, const double* H, double* F,
 int hfgpu_fock_uhf(hfgpu_handle* h, const double* Da, const double* Db, const double* H, double* Fa, double* Fb,
                    int precision) {
   if (!h || !Da || !Db || !H || !Fa || !Fb) return HFGPU_ERR_INVALID;
+  if (h->nparts > 1) return fail(h, HFGPU_ERR_STATE, "a partitioned handle builds partial J/K only: the Fock entry points add H and are refused");
   const size_t nn = (size_t)h->n * h->n;
   std::vector<double> Dt(nn), DK(2 * nn), J(nn), K(2 * nn);
   for (size_t i = 0; i < nn; ++i) {
@@ -1651,6 +1671,7 @@ int hfgpu_fock_uhf(hfgpu_handle* h, const double* Da, const double* Db, const do
 
 int hfgpu_fock_delta(hfgpu_handle* h, const double* dD, double* F, int precision) {
   if (!h || !dD || !F) return HFGPU_ERR_INVALID;
+  if (h->nparts > 1) return fail(h, HFGPU_ERR_STATE, "a partitioned handle builds partial J/K only: the Fock entry points add H and are refused");
   DeviceGuard dev_guard(h);
   int rc = dev_guard.rc;
   if (rc) return rc;
@@ -1909,6 +1930,15 @@ int hfgpu_class_stats(hfgpu_handle* h, int cls, long long* out) {
     out[7] = (long long)c[1];
     out[8] = (long long)c[2];
   }
+  return HFGPU_OK;
+}
+
+int hfgpu_set_partition(hfgpu_handle* h, int part, int nparts) {
+  if (!h) return HFGPU_ERR_INVALID;
+  if (nparts < 1 || nparts > 65536 || part < 0 || part >= nparts)
+    return fail(h, HFGPU_ERR_INVALID, "partition needs 0 <= part < nparts <= 65536");
+  h->part = part;
+  h->nparts = nparts;
   return HFGPU_OK;
 }
 

@@ -54,6 +54,8 @@ struct GradArgs {
   int smem_atoms;                    // grad_kernel: > 0 = accumulate 3 x smem_atoms entries per block in
                                      // shared memory, then one atomic per entry (0: atomics into grad)
   int warp_split;                    // grad_warp_kernel: 1 = four launches, one accumulator set each
+  int part, nparts;                  // partitioned gradients: the launch's quartet t is list entry
+                                     // t * nparts + part (nparts <= 1: t); nq counts this part's
 };
 
 template <int NA, int NB, int NC, int ND>
@@ -254,22 +256,38 @@ struct QuartetArgs {
   int* status;          // device status word (HFGPU_DEV_STAGE_TIMEOUT when a staging wait ran out)
   int stage_test;       // 1: arm the staging barrier without a copy, so that its wait runs out (test only)
   const int* abort_flag;  // device word the host sets to stop persistent launches early (nullptr: none)
+  // Partitioned builds (one molecule's quartets split over nparts devices or passes): the
+  // launch processes every nparts-th quartet of its range, starting at number `part`, and its
+  // nq is the per-part upper bound.  nparts <= 1: all quartets.  full_nq: the range's quartets
+  // when dyn_nq == nullptr.
+  int part;
+  int nparts;
+  int full_nq;
 };
 
 // Quartets this launch processes: nq, or the sum of the device-side segment counts of a
-// density-screened build.
+// density-screened build; of a partitioned build, this part's share of them.
 template <typename R>
 __device__ __forceinline__ int launch_count(const QuartetArgs<R>& qa, int nq) {
-  if (qa.dyn_nq == nullptr) return nq;
-  int tot = 0;
-  for (int k = 0; k < qa.nseg; ++k) tot += __ldg(qa.dyn_nq + k);
+  const int np = qa.nparts > 1 ? qa.nparts : 1;
+  int tot;
+  if (qa.dyn_nq == nullptr) {
+    if (np == 1) return nq;
+    tot = qa.full_nq;
+  } else {
+    tot = 0;
+    for (int k = 0; k < qa.nseg; ++k) tot += __ldg(qa.dyn_nq + k);
+  }
+  if (np > 1) tot = tot > qa.part ? (tot - qa.part + np - 1) / np : 0;
   return min(nq, tot);
 }
 
 // List position of the launch's t-th processed quartet (t < launch_count): t itself, or, in a
-// density-screened build, the t-th quartet of the segments' kept prefixes in segment order.
+// density-screened build, the t-th quartet of the segments' kept prefixes in segment order
+// (in a partitioned build, the (t nparts + part)-th).
 template <typename R>
 __device__ __forceinline__ int quartet_slot(const QuartetArgs<R>& qa, int t) {
+  if (qa.nparts > 1) t = t * qa.nparts + qa.part;
   if (qa.dyn_nq == nullptr) return t;
   for (int k = 0; k < qa.nseg - 1; ++k) {
     const int c = __ldg(qa.dyn_nq + k);
@@ -679,11 +697,13 @@ __global__ void __launch_bounds__(128) grad_kernel(GradArgs<R> a, int pure, cons
     __syncthreads();
     gout = grad_sh;
   }
+  const int np = a.nparts > 1 ? a.nparts : 1, p0 = np > 1 ? a.part : 0;
   for (int t = tid; t < nq; t += nthr) {
+    const int2 pq = quartets[(size_t)t * np + p0];
     if (pure)
-      grad_quartet<LA, LB, LC, LD, R, true, PASS>(a, tid, quartets[t], gout);
+      grad_quartet<LA, LB, LC, LD, R, true, PASS>(a, tid, pq, gout);
     else
-      grad_quartet<LA, LB, LC, LD, R, false, PASS>(a, tid, quartets[t], gout);
+      grad_quartet<LA, LB, LC, LD, R, false, PASS>(a, tid, pq, gout);
   }
   if (nsh > 0) {
     __syncthreads();
@@ -967,7 +987,7 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
   R* W = hs + Tab::NHSLOT + 1;
   R* t0 = W + Tab::NCART;
   R* t1 = t0 + Tab::NCART;
-  const int2 pq = quartets[qi];
+  const int2 pq = quartets[(size_t)qi * (a.nparts > 1 ? a.nparts : 1) + (a.nparts > 1 ? a.part : 0)];
   const PairInfo P = a.pairs[pq.x];
   const PairInfo Q = a.pairs[pq.y];
   double s8 = 8.0;

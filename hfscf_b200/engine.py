@@ -224,6 +224,11 @@ class Engine:
         keys = ("la", "lb", "lc", "ld", "screened", "high_bound", "computed", "skipped", "prim_quartets")
         return dict(zip(keys, list(out)))
 
+    def set_partition(self, part: int, nparts: int):
+        """hfgpu_set_partition: later J/K builds and gradients compute only quartets part,
+        part + nparts, ... of every class list (partial outputs, summed over the parts)."""
+        self._check(lib().hfgpu_set_partition(self.h, ctypes.c_int(part), ctypes.c_int(nparts)))
+
     def class_work(self, cls: int):
         """hfgpu_class_work: Schwarz-screened quartets of class cls and their primitive quartets."""
         out = (ctypes.c_longlong * 2)()

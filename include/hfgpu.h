@@ -222,12 +222,22 @@ int hfgpu_class_time(hfgpu_handle* h, int cls, float* ms);
  * Schwarz-screened quartets (all of them are computed by a gradient), out[1] = their primitive
  * quartets (kept primitive pairs of the bra times those of the ket).  No host synchronisation. */
 int hfgpu_class_work(const hfgpu_handle* h, int cls, long long* out);
+/* Partition of one molecule's work over nparts devices (or passes): later J/K builds and
+ * two-electron gradients of this handle process only the quartets numbered part, part + nparts,
+ * part + 2 nparts, ... of every class list (the lists are ordered by bound and primitive count,
+ * so the parts cost about the same), and their J, K, E2 and gradient outputs are this part's
+ * terms; summed over the nparts parts they equal the unpartitioned outputs up to FP64 summation
+ * order (the density screening decides on the same device bounds in every part).  The Fock
+ * entry points (fock_rhf, fock_uhf, fock_delta), which add H, return HFGPU_ERR_STATE on a
+ * partitioned handle.  nparts = 1 (the default) ends the partition.  No reference counterpart
+ * (the reference's Fock build and gradient are one OpenMP loop on one host). */
+int hfgpu_set_partition(hfgpu_handle* h, int part, int nparts);
 int hfgpu_last_launches(const hfgpu_handle* h, int* kernels);
 /* Device status word of the handle's kernels since the last call, then cleared (synchronises
  * the handle's stream): 0 = fine; 2 = a block's wait for its shared-memory staging copy ran
  * out (bounded at about 0.1 s; the block skipped its quartets, so that build is incomplete);
  * 3 = a persistent launch stopped at a host abort request.  The host-pointer entry points
- * check it themselves and return HFGPU_ERR_CUDA (2) or HFGPU_ERR_STATE (3).  No reference
+ * check it themselves and return HFGPU_ERR_CUDA for status 2 and HFGPU_ERR_STATE for status 3.  No reference
  * counterpart (the reference has no device code and exits on errors). */
 int hfgpu_device_status(hfgpu_handle* h, int* status);
 /* Host abort flag (on = 1) or its reset (on = 0), written on a stream of its own so that it
