@@ -336,6 +336,46 @@ def other_configs(local, stream, flush, oracle_refs, autotune):
     return out
 
 
+def sharded_build(eng, D, Hd, J, K, F, flush, stream, args, pg, rank, world):
+    """One molecule's Fock build partitioned over the ranks (hfgpu_set_partition(rank, world):
+    every world-th quartet of each class list) and the partial G = 2J - K summed with one NCCL
+    all-reduce per build, F = H + G on every rank.  Device time of the timed steps with CUDA
+    events on the build's stream, max over ranks; total work fixed as the ranks grow (strong)."""
+    import torch
+    F_whole = F.clone()
+    G = torch.empty_like(F)
+    eng.set_partition(rank, world)
+
+    def step():
+        eng.jk_device(D.data_ptr(), 1, D.data_ptr(), J.data_ptr(), K.data_ptr())
+        torch.sub(J, K, alpha=0.5, out=G)
+        G.mul_(2.0)
+        pg.all_reduce(G)
+        torch.add(Hd, G, out=F)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    pg.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    pg.barrier()
+    tot = torch.tensor([sum(a.elapsed_time(b) for a, b in ev) / 1e3], dtype=torch.float64, device=F.device)
+    pg.all_reduce(tot, op=pg.ReduceOp.MAX)
+    total_s = float(tot.item())
+    err = float((F - F_whole).abs().max().item())
+    eng.set_partition(0, 1)
+    return {"builds_per_s": args.steps / total_s, "ms_per_build": 1e3 * total_s / args.steps,
+            "scaling": "strong", "parts": world,
+            "collective": "one NCCL all-reduce of G = 2J - K (n^2 doubles) per build",
+            "max_abs_F_vs_whole_build": err}
+
+
 def run_ours(args, world, rank, local):
     import torch
     from hfscf_b200 import engine as E
@@ -427,6 +467,8 @@ def run_ours(args, world, rank, local):
         pg.all_reduce(tt, op=pg.ReduceOp.MAX)
         total_s = float(tt.item())
     value = world * args.steps / total_s
+    # the same molecule's build split over the ranks (only with more than one rank)
+    sharded = sharded_build(eng, D, Hd, J, K, F, flush, stream, args, pg, rank, world) if pg else None
 
     # --- end to end through the reference-facing C ABI, pinned host buffers -----------------
     Dh = torch.from_numpy(np.ascontiguousarray(res.D)).pin_memory()
@@ -515,7 +557,7 @@ def run_ours(args, world, rank, local):
                                     f"({tune_s:.2f} s, untimed)"),
                        "quartets_screened": int(sum(class_work[c]["screened"] for c in range(E.NUM_CLASSES))),
                        "quartets_computed_last_build": int(sum(class_work[c]["computed"] for c in range(E.NUM_CLASSES)))},
-            "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "sharded": sharded,
             "scf": {"guess": "SAD", "energy": res.energy, "iterations": res.iterations, "converged": res.converged,
                     "mixed_iterations": res_mx.iterations,
                     "wall_s": scf_wall, "grad_wall_s": grad_wall, "grad_max": float(np.max(np.abs(grad))),
