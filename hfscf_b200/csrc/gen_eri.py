@@ -961,14 +961,20 @@ static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, i
     grad_kernel<{la}, {lb}, {lc}, {ld}, R><<<grid, 128, sm, s>>>(a, pure, q, nq);
   }}
 }}
-template <typename Tab, typename R>
-static bool launch_grad_warp_tab(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{
+template <typename Tab, typename R, int NT>
+static bool launch_grad_warp_nt(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{
   constexpr size_t bytes = sizeof(R) * (size_t)grad_warp_slots<Tab, R>();
   if (bytes > 232448) return false;  // more shared memory than one block may have
-  auto k = grad_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab>;
+  auto k = grad_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab, NT>;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  k<<<nq, 32, bytes, s>>>(a, pure, q, nq);
+  k<<<nq, NT, bytes, s>>>(a, pure, q, nq);
   return true;
+}}
+template <typename Tab, typename R>
+static bool launch_grad_warp_tab(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{
+  // one warp per quartet, or one block of four warps per quartet
+  return a.warp_threads == 128 ? launch_grad_warp_nt<Tab, R, 128>(a, pure, q, nq, s)
+                               : launch_grad_warp_nt<Tab, R, 32>(a, pure, q, nq, s);
 }}
 template <typename CC, typename R>
 static bool launch_grad_warp_impl(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{

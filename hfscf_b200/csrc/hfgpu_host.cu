@@ -1137,6 +1137,11 @@ int grad_smem_atoms(const hfgpu_handle* h) {
   return (size_t)h->natoms * 3 * sizeof(double) <= (size_t)kGradSmemBytes ? h->natoms : 0;
 }
 
+// Gradient forms of the op-table classes: 0 one thread per quartet (global scratch), 1 one warp
+// per quartet, 2 one warp per quartet in four one-set launches, 3 one block of 128 threads per
+// quartet, 4 the same in four one-set launches.
+constexpr int kGradForms = 5;
+
 static bool grad_use_warp(const hfgpu_handle* h, int c, long long nq, bool fp32) {
   const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
   if (!L->has_grad_warp) return false;
@@ -1229,7 +1234,8 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     auto run = [&](bool fp32, long long lo, long long hi) -> int {
       const int nq = (int)part_share(h, hi - lo);
       if (nq <= 0) return HFGPU_OK;
-      gd.warp_split = gf.warp_split = h->grad_form[c] == 2 ? 1 : 0;
+      gd.warp_split = gf.warp_split = (h->grad_form[c] == 2 || h->grad_form[c] == 4) ? 1 : 0;
+      gd.warp_threads = gf.warp_threads = h->grad_form[c] >= 3 ? 128 : 32;
       if (grad_use_warp(h, c, e - b, fp32)) {
         const bool done = fp32 ? L->grad_warp_f(gf, h->pure, q + lo, nq, fp32 ? st_f : st_d)
                                : L->grad_warp_d(gd, h->pure, q + lo, nq, st_d);
@@ -2154,7 +2160,7 @@ int hfgpu_request_abort(hfgpu_handle* h, int on) {
 int hfgpu_set_grad_forms(hfgpu_handle* h, const int* forms) {
   if (!h || !forms) return HFGPU_ERR_INVALID;
   for (int c = 0; c < hfgpu::kNumClasses; ++c)
-    if (forms[c] < -1 || forms[c] > 2) return fail(h, HFGPU_ERR_INVALID, "gradient form out of range");
+    if (forms[c] < -1 || forms[c] > kGradForms - 1) return fail(h, HFGPU_ERR_INVALID, "gradient form out of range");
   for (int c = 0; c < hfgpu::kNumClasses; ++c)
     h->grad_form[c] = hfgpu::kClassLaunchers[c]->has_grad_warp ? forms[c] : -1;
   return HFGPU_OK;
@@ -2191,7 +2197,8 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
     h->grad_class_mask = 1u << c;
     float best = 1e30f;
     int best_form = 0;
-    for (int form = 0; form < 3; ++form) {  // thread, warp, warp split into four one-set passes
+    // thread, warp, warp split into four one-set passes, block of four warps (whole, split)
+    for (int form = 0; form < kGradForms; ++form) {
       h->grad_form[c] = form;
       if ((rc = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return rc;  // warm-up
       HF_CUDA(h, cudaEventRecord(e0, h->stream));
@@ -2228,7 +2235,7 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     if (h->grad_form[c] < 0) continue;
     const int keep = h->grad_form[c];
-    for (int form = 0; form < 3; ++form) {
+    for (int form = 0; form < kGradForms; ++form) {
       if (form == keep) continue;
       const int before = h->grad_form[c];
       h->grad_form[c] = form;

@@ -54,6 +54,7 @@ struct GradArgs {
   int smem_atoms;                    // grad_kernel: > 0 = accumulate 3 x smem_atoms entries per block in
                                      // shared memory, then one atomic per entry (0: atomics into grad)
   int warp_split;                    // grad_warp_kernel: 1 = four launches, one accumulator set each
+  int warp_threads;                  // grad_warp_kernel: threads per quartet (32 or 128; 0 = 32)
   int part, nparts;                  // partitioned gradients: the launch's quartet t is list entry
                                      // t * nparts + part (nparts <= 1: t); nq counts this part's
 };
@@ -968,18 +969,30 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
 // Warp-per-quartet adjoint gradient for the large classes: the weight block, the VRR one
 // order higher with its four weighted accumulations, and the HRR of the four sets with
 // the contractions against W all run lane-parallel out of shared memory, level by level
-// (generated tables, gen_eri.py gen_grad_warp).  One warp per block, one block per quartet.
+// (generated tables, gen_eri.py gen_grad_warp).  One block per quartet, of one warp or four.
 // ---------------------------------------------------------------------------
 template <typename Tab, typename R>
 __host__ __device__ constexpr int grad_warp_slots() {
   return Tab::NVSLOT + 1 + Tab::NHSLOT + 1 + 3 * Tab::NCART;
 }
 
-template <int LA, int LB, int LC, int LD, typename R, typename Tab>
-__global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, const int2* __restrict__ quartets,
+template <int NT>
+__device__ __forceinline__ void group_sync() {
+  if constexpr (NT == 32)
+    group_sync<NT>();
+  else
+    __syncthreads();
+}
+
+// NT = 32: one warp per quartet; NT = 128: one block of four warps per quartet (the same
+// shared-memory tables, each level's rows spread over four times the threads, so that a
+// quartet finishes sooner and more warps per SM hide the shared-memory latency).
+template <int LA, int LB, int LC, int LD, typename R, typename Tab, int NT = 32>
+__global__ void __launch_bounds__(NT) grad_warp_kernel(GradArgs<R> a, int pure, const int2* __restrict__ quartets,
                                                        int nq) {
+  static_assert(NT == 32 || NT == 64 || NT == 128, "threads per quartet");
   extern __shared__ __align__(16) unsigned char gwsm[];
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x;  // 0 .. NT-1
   const int qi = blockIdx.x;
   if (qi >= nq) return;
   R* vs = reinterpret_cast<R*>(gwsm);
@@ -1007,7 +1020,7 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
   {
     const int tot = dims[0] * dims[1] * dims[2] * dims[3];
     R* dstw = pure ? t0 : W;
-    for (int e = lane; e < tot; e += 32) {
+    for (int e = lane; e < tot; e += NT) {
       const int l = e % dims[3], k = (e / dims[3]) % dims[2], j = (e / (dims[3] * dims[2])) % dims[1];
       const int i = e / (dims[3] * dims[2] * dims[1]);
       const int ia = P.fa + i, jb = P.fb + j, kc = Q.fa + k, ld = Q.fb + l;
@@ -1020,7 +1033,7 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
       }
       dstw[e] = R(s8 * w);
     }
-    __syncwarp();
+    group_sync<NT>();
   }
   if (pure) {
     R* bufs[2] = {t1, t0};
@@ -1031,7 +1044,7 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
       nd[st] = nc;
       R* o = st == 3 ? W : bufs[st & 1];
       const int tot = nd[0] * nd[1] * nd[2] * nd[3];
-      for (int e = lane; e < tot; e += 32) {
+      for (int e = lane; e < tot; e += NT) {
         int id[4];
         int r = e;
         for (int q = 3; q >= 0; --q) {
@@ -1048,17 +1061,17 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
         }
         o[e] = v;
       }
-      __syncwarp();
+      group_sync<NT>();
       for (int q = 0; q < 4; ++q) dims[q] = nd[q];
       in = o;
     }
   }
-  for (int t = lane; t < Tab::NACC; t += 32) hs[t] = R(0);
+  for (int t = lane; t < Tab::NACC; t += NT) hs[t] = R(0);
   if (lane == 0) {
     vs[Tab::NVSLOT] = R(0);
     hs[Tab::NHSLOT] = R(0);
   }
-  __syncwarp();
+  group_sync<NT>();
   const PrimPair<R>* bp = a.prims + P.prim_off;
   const PrimPair<R>* kp = a.prims + Q.prim_off;
   const R* eA = a.alpha_a + P.prim_off;
@@ -1088,7 +1101,7 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
 #pragma unroll
       for (int m = 0; m <= Tab::L; ++m)
         if (lane == m) vs[m] = F[m];
-      __syncwarp();
+      group_sync<NT>();
       for (int l = 0; l < Tab::NVLEV; ++l) {
         const int e = __ldg(vl + l + 1);
         // two op rows in flight per lane: the rows of one level are independent
@@ -1110,21 +1123,21 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
           }
           vs[dst] = v;
         };
-        for (int o = __ldg(vl + l) + lane; o < e; o += 64) {
+        for (int o = __ldg(vl + l) + lane; o < e; o += 2 * NT) {
           const int4 opa = __ldg(vo + o);
-          const bool two = o + 32 < e;
-          const int4 opb = two ? __ldg(vo + o + 32) : opa;
+          const bool two = o + NT < e;
+          const int4 opb = two ? __ldg(vo + o + NT) : opa;
           body(opa);
           if (two) body(opb);
         }
-        __syncwarp();
+        group_sync<NT>();
       }
-      for (int t = lane; t < Tab::NACC; t += 32) {
+      for (int t = lane; t < Tab::NACC; t += NT) {
         const int2 ac = __ldg(acc + t);
         const R w = ac.y == 0 ? R(1) : (ac.y == 1 ? wa : (ac.y == 2 ? wb : wc));
         hs[t] += w * vs[ac.x];
       }
-      __syncwarp();
+      group_sync<NT>();
     }
   }
   // HRR of the four sets and the contractions with W, per lane into nine partial sums
@@ -1152,18 +1165,29 @@ __global__ void __launch_bounds__(32) grad_warp_kernel(GradArgs<R> a, int pure, 
         hs[op.x & 0xffff] = hs[x] + d * hs[y];
       }
     };
-    for (int o = __ldg(hl + l) + lane; o < e; o += 64) {
+    for (int o = __ldg(hl + l) + lane; o < e; o += 2 * NT) {
       const int2 opa = __ldg(ho + o);
-      const bool two = o + 32 < e;
-      const int2 opb = two ? __ldg(ho + o + 32) : opa;
+      const bool two = o + NT < e;
+      const int2 opb = two ? __ldg(ho + o + NT) : opa;
       body(opa);
       if (two) body(opb);
     }
-    __syncwarp();
+    group_sync<NT>();
   }
 #pragma unroll
   for (int c = 0; c < 9; ++c)
     for (int off = 16; off > 0; off >>= 1) g[c] += __shfl_xor_sync(0xffffffffu, g[c], off);
+  if constexpr (NT > 32) {
+    // warp sums across the block through t0 (free after the weights; the last level synced)
+    if ((lane & 31) == 0)
+#pragma unroll
+      for (int c = 0; c < 9; ++c) t0[(lane >> 5) * 9 + c] = g[c];
+    __syncthreads();
+    if (lane == 0)
+      for (int w = 1; w < NT / 32; ++w)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) g[c] += t0[w * 9 + c];
+  }
   if (lane == 0) {
     const int at[3] = {P.atom_a, P.atom_b, Q.atom_a};
 #pragma unroll

@@ -281,15 +281,17 @@ int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
 int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule);
 int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule);
 /* Gradient form per class for the classes that have several (the op-table classes (dp|dp) (dd|pp)
- * (dd|ds) (dd|dp) (dd|dd)): times one warp per quartet (whole or split per set) against one thread per quartet for each
- * class alone on the handle's lists and the given device density D (RHF weights), keeps the
- * faster; then, on whole gradients, flips each class's form where that makes the gradient at
- * least 1% faster (the classes run concurrently), and returns the forms in
- * forms[HFGPU_NUM_CLASSES] (0 thread, 1 warp, 2 warp split into four launches of one
- * accumulator set each, -1 class without a choice; may be NULL).  Until it runs, opts.grad_warp_max_waves decides by quartet count.
+ * (dd|ds) (dd|dp) (dd|dd)): times one warp or one 128-thread block per quartet (whole or split
+ * per set) against one thread per quartet for each class alone on the handle's lists and the
+ * given device density D (RHF weights), keeps the fastest; then, on whole gradients, tries the
+ * other forms per class and keeps one where it makes the gradient at least 1% faster (the
+ * classes run concurrently), and returns the forms in forms[HFGPU_NUM_CLASSES] (0 thread, 1 warp,
+ * 2 warp split into four launches of one accumulator set each, 3 block of four warps, 4 block
+ * split into four launches, -1 class without a choice; may be NULL).  Until it runs,
+ * opts.grad_warp_max_waves decides by quartet count (warp form or thread form).
  * Results do not depend on the form beyond FP64 summation order. */
 int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int repeats, int* forms);
-/* Sets the gradient forms directly (HFGPU_NUM_CLASSES ints as hfgpu_autotune_grad returns them;
+/* Sets the gradient forms directly (HFGPU_NUM_CLASSES ints, -1 .. 4, as hfgpu_autotune_grad returns them;
  * -1 = the quartet-count rule; ignored for classes without a choice). */
 int hfgpu_set_grad_forms(hfgpu_handle* h, const int* forms);
 int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule);

@@ -99,13 +99,13 @@ def test_partitioned_jk_under_every_kernel_form(form):
     assert np.max(np.abs(K - Kw[0])) < TOL_SUM
 
 
-@pytest.mark.parametrize("forms", ["thread", "warp", "split"])
+@pytest.mark.parametrize("forms", ["thread", "warp", "split", "block"])
 def test_partitioned_gradient_sums_to_the_whole(forms):
     bs = _water4()
     D = _density(bs)
     g0 = oracle.grad2e_rhf(bs, D)
     with E.Engine(bs) as eng:
-        eng.set_grad_forms({"thread": 0, "warp": 1, "split": 2}[forms])
+        eng.set_grad_forms({"thread": 0, "warp": 1, "split": 2, "block": 4}[forms])
         gw = eng.grad2e(D, 1.0)
         g = np.zeros_like(gw)
         for p in range(3):

@@ -188,25 +188,27 @@ def test_host_abort_flag_stops_persistent_builds():
 
 
 def test_gradient_form_autotuner_keeps_the_gradient():
-    """hfgpu_autotune_grad picks, per op-table class, warp or thread form; the gradient after
-    tuning equals the oracle's (FP64, 1e-10)."""
+    """hfgpu_autotune_grad picks, per op-table class, thread, warp or block form; the gradient
+    after tuning equals the oracle's (FP64, 1e-10)."""
     rng = np.random.default_rng(43)
     bs = MOLS[1][1]  # methane cc-pVDZ: d shells, every op-table class present
     D = _sym(rng, bs.nbf)
     g0 = oracle.grad2e_rhf(bs, D)
     with E.Engine(bs) as eng:
         forms = eng.autotune_grad(D, repeats=1)
-        assert set(np.unique(forms)) <= {-1, 0, 1, 2} and (forms >= 0).any()
+        assert set(np.unique(forms)) <= {-1, 0, 1, 2, 3, 4} and (forms >= 0).any()
         g = eng.grad2e(D)
     assert np.max(np.abs(g - g0)) < 1e-10
 
 
-@pytest.mark.parametrize("form", [0, 1, 2], ids=["thread", "warp", "warp-split-per-set"])
+@pytest.mark.parametrize("form", [0, 1, 2, 3, 4],
+                         ids=["thread", "warp", "warp-split-per-set", "block", "block-split-per-set"])
 @pytest.mark.parametrize("name,bs", MOLS, ids=[m[0] for m in MOLS])
 def test_every_gradient_form_matches_oracle(name, bs, form):
     """Each gradient form of the op-table classes forced in turn: one thread per quartet, one
-    warp per quartet, and the warp form split into four launches of one accumulator set each
-    (FP64 1e-10, mixed 1e-6 against the oracle)."""
+    warp per quartet, the warp form split into four launches of one accumulator set each, and
+    the same two with a block of four warps per quartet (FP64 1e-10, mixed 1e-6 against the
+    oracle)."""
     rng = np.random.default_rng(47)
     D = _sym(rng, bs.nbf)
     g0 = oracle.grad2e_rhf(bs, D)
