@@ -44,6 +44,22 @@ def test_flop_model_counts():
             assert F.class_flops(c, 10, 100, True) == F.class_flops(c, 10, 100, False)
 
 
+def test_gradient_flop_model_hand_counts_and_scaling():
+    """The frozen gradient count of (ss|ss), by hand: per primitive quartet 25 scalars, Boys
+    F_0..F_1 (34), VRR of [p0|s0] and [s0|p0] (6 x 3) and the weighted sums of the raised sets
+    (2 alpha: 3 targets, 2 beta: 4, 2 gamma: 3; two flops each) = 97; per contracted quartet the
+    HRR of (sp|ss) (3 x 2) and 4 flops for each of the nine derivative integrals = 42.  Every
+    class costs more than its energy count and scales linearly in its work."""
+    from hfscf_b200 import flopmodel as F
+    assert F.grad_per_prim_flops(0) == 97
+    assert F.grad_per_quartet_flops(0, False) == 42
+    for c in range(E.NUM_CLASSES):
+        assert F.grad_per_prim_flops(c) > F.per_prim_flops(c)
+        assert F.grad_per_quartet_flops(c, False) > F.per_quartet_flops(c, False)
+        g1 = F.grad_class_flops(c, 10, 100, True)
+        assert F.grad_class_flops(c, 20, 200, True) == pytest.approx(2 * g1)
+
+
 def test_basis_sizes_of_the_workloads():
     sizes = {}
     for w in (1, 2, 3, 4):
