@@ -972,9 +972,10 @@ static bool launch_grad_warp_nt(const GradArgs<R>& a, int pure, const int2* q, i
 }}
 template <typename Tab, typename R>
 static bool launch_grad_warp_tab(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{
-  // one warp per quartet, or one block of four warps per quartet
-  return a.warp_threads == 128 ? launch_grad_warp_nt<Tab, R, 128>(a, pure, q, nq, s)
-                               : launch_grad_warp_nt<Tab, R, 32>(a, pure, q, nq, s);
+  // one warp per quartet, or one block of four or eight warps per quartet
+  if (a.warp_threads == 256) return launch_grad_warp_nt<Tab, R, 256>(a, pure, q, nq, s);
+  if (a.warp_threads == 128) return launch_grad_warp_nt<Tab, R, 128>(a, pure, q, nq, s);
+  return launch_grad_warp_nt<Tab, R, 32>(a, pure, q, nq, s);
 }}
 template <typename CC, typename R>
 static bool launch_grad_warp_impl(const GradArgs<R>& a, int pure, const int2* q, int nq, cudaStream_t s) {{

@@ -180,7 +180,8 @@ struct hfgpu_handle {
   int sched_block[21], sched_primwarp[21], sched_warp[21], sched_cap[21];
   unsigned class_mask = ~0u;            // classes a J/K build launches (autotuning runs one at a time)
   // gradient form per class (hfgpu_autotune_grad): 1 warp per quartet, 0 one thread per
-  // quartet, -1 the quartet-count rule of opts.grad_warp_max_waves
+  // quartet, 3/4 (5/6) block of four (eight) warps per quartet (whole / split), -1 the default
+  // (grad_form_of)
   int grad_form[21];
   unsigned grad_class_mask = ~0u;       // classes a gradient launches (autotuning runs one at a time)
 
@@ -1121,8 +1122,6 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   return HFGPU_OK;
 }
 
-// Warp form for a gradient launch of nq quartets of class c: when the class has one and the
-// launch fills at most opts.grad_warp_max_waves waves of the blocks all SMs hold at once.
 // Gradient accumulation of grad_kernel: per block in shared memory when the natoms x 3
 // totals fit in kGradSmemBytes, and then no more than kGradMaxBlocks blocks for the
 // straight-line classes (their grid-stride loop takes the rest), so that the flush at the
@@ -1139,21 +1138,25 @@ int grad_smem_atoms(const hfgpu_handle* h) {
 
 // Gradient forms of the op-table classes: 0 one thread per quartet (global scratch), 1 one warp
 // per quartet, 2 one warp per quartet in four one-set launches, 3 one block of 128 threads per
-// quartet, 4 the same in four one-set launches.
-constexpr int kGradForms = 5;
+// quartet, 4 the same in four one-set launches, 5 and 6 the same with 256 threads.
+constexpr int kGradForms = 7;
+static int grad_form_threads(int form) { return form >= 5 ? 256 : (form >= 3 ? 128 : 32); }
+static bool grad_form_split(int form) { return form == 2 || form == 4 || form == 6; }
 
-static bool grad_use_warp(const hfgpu_handle* h, int c, long long nq, bool fp32) {
+// Form of a gradient launch of class c: the one hfgpu_autotune_grad or hfgpu_set_grad_forms
+// chose, else the block form (3), which was the fastest single form on every workload measured
+// (octane, anthracene, the water octamer), when the class has shared-memory tables that fit one
+// block; opts.grad_warp_max_waves <= 0 asks for the thread form instead.
+static int grad_form_of(const hfgpu_handle* h, int c, bool fp32) {
   const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
-  if (!L->has_grad_warp) return false;
+  if (!L->has_grad_warp) return 0;
   const int bytes = L->grad_warp_bytes(fp32 ? 1 : 0);
-  if (bytes <= 0 || bytes > 232448) return false;
-  if (h->grad_form[c] >= 0) return h->grad_form[c] >= 1;  // chosen by hfgpu_autotune_grad
-  if (h->opts.grad_warp_max_waves <= 0) return false;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-  const long long per_sm = std::min(32, 233472 / (bytes + 1024));  // 228 KB per SM, 1 KB reserved per block
-  return nq <= (long long)h->opts.grad_warp_max_waves * per_sm * sms;
+  if (bytes <= 0 || bytes > 232448) return 0;
+  if (h->grad_form[c] >= 0) return h->grad_form[c];
+  return h->opts.grad_warp_max_waves > 0 ? 3 : 0;
 }
+
+static bool grad_use_warp(const hfgpu_handle* h, int c, bool fp32) { return grad_form_of(h, c, fp32) >= 1; }
 
 // Quartets of a list range of n that this handle's partition processes (every nparts-th,
 // starting at number part).
@@ -1212,7 +1215,7 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     const long long nq = h->q_end[c] - h->q_beg[c];
     slice_off[c] = slice_off_f[c] = need_total;
     if (slots <= 0 || nq <= 0) continue;
-    if (grad_use_warp(h, c, nq, false) && grad_use_warp(h, c, nq, true)) continue;  // warp form: no scratch
+    if (grad_use_warp(h, c, false) && grad_use_warp(h, c, true)) continue;  // warp/block form: no scratch
     const size_t one = (size_t)slots * sizeof(double) * (size_t)table_threads(slots, nq);
     need_total += (one + 255) / 256 * 256;
     if (precision == HFGPU_MIXED) {
@@ -1234,9 +1237,10 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     auto run = [&](bool fp32, long long lo, long long hi) -> int {
       const int nq = (int)part_share(h, hi - lo);
       if (nq <= 0) return HFGPU_OK;
-      gd.warp_split = gf.warp_split = (h->grad_form[c] == 2 || h->grad_form[c] == 4) ? 1 : 0;
-      gd.warp_threads = gf.warp_threads = h->grad_form[c] >= 3 ? 128 : 32;
-      if (grad_use_warp(h, c, e - b, fp32)) {
+      const int form = grad_form_of(h, c, fp32);
+      gd.warp_split = gf.warp_split = grad_form_split(form) ? 1 : 0;
+      gd.warp_threads = gf.warp_threads = grad_form_threads(form);
+      if (form >= 1) {
         const bool done = fp32 ? L->grad_warp_f(gf, h->pure, q + lo, nq, fp32 ? st_f : st_d)
                                : L->grad_warp_d(gd, h->pure, q + lo, nq, st_d);
         if (done) {
@@ -2197,7 +2201,7 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
     h->grad_class_mask = 1u << c;
     float best = 1e30f;
     int best_form = 0;
-    // thread, warp, warp split into four one-set passes, block of four warps (whole, split)
+    // thread, warp, warp split into four one-set passes, block of four or eight warps (whole, split)
     for (int form = 0; form < kGradForms; ++form) {
       h->grad_form[c] = form;
       if ((rc = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return rc;  // warm-up

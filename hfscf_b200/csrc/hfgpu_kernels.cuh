@@ -54,7 +54,7 @@ struct GradArgs {
   int smem_atoms;                    // grad_kernel: > 0 = accumulate 3 x smem_atoms entries per block in
                                      // shared memory, then one atomic per entry (0: atomics into grad)
   int warp_split;                    // grad_warp_kernel: 1 = four launches, one accumulator set each
-  int warp_threads;                  // grad_warp_kernel: threads per quartet (32 or 128; 0 = 32)
+  int warp_threads;                  // grad_warp_kernel: threads per quartet (32, 128 or 256; 0 = 32)
   int part, nparts;                  // partitioned gradients: the launch's quartet t is list entry
                                      // t * nparts + part (nparts <= 1: t); nq counts this part's
 };
@@ -979,18 +979,18 @@ __host__ __device__ constexpr int grad_warp_slots() {
 template <int NT>
 __device__ __forceinline__ void group_sync() {
   if constexpr (NT == 32)
-    group_sync<NT>();
+    __syncwarp();
   else
     __syncthreads();
 }
 
-// NT = 32: one warp per quartet; NT = 128: one block of four warps per quartet (the same
-// shared-memory tables, each level's rows spread over four times the threads, so that a
+// NT = 32: one warp per quartet; NT = 128 or 256: one block of four or eight warps per quartet
+// (the same shared-memory tables, each level's rows spread over more threads, so that a
 // quartet finishes sooner and more warps per SM hide the shared-memory latency).
 template <int LA, int LB, int LC, int LD, typename R, typename Tab, int NT = 32>
 __global__ void __launch_bounds__(NT) grad_warp_kernel(GradArgs<R> a, int pure, const int2* __restrict__ quartets,
                                                        int nq) {
-  static_assert(NT == 32 || NT == 64 || NT == 128, "threads per quartet");
+  static_assert(NT == 32 || NT == 128 || NT == 256, "threads per quartet");
   extern __shared__ __align__(16) unsigned char gwsm[];
   const int lane = threadIdx.x;  // 0 .. NT-1
   const int qi = blockIdx.x;

@@ -303,7 +303,7 @@ class Engine:
     def autotune_grad(self, D, precision=FP64, repeats=2) -> np.ndarray:
         """hfgpu_autotune_grad on density D (host array or device tensor): the gradient form per
         class (0 thread, 1 warp, 2 warp split per accumulator set, 3 block of four warps, 4 block
-        split per set, -1 no choice)."""
+        split per set, 5 and 6 the same with eight warps, -1 no choice)."""
         import torch
         Dd = D if isinstance(D, torch.Tensor) else torch.from_numpy(_c(D)).to(torch.device("cuda", self._opts.device))
         forms = np.zeros(NUM_CLASSES, dtype=np.int32)
@@ -313,7 +313,7 @@ class Engine:
 
     def set_grad_forms(self, forms):
         """hfgpu_set_grad_forms: the gradient form per class (-1, 0 thread, 1 warp, 2 warp split,
-        3 block, 4 block split)."""
+        3 block, 4 block split, 5 block of eight warps, 6 its split)."""
         f = np.ascontiguousarray(np.broadcast_to(np.asarray(forms, dtype=np.int32), (NUM_CLASSES,)))
         self._check(lib().hfgpu_set_grad_forms(self.h, f.ctypes.data_as(_ip)))
 

@@ -67,11 +67,10 @@ typedef struct {
   int device;              /* CUDA device ordinal (default 0) */
   int warp_max_quartets;   /* (dd|dp), (dd|dd): one warp per quartet when the class has at most this many
                               quartets, one thread per quartet otherwise (default 2^30 = always; -1 = never) */
-  int grad_warp_max_waves;    /* gradient of (dp|dp) (dd|pp) (dd|ds) (dd|dp) (dd|dd): one warp per quartet
-                                 (shared memory) when the class's quartets fill at most this many waves of
-                                 the blocks the GPU holds at once, else one thread per quartet on global
-                                 scratch (default 48: longer warp-form launches hold the shared memory of
-                                 every SM and stop the other classes' kernels from overlapping; 0 = never) */
+  int grad_warp_max_waves;    /* gradient of (dp|dp) (dd|pp) (dd|ds) (dd|dp) (dd|dd) before any
+                                 hfgpu_autotune_grad / hfgpu_set_grad_forms: > 0 (default 48) one block of
+                                 four warps per quartet over shared-memory tables (form 3), 0 = one thread
+                                 per quartet on global scratch (form 0) */
   int reserved[5];          /* reserved[0] = 1: arm every shared-memory staging wait without issuing its copy,
                               so that the bounded wait runs out (tests the timeout path; builds then report
                               status 2); 0 otherwise.  reserved[1] > 0: at most this many blocks per
@@ -281,18 +280,19 @@ int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
 int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule);
 int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule);
 /* Gradient form per class for the classes that have several (the op-table classes (dp|dp) (dd|pp)
- * (dd|ds) (dd|dp) (dd|dd)): times one warp or one 128-thread block per quartet (whole or split
+ * (dd|ds) (dd|dp) (dd|dd)): times one warp or one 128- or 256-thread block per quartet (whole or split
  * per set) against one thread per quartet for each class alone on the handle's lists and the
  * given device density D (RHF weights), keeps the fastest; then, on whole gradients, tries the
  * other forms per class and keeps one where it makes the gradient at least 1% faster (the
  * classes run concurrently), and returns the forms in forms[HFGPU_NUM_CLASSES] (0 thread, 1 warp,
  * 2 warp split into four launches of one accumulator set each, 3 block of four warps, 4 block
- * split into four launches, -1 class without a choice; may be NULL).  Until it runs,
- * opts.grad_warp_max_waves decides by quartet count (warp form or thread form).
+ * split into four launches, 5 and 6 the same with blocks of eight warps, -1 class without a
+ * choice; may be NULL).  Until it runs, the
+ * classes use form 3 (opts.grad_warp_max_waves > 0) or form 0 (opts.grad_warp_max_waves = 0).
  * Results do not depend on the form beyond FP64 summation order. */
 int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int repeats, int* forms);
-/* Sets the gradient forms directly (HFGPU_NUM_CLASSES ints, -1 .. 4, as hfgpu_autotune_grad returns them;
- * -1 = the quartet-count rule; ignored for classes without a choice). */
+/* Sets the gradient forms directly (HFGPU_NUM_CLASSES ints, -1 .. 6, as hfgpu_autotune_grad returns them;
+ * -1 = the default of opts.grad_warp_max_waves; ignored for classes without a choice). */
 int hfgpu_set_grad_forms(hfgpu_handle* h, const int* forms);
 int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule);
 

@@ -87,11 +87,12 @@ def test_autotuned_schedule_gives_the_same_fock_build():
     assert np.max(np.abs(Fm1 - Fm0)) < 1e-6
 
 
-@pytest.mark.parametrize("gmax", [0, 1 << 20], ids=["thread-per-quartet", "warp-per-quartet"])
+@pytest.mark.parametrize("gmax", [0, 48], ids=["thread-per-quartet", "block-per-quartet"])
 @pytest.mark.parametrize("name,bs", MOLS, ids=[m[0] for m in MOLS])
 def test_gradient_launch_forms_match_oracle(name, bs, gmax):
-    """The large gradient classes have a thread-per-quartet and a warp-per-quartet kernel;
-    each is forced in turn (FP64, tolerance 1e-10 as in test_gpu_parity)."""
+    """The default gradient form of the large classes under opts.grad_warp_max_waves: one thread
+    per quartet (0) or one block of four warps per quartet (> 0), each in turn (FP64, tolerance
+    1e-10 as in test_gpu_parity)."""
     rng = np.random.default_rng(31)
     D = _sym(rng, bs.nbf)
     g0 = oracle.grad2e_rhf(bs, D)
@@ -196,19 +197,20 @@ def test_gradient_form_autotuner_keeps_the_gradient():
     g0 = oracle.grad2e_rhf(bs, D)
     with E.Engine(bs) as eng:
         forms = eng.autotune_grad(D, repeats=1)
-        assert set(np.unique(forms)) <= {-1, 0, 1, 2, 3, 4} and (forms >= 0).any()
+        assert set(np.unique(forms)) <= {-1, 0, 1, 2, 3, 4, 5, 6} and (forms >= 0).any()
         g = eng.grad2e(D)
     assert np.max(np.abs(g - g0)) < 1e-10
 
 
-@pytest.mark.parametrize("form", [0, 1, 2, 3, 4],
-                         ids=["thread", "warp", "warp-split-per-set", "block", "block-split-per-set"])
+@pytest.mark.parametrize("form", [0, 1, 2, 3, 4, 5, 6],
+                         ids=["thread", "warp", "warp-split-per-set", "block", "block-split-per-set",
+                              "block8", "block8-split-per-set"])
 @pytest.mark.parametrize("name,bs", MOLS, ids=[m[0] for m in MOLS])
 def test_every_gradient_form_matches_oracle(name, bs, form):
     """Each gradient form of the op-table classes forced in turn: one thread per quartet, one
     warp per quartet, the warp form split into four launches of one accumulator set each, and
-    the same two with a block of four warps per quartet (FP64 1e-10, mixed 1e-6 against the
-    oracle)."""
+    the same two with a block of four or eight warps per quartet (FP64 1e-10, mixed 1e-6
+    against the oracle)."""
     rng = np.random.default_rng(47)
     D = _sym(rng, bs.nbf)
     g0 = oracle.grad2e_rhf(bs, D)
