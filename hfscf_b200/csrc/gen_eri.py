@@ -916,10 +916,18 @@ static void launch_quartet_impl(const QuartetArgs<R>& a, const int2* q, int nq, 
   if constexpr (CC::kWarp) {{
     using Tab = typename CC::WarpTab;
     constexpr int per = warp_slots<Tab, R>();
-    const int bytes = 4 * per * (int)sizeof(R);
-    auto k = quartet_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    k<<<(nq + 3) / 4, 128, bytes, s>>>(a, q, nq);
+    if (a.warp_threads == 128) {{
+      // one block of four warps per quartet
+      const int bytes = per * (int)sizeof(R);
+      auto k = quartet_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab, 128>;
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      k<<<nq, 128, bytes, s>>>(a, q, nq);
+    }} else {{
+      const int bytes = 4 * per * (int)sizeof(R);
+      auto k = quartet_warp_kernel<{la}, {lb}, {lc}, {ld}, R, Tab>;
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      k<<<(nq + 3) / 4, 128, bytes, s>>>(a, q, nq);
+    }}
   }}
 }}
 template <typename R>

@@ -209,6 +209,9 @@ int class_warp_max(const hfgpu_handle* h, int c) {
   return w < 0 ? h->opts.warp_max_quartets : (w ? INT_MAX : -1);
 }
 
+// threads per quartet of that form: schedule entry 2 = one block of 128 threads per quartet
+int class_warp_threads(const hfgpu_handle* h, int c) { return h->sched_warp[c] == 2 ? 128 : 32; }
+
 int cuda_fail(hfgpu_handle* h, cudaError_t e, const char* where) {
   return fail(h, e == cudaErrorMemoryAllocation ? HFGPU_ERR_NOMEM : HFGPU_ERR_CUDA,
               std::string(where) + ": " + cudaGetErrorString(e));
@@ -433,6 +436,7 @@ int compute_schwarz(hfgpu_handle* h) {
     const int b = h->class_begin[c], e = h->class_begin[c + 1];
     if (e <= b) continue;
     qa.warp_max = class_warp_max(h, quartet_class(c, c));
+    qa.warp_threads = class_warp_threads(h, quartet_class(c, c));
     qa.block = h->sched_block[quartet_class(c, c)];
     qa.capped = h->sched_cap[quartet_class(c, c)];
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[quartet_class(c, c)];
@@ -1043,6 +1047,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
     qd.capped = qf.capped = h->sched_cap[c];
     qd.group = qf.group = h->sched_primwarp[c] == 1 ? 32 : h->sched_primwarp[c];
     qd.warp_max = qf.warp_max = class_warp_max(h, c);
+    qd.warp_threads = qf.warp_threads = class_warp_threads(h, c);
     qd.staged = qf.staged = (h->sched_cap[c] == 2 && L->has_staged) ? 1 : 0;
     h->ev_used[c] = false;
     if (e <= b || !((h->class_mask >> c) & 1u)) continue;
@@ -1582,6 +1587,7 @@ int hfgpu_eri_packed(hfgpu_handle* h, double* eri_out, long long eri_len) {
       HF_CUDA(h, h->d_eriq.ensure(sizeof(int2) * list.size()));
       HF_CUDA(h, cudaMemcpyAsync(h->d_eriq.p, list.data(), sizeof(int2) * list.size(), cudaMemcpyHostToDevice, h->stream));
       qa.warp_max = class_warp_max(h, quartet_class(cp, cq));
+      qa.warp_threads = class_warp_threads(h, quartet_class(cp, cq));
       qa.block = h->sched_block[quartet_class(cp, cq)];
       qa.capped = h->sched_cap[quartet_class(cp, cq)];
       hfgpu::kClassLaunchers[quartet_class(cp, cq)]->quartet_d(qa, h->d_eriq.as<int2>(), (int)list.size(), h->stream);
@@ -1979,7 +1985,7 @@ int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule) {
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     const int bs = schedule[4 * c], pw = schedule[4 * c + 1], wp = schedule[4 * c + 2], cp = schedule[4 * c + 3];
     if ((bs != 32 && bs != 64 && bs != 128) || (pw != 0 && pw != 1 && pw != 4 && pw != 8 && pw != 16 && pw != 32) ||
-        wp < -1 || wp > 1 || cp < 0 || cp > 3)
+        wp < -1 || wp > 2 || cp < 0 || cp > 3)
       return fail(h, HFGPU_ERR_INVALID, "schedule entry out of range");
   }
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
@@ -2038,7 +2044,7 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
   std::vector<Cand> kind_best((size_t)4 * hfgpu::kNumClasses, Cand{1e30f, 0, 0, 0, 0});
   auto kind_of = [&](int c, int pw, int wp, int cap) {
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
-    return wp == 1 ? 2 : (L->has_primwarp && pw > 0 ? 1 : (cap == 2 && L->has_staged ? 3 : 0));
+    return wp >= 1 ? 2 : (L->has_primwarp && pw > 0 ? 1 : (cap == 2 && L->has_staged ? 3 : 0));
   };
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     if (h->q_end[c] <= h->q_beg[c]) continue;
@@ -2046,8 +2052,8 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
     h->class_mask = 1u << c;
     float best = 1e30f;
     int bb = h->sched_block[c], bp = h->sched_primwarp[c], bw = h->sched_warp[c], bc = h->sched_cap[c];
-    const int warps[2] = {1, 0};
-    for (int wi = 0; wi < (L->has_warp ? 2 : 1); ++wi) {
+    const int warps[3] = {2, 1, 0};  // block per quartet, warp per quartet, thread forms
+    for (int wi = 0; wi < (L->has_warp ? 3 : 1); ++wi) {
       const int wp = L->has_warp ? warps[wi] : -1;
       const int pws[5] = {32, 16, 8, 4, 0};
       for (int pi = (L->has_primwarp ? 0 : 4); pi < 5; ++pi) {
@@ -2058,7 +2064,7 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
           const int bs = 32 << (cand % 3), cap = cand / 3;
           if ((cap == 1 && !L->has_capped) || (cap == 2 && !L->has_staged) || (cap == 3 && !L->has_lowres))
             continue;
-          if (wp == 1 && (bs != 64 || cap)) continue;  // the warp form has its own block shape
+          if (wp >= 1 && (bs != 64 || cap)) continue;  // the warp and block forms have their own shape
           h->sched_block[c] = bs;
           h->sched_primwarp[c] = L->has_primwarp ? pw : 1;
           h->sched_warp[c] = wp;

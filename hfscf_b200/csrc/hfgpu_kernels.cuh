@@ -242,6 +242,7 @@ struct QuartetArgs {
   double* eri;          // PACKED output
   PairInfo* pairs_rw;   // SCHWARZ output
   int warp_max;         // large classes: warp per quartet up to this many quartets
+  int warp_threads;     // threads per quartet of that form: 32 (four quartets per block) or 128
   int block;            // threads per block of the thread-per-quartet form (32, 64 or 128; 0 = 64)
   int group;            // lanes per quartet of the primitive-split form (4, 8, 16 or 32; 0 = 32)
   int capped;           // 1: the register-capped variant of the thread form (classes that have one)
@@ -717,7 +718,16 @@ __global__ void __launch_bounds__(128) grad_kernel(GradArgs<R> a, int pure, cons
 // ---------------------------------------------------------------------------
 // Warp-per-quartet kernel for the large classes (generated levelised tables).
 // ---------------------------------------------------------------------------
-template <typename R>
+// Synchronisation of the threads that share one quartet: a warp, or a whole block.
+template <int NT>
+__device__ __forceinline__ void group_sync() {
+  if constexpr (NT == 32)
+    __syncwarp();
+  else
+    __syncthreads();
+}
+
+template <typename R, int NT = 32>
 __device__ __forceinline__ void warp_to_pure(const R* src, R* dst0, R* dst1, const int* Ls, int lane, const R** out) {
   // one index at a time, ping-pong between dst0 and dst1
   int dims[4] = {ncart_of(Ls[0]), ncart_of(Ls[1]), ncart_of(Ls[2]), ncart_of(Ls[3])};
@@ -729,7 +739,7 @@ __device__ __forceinline__ void warp_to_pure(const R* src, R* dst0, R* dst1, con
     nd[st] = np;
     R* o = bufs[st & 1];
     const int tot = nd[0] * nd[1] * nd[2] * nd[3];
-    for (int e = lane; e < tot; e += 32) {
+    for (int e = lane; e < tot; e += NT) {
       int id[4];
       int r = e;
       for (int q = 3; q >= 0; --q) {
@@ -746,26 +756,26 @@ __device__ __forceinline__ void warp_to_pure(const R* src, R* dst0, R* dst1, con
       }
       o[e] = v;
     }
-    __syncwarp();
+    group_sync<NT>();
     for (int q = 0; q < 4; ++q) dims[q] = nd[q];
     in = o;
   }
   *out = in;
 }
 
-template <typename R>
+template <typename R, int NT = 32>
 __device__ __forceinline__ void warp_digest(const R* V, int NA, int NB, int NC, int ND, int fa, int fb, int fc, int fd,
                                             double s, const double* __restrict__ DJ, int nK,
                                             const double* __restrict__ DK, double* Jh, double* Kh, int n, int lane) {
   const int NCD = NC * ND;
   if (DJ != nullptr) {
-    for (int x = lane; x < NA * NB; x += 32) {
+    for (int x = lane; x < NA * NB; x += NT) {
       double acc = 0.0;
       for (int c = 0; c < NC; ++c)
         for (int d = 0; d < ND; ++d) acc += __ldg(DJ + (size_t)(fc + c) * n + fd + d) * double(V[x * NCD + c * ND + d]);
       atomicAdd(Jh + (size_t)(fa + x / NB) * n + fb + x % NB, 2.0 * s * acc);
     }
-    for (int y = lane; y < NCD; y += 32) {
+    for (int y = lane; y < NCD; y += NT) {
       double acc = 0.0;
       for (int a = 0; a < NA; ++a)
         for (int b = 0; b < NB; ++b) acc += __ldg(DJ + (size_t)(fa + a) * n + fb + b) * double(V[(a * NB + b) * NCD + y]);
@@ -775,28 +785,28 @@ __device__ __forceinline__ void warp_digest(const R* V, int NA, int NB, int NC, 
   for (int m = 0; m < nK; ++m) {
     const double* D = DK + (size_t)m * n * n;
     double* K = Kh + (size_t)m * n * n;
-    for (int x = lane; x < NA * NC; x += 32) {  // K_ac += D_bd V
+    for (int x = lane; x < NA * NC; x += NT) {  // K_ac += D_bd V
       const int a = x / NC, c = x % NC;
       double acc = 0.0;
       for (int b = 0; b < NB; ++b)
         for (int d = 0; d < ND; ++d) acc += __ldg(D + (size_t)(fb + b) * n + fd + d) * double(V[((a * NB + b) * NC + c) * ND + d]);
       atomicAdd(K + (size_t)(fa + a) * n + fc + c, s * acc);
     }
-    for (int x = lane; x < NA * ND; x += 32) {  // K_ad += D_bc V
+    for (int x = lane; x < NA * ND; x += NT) {  // K_ad += D_bc V
       const int a = x / ND, d = x % ND;
       double acc = 0.0;
       for (int b = 0; b < NB; ++b)
         for (int c = 0; c < NC; ++c) acc += __ldg(D + (size_t)(fb + b) * n + fc + c) * double(V[((a * NB + b) * NC + c) * ND + d]);
       atomicAdd(K + (size_t)(fa + a) * n + fd + d, s * acc);
     }
-    for (int x = lane; x < NB * NC; x += 32) {  // K_bc += D_ad V
+    for (int x = lane; x < NB * NC; x += NT) {  // K_bc += D_ad V
       const int b = x / NC, c = x % NC;
       double acc = 0.0;
       for (int a = 0; a < NA; ++a)
         for (int d = 0; d < ND; ++d) acc += __ldg(D + (size_t)(fa + a) * n + fd + d) * double(V[((a * NB + b) * NC + c) * ND + d]);
       atomicAdd(K + (size_t)(fb + b) * n + fc + c, s * acc);
     }
-    for (int x = lane; x < NB * ND; x += 32) {  // K_bd += D_ac V
+    for (int x = lane; x < NB * ND; x += NT) {  // K_bd += D_ac V
       const int b = x / ND, d = x % ND;
       double acc = 0.0;
       for (int a = 0; a < NA; ++a)
@@ -811,16 +821,19 @@ constexpr int warp_slots() {
   return Tab::NVSLOT + 1 + Tab::NHSLOT + 1 + 2 * Tab::NCART;
 }
 
-// One warp per unique quartet: the levelised VRR and HRR run lane-parallel out
-// of shared memory; transform and digestion are lane-parallel over the block.
-template <int LA, int LB, int LC, int LD, typename R, typename Tab>
+// One warp per unique quartet (NT = 32, four quartets per 128-thread block) or one block of
+// NT = 128 threads per quartet: the levelised VRR and HRR run lane-parallel out of shared
+// memory; transform and digestion are lane-parallel over the quartet's threads.
+template <int LA, int LB, int LC, int LD, typename R, typename Tab, int NT = 32>
 __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, const int2* __restrict__ quartets,
                                                            int nq) {
+  static_assert(NT == 32 || NT == 128, "threads per quartet");
   extern __shared__ __align__(16) unsigned char wsmem[];
+  __shared__ double wred[4];
   constexpr int PER = warp_slots<Tab, R>();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int qi = blockIdx.x * (blockDim.x >> 5) + w;
-  if (qi >= launch_count(qa, nq)) return;  // whole warp
+  const int lane = NT == 32 ? (threadIdx.x & 31) : threadIdx.x, w = NT == 32 ? (threadIdx.x >> 5) : 0;
+  const int qi = NT == 32 ? blockIdx.x * (blockDim.x >> 5) + w : blockIdx.x;
+  if (qi >= launch_count(qa, nq)) return;  // the quartet's whole warp or block
   R* vs = reinterpret_cast<R*>(wsmem) + (size_t)w * PER;
   R* hs = vs + Tab::NVSLOT + 1;
   R* A = hs + Tab::NHSLOT + 1;
@@ -846,8 +859,8 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
     vs[Tab::NVSLOT] = R(0);
     hs[Tab::NHSLOT] = R(0);
   }
-  for (int t = lane; t < Tab::NACC; t += 32) hs[t] = R(0);
-  __syncwarp();
+  for (int t = lane; t < Tab::NACC; t += NT) hs[t] = R(0);
+  group_sync<NT>();
   const PrimPair<R>* bp = a.prims + P.prim_off;
   const PrimPair<R>* kp = a.prims + Q.prim_off;
   const int4* vo = Tab::vrr();  // packed rows, see gen_eri.py pack_warp_vrr / pack_warp_hrr
@@ -872,7 +885,7 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
 #pragma unroll
       for (int m = 0; m <= Tab::L; ++m)
         if (lane == m) vs[m] = F[m];
-      __syncwarp();
+      group_sync<NT>();
       for (int l = 0; l < Tab::NVLEV; ++l) {
         const int e = __ldg(vl + l + 1);
         // two op rows in flight per lane: the rows of one level are independent
@@ -893,17 +906,17 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
           }
           vs[dst] = v;
         };
-        for (int o = __ldg(vl + l) + lane; o < e; o += 64) {
+        for (int o = __ldg(vl + l) + lane; o < e; o += 2 * NT) {
           const int4 opa = __ldg(vo + o);
-          const bool two = o + 32 < e;
-          const int4 opb = two ? __ldg(vo + o + 32) : opa;
+          const bool two = o + NT < e;
+          const int4 opb = two ? __ldg(vo + o + NT) : opa;
           body(opa);
           if (two) body(opb);
         }
-        __syncwarp();
+        group_sync<NT>();
       }
-      for (int t = lane; t < Tab::NACC; t += 32) hs[t] += vs[__ldg(accs + t)];
-      __syncwarp();
+      for (int t = lane; t < Tab::NACC; t += NT) hs[t] += vs[__ldg(accs + t)];
+      group_sync<NT>();
     }
   }
   const int2* ho = Tab::hrr();
@@ -917,23 +930,23 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
       const R d = (kd & 1) ? (dir == 0 ? CDx : (dir == 1 ? CDy : CDz)) : (dir == 0 ? ABx : (dir == 1 ? ABy : ABz));
       hs[op.x & 0xffff] = hs[(unsigned)op.x >> 16] + d * hs[op.y & 0xffff];
     };
-    for (int o = __ldg(hl + l) + lane; o < e; o += 64) {
+    for (int o = __ldg(hl + l) + lane; o < e; o += 2 * NT) {
       const int2 opa = __ldg(ho + o);
-      const bool two = o + 32 < e;
-      const int2 opb = two ? __ldg(ho + o + 32) : opa;
+      const bool two = o + NT < e;
+      const int2 opb = two ? __ldg(ho + o + NT) : opa;
       body(opa);
       if (two) body(opb);
     }
-    __syncwarp();
+    group_sync<NT>();
   }
   const int* outs = Tab::out();
-  for (int o = lane; o < Tab::NCART; o += 32) A[o] = hs[__ldg(outs + o)];
-  __syncwarp();
+  for (int o = lane; o < Tab::NCART; o += NT) A[o] = hs[__ldg(outs + o)];
+  group_sync<NT>();
   const R* V = A;
   int NA = ncart_of(LA), NB = ncart_of(LB), NC = ncart_of(LC), ND = ncart_of(LD);
   if (qa.pure) {
     const int Ls[4] = {LA, LB, LC, LD};
-    warp_to_pure<R>(A, Bb, A, Ls, lane, &V);
+    warp_to_pure<R, NT>(A, Bb, A, Ls, lane, &V);
     NA = npure_of(LA);
     NB = npure_of(LB);
     NC = npure_of(LC);
@@ -947,20 +960,26 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
     long long blk;
     int nm;
     mol_block(a.mol_off, a.mol_n, P.mol, a.n, blk, nm);
-    warp_digest<R>(V, NA, NB, NC, ND, P.fa, P.fb, Q.fa, Q.fb, s, off_ptr(a.DJ, blk), a.nK, off_ptr(a.DK, blk),
+    warp_digest<R, NT>(V, NA, NB, NC, ND, P.fa, P.fb, Q.fa, Q.fb, s, off_ptr(a.DJ, blk), a.nK, off_ptr(a.DK, blk),
                    off_ptr(a.Jh, blk), off_ptr(a.Kh, blk), nm, lane);
   } else if (qa.mode == QMODE_PACKED) {
-    for (int e = lane; e < NA * NB * NC * ND; e += 32) {
+    for (int e = lane; e < NA * NB * NC * ND; e += NT) {
       const int l = e % ND, k = (e / ND) % NC, j = (e / (ND * NC)) % NB, i = e / (ND * NC * NB);
       qa.eri[packed_index(P.fa + i, P.fb + j, Q.fa + k, Q.fb + l)] = double(V[e]);
     }
   } else {
     double m = 0.0;
-    for (int x = lane; x < NA * NB; x += 32) {
+    for (int x = lane; x < NA * NB; x += NT) {
       const int i = x / NB, j = x % NB;
       m = fmax(m, fabs(double(V[((i * NB + j) * NC + i) * ND + j])));
     }
     for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if constexpr (NT > 32) {  // the block's warps through shared memory
+      if ((lane & 31) == 0) wred[lane >> 5] = m;
+      __syncthreads();
+      if (lane == 0)
+        for (int k = 1; k < NT / 32; ++k) m = fmax(m, wred[k]);
+    }
     if (lane == 0) qa.pairs_rw[pq.x].schwarz = sqrt(m);
   }
 }
@@ -974,14 +993,6 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
 template <typename Tab, typename R>
 __host__ __device__ constexpr int grad_warp_slots() {
   return Tab::NVSLOT + 1 + Tab::NHSLOT + 1 + 3 * Tab::NCART;
-}
-
-template <int NT>
-__device__ __forceinline__ void group_sync() {
-  if constexpr (NT == 32)
-    __syncwarp();
-  else
-    __syncthreads();
 }
 
 // NT = 32: one warp per quartet; NT = 128 or 256: one block of four or eight warps per quartet

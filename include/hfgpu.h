@@ -260,8 +260,10 @@ int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
  *   [1] lanes per quartet of the primitive-split form used for quartets with at least 16
  *       primitive quartets (4, 8, 16, 32; 1 = 32; 0 = thread form; classes without that
  *       form ignore it);
- *   [2] 1/0/-1 = warp-per-quartet form for the classes that have one, (dp|pp) (dp|ds) (dp|dp)
- *       (dd|pp) (dd|ds) (dd|dp) (dd|dd) (-1 = follow opts.warp_max_quartets);
+ *   [2] 2/1/0/-1 = block-per-quartet form (128 threads per quartet) / warp-per-quartet form
+ *       (four quartets per 128-thread block) for the classes that have one, (dp|pp) (dp|ds)
+ *       (dp|dp) (dd|pp) (dd|ds) (dd|dp) (dd|dd) / thread forms (-1 = follow
+ *       opts.warp_max_quartets with the warp form);
  *   [3] variant of the thread-per-quartet form: 0 plain; 1 register-capped, for more warps
  *       per SM (the small classes (ps|ss) ... (dp|ss) have one); 2 persistent, with the
  *       class's Boys table staged into shared memory by one bulk (TMA) copy per block (the
@@ -272,7 +274,7 @@ int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
  * autotune: times every form of every class on the current geometry with device density D
  * (n x n; `repeats` builds per candidate, one class at a time on the handle's stream),
  * keeps the fastest; then, on whole builds, tries per class the best candidate of each other
- * kind of form (thread, primitive-split, warp) and keeps it where the build gets at least 1%
+ * kind of form (thread, primitive-split, warp or block) and keeps it where the build gets at least 1%
  * faster; keeps the result only if whole builds with it beat whole builds with the schedule
  * it started from, and returns the schedule in `schedule` (may be NULL).
  * Results of later builds do not depend on the schedule beyond FP64 summation order. */

@@ -80,9 +80,10 @@ def test_partitioned_jk_in_a_pure_basis_and_mixed_precision():
 
 
 # Schedules forcing one J/K form for every class that has it: thread form (plain), the
-# primitive-split form with 8 lanes, the warp-per-quartet form, the staged persistent form and
-# the low-residency form (the grids of all of them are sized from the part's share).
-FORCED = {"thread": (64, 0, 0, 0), "primwarp8": (128, 8, 0, 0), "warp": (64, 0, 1, 0),
+# primitive-split form with 8 lanes, the warp-per-quartet and block-per-quartet forms, the staged
+# persistent form and the low-residency form (the grids of all of them are sized from the part's
+# share).
+FORCED = {"thread": (64, 0, 0, 0), "primwarp8": (128, 8, 0, 0), "warp": (64, 0, 1, 0), "block": (64, 0, 2, 0),
           "staged": (64, 0, 0, 2), "lowres": (128, 0, 0, 3)}
 
 

@@ -36,7 +36,7 @@ MOLS = _molecules()
 # (block, primwarp, warp, capped) applied to every class
 # capped = 2: the persistent form with the Boys table staged in shared memory (classes of L <= 4)
 FORMS = [(32, 0, 0, 0), (64, 1, 0, 1), (128, 0, 1, 0), (64, 1, 1, 0), (64, 4, 0, 1), (32, 8, 1, 1), (128, 16, 0, 0),
-         (64, 0, 0, 2), (128, 4, 0, 2), (32, 0, 1, 2), (64, 0, 0, 3), (128, 0, -1, 3)]
+         (64, 0, 0, 2), (128, 4, 0, 2), (32, 0, 1, 2), (64, 0, 0, 3), (128, 0, -1, 3), (64, 0, 2, 0), (64, 8, 2, 0)]
 
 
 @pytest.mark.parametrize("form", FORMS, ids=[f"b{f[0]}-pw{f[1]}-w{f[2]}-c{f[3]}" for f in FORMS])
@@ -53,6 +53,19 @@ def test_every_launch_form_matches_oracle(name, bs, form):
         J, K = eng.jk(D, [D])
     assert np.max(np.abs(eri - eri0)) < ERI_TOL
     assert np.max(np.abs(J - J0)) < MAT_TOL and np.max(np.abs(K[0] - K0)) < MAT_TOL
+
+
+def test_schwarz_factors_under_the_block_form():
+    """The Schwarz pass of set_geometry runs the large classes through the scheduled form too; in
+    the block-per-quartet form its per-pair maximum is reduced over the block's warps."""
+    bs = MOLS[1][1]
+    with E.Engine(bs) as eng0:
+        q0 = eng0.schwarz()
+    with E.Engine(bs) as eng:
+        eng.set_schedule(np.tile(np.array((64, 0, 2, 0), dtype=np.int32), (E.NUM_CLASSES, 1)))
+        eng.set_geometry(bs.coords)
+        q1 = eng.schwarz()
+    assert np.max(np.abs(q1 - q0)) < 1e-12
 
 
 def test_set_schedule_rejects_bad_entries():
