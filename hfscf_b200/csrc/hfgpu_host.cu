@@ -2008,6 +2008,31 @@ int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule) {
   return HFGPU_OK;
 }
 
+// Tuner timing: the median device time of `repeats` runs of run() on the handle's stream, each
+// after a write of the buffer `flush` (larger than L2, when it could be allocated), the way the
+// bench times its steps; one untimed warm-up run first.  A median of separately timed runs
+// rather than one total keeps a single slow run from deciding a comparison.
+template <typename Run>
+static int tuner_time(hfgpu_handle* h, Run&& run, int repeats, cudaEvent_t e0, cudaEvent_t e1, const DevBuf& flush,
+                      float* ms) {
+  int rc;
+  if ((rc = run())) return rc;
+  float t[100];
+  repeats = std::max(1, std::min(repeats, 100));
+  for (int r = 0; r < repeats; ++r) {
+    if (flush.p) HF_CUDA(h, cudaMemsetAsync(flush.p, r & 0xff, flush.bytes, h->stream));
+    HF_CUDA(h, cudaEventRecord(e0, h->stream));
+    if ((rc = run())) return rc;
+    HF_CUDA(h, cudaEventRecord(e1, h->stream));
+    HF_CUDA(h, cudaEventSynchronize(e1));
+    HF_CUDA(h, cudaEventElapsedTime(&t[r], e0, e1));
+  }
+  std::sort(t, t + repeats);
+  *ms = repeats % 2 ? t[repeats / 2] : 0.5f * (t[repeats / 2 - 1] + t[repeats / 2]);
+  return HFGPU_OK;
+}
+constexpr size_t kTunerFlushBytes = (size_t)256 << 20;  // 256 MiB > the 126 MB L2
+
 // Per class, times every launch form the class has on the handle's current quartet lists
 // and the given density, one class at a time on the handle's stream, and keeps the fastest.
 int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule) {
@@ -2023,16 +2048,23 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
     cudaEventDestroy(e0);
     return fail(h, HFGPU_ERR_CUDA, "cudaEventCreate");
   }
-  struct Restore {  // the mask goes back on every exit path
+  struct Restore {  // the mask goes back and the flush buffer is freed on every exit path
     hfgpu_handle* h;
     unsigned mask;
     cudaEvent_t a, b;
+    DevBuf flush;
     ~Restore() {
       h->class_mask = mask;
       cudaEventDestroy(a);
       cudaEventDestroy(b);
+      flush.release();
     }
-  } restore{h, h->class_mask, e0, e1};
+  } restore{h, h->class_mask, e0, e1, DevBuf{}};
+  if (restore.flush.ensure(kTunerFlushBytes) != cudaSuccess) {
+    cudaGetLastError();  // no room for the flush buffer: time without it
+    restore.flush = DevBuf{};
+  }
+  auto build = [&]() { return jk_device_impl(h, D, 1, D, nullptr, nullptr, precision); };
   int start[4 * 21];
   hfgpu_get_schedule(h, start);
   // best candidate per class and kind of form: 0 thread per quartet, 1 primitive-split for
@@ -2069,14 +2101,8 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
           h->sched_primwarp[c] = L->has_primwarp ? pw : 1;
           h->sched_warp[c] = wp;
           h->sched_cap[c] = cap;
-          if ((rc = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return rc;  // warm-up
-          HF_CUDA(h, cudaEventRecord(e0, h->stream));
-          for (int r = 0; r < repeats; ++r)
-            if ((rc = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return rc;
-          HF_CUDA(h, cudaEventRecord(e1, h->stream));
-          HF_CUDA(h, cudaEventSynchronize(e1));
           float ms = 0.f;
-          HF_CUDA(h, cudaEventElapsedTime(&ms, e0, e1));
+          if ((rc = tuner_time(h, build, repeats, e0, e1, restore.flush, &ms))) return rc;
           if (ms < best) {
             best = ms;
             bb = bs;
@@ -2099,16 +2125,9 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
   // class, the best candidate of each other kind replaces the current form if the build
   // gets at least 1% faster.
   h->class_mask = restore.mask;
+  // whole builds: at least five runs per median
   auto time_builds = [&](float* ms) -> int {
-    int r0;
-    if ((r0 = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return r0;  // warm-up
-    HF_CUDA(h, cudaEventRecord(e0, h->stream));
-    for (int r = 0; r < repeats; ++r)
-      if ((r0 = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return r0;
-    HF_CUDA(h, cudaEventRecord(e1, h->stream));
-    HF_CUDA(h, cudaEventSynchronize(e1));
-    HF_CUDA(h, cudaEventElapsedTime(ms, e0, e1));
-    return HFGPU_OK;
+    return tuner_time(h, build, std::max(repeats, 5), e0, e1, restore.flush, ms);
   };
   float cur = 0.f;
   if ((rc = time_builds(&cur))) return rc;
@@ -2142,14 +2161,8 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
   for (int round = 0; round < 2; ++round)
     for (int which = 0; which < 2; ++which) {
       if ((rc = hfgpu_set_schedule(h, which ? start : tuned))) return rc;
-      if ((rc = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return rc;  // warm-up
-      HF_CUDA(h, cudaEventRecord(e0, h->stream));
-      for (int r = 0; r < repeats; ++r)
-        if ((rc = jk_device_impl(h, D, 1, D, nullptr, nullptr, precision))) return rc;
-      HF_CUDA(h, cudaEventRecord(e1, h->stream));
-      HF_CUDA(h, cudaEventSynchronize(e1));
       float ms = 0.f;
-      HF_CUDA(h, cudaEventElapsedTime(&ms, e0, e1));
+      if ((rc = time_builds(&ms))) return rc;
       (which ? t_start : t_tuned) += ms;
     }
   if ((rc = hfgpu_set_schedule(h, t_tuned <= t_start ? tuned : start))) return rc;
@@ -2191,15 +2204,22 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
     cudaEventDestroy(e0);
     return fail(h, HFGPU_ERR_CUDA, "cudaEventCreate");
   }
-  struct Restore {  // the class mask goes back on every exit path
+  struct Restore {  // the class mask goes back and the flush buffer is freed on every exit path
     hfgpu_handle* h;
     cudaEvent_t a, b;
+    DevBuf flush;
     ~Restore() {
       h->grad_class_mask = ~0u;
       cudaEventDestroy(a);
       cudaEventDestroy(b);
+      flush.release();
     }
-  } restore{h, e0, e1};
+  } restore{h, e0, e1, DevBuf{}};
+  if (restore.flush.ensure(kTunerFlushBytes) != cudaSuccess) {
+    cudaGetLastError();  // no room for the flush buffer: time without it
+    restore.flush = DevBuf{};
+  }
+  auto gradient = [&]() { return grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision); };
   // RHF weights (cJ = 2, cK = 1) on the given density, one class at a time, each form timed
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
@@ -2210,14 +2230,8 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
     // thread, warp, warp split into four one-set passes, block of four or eight warps (whole, split)
     for (int form = 0; form < kGradForms; ++form) {
       h->grad_form[c] = form;
-      if ((rc = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return rc;  // warm-up
-      HF_CUDA(h, cudaEventRecord(e0, h->stream));
-      for (int r = 0; r < repeats; ++r)
-        if ((rc = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return rc;
-      HF_CUDA(h, cudaEventRecord(e1, h->stream));
-      HF_CUDA(h, cudaEventSynchronize(e1));
       float ms = 0.f;
-      HF_CUDA(h, cudaEventElapsedTime(&ms, e0, e1));
+      if ((rc = tuner_time(h, gradient, repeats, e0, e1, restore.flush, &ms))) return rc;
       if (ms < best) {
         best = ms;
         best_form = form;
@@ -2230,15 +2244,7 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
   // class the other form replaces the chosen one if the whole gradient gets at least 1% faster.
   h->grad_class_mask = ~0u;
   auto time_all = [&](float* ms) -> int {
-    int r0;
-    if ((r0 = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return r0;  // warm-up
-    HF_CUDA(h, cudaEventRecord(e0, h->stream));
-    for (int r = 0; r < repeats; ++r)
-      if ((r0 = grad_device_impl(h, D, 2.0, 1, D, 1.0, g.as<double>(), precision))) return r0;
-    HF_CUDA(h, cudaEventRecord(e1, h->stream));
-    HF_CUDA(h, cudaEventSynchronize(e1));
-    HF_CUDA(h, cudaEventElapsedTime(ms, e0, e1));
-    return HFGPU_OK;
+    return tuner_time(h, gradient, std::max(repeats, 5), e0, e1, restore.flush, ms);
   };
   float cur = 0.f;
   if ((rc = time_all(&cur))) return rc;

@@ -91,7 +91,7 @@ def test_autotuned_schedule_gives_the_same_fock_build():
         sched = eng.autotune(D, repeats=2)
         assert sched.shape == (E.NUM_CLASSES, 4)
         assert set(np.unique(sched[:, 0])) <= {32, 64, 128}
-        assert set(np.unique(sched[:, 1])) <= {0, 1, 4, 8, 16, 32} and set(np.unique(sched[:, 2])) <= {-1, 0, 1}
+        assert set(np.unique(sched[:, 1])) <= {0, 1, 4, 8, 16, 32} and set(np.unique(sched[:, 2])) <= {-1, 0, 1, 2}
         assert set(np.unique(sched[:, 3])) <= {0, 1, 2, 3}
         assert (eng.get_schedule() == sched).all()
         F1 = eng.fock_rhf(D, H)
