@@ -2012,6 +2012,7 @@ int hfgpu_get_schedule(const hfgpu_handle* h, int* schedule) {
 // after a write of the buffer `flush` (larger than L2, when it could be allocated), the way the
 // bench times its steps; one untimed warm-up run first.  A median of separately timed runs
 // rather than one total keeps a single slow run from deciding a comparison.
+extern "C++" {
 template <typename Run>
 static int tuner_time(hfgpu_handle* h, Run&& run, int repeats, cudaEvent_t e0, cudaEvent_t e1, const DevBuf& flush,
                       float* ms) {
@@ -2031,6 +2032,7 @@ static int tuner_time(hfgpu_handle* h, Run&& run, int repeats, cudaEvent_t e0, c
   *ms = repeats % 2 ? t[repeats / 2] : 0.5f * (t[repeats / 2 - 1] + t[repeats / 2]);
   return HFGPU_OK;
 }
+}  // extern "C++"
 constexpr size_t kTunerFlushBytes = (size_t)256 << 20;  // 256 MiB > the 126 MB L2
 
 // Per class, times every launch form the class has on the handle's current quartet lists
