@@ -463,9 +463,10 @@ int bound_decade(double b) {
 // Quartet list of one class (pair classes cp >= cq), in four segments (Schwarz bound at or
 // above the mixed-precision bound / below, each split into quartets with at least
 // kPrimWarpMinPrims primitive quartets / fewer), each ordered by one stable counting sort
-// on (bound decade, largest primitive-quartet count first): the decades make the prefix
-// launches of density-screened builds possible, the counts let the 32 lanes of a warp loop
-// over similar numbers of primitive quartets.
+// on (bound decade, then the primitive shape: ket primitive pairs, then bra primitive pairs,
+// largest first): the decades make the prefix launches of density-screened builds possible,
+// the shapes let the 32 lanes of a warp run the same trip counts of both primitive loops (a
+// sort on the product alone mixes 3 x 1 with 1 x 3).
 //
 // Built in two parallel phases on all host threads.  Phase 1 filters the candidates of
 // chunks of about kListChunkWork candidate quartets (consecutive bra pairs of one class) and
@@ -473,13 +474,13 @@ int bound_decade(double b) {
 // (class, segment) with one counting sort over its chunks in order and writes it into place.
 // The lists are the same as those of one serial pass per class in bra-pair order.
 constexpr long long kListChunkWork = 1 << 20;
-constexpr int kProdSpan = 1 << 16;  // primitive-quartet counts above this share the last sort slot
+constexpr int kProdSpan = 1 << 16;  // primitive shapes above this share the last sort slot
 
 struct ListChunk {
   int cls = 0;                  // index into the class table (cp, cq)
   int P0 = 0, P1 = 0;           // bra pairs [P0, P1)
   std::vector<int2> q[4];       // survivors per segment, in list order
-  std::vector<int> key[4];      // bound decade * kProdSpan + primitive-quartet count
+  std::vector<int> key[4];      // bound decade * kProdSpan + primitive shape
   int maxprod[4] = {0, 0, 0, 0};
   long long prims = 0;          // primitive quartets of the survivors
 };
@@ -544,6 +545,9 @@ int build_quartets(hfgpu_handle* h) {
   const int threads = all_work < 2 * kListChunkWork ? 1 : (int)std::max(1u, std::thread::hardware_concurrency());
   // phase 1: filter
   const double tol = h->opts.schwarz_tol, mix = h->opts.mixed_fp32_bound;
+  // primitive shape of a quartet: ket primitive pairs * shape_mul + bra primitive pairs
+  int shape_mul = 1;
+  for (int P = 0; P < (int)h->pairs.size(); ++P) shape_mul = std::max(shape_mul, h->pairs[P].nprim + 1);
   run_parallel((int)chunks.size(), threads, [&](int ci) {
     ListChunk& c = chunks[ci];
     const int cp = cls[c.cls].first, cq = cls[c.cls].second;
@@ -556,11 +560,12 @@ int build_quartets(hfgpu_handle* h) {
         const double b = qp * h->pairs[Q].schwarz;
         if (b < tol) continue;
         c.prims += (long long)np * h->pairs[Q].nprim;
-        const int prod = std::min(np * h->pairs[Q].nprim, kProdSpan - 1);
+        const int prod = np * h->pairs[Q].nprim;
+        const int shape = (int)std::min<long long>((long long)h->pairs[Q].nprim * shape_mul + np, kProdSpan - 1);
         const int sg = (b >= mix ? 0 : 2) + (prod >= kPrimWarpMinPrims ? 0 : 1);
         c.q[sg].push_back(make_int2(P, Q));
-        c.key[sg].push_back(bound_decade(b) * kProdSpan + prod);
-        c.maxprod[sg] = std::max(c.maxprod[sg], prod);
+        c.key[sg].push_back(bound_decade(b) * kProdSpan + shape);
+        c.maxprod[sg] = std::max(c.maxprod[sg], shape);
       }
     }
   });
