@@ -294,6 +294,24 @@ def device_build_ms(eng, D, reps, torch, flush):
     return tot / reps
 
 
+def tune_best_of(eng, D0, trials, torch, flush, device):
+    """hfgpu_autotune run `trials` times on the core-guess density D0 (each run starts from the
+    schedule the previous one left); the schedule whose flushed builds on D0 were fastest (median
+    of 7) is kept.  One tuner run chooses among forms whose times differ by less than the
+    run-to-run spread of a whole build, so its result varies; the best of a few is stable."""
+    import numpy as np
+    from hfscf_b200 import engine as E
+    Dd = torch.from_numpy(np.ascontiguousarray(D0)).to(device)
+    best = None
+    for _ in range(trials):
+        sched = eng.autotune(D0, E.FP64, 3)
+        ms = sorted(device_build_ms(eng, Dd, 1, torch, flush) for _ in range(7))[3]
+        if best is None or ms < best[0]:
+            best = (ms, sched)
+    eng.set_schedule(best[1])
+    return best
+
+
 def other_configs(local, stream, flush, oracle_refs, autotune):
     """Configurations 1, 3 and 4: Fock build time, SCF + gradient time to solution in FP64 and
     mixed precision, and their errors against the oracle's energies and gradients."""
@@ -398,13 +416,16 @@ def run_ours(args, world, rank, local):
     eng = E.Engine(bs, device=local)
     eng.set_stream(stream.cuda_stream)
     # --- untimed set-up: launch schedule, converged SCF (FP64), gradient, mixed-precision SCF ---
+    dev = torch.device("cuda", local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
     tune_s = None
+    tuned_ms, tuned_sched = None, None
     if not args.no_autotune:
         from hfscf_b200.profile_case import core_guess_density
         S0, T0, V0 = E.one_electron(bs)
         t = time.perf_counter()
         D0 = core_guess_density(bs, S0, T0 + V0)
-        eng.autotune(D0, E.FP64, 3)
+        tuned_ms, tuned_sched = tune_best_of(eng, D0, 3, torch, flush, torch.device("cuda", local))
         eng.autotune_grad(D0, E.FP64, 2)
         tune_s = time.perf_counter() - t
     # SCF + gradient time-to-solution, FP64 and mixed, each from the SAD guess (the
@@ -414,13 +435,11 @@ def run_ours(args, world, rank, local):
     res_mx, grad_mx, mixed_wall, grad_mx_wall = (tts["mixed"][k] for k in ("res", "grad", "scf_s", "grad_s"))
     S, T, V = E.one_electron(bs)
     H = T + V
-    dev = torch.device("cuda", local)
     D = torch.from_numpy(np.ascontiguousarray(res.D)).to(dev)
     Hd = torch.from_numpy(np.ascontiguousarray(H)).to(dev)
     J = torch.empty((n, n), dtype=torch.float64, device=dev)
     K = torch.empty((n, n), dtype=torch.float64, device=dev)
     F = torch.empty((n, n), dtype=torch.float64, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
 
     def step():
         eng.jk_device(D.data_ptr(), 1, D.data_ptr(), J.data_ptr(), K.data_ptr())
@@ -553,8 +572,9 @@ def run_ours(args, world, rank, local):
             "config": {"workload": WORKLOAD, "nbf": n, "parallelism": f"replicas x{world}",
                        "l2": "flushed between steps (256 MiB write)",
                        "schedule": ("default" if tune_s is None else
-                                    f"hfgpu_autotune and hfgpu_autotune_grad on the core-guess density "
-                                    f"({tune_s:.2f} s, untimed)"),
+                                    f"best of three hfgpu_autotune runs, and hfgpu_autotune_grad, on the "
+                                    f"core-guess density ({tune_s:.2f} s, untimed)"),
+                       "schedule_table": None if tuned_sched is None else tuned_sched.tolist(),
                        "quartets_screened": int(sum(class_work[c]["screened"] for c in range(E.NUM_CLASSES))),
                        "quartets_computed_last_build": int(sum(class_work[c]["computed"] for c in range(E.NUM_CLASSES)))},
             "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "sharded": sharded,
