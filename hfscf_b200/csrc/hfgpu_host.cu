@@ -144,6 +144,9 @@ struct hfgpu_handle {
   std::vector<long long> q_beg, q_mid, q_end, q_hik1, q_hik2;
   std::vector<long long> q_prims;  // per class: primitive quartets of the Schwarz-screened quartets
   int part = 0, nparts = 1;        // partition of every quartet list (hfgpu_set_partition)
+  // classes of a J/K build / a gradient on the auxiliary streams concurrently (0) or one after
+  // another on one of them (1); chosen by the autotuners on whole builds
+  int jk_serial = 0, grad_serial = 0;
   // inside each of the four segments quartets are ordered by Schwarz-bound decade
   // (largest first; inside a decade by primitive-quartet count, then bra-major):
   // bucket_end[(c * 4 + seg) * kBuckets + e] is the
@@ -1043,7 +1046,7 @@ static int jk_device_impl(hfgpu_handle* h, const double* DJ, int nK, const doubl
   class_schedule(order, sidx);
   for (int i = 0; i < hfgpu::kNumClasses; ++i) {
     const int c = order[i];
-    cudaStream_t st = h->aux[sidx[i]];
+    cudaStream_t st = h->aux[h->jk_serial ? 0 : sidx[i]];
     const hfgpu::ClassLaunchers* L = hfgpu::kClassLaunchers[c];
     const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
     qd.jk.counters = cnt + 3 * c;
@@ -1242,8 +1245,8 @@ static int grad_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     const long long b = h->q_beg[c], m = h->q_mid[c], e = h->q_end[c];
     if (e <= b || !((h->grad_class_mask >> c) & 1u)) continue;
     const int slots = L->grad_scratch_slots(h->pure);
-    cudaStream_t st_d = h->aux[rr++ % hfgpu_handle::kAux];
-    cudaStream_t st_f = precision == HFGPU_MIXED ? h->aux[rr++ % hfgpu_handle::kAux] : st_d;
+    cudaStream_t st_d = h->aux[h->grad_serial ? 0 : rr++ % hfgpu_handle::kAux];
+    cudaStream_t st_f = precision == HFGPU_MIXED ? h->aux[h->grad_serial ? 0 : rr++ % hfgpu_handle::kAux] : st_d;
     auto run = [&](bool fp32, long long lo, long long hi) -> int {
       const int nq = (int)part_share(h, hi - lo);
       if (nq <= 0) return HFGPU_OK;
@@ -2173,6 +2176,18 @@ int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats,
       (which ? t_start : t_tuned) += ms;
     }
   if ((rc = hfgpu_set_schedule(h, t_tuned <= t_start ? tuned : start))) return rc;
+  // the classes concurrently on the auxiliary streams, or one after another
+  {
+    float t_conc = 0.f, t_ser = 0.f;
+    for (int round = 0; round < 2; ++round)
+      for (int ser = 0; ser < 2; ++ser) {
+        h->jk_serial = ser;
+        float ms = 0.f;
+        if ((rc = time_builds(&ms))) return rc;
+        (ser ? t_ser : t_conc) += ms;
+      }
+    h->jk_serial = t_ser < 0.99f * t_conc ? 1 : 0;
+  }
   return schedule ? hfgpu_get_schedule(h, schedule) : HFGPU_OK;
 }
 
@@ -2269,6 +2284,18 @@ int hfgpu_autotune_grad(hfgpu_handle* h, const double* D, int precision, int rep
       else
         h->grad_form[c] = before;
     }
+  }
+  // the classes concurrently on the auxiliary streams, or one after another
+  {
+    float t_conc = 0.f, t_ser = 0.f;
+    for (int round = 0; round < 2; ++round)
+      for (int ser = 0; ser < 2; ++ser) {
+        h->grad_serial = ser;
+        float ms = 0.f;
+        if ((rc = time_all(&ms))) return rc;
+        (ser ? t_ser : t_conc) += ms;
+      }
+    h->grad_serial = t_ser < 0.99f * t_conc ? 1 : 0;
   }
   if (forms)
     for (int c = 0; c < hfgpu::kNumClasses; ++c) forms[c] = h->grad_form[c];

@@ -276,7 +276,11 @@ int hfgpu_setup_times(const hfgpu_handle* h, double* ms);
  * keeps the fastest; then, on whole builds, tries per class the best candidate of each other
  * kind of form (thread, primitive-split, warp or block) and keeps it where the build gets at least 1%
  * faster; keeps the result only if whole builds with it beat whole builds with the schedule
- * it started from, and returns the schedule in `schedule` (may be NULL).
+ * it started from, and returns the schedule in `schedule` (may be NULL).  Last, it times the
+ * classes of a build one after another on one stream against concurrently on six and keeps
+ * the serial order where it is at least 1% faster (the handle keeps that choice; it is not
+ * part of the schedule array).  Every timing is the median of separately timed runs, each
+ * after an L2 flush.
  * Results of later builds do not depend on the schedule beyond FP64 summation order. */
 #define HFGPU_NUM_CLASSES 21
 int hfgpu_autotune(hfgpu_handle* h, const double* D, int precision, int repeats, int* schedule);
@@ -286,7 +290,8 @@ int hfgpu_set_schedule(hfgpu_handle* h, const int* schedule);
  * per set) against one thread per quartet for each class alone on the handle's lists and the
  * given device density D (RHF weights), keeps the fastest; then, on whole gradients, tries the
  * other forms per class and keeps one where it makes the gradient at least 1% faster (the
- * classes run concurrently), and returns the forms in forms[HFGPU_NUM_CLASSES] (0 thread, 1 warp,
+ * classes run concurrently; last, one after another on one stream against concurrently, as for
+ * the J/K build), and returns the forms in forms[HFGPU_NUM_CLASSES] (0 thread, 1 warp,
  * 2 warp split into four launches of one accumulator set each, 3 block of four warps, 4 block
  * split into four launches, 5 and 6 the same with blocks of eight warps, -1 class without a
  * choice; may be NULL).  Until it runs, the
