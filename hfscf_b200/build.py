@@ -54,6 +54,9 @@ def _compile(src, verbose):
     deps = [src] + _common_headers() + [os.path.join(CSRC, "hfgpu_onee.h")]
     if base.startswith("inst_"):
         deps.append(os.path.join(GEN, "class_" + base[5:] + ".cuh"))
+    elif base.startswith("hess_") and base != "hess_dispatch":
+        deps += [os.path.join(GEN, base + ".cuh"), os.path.join(CSRC, "hfgpu_hess_kernels.cuh"),
+                 os.path.join(CSRC, "hfgpu_hess_launch.h")]
     else:  # hand-written sources: every hand-written header counts
         deps += sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")))
     stamp = obj + ".sha1"
@@ -75,13 +78,20 @@ def _compile(src, verbose):
 def build(jobs: int | None = None, verbose: bool = False) -> str:
     os.makedirs(OBJ, exist_ok=True)
     generate()
-    srcs = sorted(glob.glob(os.path.join(GEN, "inst_*.cu"))) + [os.path.join(GEN, "dispatch.cu"),
+    srcs = sorted(glob.glob(os.path.join(GEN, "inst_*.cu"))) + sorted(glob.glob(os.path.join(GEN, "hess_*.cu"))) + \
+        [os.path.join(GEN, "dispatch.cu"),
                                                                  os.path.join(CSRC, "hfgpu_host.cu"),
                                                                  os.path.join(CSRC, "hfgpu_noalloc.cu"),
                                                                  os.path.join(CSRC, "hfgpu_onee.cpp")]
     # largest classes first so they do not finish last
-    srcs.sort(key=lambda s: -os.path.getsize(os.path.join(GEN, "class_" + os.path.basename(s)[5:-3] + ".cuh"))
-              if os.path.basename(s).startswith("inst_") else 0)
+    def _size(s):
+        b = os.path.basename(s)
+        if b.startswith("inst_"):
+            return os.path.getsize(os.path.join(GEN, "class_" + b[5:-3] + ".cuh"))
+        if b.startswith("hess_") and b != "hess_dispatch.cu":
+            return os.path.getsize(os.path.join(GEN, b[:-3] + ".cuh"))
+        return 0
+    srcs.sort(key=lambda s: -_size(s))
     jobs = jobs or os.cpu_count() or 4
     changed = False
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:

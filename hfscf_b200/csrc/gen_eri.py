@@ -1045,6 +1045,29 @@ const ClassLaunchers launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_quartet<d
 """
 
 
+HESS_INST_TEMPLATE = """// GENERATED by gen_eri.py -- do not edit.
+#include "../hfgpu_hess_kernels.cuh"
+#include "hess_{t}.cuh"
+#include "../hfgpu_hess_launch.h"
+
+namespace hfgpu {{
+static void launch_hess(const GradArgs<double>& a, const HessOut& o, int pure, const int2* q, int nq, int grid,
+                        int smem, cudaStream_t s) {{
+  if (nq <= 0) return;
+  auto k = hess_kernel<{la}, {lb}, {lc}, {ld}, HessTable{t}>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  k<<<grid, 128, smem, s>>>(a, o, pure, q, nq);
+}}
+static int hess_scratch_slots(int) {{
+  return HessTable{t}::NVSLOT + HessTable{t}::NHSLOT + 45 +
+         3 * BlockDims<{la}, {lb}, {lc}, {ld}, false>::NCART;
+}}
+extern const HessLaunchers hess_launchers_{t};
+const HessLaunchers hess_launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_hess, &hess_scratch_slots}};
+}}  // namespace hfgpu
+"""
+
+
 def main(outdir):
     import os
     os.makedirs(outdir, exist_ok=True)
@@ -1068,6 +1091,27 @@ def main(outdir):
         la, lb, lc, ld = c
         write_if_changed(os.path.join(outdir, f"inst_{t}.cu"), INST_TEMPLATE.format(t=t, la=la, lb=lb, lc=lc, ld=ld))
         names.append(t)
+    # the adjoint Hessian: one table header and one launcher unit per class
+    hnames = []
+    meta["hess"] = []
+    for c in cls:
+        t = "".join(map(str, c))
+        code_h, mh = gen_hess_table(*c)
+        meta["hess"].append(mh)
+        write_if_changed(os.path.join(outdir, f"hess_{t}.cuh"),
+                         "// GENERATED by gen_eri.py -- do not edit.\n#pragma once\n#include \"common.cuh\"\n\n" +
+                         code_h + "\n")
+        la, lb, lc, ld = c
+        write_if_changed(os.path.join(outdir, f"hess_{t}.cu"), HESS_INST_TEMPLATE.format(t=t, la=la, lb=lb, lc=lc, ld=ld))
+        hnames.append(t)
+    hd = ["// GENERATED by gen_eri.py -- do not edit.", '#include "../hfgpu_hess_launch.h"', "namespace hfgpu {"]
+    hd += [f"extern const HessLaunchers hess_launchers_{t};" for t in hnames]
+    hd.append(f"const HessLaunchers* const kHessLaunchers[{len(hnames)}] = {{")
+    hd += [f"  &hess_launchers_{t}," for t in hnames]
+    hd.append("};")
+    hd.append(f"const int kNumHessClasses = {len(hnames)};")
+    hd.append("}  // namespace hfgpu")
+    write_if_changed(os.path.join(outdir, "hess_dispatch.cu"), "\n".join(hd) + "\n")
     disp = ["// GENERATED by gen_eri.py -- do not edit.", '#include "../hfgpu_launch.h"', "namespace hfgpu {"]
     for t in names:
         disp.append(f"extern const ClassLaunchers launchers_{t};")
@@ -1691,6 +1735,195 @@ def gen_warp_class(la, lb, lc, ld):
     meta = {"class": [la, lb, lc, ld], "vrr_ops": len(vrows), "vrr_levels": len(vlev) - 1, "vrr_slots": nvs,
             "acc": nacc, "hrr_ops": len(hrows), "hrr_levels": len(hlv) - 1, "hrr_slots": nhs,
             "smem_doubles_per_warp": nvs + 1 + nhs + 1 + 2 * ncart_blk}
+    return "\n".join(s), meta
+
+
+
+# ---------------------------------------------------------------------------
+# Adjoint second derivatives (the two-electron part of the Hessian at a fixed density):
+# H[X][Y] += sum_abcd W_abcd d2(ab|cd)/dX dY for X, Y in {A, B, C} x {x, y, z}; centre D
+# follows from translational invariance on the host side of the kernel.  A derivative by
+# centre P in direction i acts on a primitive as 2 alpha_P (p + 1_i) - p_i (p - 1_i); applying
+# it twice gives integrals with the angular momentum of up to two centres shifted by one or two,
+# weighted by one of ten exponent products (HESS_SETS; the factors 2 alpha are in the weights).
+# ---------------------------------------------------------------------------
+HESS_SETS = [(), ("A",), ("B",), ("C",), ("A", "A"), ("B", "B"), ("C", "C"), ("A", "B"), ("A", "C"), ("B", "C")]
+HESS_COORDS = [(P, i) for P in range(3) for i in range(3)]
+HESS_PAIRS = [(r, s) for r in range(9) for s in range(r, 9)]   # 45 outputs, upper triangle
+
+
+def _d1(P, i, comps):
+    """First derivative by centre P (0, 1, 2 = A, B, C) in direction i of the Cartesian
+    components comps = (a, b, c, d): [(coefficient, weight centres, shifted components)]."""
+    up = list(comps)
+    up[P] = add(comps[P], i)
+    out = [(1, ("ABC"[P],), tuple(up))]
+    v = comps[P][i]
+    if v > 0:
+        dn = list(comps)
+        dn[P] = add(comps[P], i, -1)
+        out.append((-v, (), tuple(dn)))
+    return out
+
+
+def hess_terms(la, lb, lc, ld):
+    """[(output index, W index, coefficient, set index, a, b, c, d)]: the second derivative
+    of (ab|cd) by coordinates r <= s of HESS_PAIRS as integer combinations of shifted
+    integrals of the ten weight sets."""
+    terms = []
+    w = 0
+    for a in cart(la):
+        for b in cart(lb):
+            for c in cart(lc):
+                for d in cart(ld):
+                    comps = (a, b, c, d)
+                    for hi, (r, s) in enumerate(HESS_PAIRS):
+                        (P, i), (Q, j) = HESS_COORDS[r], HESS_COORDS[s]
+                        acc = {}
+                        for c1, w1, comps1 in _d1(Q, j, comps):
+                            for c2, w2, comps2 in _d1(P, i, comps1):
+                                key = (tuple(sorted(w1 + w2)), comps2)
+                                acc[key] = acc.get(key, 0) + c1 * c2
+                        for (ws, cs), k in sorted(acc.items()):
+                            if k:
+                                terms.append((hi, w, k, HESS_SETS.index(ws)) + cs)
+                    w += 1
+    return terms
+
+
+def pack_hess_hrr(r):
+    """HRR op {dst | x<<16, y | kind<<16 | dir<<20} (kind 0 bra, 1 ket) or contraction
+    {W index | x<<16, (coef + 128) | 2<<16 | out<<20}."""
+    kind = r[0]
+    if kind == 2:
+        _, hi, wi, x, k = r
+        assert -128 <= k < 128 and 0 <= hi < 45
+        return (_i32(_u16(wi) | _u16(x) << 16), _i32((k + 128) | 2 << 16 | hi << 20))
+    _, i, dst, x, y = r
+    return (_i32(_u16(dst) | _u16(x) << 16), _i32(_u16(y) | kind << 16 | i << 20))
+
+
+def gen_hess_table(la, lb, lc, ld):
+    """Op tables of the adjoint Hessian of one class, run by hess_table() (one thread per
+    quartet on thread-interleaved scratch): the VRR two orders higher with every target
+    accumulated into the weight sets that need it, the HRR of each set to the shifted
+    classes, and one contraction row per term of hess_terms."""
+    L = la + lb + lc + ld + 2
+    terms = hess_terms(la, lb, lc, ld)
+    # HRR over lazily numbered values: accumulators ("acc", set, e, f) first discovered, the
+    # intermediate values after; both renumbered below
+    acc_ids, hnodes, hops = {}, {}, []
+    counter = [0]
+
+    def new_id():
+        counter[0] += 1
+        return ("h", counter[0] - 1)
+
+    def ket(k, e, c, d):
+        key = ("k", k, e, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(d) == 0:
+            v = ("acc", k, e, c)
+            acc_ids.setdefault(v, len(acc_ids))
+        else:
+            i = max(range(3), key=lambda q: (d[q], -q))
+            d1 = add(d, i, -1)
+            x, y = ket(k, e, add(c, i), d1), ket(k, e, c, d1)
+            v = new_id()
+            hops.append((1, i, v, x, y))
+        hnodes[key] = v
+        return v
+
+    def bra(k, a, b, c, d):
+        key = ("b", k, a, b, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(b) == 0:
+            v = ket(k, a, c, d)
+        else:
+            i = max(range(3), key=lambda q: (b[q], -q))
+            b1 = add(b, i, -1)
+            x, y = bra(k, add(a, i), b1, c, d), bra(k, a, b1, c, d)
+            v = new_id()
+            hops.append((0, i, v, x, y))
+        hnodes[key] = v
+        return v
+
+    for hi, wi, k, si, a, b, c, d in terms:
+        x = bra(si, a, b, c, d)
+        hops.append((2, hi, wi, x, k))
+    nacc = len(acc_ids)
+    # value numbering for the HRR region: slot 0 = zero, accumulator j at 1 + j, then the rest
+    vid = {v: 1 + j for v, j in acc_ids.items()}
+    nxt = [1 + nacc]
+
+    def num(v):
+        if v not in vid:
+            vid[v] = nxt[0]
+            nxt[0] += 1
+        return vid[v]
+
+    huses, hdefs = [], []
+    for o in hops:
+        if o[0] == 2:
+            huses.append([num(o[3])])
+            hdefs.append([])
+        else:
+            huses.append([num(o[3]), num(o[4])])
+            hdefs.append([num(o[2])])
+    hpre = {1 + j: 1 + j for j in range(nacc)}
+    hslot, nhslot = linear_scan(nxt[0], huses, hdefs, hpre)
+    hrows = []
+    for o in hops:
+        if o[0] == 2:
+            _, hi, wi, x, k = o
+            hrows.append((2, hi, wi, hslot[vid[x]], k))
+        else:
+            kind, i, v, x, y = o
+            hrows.append((kind, i, hslot[vid[v]], hslot[vid[x]], hslot[vid[y]]))
+    # VRR: every accumulator is [e0|f0]^(0) of its set
+    dag = Dag(L)
+    tgt_nodes = {}
+    for (_, k, e, f), j in acc_ids.items():
+        tgt_nodes.setdefault(dag.get(e, f, 0), []).append((k, j))
+    ops, uses, defs = [], [], []
+    for nid, node in enumerate(dag.nodes):
+        if node[0] != "F":
+            kind, i, a, b, c, d, g, k1, k2 = node
+            ops.append(["K" if kind == "K" else "B", i, nid, a, b, c, d, g, k1, k2])
+            uses.append([x for x in (a, b, c, d, g) if x >= 0])
+            defs.append([nid])
+        for (k, j) in tgt_nodes.get(nid, []):
+            ops.append(["A", k, j, nid, -1, -1, -1, -1, 0, 0])
+            uses.append([nid])
+            defs.append([])
+    pre = {m: 1 + m for m in range(L + 1)}  # F[m] lives in slot 1+m
+    slot, nvslot = linear_scan(len(dag.nodes), uses, defs, pre)
+    kinds = {"B": 0, "K": 1, "A": 2}
+    vrows = []
+    for o in ops:
+        k, i, dst, a, b, c, d, g, k1, k2 = o
+        if k == "A":
+            vrows.append((2, i, dst, slot[a], 0, 0, 0, 0, 0, 0))
+        else:
+            sl = lambda x: slot[x] if x >= 0 else 0
+            vrows.append((kinds[k], i, slot[dst], sl(a), sl(b), sl(c), sl(d), sl(g), k1, k2))
+    t = f"{la}{lb}{lc}{ld}"
+    s = [f"// table-mode adjoint Hessian of class {t}: {len(vrows)} VRR ops over {nvslot} slots, {nacc} "
+         f"accumulators in {len(HESS_SETS)} weight sets, {len(hrows)} HRR/contraction ops over {nhslot} slots"]
+    s.append(f"__device__ const int4 hvrr_{t}[{len(vrows)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_grad_vrr(r))) + "}," for r in vrows]
+    s.append("};")
+    s.append(f"__device__ const int2 hhrr_{t}[{len(hrows)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_hess_hrr(r))) + "}," for r in hrows]
+    s.append("};")
+    s.append(f"struct HessTable{t} {{ static constexpr int L = {L}, NVOPS = {len(vrows)}, NVSLOT = {nvslot}, "
+             f"NACC = {nacc}, NHOPS = {len(hrows)}, NHSLOT = {nhslot}; "
+             f"static __device__ const int4* vrr() {{ return hvrr_{t}; }} "
+             f"static __device__ const int2* hrr() {{ return hhrr_{t}; }} }};")
+    meta = {"class": [la, lb, lc, ld], "vrr_ops": len(vrows), "vrr_slots": nvslot, "accumulators": nacc,
+            "hrr_ops": len(hrows), "hrr_slots": nhslot, "terms": len(terms)}
     return "\n".join(s), meta
 
 

@@ -1,0 +1,218 @@
+// Adjoint second derivatives of the two-electron energy at a fixed density: the two-electron
+// part of the analytic Hessian, sum_abcd W_abcd d2(ab|cd)/dX dY, with the same weight block
+// W as the adjoint gradient (RHF: W = 8 s [2 D_ab D_cd - (D_ac D_bd + D_ad D_bc)/2]).
+//
+// Replaces the reference's second-derivative ERI tensors and their contraction:
+// Erios::compute_contracted_shell_quartet_deriv2_qq / _pq (src/integrals/hfscf_oserideriv2qq.cpp:28-853,
+// hfscf_oserideriv2pq.cpp:23-891) and Mol::scf_hessian::calc_scf_hessian_tei
+// (src/hessian/hfscf_hessian_ints.cpp:20-303), which store six packed derivative tensors per
+// direction pair and then contract them once per atom pair.  Here nothing is stored: one thread
+// per unique shell quartet runs the class's generated op tables (gen_eri.py gen_hess_table) on
+// thread-interleaved global scratch, contracts every shifted integral with W on the fly and adds
+// the quartet's 12 x 12 block (centres A, B, C, D by x, y, z; D from translational invariance)
+// into the 3 natoms x 3 natoms Hessian.
+#pragma once
+#include "hfgpu_kernels.cuh"
+
+// Hessian output of a launch: 3 natoms x 3 natoms, row-major.  smem > 0: the block sums its
+// contributions in shared memory (9 natoms^2 doubles) and adds them once at its end.
+struct HessOut {
+  double* __restrict__ hess;
+  int natoms;
+  int smem;
+};
+
+// Executor of a table-mode Hessian class.  Weight sets, in the generator's order:
+// 1, 2a_a, 2a_b, 2a_c, (2a_a)^2, (2a_b)^2, (2a_c)^2, 2a_a 2a_b, 2a_a 2a_c, 2a_b 2a_c.
+// h45: the 45 upper-triangle entries of the 9 x 9 block over (A, B, C) x (x, y, z).
+template <typename Tab>
+__device__ void hess_table(const PrimPair<double>* __restrict__ bp, const double* __restrict__ ea,
+                           const double* __restrict__ eb, int nbp, const PrimPair<double>* __restrict__ kp,
+                           const double* __restrict__ ec, int nkp, double ABx, double ABy, double ABz, double CDx,
+                           double CDy, double CDz, const BoysTable<double>& boys, Strided<double> W,
+                           Strided<double> vs, Strided<double> hs, Strided<double> h45) {
+  using R = double;
+  vs[0] = R(0);
+  hs[0] = R(0);
+  for (int x = 1; x <= Tab::NACC; ++x) hs[x] = R(0);
+  const int4* vo = Tab::vrr();  // packed rows: gen_eri.py pack_grad_vrr / pack_hess_hrr
+  const int2* ho = Tab::hrr();
+  for (int ib = 0; ib < nbp; ++ib) {
+    const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;
+    const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;
+    const R wa = R(2) * ea[ib], wb = R(2) * eb[ib];
+    for (int ik = 0; ik < nkp; ++ik) {
+      const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;
+      const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;
+      const R wc = R(2) * ec[ik];
+      const R pq = p + q;
+      const R rsq = rsqrt_t(pq);
+      const R ipq = rsq * rsq;
+      const R rho = p * q * ipq;
+      const R rp = q * ipq, rq = p * ipq;
+      const R inv2p = R(0.5) * ip, inv2q = R(0.5) * iq, inv2pq = R(0.5) * ipq;
+      const R PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+      const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+      const R pre = Kab * Kcd * rsq;
+      R F[Tab::L + 1];
+      boys.template eval<Tab::L>(T, pre, F);
+#pragma unroll
+      for (int m = 0; m <= Tab::L; ++m) vs[1 + m] = F[m];
+      for (int o = 0; o < Tab::NVOPS; ++o) {
+        const int4 op = __ldg(vo + o);
+        const int kind = op.w & 15, dir = (op.w >> 4) & 15, dst = op.x & 0xffff;
+        const int sa = (unsigned)op.x >> 16, sb = op.y & 0xffff, sc = (unsigned)op.y >> 16, sd = op.z & 0xffff;
+        if (kind == 2) {
+          R w;
+          switch (dir) {
+            case 0: w = R(1); break;
+            case 1: w = wa; break;
+            case 2: w = wb; break;
+            case 3: w = wc; break;
+            case 4: w = wa * wa; break;
+            case 5: w = wb * wb; break;
+            case 6: w = wc * wc; break;
+            case 7: w = wa * wb; break;
+            case 8: w = wa * wc; break;
+            default: w = wb * wc; break;
+          }
+          hs[1 + dst] += w * vs[sa];
+          continue;
+        }
+        const R PQd = dir == 0 ? PQx : (dir == 1 ? PQy : PQz);
+        const int k1 = (op.w >> 8) & 255;
+        if (kind == 0) {
+          const R PA = dir == 0 ? PAx : (dir == 1 ? PAy : PAz);
+          vs[dst] = PA * vs[sa] - rp * PQd * vs[sb] + small_int<R>(k1) * inv2p * (vs[sc] - rp * vs[sd]);
+        } else {
+          const R QC = dir == 0 ? QCx : (dir == 1 ? QCy : QCz);
+          const int sg = (unsigned)op.z >> 16, k2 = (unsigned)op.w >> 16;
+          vs[dst] = QC * vs[sa] + rq * PQd * vs[sb] + small_int<R>(k1) * inv2q * (vs[sc] - rq * vs[sd]) +
+                    small_int<R>(k2) * inv2pq * vs[sg];
+        }
+      }
+    }
+  }
+  for (int x = 0; x < 45; ++x) h45[x] = R(0);
+  for (int o = 0; o < Tab::NHOPS; ++o) {
+    const int2 op = __ldg(ho + o);
+    const int kind = (op.y >> 16) & 15;
+    const int sx = (unsigned)op.x >> 16;
+    if (kind == 2) {
+      const int wi = op.x & 0xffff, k = (op.y & 0xffff) - 128, hi = (op.y >> 20) & 63;
+      h45[hi] += R(k) * W[wi] * hs[sx];
+    } else {
+      const int dst = op.x & 0xffff, sy = op.y & 0xffff, dir = (op.y >> 20) & 15;
+      const R d = kind == 0 ? (dir == 0 ? ABx : (dir == 1 ? ABy : ABz)) : (dir == 0 ? CDx : (dir == 1 ? CDy : CDz));
+      hs[dst] = hs[sx] + d * hs[sy];
+    }
+  }
+}
+
+// Position of coordinate pair (r, s), r <= s, of the 9 x 9 block in the 45-entry upper triangle.
+__device__ __forceinline__ int hess_tri(int r, int s) { return r * 9 - r * (r - 1) / 2 + (s - r); }
+
+template <int LA, int LB, int LC, int LD, bool PURE, typename Tab>
+__device__ __forceinline__ void hess_quartet(const GradArgs<double>& a, const HessOut& o, int tid, const int2 pq,
+                                             double* hout, int n3) {
+  using Dm = BlockDims<LA, LB, LC, LD, PURE>;
+  const PairInfo P = a.pairs[pq.x];
+  const PairInfo Q = a.pairs[pq.y];
+  double s = 8.0;
+  if (P.sa == P.sb) s *= 0.5;
+  if (Q.sa == Q.sb) s *= 0.5;
+  if (pq.x == pq.y) s *= 0.5;
+  // scratch per thread: [VRR slots | HRR slots | 45 outputs | W cart | 2 transform buffers]
+  double* base = a.scratch + tid;
+  const int st = a.scratch_threads;
+  Strided<double> vs{base, st};
+  Strided<double> hs{base + (size_t)Tab::NVSLOT * st, st};
+  Strided<double> h45{base + (size_t)(Tab::NVSLOT + Tab::NHSLOT) * st, st};
+  Strided<double> Wc{base + (size_t)(Tab::NVSLOT + Tab::NHSLOT + 45) * st, st};
+  Strided<double> t0{base + (size_t)(Tab::NVSLOT + Tab::NHSLOT + 45 + Dm::NCART) * st, st};
+  Strided<double> t1{base + (size_t)(Tab::NVSLOT + Tab::NHSLOT + 45 + 2 * Dm::NCART) * st, st};
+  if constexpr (PURE) {
+    grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb, Q.fa, Q.fb, s, t0);
+    // pure -> Cartesian weights, one index at a time: t0 -> t1 -> t0 -> t1 -> Wc
+    const int Ls[4] = {LA, LB, LC, LD};
+    int dims[4] = {Dm::NA, Dm::NB, Dm::NC, Dm::ND};
+    Strided<double> src = t0, dst = t1;
+    for (int stp = 0; stp < 4; ++stp) {
+      const int nc = ncart_of(Ls[stp]), np = npure_of(Ls[stp]);
+      int nd[4] = {dims[0], dims[1], dims[2], dims[3]};
+      nd[stp] = nc;
+      Strided<double> out = (stp == 3) ? Wc : dst;
+      const int tot = nd[0] * nd[1] * nd[2] * nd[3];
+      for (int e = 0; e < tot; ++e) {
+        int id[4];
+        int r = e;
+        for (int qq = 3; qq >= 0; --qq) {
+          id[qq] = r % nd[qq];
+          r /= nd[qq];
+        }
+        double v = 0.0;
+        for (int c = 0; c < np; ++c) {
+          const double y = c_ylm[Ls[stp]][id[stp] * np + c];
+          if (y == 0.0) continue;
+          int jd[4] = {id[0], id[1], id[2], id[3]};
+          jd[stp] = c;
+          v += y * src[((jd[0] * dims[1] + jd[1]) * dims[2] + jd[2]) * dims[3] + jd[3]];
+        }
+        out[e] = v;
+      }
+      for (int qq = 0; qq < 4; ++qq) dims[qq] = nd[qq];
+      Strided<double> tmp = src;
+      src = dst;
+      dst = tmp;
+    }
+  } else {
+    grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb, Q.fa, Q.fb, s, Wc);
+  }
+  hess_table<Tab>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
+                  a.prims + Q.prim_off, a.alpha_a + Q.prim_off, Q.nprim, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz,
+                  a.boys, Wc, vs, hs, h45);
+  // 12 x 12 block over centres A, B, C, D: a D row or column is minus the sum of the A, B, C ones
+  const int at[4] = {P.atom_a, P.atom_b, Q.atom_a, Q.atom_b};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double hx[4][4];
+      for (int X = 0; X < 3; ++X)
+        for (int Y = 0; Y < 3; ++Y) {
+          const int r = 3 * X + i, c = 3 * Y + j;
+          hx[X][Y] = r <= c ? h45[hess_tri(r, c)] : h45[hess_tri(c, r)];
+        }
+      for (int X = 0; X < 3; ++X) hx[X][3] = -(hx[X][0] + hx[X][1] + hx[X][2]);
+      for (int Y = 0; Y < 4; ++Y) hx[3][Y] = -(hx[0][Y] + hx[1][Y] + hx[2][Y]);
+      for (int X = 0; X < 4; ++X)
+        for (int Y = 0; Y < 4; ++Y)
+          if (hx[X][Y] != 0.0) atomicAdd(hout + (size_t)(3 * at[X] + i) * n3 + 3 * at[Y] + j, hx[X][Y]);
+    }
+}
+
+template <int LA, int LB, int LC, int LD, typename Tab>
+__global__ void __launch_bounds__(128) hess_kernel(GradArgs<double> a, HessOut o, int pure,
+                                                   const int2* __restrict__ quartets, int nq) {
+  extern __shared__ double hess_sh[];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthr = gridDim.x * blockDim.x;
+  const int n3 = 3 * o.natoms;
+  double* hout = o.hess;
+  if (o.smem) {
+    for (int i = threadIdx.x; i < n3 * n3; i += blockDim.x) hess_sh[i] = 0.0;
+    __syncthreads();
+    hout = hess_sh;
+  }
+  const int np = a.nparts > 1 ? a.nparts : 1, p0 = np > 1 ? a.part : 0;
+  for (int t = tid; t < nq; t += nthr) {
+    const int2 pq = quartets[(size_t)t * np + p0];
+    if (pure)
+      hess_quartet<LA, LB, LC, LD, true, Tab>(a, o, tid, pq, hout, n3);
+    else
+      hess_quartet<LA, LB, LC, LD, false, Tab>(a, o, tid, pq, hout, n3);
+  }
+  if (o.smem) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < n3 * n3; i += blockDim.x)
+      if (hess_sh[i] != 0.0) atomicAdd(o.hess + i, hess_sh[i]);
+  }
+}

@@ -1,0 +1,24 @@
+// Host-visible launchers of the per-class adjoint Hessian kernels (one translation unit per class,
+// generated by gen_eri.py next to the J/K and gradient units).
+#pragma once
+#include <cuda_runtime.h>
+
+template <typename R>
+struct GradArgs;
+struct HessOut;
+
+namespace hfgpu {
+
+struct HessLaunchers {
+  int la, lb, lc, ld;
+  // hess_kernel over quartets q[0, nq) with grid blocks of 128 threads and smem bytes of
+  // dynamic shared memory (0: atomics straight into the output)
+  void (*launch)(const GradArgs<double>&, const HessOut&, int pure, const int2* q, int nq, int grid, int smem,
+                 cudaStream_t);
+  int (*scratch_slots)(int pure);  // doubles of scratch per thread
+};
+
+extern const HessLaunchers* const kHessLaunchers[];
+extern const int kNumHessClasses;
+
+}  // namespace hfgpu

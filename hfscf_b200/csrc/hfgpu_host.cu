@@ -14,6 +14,8 @@
 #include "../../include/hfgpu.h"
 #include "hfgpu_kernels.cuh"
 #include "hfgpu_launch.h"
+#include "hfgpu_hess_kernels.cuh"
+#include "hfgpu_hess_launch.h"
 #include "hfgpu_onee.h"
 #include "hfgpu_onee_kernels.cuh"
 #include "hfgpu_batch_eigh.cuh"
@@ -1780,6 +1782,118 @@ int hfgpu_grad2e_uhf_backward(hfgpu_handle* h, const double* Da, const double* D
   for (size_t i = 0; i < nn; ++i) Dt[i] = Da[i] + Db[i];
   const double* dk[2] = {Da, Db};
   return grad_host(h, Dt.data(), 0.5, 2, dk, 0.5, scale, dE_dR, precision);
+}
+
+// ---- Two-electron part of the Hessian at a fixed density (adjoint second derivatives) ----
+// The classes run one after another on the handle's stream and share one scratch buffer:
+// each class gets as many threads (whole 128-thread blocks) as kHessScratchBudget holds, at
+// most one per quartet, and loops over the rest.
+constexpr size_t kHessScratchBudget = (size_t)512 << 20;
+constexpr size_t kHessSmemBytes = 96 * 1024;  // per-block Hessian in shared memory up to 36 atoms
+
+static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
+                            double* hess) {
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  if (h->batched) return fail(h, HFGPU_ERR_UNSUPPORTED, "the Hessian takes a single-molecule handle");
+  if (hfgpu::kNumHessClasses != hfgpu::kNumClasses) return fail(h, HFGPU_ERR_STATE, "Hessian class table");
+  GradArgs<double> gd{};
+  gd.pairs = h->d_pairs.as<PairInfo>();
+  gd.prims = h->d_prim_d.as<PrimPair<double>>();
+  const size_t np = std::max<size_t>(h->nprimpairs, 1);
+  gd.alpha_a = h->d_alpha_d.as<double>();
+  gd.alpha_b = h->d_alpha_d.as<double>() + np;
+  gd.boys.tab = h->d_boys_d.as<double>();
+  gd.n = h->n;
+  gd.DJ = DJ; gd.cJ = cJ; gd.nK = nK; gd.DK = DK; gd.cK = cK; gd.grad = nullptr;
+  gd.part = h->part;
+  gd.nparts = h->nparts;
+  const size_t n3 = 3 * (size_t)h->natoms;
+  const size_t smem = sizeof(double) * n3 * n3;
+  HessOut o{hess, h->natoms, smem <= kHessSmemBytes ? 1 : 0};
+  const int2* q = h->d_quart.as<int2>();
+  auto threads_of = [&](int slots, long long nq) -> long long {
+    long long thr = (long long)(kHessScratchBudget / ((size_t)slots * sizeof(double)));
+    thr = std::min<long long>(thr, ((nq + 127) / 128) * 128);
+    return std::max<long long>(128, thr / 128 * 128);
+  };
+  size_t need = 0;
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    const hfgpu::HessLaunchers* L = hfgpu::kHessLaunchers[c];
+    const hfgpu::ClassLaunchers* C = hfgpu::kClassLaunchers[c];
+    if (L->la != C->la || L->lb != C->lb || L->lc != C->lc || L->ld != C->ld)
+      return fail(h, HFGPU_ERR_STATE, "Hessian class order");
+    const long long nq = part_share(h, h->q_end[c] - h->q_beg[c]);
+    if (nq <= 0) continue;
+    const int slots = L->scratch_slots(h->pure);
+    need = std::max(need, (size_t)slots * sizeof(double) * (size_t)threads_of(slots, nq));
+  }
+  if (need) HF_CUDA(h, h->d_scratch.ensure(need));
+  for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
+    const hfgpu::HessLaunchers* L = hfgpu::kHessLaunchers[c];
+    const long long nq = part_share(h, h->q_end[c] - h->q_beg[c]);
+    if (nq <= 0) continue;
+    const int slots = L->scratch_slots(h->pure);
+    const long long thr = threads_of(slots, nq);
+    if ((size_t)slots * sizeof(double) * (size_t)thr > h->d_scratch.bytes)
+      return fail(h, HFGPU_ERR_NOMEM, "Hessian scratch too small");
+    gd.scratch = h->d_scratch.as<double>();
+    gd.scratch_threads = (int)thr;
+    L->launch(gd, o, h->pure, q + h->q_beg[c], (int)nq, (int)(thr / 128), o.smem ? (int)smem : 0, h->stream);
+    HF_CHECK_LAUNCH(h, "hess kernel");
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_hess2e_device(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
+                        double* hess) {
+  if (!h || !hess || nK < 0 || (nK > 0 && !DK)) return HFGPU_ERR_INVALID;
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
+  if (rc) return rc;
+  return hess_device_impl(h, DJ, cJ, nK, DK, cK, hess);
+}
+
+static int hess_host(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* const* DKs, double cK,
+                     double scale, double* hess) {
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
+  if (rc) return rc;
+  const size_t nn = (size_t)h->n * h->n;
+  const size_t n3 = 3 * (size_t)h->natoms;
+  HF_CUDA(h, h->d_mats.ensure(sizeof(double) * (nn * (1 + nK) + n3 * n3)));
+  double* dDJ = h->d_mats.as<double>();
+  double* dDK = dDJ + nn;
+  double* dH = dDK + nK * nn;
+  HF_CUDA(h, cudaMemcpyAsync(dDJ, DJ, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream));
+  for (int m = 0; m < nK; ++m)
+    HF_CUDA(h, cudaMemcpyAsync(dDK + m * nn, DKs[m], sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream));
+  HF_CUDA(h, cudaMemsetAsync(dH, 0, sizeof(double) * n3 * n3, h->stream));
+  if ((rc = hess_device_impl(h, dDJ, cJ, nK, dDK, cK, dH))) return rc;
+  std::vector<double> H(n3 * n3);
+  HF_CUDA(h, cudaMemcpyAsync(H.data(), dH, sizeof(double) * H.size(), cudaMemcpyDeviceToHost, h->stream));
+  HF_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (size_t i = 0; i < H.size(); ++i) {
+    if (!std::isfinite(H[i])) return fail(h, HFGPU_ERR_NONFINITE, "non-finite Hessian");
+    hess[i] += scale * H[i];
+  }
+  return HFGPU_OK;
+}
+
+int hfgpu_hess2e(hfgpu_handle* h, const double* D, double scale, double* hess) {
+  if (!h || !D || !hess) return HFGPU_ERR_INVALID;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  const double* dk[1] = {D};
+  return hess_host(h, D, 2.0, 1, dk, 1.0, scale, hess);
+}
+
+int hfgpu_hess2e_uhf(hfgpu_handle* h, const double* Da, const double* Db, double scale, double* hess) {
+  if (!h || !Da || !Db || !hess) return HFGPU_ERR_INVALID;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  const size_t nn = (size_t)h->n * h->n;
+  std::vector<double> Dt(nn);
+  for (size_t i = 0; i < nn; ++i) Dt[i] = Da[i] + Db[i];
+  const double* dk[2] = {Da, Db};
+  return hess_host(h, Dt.data(), 0.5, 2, dk, 0.5, scale, hess);
 }
 
 // Host-only basis view for the one-electron code (normalised coefficients).

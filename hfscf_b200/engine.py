@@ -370,6 +370,24 @@ class Engine:
                                                     ctypes.c_int(precision)))
         return g
 
+    def hess2e(self, D, scale=1.0) -> np.ndarray:
+        """Two-electron part of the RHF Hessian at fixed D, (3 natoms, 3 natoms): the reference's
+        m_hessianC + m_hessianEx (Mol::scf_hessian::calc_scf_hessian_tei), by hfgpu_hess2e."""
+        n3 = 3 * self.basis.natoms
+        H = np.zeros((n3, n3))
+        self._check(lib().hfgpu_hess2e(self.h, _p(_c(D)), ctypes.c_double(scale), _p(H)))
+        return H
+
+    def hess2e_uhf(self, Da, Db, scale=1.0) -> np.ndarray:
+        n3 = 3 * self.basis.natoms
+        H = np.zeros((n3, n3))
+        self._check(lib().hfgpu_hess2e_uhf(self.h, _p(_c(Da)), _p(_c(Db)), ctypes.c_double(scale), _p(H)))
+        return H
+
+    def hess2e_device(self, DJ_ptr, cJ, nK, DK_ptr, cK, hess_ptr):
+        self._check(lib().hfgpu_hess2e_device(self.h, ctypes.c_void_p(DJ_ptr), ctypes.c_double(cJ), ctypes.c_int(nK),
+                                              ctypes.c_void_p(DK_ptr), ctypes.c_double(cK), ctypes.c_void_p(hess_ptr)))
+
 
 NUM_CLASSES = 21
 

@@ -128,7 +128,22 @@ int hfgpu_grad2e_backward(hfgpu_handle* h, const double* D, double scale, double
 int hfgpu_grad2e_uhf_backward(hfgpu_handle* h, const double* Da, const double* Db, double scale, double* dE_dR,
                               int precision);
 
+/* Two-electron part of the analytic Hessian at a fixed density, replacing the reference's
+ * second-derivative ERI tensors and their contraction in Mol::scf_hessian::calc_scf_hessian_tei
+ * (src/hessian/hfscf_hessian_ints.cpp:20-303; Erios::compute_contracted_shell_quartet_deriv2_qq/_pq,
+ * src/integrals/hfscf_oserideriv2qq.cpp:28-853, hfscf_oserideriv2pq.cpp:23-891).
+ * hess (3 natoms x 3 natoms, row-major) += scale * d2E2/dX dY with E2 as for
+ * hfgpu_grad2e_backward: for RHF the reference's m_hessianC + m_hessianEx.  Second-derivative
+ * integrals are recomputed per quartet and contracted with the density on the fly, never stored.
+ * FP64 only; single-molecule handles (HFGPU_ERR_UNSUPPORTED for a batched handle). */
+int hfgpu_hess2e(hfgpu_handle* h, const double* D, double scale, double* hess);
+int hfgpu_hess2e_uhf(hfgpu_handle* h, const double* Da, const double* Db, double scale, double* hess);
+
 /* Device-pointer variants (enqueue on the handle's stream, no host synchronisation). */
+/* hess (device, 3 natoms x 3 natoms) += sum W d2(ab|cd)/dX dY with the weights of
+ * hfgpu_grad2e_device (RHF: DJ = D, cJ = 2, DK = D, cK = 1). */
+int hfgpu_hess2e_device(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
+                        double* hess);
 int hfgpu_jk_device(hfgpu_handle* h, const double* DJ, int nK, const double* DK, double* J, double* K,
                     int precision);
 int hfgpu_grad2e_device(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,

@@ -184,6 +184,20 @@ def ref_deriv1(basis, coords=(1, 1, 1), cutoff=1e-14) -> np.ndarray:
     return out
 
 
+def ref_hess2e(basis, D, cutoff=1e-14):
+    """Two-electron part of the RHF Hessian at a fixed density D, (3 natoms, 3 natoms), as
+    hessC + hessEx of Mol::scf_hessian::calc_scf_hessian_tei (src/hessian/hfscf_hessian_ints.cpp:20-303),
+    from the reference's second-derivative shell routines (hfscf_oserideriv2qq.cpp, _pq.cpp).
+    Returns (hessC, hessEx)."""
+    args, f = _flat(basis)
+    na3 = 3 * basis.natoms
+    hc, he = np.zeros((na3, na3)), np.zeros((na3, na3))
+    rc = ref().hfref_hess2e(*args, ctypes.c_double(cutoff), _p(f["atom"], ctypes.c_int), ctypes.c_int(basis.natoms),
+                            _p(np.ascontiguousarray(D, dtype=np.float64)), _p(hc), _p(he))
+    assert rc == 0
+    return hc, he
+
+
 def ref_onee(basis):
     """S, T, V from the reference's one-electron shell routines (hfscf_osoverlap.cpp,
     hfscf_osnuclear.cpp) over the driver loop of hfscf_hf_hamiltonian.cpp:14-37."""

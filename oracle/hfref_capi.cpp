@@ -16,6 +16,8 @@
 //       (src/scfsolver/hfscf_hf_hamiltonian.cpp:67-112)
 //   - hfref_deriv1: Mol::scf_gradient::calc_coulomb_exchange_integral_centers
 //       (src/gradient/hfscf_grad_ints.cpp:110-151)
+//   - hfref_hess2e: Mol::scf_hessian::calc_scf_hessian_tei
+//       (src/hessian/hfscf_hessian_ints.cpp:20-303)
 // Shell offsets follow BASIS::Basisset::get_shells (src/basis/hfscf_basis.cpp:244-274)
 // and shell pairs are built for all ordered pairs as in
 // MOLEC::Molecule::create_shell_pairs (src/molecule/hfscf_molecule.cpp:661-669).
@@ -445,6 +447,189 @@ int hfref_time_grad_sample(int nshell, const int* L, const double* xyz, const in
   const double frac = (double)ij.size() / (0.5 * (double)n * (double)(n + 1));
   *t_contract_s = (omp_get_wtime() - t2) / frac;
   *checksum = c;
+  return 0;
+}
+
+// Two-electron part of the RHF Hessian at a fixed density D (n x n, row-major, without the
+// factor 2 of the closed-shell density): hessC = sum D_ij D_kl 2 d2(ij|kl)/dX dY and
+// hessEx = -sum D_ij D_kl d2(ik|jl)/dX dY, both 3 natoms x 3 natoms, row-major, from the
+// reference's second-derivative shell routines Erios::compute_contracted_shell_quartet_deriv2_qq
+// and _pq.  The loops, the translational-invariance relations and the per-atom masks restate
+// Mol::scf_hessian::calc_scf_hessian_tei (src/hessian/hfscf_hessian_ints.cpp:20-303); the
+// reference skips the off-diagonal direction pairs of a planar or linear molecule (zero by
+// symmetry in its aligned frame, :145-166), here every direction pair is computed.
+// shell_atom maps shells to atoms.
+int hfref_hess2e(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
+                 const double* coef, int pure, double cutoff, const int* shell_atom, int natoms, const double* Dm,
+                 double* hessC, double* hessEx) {
+  using tensor4dmath::symm4dTensor;
+  using tensor4dmath::tensor4d;
+  auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, pure);
+  const Eigen::Index n = pure ? b->npure : b->ncart;
+  const int na3 = 3 * natoms;
+  // mask[atom][function]: the function sits on the atom
+  std::vector<std::vector<bool>> mask((size_t)natoms, std::vector<bool>((size_t)n, false));
+  {
+    Eigen::Index f = 0;
+    for (int s = 0; s < nshell; ++s) {
+      const int nf = pure ? 2 * L[s] + 1 : (L[s] + 1) * (L[s] + 2) / 2;
+      for (int k = 0; k < nf; ++k) mask[(size_t)shell_atom[s]][(size_t)(f + k)] = true;
+      f += nf;
+    }
+  }
+  auto D = [&](Eigen::Index k, Eigen::Index l) { return Dm[k * n + l]; };
+  for (int q = 0; q < na3 * na3; ++q) hessC[q] = hessEx[q] = 0.0;
+  ERIOS::Erios os(pure != 0, cutoff);
+  // XX, YY, ZZ
+  for (int cart2 = 0; cart2 < 3; ++cart2) {
+    symm4dTensor<double> AA(n), AB(n), AC(n), BD(n), CC(n), CD(n);
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < nshell; ++i)
+      for (int j = 0; j <= i; ++j)
+        for (int k = 0; k < nshell; ++k)
+          for (int l = 0; l <= k; ++l)
+            os.compute_contracted_shell_quartet_deriv2_qq(AA, AB, AC, BD, CC, CD, b->pairs[i * nshell + j],
+                                                          b->pairs[k * nshell + l], cart2);
+    for (int atom = 0; atom < natoms; ++atom) {
+      const std::vector<bool>& m1 = mask[(size_t)atom];
+      for (int atom2 = 0; atom2 <= atom; ++atom2) {
+        const std::vector<bool>& m2 = mask[(size_t)atom2];
+        symm4dTensor<double> t(n);
+#pragma omp parallel for schedule(dynamic)
+        for (Eigen::Index i = 0; i < n; ++i)
+          for (Eigen::Index j = 0; j <= i; ++j) {
+            const Eigen::Index ij = hfscfmath::index_ij(i, j);
+            for (Eigen::Index k = 0; k < n; ++k)
+              for (Eigen::Index l = 0; l <= k; ++l) {
+                if (ij > hfscfmath::index_ij(k, l)) continue;
+                const double ad = -(AA(i, j, k, l) + AB(i, j, k, l) + AC(i, j, k, l));
+                const double dd = -(ad + BD(i, j, k, l) + CD(i, j, k, l));
+                const double bb = AA(i, j, k, l) + 2 * AC(i, j, k, l) + 2 * ad + CC(i, j, k, l) +
+                                  2 * CD(i, j, k, l) + dd;
+                const double bc = -(AC(i, j, k, l) + CC(i, j, k, l) + CD(i, j, k, l));
+                double v = 0.0;
+                if (atom == atom2) {
+                  if (m1[i]) v += AA(i, j, k, l);
+                  if (m1[j]) v += bb;
+                  if (m1[k]) v += CC(i, j, k, l);
+                  if (m1[l]) v += dd;
+                  if (m1[i] && m1[j]) v += 2 * AB(i, j, k, l);
+                  if (m1[i] && m1[k]) v += 2 * AC(i, j, k, l);
+                  if (m1[i] && m1[l]) v += 2 * ad;
+                  if (m1[j] && m1[k]) v += 2 * bc;
+                  if (m1[j] && m1[l]) v += 2 * BD(i, j, k, l);
+                  if (m1[k] && m1[l]) v += 2 * CD(i, j, k, l);
+                } else {
+                  if ((m1[i] && m2[j]) || (m1[j] && m2[i])) v += AB(i, j, k, l);
+                  if ((m1[i] && m2[k]) || (m1[k] && m2[i])) v += AC(i, j, k, l);
+                  if ((m1[i] && m2[l]) || (m1[l] && m2[i])) v += ad;
+                  if ((m1[j] && m2[k]) || (m1[k] && m2[j])) v += bc;
+                  if ((m1[j] && m2[l]) || (m1[l] && m2[j])) v += BD(i, j, k, l);
+                  if ((m1[k] && m2[l]) || (m1[l] && m2[k])) v += CD(i, j, k, l);
+                }
+                t(i, j, k, l) = v;
+              }
+          }
+        double hc = 0.0, he = 0.0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : hc, he)
+        for (Eigen::Index i = 0; i < n; ++i)
+          for (Eigen::Index j = i; j < n; ++j) {
+            double gc = 0.0, ge = 0.0;
+            for (Eigen::Index k = 0; k < n; ++k)
+              for (Eigen::Index l = 0; l < n; ++l) {
+                gc += D(k, l) * (2.0 * t(i, j, k, l));
+                ge -= D(k, l) * t(i, k, j, l);
+              }
+            const double w = i == j ? 1.0 : 2.0;  // dG(j, i) = dG(i, j)
+            hc += w * D(i, j) * gc;
+            he += w * D(i, j) * ge;
+          }
+        const int r = 3 * atom + cart2, c = 3 * atom2 + cart2;
+        hessC[r * na3 + c] = hessC[c * na3 + r] = hc;
+        hessEx[r * na3 + c] = hessEx[c * na3 + r] = he;
+      }
+    }
+  }
+  // XY, XZ, YZ
+  for (int cart2 = 3; cart2 <= 5; ++cart2) {
+    tensor4d<double> AA(n), AB(n), AC(n);
+    AA.setZero();
+    AB.setZero();
+    AC.setZero();
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < nshell; ++i)
+      for (int j = 0; j < nshell; ++j)
+        for (int k = 0; k < nshell; ++k)
+          for (int l = 0; l < nshell; ++l)
+            os.compute_contracted_shell_quartet_deriv2_pq(AA, AB, AC, b->pairs[i * nshell + j],
+                                                          b->pairs[k * nshell + l], cart2,
+                                                          l <= k ? ERIOS::Permute::ALL : ERIOS::Permute::ACONLY);
+    for (int atom = 0; atom < natoms; ++atom) {
+      const std::vector<bool>& m1 = mask[(size_t)atom];
+      for (int atom2 = 0; atom2 < natoms; ++atom2) {
+        const std::vector<bool>& m2 = mask[(size_t)atom2];
+        tensor4d<double> t(n);
+#pragma omp parallel for schedule(dynamic)
+        for (Eigen::Index i = 0; i < n; ++i)
+          for (Eigen::Index j = 0; j < n; ++j)
+            for (Eigen::Index k = 0; k < n; ++k)
+              for (Eigen::Index l = 0; l < n; ++l) {
+                const double ad = -(AA(i, j, k, l) + AB(i, j, k, l) + AC(i, j, k, l));
+                const double ad1 = -(AA(i, j, k, l) + AB(j, i, k, l) + AC(k, l, i, j));
+                const double dd = -(ad + AC(j, i, l, k) + AB(k, l, i, j));
+                const double bb = AA(i, j, k, l) + AC(i, j, k, l) + ad + AC(k, l, i, j) + AA(k, l, i, j) +
+                                  AB(k, l, i, j) + ad1 + AB(l, k, i, j) + dd;
+                const double bc = -(AC(i, j, k, l) + AA(k, l, i, j) + AB(l, k, i, j));
+                const double bc1 = -(AC(k, l, i, j) + AA(k, l, i, j) + AB(k, l, i, j));
+                const double bd1 = -(ad1 + AB(l, k, i, j) + dd);
+                double v = 0.0;
+                if (atom == atom2) {
+                  if (m1[i]) v += AA(i, j, k, l);
+                  if (m1[j]) v += bb;
+                  if (m1[k]) v += AA(k, l, i, j);
+                  if (m1[l]) v += dd;
+                  if (m1[i] && m1[j]) v += 2 * AB(i, j, k, l);
+                  if (m1[i] && m1[k]) v += 2 * AC(i, j, k, l);
+                  if (m1[i] && m1[l]) v += 2 * ad;
+                  if (m1[j] && m1[k]) v += 2 * bc;
+                  if (m1[j] && m1[l]) v += 2 * AC(j, i, l, k);
+                  if (m1[k] && m1[l]) v += 2 * AB(k, l, i, j);
+                } else {
+                  if (m1[i] && m2[j]) v += AB(i, j, k, l);
+                  if (m1[j] && m2[i]) v += AB(j, i, k, l);
+                  if (m1[i] && m2[k]) v += AC(i, j, k, l);
+                  if (m1[k] && m2[i]) v += AC(k, l, i, j);
+                  if (m1[i] && m2[l]) v += ad;
+                  if (m1[l] && m2[i]) v += ad1;
+                  if (m1[j] && m2[k]) v += bc;
+                  if (m1[k] && m2[j]) v += bc1;
+                  if (m1[j] && m2[l]) v += AC(j, i, l, k);
+                  if (m1[l] && m2[j]) v += bd1;
+                  if (m1[k] && m2[l]) v += AB(k, l, i, j);
+                  if (m1[l] && m2[k]) v += AB(l, k, i, j);
+                }
+                t(i, j, k, l) = v;
+              }
+        double hc = 0.0, he = 0.0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : hc, he)
+        for (Eigen::Index i = 0; i < n; ++i)
+          for (Eigen::Index j = 0; j < n; ++j) {
+            double gc = 0.0, ge = 0.0;
+            for (Eigen::Index k = 0; k < n; ++k)
+              for (Eigen::Index l = 0; l < n; ++l) {
+                gc += D(k, l) * (2.0 * t(i, j, k, l));
+                ge -= D(k, l) * t(i, k, j, l);
+              }
+            hc += D(i, j) * gc;
+            he += D(i, j) * ge;
+          }
+        const int d1 = cart2 == 5 ? 1 : 0, d2 = cart2 == 3 ? 1 : 2;
+        const int r = 3 * atom + d1, c = 3 * atom2 + d2;
+        hessC[r * na3 + c] = hessC[c * na3 + r] = hc;
+        hessEx[r * na3 + c] = hessEx[c * na3 + r] = he;
+      }
+    }
+  }
   return 0;
 }
 
