@@ -354,6 +354,60 @@ def other_configs(local, stream, flush, oracle_refs, autotune):
     return out
 
 
+HESS_WORKLOADS = (("(H2O)4 RHF/6-31G* (Cartesian d, 76 functions)", "w4"),
+                  (CONFIG_NAMES[4], 4), (CONFIG_NAMES[2], 2))
+
+
+def hessian_basis(key):
+    """Basis of a Hessian workload: the (H2O)8 and octane configurations, and a water tetramer
+    built like the octamer (first four lattice sites, the octamer's seed)."""
+    from hfscf_b200 import basis as B, molecules as M
+    if key == "w4":
+        rng = np.random.default_rng(M.SEED_BASE + 4)
+        Z, x = M.water_cluster(4, 2.9, rng, 0.1)
+        return B.build_basis("6-31g*", Z, np.asarray(x) * M.A2B, pure=False)
+    Z, x, name, pure = M.workload(key)
+    return B.build_basis(name, Z, x, pure=pure)
+
+
+def hessian_section(local, stream, flush):
+    """Two-electron part of the RHF Hessian at the converged density (hfgpu_hess2e_device, the
+    adjoint second-derivative kernels): device time per Hessian (CUDA events on the engine's
+    stream, L2 flushed before each, median of 3 after one warm-up)."""
+    import torch
+    from hfscf_b200 import engine as E
+    from hfscf_b200 import scf
+    out = {}
+    dev = torch.device("cuda", local)
+    for name, key in HESS_WORKLOADS:
+        bs = hessian_basis(key)
+        eng = E.Engine(bs, device=local)
+        eng.set_stream(stream.cuda_stream)
+        res = scf.rhf(bs, engine=eng, guess="core")
+        D = torch.from_numpy(np.ascontiguousarray(res.D)).to(dev)
+        n3 = 3 * bs.natoms
+        H = torch.zeros((n3, n3), dtype=torch.float64, device=dev)
+        times = []
+        for k in range(4):
+            H.zero_()
+            flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            eng.hess2e_device(D.data_ptr(), 2.0, 1, D.data_ptr(), 1.0, H.data_ptr())
+            b.record(stream)
+            b.synchronize()
+            if k:
+                times.append(a.elapsed_time(b))
+        Hh = H.cpu().numpy()
+        ms = float(np.median(times))
+        out[str(key)] = {"workload": name, "nbf": bs.nbf, "natoms": bs.natoms, "hess2e_ms": ms,
+                         "hessians_per_s": 1e3 / ms, "max_abs_asymmetry": float(np.max(np.abs(Hh - Hh.T))),
+                         "max_abs_translational_residual": float(np.max(np.abs(Hh.reshape(n3, -1, 3).sum(axis=1))))}
+        eng.close()
+        torch.cuda.set_stream(stream)
+    return out
+
+
 def sharded_build(eng, D, Hd, J, K, F, flush, stream, args, pg, rank, world):
     """One molecule's Fock build partitioned over the ranks (hfgpu_set_partition(rank, world):
     every world-th quartet of each class list) and the partial G = 2J - K summed with one NCCL
@@ -630,6 +684,7 @@ def run_ours(args, world, rank, local):
             line["scf"]["mixed_max_abs_dgrad_vs_oracle"] = float(np.max(np.abs(grad_mx - g0)))
     if not args.no_configs and world == 1:
         line["configs"] = other_configs(local, stream, flush, refs, not args.no_autotune)
+        line["hessian"] = hessian_section(local, stream, flush)
     if not args.no_batch:
         # batched-mode workload: 512 seeded small molecules, SCF + gradient each, in one batched handle
         from hfscf_b200 import batch as BT
@@ -683,6 +738,20 @@ def run_ours(args, world, rank, local):
                 cb["t_grad_s"] = gref["t_grad_s"]
                 cb["t_scf_plus_grad_s"] = cb["t_scf_s"] + gref["t_grad_s"]
                 cb["scf_plus_grad_ratio_reference_over_fp64"] = cb["t_scf_plus_grad_s"] / (scf_wall + grad_wall)
+            # the reference's Hessian two-electron part on the water tetramer (sampled; the larger
+            # workloads need tens of GB of derivative tensors and hours of its per-atom-pair loops)
+            try:
+                import oracle
+                if oracle.ref_available() and "hessian" in line:
+                    rh = oracle.ref_time_hess_sample(hessian_basis("w4"), stride=20)
+                    rh["sample"] = ("second-derivative shell routines over every 20th quartet of one xx and one xy "
+                                    "loop, scaled; assembly + contraction of one atom pair of each kind, scaled to "
+                                    "all pairs and direction pairs (hfscf_hessian_ints.cpp:20-303)")
+                    rh["workload"] = HESS_WORKLOADS[0][0]
+                    rh["ratio_reference_over_ours"] = rh["t_hess2e_s"] / (line["hessian"]["w4"]["hess2e_ms"] / 1e3)
+                    cb["hessian"] = rh
+            except Exception as exc:  # the Fock-build baseline stands without it
+                cb["hessian"] = {"error": repr(exc)}
             line["cpu_baseline"] = cb
     if rank == 0:
         print(json.dumps(line))

@@ -1927,5 +1927,139 @@ def gen_hess_table(la, lb, lc, ld):
     return "\n".join(s), meta
 
 
+
+def gen_hess_block(la, lb, lc, ld):
+    """Levelised op tables of the adjoint Hessian of one class for one block of threads per
+    quartet (hess_block_kernel): the VRR two orders higher and the HRR of the ten weight sets
+    are levelised (an op reads only values of earlier levels), so a level's ops run
+    thread-parallel; each HRR level ends with its contraction rows, sorted by output entry,
+    which the threads take in contiguous chunks (one register sum per run of equal entries)."""
+    L = la + lb + lc + ld + 2
+    terms = hess_terms(la, lb, lc, ld)
+    hnodes, hinfo, hdeps, acc_key = {}, {}, {}, {}
+    nxt = [0]
+
+    def new_id():
+        nxt[0] += 1
+        return ("h", nxt[0] - 1)
+
+    def ket(k, e, c, d):
+        key = ("k", k, e, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(d) == 0:
+            v = ("acc", k, e, c)
+            acc_key.setdefault(v, len(acc_key))
+        else:
+            i = max(range(3), key=lambda q: (d[q], -q))
+            d1 = add(d, i, -1)
+            x, y = ket(k, e, add(c, i), d1), ket(k, e, c, d1)
+            v = new_id()
+            hinfo[v], hdeps[v] = (1, i, x, y), [x, y]
+        hnodes[key] = v
+        return v
+
+    def bra(k, a, b, c, d):
+        key = ("b", k, a, b, c, d)
+        if key in hnodes:
+            return hnodes[key]
+        if sum(b) == 0:
+            v = ket(k, a, c, d)
+        else:
+            i = max(range(3), key=lambda q: (b[q], -q))
+            b1 = add(b, i, -1)
+            x, y = bra(k, add(a, i), b1, c, d), bra(k, a, b1, c, d)
+            v = new_id()
+            hinfo[v], hdeps[v] = (0, i, x, y), [x, y]
+        hnodes[key] = v
+        return v
+
+    cops = [(hi, wi, bra(si, a, b, c, d), k) for hi, wi, k, si, a, b, c, d in terms]
+    nacc = len(acc_key)
+    # number every HRR value: accumulators 0 .. nacc-1 (the inputs), the rest after
+    num = {v: j for v, j in acc_key.items()}
+    for v in hinfo:
+        num[v] = len(num)
+    hord = [num[v] for v in hinfo]  # creation order is topological
+    hdeps_n = {num[v]: [num[x] for x in hdeps[v]] for v in hinfo}
+    hlev = _levelise([(v, hdeps_n[v]) for v in hord], nacc)
+    clev = [1 + hlev[num[x]] for (_, _, x, _) in cops]
+    readers = [(l, [num[x]]) for l, (_, _, x, _) in zip(clev, cops)]
+    hpre = {j: j for j in range(nacc)}
+    hslot, nhs = _alloc_levels_with_readers(sorted(hord, key=lambda v: (hlev[v], v)), hdeps_n, hlev, hpre, set(),
+                                            readers)
+    ZH = nhs
+    inv = {num[v]: v for v in hinfo}
+    maxl = max([hlev[v] for v in hord] + clev + [0])
+    hrows, hlv = [], []
+    by_l = {}
+    for v in hord:
+        by_l.setdefault(hlev[v], [[], []])[0].append(v)
+    for j, l in enumerate(clev):
+        by_l.setdefault(l, [[], []])[1].append(j)
+    for l in range(1, maxl + 1):
+        ops_l, con_l = by_l.get(l, [[], []])
+        start = len(hrows)
+        for v in ops_l:
+            kind, i, x, y = hinfo[inv[v]]
+            hrows.append((kind, i, hslot[v], hslot[num[x]], hslot[num[y]]))
+        mid = len(hrows)
+        for j in sorted(con_l, key=lambda j: (cops[j][0], cops[j][1])):
+            hi, wi, x, k = cops[j]
+            hrows.append((2, hi, wi, hslot[num[x]], k))
+        hlv.append((start, mid))
+    hlv.append((len(hrows), len(hrows)))
+    # VRR, levelised; accumulator j <- weight(set) * value at slot
+    dag = Dag(L)
+    acc_src, acc_set = [0] * nacc, [0] * nacc
+    for (_, k, e, f), j in acc_key.items():
+        acc_src[j] = dag.get(e, f, 0)
+        acc_set[j] = k
+    ops = [(nid, nd) for nid, nd in enumerate(dag.nodes) if nd[0] != "F"]
+    deps = {nid: [x for x in nd[2:7] if x >= 0] for nid, nd in ops}
+    lev = _levelise([(nid, deps[nid]) for nid, _ in ops], L + 1)
+    vorder = sorted([nid for nid, _ in ops], key=lambda n: (lev[n], n))
+    pre = {m: m for m in range(L + 1)}
+    slot, nvs = _alloc_levels(vorder, deps, lev, pre, set(acc_src))
+    ZV = nvs
+    nodes = dict(ops)
+    vrows, vlev, cur = [], [0], 1
+    for nid in vorder:
+        while lev[nid] > cur:
+            vlev.append(len(vrows))
+            cur += 1
+        kind, i, a, b, c, d, g, k1, k2 = nodes[nid]
+        s_ = lambda x: slot[x] if x >= 0 else ZV
+        vrows.append(((1 if kind == "K" else 0) | (i << 2), slot[nid], s_(a), s_(b), s_(c), s_(d), s_(g),
+                      k1 | (k2 << 8)))
+    vlev.append(len(vrows))
+    t = f"{la}{lb}{lc}{ld}"
+    ncart_blk = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
+    s = [f"// block-mode adjoint Hessian of class {t}: {len(vrows)} VRR ops in {len(vlev) - 1} levels over "
+         f"{nvs} slots, {nacc} accumulators, {len(hrows)} HRR/contraction ops in {len(hlv) - 1} levels over "
+         f"{nhs} slots"]
+    s.append(f"__device__ const int4 hbv_{t}[{max(len(vrows), 1)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_warp_vrr(r))) + "}," for r in vrows]
+    s.append("};")
+    s.append(f"__device__ const int hbv_lv_{t}[{len(vlev)}] = {{{','.join(map(str, vlev))}}};")
+    s.append(f"__device__ const int2 hba_{t}[{nacc}] = {{" +
+             ",".join("{%d,%d}" % (slot[n], k) for n, k in zip(acc_src, acc_set)) + "};")
+    s.append(f"__device__ const int2 hbh_{t}[{max(len(hrows), 1)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_hess_hrr(r))) + "}," for r in hrows]
+    s.append("};")
+    s.append(f"__device__ const int2 hbh_lv_{t}[{len(hlv)}] = {{" + ",".join("{%d,%d}" % p for p in hlv) + "};")
+    s.append(f"struct HessBlockTab{t} {{ static constexpr int L = {L}, NVLEV = {len(vlev) - 1}, NVSLOT = {nvs}, "
+             f"NACC = {nacc}, NHLEV = {len(hlv) - 1}, NHSLOT = {nhs}, NCART = {ncart_blk}; "
+             f"static __device__ const int4* vrr() {{ return hbv_{t}; }} "
+             f"static __device__ const int* vlev() {{ return hbv_lv_{t}; }} "
+             f"static __device__ const int2* acc() {{ return hba_{t}; }} "
+             f"static __device__ const int2* hrr() {{ return hbh_{t}; }} "
+             f"static __device__ const int2* hlev() {{ return hbh_lv_{t}; }} }};")
+    meta = {"class": [la, lb, lc, ld], "vrr_ops": len(vrows), "vrr_levels": len(vlev) - 1, "vrr_slots": nvs,
+            "acc": nacc, "hrr_ops": len(hrows), "hrr_levels": len(hlv) - 1, "hrr_slots": nhs,
+            "slots": nvs + 1 + nhs + 1 + 45 + 3 * ncart_blk}
+    return "\n".join(s), meta
+
+
 if __name__ == "__main__":
     main(sys.argv[1])

@@ -1785,10 +1785,11 @@ int hfgpu_grad2e_uhf_backward(hfgpu_handle* h, const double* Da, const double* D
 }
 
 // ---- Two-electron part of the Hessian at a fixed density (adjoint second derivatives) ----
-// The classes run one after another on the handle's stream and share one scratch buffer:
-// each class gets as many threads (whole 128-thread blocks) as kHessScratchBudget holds, at
-// most one per quartet, and loops over the rest.
-constexpr size_t kHessScratchBudget = (size_t)512 << 20;
+// Each class gets its own slice of one scratch buffer and runs on an auxiliary stream (fork/join
+// with the handle's stream, as the J/K classes do), so the few-quartet, long-table d classes
+// overlap the many-quartet s/p classes.  A class gets as many threads (whole 128-thread blocks)
+// as kHessScratchBudget holds, at most one per quartet, and loops over the rest.
+constexpr size_t kHessScratchBudget = (size_t)256 << 20;
 constexpr size_t kHessSmemBytes = 96 * 1024;  // per-block Hessian in shared memory up to 36 atoms
 
 static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
@@ -1816,32 +1817,37 @@ static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     thr = std::min<long long>(thr, ((nq + 127) / 128) * 128);
     return std::max<long long>(128, thr / 128 * 128);
   };
-  size_t need = 0;
+  size_t off[32] = {0}, need = 0;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) {
     const hfgpu::HessLaunchers* L = hfgpu::kHessLaunchers[c];
     const hfgpu::ClassLaunchers* C = hfgpu::kClassLaunchers[c];
     if (L->la != C->la || L->lb != C->lb || L->lc != C->lc || L->ld != C->ld)
       return fail(h, HFGPU_ERR_STATE, "Hessian class order");
+    off[c] = need;
     const long long nq = part_share(h, h->q_end[c] - h->q_beg[c]);
     if (nq <= 0) continue;
     const int slots = L->scratch_slots(h->pure);
-    need = std::max(need, (size_t)slots * sizeof(double) * (size_t)threads_of(slots, nq));
+    need += ((size_t)slots * sizeof(double) * (size_t)threads_of(slots, nq) + 255) / 256 * 256;
   }
   if (need) HF_CUDA(h, h->d_scratch.ensure(need));
+  int rc = fork_streams(h);
+  if (rc) return rc;
+  int rr = 0;
   for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
     const hfgpu::HessLaunchers* L = hfgpu::kHessLaunchers[c];
     const long long nq = part_share(h, h->q_end[c] - h->q_beg[c]);
     if (nq <= 0) continue;
     const int slots = L->scratch_slots(h->pure);
     const long long thr = threads_of(slots, nq);
-    if ((size_t)slots * sizeof(double) * (size_t)thr > h->d_scratch.bytes)
+    if (off[c] + (size_t)slots * sizeof(double) * (size_t)thr > h->d_scratch.bytes)
       return fail(h, HFGPU_ERR_NOMEM, "Hessian scratch too small");
-    gd.scratch = h->d_scratch.as<double>();
+    gd.scratch = reinterpret_cast<double*>(h->d_scratch.as<unsigned char>() + off[c]);
     gd.scratch_threads = (int)thr;
-    L->launch(gd, o, h->pure, q + h->q_beg[c], (int)nq, (int)(thr / 128), o.smem ? (int)smem : 0, h->stream);
+    L->launch(gd, o, h->pure, q + h->q_beg[c], (int)nq, (int)(thr / 128), o.smem ? (int)smem : 0,
+              h->aux[rr++ % hfgpu_handle::kAux]);
     HF_CHECK_LAUNCH(h, "hess kernel");
   }
-  return HFGPU_OK;
+  return join_streams(h);
 }
 
 int hfgpu_hess2e_device(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,

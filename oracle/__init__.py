@@ -198,6 +198,22 @@ def ref_hess2e(basis, D, cutoff=1e-14):
     return hc, he
 
 
+def ref_time_hess_sample(basis, stride=20, cutoff=1e-14):
+    """Seconds of the reference's Hessian two-electron part (hfref_time_hess_sample): per direction
+    pair the sampled second-derivative shell routines (qq, pq) scaled to their whole loops, and
+    the assembly + contraction of one atom pair of each kind; total = 3 (qq + pq) +
+    3 natoms (natoms + 1) / 2 pair_qq + 3 natoms^2 pair_pq."""
+    args, f = _flat(basis)
+    t = [ctypes.c_double() for _ in range(4)]
+    rc = ref().hfref_time_hess_sample(*args, ctypes.c_double(cutoff), _p(f["atom"], ctypes.c_int),
+                                      ctypes.c_int(basis.natoms), ctypes.c_int(stride), *[ctypes.byref(x) for x in t])
+    assert rc == 0
+    qq, pq, pqq, ppq = (x.value for x in t)
+    na = basis.natoms
+    return {"t_qq_ints_s": qq, "t_pq_ints_s": pq, "t_pair_qq_s": pqq, "t_pair_pq_s": ppq,
+            "t_hess2e_s": 3 * (qq + pq) + 3 * na * (na + 1) / 2 * pqq + 3 * na * na * ppq}
+
+
 def ref_onee(basis):
     """S, T, V from the reference's one-electron shell routines (hfscf_osoverlap.cpp,
     hfscf_osnuclear.cpp) over the driver loop of hfscf_hf_hamiltonian.cpp:14-37."""

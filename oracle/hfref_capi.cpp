@@ -21,6 +21,7 @@
 // Shell offsets follow BASIS::Basisset::get_shells (src/basis/hfscf_basis.cpp:244-274)
 // and shell pairs are built for all ordered pairs as in
 // MOLEC::Molecule::create_shell_pairs (src/molecule/hfscf_molecule.cpp:661-669).
+#include <array>
 #include <cstdint>
 #include <memory>
 #include <vector>
@@ -629,6 +630,161 @@ int hfref_hess2e(int nshell, const int* L, const double* xyz, const int* nprim, 
         hessEx[r * na3 + c] = hessEx[c * na3 + r] = he;
       }
     }
+  }
+  return 0;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// Timing sample of the reference's Hessian two-electron part (calc_scf_hessian_tei,
+// src/hessian/hfscf_hessian_ints.cpp:20-303) on all OpenMP threads: the second-derivative
+// shell routines of one direction pair of each kind (xx via deriv2_qq, xy via deriv2_pq) over
+// every `stride`-th shell quartet of its loop, scaled to the whole loop (*t_qq_ints, *t_pq_ints,
+// per direction pair), and the per-atom-pair assembly + contraction of one atom pair of each
+// kind (*t_pair_qq, *t_pair_pq).  The whole term costs 3 (t_qq_ints + t_pq_ints) +
+// 3 natoms (natoms + 1) / 2 t_pair_qq + 3 natoms^2 t_pair_pq.
+int hfref_time_hess_sample(int nshell, const int* L, const double* xyz, const int* nprim, const double* alpha,
+                           const double* coef, int pure, double cutoff, const int* shell_atom, int natoms,
+                           int stride, double* t_qq_ints, double* t_pq_ints, double* t_pair_qq,
+                           double* t_pair_pq) {
+  using tensor4dmath::symm4dTensor;
+  using tensor4dmath::tensor4d;
+  auto b = make_basis(nshell, L, xyz, nprim, alpha, coef, pure);
+  const Eigen::Index n = pure ? b->npure : b->ncart;
+  std::vector<std::vector<bool>> mask((size_t)natoms, std::vector<bool>((size_t)n, false));
+  {
+    Eigen::Index f = 0;
+    for (int s = 0; s < nshell; ++s) {
+      const int nf = pure ? 2 * L[s] + 1 : (L[s] + 1) * (L[s] + 2) / 2;
+      for (int k = 0; k < nf; ++k) mask[(size_t)shell_atom[s]][(size_t)(f + k)] = true;
+      f += nf;
+    }
+  }
+  std::vector<double> D((size_t)(n * n), 1e-2);
+  ERIOS::Erios os(pure != 0, cutoff);
+  const int a1 = natoms > 1 ? 1 : 0, a0 = 0;
+  {
+    std::vector<std::array<int, 4>> qs;
+    for (int i = 0; i < nshell; ++i)
+      for (int j = 0; j <= i; ++j)
+        for (int k = 0; k < nshell; ++k)
+          for (int l = 0; l <= k; ++l) qs.push_back({i, j, k, l});
+    std::vector<std::array<int, 4>> pick;
+    for (size_t q = 0; q < qs.size(); q += (size_t)stride) pick.push_back(qs[q]);
+    symm4dTensor<double> AA(n), AB(n), AC(n), BD(n), CC(n), CD(n);
+    double t0 = omp_get_wtime();
+#pragma omp parallel for schedule(dynamic)
+    for (long long q = 0; q < (long long)pick.size(); ++q) {
+      const auto& s = pick[(size_t)q];
+      os.compute_contracted_shell_quartet_deriv2_qq(AA, AB, AC, BD, CC, CD, b->pairs[s[0] * nshell + s[1]],
+                                                    b->pairs[s[2] * nshell + s[3]], 0);
+    }
+    *t_qq_ints = (omp_get_wtime() - t0) * (double)qs.size() / (double)std::max<size_t>(pick.size(), 1);
+    // one atom pair: the mask assembly into a packed tensor and the Coulomb/exchange contraction
+    const std::vector<bool>& m1 = mask[(size_t)a1];
+    const std::vector<bool>& m2 = mask[(size_t)a0];
+    t0 = omp_get_wtime();
+    symm4dTensor<double> t(n);
+#pragma omp parallel for schedule(dynamic)
+    for (Eigen::Index i = 0; i < n; ++i)
+      for (Eigen::Index j = 0; j <= i; ++j) {
+        const Eigen::Index ij = hfscfmath::index_ij(i, j);
+        for (Eigen::Index k = 0; k < n; ++k)
+          for (Eigen::Index l = 0; l <= k; ++l) {
+            if (ij > hfscfmath::index_ij(k, l)) continue;
+            const double ad = -(AA(i, j, k, l) + AB(i, j, k, l) + AC(i, j, k, l));
+            const double dd = -(ad + BD(i, j, k, l) + CD(i, j, k, l));
+            const double bc = -(AC(i, j, k, l) + CC(i, j, k, l) + CD(i, j, k, l));
+            double v = 0.0;
+            if ((m1[i] && m2[j]) || (m1[j] && m2[i])) v += AB(i, j, k, l);
+            if ((m1[i] && m2[k]) || (m1[k] && m2[i])) v += AC(i, j, k, l);
+            if ((m1[i] && m2[l]) || (m1[l] && m2[i])) v += ad;
+            if ((m1[j] && m2[k]) || (m1[k] && m2[j])) v += bc;
+            if ((m1[j] && m2[l]) || (m1[l] && m2[j])) v += BD(i, j, k, l);
+            if ((m1[k] && m2[l]) || (m1[l] && m2[k])) v += CD(i, j, k, l) + 0.0 * dd;
+            t(i, j, k, l) = v;
+          }
+      }
+    double hc = 0.0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : hc)
+    for (Eigen::Index i = 0; i < n; ++i)
+      for (Eigen::Index j = i; j < n; ++j) {
+        double gc = 0.0, ge = 0.0;
+        for (Eigen::Index k = 0; k < n; ++k)
+          for (Eigen::Index l = 0; l < n; ++l) {
+            gc += D[(size_t)(k * n + l)] * (2.0 * t(i, j, k, l));
+            ge -= D[(size_t)(k * n + l)] * t(i, k, j, l);
+          }
+        hc += D[(size_t)(i * n + j)] * (gc + ge);
+      }
+    *t_pair_qq = omp_get_wtime() - t0 + 0.0 * hc;
+  }
+  {
+    std::vector<std::array<int, 4>> qs;
+    for (int i = 0; i < nshell; ++i)
+      for (int j = 0; j < nshell; ++j)
+        for (int k = 0; k < nshell; ++k)
+          for (int l = 0; l < nshell; ++l) qs.push_back({i, j, k, l});
+    std::vector<std::array<int, 4>> pick;
+    for (size_t q = 0; q < qs.size(); q += (size_t)stride) pick.push_back(qs[q]);
+    tensor4d<double> AA(n), AB(n), AC(n);
+    AA.setZero();
+    AB.setZero();
+    AC.setZero();
+    double t0 = omp_get_wtime();
+#pragma omp parallel for schedule(dynamic)
+    for (long long q = 0; q < (long long)pick.size(); ++q) {
+      const auto& s = pick[(size_t)q];
+      os.compute_contracted_shell_quartet_deriv2_pq(AA, AB, AC, b->pairs[s[0] * nshell + s[1]],
+                                                    b->pairs[s[2] * nshell + s[3]], 3,
+                                                    s[3] <= s[2] ? ERIOS::Permute::ALL : ERIOS::Permute::ACONLY);
+    }
+    *t_pq_ints = (omp_get_wtime() - t0) * (double)qs.size() / (double)std::max<size_t>(pick.size(), 1);
+    const std::vector<bool>& m1 = mask[(size_t)a1];
+    const std::vector<bool>& m2 = mask[(size_t)a0];
+    t0 = omp_get_wtime();
+    tensor4d<double> t(n);
+#pragma omp parallel for schedule(dynamic)
+    for (Eigen::Index i = 0; i < n; ++i)
+      for (Eigen::Index j = 0; j < n; ++j)
+        for (Eigen::Index k = 0; k < n; ++k)
+          for (Eigen::Index l = 0; l < n; ++l) {
+            const double ad = -(AA(i, j, k, l) + AB(i, j, k, l) + AC(i, j, k, l));
+            const double ad1 = -(AA(i, j, k, l) + AB(j, i, k, l) + AC(k, l, i, j));
+            const double dd = -(ad + AC(j, i, l, k) + AB(k, l, i, j));
+            const double bc = -(AC(i, j, k, l) + AA(k, l, i, j) + AB(l, k, i, j));
+            const double bc1 = -(AC(k, l, i, j) + AA(k, l, i, j) + AB(k, l, i, j));
+            const double bd1 = -(ad1 + AB(l, k, i, j) + dd);
+            double v = 0.0;
+            if (m1[i] && m2[j]) v += AB(i, j, k, l);
+            if (m1[j] && m2[i]) v += AB(j, i, k, l);
+            if (m1[i] && m2[k]) v += AC(i, j, k, l);
+            if (m1[k] && m2[i]) v += AC(k, l, i, j);
+            if (m1[i] && m2[l]) v += ad;
+            if (m1[l] && m2[i]) v += ad1;
+            if (m1[j] && m2[k]) v += bc;
+            if (m1[k] && m2[j]) v += bc1;
+            if (m1[j] && m2[l]) v += AC(j, i, l, k);
+            if (m1[l] && m2[j]) v += bd1;
+            if (m1[k] && m2[l]) v += AB(k, l, i, j);
+            if (m1[l] && m2[k]) v += AB(l, k, i, j);
+            t(i, j, k, l) = v;
+          }
+    double hc = 0.0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : hc)
+    for (Eigen::Index i = 0; i < n; ++i)
+      for (Eigen::Index j = 0; j < n; ++j) {
+        double gc = 0.0, ge = 0.0;
+        for (Eigen::Index k = 0; k < n; ++k)
+          for (Eigen::Index l = 0; l < n; ++l) {
+            gc += D[(size_t)(k * n + l)] * (2.0 * t(i, j, k, l));
+            ge -= D[(size_t)(k * n + l)] * t(i, k, j, l);
+          }
+        hc += D[(size_t)(i * n + j)] * (gc + ge);
+      }
+    *t_pair_pq = omp_get_wtime() - t0 + 0.0 * hc;
   }
   return 0;
 }
