@@ -1062,8 +1062,31 @@ static int hess_scratch_slots(int) {{
   return HessTable{t}::NVSLOT + HessTable{t}::NHSLOT + 45 +
          3 * BlockDims<{la}, {lb}, {lc}, {ld}, false>::NCART;
 }}
+// block form: the whole table in shared memory when it fits, else the HRR slots in global scratch
+constexpr size_t kSmAll = sizeof(double) * hess_block_shared_doubles<HessBlockTab{t}>(false);
+constexpr size_t kSmPart = sizeof(double) * hess_block_shared_doubles<HessBlockTab{t}>(true);
+constexpr size_t kSmMax = 227 * 1024;
+static int hess_block_global_slots() {{ return kSmAll <= kSmMax ? 0 : HessBlockTab{t}::NHSLOT + 1; }}
+static bool launch_hess_block(const GradArgs<double>& a, const HessOut& o, int pure, const int2* q, int nq, int grid,
+                              cudaStream_t s) {{
+  if (nq <= 0) return true;
+  if constexpr (kSmAll <= kSmMax) {{
+    auto k = hess_block_kernel<{la}, {lb}, {lc}, {ld}, HessBlockTab{t}, false>;
+    if (kSmAll > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmAll);
+    k<<<grid, 128, kSmAll, s>>>(a, o, pure, q, nq);
+    return true;
+  }} else if constexpr (kSmPart <= kSmMax) {{
+    auto k = hess_block_kernel<{la}, {lb}, {lc}, {ld}, HessBlockTab{t}, true>;
+    if (kSmPart > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmPart);
+    k<<<grid, 128, kSmPart, s>>>(a, o, pure, q, nq);
+    return true;
+  }} else {{
+    return false;
+  }}
+}}
 extern const HessLaunchers hess_launchers_{t};
-const HessLaunchers hess_launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_hess, &hess_scratch_slots}};
+const HessLaunchers hess_launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_hess, &hess_scratch_slots,
+                                          &launch_hess_block, &hess_block_global_slots}};
 }}  // namespace hfgpu
 """
 
@@ -1098,9 +1121,11 @@ def main(outdir):
         t = "".join(map(str, c))
         code_h, mh = gen_hess_table(*c)
         meta["hess"].append(mh)
+        code_b, mb = gen_hess_block(*c)
+        mh["block"] = mb
         write_if_changed(os.path.join(outdir, f"hess_{t}.cuh"),
                          "// GENERATED by gen_eri.py -- do not edit.\n#pragma once\n#include \"common.cuh\"\n\n" +
-                         code_h + "\n")
+                         code_h + "\n\n" + code_b + "\n")
         la, lb, lc, ld = c
         write_if_changed(os.path.join(outdir, f"hess_{t}.cu"), HESS_INST_TEMPLATE.format(t=t, la=la, lb=lb, lc=lc, ld=ld))
         hnames.append(t)
@@ -1928,6 +1953,18 @@ def gen_hess_table(la, lb, lc, ld):
 
 
 
+def pack_hess_block_hrr(r):
+    """Block-form HRR row {dst, x, y, kind | dir<<2} (kind 0 bra, 1 ket) or contraction row
+    {W index, x, 0, 2 | out<<4 | (coef + 128)<<10}: full 32-bit slot numbers (the level-wise
+    slot allocation of the large classes needs more than 2^16)."""
+    if r[0] == 2:
+        _, hi, wi, x, k = r
+        assert -128 <= k < 128 and 0 <= hi < 45
+        return (wi, x, 0, 2 | hi << 4 | (k + 128) << 10)
+    kind, i, dst, x, y = r
+    return (dst, x, y, kind | i << 2)
+
+
 def gen_hess_block(la, lb, lc, ld):
     """Levelised op tables of the adjoint Hessian of one class for one block of threads per
     quartet (hess_block_kernel): the VRR two orders higher and the HRR of the ten weight sets
@@ -1988,7 +2025,6 @@ def gen_hess_block(la, lb, lc, ld):
     hpre = {j: j for j in range(nacc)}
     hslot, nhs = _alloc_levels_with_readers(sorted(hord, key=lambda v: (hlev[v], v)), hdeps_n, hlev, hpre, set(),
                                             readers)
-    ZH = nhs
     inv = {num[v]: v for v in hinfo}
     maxl = max([hlev[v] for v in hord] + clev + [0])
     hrows, hlv = [], []
@@ -2044,8 +2080,8 @@ def gen_hess_block(la, lb, lc, ld):
     s.append(f"__device__ const int hbv_lv_{t}[{len(vlev)}] = {{{','.join(map(str, vlev))}}};")
     s.append(f"__device__ const int2 hba_{t}[{nacc}] = {{" +
              ",".join("{%d,%d}" % (slot[n], k) for n, k in zip(acc_src, acc_set)) + "};")
-    s.append(f"__device__ const int2 hbh_{t}[{max(len(hrows), 1)}] = {{")
-    s += ["  {" + ",".join(map(str, pack_hess_hrr(r))) + "}," for r in hrows]
+    s.append(f"__device__ const int4 hbh_{t}[{max(len(hrows), 1)}] = {{")
+    s += ["  {" + ",".join(map(str, pack_hess_block_hrr(r))) + "}," for r in hrows]
     s.append("};")
     s.append(f"__device__ const int2 hbh_lv_{t}[{len(hlv)}] = {{" + ",".join("{%d,%d}" % p for p in hlv) + "};")
     s.append(f"struct HessBlockTab{t} {{ static constexpr int L = {L}, NVLEV = {len(vlev) - 1}, NVSLOT = {nvs}, "
@@ -2053,7 +2089,7 @@ def gen_hess_block(la, lb, lc, ld):
              f"static __device__ const int4* vrr() {{ return hbv_{t}; }} "
              f"static __device__ const int* vlev() {{ return hbv_lv_{t}; }} "
              f"static __device__ const int2* acc() {{ return hba_{t}; }} "
-             f"static __device__ const int2* hrr() {{ return hbh_{t}; }} "
+             f"static __device__ const int4* hrr() {{ return hbh_{t}; }} "
              f"static __device__ const int2* hlev() {{ return hbh_lv_{t}; }} }};")
     meta = {"class": [la, lb, lc, ld], "vrr_ops": len(vrows), "vrr_levels": len(vlev) - 1, "vrr_slots": nvs,
             "acc": nacc, "hrr_ops": len(hrows), "hrr_levels": len(hlv) - 1, "hrr_slots": nhs,

@@ -216,3 +216,233 @@ __global__ void __launch_bounds__(128) hess_kernel(GradArgs<double> a, HessOut o
       if (hess_sh[i] != 0.0) atomicAdd(o.hess + i, hess_sh[i]);
   }
 }
+
+// ---------------------------------------------------------------------------
+// Block form: one block of NT threads per quartet over levelised tables (gen_eri.py
+// gen_hess_block).  The ops of one level read only values of earlier levels, so the threads run
+// a level's ops in parallel and synchronise between levels.  The VRR slots, the weights and the
+// 45 outputs live in shared memory; the HRR slots (accumulators first) too when the whole table
+// fits (HS_GLOBAL false), else in a per-block region of global scratch (the two largest classes).
+// Each HRR level ends with its contraction rows sorted by output entry; a thread takes a
+// contiguous chunk of them and adds one register sum per run of equal entries.
+// ---------------------------------------------------------------------------
+template <typename Tab>
+__host__ __device__ constexpr int hess_block_shared_doubles(bool hs_global) {
+  return Tab::NVSLOT + 1 + (hs_global ? 0 : Tab::NHSLOT + 1) + 3 * Tab::NCART + 45;
+}
+
+template <int LA, int LB, int LC, int LD, typename Tab, bool HS_GLOBAL, int NT = 128>
+__global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, HessOut o, int pure,
+                                                        const int2* __restrict__ quartets, int nq) {
+  using R = double;
+  extern __shared__ __align__(16) unsigned char hbsm[];
+  const int tid = threadIdx.x;
+  R* vs = reinterpret_cast<R*>(hbsm);
+  R* hs;
+  R* W;
+  if constexpr (HS_GLOBAL) {
+    hs = a.scratch + (size_t)blockIdx.x * (Tab::NHSLOT + 1);
+    W = vs + Tab::NVSLOT + 1;
+  } else {
+    hs = vs + Tab::NVSLOT + 1;
+    W = hs + Tab::NHSLOT + 1;
+  }
+  R* t0 = W + Tab::NCART;
+  R* t1 = t0 + Tab::NCART;
+  R* h45 = t1 + Tab::NCART;
+  const int n3 = 3 * o.natoms;
+  const int np = a.nparts > 1 ? a.nparts : 1, p0 = np > 1 ? a.part : 0;
+  for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
+    const int2 pq = quartets[(size_t)qi * np + p0];
+    const PairInfo P = a.pairs[pq.x];
+    const PairInfo Q = a.pairs[pq.y];
+    double s8 = 8.0;
+    if (P.sa == P.sb) s8 *= 0.5;
+    if (Q.sa == Q.sb) s8 *= 0.5;
+    if (pq.x == pq.y) s8 *= 0.5;
+    // weight block in the final basis (t0 when pure), then back to Cartesian one index at a time
+    const int Ls[4] = {LA, LB, LC, LD};
+    int dims[4];
+    for (int q = 0; q < 4; ++q) dims[q] = pure ? npure_of(Ls[q]) : ncart_of(Ls[q]);
+    {
+      const int tot = dims[0] * dims[1] * dims[2] * dims[3];
+      R* dstw = pure ? t0 : W;
+      for (int e = tid; e < tot; e += NT) {
+        const int l = e % dims[3], k = (e / dims[3]) % dims[2], j = (e / (dims[3] * dims[2])) % dims[1];
+        const int i = e / (dims[3] * dims[2] * dims[1]);
+        const int ia = P.fa + i, jb = P.fb + j, kc = Q.fa + k, ld = Q.fb + l;
+        const int n = a.n;
+        double w = a.DJ ? a.cJ * __ldg(a.DJ + (size_t)ia * n + jb) * __ldg(a.DJ + (size_t)kc * n + ld) : 0.0;
+        for (int m = 0; m < a.nK; ++m) {
+          const double* D = a.DK + (size_t)m * n * n;
+          w -= 0.5 * a.cK *
+               (__ldg(D + (size_t)ia * n + kc) * __ldg(D + (size_t)jb * n + ld) +
+                __ldg(D + (size_t)ia * n + ld) * __ldg(D + (size_t)jb * n + kc));
+        }
+        dstw[e] = s8 * w;
+      }
+      __syncthreads();
+    }
+    if (pure) {
+      R* bufs[2] = {t1, t0};
+      const R* in = t0;
+      for (int st = 0; st < 4; ++st) {
+        const int nc = ncart_of(Ls[st]), npu = npure_of(Ls[st]);
+        int nd[4] = {dims[0], dims[1], dims[2], dims[3]};
+        nd[st] = nc;
+        R* out = st == 3 ? W : bufs[st & 1];
+        const int tot = nd[0] * nd[1] * nd[2] * nd[3];
+        for (int e = tid; e < tot; e += NT) {
+          int id[4];
+          int r = e;
+          for (int q = 3; q >= 0; --q) {
+            id[q] = r % nd[q];
+            r /= nd[q];
+          }
+          R v = R(0);
+          for (int c = 0; c < npu; ++c) {
+            const double y = c_ylm[Ls[st]][id[st] * npu + c];
+            if (y == 0.0) continue;
+            int jd[4] = {id[0], id[1], id[2], id[3]};
+            jd[st] = c;
+            v += y * in[((jd[0] * dims[1] + jd[1]) * dims[2] + jd[2]) * dims[3] + jd[3]];
+          }
+          out[e] = v;
+        }
+        __syncthreads();
+        for (int q = 0; q < 4; ++q) dims[q] = nd[q];
+        in = out;
+      }
+    }
+    for (int t = tid; t < Tab::NACC; t += NT) hs[t] = R(0);
+    for (int t = tid; t < 45; t += NT) h45[t] = R(0);
+    if (tid == 0) vs[Tab::NVSLOT] = R(0);
+    __syncthreads();
+    const PrimPair<R>* bp = a.prims + P.prim_off;
+    const PrimPair<R>* kp = a.prims + Q.prim_off;
+    const R* eA = a.alpha_a + P.prim_off;
+    const R* eB = a.alpha_b + P.prim_off;
+    const R* eC = a.alpha_a + Q.prim_off;
+    const int4* vo = Tab::vrr();
+    const int* vl = Tab::vlev();
+    const int2* acc = Tab::acc();
+    for (int ib = 0; ib < P.nprim; ++ib) {
+      const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;
+      const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;
+      const R wa = R(2) * eA[ib], wb = R(2) * eB[ib];
+      for (int ik = 0; ik < Q.nprim; ++ik) {
+        const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;
+        const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;
+        const R wc = R(2) * eC[ik];
+        const R pqs = p + q;
+        const R rs = rsqrt_t(pqs);
+        const R ipq = rs * rs;
+        const R rho = p * q * ipq;
+        const R rp = q * ipq, rq = p * ipq;
+        const R inv2p = R(0.5) * ip, inv2q = R(0.5) * iq, inv2pq = R(0.5) * ipq;
+        const R PQx = Px - Qx, PQy = Py - Qy, PQz = Pz - Qz;
+        const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+        if (tid <= Tab::L) {
+          R F[Tab::L + 1];
+          a.boys.template eval<Tab::L>(T, Kab * Kcd * rs, F);
+#pragma unroll
+          for (int m = 0; m <= Tab::L; ++m)
+            if (tid == m) vs[m] = F[m];
+        }
+        __syncthreads();
+        for (int l = 0; l < Tab::NVLEV; ++l) {
+          const int e = __ldg(vl + l + 1);
+          for (int oi = __ldg(vl + l) + tid; oi < e; oi += NT) {
+            const int4 op = __ldg(vo + oi);
+            const int dst = op.x & 0xffff, sa = (unsigned)op.x >> 16, sb = op.y & 0xffff, sc = (unsigned)op.y >> 16;
+            const int sd = op.z & 0xffff, kd = op.w & 255, k12 = (unsigned)op.w >> 8;
+            const int dir = kd >> 2;
+            const R PQd = dir == 0 ? PQx : (dir == 1 ? PQy : PQz);
+            const R k1 = small_int<R>(k12 & 255);
+            R v;
+            if ((kd & 1) == 0) {
+              const R PA = dir == 0 ? PAx : (dir == 1 ? PAy : PAz);
+              v = PA * vs[sa] - rp * PQd * vs[sb] + k1 * inv2p * (vs[sc] - rp * vs[sd]);
+            } else {
+              const R QC = dir == 0 ? QCx : (dir == 1 ? QCy : QCz);
+              const int sg = (unsigned)op.z >> 16;
+              v = QC * vs[sa] + rq * PQd * vs[sb] + k1 * inv2q * (vs[sc] - rq * vs[sd]) +
+                  small_int<R>(k12 >> 8) * inv2pq * vs[sg];
+            }
+            vs[dst] = v;
+          }
+          __syncthreads();
+        }
+        for (int t = tid; t < Tab::NACC; t += NT) {
+          const int2 ac = __ldg(acc + t);
+          R w;
+          switch (ac.y) {
+            case 0: w = R(1); break;
+            case 1: w = wa; break;
+            case 2: w = wb; break;
+            case 3: w = wc; break;
+            case 4: w = wa * wa; break;
+            case 5: w = wb * wb; break;
+            case 6: w = wc * wc; break;
+            case 7: w = wa * wb; break;
+            case 8: w = wa * wc; break;
+            default: w = wb * wc; break;
+          }
+          hs[t] += w * vs[ac.x];
+        }
+        __syncthreads();
+      }
+    }
+    // HRR levels; each ends with its contraction rows (sorted by output entry), taken by the
+    // threads in contiguous chunks
+    const int4* ho = Tab::hrr();
+    const int2* hl = Tab::hlev();
+    const R ABx = P.ABx, ABy = P.ABy, ABz = P.ABz, CDx = Q.ABx, CDy = Q.ABy, CDz = Q.ABz;
+    for (int l = 0; l < Tab::NHLEV; ++l) {
+      const int2 lv = __ldg(hl + l);
+      const int end = __ldg(hl + l + 1).x;
+      for (int oi = lv.x + tid; oi < lv.y; oi += NT) {
+        const int4 op = __ldg(ho + oi);
+        const int dir = (op.w >> 2) & 3;
+        const R d = (op.w & 1) ? (dir == 0 ? CDx : (dir == 1 ? CDy : CDz)) : (dir == 0 ? ABx : (dir == 1 ? ABy : ABz));
+        hs[op.x] = hs[op.y] + d * hs[op.z];
+      }
+      const int nc = end - lv.y;
+      if (nc > 0) {
+        const int chunk = (nc + NT - 1) / NT;
+        const int c0 = lv.y + tid * chunk, c1 = min(c0 + chunk, end);
+        int cur = -1;
+        R sum = R(0);
+        for (int oi = c0; oi < c1; ++oi) {
+          const int4 op = __ldg(ho + oi);
+          const int hi = (op.w >> 4) & 63, k = ((op.w >> 10) & 255) - 128;
+          if (hi != cur) {
+            if (cur >= 0) atomicAdd(h45 + cur, sum);
+            cur = hi;
+            sum = R(0);
+          }
+          sum += R(k) * W[op.x] * hs[op.y];
+        }
+        if (cur >= 0) atomicAdd(h45 + cur, sum);
+      }
+      __syncthreads();
+    }
+    // the 12 x 12 block over centres A, B, C, D into the Hessian (D by translational invariance)
+    if (tid < 9) {
+      const int i = tid / 3, j = tid % 3;
+      const int at[4] = {P.atom_a, P.atom_b, Q.atom_a, Q.atom_b};
+      double hx[4][4];
+      for (int X = 0; X < 3; ++X)
+        for (int Y = 0; Y < 3; ++Y) {
+          const int r = 3 * X + i, c = 3 * Y + j;
+          hx[X][Y] = r <= c ? h45[hess_tri(r, c)] : h45[hess_tri(c, r)];
+        }
+      for (int X = 0; X < 3; ++X) hx[X][3] = -(hx[X][0] + hx[X][1] + hx[X][2]);
+      for (int Y = 0; Y < 4; ++Y) hx[3][Y] = -(hx[0][Y] + hx[1][Y] + hx[2][Y]);
+      for (int X = 0; X < 4; ++X)
+        for (int Y = 0; Y < 4; ++Y)
+          if (hx[X][Y] != 0.0) atomicAdd(o.hess + (size_t)(3 * at[X] + i) * n3 + 3 * at[Y] + j, hx[X][Y]);
+    }
+    __syncthreads();
+  }
+}

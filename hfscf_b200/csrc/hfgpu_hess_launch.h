@@ -16,6 +16,11 @@ struct HessLaunchers {
   void (*launch)(const GradArgs<double>&, const HessOut&, int pure, const int2* q, int nq, int grid, int smem,
                  cudaStream_t);
   int (*scratch_slots)(int pure);  // doubles of scratch per thread
+  // block form (hess_block_kernel, one block of 128 threads per quartet, grid-stride); false when
+  // the class's tables do not fit one block's shared memory
+  bool (*launch_block)(const GradArgs<double>&, const HessOut&, int pure, const int2* q, int nq, int grid,
+                       cudaStream_t);
+  int (*block_global_slots)();  // doubles of global scratch per block of the block form (0: none)
 };
 
 extern const HessLaunchers* const kHessLaunchers[];

@@ -189,6 +189,11 @@ struct hfgpu_handle {
   // (grad_form_of)
   int grad_form[21];
   unsigned grad_class_mask = ~0u;       // classes a gradient launches (autotuning runs one at a time)
+  // Hessian form (hfgpu_set_hess_form): -1 by table size, 0 one thread per quartet, 1 one block
+  // per quartet wherever the class has the block form
+  int hess_form = -1;
+  int hess_cls_form[21];                // per class (hfgpu_autotune_hess): 0 thread, 1 block, -1 hess_form
+  unsigned hess_class_mask = ~0u;       // classes a Hessian launches (autotuning runs one at a time)
 
   hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21), q_prims(21) {
     for (int c = 0; c < 21; ++c) {
@@ -197,6 +202,7 @@ struct hfgpu_handle {
       sched_warp[c] = c < hfgpu::kNumClasses && hfgpu::kClassLaunchers[c]->warp_default ? -1 : 0;
       sched_cap[c] = 0;
       grad_form[c] = -1;
+      hess_cls_form[c] = -1;
     }
   }
 };
@@ -1785,12 +1791,16 @@ int hfgpu_grad2e_uhf_backward(hfgpu_handle* h, const double* Da, const double* D
 }
 
 // ---- Two-electron part of the Hessian at a fixed density (adjoint second derivatives) ----
-// Each class gets its own slice of one scratch buffer and runs on an auxiliary stream (fork/join
-// with the handle's stream, as the J/K classes do), so the few-quartet, long-table d classes
-// overlap the many-quartet s/p classes.  A class gets as many threads (whole 128-thread blocks)
-// as kHessScratchBudget holds, at most one per quartet, and loops over the rest.
-constexpr size_t kHessScratchBudget = (size_t)256 << 20;
+// The classes run on the auxiliary streams (fork/join with the handle's stream, as the J/K
+// classes do), so the few-quartet, long-table d classes overlap the many-quartet s/p classes.
+// Every auxiliary stream owns one slice of the scratch buffer, which its classes use one after
+// another; a class gets as many threads (whole 128-thread blocks) as kHessScratchBudget holds
+// (enough to fill the GPU for the largest tables), at most one per quartet, and loops over the rest.
+constexpr size_t kHessScratchBudget = (size_t)2 << 30;
 constexpr size_t kHessSmemBytes = 96 * 1024;  // per-block Hessian in shared memory up to 36 atoms
+constexpr int kHessBlockMinSlots = 1000;       // thread-form tables from this size run in the block form,
+constexpr long long kHessBlockMaxQuartets = 4096;  // and so do classes with at most this many quartets
+constexpr long long kHessBlockGrid = 296;      // blocks of a block-form launch with global HRR slots
 
 static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
                             double* hess) {
@@ -1817,37 +1827,97 @@ static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     thr = std::min<long long>(thr, ((nq + 127) / 128) * 128);
     return std::max<long long>(128, thr / 128 * 128);
   };
-  size_t off[32] = {0}, need = 0;
-  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+  // form per class: the block form (one block of 128 threads per quartet over levelised tables)
+  // for the classes whose one-thread tables are large or whose quartets are too few to fill the
+  // GPU with threads -- one thread would run a long chain of dependent table ops on global
+  // scratch -- the thread form for the small classes with many quartets
+  auto use_block = [&](int c) -> bool {
+    if (h->hess_cls_form[c] >= 0) return h->hess_cls_form[c] == 1;
+    if (h->hess_form == 0) return false;
+    if (h->hess_form == 1) return true;
+    return hfgpu::kHessLaunchers[c]->scratch_slots(h->pure) >= kHessBlockMinSlots ||
+           part_share(h, h->q_end[c] - h->q_beg[c]) <= kHessBlockMaxQuartets;
+  };
+  // block-form grid: one block per quartet, or kHessBlockGrid blocks when the HRR slots live in
+  // global scratch (one region per block)
+  auto block_grid = [&](int c, long long nq) -> long long {
+    return hfgpu::kHessLaunchers[c]->block_global_slots() > 0 ? std::min<long long>(nq, kHessBlockGrid) : nq;
+  };
+  // classes largest first, round-robin over the auxiliary streams; each stream's slice is the
+  // largest need of its classes
+  constexpr int kS = hfgpu_handle::kAux;
+  int stream_of[32];
+  size_t slice[kS] = {0}, off[kS] = {0}, need = 0;
+  int rr = 0;
+  for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
     const hfgpu::HessLaunchers* L = hfgpu::kHessLaunchers[c];
     const hfgpu::ClassLaunchers* C = hfgpu::kClassLaunchers[c];
     if (L->la != C->la || L->lb != C->lb || L->lc != C->lc || L->ld != C->ld)
       return fail(h, HFGPU_ERR_STATE, "Hessian class order");
-    off[c] = need;
+    stream_of[c] = -1;
     const long long nq = part_share(h, h->q_end[c] - h->q_beg[c]);
-    if (nq <= 0) continue;
-    const int slots = L->scratch_slots(h->pure);
-    need += ((size_t)slots * sizeof(double) * (size_t)threads_of(slots, nq) + 255) / 256 * 256;
+    if (nq <= 0 || !((h->hess_class_mask >> c) & 1u)) continue;
+    stream_of[c] = rr++ % kS;
+    size_t bytes;
+    if (use_block(c)) {
+      bytes = sizeof(double) * (size_t)L->block_global_slots() * (size_t)block_grid(c, nq);
+    } else {
+      const int slots = L->scratch_slots(h->pure);
+      bytes = (size_t)slots * sizeof(double) * (size_t)threads_of(slots, nq);
+    }
+    slice[stream_of[c]] = std::max(slice[stream_of[c]], (bytes + 255) / 256 * 256);
+  }
+  for (int st = 0; st < kS; ++st) {
+    off[st] = need;
+    need += slice[st];
   }
   if (need) HF_CUDA(h, h->d_scratch.ensure(need));
   int rc = fork_streams(h);
   if (rc) return rc;
-  int rr = 0;
   for (int c = hfgpu::kNumClasses - 1; c >= 0; --c) {
+    if (stream_of[c] < 0) continue;
     const hfgpu::HessLaunchers* L = hfgpu::kHessLaunchers[c];
     const long long nq = part_share(h, h->q_end[c] - h->q_beg[c]);
-    if (nq <= 0) continue;
+    if (use_block(c)) {
+      const int st = stream_of[c];
+      const long long grid = block_grid(c, nq);
+      if (sizeof(double) * (size_t)L->block_global_slots() * (size_t)grid > slice[st] ||
+          off[st] + slice[st] > h->d_scratch.bytes)
+        return fail(h, HFGPU_ERR_NOMEM, "Hessian scratch too small");
+      gd.scratch = reinterpret_cast<double*>(h->d_scratch.as<unsigned char>() + off[st]);
+      gd.scratch_threads = 0;
+      if (L->launch_block(gd, o, h->pure, q + h->q_beg[c], (int)nq, (int)grid, h->aux[st])) {
+        HF_CHECK_LAUNCH(h, "hess block kernel");
+        continue;
+      }
+      if (h->hess_form == 1) return fail(h, HFGPU_ERR_UNSUPPORTED, "class without a Hessian block form");
+    }
     const int slots = L->scratch_slots(h->pure);
     const long long thr = threads_of(slots, nq);
-    if (off[c] + (size_t)slots * sizeof(double) * (size_t)thr > h->d_scratch.bytes)
+    const int st = stream_of[c];
+    if ((size_t)slots * sizeof(double) * (size_t)thr > slice[st] || off[st] + slice[st] > h->d_scratch.bytes)
       return fail(h, HFGPU_ERR_NOMEM, "Hessian scratch too small");
-    gd.scratch = reinterpret_cast<double*>(h->d_scratch.as<unsigned char>() + off[c]);
+    gd.scratch = reinterpret_cast<double*>(h->d_scratch.as<unsigned char>() + off[st]);
     gd.scratch_threads = (int)thr;
-    L->launch(gd, o, h->pure, q + h->q_beg[c], (int)nq, (int)(thr / 128), o.smem ? (int)smem : 0,
-              h->aux[rr++ % hfgpu_handle::kAux]);
+    L->launch(gd, o, h->pure, q + h->q_beg[c], (int)nq, (int)(thr / 128), o.smem ? (int)smem : 0, h->aux[st]);
     HF_CHECK_LAUNCH(h, "hess kernel");
   }
   return join_streams(h);
+}
+
+int hfgpu_set_hess_form(hfgpu_handle* h, int form) {
+  if (!h || form < -1 || form > 1) return HFGPU_ERR_INVALID;
+  h->hess_form = form;
+  for (int c = 0; c < 21; ++c) h->hess_cls_form[c] = -1;
+  return HFGPU_OK;
+}
+
+int hfgpu_set_hess_forms(hfgpu_handle* h, const int* forms) {
+  if (!h || !forms) return HFGPU_ERR_INVALID;
+  for (int c = 0; c < hfgpu::kNumClasses; ++c)
+    if (forms[c] < -1 || forms[c] > 1) return HFGPU_ERR_INVALID;
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) h->hess_cls_form[c] = forms[c];
+  return HFGPU_OK;
 }
 
 int hfgpu_hess2e_device(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
@@ -2328,6 +2398,63 @@ int hfgpu_set_grad_forms(hfgpu_handle* h, const int* forms) {
     if (forms[c] < -1 || forms[c] > kGradForms - 1) return fail(h, HFGPU_ERR_INVALID, "gradient form out of range");
   for (int c = 0; c < hfgpu::kNumClasses; ++c)
     h->grad_form[c] = hfgpu::kClassLaunchers[c]->has_grad_warp ? forms[c] : -1;
+  return HFGPU_OK;
+}
+
+// Hessian form per class: each class alone, one thread per quartet against one block per
+// quartet, on RHF weights of the device density D; the faster is kept.
+int hfgpu_autotune_hess(hfgpu_handle* h, const double* D, int repeats, int* forms) {
+  if (!h || !D) return HFGPU_ERR_INVALID;
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
+  if (rc) return rc;
+  if (!h->have_geometry) return fail(h, HFGPU_ERR_STATE, "no geometry set");
+  if (h->batched) return fail(h, HFGPU_ERR_UNSUPPORTED, "the Hessian takes a single-molecule handle");
+  repeats = std::max(1, std::min(repeats, 100));
+  DevBuf hb;
+  const size_t n3 = 3 * (size_t)std::max(h->natoms, 1);
+  HF_CUDA(h, hb.ensure(sizeof(double) * n3 * n3));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  HF_CUDA(h, cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(h, HFGPU_ERR_CUDA, "cudaEventCreate");
+  }
+  struct Restore {
+    hfgpu_handle* h;
+    cudaEvent_t a, b;
+    DevBuf flush;
+    ~Restore() {
+      h->hess_class_mask = ~0u;
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      flush.release();
+    }
+  } restore{h, e0, e1, DevBuf{}};
+  if (restore.flush.ensure(kTunerFlushBytes) != cudaSuccess) {
+    cudaGetLastError();
+    restore.flush = DevBuf{};
+  }
+  auto hessian = [&]() { return hess_device_impl(h, D, 2.0, 1, D, 1.0, hb.as<double>()); };
+  for (int c = 0; c < hfgpu::kNumClasses; ++c) {
+    if (h->q_end[c] <= h->q_beg[c]) continue;
+    h->hess_class_mask = 1u << c;
+    float best = 1e30f;
+    int best_form = 0;
+    for (int form = 0; form < 2; ++form) {
+      h->hess_cls_form[c] = form;
+      float ms = 0.f;
+      if ((rc = tuner_time(h, hessian, repeats, e0, e1, restore.flush, &ms))) return rc;
+      if (ms < best) {
+        best = ms;
+        best_form = form;
+      }
+    }
+    h->hess_cls_form[c] = best_form;
+  }
+  if (forms)
+    for (int c = 0; c < hfgpu::kNumClasses; ++c) forms[c] = h->hess_cls_form[c];
+  hb.release();
   return HFGPU_OK;
 }
 

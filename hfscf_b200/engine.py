@@ -378,6 +378,21 @@ class Engine:
         self._check(lib().hfgpu_hess2e(self.h, _p(_c(D)), ctypes.c_double(scale), _p(H)))
         return H
 
+    def set_hess_form(self, form: int):
+        """hfgpu_set_hess_form: -1 by table size (default), 0 thread per quartet, 1 block per quartet."""
+        self._check(lib().hfgpu_set_hess_form(self.h, ctypes.c_int(form)))
+
+    def autotune_hess(self, D_ptr, repeats=2):
+        """hfgpu_autotune_hess on a device density: per class the faster of the thread and block
+        forms; returns the chosen forms."""
+        forms = (ctypes.c_int * NUM_CLASSES)()
+        self._check(lib().hfgpu_autotune_hess(self.h, ctypes.c_void_p(D_ptr), ctypes.c_int(repeats), forms))
+        return list(forms)
+
+    def set_hess_forms(self, forms):
+        arr = (ctypes.c_int * NUM_CLASSES)(*forms)
+        self._check(lib().hfgpu_set_hess_forms(self.h, arr))
+
     def hess2e_uhf(self, Da, Db, scale=1.0) -> np.ndarray:
         n3 = 3 * self.basis.natoms
         H = np.zeros((n3, n3))

@@ -138,6 +138,17 @@ int hfgpu_grad2e_uhf_backward(hfgpu_handle* h, const double* Da, const double* D
  * FP64 only; single-molecule handles (HFGPU_ERR_UNSUPPORTED for a batched handle). */
 int hfgpu_hess2e(hfgpu_handle* h, const double* D, double scale, double* hess);
 int hfgpu_hess2e_uhf(hfgpu_handle* h, const double* Da, const double* Db, double scale, double* hess);
+/* Launch form of the Hessian classes: -1 (default) one block of 128 threads per quartet for the
+ * classes with large op tables and one thread per quartet for the others, 0 one thread per
+ * quartet everywhere, 1 one block per quartet everywhere.  The results agree to rounding. */
+int hfgpu_set_hess_form(hfgpu_handle* h, int form);
+/* Per class (HFGPU_NUM_CLASSES ints: 0 thread, 1 block, -1 the rule of hfgpu_set_hess_form), as
+ * hfgpu_autotune_hess returns them. */
+int hfgpu_set_hess_forms(hfgpu_handle* h, const int* forms);
+/* Times every class alone in both forms on RHF weights of the device density D (median of
+ * `repeats` runs, L2 flushed before each) and keeps the faster per class; forms (may be NULL)
+ * receives the choice.  No counterpart in the reference (which has one CPU code path). */
+int hfgpu_autotune_hess(hfgpu_handle* h, const double* D, int repeats, int* forms);
 
 /* Device-pointer variants (enqueue on the handle's stream, no host synchronisation). */
 /* hess (device, 3 natoms x 3 natoms) += sum W d2(ab|cd)/dX dY with the weights of

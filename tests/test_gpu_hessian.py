@@ -54,11 +54,18 @@ def _ref_hessian(bs, D):
     return hc + he
 
 
+FORMS = [(-1, "default"), (0, "thread"), (1, "block")]
+
+
+@pytest.mark.parametrize("form", [f for f, _ in FORMS], ids=[n for _, n in FORMS])
 @pytest.mark.parametrize("name,bs", MOLS, ids=[m[0] for m in MOLS])
-def test_hess2e_matches_reference(name, bs):
+def test_hess2e_matches_reference(name, bs, form):
+    """Every launch form (one thread per quartet on global scratch, one block per quartet over
+    levelised tables, and the default mix of the two) against the reference."""
     rng = np.random.default_rng(3)
     D = _sym(rng, bs.nbf)
     with E.Engine(bs) as eng:
+        eng.set_hess_form(form)
         H = eng.hess2e(D)
     Href = _ref_hessian(bs, D)
     assert np.max(np.abs(H - Href)) < HESS_TOL, np.max(np.abs(H - Href))
