@@ -233,6 +233,23 @@ class GpuGradient {
   hfgpu_precision precision_;
 };
 
+// The two-electron part of the analytic Hessian, in place of Mol::scf_hessian::calc_scf_hessian_tei
+// (src/hessian/hfscf_hessian_ints.cpp:20-303): hess (3 natoms x 3 natoms, row-major) += the
+// reference's m_hessianC + m_hessianEx at d_mat, from second-derivative integrals that are never stored.
+class GpuHessian {
+ public:
+  explicit GpuHessian(Engine& engine) : eng_(engine) {}
+  void calc_scf_hessian_tei(const double* d_mat, double* hess) const {
+    check(hfgpu_hess2e(eng_.handle(), d_mat, 1.0, hess), eng_.handle(), "hfgpu_hess2e");
+  }
+  void calc_scf_hessian_tei_uhf(const double* d_mat_a, const double* d_mat_b, double* hess) const {
+    check(hfgpu_hess2e_uhf(eng_.handle(), d_mat_a, d_mat_b, 1.0, hess), eng_.handle(), "hfgpu_hess2e_uhf");
+  }
+
+ private:
+  Engine& eng_;
+};
+
 }  // namespace hfgpu
 
 #endif

@@ -7,7 +7,8 @@
 //     nprim[nshell]; exps[sum nprim]; coefs[sum nprim]; xyz[natoms*3] (bohr); D[n*n]; H[n*n]
 //   OUTPUT (raw float64): the packed ERI vector filled quartet by quartet as
 //     create_repulsion_matrix fills it (src/scfsolver/hfscf_hf_hamiltonian.cpp:77-111, screening
-//     on), F = H + 2J[D] - K[D], and the two-electron gradient (natoms x 3)
+//     on), F = H + 2J[D] - K[D], the two-electron gradient (natoms x 3) and the two-electron
+//     Hessian (3 natoms x 3 natoms)
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -64,11 +65,14 @@ int main(int argc, char** argv) {
     jk.update_fock_matrix(D.data(), H.data(), F.data());
     hfgpu::GpuGradient gr(eng);
     gr.calc_two_electron_gradient_rhf(D.data(), grad.data());
+    std::vector<double> hess(9 * (size_t)natoms * natoms, 0.0);
+    hfgpu::GpuHessian(eng).calc_scf_hessian_tei(D.data(), hess.data());
     FILE* out = std::fopen(argv[2], "wb");
     if (!out) return 2;
     std::fwrite(eri.data(), sizeof(double), eri.size(), out);
     std::fwrite(F.data(), sizeof(double), F.size(), out);
     std::fwrite(grad.data(), sizeof(double), grad.size(), out);
+    std::fwrite(hess.data(), sizeof(double), hess.size(), out);
     std::fclose(out);
   } catch (const hfgpu::Error& e) {
     std::cerr << "hfgpu error " << e.code() << ": " << e.what() << "\n";

@@ -4,8 +4,10 @@ unit would be, linked against libhfgpu.so, and run.
 CPU: the program compiles and links against the header and the library (no GPU needed).
 GPU: the program fills the packed ERI vector quartet by quartet through GpuErios (the
 reference's create_repulsion_matrix loop, screening on), one Fock build through GpuJK and the
-two-electron gradient through GpuGradient; each is checked against the oracle (ERIs 1e-11,
-F 1e-10, gradient 1e-10; screened slots below the reference's screen_tol 1e-12 may be zero).
+two-electron gradient through GpuGradient and the two-electron Hessian through GpuHessian; each
+is checked against the oracle (ERIs 1e-11, F 1e-10, gradient 1e-10, Hessian 1e-9 against the
+reference's own second-derivative code; screened slots below the reference's screen_tol 1e-12
+may be zero).
 """
 import os
 import shutil
@@ -66,10 +68,16 @@ def test_cpp_boundary_matches_oracle(tmp_path, pure):
     assert r.returncode == 0, r.stderr
     data = np.fromfile(out, dtype=np.float64)
     nl = oracle.packed_len(n)
-    eri, F, g = data[:nl], data[nl:nl + n * n].reshape(n, n), data[nl + n * n:].reshape(bs.natoms, 3)
+    na = bs.natoms
+    eri, F = data[:nl], data[nl:nl + n * n].reshape(n, n)
+    g = data[nl + n * n:nl + n * n + 3 * na].reshape(na, 3)
+    hess = data[nl + n * n + 3 * na:].reshape(3 * na, 3 * na)
     eri0 = oracle.eri_packed(bs)
     err = np.abs(eri - eri0)
     screened = (eri == 0.0) & (np.abs(eri0) < 1e-12)
     assert np.max(np.where(screened, 0.0, err)) < 1e-11
     assert np.max(np.abs(F - oracle.fock_rhf(eri0, D, H))) < 1e-10
     assert np.max(np.abs(g - oracle.grad2e_rhf(bs, D))) < 1e-10
+    if oracle.ref_available():
+        hc, he = oracle.ref_hess2e(bs, D)
+        assert np.max(np.abs(hess - (hc + he))) < 1e-9
