@@ -1,6 +1,7 @@
 // Host side of the hfgpu engine: basis set-up, primitive-pair data, Schwarz
 // factors, screened quartet lists, and the C ABI of include/hfgpu.h.
 #include <algorithm>
+#include <cooperative_groups.h>
 #include <atomic>
 #include <chrono>
 #include <thread>
@@ -192,6 +193,8 @@ struct hfgpu_handle {
   // Hessian form (hfgpu_set_hess_form): -1 by table size, 0 one thread per quartet, 1 one block
   // per quartet wherever the class has the block form
   int hess_form = -1;
+  int purify_blocks = -1;               // co-resident blocks of the cooperative purification (0: not available)
+  int purify_coop = 1;                  // hfgpu_set_purify_mode: 1 one cooperative launch, 0 two launches per step
   int hess_cls_form[21];                // per class (hfgpu_autotune_hess): 0 thread, 1 block, -1 hess_form
   unsigned hess_class_mask = ~0u;       // classes a Hessian launches (autotuning runs one at a time)
 
@@ -892,6 +895,93 @@ __global__ void purify_update_kernel(double* __restrict__ A, const double* __res
   }
   if (frozen || e >= (long long)n * n) return;
   A[e] = step[0] > (double)nocc ? C[e] : 2.0 * A[e] - C[e];
+}
+
+// The same purification as one cooperative launch: every block owns 16 x 16 output tiles
+// (grid-stride), computes the Gershgorin bounds itself, and the blocks meet at a grid-wide
+// barrier twice per step (after the squares and traces, after the update of their own tiles);
+// once a step freezes, every block leaves the loop at the same step, so the frozen steps cost
+// nothing.  Same arithmetic, step for step, as the kernels above.
+__global__ void __launch_bounds__(kPurifyTile * kPurifyTile) purify_coop_kernel(
+    const double* __restrict__ F, int n, int nocc, int max_steps, double tol, double* __restrict__ A,
+    double* __restrict__ C, double* __restrict__ slots, double* __restrict__ err) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double ta[kPurifyTile][kPurifyTile + 1], tb[kPurifyTile][kPurifyTile + 1];
+  __shared__ double red[2][kPurifyTile * kPurifyTile];
+  const int tx = threadIdx.x % kPurifyTile, ty = threadIdx.x / kPurifyTile;
+  const int nt = (n + kPurifyTile - 1) / kPurifyTile;
+  const int ntiles = nt * nt;
+  // Gershgorin bounds of F, by every block for itself
+  double lo = 1e300, hi = -1e300;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double r = 0.0;
+    for (int j = 0; j < n; ++j)
+      if (j != i) r += fabs(F[(size_t)i * n + j]);
+    lo = fmin(lo, F[(size_t)i * n + i] - r);
+    hi = fmax(hi, F[(size_t)i * n + i] + r);
+  }
+  red[0][threadIdx.x] = lo;
+  red[1][threadIdx.x] = hi;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+    if ((int)threadIdx.x < off) {
+      red[0][threadIdx.x] = fmin(red[0][threadIdx.x], red[0][threadIdx.x + off]);
+      red[1][threadIdx.x] = fmax(red[1][threadIdx.x], red[1][threadIdx.x + off]);
+    }
+    __syncthreads();
+  }
+  const double emin = red[0][0], emax = red[1][0];
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int row = (t / nt) * kPurifyTile + ty, col = (t % nt) * kPurifyTile + tx;
+    if (row < n && col < n) A[(size_t)row * n + col] = ((row == col ? emax : 0.0) - F[(size_t)row * n + col]) / (emax - emin);
+  }
+  if (blockIdx.x == 0)
+    for (int i = threadIdx.x; i < 3 * (max_steps + 1); i += blockDim.x) slots[i] = 0.0;
+  grid.sync();
+  for (int k = 0; k < max_steps; ++k) {
+    double* step = slots + 3 * k;
+    // the step's flags and traces are read from L2 (__ldcg), never from a block's L1, so that every
+    // block takes the same decision after the barrier
+    if (__ldcg(step + 2) != 0.0) break;  // frozen at an earlier step
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const int row = (t / nt) * kPurifyTile + ty, col = (t % nt) * kPurifyTile + tx;
+      double acc = 0.0;
+      for (int k0 = 0; k0 < n; k0 += kPurifyTile) {
+        ta[ty][tx] = (row < n && k0 + tx < n) ? A[(size_t)row * n + k0 + tx] : 0.0;
+        tb[ty][tx] = (k0 + ty < n && col < n) ? A[(size_t)(k0 + ty) * n + col] : 0.0;
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kPurifyTile; ++kk) acc = fma(ta[ty][kk], tb[kk][tx], acc);
+        __syncthreads();
+      }
+      if (row < n && col < n) {
+        C[(size_t)row * n + col] = acc;
+        if (row == col) {
+          atomicAdd(step + 0, A[(size_t)row * n + col]);
+          atomicAdd(step + 1, acc);
+        }
+      }
+    }
+    grid.sync();
+    const double tr = __ldcg(step + 0), tr2 = __ldcg(step + 1);
+    const bool frozen = (tr - tr2) < tol;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      step[5] = frozen ? 1.0 : 0.0;  // the next step's flag
+      *err = frozen ? tr - tr2 : 1.0;
+    }
+    if (!frozen) {
+      const bool up = tr > (double)nocc;
+      for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int row = (t / nt) * kPurifyTile + ty, col = (t % nt) * kPurifyTile + tx;
+        if (row < n && col < n) {
+          const size_t e = (size_t)row * n + col;
+          A[e] = up ? C[e] : 2.0 * A[e] - C[e];
+        }
+      }
+    }
+    grid.sync();
+  }
 }
 
 // FP64 FMA throughput probe: 8 independent FMA chains per thread.
@@ -2563,6 +2653,29 @@ int hfgpu_purify_device(hfgpu_handle* h, const double* Fo, int n, int nocc, int 
   double* C = h->d_purify.as<double>();
   double* slots = C + nn;
   double* bounds = slots + nslot;
+  // one cooperative launch when the device supports it and the grid fits at once
+  if (h->purify_blocks < 0) {
+    int coop = 0, sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, h->device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, purify_coop_kernel, kPurifyTile * kPurifyTile,
+                                                              0) == cudaSuccess)
+      h->purify_blocks = per_sm * sms;
+    else
+      h->purify_blocks = 0;
+    cudaGetLastError();
+  }
+  if (h->purify_blocks > 0 && h->purify_coop) {
+    const int nt = (n + kPurifyTile - 1) / kPurifyTile;
+    int grid = std::min(nt * nt, h->purify_blocks);
+    double tol = 1e-11;
+    void* args[] = {(void*)&Fo, (void*)&n, (void*)&nocc, (void*)&max_steps, (void*)&tol, (void*)&P, (void*)&C,
+                    (void*)&slots, (void*)&err};
+    HF_CUDA(h, cudaLaunchCooperativeKernel((const void*)purify_coop_kernel, dim3(grid), dim3(kPurifyTile * kPurifyTile),
+                                           args, 0, h->stream));
+    HF_CHECK_LAUNCH(h, "cooperative purification");
+    return HFGPU_OK;
+  }
   purify_bounds_kernel<<<1, 1024, 0, h->stream>>>(Fo, n, slots, nslot, bounds);
   const int eb = (int)((nn + 255) / 256);
   purify_init_kernel<<<eb, 256, 0, h->stream>>>(Fo, n, bounds, P);
@@ -2572,6 +2685,12 @@ int hfgpu_purify_device(hfgpu_handle* h, const double* Fo, int n, int nocc, int 
     purify_update_kernel<<<eb, 256, 0, h->stream>>>(P, C, n, nocc, 1e-11, slots + 3 * k, slots + 3 * (k + 1), err);
   }
   HF_CHECK_LAUNCH(h, "purification");
+  return HFGPU_OK;
+}
+
+int hfgpu_set_purify_mode(hfgpu_handle* h, int cooperative) {
+  if (!h || cooperative < 0 || cooperative > 1) return HFGPU_ERR_INVALID;
+  h->purify_coop = cooperative;
   return HFGPU_OK;
 }
 

@@ -338,6 +338,10 @@ class Engine:
                                               ctypes.c_int(max_steps), ctypes.c_void_p(P_ptr),
                                               ctypes.c_void_p(err_ptr)))
 
+    def set_purify_mode(self, cooperative: int):
+        """hfgpu_set_purify_mode: 1 one cooperative launch per purification, 0 two launches per step."""
+        self._check(lib().hfgpu_set_purify_mode(self.h, ctypes.c_int(cooperative)))
+
     def request_abort(self, on=True):
         """hfgpu_request_abort: set (or reset) the host abort flag of the persistent launches."""
         self._check(lib().hfgpu_request_abort(self.h, ctypes.c_int(int(on))))

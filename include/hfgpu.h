@@ -227,6 +227,10 @@ int hfgpu_one_electron_grad_device(hfgpu_handle* h, const double* Z, const doubl
  * Mol::hf_solver::calc_density_matrix (src/scfsolver/hfscf_hf_solver.cpp:206-231) for a
  * closed-shell density: C_occ C_occ^T is that projector.  Enqueued on the handle's stream. */
 int hfgpu_purify_device(hfgpu_handle* h, const double* Fo, int n, int nocc, int max_steps, double* P, double* err);
+/* Launch form of hfgpu_purify_device: 1 (default) one cooperative launch whose blocks meet at a
+ * grid-wide barrier between the phases of a step and all stop at the step that converged (when
+ * the device supports cooperative launches), 0 two launches per step for every step. */
+int hfgpu_set_purify_mode(hfgpu_handle* h, int cooperative);
 
 /* Counters of the last J/K build: quartets launched and quartets skipped by density screening. */
 int hfgpu_last_counts(const hfgpu_handle* h, long long* launched, long long* skipped);

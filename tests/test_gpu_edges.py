@@ -150,10 +150,13 @@ def test_setup_times_and_list_segments_cover_every_screened_quartet():
     assert listed == int(np.count_nonzero(prod[iu] >= 1e-12))
 
 
-@pytest.mark.parametrize("n,nocc", [(7, 3), (152, 40), (210, 33)])
-def test_purification_matches_the_diagonalisation_projector(n, nocc):
+@pytest.mark.parametrize("coop", [1, 0], ids=["cooperative", "two-launches-per-step"])
+@pytest.mark.parametrize("n,nocc", [(7, 3), (152, 40), (210, 33), (700, 150)])
+def test_purification_matches_the_diagonalisation_projector(n, nocc, coop):
     """hfgpu_purify_device: the projector onto the nocc lowest eigenvectors of a symmetric matrix
-    with a gap, against numpy's eigh (1e-10), and a reported trace error below 1e-10."""
+    with a gap, against numpy's eigh (1e-10), and a reported trace error below 1e-10; in the one
+    cooperative launch and in the two-launches-per-step form (n = 700: more tiles than one wave
+    of co-resident blocks, so the cooperative blocks loop over tiles)."""
     import torch
     rng = np.random.default_rng(n)
     Q, _ = np.linalg.qr(rng.normal(size=(n, n)))
@@ -165,6 +168,7 @@ def test_purification_matches_the_diagonalisation_projector(n, nocc):
     bs = B.build_basis("sto-3g", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR)
     dev = torch.device("cuda", 0)
     with E.Engine(bs) as eng:
+        eng.set_purify_mode(coop)
         F = torch.from_numpy(Fo).to(dev)
         P = torch.empty_like(F)
         err = torch.zeros((), dtype=torch.float64, device=dev)
@@ -174,7 +178,8 @@ def test_purification_matches_the_diagonalisation_projector(n, nocc):
         assert np.max(np.abs(P.cpu().numpy() - P0)) < 1e-10
 
 
-def test_purification_reports_a_missing_gap():
+@pytest.mark.parametrize("coop", [1, 0], ids=["cooperative", "two-launches-per-step"])
+def test_purification_reports_a_missing_gap(coop):
     """Two equal eigenvalues at the Fermi level: no projector separates them, the purification
     does not converge and says so (err = 1), so the SCF diagonalises instead.  (24 steps: far
     more would let rounding split the pair, 2^-53 doubling each step.)"""
@@ -189,6 +194,7 @@ def test_purification_reports_a_missing_gap():
     bs = B.build_basis("sto-3g", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR)
     dev = torch.device("cuda", 0)
     with E.Engine(bs) as eng:
+        eng.set_purify_mode(coop)
         F = torch.from_numpy(Fo).to(dev)
         P = torch.empty_like(F)
         err = torch.zeros((), dtype=torch.float64, device=dev)
