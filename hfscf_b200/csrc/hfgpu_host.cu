@@ -1575,10 +1575,12 @@ int hfgpu_create(const hfgpu_basis* b, const hfgpu_opts* opts, hfgpu_handle** ou
     return HFGPU_ERR_CUDA;
   }
   h->own_stream = true;
-  const std::vector<double> bt = boys_table<double>(7);
-  const std::vector<float> btf = boys_table<float>(4);
-  const std::vector<double> bpd = boys_planes(bt);
-  const std::vector<float> bpf = boys_planes(btf);
+  // the tables are constants: computed once per process (the long-double series take milliseconds),
+  // uploaded per handle
+  static const std::vector<double> bt = boys_table<double>(7);
+  static const std::vector<float> btf = boys_table<float>(4);
+  static const std::vector<double> bpd = boys_planes(bt);
+  static const std::vector<float> bpf = boys_planes(btf);
   if (h->d_boys_d.ensure(sizeof(double) * bt.size()) || h->d_boys_f.ensure(sizeof(float) * btf.size()) ||
       h->d_boys_pd.ensure(sizeof(double) * bpd.size()) || h->d_boys_pf.ensure(sizeof(float) * bpf.size()) ||
       h->d_status.ensure(sizeof(int)) || h->d_abort.ensure(sizeof(int)) ||
