@@ -31,6 +31,8 @@ from . import engine as eng
 from .basis import Basis, build_basis, nuclear_repulsion, nuclear_repulsion_gradient
 from .scf import DIIS_EPS
 
+PURIFY_TOL = 1e-10  # largest tr P - tr P^2 accepted from a molecule's purification
+PURIFY_STEPS = 64   # squarings of one purification (each molecule stops at its converged step)
 PAD_DIAG = 1.0e3  # padded diagonal of F: far above every occupied orbital energy
 
 
@@ -112,6 +114,13 @@ class BatchEngine:
                                                ctypes.c_void_p(V.data_ptr()),
                                                ctypes.c_void_p(sweeps.data_ptr() if sweeps is not None else 0)))
 
+    def purify(self, Fo, nocc, P, err, max_steps=64):
+        """hfgpu_batch_purify_device: P = projector onto the nocc lowest eigenvectors of every
+        molecule's block of the padded Fo [nmol, nmax, nmax]; err [nmol] (device tensors; nocc int32)."""
+        self._check(eng.lib().hfgpu_batch_purify_device(self.h, ctypes.c_void_p(Fo.data_ptr()),
+                                                        ctypes.c_void_p(nocc.data_ptr()), ctypes.c_int(max_steps),
+                                                        ctypes.c_void_p(P.data_ptr()), ctypes.c_void_p(err.data_ptr())))
+
     def grad2e_device(self, D, grad, precision=eng.FP64):
         self._check(eng.lib().hfgpu_batch_grad2e_device(self.h, ctypes.c_void_p(D.data_ptr()),
                                                         ctypes.c_void_p(grad.data_ptr()), ctypes.c_int(precision)))
@@ -159,10 +168,13 @@ class _Layout:
 
 
 def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-10, rms_tol=1e-8,
-              max_iter=60, use_graph=True, gradient=True, autotune=False, diag="gpu", diis_range=5,
+              max_iter=60, use_graph=True, gradient=True, autotune=False, diag="purify", diis_range=5,
               schedule=None):
     """Converged RHF energies (and gradients) of every molecule of the batch.  ``diag``:
-    "gpu" diagonalises every molecule's Fock matrix in one launch of the batched Jacobi
+    "purify" (default) takes every molecule's density from one launch of the batched
+    trace-correcting purification (hfgpu_batch_purify_device, molecules of up to 116 functions),
+    diagonalising with the batched Jacobi kernel instead in an iteration where some molecule's
+    purification did not converge; "gpu" diagonalises every iteration with the batched Jacobi
     kernel (hfgpu_batch_eigh, molecules of up to 118 functions); "host" runs LAPACK per
     molecule on a host thread pool.  ``autotune`` runs hfgpu_autotune on the first density
     before the graph is captured (off by default: for 512 small molecules it cost 2.4 s and
@@ -201,7 +213,9 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     Vev = torch.empty((nmol, nmax, nmax), dtype=torch.float64, device=dev)
     # symmetric orthogonalisers X = S^-1/2 (padding: identity)
     Xh = []
-    if diag == "gpu":
+    if diag == "purify" and nmax > 116:
+        diag = "gpu"  # the purification keeps a molecule's matrix in one block's shared memory
+    if diag in ("gpu", "purify"):
         be.eigh(S, Wev, Vev)
         X = (Vev * Wev.rsqrt()[:, None, :]) @ Vev.transpose(1, 2)
     else:
@@ -231,7 +245,20 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
         C = X @ Vev
         return (C * occ[:, None, :]) @ C.transpose(1, 2)
 
+    nocc_d = torch.tensor(nocc_h, dtype=torch.int32, device=dev)
+    Ppur = torch.empty((nmol, nmax, nmax), dtype=torch.float64, device=dev)
+    perr = torch.empty(nmol, dtype=torch.float64, device=dev)
+    fallbacks = [0]
+
+    def density_purify(F):
+        Fp = X.transpose(1, 2) @ F @ X
+        Fp = (0.5 * (Fp + Fp.transpose(1, 2))).contiguous()
+        be.purify(Fp, nocc_d, Ppur, perr, PURIFY_STEPS)
+        return X @ Ppur @ X.transpose(1, 2)
+
     def density(F):
+        if diag == "purify":
+            return density_purify(F)
         if diag == "gpu":
             return density_gpu(F)
         Fh = lay.to_block(F).cpu().numpy()
@@ -247,6 +274,9 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
         return lay.to_pad(torch.from_numpy(Dh).to(dev))
 
     D = density(H)
+    if diag == "purify" and bool((perr >= PURIFY_TOL).any()):
+        D = density_gpu(H)
+        fallbacks[0] += 1
     Dblk = lay.to_block(D).contiguous()
     Jblk = torch.zeros_like(Dblk)
     Kblk = torch.zeros_like(Dblk)
@@ -331,9 +361,23 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
         D = density(F)
         E = ((D * (H + F)).sum(dim=(1, 2)) - PAD_DIAG * 0)  # padded entries of D are zero
         conv = (rms < rms_tol) & ((E - E_prev).abs() < e_tol)
+        if diag == "purify":
+            # one host read per iteration: whether every molecule converged, and whether some
+            # molecule's purification did not (then this iteration diagonalises instead)
+            flags = torch.stack([(perr >= PURIFY_TOL).any(), (converged | conv).all()]).cpu()
+            if bool(flags[0]):
+                fallbacks[0] += 1
+                D = density_gpu(F)
+                E = (D * (H + F)).sum(dim=(1, 2))
+                conv = (rms < rms_tol) & ((E - E_prev).abs() < e_tol)
+                done = bool((converged | conv).all())
+            else:
+                done = bool(flags[1])
+        else:
+            done = bool((converged | conv).all())
         converged |= conv
         E_prev = E
-        if bool(converged.all()):
+        if done:
             break
     torch.cuda.synchronize()
     t_scf = time.perf_counter() - t1
@@ -347,7 +391,7 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     enuc = np.array([nuclear_repulsion(b.Z, b.coords) for b in bases])
     out = {"energies": E_el + enuc, "iterations": it, "converged": converged.cpu().numpy(),
            "setup_s": t_setup, "setup_stages_s": stages, "scf_s": t_scf, "graph": graph is not None,
-           "autotuned": tuned, "schedule": schedule,
+           "autotuned": tuned, "schedule": schedule, "density": diag, "diag_fallbacks": fallbacks[0],
            "build_ms_mean": float(np.mean([a.elapsed_time(b) for a, b in build_events])), "nmol": nmol,
            "final_s": time.perf_counter() - t_fin}
     if gradient:

@@ -20,6 +20,7 @@
 #include "hfgpu_onee.h"
 #include "hfgpu_onee_kernels.cuh"
 #include "hfgpu_batch_eigh.cuh"
+#include "hfgpu_batch_purify.cuh"
 
 namespace {
 
@@ -2204,6 +2205,25 @@ int hfgpu_batch_eigh(hfgpu_handle* h, const double* A, double* W, double* V, int
   const int* mol_n = reinterpret_cast<const int*>(h->d_mol.as<long long>() + h->nmol);
   batch_jacobi_kernel<<<h->nmol, kJacobiThreads, smem, h->stream>>>(A, nmax, mol_n, W, V, 30, sweeps);
   HF_CHECK_LAUNCH(h, "batched eigensolver");
+  return HFGPU_OK;
+}
+
+int hfgpu_batch_purify_device(hfgpu_handle* h, const double* Fo, const int* nocc, int max_steps, double* P,
+                              double* err) {
+  if (!h || !Fo || !nocc || !P || !err || max_steps <= 0 || max_steps > 256) return HFGPU_ERR_INVALID;
+  if (!h->batched) return fail(h, HFGPU_ERR_UNSUPPORTED, "hfgpu_batch_purify_device needs a batched handle");
+  const int nmax = h->n;
+  if (nmax > kBatchPurifyMaxN)
+    return fail(h, HFGPU_ERR_UNSUPPORTED, "batched purification: a molecule has more than 116 functions");
+  DeviceGuard dev_guard(h);
+  int rc = dev_guard.rc;
+  if (rc) return rc;
+  const size_t smem = batch_purify_smem_bytes(nmax);
+  HF_CUDA(h, cudaFuncSetAttribute(batch_purify_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int* mol_n = reinterpret_cast<const int*>(h->d_mol.as<long long>() + h->nmol);
+  batch_purify_kernel<<<h->nmol, kBatchPurifyThreads, smem, h->stream>>>(Fo, nmax, mol_n, nocc, max_steps, 1e-11, P,
+                                                                          err);
+  HF_CHECK_LAUNCH(h, "batched purification");
   return HFGPU_OK;
 }
 

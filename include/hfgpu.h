@@ -196,6 +196,16 @@ int hfgpu_batch_grad2e_device(hfgpu_handle* h, const double* D, double* grad, in
  * through as identity eigenvectors.  sweeps (device, nmol ints, may be NULL) receives the
  * Jacobi sweeps each molecule took.  Device pointers, enqueued on the handle's stream. */
 int hfgpu_batch_eigh(hfgpu_handle* h, const double* A, double* W, double* V, int* sweeps);
+/* The batched SCF's density step without a diagonalisation: P (nmol x nmax x nmax, padded, zero
+ * outside each block) = the projector onto the nocc[b] lowest eigenvectors of every molecule's
+ * orthonormal-basis Fock block in Fo (same layout), by trace-correcting purification, one thread
+ * block per molecule with the matrix in shared memory (molecules of up to 116 functions); each
+ * stops at its own converged step.  err[b] (device) = tr P - tr P^2 there, or 1 when max_steps did
+ * not converge (diagonalise that iteration instead).  nocc: device ints.  Replaces, for a
+ * closed-shell density, the diagonalisation of Mol::hf_solver::calc_density_matrix
+ * (src/scfsolver/hfscf_hf_solver.cpp:206-231).  Enqueued on the handle's stream. */
+int hfgpu_batch_purify_device(hfgpu_handle* h, const double* Fo, const int* nocc, int max_steps, double* P,
+                              double* err);
 
 /* One-electron matrices S, T, V (n x n) for the basis at xyz (bohr), on the host CPU.
  * Z: nuclear charges per atom.  Needs no handle and no GPU (the reference's

@@ -40,8 +40,8 @@ def test_batch_jk_matches_single_molecule_engine():
     be.close()
 
 
-@pytest.mark.parametrize("use_graph,diag", [(True, "gpu"), (False, "gpu"), (True, "host")],
-                         ids=["cuda-graph", "eager", "host-diag"])
+@pytest.mark.parametrize("use_graph,diag", [(True, "purify"), (True, "gpu"), (False, "gpu"), (True, "host")],
+                         ids=["cuda-graph-purify", "cuda-graph", "eager", "host-diag"])
 def test_batch_scf_and_gradients_match_single_molecule_runs(use_graph, diag):
     bases = _mols(10)
     out = batch.batch_rhf(bases, use_graph=use_graph, e_tol=1e-11, rms_tol=1e-9, diag=diag)
@@ -52,6 +52,40 @@ def test_batch_scf_and_gradients_match_single_molecule_runs(use_graph, diag):
             g = scf.rhf_gradient(b, r, e1)
         assert abs(out["energies"][m] - r.energy) < 1e-8
         assert np.max(np.abs(out["gradients"][m] - g)) < 1e-6
+
+
+def test_batched_purification_matches_the_eigh_projector():
+    """hfgpu_batch_purify_device: every molecule's projector onto its nocc lowest eigenvectors,
+    for random symmetric blocks of uneven size with a gap at nocc (padded like the SCF's Fock
+    batch), against numpy's eigh (1e-10), with each reported trace error below 1e-10."""
+    import torch
+    bases = _mols(9, seed=7)
+    be = batch.BatchEngine(bases)
+    nmol, nmax = len(bases), int(be.nbf.max())
+    rng = np.random.default_rng(6)
+    A = np.zeros((nmol, nmax, nmax))
+    P0 = np.zeros_like(A)
+    nocc = []
+    for k in range(nmol):
+        n = int(be.nbf[k])
+        no = max(1, n // 3)
+        nocc.append(no)
+        Q, _ = np.linalg.qr(rng.normal(size=(n, n)))
+        w = np.sort(np.concatenate([rng.uniform(-30.0, -0.4, no), rng.uniform(0.3, 5.0, n - no)]))
+        A[k, :n, :n] = 0.5 * ((Q * w) @ Q.T + ((Q * w) @ Q.T).T)
+        A[k, np.arange(n, nmax), np.arange(n, nmax)] = 1e3
+        P0[k, :n, :n] = Q[:, :no] @ Q[:, :no].T
+    dev = torch.device("cuda", 0)
+    Ad = torch.from_numpy(A).to(dev)
+    P = torch.full((nmol, nmax, nmax), 7.0, dtype=torch.float64, device=dev)
+    err = torch.zeros(nmol, dtype=torch.float64, device=dev)
+    nd = torch.tensor(nocc, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    be.purify(Ad, nd, P, err)
+    torch.cuda.synchronize()
+    assert float(err.max()) < 1e-10
+    assert np.max(np.abs(P.cpu().numpy() - P0)) < 1e-10  # zero outside each block too
+    be.close()
 
 
 def test_batched_eigensolver_matches_lapack():
