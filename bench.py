@@ -711,7 +711,8 @@ def run_ours(args, world, rank, local):
                          "close_s": rb["close_s"], "iterations": rb["iterations"],
                          "converged": int(rb["converged"].sum()), "cuda_graph": rb["graph"], "autotuned": rb["autotuned"],
                          "schedule": f"hfgpu_autotune on the batch, untimed ({t_tune:.2f} s incl. its set-up)",
-                         "jk_build_ms": rb["build_ms_mean"], "nbf_total": int(sum(b.nbf for b in bb))}
+                         "jk_build_ms": rb["build_ms_mean"], "nbf_total": int(sum(b.nbf for b in bb)),
+                         "density_step": rb["density"], "diag_fallback_iterations": rb["diag_fallbacks"]}
         # the same batch in mixed precision (FP32 quartets below the Schwarz bound 1e-4)
         torch.cuda.synchronize()
         tb = time.perf_counter()
