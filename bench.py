@@ -656,15 +656,22 @@ def run_ours(args, world, rank, local):
     # allows at the FP32:FP64 issue ratio of 2:1, and the time of the SCF outside the Fock builds,
     # which mixed precision does not touch.
     f32_flops = 0.0
+    per_class = {}
     for c in range(E.NUM_CLASSES):
         w = class_work[c]
         if w["screened"] > 0:
-            f32_flops += flops_c[c] * (w["screened"] - w["high_bound"]) / w["screened"]
+            share = (w["screened"] - w["high_bound"]) / w["screened"]
+            f32_flops += flops_c[c] * share
+            per_class["".join("spd"[w[k]] for k in ("la", "lb", "lc", "ld"))] = {
+                "flop_share_of_build": round(flops_c[c] / total_flops, 4),
+                "fp32_quartet_share": round(share, 4),
+                "bound_fp64_over_mixed": round(1.0 / ((1.0 - share) + 0.5 * share), 3)}
     f32 = f32_flops / total_flops
     t_build64 = sum(res.fock_times)
     t_buildmx = sum(res_mx.fock_times)
     line["mixed_accounting"] = {
         "fp32_flop_share_of_build": f32,
+        "per_class": per_class,
         "per_build_bound_fp64_over_mixed": 1.0 / ((1.0 - f32) + 0.5 * f32),
         "fp64_scf_builds_s": t_build64, "fp64_scf_other_s": scf_wall - t_build64,
         "mixed_scf_builds_s": t_buildmx, "mixed_scf_other_s": mixed_wall - t_buildmx,

@@ -2,6 +2,7 @@
 
     python -m hfscf_b200.profile_case jk   --workload 2 [--precision mixed] [--repeat 3]
     python -m hfscf_b200.profile_case grad --workload 3 [--repeat 1]
+    python -m hfscf_b200.profile_case hess --workload 4 [--repeat 1] [--hess-form 0|1]
     python -m hfscf_b200.profile_case jk   --workload 2 --variant 2   (every class in the staged form)
 
 Builds the named workload's basis (``molecules.workload``: 1 = H2O/cc-pVDZ,
@@ -37,7 +38,7 @@ def core_guess_density(bs, S, H):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("op", choices=("jk", "grad"))
+    ap.add_argument("op", choices=("jk", "grad", "hess"))
     ap.add_argument("--workload", type=int, default=2)
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
     ap.add_argument("--repeat", type=int, default=3)
@@ -47,6 +48,8 @@ def main(argv=None):
     ap.add_argument("--variant", type=int, choices=(0, 1, 2), default=None,
                     help="thread-form variant for every class (schedule column 3: 0 plain, 1 capped, "
                          "2 staged persistent)")
+    ap.add_argument("--hess-form", type=int, choices=(-1, 0, 1), default=-1,
+                    help="hess: -1 default per class, 0 one thread per quartet, 1 one block per quartet")
     a = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("profile_case needs a CUDA device")
@@ -74,10 +77,16 @@ def main(argv=None):
         J = torch.empty((n, n), dtype=torch.float64, device=dev)
         K = torch.empty((n, n), dtype=torch.float64, device=dev)
         g = torch.zeros((bs.natoms, 3), dtype=torch.float64, device=dev)
+        Hs = torch.zeros((3 * bs.natoms, 3 * bs.natoms), dtype=torch.float64, device=dev)
+        if a.op == "hess":
+            eng.set_hess_form(a.hess_form)
 
         def once():
             if a.op == "jk":
                 eng.jk_device(Dd.data_ptr(), 1, Dd.data_ptr(), J.data_ptr(), K.data_ptr(), prec)
+            elif a.op == "hess":
+                # two-electron Hessian of sum D (2J - K) at fixed D (RHF weights, as hfgpu_hess2e)
+                eng.hess2e_device(Dd.data_ptr(), 2.0, 1, Dd.data_ptr(), 1.0, Hs.data_ptr())
             else:
                 # RHF two-electron gradient of sum D (2J - K): cJ = 2, cK = 1 (as hfgpu_grad2e_backward)
                 eng.grad2e_device(Dd.data_ptr(), 2.0, 1, Dd.data_ptr(), 1.0, g.data_ptr(), prec)
