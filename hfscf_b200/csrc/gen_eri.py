@@ -1084,9 +1084,22 @@ static bool launch_hess_block(const GradArgs<double>& a, const HessOut& o, int p
     return false;
   }}
 }}
+// warp form: four quartets per 128-thread block, one warp each, every warp's tables in shared memory
+static bool launch_hess_warp(const GradArgs<double>& a, const HessOut& o, int pure, const int2* q, int nq,
+                             cudaStream_t s) {{
+  if (nq <= 0) return true;
+  if constexpr (4 * kSmAll <= kSmMax) {{
+    auto k = hess_block_kernel<{la}, {lb}, {lc}, {ld}, HessBlockTab{t}, false, 32>;
+    if (4 * kSmAll > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(4 * kSmAll));
+    k<<<(nq + 3) / 4, 128, 4 * kSmAll, s>>>(a, o, pure, q, nq);
+    return true;
+  }} else {{
+    return false;
+  }}
+}}
 extern const HessLaunchers hess_launchers_{t};
 const HessLaunchers hess_launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_hess, &hess_scratch_slots,
-                                          &launch_hess_block, &hess_block_global_slots}};
+                                          &launch_hess_block, &hess_block_global_slots, &launch_hess_warp}};
 }}  // namespace hfgpu
 """
 

@@ -231,13 +231,18 @@ __host__ __device__ constexpr int hess_block_shared_doubles(bool hs_global) {
   return Tab::NVSLOT + 1 + (hs_global ? 0 : Tab::NHSLOT + 1) + 3 * Tab::NCART + 45;
 }
 
+// NT = 128: one block per quartet; NT = 32: one warp per quartet, four quartets per 128-thread
+// block, each warp with its own shared-memory region (the small classes, whose levels hold a
+// few dozen ops), synchronised with __syncwarp.
 template <int LA, int LB, int LC, int LD, typename Tab, bool HS_GLOBAL, int NT = 128>
-__global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, HessOut o, int pure,
-                                                        const int2* __restrict__ quartets, int nq) {
+__global__ void __launch_bounds__(128) hess_block_kernel(GradArgs<double> a, HessOut o, int pure,
+                                                         const int2* __restrict__ quartets, int nq) {
+  static_assert(NT == 128 || (NT == 32 && !HS_GLOBAL), "threads per quartet");
   using R = double;
   extern __shared__ __align__(16) unsigned char hbsm[];
-  const int tid = threadIdx.x;
-  R* vs = reinterpret_cast<R*>(hbsm);
+  constexpr int GROUPS = 128 / NT;  // quartets per block
+  const int tid = threadIdx.x % NT, grp = threadIdx.x / NT;
+  R* vs = reinterpret_cast<R*>(hbsm) + (size_t)grp * hess_block_shared_doubles<Tab>(HS_GLOBAL);
   R* hs;
   R* W;
   if constexpr (HS_GLOBAL) {
@@ -252,7 +257,9 @@ __global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, Hess
   R* h45 = t1 + Tab::NCART;
   const int n3 = 3 * o.natoms;
   const int np = a.nparts > 1 ? a.nparts : 1, p0 = np > 1 ? a.part : 0;
-  for (int qi = blockIdx.x; qi < nq; qi += gridDim.x) {
+  for (int qb = blockIdx.x * GROUPS; qb < nq; qb += gridDim.x * GROUPS) {
+    const int qi = qb + grp;
+    if (qi >= nq) break;  // only a warp of an NT = 32 block gets here: its barriers are its own
     const int2 pq = quartets[(size_t)qi * np + p0];
     const PairInfo P = a.pairs[pq.x];
     const PairInfo Q = a.pairs[pq.y];
@@ -281,7 +288,7 @@ __global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, Hess
         }
         dstw[e] = s8 * w;
       }
-      __syncthreads();
+      group_sync<NT>();
     }
     if (pure) {
       R* bufs[2] = {t1, t0};
@@ -309,7 +316,7 @@ __global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, Hess
           }
           out[e] = v;
         }
-        __syncthreads();
+        group_sync<NT>();
         for (int q = 0; q < 4; ++q) dims[q] = nd[q];
         in = out;
       }
@@ -317,7 +324,7 @@ __global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, Hess
     for (int t = tid; t < Tab::NACC; t += NT) hs[t] = R(0);
     for (int t = tid; t < 45; t += NT) h45[t] = R(0);
     if (tid == 0) vs[Tab::NVSLOT] = R(0);
-    __syncthreads();
+    group_sync<NT>();
     const PrimPair<R>* bp = a.prims + P.prim_off;
     const PrimPair<R>* kp = a.prims + Q.prim_off;
     const R* eA = a.alpha_a + P.prim_off;
@@ -349,7 +356,7 @@ __global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, Hess
           for (int m = 0; m <= Tab::L; ++m)
             if (tid == m) vs[m] = F[m];
         }
-        __syncthreads();
+        group_sync<NT>();
         for (int l = 0; l < Tab::NVLEV; ++l) {
           const int e = __ldg(vl + l + 1);
           for (int oi = __ldg(vl + l) + tid; oi < e; oi += NT) {
@@ -371,7 +378,7 @@ __global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, Hess
             }
             vs[dst] = v;
           }
-          __syncthreads();
+          group_sync<NT>();
         }
         for (int t = tid; t < Tab::NACC; t += NT) {
           const int2 ac = __ldg(acc + t);
@@ -390,7 +397,7 @@ __global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, Hess
           }
           hs[t] += w * vs[ac.x];
         }
-        __syncthreads();
+        group_sync<NT>();
       }
     }
     // HRR levels; each ends with its contraction rows (sorted by output entry), taken by the
@@ -425,7 +432,7 @@ __global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, Hess
         }
         if (cur >= 0) atomicAdd(h45 + cur, sum);
       }
-      __syncthreads();
+      group_sync<NT>();
     }
     // the 12 x 12 block over centres A, B, C, D into the Hessian (D by translational invariance)
     if (tid < 9) {
@@ -443,6 +450,6 @@ __global__ void __launch_bounds__(NT) hess_block_kernel(GradArgs<double> a, Hess
         for (int Y = 0; Y < 4; ++Y)
           if (hx[X][Y] != 0.0) atomicAdd(o.hess + (size_t)(3 * at[X] + i) * n3 + 3 * at[Y] + j, hx[X][Y]);
     }
-    __syncthreads();
+    group_sync<NT>();
   }
 }

@@ -21,6 +21,9 @@ struct HessLaunchers {
   bool (*launch_block)(const GradArgs<double>&, const HessOut&, int pure, const int2* q, int nq, int grid,
                        cudaStream_t);
   int (*block_global_slots)();  // doubles of global scratch per block of the block form (0: none)
+  // warp form (hess_block_kernel with one warp per quartet, four per block); false when four
+  // quartets' tables do not fit one block's shared memory
+  bool (*launch_warp)(const GradArgs<double>&, const HessOut&, int pure, const int2* q, int nq, cudaStream_t);
 };
 
 extern const HessLaunchers* const kHessLaunchers[];

@@ -192,11 +192,11 @@ struct hfgpu_handle {
   int grad_form[21];
   unsigned grad_class_mask = ~0u;       // classes a gradient launches (autotuning runs one at a time)
   // Hessian form (hfgpu_set_hess_form): -1 by table size, 0 one thread per quartet, 1 one block
-  // per quartet wherever the class has the block form
+  // per quartet, 2 one warp per quartet (where the class's tables fit)
   int hess_form = -1;
   int purify_blocks = -1;               // co-resident blocks of the cooperative purification (0: not available)
   int purify_coop = 1;                  // hfgpu_set_purify_mode: 1 one cooperative launch, 0 two launches per step
-  int hess_cls_form[21];                // per class (hfgpu_autotune_hess): 0 thread, 1 block, -1 hess_form
+  int hess_cls_form[21];                // per class (hfgpu_autotune_hess): 0 thread, 1 block, 2 warp, -1 hess_form
   unsigned hess_class_mask = ~0u;       // classes a Hessian launches (autotuning runs one at a time)
 
   hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21), q_prims(21) {
@@ -1920,17 +1920,19 @@ static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     thr = std::min<long long>(thr, ((nq + 127) / 128) * 128);
     return std::max<long long>(128, thr / 128 * 128);
   };
-  // form per class: the block form (one block of 128 threads per quartet over levelised tables)
-  // for the classes whose one-thread tables are large or whose quartets are too few to fill the
-  // GPU with threads -- one thread would run a long chain of dependent table ops on global
-  // scratch -- the thread form for the small classes with many quartets
-  auto use_block = [&](int c) -> bool {
-    if (h->hess_cls_form[c] >= 0) return h->hess_cls_form[c] == 1;
-    if (h->hess_form == 0) return false;
-    if (h->hess_form == 1) return true;
-    return hfgpu::kHessLaunchers[c]->scratch_slots(h->pure) >= kHessBlockMinSlots ||
-           part_share(h, h->q_end[c] - h->q_beg[c]) <= kHessBlockMaxQuartets;
+  // form per class: 0 one thread per quartet on global scratch, 1 one block of 128 threads per
+  // quartet over levelised tables, 2 one warp per quartet over the same tables.  Default: the block
+  // form for the classes whose tables are large or whose quartets are too few to fill the GPU
+  // (one thread would run a long chain of dependent table ops on global scratch), the warp form
+  // for the small many-quartet classes (their levels hold a few dozen ops).
+  auto form_of = [&](int c) -> int {
+    if (h->hess_cls_form[c] >= 0) return h->hess_cls_form[c];
+    if (h->hess_form >= 0) return h->hess_form;
+    const bool big = hfgpu::kHessLaunchers[c]->scratch_slots(h->pure) >= kHessBlockMinSlots ||
+                     part_share(h, h->q_end[c] - h->q_beg[c]) <= kHessBlockMaxQuartets;
+    return big ? 1 : 2;
   };
+  auto use_block = [&](int c) -> bool { return form_of(c) >= 1; };
   // block-form grid: one block per quartet, or kHessBlockGrid blocks when the HRR slots live in
   // global scratch (one region per block)
   auto block_grid = [&](int c, long long nq) -> long long {
@@ -1979,11 +1981,15 @@ static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
         return fail(h, HFGPU_ERR_NOMEM, "Hessian scratch too small");
       gd.scratch = reinterpret_cast<double*>(h->d_scratch.as<unsigned char>() + off[st]);
       gd.scratch_threads = 0;
+      if (form_of(c) == 2 && L->launch_warp(gd, o, h->pure, q + h->q_beg[c], (int)nq, h->aux[st])) {
+        HF_CHECK_LAUNCH(h, "hess warp kernel");
+        continue;
+      }
       if (L->launch_block(gd, o, h->pure, q + h->q_beg[c], (int)nq, (int)grid, h->aux[st])) {
         HF_CHECK_LAUNCH(h, "hess block kernel");
         continue;
       }
-      if (h->hess_form == 1) return fail(h, HFGPU_ERR_UNSUPPORTED, "class without a Hessian block form");
+      if (h->hess_form >= 1) return fail(h, HFGPU_ERR_UNSUPPORTED, "class without a Hessian block form");
     }
     const int slots = L->scratch_slots(h->pure);
     const long long thr = threads_of(slots, nq);
@@ -1999,7 +2005,7 @@ static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
 }
 
 int hfgpu_set_hess_form(hfgpu_handle* h, int form) {
-  if (!h || form < -1 || form > 1) return HFGPU_ERR_INVALID;
+  if (!h || form < -1 || form > 2) return HFGPU_ERR_INVALID;
   h->hess_form = form;
   for (int c = 0; c < 21; ++c) h->hess_cls_form[c] = -1;
   return HFGPU_OK;
@@ -2008,7 +2014,7 @@ int hfgpu_set_hess_form(hfgpu_handle* h, int form) {
 int hfgpu_set_hess_forms(hfgpu_handle* h, const int* forms) {
   if (!h || !forms) return HFGPU_ERR_INVALID;
   for (int c = 0; c < hfgpu::kNumClasses; ++c)
-    if (forms[c] < -1 || forms[c] > 1) return HFGPU_ERR_INVALID;
+    if (forms[c] < -1 || forms[c] > 2) return HFGPU_ERR_INVALID;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) h->hess_cls_form[c] = forms[c];
   return HFGPU_OK;
 }
@@ -2513,8 +2519,8 @@ int hfgpu_set_grad_forms(hfgpu_handle* h, const int* forms) {
   return HFGPU_OK;
 }
 
-// Hessian form per class: each class alone, one thread per quartet against one block per
-// quartet, on RHF weights of the device density D; the faster is kept.
+// Hessian form per class: each class alone, one thread, one block or one warp per quartet, on RHF
+// weights of the device density D; the fastest is kept.
 int hfgpu_autotune_hess(hfgpu_handle* h, const double* D, int repeats, int* forms) {
   if (!h || !D) return HFGPU_ERR_INVALID;
   DeviceGuard dev_guard(h);
@@ -2553,7 +2559,7 @@ int hfgpu_autotune_hess(hfgpu_handle* h, const double* D, int repeats, int* form
     h->hess_class_mask = 1u << c;
     float best = 1e30f;
     int best_form = 0;
-    for (int form = 0; form < 2; ++form) {
+    for (int form = 0; form < 3; ++form) {
       h->hess_cls_form[c] = form;
       float ms = 0.f;
       if ((rc = tuner_time(h, hessian, repeats, e0, e1, restore.flush, &ms))) return rc;

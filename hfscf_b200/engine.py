@@ -383,7 +383,7 @@ class Engine:
         return H
 
     def set_hess_form(self, form: int):
-        """hfgpu_set_hess_form: -1 by table size (default), 0 thread per quartet, 1 block per quartet."""
+        """hfgpu_set_hess_form: -1 by table size (default), 0 thread, 1 block, 2 warp per quartet."""
         self._check(lib().hfgpu_set_hess_form(self.h, ctypes.c_int(form)))
 
     def autotune_hess(self, D_ptr, repeats=2):

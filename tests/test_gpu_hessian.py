@@ -54,14 +54,14 @@ def _ref_hessian(bs, D):
     return hc + he
 
 
-FORMS = [(-1, "default"), (0, "thread"), (1, "block")]
+FORMS = [(-1, "default"), (0, "thread"), (1, "block"), (2, "warp")]
 
 
 @pytest.mark.parametrize("form", [f for f, _ in FORMS], ids=[n for _, n in FORMS])
 @pytest.mark.parametrize("name,bs", MOLS, ids=[m[0] for m in MOLS])
 def test_hess2e_matches_reference(name, bs, form):
-    """Every launch form (one thread per quartet on global scratch, one block per quartet over
-    levelised tables, and the default mix of the two) against the reference."""
+    """Every launch form (one thread per quartet on global scratch, one block or one warp per
+    quartet over levelised tables, and the default mix) against the reference."""
     rng = np.random.default_rng(3)
     D = _sym(rng, bs.nbf)
     with E.Engine(bs) as eng:
