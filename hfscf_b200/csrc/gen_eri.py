@@ -793,10 +793,12 @@ def class_header(c):
     parts += [code_g, ""]
     mg["table"] = not straight
     # the op-table classes also get the warp-per-quartet form (measured faster than one thread
-    # per quartet on global scratch for every one of them; the straight-line classes stay threads)
-    # (the straight-line classes keep one thread per quartet: warp forms generated for those with
-    # more than 150 accumulators measured slower at n-octane and anthracene sizes, 29.6 against
-    # 25.7 ms and 216 against 189 ms per gradient)
+    # per quartet on global scratch for every one of them).  The straight-line classes keep one
+    # thread per quartet: warp forms generated for those with more than 150 accumulators measured
+    # slower at n-octane and anthracene sizes (29.6 against 25.7 ms and 216 against 189 ms per
+    # gradient), and with the block forms offered to the autotuner as well it kept the four-pass
+    # thread form for all but one of them (octane 17.9 -> 17.0 ms, anthracene 135 -> 121 ms, for
+    # 3-8x the tuning time)
     gwarp = not straight
     if gwarp:
         gwcode, gwmeta = gen_grad_warp(*c)

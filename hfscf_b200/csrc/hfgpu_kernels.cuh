@@ -990,9 +990,16 @@ __global__ void __launch_bounds__(128) quartet_warp_kernel(QuartetArgs<R> qa, co
 // the contractions against W all run lane-parallel out of shared memory, level by level
 // (generated tables, gen_eri.py gen_grad_warp).  One block per quartet, of one warp or four.
 // ---------------------------------------------------------------------------
+// t0 holds a pure weight block or an intermediate of its transform (NCART values), and at the end
+// the per-warp gradient sums of a multi-warp block (9 per warp, up to 8 warps): at least 72.
+template <typename Tab, typename R>
+__host__ __device__ constexpr int grad_warp_t0() {
+  return Tab::NCART > 72 ? Tab::NCART : 72;
+}
+
 template <typename Tab, typename R>
 __host__ __device__ constexpr int grad_warp_slots() {
-  return Tab::NVSLOT + 1 + Tab::NHSLOT + 1 + 3 * Tab::NCART;
+  return Tab::NVSLOT + 1 + Tab::NHSLOT + 1 + 2 * Tab::NCART + grad_warp_t0<Tab, R>();
 }
 
 // NT = 32: one warp per quartet; NT = 128 or 256: one block of four or eight warps per quartet
@@ -1010,7 +1017,7 @@ __global__ void __launch_bounds__(NT) grad_warp_kernel(GradArgs<R> a, int pure, 
   R* hs = vs + Tab::NVSLOT + 1;
   R* W = hs + Tab::NHSLOT + 1;
   R* t0 = W + Tab::NCART;
-  R* t1 = t0 + Tab::NCART;
+  R* t1 = t0 + grad_warp_t0<Tab, R>();
   const int2 pq = quartets[(size_t)qi * (a.nparts > 1 ? a.nparts : 1) + (a.nparts > 1 ? a.part : 0)];
   const PairInfo P = a.pairs[pq.x];
   const PairInfo Q = a.pairs[pq.y];
