@@ -6,7 +6,8 @@ Two ways to spread the two-electron path over ranks:
     collective; only the max-over-ranks of the timed region is reduced;
   * one molecule partitioned (hfgpu_set_partition): every rank computes every world-th
     quartet of each class list, and the partial two-electron terms are summed with one
-    all-reduce per build (n^2 doubles: G = 2J - K) or per gradient (natoms x 3), the
+    all-reduce per build (n^2 doubles: G = 2J - K), per gradient (natoms x 3) or per
+    two-electron Hessian (3 natoms x 3 natoms), the
     exchange step of the multi-GPU Fock build (the reference's build is one OpenMP loop on
     one host, hfscf_hf_solver.cpp:254-286).
 """
@@ -82,6 +83,14 @@ class ShardedFock:
         if self.device is not None:
             g = g.to(self.device)
         return allreduce_sum_(g).cpu().numpy()
+
+    def hess2e(self, D: np.ndarray, scale: float = 1.0) -> np.ndarray:
+        """Two-electron RHF Hessian (3 natoms x 3 natoms), summed over the ranks' parts: one
+        all-reduce of 9 natoms^2 doubles."""
+        Hm = torch.from_numpy(np.ascontiguousarray(self.engine.hess2e(D, scale)))
+        if self.device is not None:
+            Hm = Hm.to(self.device)
+        return allreduce_sum_(Hm).cpu().numpy()
 
     def close(self):
         self.engine.set_partition(0, 1)

@@ -86,6 +86,14 @@ class _PartEngine:
         w = (np.arange(g.size).reshape(g.shape) % self.nparts) == self.part
         return g * w
 
+    def hess2e(self, D, scale=1.0):
+        import numpy as np
+        import oracle
+        hc, he = oracle.ref_hess2e(self.bs, D)
+        Hm = scale * (hc + he)
+        w = (np.arange(Hm.size).reshape(Hm.shape) % self.nparts) == self.part
+        return Hm * w
+
     def one_electron_grad(self, D, Q, cD, cQ):
         import oracle
         return oracle.ref_onee_grad(self.bs, D, Q, cD, cQ)
@@ -108,15 +116,17 @@ def _sharded_worker(rank, world, port, q):
         fk = D.ShardedFock(_PartEngine(bs))
         res = scf.rhf(bs, fock=fk, H=T + V, S=S)
         g = D.sharded_rhf_gradient(bs, res, fk)
-        q.put((rank, res.energy, res.iterations, g))
+        h = fk.hess2e(res.D)
+        q.put((rank, res.energy, res.iterations, g, h))
     finally:
         dist.destroy_process_group()
 
 
 def test_partitioned_scf_and_gradient_sum_the_parts_over_two_gloo_ranks():
-    """One molecule's Fock build and two-electron gradient split over two ranks (each rank's
-    engine returns only its part), summed by ShardedFock's all-reduce: both ranks run the same
-    SCF and get the energy and gradient of the unpartitioned oracle run."""
+    """One molecule's Fock build, two-electron gradient and two-electron Hessian split over two
+    ranks (each rank's engine returns only its part), summed by ShardedFock's all-reduce: both
+    ranks run the same SCF and get the energy, gradient and Hessian of the unpartitioned oracle
+    run."""
     import numpy as np
     import oracle
     from hfscf_b200 import basis as B
@@ -140,7 +150,9 @@ def test_partitioned_scf_and_gradient_sum_the_parts_over_two_gloo_ranks():
     whole = _PartEngine(bs)
     ref = scf.rhf(bs, fock=lambda Dm, H: H + 2.0 * whole.jk(Dm, [Dm])[0] - whole.jk(Dm, [Dm])[1][0], H=T + V, S=S)
     gref = scf.rhf_gradient(bs, ref, whole)
-    for _, e, it, g in out:
+    href = whole.hess2e(ref.D)
+    for _, e, it, g, h in out:
         assert abs(e - ref.energy) < 1e-10
         assert it == ref.iterations
         assert np.max(np.abs(g - gref)) < 1e-10
+        assert np.max(np.abs(h - href)) < 1e-10  # the two-electron Hessian's parts summed too

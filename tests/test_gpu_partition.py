@@ -162,3 +162,22 @@ def test_fock_entry_points_are_refused_on_a_partitioned_handle_and_bad_partition
         F = eng.fock_rhf(D, H)  # usable again, whole build
         J, K = oracle.jk(oracle.eri_packed(bs), D)
         assert np.max(np.abs(F - (H + 2.0 * J - K))) < TOL_ORACLE
+
+
+@pytest.mark.parametrize("form", [-1, 0, 1, 2], ids=["default", "thread", "block", "warp"])
+def test_partitioned_hessian_sums_to_the_whole(form):
+    """The two-electron Hessian honours the partition: its parts, summed as an all-reduce of the
+    3 natoms x 3 natoms blocks would sum them, equal the whole Hessian (1e-11) in every form."""
+    Z, x = M.water_cluster(2, 2.9, np.random.default_rng(17), 0.1)
+    bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    D = _density(bs)
+    with E.Engine(bs, density_tol=0.0) as eng:
+        eng.set_hess_form(form)
+        H = eng.hess2e(D)
+        Hs = np.zeros_like(H)
+        for p in range(3):
+            eng.set_partition(p, 3)
+            Hs += eng.hess2e(D)
+        eng.set_partition(0, 1)
+    assert np.max(np.abs(Hs - H)) < TOL_SUM
+    assert np.max(np.abs(H)) > 1e-3
