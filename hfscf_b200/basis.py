@@ -137,24 +137,21 @@ def build_basis(name: str, Z, coords_bohr, pure: bool | None = None) -> Basis:
 
 
 def nuclear_repulsion(Z, coords) -> float:
+    """sum_{a > b} Z_a Z_b / |R_a - R_b| (all pairs at once)."""
     Z = np.asarray(Z, dtype=np.float64)
     c = np.asarray(coords, dtype=np.float64)
-    e = 0.0
-    for i in range(len(Z)):
-        for j in range(i):
-            e += Z[i] * Z[j] / np.linalg.norm(c[i] - c[j])
-    return float(e)
+    if len(Z) < 2:
+        return 0.0
+    i, j = np.tril_indices(len(Z), -1)
+    r = np.sqrt(((c[i] - c[j]) ** 2).sum(axis=1))
+    return float(np.sum(Z[i] * Z[j] / r))
 
 
 def nuclear_repulsion_gradient(Z, coords) -> np.ndarray:
+    """d/dR_a of the nuclear repulsion: -sum_{b != a} Z_a Z_b (R_a - R_b) / |R_a - R_b|^3."""
     Z = np.asarray(Z, dtype=np.float64)
     c = np.asarray(coords, dtype=np.float64)
-    g = np.zeros_like(c)
-    for a in range(len(Z)):
-        for b in range(len(Z)):
-            if a == b:
-                continue
-            d = c[a] - c[b]
-            r = np.linalg.norm(d)
-            g[a] -= Z[a] * Z[b] * d / r ** 3
-    return g
+    d = c[:, None, :] - c[None, :, :]
+    r = np.sqrt((d * d).sum(axis=2))
+    np.fill_diagonal(r, np.inf)
+    return -np.sum((Z[:, None] * Z[None, :] / r ** 3)[:, :, None] * d, axis=1)
