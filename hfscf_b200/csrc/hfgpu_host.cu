@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -468,10 +469,16 @@ int compute_schwarz(hfgpu_handle* h) {
 constexpr int kPrimWarpMinPrims = 16;  // primitive quartets per quartet for the primitive-split kernel
 constexpr int kBuckets = 18;           // Schwarz-bound decades of the quartet lists
 
+// Decade of a Schwarz bound: 0 for b >= 1, else the e >= 1 with b in [10^-e, 10^(1-e)) (the last
+// decade also takes everything smaller), by comparisons with the same powers of ten that bound the
+// decades on the device (kDecadeUpper), which is all the density-screened launches rely on.
 int bound_decade(double b) {
+  static const double lo[kBuckets] = {1.0,  1e-1,  1e-2,  1e-3,  1e-4,  1e-5,  1e-6,  1e-7,  1e-8,
+                                      1e-9, 1e-10, 1e-11, 1e-12, 1e-13, 1e-14, 1e-15, 1e-16, 1e-17};
   if (b >= 1.0) return 0;
-  const int e = (int)std::ceil(-std::log10(b));  // b in [10^-e, 10^(1-e))
-  return std::min(std::max(e, 1), kBuckets - 1);
+  int e = 1;
+  while (e < kBuckets - 1 && b < lo[e]) ++e;
+  return e;
 }
 
 // Screened unique quartets (P <= Q within a class; bra class >= ket class), per class.
@@ -563,6 +570,14 @@ int build_quartets(hfgpu_handle* h) {
   // primitive shape of a quartet: ket primitive pairs * shape_mul + bra primitive pairs
   int shape_mul = 1;
   for (int P = 0; P < (int)h->pairs.size(); ++P) shape_mul = std::max(shape_mul, h->pairs[P].nprim + 1);
+  // the pairs' Schwarz factors and primitive counts as plain arrays (the inner loop reads them
+  // for every candidate ket; PairInfo is 72 bytes)
+  std::vector<double> pq_s(h->pairs.size());
+  std::vector<int> pq_n(h->pairs.size());
+  for (size_t P = 0; P < h->pairs.size(); ++P) {
+    pq_s[P] = h->pairs[P].schwarz;
+    pq_n[P] = h->pairs[P].nprim;
+  }
   run_parallel((int)chunks.size(), threads, [&](int ci) {
     ListChunk& c = chunks[ci];
     const int cp = cls[c.cls].first, cq = cls[c.cls].second;
@@ -572,11 +587,12 @@ int build_quartets(hfgpu_handle* h) {
       int k0, ke;
       ket_range(cp, cq, P, k0, ke);
       for (int Q = k0; Q < ke; ++Q) {
-        const double b = qp * h->pairs[Q].schwarz;
+        const double b = qp * pq_s[Q];
         if (b < tol) continue;
-        c.prims += (long long)np * h->pairs[Q].nprim;
-        const int prod = np * h->pairs[Q].nprim;
-        const int shape = (int)std::min<long long>((long long)h->pairs[Q].nprim * shape_mul + np, kProdSpan - 1);
+        const int nq = pq_n[Q];
+        c.prims += (long long)np * nq;
+        const int prod = np * nq;
+        const int shape = (int)std::min<long long>((long long)nq * shape_mul + np, kProdSpan - 1);
         const int sg = (b >= mix ? 0 : 2) + (prod >= kPrimWarpMinPrims ? 0 : 1);
         c.q[sg].push_back(make_int2(P, Q));
         c.key[sg].push_back(bound_decade(b) * kProdSpan + shape);
@@ -594,7 +610,9 @@ int build_quartets(hfgpu_handle* h) {
     }
     seg_base[(size_t)i * 5 + 4] = total;
   }
-  std::vector<int2> all((size_t)total);
+  // left uninitialised: every slot is written by the scatter below (a zero-filled vector of the
+  // octane-to-batch sizes, 10^7-10^8 quartets, cost 0.15 s of single-threaded page touching)
+  std::unique_ptr<int2[]> all(new int2[(size_t)std::max<long long>(total, 1)]);
   h->bucket_end.assign((size_t)hfgpu::kNumClasses * 4 * kBuckets, 0);
   // phase 2: one stable counting sort per (class, segment) on (decade, count descending),
   // itself parallel over the class's chunks: (a) per-chunk key histograms, (b) per (class,
@@ -659,9 +677,10 @@ int build_quartets(hfgpu_handle* h) {
   }
   h->nquartets = total;
   const auto t1 = clk::now();
-  HF_CUDA(h, h->d_quart.ensure(sizeof(int2) * std::max<size_t>(all.size(), 1)));
-  if (!all.empty())
-    HF_CUDA(h, cudaMemcpyAsync(h->d_quart.p, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, h->stream));
+  HF_CUDA(h, h->d_quart.ensure(sizeof(int2) * (size_t)std::max<long long>(total, 1)));
+  if (total > 0)
+    HF_CUDA(h, cudaMemcpyAsync(h->d_quart.p, all.get(), sizeof(int2) * (size_t)total, cudaMemcpyHostToDevice,
+                               h->stream));
   {
     // launch table of the density-screened builds (see launch_counts_kernel)
     const int nslot = hfgpu::kNumClasses * 4;
