@@ -279,6 +279,20 @@ struct DeviceGuard {
   DeviceGuard& operator=(const DeviceGuard&) = delete;
 };
 
+// Runs f(0) ... f(ntask - 1) on up to max_threads threads (the caller's thread among them).
+template <typename F>
+void run_parallel(int ntask, int max_threads, F&& f) {
+  std::atomic<int> next{0};
+  auto work = [&]() {
+    for (int i = next++; i < ntask; i = next++) f(i);
+  };
+  const int nthr = std::max(1, std::min(ntask, max_threads));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+}
+
 // Primitive pairs of every canonical shell pair; pairs sorted by class, then by
 // primitive count (descending) so that quartet lists group equal loop lengths.
 int build_pairs(hfgpu_handle* h) {
@@ -308,83 +322,140 @@ int build_pairs(hfgpu_handle* h) {
       });
       h->cm_begin[(size_t)c * nm1 + m] = (int)(it - tmp.begin());
     }
-  // largest |Kp| and smallest p over all primitive pairs, for the primitive-pair cut
-  double kp_max = 0.0, p_min = 1e300;
-  for (const Tmp& t : tmp) {
+  // The primitive pairs are made on all host threads, in chunks of consecutive pairs: (1) the
+  // largest |Kp| and smallest p over all primitive pairs, for the primitive-pair cut, (2) the
+  // kept primitive pairs of every pair, (3) after a prefix sum, every pair's records at its offset.
+  // Same arithmetic and order as one pass over the pairs.
+  const int npairs = (int)tmp.size();
+  const int threads = npairs < 4096 ? 1 : (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nchunk = std::max(1, std::min(npairs, 8 * threads));
+  auto chunk_range = [&](int ci, int& x0, int& x1) {
+    x0 = (int)((long long)npairs * ci / nchunk);
+    x1 = (int)((long long)npairs * (ci + 1) / nchunk);
+  };
+  // K of primitive pair (i, j) of pair t (self pairs: (i, j) and (j, i) stored once, K doubled)
+  auto prim_k = [&](const Tmp& t, double R2, int i, int j, double& p) {
+    const double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
+    p = a1 + a2;
+    return std::exp(-a1 * a2 / p * R2) * h->coefs[h->prim_off[t.sa] + i] * h->coefs[h->prim_off[t.sb] + j] *
+           ((t.sa == t.sb && j > i) ? 2.0 : 1.0);
+  };
+  auto pair_r2 = [&](const Tmp& t) {
     const double* A = &h->xyz[3 * h->shell_atom[t.sa]];
     const double* B = &h->xyz[3 * h->shell_atom[t.sb]];
-    const double R2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
-    for (int i = 0; i < h->nprim[t.sa]; ++i)
-      for (int j = 0; j < h->nprim[t.sb]; ++j) {
-        const double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
-        const double p = a1 + a2;
-        const double fold = (t.sa == t.sb && i != j) ? 2.0 : 1.0;  // see the folding below
-        const double kp = fold * std::fabs(std::exp(-a1 * a2 / p * R2) * h->coefs[h->prim_off[t.sa] + i] *
-                                           h->coefs[h->prim_off[t.sb] + j]) * std::sqrt(PI_2_5) / p;
-        kp_max = std::max(kp_max, kp);
-        p_min = std::min(p_min, p);
-      }
+    return (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
+  };
+  std::vector<double> ck_max(nchunk, 0.0), cp_min(nchunk, 1e300);
+  run_parallel(nchunk, threads, [&](int ci) {
+    int x0, x1;
+    chunk_range(ci, x0, x1);
+    double km = 0.0, pm = 1e300;
+    for (int x = x0; x < x1; ++x) {
+      const Tmp& t = tmp[x];
+      const double R2 = pair_r2(t);
+      for (int i = 0; i < h->nprim[t.sa]; ++i)
+        for (int j = 0; j < h->nprim[t.sb]; ++j) {
+          const double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
+          const double p = a1 + a2;
+          const double fold = (t.sa == t.sb && i != j) ? 2.0 : 1.0;  // see the folding below
+          const double kp = fold * std::fabs(std::exp(-a1 * a2 / p * R2) * h->coefs[h->prim_off[t.sa] + i] *
+                                             h->coefs[h->prim_off[t.sb] + j]) * std::sqrt(PI_2_5) / p;
+          km = std::max(km, kp);
+          pm = std::min(pm, p);
+        }
+    }
+    ck_max[ci] = km;
+    cp_min[ci] = pm;
+  });
+  double kp_max = 0.0, p_min = 1e300;
+  for (int ci = 0; ci < nchunk; ++ci) {
+    kp_max = std::max(kp_max, ck_max[ci]);
+    p_min = std::min(p_min, cp_min[ci]);
   }
   const double kp_cut = kPrimQuartetCut * std::sqrt(2.0 * p_min) / std::max(kp_max, 1e-300);
-  h->pairs.assign(tmp.size(), PairInfo{});
-  std::vector<PrimPair<double>> pd;
-  std::vector<double> aa, ab;
-  pd.reserve(tmp.size() * 4);
-  for (int c = 0; c <= kPairClasses; ++c) h->class_begin[c] = (int)tmp.size();
-  for (size_t x = 0; x < tmp.size(); ++x) {
-    const Tmp& t = tmp[x];
-    h->class_begin[t.cls] = std::min(h->class_begin[t.cls], (int)x);
-    PairInfo& P = h->pairs[x];
-    P.sa = t.sa;
-    P.sb = t.sb;
-    P.fa = h->first[t.sa];
-    P.fb = h->first[t.sb];
-    P.cls = t.cls;
-    P.mol = t.mol;
-    P.atom_a = h->shell_atom[t.sa];
-    P.atom_b = h->shell_atom[t.sb];
-    const double* A = &h->xyz[3 * P.atom_a];
-    const double* B = &h->xyz[3 * P.atom_b];
-    P.ABx = A[0] - B[0];
-    P.ABy = A[1] - B[1];
-    P.ABz = A[2] - B[2];
-    const double R2 = P.ABx * P.ABx + P.ABy * P.ABy + P.ABz * P.ABz;
-    P.prim_off = (int)pd.size();
-    // A pair of a shell with itself has A = B, so primitive pairs (i, j) and (j, i) have the
-    // same p, P, PA and K: they are stored once, j >= i, with K doubled for j > i.  For the
-    // gradient both exponent weights become (a_i + a_j)/2: the A and B derivatives then
-    // have the right sum, which is all that reaches the atom the two centres share.
-    const bool self = t.sa == t.sb;
-    for (int i = 0; i < h->nprim[t.sa]; ++i)
-      for (int j = self ? i : 0; j < h->nprim[t.sb]; ++j) {
-        double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
-        const double c1 = h->coefs[h->prim_off[t.sa] + i], c2 = h->coefs[h->prim_off[t.sb] + j];
-        const double p = a1 + a2;
-        const double K = std::exp(-a1 * a2 / p * R2) * c1 * c2 * (self && j > i ? 2.0 : 1.0);
-        double eb2 = a2 * a2;  // the kinetic integral is quadratic in the ket exponent
-        if (self && j > i) {
-          eb2 = 0.5 * (a1 * a1 + a2 * a2);
-          a1 = a2 = 0.5 * p;
+  // (2) kept primitive pairs per pair
+  std::vector<int> kept(npairs + 1, 0);
+  run_parallel(nchunk, threads, [&](int ci) {
+    int x0, x1;
+    chunk_range(ci, x0, x1);
+    for (int x = x0; x < x1; ++x) {
+      const Tmp& t = tmp[x];
+      const double R2 = pair_r2(t);
+      const bool self = t.sa == t.sb;
+      int k = 0;
+      for (int i = 0; i < h->nprim[t.sa]; ++i)
+        for (int j = self ? i : 0; j < h->nprim[t.sb]; ++j) {
+          double p;
+          const double K = prim_k(t, R2, i, j, p);
+          if (!(std::fabs(K) * std::sqrt(PI_2_5) / p < kp_cut)) ++k;
         }
-        if (std::fabs(K) * std::sqrt(PI_2_5) / p < kp_cut) continue;
-        PrimPair<double> q;
-        q.p = p;
-        q.ip = 1.0 / p;
-        q.eb2 = eb2;
-        q.Px = (a1 * A[0] + a2 * B[0]) / p;
-        q.Py = (a1 * A[1] + a2 * B[1]) / p;
-        q.Pz = (a1 * A[2] + a2 * B[2]) / p;
-        q.PAx = q.Px - A[0];
-        q.PAy = q.Py - A[1];
-        q.PAz = q.Pz - A[2];
-        q.Kp = K * std::sqrt(PI_2_5) / p;
-        pd.push_back(q);
-        aa.push_back(a1);
-        ab.push_back(a2);
-      }
-    P.nprim = (int)pd.size() - P.prim_off;
-    P.schwarz = 0.0;
-  }
+      kept[x + 1] = k;
+    }
+  });
+  for (int x = 0; x < npairs; ++x) kept[x + 1] += kept[x];
+  h->pairs.assign(tmp.size(), PairInfo{});
+  std::vector<PrimPair<double>> pd((size_t)kept[npairs]);
+  std::vector<double> aa((size_t)kept[npairs]), ab((size_t)kept[npairs]);
+  for (int c = 0; c <= kPairClasses; ++c) h->class_begin[c] = (int)tmp.size();
+  for (size_t x = 0; x < tmp.size(); ++x) h->class_begin[tmp[x].cls] = std::min(h->class_begin[tmp[x].cls], (int)x);
+  // (3) the records
+  run_parallel(nchunk, threads, [&](int ci) {
+    int x0, x1;
+    chunk_range(ci, x0, x1);
+    for (int x = x0; x < x1; ++x) {
+      const Tmp& t = tmp[x];
+      PairInfo& P = h->pairs[x];
+      P.sa = t.sa;
+      P.sb = t.sb;
+      P.fa = h->first[t.sa];
+      P.fb = h->first[t.sb];
+      P.cls = t.cls;
+      P.mol = t.mol;
+      P.atom_a = h->shell_atom[t.sa];
+      P.atom_b = h->shell_atom[t.sb];
+      const double* A = &h->xyz[3 * P.atom_a];
+      const double* B = &h->xyz[3 * P.atom_b];
+      P.ABx = A[0] - B[0];
+      P.ABy = A[1] - B[1];
+      P.ABz = A[2] - B[2];
+      const double R2 = P.ABx * P.ABx + P.ABy * P.ABy + P.ABz * P.ABz;
+      P.prim_off = kept[x];
+      // A pair of a shell with itself has A = B, so primitive pairs (i, j) and (j, i) have the
+      // same p, P, PA and K: they are stored once, j >= i, with K doubled for j > i.  For the
+      // gradient both exponent weights become (a_i + a_j)/2: the A and B derivatives then
+      // have the right sum, which is all that reaches the atom the two centres share.
+      const bool self = t.sa == t.sb;
+      int o = kept[x];
+      for (int i = 0; i < h->nprim[t.sa]; ++i)
+        for (int j = self ? i : 0; j < h->nprim[t.sb]; ++j) {
+          double a1 = h->exps[h->prim_off[t.sa] + i], a2 = h->exps[h->prim_off[t.sb] + j];
+          double p;
+          const double K = prim_k(t, R2, i, j, p);
+          double eb2 = a2 * a2;  // the kinetic integral is quadratic in the ket exponent
+          if (self && j > i) {
+            eb2 = 0.5 * (a1 * a1 + a2 * a2);
+            a1 = a2 = 0.5 * p;
+          }
+          if (std::fabs(K) * std::sqrt(PI_2_5) / p < kp_cut) continue;
+          PrimPair<double>& q = pd[(size_t)o];
+          q.p = p;
+          q.ip = 1.0 / p;
+          q.eb2 = eb2;
+          q.Px = (a1 * A[0] + a2 * B[0]) / p;
+          q.Py = (a1 * A[1] + a2 * B[1]) / p;
+          q.Pz = (a1 * A[2] + a2 * B[2]) / p;
+          q.PAx = q.Px - A[0];
+          q.PAy = q.Py - A[1];
+          q.PAz = q.Pz - A[2];
+          q.Kp = K * std::sqrt(PI_2_5) / p;
+          aa[(size_t)o] = a1;
+          ab[(size_t)o] = a2;
+          ++o;
+        }
+      P.nprim = o - kept[x];
+      P.schwarz = 0.0;
+    }
+  });
   for (int c = kPairClasses - 1; c >= 0; --c)
     if (h->class_begin[c] > h->class_begin[c + 1]) h->class_begin[c] = h->class_begin[c + 1];
   h->nprimpairs = (int)pd.size();
@@ -506,20 +577,6 @@ struct ListChunk {
   int maxprod[4] = {0, 0, 0, 0};
   long long prims = 0;          // primitive quartets of the survivors
 };
-
-// Runs f(0) ... f(ntask - 1) on up to max_threads threads (the caller's thread among them).
-template <typename F>
-void run_parallel(int ntask, int max_threads, F&& f) {
-  std::atomic<int> next{0};
-  auto work = [&]() {
-    for (int i = next++; i < ntask; i = next++) f(i);
-  };
-  const int nthr = std::max(1, std::min(ntask, max_threads));
-  std::vector<std::thread> pool;
-  for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
-  work();
-  for (auto& t : pool) t.join();
-}
 
 int build_quartets(hfgpu_handle* h) {
   using clk = std::chrono::steady_clock;
