@@ -169,7 +169,7 @@ class _Layout:
 
 def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-10, rms_tol=1e-8,
               max_iter=60, use_graph=True, gradient=True, autotune=False, diag="purify", diis_range=5,
-              schedule=None):
+              schedule=None, freeze_converged=False):
     """Converged RHF energies (and gradients) of every molecule of the batch.  ``diag``:
     "purify" (default) takes every molecule's density from one launch of the batched
     trace-correcting purification (hfgpu_batch_purify_device, molecules of up to 116 functions),
@@ -180,7 +180,12 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     before the graph is captured (off by default: for 512 small molecules it cost 2.4 s and
     bought nothing over the default schedule).  ``schedule``: a launch schedule to use instead
     (e.g. one the autotuner returned for the same batch in an earlier, untimed run); the result
-    dict's "schedule" is the schedule the run used."""
+    dict's "schedule" is the schedule the run used.  ``freeze_converged``: a molecule that has
+    met the convergence test stops iterating, as its own SCF would (its density and energy are
+    kept, its quartets are skipped by the density screening of the later builds); without it
+    every molecule iterates until the last one converges (the default: the frozen molecules' quartets
+    are still launched and skipped one by one, so freezing saved no time on the 512-molecule
+    batch, 0.64 against 0.65 s of SCF, and moved no energy by more than 3e-13 Eh)."""
     dev = torch.device("cuda", device)
     t0 = time.perf_counter()
     stages = {}
@@ -321,7 +326,12 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     t1 = time.perf_counter()
     while it < max_iter:
         it += 1
-        Dblk.copy_(lay.to_block(D))
+        if freeze_converged and it > 1:
+            # a converged molecule stops, as its own SCF would: its block of the density is zeroed
+            # for the build (density screening then skips its quartets) and its D is kept
+            Dblk.copy_(lay.to_block(D * (~converged).to(D.dtype)[:, None, None]))
+        else:
+            Dblk.copy_(lay.to_block(D))
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         if graph is not None:
@@ -358,9 +368,16 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
             rhs[:, m] = -1.0
             c = torch.linalg.solve(B, rhs)[:, :m]
             F = torch.einsum("bk,bkij->bij", c, hF)
+        D_prev = D
         D = density(F)
         E = ((D * (H + F)).sum(dim=(1, 2)) - PAD_DIAG * 0)  # padded entries of D are zero
         conv = (rms < rms_tol) & ((E - E_prev).abs() < e_tol)
+        if freeze_converged:
+            # molecules converged at an earlier iteration keep their density and energy (their
+            # F of this iteration was built from a zero density block and is not used)
+            D = torch.where(converged[:, None, None], D_prev, D)
+            E = torch.where(converged, E_prev, E)
+            conv = conv | converged
         if diag == "purify":
             # one host read per iteration: whether every molecule converged, and whether some
             # molecule's purification did not (then this iteration diagonalises instead)
@@ -370,6 +387,10 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
                 D = density_gpu(F)
                 E = (D * (H + F)).sum(dim=(1, 2))
                 conv = (rms < rms_tol) & ((E - E_prev).abs() < e_tol)
+                if freeze_converged:
+                    D = torch.where(converged[:, None, None], D_prev, D)
+                    E = torch.where(converged, E_prev, E)
+                    conv = conv | converged
                 done = bool((converged | conv).all())
             else:
                 done = bool(flags[1])

@@ -40,11 +40,12 @@ def test_batch_jk_matches_single_molecule_engine():
     be.close()
 
 
-@pytest.mark.parametrize("use_graph,diag", [(True, "purify"), (True, "gpu"), (False, "gpu"), (True, "host")],
-                         ids=["cuda-graph-purify", "cuda-graph", "eager", "host-diag"])
-def test_batch_scf_and_gradients_match_single_molecule_runs(use_graph, diag):
+@pytest.mark.parametrize("use_graph,diag,freeze", [(True, "purify", False), (True, "purify", True),
+                                                   (True, "gpu", False), (False, "gpu", False), (True, "host", False)],
+                         ids=["cuda-graph-purify", "cuda-graph-purify-freeze", "cuda-graph", "eager", "host-diag"])
+def test_batch_scf_and_gradients_match_single_molecule_runs(use_graph, diag, freeze):
     bases = _mols(10)
-    out = batch.batch_rhf(bases, use_graph=use_graph, e_tol=1e-11, rms_tol=1e-9, diag=diag)
+    out = batch.batch_rhf(bases, use_graph=use_graph, e_tol=1e-11, rms_tol=1e-9, diag=diag, freeze_converged=freeze)
     assert out["converged"].all()
     for m, b in enumerate(bases):
         with E.Engine(b) as e1:
