@@ -167,9 +167,31 @@ class _Layout:
         return out
 
 
+def batch_sad_guess(bases: list[Basis], nmax: int) -> np.ndarray:
+    """SAD guess of every molecule, padded to nmax (the reference's default guess,
+    Mol::hf_solver::get_sad_guess, src/scfsolver/hfscf_hf_solver.cpp:478-553): the atomic UHF of
+    each (basis set, element) pair runs once (scf.sad_atom_density on a GPU engine of that atom's
+    shells) and its spin-averaged density is copied onto every atom of that element in every
+    molecule with that basis set."""
+    from . import scf as _scf
+    cache = {}
+    D = np.zeros((len(bases), nmax, nmax))
+    for k, b in enumerate(bases):
+        bf_atom = b.bf_atom()
+        for a, Zc in enumerate(b.Z):
+            key = (b.name, bool(b.pure), int(Zc))
+            if key not in cache:
+                with eng.Engine(_scf.atom_basis(b, a)) as e:
+                    S, T, V = e.one_electron()
+                    cache[key] = _scf.sad_atom_density(int(Zc), S, T, V, lambda DJ, DKs: e.jk(DJ, DKs))
+            f = np.nonzero(bf_atom == a)[0]
+            D[k, f[0]:f[-1] + 1, f[0]:f[-1] + 1] = cache[key]
+    return D
+
+
 def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-10, rms_tol=1e-8,
               max_iter=60, use_graph=True, gradient=True, autotune=False, diag="purify", diis_range=5,
-              schedule=None, freeze_converged=False):
+              schedule=None, freeze_converged=False, guess="sad"):
     """Converged RHF energies (and gradients) of every molecule of the batch.  ``diag``:
     "purify" (default) takes every molecule's density from one launch of the batched
     trace-correcting purification (hfgpu_batch_purify_device, molecules of up to 116 functions),
@@ -180,7 +202,9 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
     before the graph is captured (off by default: for 512 small molecules it cost 2.4 s and
     bought nothing over the default schedule).  ``schedule``: a launch schedule to use instead
     (e.g. one the autotuner returned for the same batch in an earlier, untimed run); the result
-    dict's "schedule" is the schedule the run used.  ``freeze_converged``: a molecule that has
+    dict's "schedule" is the schedule the run used.  ``guess``: "sad" (default, the
+    reference's default: superposition of atomic densities, batch_sad_guess) or "core" (the
+    orbitals of the core Hamiltonian).  ``freeze_converged``: a molecule that has
     met the convergence test stops iterating, as its own SCF would (its density and energy are
     kept, its quartets are skipped by the density screening of the later builds); without it
     every molecule iterates until the last one converges (the default: the frozen molecules' quartets
@@ -278,10 +302,13 @@ def batch_rhf(bases: list[Basis], device: int = 0, precision=eng.FP64, e_tol=1e-
         list(pool.map(one, range(nmol)))
         return lay.to_pad(torch.from_numpy(Dh).to(dev))
 
-    D = density(H)
-    if diag == "purify" and bool((perr >= PURIFY_TOL).any()):
-        D = density_gpu(H)
-        fallbacks[0] += 1
+    if guess == "sad":
+        D = torch.from_numpy(batch_sad_guess(bases, nmax)).to(dev)
+    else:
+        D = density(H)
+        if diag == "purify" and bool((perr >= PURIFY_TOL).any()):
+            D = density_gpu(H)
+            fallbacks[0] += 1
     Dblk = lay.to_block(D).contiguous()
     Jblk = torch.zeros_like(Dblk)
     Kblk = torch.zeros_like(Dblk)
