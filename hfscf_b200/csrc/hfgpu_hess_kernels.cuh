@@ -6,11 +6,14 @@
 // Erios::compute_contracted_shell_quartet_deriv2_qq / _pq (src/integrals/hfscf_oserideriv2qq.cpp:28-853,
 // hfscf_oserideriv2pq.cpp:23-891) and Mol::scf_hessian::calc_scf_hessian_tei
 // (src/hessian/hfscf_hessian_ints.cpp:20-303), which store six packed derivative tensors per
-// direction pair and then contract them once per atom pair.  Here nothing is stored: one thread
-// per unique shell quartet runs the class's generated op tables (gen_eri.py gen_hess_table) on
-// thread-interleaved global scratch, contracts every shifted integral with W on the fly and adds
-// the quartet's 12 x 12 block (centres A, B, C, D by x, y, z; D from translational invariance)
-// into the 3 natoms x 3 natoms Hessian.
+// direction pair and then contract them once per atom pair.  Here nothing is stored: per unique
+// shell quartet the class's generated op tables run the VRR two orders higher, the HRR of ten
+// exponent-weighted sets and the contraction of every shifted integral with W, and the quartet's
+// 12 x 12 block (centres A, B, C, D by x, y, z; D from translational invariance) is added into
+// the 3 natoms x 3 natoms Hessian.  Three forms: hess_kernel, one thread per quartet on
+// thread-interleaved global scratch (gen_eri.py gen_hess_table); hess_block_kernel with one
+// block of 128 threads or one warp per quartet over levelised tables in shared memory
+// (gen_hess_block).
 #pragma once
 #include "hfgpu_kernels.cuh"
 
