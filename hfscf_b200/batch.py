@@ -177,15 +177,15 @@ def batch_sad_guess(bases: list[Basis], nmax: int) -> np.ndarray:
     cache = {}
     D = np.zeros((len(bases), nmax, nmax))
     for k, b in enumerate(bases):
-        bf_atom = b.bf_atom()
-        for a, Zc in enumerate(b.Z):
+        # an atom's functions are contiguous, atoms in order
+        off = np.concatenate([[0], np.cumsum(np.bincount(b.bf_atom(), minlength=len(b.Z)))])
+        for a, Zc in enumerate(b.Z.tolist()):
             key = (b.name, bool(b.pure), int(Zc))
             if key not in cache:
                 with eng.Engine(_scf.atom_basis(b, a)) as e:
                     S, T, V = e.one_electron()
                     cache[key] = _scf.sad_atom_density(int(Zc), S, T, V, lambda DJ, DKs: e.jk(DJ, DKs))
-            f = np.nonzero(bf_atom == a)[0]
-            D[k, f[0]:f[-1] + 1, f[0]:f[-1] + 1] = cache[key]
+            D[k, off[a]:off[a + 1], off[a]:off[a + 1]] = cache[key]
     return D
 
 
