@@ -108,6 +108,7 @@ class Engine:
         if grad_max_blocks is not None:
             o.reserved[1] = grad_max_blocks
         self._opts = o
+        self.stream_ptr = None  # the handle's own stream until set_stream
         h = ctypes.c_void_p()
         self._check(lib().hfgpu_create(ctypes.byref(self._bv.s), ctypes.byref(o), ctypes.byref(h)), None)
         self.h = h
@@ -199,6 +200,7 @@ class Engine:
     # --- device-pointer calls (torch tensors or raw addresses) -----------------
     def set_stream(self, stream_ptr: int | None):
         self._check(lib().hfgpu_set_stream(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+        self.stream_ptr = stream_ptr or None
 
     def jk_device(self, DJ_ptr, nK, DK_ptr, J_ptr, K_ptr, precision=FP64):
         self._check(lib().hfgpu_jk_device(self.h, ctypes.c_void_p(DJ_ptr), ctypes.c_int(nK), ctypes.c_void_p(DK_ptr),

@@ -436,11 +436,42 @@ def rhf_gradient(basis: Basis, res: ScfResult, engine, precision=eng.FP64):
     """Full RHF gradient (natoms x 3), as Mol::scf_gradient::calc_scf_gradient_rhf
     (src/gradient/hfscf_grad_rhf.cpp:7-178) assembles it."""
     D, F = res.D, res.F
+    if isinstance(engine, eng.Engine):
+        return _rhf_gradient_device(basis, D, F, engine, precision)
     Q = D @ F @ D
     g = engine.grad2e(D, 1.0, precision)
     g += engine.one_electron_grad(D, Q, 2.0, -2.0)
     g += nuclear_repulsion_gradient(basis.Z, basis.coords)
     return g
+
+
+def _rhf_gradient_device(basis: Basis, D, F, engine, precision):
+    """rhf_gradient on the engine's GPU: Q = D F D there, and the two-electron term
+    (hfgpu_grad2e_device, RHF weights) and the one-electron term (hfgpu_one_electron_grad_device)
+    on two streams at once, so the one-electron kernel runs beside the tail of the two-electron
+    classes; one host read of the summed gradient."""
+    import torch
+    dev = torch.device("cuda", engine._opts.device)
+    prev = engine.stream_ptr
+    s2, s1 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    Dd = torch.from_numpy(np.ascontiguousarray(D)).to(dev)
+    Fd = torch.from_numpy(np.ascontiguousarray(F)).to(dev)
+    Qd = (Dd @ Fd @ Dd).contiguous()
+    g2 = torch.zeros((basis.natoms, 3), dtype=torch.float64, device=dev)
+    g1 = torch.zeros_like(g2)
+    torch.cuda.synchronize(dev)  # inputs in place before either stream starts
+    try:
+        engine.set_stream(s2.cuda_stream)
+        engine.grad2e_device(Dd.data_ptr(), 2.0, 1, Dd.data_ptr(), 1.0, g2.data_ptr(), precision)
+        engine.set_stream(s1.cuda_stream)
+        engine.one_electron_grad_device(Dd.data_ptr(), Qd.data_ptr(), 2.0, -2.0, g1.data_ptr())
+        torch.cuda.synchronize(dev)
+    finally:
+        engine.set_stream(prev)
+    g = (g2 + g1).cpu().numpy()
+    if not np.all(np.isfinite(g)):
+        raise eng.HfgpuError(5, "non-finite gradient")
+    return g + nuclear_repulsion_gradient(basis.Z, basis.coords)
 
 
 def uhf(basis: Basis, engine, *, multiplicity=1, e_tol=1e-10, rms_tol=1e-8, diis_range=5, max_iter=100,
