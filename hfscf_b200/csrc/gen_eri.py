@@ -640,40 +640,48 @@ def gen_grad_class(la, lb, lc, ld):
 GRAD_SETS = ("U", "A", "B", "C")
 
 
-def gen_grad_class_pass(la, lb, lc, ld, pset):
-    """The part of gen_grad_class that one accumulator set carries: the VRR (one order higher)
-    of the set's targets only, the set's accumulation (weight 1, 2 alpha_a, 2 alpha_b or
-    2 alpha_c), its HRR, and the gradient terms that read it -- for A, B, C the
-    2 alpha (a+1_i b|cd)-type terms of that centre; for U the -a_i (a-1_i b|cd)-type terms of all
-    three centres.  The four passes add up to the whole gradient; each keeps about a quarter
-    of the accumulators of the one-pass form, at the price of recomputing the shared part of
-    the recurrence."""
+def gen_grad_class_pass(la, lb, lc, ld, psets):
+    """The part of gen_grad_class that some of the accumulator sets carry (psets: one set name or
+    a tuple of them): the VRR (one order higher) of those sets' targets only, their accumulation
+    (weight 1, 2 alpha_a, 2 alpha_b or 2 alpha_c), their HRR, and the gradient terms that read
+    them -- for A, B, C the 2 alpha (a+1_i b|cd)-type terms of that centre; for U the
+    -a_i (a-1_i b|cd)-type terms of all three centres.  Passes whose sets cover U, A, B, C once
+    add up to the whole gradient; each keeps a share of the accumulators of the one-pass form, at
+    the price of recomputing the shared part of the recurrence."""
+    if isinstance(psets, str):
+        psets = (psets,)
     L = la + lb + lc + ld + 1
     em = Emitter("      ")
     vrr = VRR(em)
-    order = grad_sets(la, lb, lc, ld)[pset]
-    vals = {t: vrr.get(t[0], t[1], 0) for t in order}
+    allsets = grad_sets(la, lb, lc, ld)
+    idx, adds_src, nacc = {}, [], 0
+    for k in psets:
+        for t in allsets[k]:
+            idx[(k, t)] = nacc
+            adds_src.append((k, t))
+            nacc += 1
+    targets = sorted({t for _, t in adds_src}, key=lambda t: (sum(t[0]), cidx(t[0]), sum(t[1]), cidx(t[1])))
+    vals = {t: vrr.get(t[0], t[1], 0) for t in targets}
     prim_body = list(em.lines)
-    idx = {t: i for i, t in enumerate(order)}
-    nacc = len(order)
     em2 = Emitter("  ")
-    hr = HRR(em2, lambda e, f: f"acc[{idx[(e, f)]}]", prefix=f"h{pset}")
+    hr = {k: HRR(em2, (lambda kk: (lambda e, f: f"acc[{idx[(kk, (e, f))]}]"))(k), prefix=f"h{k}") for k in psets}
     gt = grad_terms(la, lb, lc, ld)
     outs = {}
     for (cen, dr), items in gt.items():
         terms = []
         for wi, tl in items:
             for coef, st, a, b, c, d in tl:
-                if st != pset:
+                if st not in psets:
                     continue
-                v = hr.bra(a, b, c, d)
+                v = hr[st].bra(a, b, c, d)
                 terms.append(f"W[{wi}] * {v}" if coef == 1 else f"{lit(coef)} * W[{wi}] * {v}")
         outs[(cen, dr)] = terms
     for (cen, dr), terms in outs.items():
         em2.emit(f"g{cen}[{dr}] = " + (" + ".join(terms) if terms else "R(0)") + ";", 3 * len(terms))
-    wname = {"U": None, "A": "wa", "B": "wb", "C": "wc"}[pset]
-    fn = f"grad_{la}{lb}{lc}{ld}_{pset}"
-    s = [f"// adjoint gradient of ({'spdf'[la]}{'spdf'[lb]}|{'spdf'[lc]}{'spdf'[ld]}), set {pset} only: {nacc} "
+    wname = {"U": None, "A": "wa", "B": "wb", "C": "wc"}
+    tag_sets = "".join(psets)
+    fn = f"grad_{la}{lb}{lc}{ld}_{tag_sets}"
+    s = [f"// adjoint gradient of ({'spdf'[la]}{'spdf'[lb]}|{'spdf'[lc]}{'spdf'[ld]}), sets {tag_sets} only: {nacc} "
          f"accumulators, {len(vrr.memo)} VRR values"]
     s.append("template <typename R>")
     s.append(f"__device__ __forceinline__ void {fn}({GRAD_SIG}) {{")
@@ -693,8 +701,8 @@ def gen_grad_class_pass(la, lb, lc, ld, pset):
     s.append(PRIM_HEADER.rstrip("\n"))
     s.append(f"      R F[{L + 1}];")
     s.append(f"      boys.template eval<{L}>(T, pre, F);")
-    adds = [(vals[t], f"      acc[{idx[t]}] += {vals[t]};" if wname is None else
-             f"      acc[{idx[t]}] += {wname} * {vals[t]};") for t in order]
+    adds = [(vals[t], f"      acc[{idx[(k, t)]}] += {vals[t]};" if wname[k] is None else
+             f"      acc[{idx[(k, t)]}] += {wname[k]} * {vals[t]};") for k, t in adds_src]
     s += interleave_accumulation(prim_body, adds)
     s.append("    }")
     s.append("  }")
@@ -716,6 +724,7 @@ def classes():
 
 GRAD_STRAIGHT_MAX_VRR = 900   # larger gradient classes run in table mode
 GRAD_SPLIT_MIN_ACC = 150      # straight-line gradient classes with this many accumulators run as 4 passes
+GRAD_PAIR_MAX_ACC = 160       # ... or as 2 passes of two sets each when both halves stay below this
 
 
 def class_args_sig():
@@ -840,8 +849,16 @@ def class_header(c):
     parts.append("  template <typename R>")
     parts.append(f"  static __device__ __forceinline__ void from_pure(const R* __restrict__ in, R* __restrict__ out) {{ from_pure_{t}<R>(in, out); }}")
     # the straight-line classes whose one-pass accumulators spill run as four passes, one
-    # accumulator set each (gen_grad_class_pass)
+    # accumulator set each (gen_grad_class_pass), or as two passes (sets U and A, sets B and C)
+    # when each half stays below GRAD_PAIR_MAX_ACC accumulators: the recurrence is then
+    # recomputed once instead of three times
     npass = 4 if straight and mg["accumulators"] >= GRAD_SPLIT_MIN_ACC else 1
+    pass_sets = [(ps,) for ps in GRAD_SETS]
+    if npass == 4:
+        nset = {k: len(v) for k, v in grad_sets(*c).items()}
+        if max(nset["U"] + nset["A"], nset["B"] + nset["C"]) < GRAD_PAIR_MAX_ACC:
+            npass = 2
+            pass_sets = [("U", "A"), ("B", "C")]
     mg["passes"] = npass
     parts.append(f"  static constexpr int kGradPasses = {npass};")
     if straight:
@@ -849,16 +866,16 @@ def class_header(c):
         parts.append(f"  static __device__ __forceinline__ void grad({GRAD_SIG}) {{ grad_{t}<R>({GRAD_ARGS}); }}")
     if npass > 1:
         pcodes = []
-        for pi, ps in enumerate(GRAD_SETS):
+        for pi, ps in enumerate(pass_sets):
             pcode, pm = gen_grad_class_pass(la, lb, lc, ld, ps)
             pcodes += [pcode, ""]
-            mg[f"pass_{ps}"] = pm
+            mg["pass_" + "".join(ps)] = pm
         at = parts.index("template <>")  # the pass functions go before the ClassCode specialisation
         parts[at:at] = pcodes
         parts.append("  template <typename R, int PASS>")
         parts.append(f"  static __device__ __forceinline__ void grad_pass({GRAD_SIG}) {{")
-        for pi, ps in enumerate(GRAD_SETS):
-            parts.append(f"    if constexpr (PASS == {pi}) grad_{t}_{ps}<R>({GRAD_ARGS});")
+        for pi, ps in enumerate(pass_sets):
+            parts.append(f"    if constexpr (PASS == {pi}) grad_{t}_{''.join(ps)}<R>({GRAD_ARGS});")
         parts.append("  }")
     parts.append("};")
     return "\n".join(parts) + "\n", m, mg
@@ -967,6 +984,10 @@ static void launch_grad(const GradArgs<R>& a, int pure, const int2* q, int nq, i
     grad_kernel<{la}, {lb}, {lc}, {ld}, R, 1><<<grid, 128, sm, s>>>(a, pure, q, nq);
     grad_kernel<{la}, {lb}, {lc}, {ld}, R, 2><<<grid, 128, sm, s>>>(a, pure, q, nq);
     grad_kernel<{la}, {lb}, {lc}, {ld}, R, 3><<<grid, 128, sm, s>>>(a, pure, q, nq);
+  }} else if constexpr (ClassCode<{la}, {lb}, {lc}, {ld}>::kGradPasses == 2) {{
+    // one launch per pair of accumulator sets (U with A, B with C)
+    grad_kernel<{la}, {lb}, {lc}, {ld}, R, 0><<<grid, 128, sm, s>>>(a, pure, q, nq);
+    grad_kernel<{la}, {lb}, {lc}, {ld}, R, 1><<<grid, 128, sm, s>>>(a, pure, q, nq);
   }} else {{
     grad_kernel<{la}, {lb}, {lc}, {ld}, R><<<grid, 128, sm, s>>>(a, pure, q, nq);
   }}

@@ -582,7 +582,8 @@ __device__ __forceinline__ void grad_weights(const double* __restrict__ DJ, doub
 }
 
 // PASS < 0: the whole gradient of the quartet; PASS = 0..3: the part that accumulator set
-// U, A, B or C carries (classes generated with kGradPasses = 4 run one launch per pass).
+// U, A, B or C carries (classes generated with kGradPasses = 4 run one launch per pass); for
+// kGradPasses = 2, PASS = 0, 1: the part that sets U and A, or B and C, carry.
 template <int LA, int LB, int LC, int LD, typename R, bool PURE, int PASS = -1>
 __device__ __forceinline__ void grad_quartet(const GradArgs<R>& a, int tid, const int2 pq, double* gout) {
   using Dm = BlockDims<LA, LB, LC, LD, PURE>;
