@@ -705,11 +705,22 @@ def run_ours(args, world, rank, local):
         tuned_sched = BT.batch_rhf(bb, device=local, autotune=True, gradient=False, max_iter=2)["schedule"]
         t_tune = time.perf_counter() - t_tune
         torch.cuda.set_stream(stream)
-        torch.cuda.synchronize()
-        tb = time.perf_counter()
-        rb = BT.batch_rhf(bb, device=local, schedule=tuned_sched)
-        wall = DI.max_over_ranks(time.perf_counter() - tb, dev)
-        torch.cuda.set_stream(stream)
+
+        def timed_batch(**kw):
+            """Three whole runs (set-up, SCF, gradients; each wall-clock, max over ranks); the run of
+            median wall time is reported, with all three walls (a run's host-side set-up varied
+            from 0.4 to 1.2 s between otherwise equal runs)."""
+            runs = []
+            for _ in range(3):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                r = BT.batch_rhf(bb, device=local, schedule=tuned_sched, **kw)
+                runs.append((DI.max_over_ranks(time.perf_counter() - t0, dev), r))
+                torch.cuda.set_stream(stream)
+            runs.sort(key=lambda x: x[0])
+            return runs[1][0], runs[1][1], [round(w, 4) for w, _ in runs]
+
+        wall, rb, walls = timed_batch()
         line["batch"] = {"workload": "512 seeded molecules ((H2O)1-6, CH4, C2H6, NH3; STO-3G or 6-31G*), "
                                      "RHF to convergence + RHF gradient each, one batched handle",
                          "molecules_per_s": 512 / wall, "wall_s": wall, "setup_s": rb["setup_s"],
@@ -719,14 +730,12 @@ def run_ours(args, world, rank, local):
                          "converged": int(rb["converged"].sum()), "cuda_graph": rb["graph"], "autotuned": rb["autotuned"],
                          "schedule": f"hfgpu_autotune on the batch, untimed ({t_tune:.2f} s incl. its set-up)",
                          "jk_build_ms": rb["build_ms_mean"], "nbf_total": int(sum(b.nbf for b in bb)),
-                         "density_step": rb["density"], "diag_fallback_iterations": rb["diag_fallbacks"]}
+                         "density_step": rb["density"], "diag_fallback_iterations": rb["diag_fallbacks"],
+                         "runs": "median of three whole runs", "walls_s": walls}
         # the same batch in mixed precision (FP32 quartets below the Schwarz bound 1e-4)
-        torch.cuda.synchronize()
-        tb = time.perf_counter()
-        rbm = BT.batch_rhf(bb, device=local, precision=E.MIXED, schedule=tuned_sched)
-        wall_m = DI.max_over_ranks(time.perf_counter() - tb, dev)
-        torch.cuda.set_stream(stream)
-        line["batch"]["mixed"] = {"molecules_per_s": 512 / wall_m, "wall_s": wall_m, "setup_s": rbm["setup_s"],
+        wall_m, rbm, walls_m = timed_batch(precision=E.MIXED)
+        line["batch"]["mixed"] = {"molecules_per_s": 512 / wall_m, "wall_s": wall_m, "walls_s": walls_m,
+                                  "setup_s": rbm["setup_s"],
                                   "scf_s": rbm["scf_s"], "grad_s": rbm["grad_s"], "iterations": rbm["iterations"],
                                   "converged": int(rbm["converged"].sum()),
                                   "max_abs_dE_vs_fp64": float(np.max(np.abs(rbm["energies"] - rb["energies"])))}
