@@ -167,13 +167,15 @@ class _Layout:
         return out
 
 
-def batch_sad_guess(bases: list[Basis], nmax: int) -> np.ndarray:
+def batch_sad_guess(bases: list[Basis], nmax: int, engine_factory=None) -> np.ndarray:
     """SAD guess of every molecule, padded to nmax (the reference's default guess,
     Mol::hf_solver::get_sad_guess, src/scfsolver/hfscf_hf_solver.cpp:478-553): the atomic UHF of
     each (basis set, element) pair runs once (scf.sad_atom_density on a GPU engine of that atom's
     shells) and its spin-averaged density is copied onto every atom of that element in every
-    molecule with that basis set."""
+    molecule with that basis set.  ``engine_factory(atom_basis)`` makes the context-managed engine
+    of an atom (default: eng.Engine)."""
     from . import scf as _scf
+    factory = engine_factory or eng.Engine
     cache = {}
     D = np.zeros((len(bases), nmax, nmax))
     for k, b in enumerate(bases):
@@ -182,7 +184,7 @@ def batch_sad_guess(bases: list[Basis], nmax: int) -> np.ndarray:
         for a, Zc in enumerate(b.Z.tolist()):
             key = (b.name, bool(b.pure), int(Zc))
             if key not in cache:
-                with eng.Engine(_scf.atom_basis(b, a)) as e:
+                with factory(_scf.atom_basis(b, a)) as e:
                     S, T, V = e.one_electron()
                     cache[key] = _scf.sad_atom_density(int(Zc), S, T, V, lambda DJ, DKs: e.jk(DJ, DKs))
             D[k, off[a]:off[a + 1], off[a]:off[a + 1]] = cache[key]

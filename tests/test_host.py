@@ -285,3 +285,50 @@ def test_hessian_generator_second_derivative_rule_pointwise():
                 fd += sgn * prod(comps, cc)
             fd /= 4 * h * h
             assert abs(rule[wi, hi] - fd) < 1e-5 * max(1.0, abs(fd)), (comps, r, s, rule[wi, hi], fd)
+
+
+class _OracleAtomEngine:
+    """Stand-in for an atom's GPU engine in the SAD guess: S, T, V from the reference's own
+    one-electron routines and J/K from the C restatement's packed ERIs (host only)."""
+
+    def __init__(self, bs):
+        import oracle
+        self.bs = bs
+        self.eri = oracle.eri_packed(bs)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+    def one_electron(self):
+        import oracle
+        return oracle.ref_onee(self.bs)
+
+    def jk(self, DJ, DKs):
+        import oracle
+        return oracle.jk(self.eri, DJ)[0], [oracle.jk(self.eri, Dk)[1] for Dk in DKs]
+
+
+def test_batched_sad_guess_equals_the_per_molecule_guess():
+    """batch_sad_guess runs the atomic UHF once per (basis set, element) and copies it onto every
+    atom: each molecule's padded block equals scf.sad_guess of that molecule with the same atomic
+    engines (host J/K) to 1e-8 (the atomic density is the same wherever the atom sits; the
+    atomic runs, stopped at the SAD tolerances of rms 1e-6, differ in the last digits with the
+    atom's position), and the padding is zero."""
+    import oracle
+    from hfscf_b200 import batch as BT
+    from hfscf_b200 import scf
+    if not oracle.ref_available():
+        pytest.skip("reference library not built here")
+    mols = M.batch_molecules(512)[:8]
+    bases = BT.batch_bases(mols)
+    assert len({b.name for b in bases}) == 2  # both basis sets of the mix
+    nmax = max(b.nbf for b in bases)
+    D = BT.batch_sad_guess(bases, nmax, engine_factory=_OracleAtomEngine)
+    for k, b in enumerate(bases):
+        Dk = scf.sad_guess(b, engine_factory=_OracleAtomEngine)
+        n = b.nbf
+        assert np.abs(D[k, :n, :n] - Dk).max() < 1e-8
+        assert not D[k, n:, :].any() and not D[k, :, n:].any()
