@@ -55,8 +55,8 @@ def _compile(src, verbose):
     if base.startswith("inst_"):
         deps.append(os.path.join(GEN, "class_" + base[5:] + ".cuh"))
     elif base.startswith("hess_") and base != "hess_dispatch":
-        deps += [os.path.join(GEN, base + ".cuh"), os.path.join(CSRC, "hfgpu_hess_kernels.cuh"),
-                 os.path.join(CSRC, "hfgpu_hess_launch.h")]
+        deps += [os.path.join(GEN, base + ".cuh"), os.path.join(GEN, "class_" + base[5:] + ".cuh"),
+                 os.path.join(CSRC, "hfgpu_hess_kernels.cuh"), os.path.join(CSRC, "hfgpu_hess_launch.h")]
     else:  # hand-written sources: every hand-written header counts
         deps += sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")))
     stamp = obj + ".sha1"

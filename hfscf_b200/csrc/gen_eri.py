@@ -1070,7 +1070,7 @@ const ClassLaunchers launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_quartet<d
 
 HESS_INST_TEMPLATE = """// GENERATED by gen_eri.py -- do not edit.
 #include "../hfgpu_hess_kernels.cuh"
-#include "hess_{t}.cuh"
+{line_include}#include "hess_{t}.cuh"
 #include "../hfgpu_hess_launch.h"
 
 namespace hfgpu {{
@@ -1120,11 +1120,28 @@ static bool launch_hess_warp(const GradArgs<double>& a, const HessOut& o, int pu
     return false;
   }}
 }}
+{line_fn}
 extern const HessLaunchers hess_launchers_{t};
 const HessLaunchers hess_launchers_{t} = {{{la}, {lb}, {lc}, {ld}, &launch_hess, &hess_scratch_slots,
-                                          &launch_hess_block, &hess_block_global_slots, &launch_hess_warp}};
+                                          &launch_hess_block, &hess_block_global_slots, &launch_hess_warp,
+                                          {has_line}, &launch_hess_line}};
 }}  // namespace hfgpu
 """
+
+# straight-line form (gen_hess_line): one thread per quartet, grid-stride over grid blocks
+HESS_LINE_LAUNCH = """// straight-line form: one thread per quartet on register code, grid blocks of 128 threads
+static bool launch_hess_line(const GradArgs<double>& a, const HessOut& o, int pure, const int2* q, int nq, int grid,
+                             int smem, cudaStream_t s) {{
+  if (nq <= 0) return true;
+  auto k = hess_line_kernel<{la}, {lb}, {lc}, {ld}, HessLine{t}>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  k<<<grid, 128, smem, s>>>(a, o, pure, q, nq);
+  return true;
+}}"""
+HESS_LINE_NONE = """// no straight-line form: a weight set of the class needs more than HESS_LINE_MAX_SET accumulators
+static bool launch_hess_line(const GradArgs<double>&, const HessOut&, int, const int2*, int, int, int, cudaStream_t) {
+  return false;
+}"""
 
 
 def main(outdir):
@@ -1159,11 +1176,18 @@ def main(outdir):
         meta["hess"].append(mh)
         code_b, mb = gen_hess_block(*c)
         mh["block"] = mb
+        code_l, ml = gen_hess_line(*c)
+        mh["line"] = ml
         write_if_changed(os.path.join(outdir, f"hess_{t}.cuh"),
                          "// GENERATED by gen_eri.py -- do not edit.\n#pragma once\n#include \"common.cuh\"\n\n" +
-                         code_h + "\n\n" + code_b + "\n")
+                         code_h + "\n\n" + code_b + "\n" + ("\n" + code_l + "\n" if code_l else ""))
         la, lb, lc, ld = c
-        write_if_changed(os.path.join(outdir, f"hess_{t}.cu"), HESS_INST_TEMPLATE.format(t=t, la=la, lb=lb, lc=lc, ld=ld))
+        line = code_l is not None
+        write_if_changed(os.path.join(outdir, f"hess_{t}.cu"), HESS_INST_TEMPLATE.format(
+            t=t, la=la, lb=lb, lc=lc, ld=ld,
+            line_include=f'#include "class_{t}.cuh"  // ClassCode::from_pure of the straight-line form\n' if line else "",
+            line_fn=(HESS_LINE_LAUNCH.format(t=t, la=la, lb=lb, lc=lc, ld=ld) if line else HESS_LINE_NONE),
+            has_line="true" if line else "false"))
         hnames.append(t)
     hd = ["// GENERATED by gen_eri.py -- do not edit.", '#include "../hfgpu_hess_launch.h"', "namespace hfgpu {"]
     hd += [f"extern const HessLaunchers hess_launchers_{t};" for t in hnames]
@@ -2131,6 +2155,144 @@ def gen_hess_block(la, lb, lc, ld):
             "acc": nacc, "hrr_ops": len(hrows), "hrr_levels": len(hlv) - 1, "hrr_slots": nhs,
             "slots": nvs + 1 + nhs + 1 + 45 + 3 * ncart_blk}
     return "\n".join(s), meta
+
+
+HESS_LINE_MAX_SET = 64    # classes whose weight sets need at most this many accumulators each get
+                          # the straight-line form (with 96 or more, (ds|ps), (dp|ss) and (pp|ps)
+                          # spilled 4-11 KB per thread)
+HESS_LINE_PASS_ACC = 64   # ... split into passes of at most this many accumulators each (a single
+                          # weight set with more runs as one pass of its own)
+# weight of each set of HESS_SETS as a named register, and its definition in the bra or ket
+# primitive loop; set 0 has weight 1
+HESS_WEIGHT = [None, "wa", "wb", "wc", "waa", "wbb", "wcc", "wab", "wac", "wbc"]
+HESS_WEIGHT_DEF = {"waa": "wa * wa", "wbb": "wb * wb", "wab": "wa * wb",
+                   "wcc": "wc * wc", "wac": "wa * wc", "wbc": "wb * wc"}
+HESS_LINE_SIG = ("const PrimPair<R>* __restrict__ bp, const R* __restrict__ ea, const R* __restrict__ eb, int nbp, "
+                 "const PrimPair<R>* __restrict__ kp, const R* __restrict__ ec, int nkp, R ABx, R ABy, R ABz, "
+                 "R CDx, R CDy, R CDz, const BoysTable<R>& boys, WF&& weights, SF&& scatter")
+HESS_LINE_ARGS = "bp, ea, eb, nbp, kp, ec, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, weights, scatter"
+
+
+def hess_set_needs(la, lb, lc, ld, terms=None):
+    """Per weight set of HESS_SETS: the contracted [e0|f0] values its HRR reads, in first-use order."""
+    terms = hess_terms(la, lb, lc, ld) if terms is None else terms
+    out = []
+    for k in range(len(HESS_SETS)):
+        need = {}
+
+        def record(e, f):
+            need.setdefault((e, f), len(need))
+            return "x"
+
+        hr = HRR(Emitter(), record, prefix="h")
+        for hi, wi, kk, si, a, b, c, d in terms:
+            if si == k:
+                hr.bra(a, b, c, d)
+        out.append(list(need))
+    return out
+
+
+def gen_hess_line(la, lb, lc, ld):
+    """Straight-line adjoint Hessian of one class for one thread per quartet, every value in
+    registers (the small many-quartet classes, which the table forms run slowly: a level
+    barrier or a global-scratch round trip per handful of ops).  The ten weight sets are packed,
+    in HESS_SETS order, into passes of at most HESS_LINE_PASS_ACC accumulators.  A pass runs the
+    primitive loops with the VRR of its sets' targets only, then fetches the quartet's weight
+    block (weights(W), Cartesian), runs the HRR of its sets, contracts them into the 45 entries
+    of the 9 x 9 block and hands those to scatter(h45); nothing but the accumulators lives
+    through a pass's primitive loops.  None when a weight set of the class needs more than
+    HESS_LINE_MAX_SET accumulators (a pass of that size spills)."""
+    terms = hess_terms(la, lb, lc, ld)
+    needs = hess_set_needs(la, lb, lc, ld, terms)
+    if max(len(n) for n in needs) > HESS_LINE_MAX_SET:
+        return None, None
+    passes, cur, ncur = [], [], 0
+    for k, n in enumerate(needs):
+        if not n:
+            continue
+        if cur and ncur + len(n) > HESS_LINE_PASS_ACC:
+            passes.append(cur)
+            cur, ncur = [], 0
+        cur.append(k)
+        ncur += len(n)
+    if cur:
+        passes.append(cur)
+    t = f"{la}{lb}{lc}{ld}"
+    ncw = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
+    s = []
+    pmeta = []
+    for pi, psets in enumerate(passes):
+        idx = {}
+        for k in psets:
+            for ef in needs[k]:
+                idx[(k,) + ef] = len(idx)
+        nacc = len(idx)
+        em2 = Emitter("    ")
+        hr = {k: HRR(em2, (lambda kk: (lambda e, f: f"acc[{idx[(kk, e, f)]}]"))(k), prefix=f"h{pi}_{k}")
+              for k in psets}
+        out = {}
+        for hi, wi, kk, si, a, b, c, d in terms:
+            if si in psets:
+                v = hr[si].bra(a, b, c, d)
+                out.setdefault(hi, []).append(f"W[{wi}] * {v}" if kk == 1 else f"{lit(kk)} * W[{wi}] * {v}")
+        for hi in range(45):
+            if hi in out:
+                em2.emit(f"h45[{hi}] = " + " + ".join(out[hi]) + ";", 3 * len(out[hi]))
+            else:
+                em2.emit(f"h45[{hi}] = R(0);")
+        em = Emitter("        ")
+        vrr = VRR(em)
+        targets = sorted({(e, f) for (_, e, f) in idx}, key=lambda q: (sum(q[0]), cidx(q[0]), sum(q[1]), cidx(q[1])))
+        vals = {q: vrr.get(q[0], q[1], 0) for q in targets}
+        Lp = max(sum(e) + sum(f) for e, f in targets)
+        used = {HESS_WEIGHT[k] for k in psets if HESS_WEIGHT[k]}
+        s.append(f"  {{  // pass {pi}: weight sets {psets}, {nacc} accumulators, {len(vrr.memo)} VRR values")
+        s.append(f"    R acc[{nacc}];")
+        s.append("#pragma unroll")
+        s.append(f"    for (int t = 0; t < {nacc}; ++t) acc[t] = R(0);")
+        s.append("    for (int ib = 0; ib < nbp; ++ib) {")
+        s.append("      const R p = bp[ib].p, ip = bp[ib].ip, Px = bp[ib].Px, Py = bp[ib].Py, Pz = bp[ib].Pz;")
+        s.append("      const R PAx = bp[ib].PAx, PAy = bp[ib].PAy, PAz = bp[ib].PAz, Kab = bp[ib].Kp;")
+        s.append("      const R wa = R(2) * ea[ib], wb = R(2) * eb[ib];")
+        s.append("      (void)wa; (void)wb;")
+        for w in ("waa", "wbb", "wab"):
+            if w in used:
+                s.append(f"      const R {w} = {HESS_WEIGHT_DEF[w]};")
+        s.append("      for (int ik = 0; ik < nkp; ++ik) {")
+        s.append("        const R q = kp[ik].p, iq = kp[ik].ip, Qx = kp[ik].Px, Qy = kp[ik].Py, Qz = kp[ik].Pz;")
+        s.append("        const R QCx = kp[ik].PAx, QCy = kp[ik].PAy, QCz = kp[ik].PAz, Kcd = kp[ik].Kp;")
+        s.append("        const R wc = R(2) * ec[ik];")
+        s.append("        (void)wc;")
+        for w in ("wcc", "wac", "wbc"):
+            if w in used:
+                s.append(f"        const R {w} = {HESS_WEIGHT_DEF[w]};")
+        s += ["  " + line for line in PRIM_HEADER.rstrip("\n").split("\n")]
+        s.append(f"        R F[{Lp + 1}];")
+        s.append(f"        boys.template eval<{Lp}>(T, pre, F);")
+        adds = []
+        for (k, e, f), j in idx.items():
+            v = vals[(e, f)]
+            w = HESS_WEIGHT[k]
+            adds.append((v, f"        acc[{j}] += {v};" if w is None else f"        acc[{j}] += {w} * {v};"))
+        s += interleave_accumulation(list(em.lines), adds)
+        s.append("      }")
+        s.append("    }")
+        s.append(f"    R W[{ncw}];")
+        s.append("    weights(W);")
+        s.append("    R h45[45];")
+        s += em2.lines
+        s.append("    scatter(h45);")
+        s.append("  }")
+        pmeta.append({"sets": psets, "accumulators": nacc, "vrr_values": len(vrr.memo), "boys_m": Lp})
+    head = [f"// straight-line adjoint Hessian of ({'spdf'[la]}{'spdf'[lb]}|{'spdf'[lc]}{'spdf'[ld]}): "
+            f"{len(passes)} passes, {sum(m['accumulators'] for m in pmeta)} accumulators",
+            "template <typename R, typename WF, typename SF>",
+            f"__device__ __forceinline__ void hess_line_{t}({HESS_LINE_SIG}) {{"]
+    s = head + s + ["}", f"struct HessLine{t} {{",
+                    "  template <typename R, typename WF, typename SF>",
+                    f"  static __device__ __forceinline__ void run({HESS_LINE_SIG}) {{ hess_line_{t}<R>({HESS_LINE_ARGS}); }}",
+                    "};"]
+    return "\n".join(s), {"class": [la, lb, lc, ld], "passes": pmeta}
 
 
 if __name__ == "__main__":

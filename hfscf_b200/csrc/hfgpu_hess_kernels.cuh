@@ -10,10 +10,11 @@
 // shell quartet the class's generated op tables run the VRR two orders higher, the HRR of ten
 // exponent-weighted sets and the contraction of every shifted integral with W, and the quartet's
 // 12 x 12 block (centres A, B, C, D by x, y, z; D from translational invariance) is added into
-// the 3 natoms x 3 natoms Hessian.  Three forms: hess_kernel, one thread per quartet on
+// the 3 natoms x 3 natoms Hessian.  Four forms: hess_kernel, one thread per quartet on
 // thread-interleaved global scratch (gen_eri.py gen_hess_table); hess_block_kernel with one
 // block of 128 threads or one warp per quartet over levelised tables in shared memory
-// (gen_hess_block).
+// (gen_hess_block); hess_line_kernel, one thread per quartet on straight-line register code
+// (gen_hess_line, the classes whose weight sets need at most 64 accumulators each).
 #pragma once
 #include "hfgpu_kernels.cuh"
 
@@ -115,6 +116,36 @@ __device__ void hess_table(const PrimPair<double>* __restrict__ bp, const double
 // Position of coordinate pair (r, s), r <= s, of the 9 x 9 block in the 45-entry upper triangle.
 __device__ __forceinline__ int hess_tri(int r, int s) { return r * 9 - r * (r - 1) / 2 + (s - r); }
 
+// Adds the quartet's 12 x 12 block over centres A, B, C, D (atoms at[0..3]) into the
+// 3 natoms x 3 natoms Hessian hout: the A, B, C part from the 45 entries h45, a D row or column
+// as minus the sum of the A, B, C ones (translational invariance).
+template <typename H>
+__device__ __forceinline__ void hess_add_block(const H& h45, const int (&at)[4], double* hout, int n3) {
+  // unrolled, so that a register array h45 is read at constant indexes
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      double hx[4][4];
+#pragma unroll
+      for (int X = 0; X < 3; ++X)
+#pragma unroll
+        for (int Y = 0; Y < 3; ++Y) {
+          const int r = 3 * X + i, c = 3 * Y + j;
+          hx[X][Y] = r <= c ? h45[hess_tri(r, c)] : h45[hess_tri(c, r)];
+        }
+#pragma unroll
+      for (int X = 0; X < 3; ++X) hx[X][3] = -(hx[X][0] + hx[X][1] + hx[X][2]);
+#pragma unroll
+      for (int Y = 0; Y < 4; ++Y) hx[3][Y] = -(hx[0][Y] + hx[1][Y] + hx[2][Y]);
+#pragma unroll
+      for (int X = 0; X < 4; ++X)
+#pragma unroll
+        for (int Y = 0; Y < 4; ++Y)
+          if (hx[X][Y] != 0.0) atomicAdd(hout + (size_t)(3 * at[X] + i) * n3 + 3 * at[Y] + j, hx[X][Y]);
+    }
+}
+
 template <int LA, int LB, int LC, int LD, bool PURE, typename Tab>
 __device__ __forceinline__ void hess_quartet(const GradArgs<double>& a, const HessOut& o, int tid, const int2 pq,
                                              double* hout, int n3) {
@@ -174,22 +205,8 @@ __device__ __forceinline__ void hess_quartet(const GradArgs<double>& a, const He
   hess_table<Tab>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
                   a.prims + Q.prim_off, a.alpha_a + Q.prim_off, Q.nprim, P.ABx, P.ABy, P.ABz, Q.ABx, Q.ABy, Q.ABz,
                   a.boys, Wc, vs, hs, h45);
-  // 12 x 12 block over centres A, B, C, D: a D row or column is minus the sum of the A, B, C ones
   const int at[4] = {P.atom_a, P.atom_b, Q.atom_a, Q.atom_b};
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      double hx[4][4];
-      for (int X = 0; X < 3; ++X)
-        for (int Y = 0; Y < 3; ++Y) {
-          const int r = 3 * X + i, c = 3 * Y + j;
-          hx[X][Y] = r <= c ? h45[hess_tri(r, c)] : h45[hess_tri(c, r)];
-        }
-      for (int X = 0; X < 3; ++X) hx[X][3] = -(hx[X][0] + hx[X][1] + hx[X][2]);
-      for (int Y = 0; Y < 4; ++Y) hx[3][Y] = -(hx[0][Y] + hx[1][Y] + hx[2][Y]);
-      for (int X = 0; X < 4; ++X)
-        for (int Y = 0; Y < 4; ++Y)
-          if (hx[X][Y] != 0.0) atomicAdd(hout + (size_t)(3 * at[X] + i) * n3 + 3 * at[Y] + j, hx[X][Y]);
-    }
+  hess_add_block(h45, at, hout, n3);
 }
 
 template <int LA, int LB, int LC, int LD, typename Tab>
@@ -212,6 +229,67 @@ __global__ void __launch_bounds__(128) hess_kernel(GradArgs<double> a, HessOut o
       hess_quartet<LA, LB, LC, LD, true, Tab>(a, o, tid, pq, hout, n3);
     else
       hess_quartet<LA, LB, LC, LD, false, Tab>(a, o, tid, pq, hout, n3);
+  }
+  if (o.smem) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < n3 * n3; i += blockDim.x)
+      if (hess_sh[i] != 0.0) atomicAdd(o.hess + i, hess_sh[i]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Straight-line form: one thread per quartet, the class's generated code (gen_eri.py
+// gen_hess_line) with every value in registers, in passes of a few weight sets each; every pass
+// adds its share of the quartet's 12 x 12 block into the output.  For the small many-quartet
+// classes, whose table forms spend their time on level barriers or on global scratch round
+// trips rather than on the few dozen ops of a level.
+// ---------------------------------------------------------------------------
+template <int LA, int LB, int LC, int LD, bool PURE, typename Line>
+__device__ __forceinline__ void hess_line_quartet(const GradArgs<double>& a, const int2 pq, double* hout, int n3) {
+  using Dm = BlockDims<LA, LB, LC, LD, PURE>;
+  const PairInfo P = a.pairs[pq.x];
+  const PairInfo Q = a.pairs[pq.y];
+  double s = 8.0;
+  if (P.sa == P.sb) s *= 0.5;
+  if (Q.sa == Q.sb) s *= 0.5;
+  if (pq.x == pq.y) s *= 0.5;
+  // the weight block, Cartesian, fetched by each pass after its primitive loops
+  auto weights = [&](double* Wc) {
+    if constexpr (PURE) {
+      double Wp[Dm::NOUT];
+      grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb, Q.fa, Q.fb, s, Wp);
+      ClassCode<LA, LB, LC, LD>::template from_pure<double>(Wp, Wc);
+    } else {
+      grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb, Q.fa, Q.fb, s, Wc);
+    }
+  };
+  const int at[4] = {P.atom_a, P.atom_b, Q.atom_a, Q.atom_b};
+  auto scatter = [&](const double* h45) { hess_add_block(h45, at, hout, n3); };
+  Line::template run<double>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
+                             a.prims + Q.prim_off, a.alpha_a + Q.prim_off, Q.nprim, P.ABx, P.ABy, P.ABz, Q.ABx,
+                             Q.ABy, Q.ABz, a.boys, weights, scatter);
+}
+
+template <int LA, int LB, int LC, int LD, typename Line>
+__global__ void __launch_bounds__(128) hess_line_kernel(GradArgs<double> a, HessOut o, int pure,
+                                                        const int2* __restrict__ quartets, int nq) {
+  extern __shared__ double hess_sh[];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthr = gridDim.x * blockDim.x;
+  const int n3 = 3 * o.natoms;
+  double* hout = o.hess;
+  if (o.smem) {
+    for (int i = threadIdx.x; i < n3 * n3; i += blockDim.x) hess_sh[i] = 0.0;
+    __syncthreads();
+    hout = hess_sh;
+  }
+  const int np = a.nparts > 1 ? a.nparts : 1, p0 = np > 1 ? a.part : 0;
+  for (int t = tid; t < nq; t += nthr) {
+    const int2 pq = quartets[(size_t)t * np + p0];
+    if (pure)
+      hess_line_quartet<LA, LB, LC, LD, true, Line>(a, pq, hout, n3);
+    else
+      hess_line_quartet<LA, LB, LC, LD, false, Line>(a, pq, hout, n3);
   }
   if (o.smem) {
     __syncthreads();

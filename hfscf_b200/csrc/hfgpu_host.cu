@@ -192,12 +192,14 @@ struct hfgpu_handle {
   // (grad_form_of)
   int grad_form[21];
   unsigned grad_class_mask = ~0u;       // classes a gradient launches (autotuning runs one at a time)
-  // Hessian form (hfgpu_set_hess_form): -1 by table size, 0 one thread per quartet, 1 one block
-  // per quartet, 2 one warp per quartet (where the class's tables fit)
+  // Hessian form (hfgpu_set_hess_form): -1 by class, 0 one thread per quartet, 1 one block per
+  // quartet, 2 one warp per quartet (where the class's tables fit), 3 one thread per quartet on
+  // straight-line code (where the class has it)
   int hess_form = -1;
   int purify_blocks = -1;               // co-resident blocks of the cooperative purification (0: not available)
   int purify_coop = 1;                  // hfgpu_set_purify_mode: 1 one cooperative launch, 0 two launches per step
-  int hess_cls_form[21];                // per class (hfgpu_autotune_hess): 0 thread, 1 block, 2 warp, -1 hess_form
+  int hess_cls_form[21];                // per class (hfgpu_autotune_hess): 0 thread, 1 block, 2 warp, 3 line,
+                                        // -1 hess_form
   unsigned hess_class_mask = ~0u;       // classes a Hessian launches (autotuning runs one at a time)
 
   hfgpu_handle() : q_beg(21), q_mid(21), q_end(21), q_hik1(21), q_hik2(21), q_prims(21) {
@@ -1969,6 +1971,7 @@ constexpr size_t kHessScratchBudget = (size_t)2 << 30;
 constexpr size_t kHessSmemBytes = 96 * 1024;  // per-block Hessian in shared memory up to 36 atoms
 constexpr int kHessBlockMinSlots = 1000;       // thread-form tables from this size run in the block form,
 constexpr long long kHessBlockMaxQuartets = 4096;  // and so do classes with at most this many quartets
+constexpr long long kHessLineGrid = 4 * 148;     // straight-line form: at most four blocks per SM, grid-stride
 constexpr long long kHessBlockGrid = 296;      // blocks of a block-form launch with global HRR slots
 
 static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK, const double* DK, double cK,
@@ -1997,18 +2000,23 @@ static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     return std::max<long long>(128, thr / 128 * 128);
   };
   // form per class: 0 one thread per quartet on global scratch, 1 one block of 128 threads per
-  // quartet over levelised tables, 2 one warp per quartet over the same tables.  Default: the block
-  // form for the classes whose tables are large or whose quartets are too few to fill the GPU
-  // (one thread would run a long chain of dependent table ops on global scratch), the warp form
-  // for the small many-quartet classes (their levels hold a few dozen ops).
+  // quartet over levelised tables, 2 one warp per quartet over the same tables, 3 one thread per
+  // quartet on straight-line register code (the classes that have it; a class without it takes
+  // the default).  Default: the straight-line form where the class has one; else the block form
+  // for the classes whose tables are large or whose quartets are too few to fill the GPU (one
+  // thread would run a long chain of dependent table ops on global scratch), the warp form for
+  // the small many-quartet classes (their levels hold a few dozen ops).
   auto form_of = [&](int c) -> int {
-    if (h->hess_cls_form[c] >= 0) return h->hess_cls_form[c];
-    if (h->hess_form >= 0) return h->hess_form;
+    const bool line = hfgpu::kHessLaunchers[c]->has_line;
+    int f = h->hess_cls_form[c] >= 0 ? h->hess_cls_form[c] : h->hess_form;
+    if (f == 3 && !line) f = -1;
+    if (f >= 0) return f;
+    if (line) return 3;
     const bool big = hfgpu::kHessLaunchers[c]->scratch_slots(h->pure) >= kHessBlockMinSlots ||
                      part_share(h, h->q_end[c] - h->q_beg[c]) <= kHessBlockMaxQuartets;
     return big ? 1 : 2;
   };
-  auto use_block = [&](int c) -> bool { return form_of(c) >= 1; };
+  auto use_block = [&](int c) -> bool { return form_of(c) == 1 || form_of(c) == 2; };
   // block-form grid: one block per quartet, or kHessBlockGrid blocks when the HRR slots live in
   // global scratch (one region per block)
   auto block_grid = [&](int c, long long nq) -> long long {
@@ -2030,7 +2038,9 @@ static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     if (nq <= 0 || !((h->hess_class_mask >> c) & 1u)) continue;
     stream_of[c] = rr++ % kS;
     size_t bytes;
-    if (use_block(c)) {
+    if (form_of(c) == 3) {
+      bytes = 0;
+    } else if (use_block(c)) {
       bytes = sizeof(double) * (size_t)L->block_global_slots() * (size_t)block_grid(c, nq);
     } else {
       const int slots = L->scratch_slots(h->pure);
@@ -2049,6 +2059,14 @@ static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
     if (stream_of[c] < 0) continue;
     const hfgpu::HessLaunchers* L = hfgpu::kHessLaunchers[c];
     const long long nq = part_share(h, h->q_end[c] - h->q_beg[c]);
+    if (form_of(c) == 3) {
+      const long long grid = std::min<long long>((nq + 127) / 128, kHessLineGrid);
+      if (!L->launch_line(gd, o, h->pure, q + h->q_beg[c], (int)nq, (int)grid, o.smem ? (int)smem : 0,
+                          h->aux[stream_of[c]]))
+        return fail(h, HFGPU_ERR_STATE, "class without a Hessian straight-line form");
+      HF_CHECK_LAUNCH(h, "hess line kernel");
+      continue;
+    }
     if (use_block(c)) {
       const int st = stream_of[c];
       const long long grid = block_grid(c, nq);
@@ -2081,7 +2099,7 @@ static int hess_device_impl(hfgpu_handle* h, const double* DJ, double cJ, int nK
 }
 
 int hfgpu_set_hess_form(hfgpu_handle* h, int form) {
-  if (!h || form < -1 || form > 2) return HFGPU_ERR_INVALID;
+  if (!h || form < -1 || form > 3) return HFGPU_ERR_INVALID;
   h->hess_form = form;
   for (int c = 0; c < 21; ++c) h->hess_cls_form[c] = -1;
   return HFGPU_OK;
@@ -2090,7 +2108,7 @@ int hfgpu_set_hess_form(hfgpu_handle* h, int form) {
 int hfgpu_set_hess_forms(hfgpu_handle* h, const int* forms) {
   if (!h || !forms) return HFGPU_ERR_INVALID;
   for (int c = 0; c < hfgpu::kNumClasses; ++c)
-    if (forms[c] < -1 || forms[c] > 2) return HFGPU_ERR_INVALID;
+    if (forms[c] < -1 || forms[c] > 3) return HFGPU_ERR_INVALID;
   for (int c = 0; c < hfgpu::kNumClasses; ++c) h->hess_cls_form[c] = forms[c];
   return HFGPU_OK;
 }
@@ -2595,8 +2613,9 @@ int hfgpu_set_grad_forms(hfgpu_handle* h, const int* forms) {
   return HFGPU_OK;
 }
 
-// Hessian form per class: each class alone, one thread, one block or one warp per quartet, on RHF
-// weights of the device density D; the fastest is kept.
+// Hessian form per class: each class alone, one thread (global scratch), one block or one warp
+// per quartet, or one thread on straight-line code where the class has it, on RHF weights of the
+// device density D; the fastest is kept.
 int hfgpu_autotune_hess(hfgpu_handle* h, const double* D, int repeats, int* forms) {
   if (!h || !D) return HFGPU_ERR_INVALID;
   DeviceGuard dev_guard(h);
@@ -2635,7 +2654,8 @@ int hfgpu_autotune_hess(hfgpu_handle* h, const double* D, int repeats, int* form
     h->hess_class_mask = 1u << c;
     float best = 1e30f;
     int best_form = 0;
-    for (int form = 0; form < 3; ++form) {
+    for (int form = 0; form < 4; ++form) {
+      if (form == 3 && !hfgpu::kHessLaunchers[c]->has_line) continue;
       h->hess_cls_form[c] = form;
       float ms = 0.f;
       if ((rc = tuner_time(h, hessian, repeats, e0, e1, restore.flush, &ms))) return rc;

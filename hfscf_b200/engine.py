@@ -385,14 +385,22 @@ class Engine:
         return H
 
     def set_hess_form(self, form: int):
-        """hfgpu_set_hess_form: -1 by table size (default), 0 thread, 1 block, 2 warp per quartet."""
+        """hfgpu_set_hess_form: -1 by class (default), 0 thread (global scratch), 1 block, 2 warp per
+        quartet, 3 thread on straight-line register code where the class has it."""
         self._check(lib().hfgpu_set_hess_form(self.h, ctypes.c_int(form)))
 
-    def autotune_hess(self, D_ptr, repeats=2):
-        """hfgpu_autotune_hess on a device density: per class the faster of the thread and block
-        forms; returns the chosen forms."""
+    def autotune_hess(self, D, repeats=2):
+        """hfgpu_autotune_hess on density D (host array, device tensor or device pointer): per
+        class the fastest of the thread, block, warp and straight-line forms; returns the chosen
+        forms (0 thread, 1 block, 2 warp, 3 straight-line)."""
+        import torch
+        if isinstance(D, int):
+            ptr = D
+        else:
+            Dd = D if isinstance(D, torch.Tensor) else torch.from_numpy(_c(D)).to(torch.device("cuda", self._opts.device))
+            ptr = Dd.data_ptr()
         forms = (ctypes.c_int * NUM_CLASSES)()
-        self._check(lib().hfgpu_autotune_hess(self.h, ctypes.c_void_p(D_ptr), ctypes.c_int(repeats), forms))
+        self._check(lib().hfgpu_autotune_hess(self.h, ctypes.c_void_p(ptr), ctypes.c_int(repeats), forms))
         return list(forms)
 
     def set_hess_forms(self, forms):

@@ -2,7 +2,7 @@
 
     python -m hfscf_b200.profile_case jk   --workload 2 [--precision mixed] [--repeat 3]
     python -m hfscf_b200.profile_case grad --workload 3 [--repeat 1]
-    python -m hfscf_b200.profile_case hess --workload 4 [--repeat 1] [--hess-form 0|1|2]
+    python -m hfscf_b200.profile_case hess --workload 4 [--repeat 1] [--hess-form 0|1|2|3]
     python -m hfscf_b200.profile_case jk   --workload 2 --variant 2   (every class in the staged form)
 
 Builds the named workload's basis (``molecules.workload``: 1 = H2O/cc-pVDZ,
@@ -48,7 +48,7 @@ def main(argv=None):
     ap.add_argument("--variant", type=int, choices=(0, 1, 2), default=None,
                     help="thread-form variant for every class (schedule column 3: 0 plain, 1 capped, "
                          "2 staged persistent)")
-    ap.add_argument("--hess-form", type=int, choices=(-1, 0, 1, 2), default=-1,
+    ap.add_argument("--hess-form", type=int, choices=(-1, 0, 1, 2, 3), default=-1,
                     help="hess: -1 default per class, 0 one thread, 1 one block, 2 one warp per quartet")
     a = ap.parse_args(argv)
     if not torch.cuda.is_available():

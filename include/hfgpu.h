@@ -138,14 +138,17 @@ int hfgpu_grad2e_uhf_backward(hfgpu_handle* h, const double* Da, const double* D
  * FP64 only; single-molecule handles (HFGPU_ERR_UNSUPPORTED for a batched handle). */
 int hfgpu_hess2e(hfgpu_handle* h, const double* D, double scale, double* hess);
 int hfgpu_hess2e_uhf(hfgpu_handle* h, const double* Da, const double* Db, double scale, double* hess);
-/* Launch form of the Hessian classes: -1 (default) one block of 128 threads per quartet for the
- * classes with large op tables or few quartets and one warp per quartet for the others, 0 one
- * thread per quartet everywhere, 1 one block per quartet everywhere, 2 one warp per quartet
- * wherever four quartets' tables fit one block (the block form elsewhere).  The results agree
- * to rounding. */
+/* Launch form of the Hessian classes: -1 (default) one thread per quartet on straight-line
+ * register code for the small classes that have it ((ss|ss), (ps|ss), (ps|ps), (pp|ss), (ds|ss):
+ * the classes whose weight sets need at most 64 accumulators each), else one block of 128
+ * threads per quartet for the classes with large op tables or few quartets and one warp per
+ * quartet for the others; 0 one thread per quartet on global scratch everywhere, 1 one block per
+ * quartet everywhere, 2 one warp per quartet wherever four quartets' tables fit one block (the
+ * block form elsewhere), 3 the straight-line form wherever the class has it (the default
+ * elsewhere).  The results agree to rounding. */
 int hfgpu_set_hess_form(hfgpu_handle* h, int form);
-/* Per class (HFGPU_NUM_CLASSES ints: 0 thread, 1 block, 2 warp, -1 the rule of hfgpu_set_hess_form), as
- * hfgpu_autotune_hess returns them. */
+/* Per class (HFGPU_NUM_CLASSES ints: 0 thread, 1 block, 2 warp, 3 straight-line, -1 the rule of
+ * hfgpu_set_hess_form), as hfgpu_autotune_hess returns them. */
 int hfgpu_set_hess_forms(hfgpu_handle* h, const int* forms);
 /* Times every class alone in each form on RHF weights of the device density D (median of
  * `repeats` runs, L2 flushed before each) and keeps the faster per class; forms (may be NULL)

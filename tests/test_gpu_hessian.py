@@ -54,14 +54,15 @@ def _ref_hessian(bs, D):
     return hc + he
 
 
-FORMS = [(-1, "default"), (0, "thread"), (1, "block"), (2, "warp")]
+FORMS = [(-1, "default"), (0, "thread"), (1, "block"), (2, "warp"), (3, "line")]
 
 
 @pytest.mark.parametrize("form", [f for f, _ in FORMS], ids=[n for _, n in FORMS])
 @pytest.mark.parametrize("name,bs", MOLS, ids=[m[0] for m in MOLS])
 def test_hess2e_matches_reference(name, bs, form):
     """Every launch form (one thread per quartet on global scratch, one block or one warp per
-    quartet over levelised tables, and the default mix) against the reference."""
+    quartet over levelised tables, one thread per quartet on straight-line register code for the
+    classes that have it, and the default mix) against the reference."""
     rng = np.random.default_rng(3)
     D = _sym(rng, bs.nbf)
     with E.Engine(bs) as eng:
@@ -161,3 +162,27 @@ def test_hess2e_rejects_batched_handles():
         assert not H.any()
     finally:
         be.close()
+
+
+def test_hess2e_autotuned_forms_match_default():
+    """hfgpu_autotune_hess times every class in each form it has (the straight-line form only
+    where the class has one) and keeps the fastest; the Hessian with the chosen forms equals the
+    default one to rounding, and a form set per class through hfgpu_set_hess_forms is reapplied."""
+    Z, x = M.water_cluster(2, 2.9, np.random.default_rng(5), 0.1)
+    bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
+    rng = np.random.default_rng(8)
+    D = _sym(rng, bs.nbf, 0.3)
+    # class order of a handle: (ss|ss), (ps|ss), (ps|ps), (pp|ss), (pp|ps), (pp|pp), (ds|ss), ...;
+    # the classes with a straight-line form are (ss|ss), (ps|ss), (ps|ps), (pp|ss) and (ds|ss)
+    line_classes = {0, 1, 2, 3, 6}
+    with E.Engine(bs, density_tol=0.0) as eng:
+        H0 = eng.hess2e(D)
+        forms = eng.autotune_hess(D, repeats=1)
+        H1 = eng.hess2e(D)
+        eng.set_hess_forms([3 if f == 3 else 1 for f in forms])
+        H2 = eng.hess2e(D)
+    assert len(forms) == E.NUM_CLASSES
+    assert all(f in (0, 1, 2, 3) for f in forms)
+    assert all(c in line_classes for c, f in enumerate(forms) if f == 3)
+    assert np.max(np.abs(H1 - H0)) < 1e-11
+    assert np.max(np.abs(H2 - H0)) < 1e-11

@@ -164,7 +164,7 @@ def test_fock_entry_points_are_refused_on_a_partitioned_handle_and_bad_partition
         assert np.max(np.abs(F - (H + 2.0 * J - K))) < TOL_ORACLE
 
 
-@pytest.mark.parametrize("form", [-1, 0, 1, 2], ids=["default", "thread", "block", "warp"])
+@pytest.mark.parametrize("form", [-1, 0, 1, 2, 3], ids=["default", "thread", "block", "warp", "line"])
 def test_partitioned_hessian_sums_to_the_whole(form):
     """The two-electron Hessian honours the partition: its parts, summed as an all-reduce of the
     3 natoms x 3 natoms blocks would sum them, equal the whole Hessian (1e-11) in every form."""
