@@ -1134,11 +1134,12 @@ static bool launch_hess_line(const GradArgs<double>& a, const HessOut& o, int pu
                              int smem, cudaStream_t s) {{
   if (nq <= 0) return true;
   auto k = hess_line_kernel<{la}, {lb}, {lc}, {ld}, HessLine{t}>;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  k<<<grid, 128, smem, s>>>(a, o, pure, q, nq);
+  const int bytes = smem + kHessLineH45Bytes;  // the block's Hessian (smem > 0) and the h45 slices
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  k<<<grid, kHessLineThreads, bytes, s>>>(a, o, pure, q, nq);
   return true;
 }}"""
-HESS_LINE_NONE = """// no straight-line form: a weight set of the class needs more than HESS_LINE_MAX_SET accumulators
+HESS_LINE_NONE = """// no straight-line form: the class's passes would spill or be too many (gen_hess_line)
 static bool launch_hess_line(const GradArgs<double>&, const HessOut&, int, const int2*, int, int, int, cudaStream_t) {
   return false;
 }"""
@@ -2157,11 +2158,8 @@ def gen_hess_block(la, lb, lc, ld):
     return "\n".join(s), meta
 
 
-HESS_LINE_MAX_SET = 64    # classes whose weight sets need at most this many accumulators each get
-                          # the straight-line form (with 96 or more, (ds|ps), (dp|ss) and (pp|ps)
-                          # spilled 4-11 KB per thread)
-HESS_LINE_PASS_ACC = 64   # ... split into passes of at most this many accumulators each (a single
-                          # weight set with more runs as one pass of its own)
+HESS_LINE_PASS_ACC = 64   # accumulators of one pass of the straight-line Hessian form
+HESS_LINE_MAX_PASSES = 24  # classes that need more passes keep the table forms only
 # weight of each set of HESS_SETS as a named register, and its definition in the bra or ket
 # primitive loop; set 0 has weight 1
 HESS_WEIGHT = [None, "wa", "wb", "wc", "waa", "wbb", "wcc", "wab", "wac", "wbc"]
@@ -2169,77 +2167,108 @@ HESS_WEIGHT_DEF = {"waa": "wa * wa", "wbb": "wb * wb", "wab": "wa * wb",
                    "wcc": "wc * wc", "wac": "wa * wc", "wbc": "wb * wc"}
 HESS_LINE_SIG = ("const PrimPair<R>* __restrict__ bp, const R* __restrict__ ea, const R* __restrict__ eb, int nbp, "
                  "const PrimPair<R>* __restrict__ kp, const R* __restrict__ ec, int nkp, R ABx, R ABy, R ABz, "
-                 "R CDx, R CDy, R CDz, const BoysTable<R>& boys, WF&& weights, SF&& scatter")
-HESS_LINE_ARGS = "bp, ea, eb, nbp, kp, ec, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, weights, scatter"
+                 "R CDx, R CDy, R CDz, const BoysTable<R>& boys, WF&& weights, H h45")
+HESS_LINE_ARGS = "bp, ea, eb, nbp, kp, ec, nkp, ABx, ABy, ABz, CDx, CDy, CDz, boys, weights, h45"
 
 
-def hess_set_needs(la, lb, lc, ld, terms=None):
-    """Per weight set of HESS_SETS: the contracted [e0|f0] values its HRR reads, in first-use order."""
-    terms = hess_terms(la, lb, lc, ld) if terms is None else terms
-    out = []
+def hess_term_needs(terms):
+    """The contracted [e0|f0] values the HRR of the given terms (one weight set) reads."""
+    need = {}
+
+    def record(e, f):
+        need.setdefault((e, f), len(need))
+        return "x"
+
+    hr = HRR(Emitter(), record, prefix="h")
+    for hi, wi, kk, si, a, b, c, d in terms:
+        hr.bra(a, b, c, d)
+    return list(need)
+
+
+def hess_line_units(la, lb, lc, ld, terms):
+    """The contraction terms cut into units [(set, terms, needed [e0|f0] values)] of at most
+    HESS_LINE_PASS_ACC accumulators where possible: a weight set whole, or split by the bra
+    component a of the differentiated integral (its W index), else by the ket component c, else
+    by both -- the HRR of each part then reads only the values near its own components."""
+    nb, nc, nd = ncart(lb), ncart(lc), ncart(ld)
+    keys = [lambda t: t[1] // (nb * nc * nd), lambda t: (t[1] // nd) % nc,
+            lambda t: (t[1] // (nb * nc * nd), (t[1] // nd) % nc)]
+    units = []
     for k in range(len(HESS_SETS)):
-        need = {}
+        tk = [t for t in terms if t[3] == k]
+        if not tk:
+            continue
+        whole = hess_term_needs(tk)
+        if len(whole) <= HESS_LINE_PASS_ACC:
+            units.append((k, tk, whole))
+            continue
+        best = None
+        for key in keys:
+            groups = {}
+            for t in tk:
+                groups.setdefault(key(t), []).append(t)
+            parts = [(k, g, hess_term_needs(g)) for _, g in sorted(groups.items())]
+            worst = max(len(u[2]) for u in parts)
+            if best is None or worst < best[0]:
+                best = (worst, parts)
+            if worst <= HESS_LINE_PASS_ACC:
+                break
+        units += best[1]
+    return units
 
-        def record(e, f):
-            need.setdefault((e, f), len(need))
-            return "x"
 
-        hr = HRR(Emitter(), record, prefix="h")
-        for hi, wi, kk, si, a, b, c, d in terms:
-            if si == k:
-                hr.bra(a, b, c, d)
-        out.append(list(need))
-    return out
+def hess_line_passes(la, lb, lc, ld, terms=None):
+    """Units packed, in order, into passes of at most HESS_LINE_PASS_ACC distinct accumulators
+    (a unit larger than that runs alone): [[(set, terms, needs), ...], ...]."""
+    terms = hess_terms(la, lb, lc, ld) if terms is None else terms
+    passes, cur, keys = [], [], set()
+    for u in hess_line_units(la, lb, lc, ld, terms):
+        ukeys = {(u[0],) + ef for ef in u[2]}
+        if cur and len(keys | ukeys) > HESS_LINE_PASS_ACC:
+            passes.append(cur)
+            cur, keys = [], set()
+        cur.append(u)
+        keys |= ukeys
+    if cur:
+        passes.append(cur)
+    return passes
 
 
 def gen_hess_line(la, lb, lc, ld):
     """Straight-line adjoint Hessian of one class for one thread per quartet, every value in
-    registers (the small many-quartet classes, which the table forms run slowly: a level
-    barrier or a global-scratch round trip per handful of ops).  The ten weight sets are packed,
-    in HESS_SETS order, into passes of at most HESS_LINE_PASS_ACC accumulators.  A pass runs the
-    primitive loops with the VRR of its sets' targets only, then fetches the quartet's weight
-    block (weights(W), Cartesian), runs the HRR of its sets, contracts them into the 45 entries
-    of the 9 x 9 block and hands those to scatter(h45); nothing but the accumulators lives
-    through a pass's primitive loops.  None when a weight set of the class needs more than
-    HESS_LINE_MAX_SET accumulators (a pass of that size spills)."""
+    registers (the many-quartet classes, which the table forms run slowly: a level barrier or a
+    global-scratch round trip per handful of ops).  The contraction terms are cut into passes of
+    at most HESS_LINE_PASS_ACC accumulators (hess_line_passes).  A pass runs the primitive loops
+    with the VRR of its targets only, then fetches the quartet's weight block (weights(W),
+    Cartesian), runs the HRR its terms read and adds them into the 45 entries h45 of the 9 x 9
+    block (an accessor to the thread's slice of shared memory), so that nothing but a pass's
+    accumulators lives through its primitive loops.  None when a unit still needs more than
+    HESS_LINE_PASS_ACC accumulators or the class more than HESS_LINE_MAX_PASSES passes."""
     terms = hess_terms(la, lb, lc, ld)
-    needs = hess_set_needs(la, lb, lc, ld, terms)
-    if max(len(n) for n in needs) > HESS_LINE_MAX_SET:
+    passes = hess_line_passes(la, lb, lc, ld, terms)
+    if len(passes) > HESS_LINE_MAX_PASSES or max(len(u[2]) for p in passes for u in p) > HESS_LINE_PASS_ACC:
         return None, None
-    passes, cur, ncur = [], [], 0
-    for k, n in enumerate(needs):
-        if not n:
-            continue
-        if cur and ncur + len(n) > HESS_LINE_PASS_ACC:
-            passes.append(cur)
-            cur, ncur = [], 0
-        cur.append(k)
-        ncur += len(n)
-    if cur:
-        passes.append(cur)
     t = f"{la}{lb}{lc}{ld}"
     ncw = ncart(la) * ncart(lb) * ncart(lc) * ncart(ld)
     s = []
     pmeta = []
-    for pi, psets in enumerate(passes):
+    for pi, units in enumerate(passes):
         idx = {}
-        for k in psets:
-            for ef in needs[k]:
-                idx[(k,) + ef] = len(idx)
+        for k, _, need in units:
+            for ef in need:
+                idx.setdefault((k,) + ef, len(idx))
+        psets = sorted({u[0] for u in units})
         nacc = len(idx)
         em2 = Emitter("    ")
         hr = {k: HRR(em2, (lambda kk: (lambda e, f: f"acc[{idx[(kk, e, f)]}]"))(k), prefix=f"h{pi}_{k}")
               for k in psets}
         out = {}
-        for hi, wi, kk, si, a, b, c, d in terms:
-            if si in psets:
+        for k, tl, _ in units:
+            for hi, wi, kk, si, a, b, c, d in tl:
                 v = hr[si].bra(a, b, c, d)
                 out.setdefault(hi, []).append(f"W[{wi}] * {v}" if kk == 1 else f"{lit(kk)} * W[{wi}] * {v}")
-        for hi in range(45):
-            if hi in out:
-                em2.emit(f"h45[{hi}] = " + " + ".join(out[hi]) + ";", 3 * len(out[hi]))
-            else:
-                em2.emit(f"h45[{hi}] = R(0);")
+        for hi in sorted(out):
+            em2.emit(f"h45[{hi}] += " + " + ".join(out[hi]) + ";", 3 * len(out[hi]))
         em = Emitter("        ")
         vrr = VRR(em)
         targets = sorted({(e, f) for (_, e, f) in idx}, key=lambda q: (sum(q[0]), cidx(q[0]), sum(q[1]), cidx(q[1])))
@@ -2279,17 +2308,16 @@ def gen_hess_line(la, lb, lc, ld):
         s.append("    }")
         s.append(f"    R W[{ncw}];")
         s.append("    weights(W);")
-        s.append("    R h45[45];")
         s += em2.lines
-        s.append("    scatter(h45);")
         s.append("  }")
         pmeta.append({"sets": psets, "accumulators": nacc, "vrr_values": len(vrr.memo), "boys_m": Lp})
     head = [f"// straight-line adjoint Hessian of ({'spdf'[la]}{'spdf'[lb]}|{'spdf'[lc]}{'spdf'[ld]}): "
-            f"{len(passes)} passes, {sum(m['accumulators'] for m in pmeta)} accumulators",
-            "template <typename R, typename WF, typename SF>",
+            f"{len(passes)} passes, {sum(m['accumulators'] for m in pmeta)} accumulators, "
+            f"{sum(m['vrr_values'] for m in pmeta)} VRR values",
+            "template <typename R, typename WF, typename H>",
             f"__device__ __forceinline__ void hess_line_{t}({HESS_LINE_SIG}) {{"]
     s = head + s + ["}", f"struct HessLine{t} {{",
-                    "  template <typename R, typename WF, typename SF>",
+                    "  template <typename R, typename WF, typename H>",
                     f"  static __device__ __forceinline__ void run({HESS_LINE_SIG}) {{ hess_line_{t}<R>({HESS_LINE_ARGS}); }}",
                     "};"]
     return "\n".join(s), {"class": [la, lb, lc, ld], "passes": pmeta}

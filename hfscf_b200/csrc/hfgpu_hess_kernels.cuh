@@ -14,7 +14,7 @@
 // thread-interleaved global scratch (gen_eri.py gen_hess_table); hess_block_kernel with one
 // block of 128 threads or one warp per quartet over levelised tables in shared memory
 // (gen_hess_block); hess_line_kernel, one thread per quartet on straight-line register code
-// (gen_hess_line, the classes whose weight sets need at most 64 accumulators each).
+// (gen_hess_line, the classes whose terms fit at most 24 passes of 64 accumulators).
 #pragma once
 #include "hfgpu_kernels.cuh"
 
@@ -239,13 +239,45 @@ __global__ void __launch_bounds__(128) hess_kernel(GradArgs<double> a, HessOut o
 
 // ---------------------------------------------------------------------------
 // Straight-line form: one thread per quartet, the class's generated code (gen_eri.py
-// gen_hess_line) with every value in registers, in passes of a few weight sets each; every pass
-// adds its share of the quartet's 12 x 12 block into the output.  For the small many-quartet
-// classes, whose table forms spend their time on level barriers or on global scratch round
-// trips rather than on the few dozen ops of a level.
+// gen_hess_line) with every value in registers, in passes of at most 64 accumulators.  Each pass
+// adds its terms into the thread's 45 entries of the 9 x 9 block, kept in shared memory (45 x 128
+// doubles per block, behind the block's Hessian when that is in shared memory too) so that they
+// hold no registers through the primitive loops; the 12 x 12 block goes into the output once per
+// quartet.  For the many-quartet classes, whose table forms spend their time on level barriers
+// or on global scratch round trips rather than on the few dozen ops of a level.
 // ---------------------------------------------------------------------------
+constexpr int kHessLineThreads = 128;
+constexpr int kHessLineH45Bytes = 45 * kHessLineThreads * (int)sizeof(double);
+
+// grad_weights with every loop over the block unrolled, so that W stays in registers
+template <int NA, int NB, int NC, int ND>
+__device__ __forceinline__ void hess_line_weights(const double* __restrict__ DJ, double cJ, int nK,
+                                                  const double* __restrict__ DK, double cK, int n, int fa, int fb,
+                                                  int fc, int fd, double s8, double* W) {
+#pragma unroll
+  for (int i = 0; i < NA; ++i)
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const double dab = DJ ? __ldg(DJ + (size_t)(fa + i) * n + fb + j) : 0.0;
+#pragma unroll
+      for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int l = 0; l < ND; ++l) {
+          double w = DJ ? cJ * dab * __ldg(DJ + (size_t)(fc + k) * n + fd + l) : 0.0;
+          for (int m = 0; m < nK; ++m) {
+            const double* D = DK + (size_t)m * n * n;
+            w -= 0.5 * cK *
+                 (__ldg(D + (size_t)(fa + i) * n + fc + k) * __ldg(D + (size_t)(fb + j) * n + fd + l) +
+                  __ldg(D + (size_t)(fa + i) * n + fd + l) * __ldg(D + (size_t)(fb + j) * n + fc + k));
+          }
+          W[((i * NB + j) * NC + k) * ND + l] = s8 * w;
+        }
+    }
+}
+
 template <int LA, int LB, int LC, int LD, bool PURE, typename Line>
-__device__ __forceinline__ void hess_line_quartet(const GradArgs<double>& a, const int2 pq, double* hout, int n3) {
+__device__ __forceinline__ void hess_line_quartet(const GradArgs<double>& a, const int2 pq, Strided<double> h45,
+                                                  double* hout, int n3) {
   using Dm = BlockDims<LA, LB, LC, LD, PURE>;
   const PairInfo P = a.pairs[pq.x];
   const PairInfo Q = a.pairs[pq.y];
@@ -257,39 +289,47 @@ __device__ __forceinline__ void hess_line_quartet(const GradArgs<double>& a, con
   auto weights = [&](double* Wc) {
     if constexpr (PURE) {
       double Wp[Dm::NOUT];
-      grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb, Q.fa, Q.fb, s, Wp);
+      hess_line_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb, Q.fa, Q.fb, s,
+                                                        Wp);
       ClassCode<LA, LB, LC, LD>::template from_pure<double>(Wp, Wc);
     } else {
-      grad_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb, Q.fa, Q.fb, s, Wc);
+      hess_line_weights<Dm::NA, Dm::NB, Dm::NC, Dm::ND>(a.DJ, a.cJ, a.nK, a.DK, a.cK, a.n, P.fa, P.fb, Q.fa, Q.fb, s,
+                                                        Wc);
     }
   };
-  const int at[4] = {P.atom_a, P.atom_b, Q.atom_a, Q.atom_b};
-  auto scatter = [&](const double* h45) { hess_add_block(h45, at, hout, n3); };
+#pragma unroll
+  for (int x = 0; x < 45; ++x) h45[x] = 0.0;
   Line::template run<double>(a.prims + P.prim_off, a.alpha_a + P.prim_off, a.alpha_b + P.prim_off, P.nprim,
                              a.prims + Q.prim_off, a.alpha_a + Q.prim_off, Q.nprim, P.ABx, P.ABy, P.ABz, Q.ABx,
-                             Q.ABy, Q.ABz, a.boys, weights, scatter);
+                             Q.ABy, Q.ABz, a.boys, weights, h45);
+  const int at[4] = {P.atom_a, P.atom_b, Q.atom_a, Q.atom_b};
+  hess_add_block(h45, at, hout, n3);
 }
 
+// dynamic shared memory: [the block's Hessian, 9 natoms^2 doubles, when o.smem | h45 slices]
 template <int LA, int LB, int LC, int LD, typename Line>
-__global__ void __launch_bounds__(128) hess_line_kernel(GradArgs<double> a, HessOut o, int pure,
-                                                        const int2* __restrict__ quartets, int nq) {
+__global__ void __launch_bounds__(kHessLineThreads) hess_line_kernel(GradArgs<double> a, HessOut o, int pure,
+                                                                     const int2* __restrict__ quartets, int nq) {
   extern __shared__ double hess_sh[];
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int nthr = gridDim.x * blockDim.x;
   const int n3 = 3 * o.natoms;
   double* hout = o.hess;
+  double* h45_base = hess_sh;
   if (o.smem) {
     for (int i = threadIdx.x; i < n3 * n3; i += blockDim.x) hess_sh[i] = 0.0;
     __syncthreads();
     hout = hess_sh;
+    h45_base = hess_sh + n3 * n3;
   }
+  const Strided<double> h45{h45_base + threadIdx.x, kHessLineThreads};
   const int np = a.nparts > 1 ? a.nparts : 1, p0 = np > 1 ? a.part : 0;
   for (int t = tid; t < nq; t += nthr) {
     const int2 pq = quartets[(size_t)t * np + p0];
     if (pure)
-      hess_line_quartet<LA, LB, LC, LD, true, Line>(a, pq, hout, n3);
+      hess_line_quartet<LA, LB, LC, LD, true, Line>(a, pq, h45, hout, n3);
     else
-      hess_line_quartet<LA, LB, LC, LD, false, Line>(a, pq, hout, n3);
+      hess_line_quartet<LA, LB, LC, LD, false, Line>(a, pq, h45, hout, n3);
   }
   if (o.smem) {
     __syncthreads();

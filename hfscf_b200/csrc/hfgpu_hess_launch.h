@@ -25,7 +25,8 @@ struct HessLaunchers {
   // quartets' tables do not fit one block's shared memory
   bool (*launch_warp)(const GradArgs<double>&, const HessOut&, int pure, const int2* q, int nq, cudaStream_t);
   // straight-line form (hess_line_kernel, one thread per quartet on register code, grid blocks of
-  // 128 threads, smem bytes of dynamic shared memory as for launch); false when the class has none
+  // 128 threads; smem as for launch, to which the launcher adds the threads' 45-entry slices);
+  // false when the class has none
   bool has_line;
   bool (*launch_line)(const GradArgs<double>&, const HessOut&, int pure, const int2* q, int nq, int grid, int smem,
                       cudaStream_t);

@@ -139,8 +139,8 @@ int hfgpu_grad2e_uhf_backward(hfgpu_handle* h, const double* Da, const double* D
 int hfgpu_hess2e(hfgpu_handle* h, const double* D, double scale, double* hess);
 int hfgpu_hess2e_uhf(hfgpu_handle* h, const double* Da, const double* Db, double scale, double* hess);
 /* Launch form of the Hessian classes: -1 (default) one thread per quartet on straight-line
- * register code for the small classes that have it ((ss|ss), (ps|ss), (ps|ps), (pp|ss), (ds|ss):
- * the classes whose weight sets need at most 64 accumulators each), else one block of 128
+ * register code for the many-quartet classes that have it ((ss|ss), (ps|ss), (ps|ps), (pp|ss),
+ * (pp|ps), (ds|ss), (ds|ps), (dp|ss)), else one block of 128
  * threads per quartet for the classes with large op tables or few quartets and one warp per
  * quartet for the others; 0 one thread per quartet on global scratch everywhere, 1 one block per
  * quartet everywhere, 2 one warp per quartet wherever four quartets' tables fit one block (the

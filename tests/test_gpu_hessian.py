@@ -172,9 +172,10 @@ def test_hess2e_autotuned_forms_match_default():
     bs = B.build_basis("6-31g*", Z, np.asarray(x) * B.ANGSTROM_TO_BOHR, pure=False)
     rng = np.random.default_rng(8)
     D = _sym(rng, bs.nbf, 0.3)
-    # class order of a handle: (ss|ss), (ps|ss), (ps|ps), (pp|ss), (pp|ps), (pp|pp), (ds|ss), ...;
-    # the classes with a straight-line form are (ss|ss), (ps|ss), (ps|ps), (pp|ss) and (ds|ss)
-    line_classes = {0, 1, 2, 3, 6}
+    # class order of a handle: (ss|ss), (ps|ss), (ps|ps), (pp|ss), (pp|ps), (pp|pp), (ds|ss),
+    # (ds|ps), (ds|pp), (ds|ds), (dp|ss), ...; the classes with a straight-line form are
+    # (ss|ss), (ps|ss), (ps|ps), (pp|ss), (pp|ps), (ds|ss), (ds|ps) and (dp|ss)
+    line_classes = {0, 1, 2, 3, 4, 6, 7, 10}
     with E.Engine(bs, density_tol=0.0) as eng:
         H0 = eng.hess2e(D)
         forms = eng.autotune_hess(D, repeats=1)
