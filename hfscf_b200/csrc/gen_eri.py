@@ -2245,6 +2245,10 @@ def gen_hess_line(la, lb, lc, ld):
     accumulators lives through its primitive loops.  None when a unit still needs more than
     HESS_LINE_PASS_ACC accumulators or the class more than HESS_LINE_MAX_PASSES passes."""
     terms = hess_terms(la, lb, lc, ld)
+    # the sets share no accumulators, so the passes number at least their total over the pass size
+    total = sum(len(hess_term_needs([t for t in terms if t[3] == k])) for k in range(len(HESS_SETS)))
+    if total > HESS_LINE_MAX_PASSES * HESS_LINE_PASS_ACC:
+        return None, None
     passes = hess_line_passes(la, lb, lc, ld, terms)
     if len(passes) > HESS_LINE_MAX_PASSES or max(len(u[2]) for p in passes for u in p) > HESS_LINE_PASS_ACC:
         return None, None

@@ -287,6 +287,35 @@ def test_hessian_generator_second_derivative_rule_pointwise():
             assert abs(rule[wi, hi] - fd) < 1e-5 * max(1.0, abs(fd)), (comps, r, s, rule[wi, hi], fd)
 
 
+def test_hessian_line_form_passes_cover_every_term_once():
+    """The straight-line Hessian form (gen_eri.gen_hess_line) cuts the contraction terms into
+    units and packs them into passes; together the passes must hold every term of hess_terms
+    exactly once, each pass at most HESS_LINE_PASS_ACC accumulators, each unit's accumulators
+    exactly the [e0|f0] values its own HRR reads.  The classes that get the form are the eight
+    many-quartet classes the C header names."""
+    g = _gen_eri()
+    _, cls = g.classes()
+    with_line = []
+    for c in cls:
+        terms = g.hess_terms(*c)
+        code, meta = g.gen_hess_line(*c)
+        if code is None:
+            continue
+        with_line.append(tuple(c))
+        passes = g.hess_line_passes(*c, terms)
+        assert len(passes) == len(meta["passes"]) <= g.HESS_LINE_MAX_PASSES
+        seen = sorted(t for p in passes for _, tl, _ in p for t in tl)
+        assert seen == sorted(terms)
+        for p, m in zip(passes, meta["passes"]):
+            keys = {(k,) + ef for k, _, need in p for ef in need}
+            assert len(keys) == m["accumulators"] <= g.HESS_LINE_PASS_ACC
+            for k, tl, need in p:
+                assert all(t[3] == k for t in tl)
+                assert sorted(need) == sorted(g.hess_term_needs(tl))
+    assert with_line == [(0, 0, 0, 0), (1, 0, 0, 0), (1, 0, 1, 0), (1, 1, 0, 0), (1, 1, 1, 0),
+                         (2, 0, 0, 0), (2, 0, 1, 0), (2, 1, 0, 0)]
+
+
 class _OracleAtomEngine:
     """Stand-in for an atom's GPU engine in the SAD guess: S, T, V from the reference's own
     one-electron routines and J/K from the C restatement's packed ERIs (host only)."""
